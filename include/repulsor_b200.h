@@ -1,0 +1,171 @@
+/*
+ * repulsor_b200 -- C ABI of the B200 implementation of Repulsor's multipole-
+ * accelerated tangent-point path.
+ *
+ * One `rpb_mesh` replaces a Repulsor `SimplicialMesh` together with its cached
+ * ClusterTree / BlockClusterTree and the metric-value cache. All arrays in these
+ * signatures are plain host pointers unless the function name ends in `_device`
+ * (device pointers on the mesh's CUDA stream). Every function returns an
+ * `rpb_status`; `rpb_last_error` gives the message of the last failure.
+ *
+ * Citations name the reference interface each entry point replaces
+ * (paths inside HenrikSchumacher/Repulsor).
+ */
+#ifndef REPULSOR_B200_H
+#define REPULSOR_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum rpb_status {
+    RPB_OK = 0,
+    RPB_EINVAL = 1,      /* invalid argument (the reference prints via eprint and does nothing) */
+    RPB_ENOTCONV = 2,    /* solver reached max_iter above the tolerance */
+    RPB_ESTALL = 3,      /* solver stagnated */
+    RPB_ECUDA = 4,       /* CUDA runtime error */
+    RPB_ENOMEM = 5,      /* device allocation failed */
+    RPB_ETIMEOUT = 6     /* a bounded device-side wait gave up */
+} rpb_status;
+
+typedef struct rpb_mesh rpb_mesh;
+
+/* ClusterTreeSettings / BlockClusterTreeSettings / AdaptivitySettings
+ * (src/Settings.hpp:5-54, overrides of src/SimplicialMesh.hpp:592-595). */
+typedef struct rpb_settings {
+    int    split_threshold;          /* only 1 is supported (the reference default) */
+    double far_field_separation;     /* theta of the AABB MAC, default 0.5 */
+    double near_field_separation;    /* AdaptivitySettings::theta, default 10 */
+    double near_field_intersection;  /* AdaptivitySettings::intersection_theta, default 1e10 (unused by the
+                                        classification, which the reference also ties to theta) */
+    int    max_refinement;           /* very-near subdivision limit, default 30 */
+    int    thread_count;             /* host threads for the tree build (0 = hardware concurrency) */
+    int    device;                   /* CUDA device ordinal */
+} rpb_settings;
+
+typedef struct rpb_stats {
+    int64_t vertex_count;
+    int64_t simplex_count;
+    int64_t cluster_count;
+    int64_t tree_depth;
+    int64_t near_nnz;                /* full symmetric storage (both triangles) */
+    int64_t far_nnz;
+    int64_t verynear_nnz;
+    int64_t inter_nnz;
+    double  tree_build_seconds;
+    int64_t device_bytes;            /* device memory held by the mesh */
+} rpb_stats;
+
+/* Fills `s` with the reference defaults. */
+rpb_status rpb_default_settings(rpb_settings* s);
+
+/* Last error message of this thread ("" if none). */
+const char* rpb_last_error(void);
+
+/* --- mesh ------------------------------------------------------------------------------- */
+
+/* SimplicialMesh(V, nV, S, nS[, charges]) (src/SimplicialMesh.hpp:154-220) followed by
+ * GetClusterTree()/GetBlockClusterTree() (src/SimplicialMesh.hpp:470-607): builds the
+ * cluster tree and the block cluster tree on the host (frozen coordinates) and uploads
+ * them. V: nV x amb_dim row-major doubles; S: nS x (dom_dim+1) row-major ints;
+ * charges: nV doubles or NULL (all ones). Only amb_dim = 3 and dom_dim in {1,2}. */
+rpb_status rpb_mesh_create(int dom_dim, int amb_dim, const double* V, int64_t nV, const int* S, int64_t nS,
+                           const double* charges, const rpb_settings* settings, rpb_mesh** out);
+
+rpb_status rpb_mesh_destroy(rpb_mesh* m);
+
+rpb_status rpb_mesh_stats(const rpb_mesh* m, rpb_stats* out);
+
+/* CUDA stream used by all work of this mesh (a cudaStream_t passed as void*).
+ * set: the caller keeps ownership of `stream`; NULL restores the mesh's own stream.
+ * No reference counterpart: Repulsor runs on host threads only. */
+rpb_status rpb_mesh_set_stream(rpb_mesh* m, void* stream);
+rpb_status rpb_mesh_get_stream(const rpb_mesh* m, void** stream);
+
+/* SimplicialMesh::SemiStaticUpdate (src/SimplicialMesh.hpp:354-376): new coordinates,
+ * same tree and pair lists; recomputes primitive data and the cluster moment upsweep.
+ * transp != 0 reads V column-major (3 x nV). */
+rpb_status rpb_mesh_semistatic_update(rpb_mesh* m, const double* V, int transp);
+rpb_status rpb_mesh_semistatic_update_device(rpb_mesh* m, const double* V_dev);
+
+/* Tree inspection (ClusterTree::PrimitiveOrdering/ClusterBegin/End/Left/Right,
+ * src/ClusterTree/ClusterTreeBase.hpp:298-578). Arrays sized simplex_count / cluster_count. */
+rpb_status rpb_mesh_tree(const rpb_mesh* m, int* perm, int* C_begin, int* C_end, int* C_left, int* C_right);
+
+/* BlockClusterTree patterns Near()/Far()/VeryNear()/PrimitiveIntersectionMatrix()
+ * (src/BlockClusterTree.hpp:161-179). which: 0 near, 1 far, 2 very-near, 3 intersecting.
+ * rowptr: rows+1 entries, colidx: nnz entries (full symmetric CSR, sorted). */
+rpb_status rpb_mesh_pattern(const rpb_mesh* m, int which, int64_t* rowptr, int* colidx);
+
+/* --- host-only tree construction ---------------------------------------------------------- */
+
+/* ClusterTree + BlockClusterTree construction alone, without a device (the host half of
+ * SimplicialMesh::GetClusterTree/GetBlockClusterTree, src/SimplicialMesh.hpp:470-607;
+ * ClusterTree ctor src/ClusterTree.hpp:115-180; BlockClusterTree::ComputeBlocks
+ * src/BlockClusterTree.hpp:234-330). Used to inspect and cross-check tree parity. */
+typedef struct rpb_host_tree rpb_host_tree;
+rpb_status rpb_tree_build_host(int dom_dim, const double* V, int64_t nV, const int* S, int64_t nS,
+                               const rpb_settings* settings, rpb_host_tree** out);
+rpb_status rpb_tree_host_stats(const rpb_host_tree* t, rpb_stats* out);
+rpb_status rpb_tree_host_arrays(const rpb_host_tree* t, int* perm, int* C_begin, int* C_end, int* C_left,
+                                int* C_right);
+rpb_status rpb_tree_host_pattern(const rpb_host_tree* t, int which, int64_t* rowptr, int* colidx);
+rpb_status rpb_tree_host_destroy(rpb_host_tree* t);
+
+/* SimplicialMesh::H1Solver().Solve on the host (src/SimplicialMesh/H1Metric.hpp:208-257):
+ * X = H1^{-1} B with H1 = stiffness + mass of the given coordinates, factorized by the
+ * same nested-dissection-ordered sparse Cholesky the GPU preconditioner uploads.
+ * B, X: nV x nrhs row-major. */
+rpb_status rpb_h1_solve_host(const rpb_host_tree* t, const double* V, const int* S, const double* B, double* X,
+                             int nrhs);
+
+/* --- TangentPointEnergy0 (src/Energies/TangentPointEnergy0.hpp:35-86) -------------------- */
+
+/* EnergyBase::Value (src/Energies/EnergyBase.hpp:40-56). */
+rpb_status rpb_tpe0_value(rpb_mesh* m, double q, double p, double* energy);
+
+/* EnergyBase::Differential(M, alpha, beta, Y, ldY) (src/Energies/EnergyBase.hpp:90-104):
+ * Y = alpha * dE + beta * Y, Y: nV x ldY host doubles; returns the energy. */
+rpb_status rpb_tpe0_differential(rpb_mesh* m, double q, double p, double alpha, double beta, double* Y, int ldY,
+                                 double* energy);
+
+/* Same with Y a device pointer (nV x ldY) on the mesh stream; energy written to host. */
+rpb_status rpb_tpe0_differential_device(rpb_mesh* m, double q, double p, double alpha, double beta, double* Y_dev,
+                                        int ldY, double* energy);
+
+/* --- TangentPointMetric0 (src/Metrics/TangentPointMetric0.hpp:57-126) ---------------------- */
+
+/* MetricBase::MultiplyMetric (src/Metrics/MetricDimRestricted.hpp:109-139):
+ * Y = alpha * A X + beta * Y with nrhs = 3; flags: bit0 VF, bit1 NF, bit2 FF. */
+rpb_status rpb_tpm0_multiply(rpb_mesh* m, double q, double p, double alpha, const double* X, int ldX, double beta,
+                             double* Y, int ldY, int nrhs, int flags);
+rpb_status rpb_tpm0_multiply_device(rpb_mesh* m, double q, double p, double alpha, const double* X_dev, int ldX,
+                                    double beta, double* Y_dev, int ldY, int nrhs, int flags);
+
+/* MetricBase::MultiplyPreconditioner (src/Metrics/TangentPointMetric0.hpp:88-126):
+ * Y = alpha * H1^{-1} L_{2-s} H1^{-1} X + beta * Y. */
+rpb_status rpb_tpm0_precondition(rpb_mesh* m, double q, double p, double alpha, const double* X, int ldX,
+                                 double beta, double* Y, int ldY, int nrhs);
+
+/* Preconditioner kinds for rpb_tpm0_solve. */
+typedef enum rpb_precond {
+    RPB_PRECOND_NONE = 0,        /* plain CG */
+    RPB_PRECOND_REFERENCE = 1,   /* H1^{-1} L_{2-s} H1^{-1} (the reference's preconditioner) */
+    RPB_PRECOND_LEARNED = 2      /* per-cluster MLP in flexible CG, falls back to REFERENCE on stall */
+} rpb_precond;
+
+/* MetricBase::Solve (src/Metrics/MetricDimRestricted.hpp:232-289):
+ * X = alpha * A^{-1} B + beta * X by (flexible) preconditioned CG with FP64 inner
+ * products; stops when the true relative residual of every column is <= tol.
+ * iterations / rel_residual (3 entries) may be NULL. */
+rpb_status rpb_tpm0_solve(rpb_mesh* m, double q, double p, double alpha, const double* B, int ldB, double beta,
+                          double* X, int ldX, int nrhs, int max_iter, double tol, int precond, int* iterations,
+                          double* rel_residual);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* REPULSOR_B200_H */

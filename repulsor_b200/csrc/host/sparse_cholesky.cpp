@@ -1,0 +1,263 @@
+// H1 metric, nested-dissection ordering and up-looking sparse Cholesky (host).
+#include "sparse_cholesky.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+
+namespace rpb {
+
+CsrMatrix assemble_h1(int dom, const double* V, int nV, const int* S, int N, double ws, double wm)
+{
+    const int size = dom + 1;
+    const double std_vol = (dom == 1) ? 1.0 : 0.5;       // 1/n!
+    const double fact = (dom == 1) ? 6.0 : 24.0;         // (n+2)!
+    const double m_factor = wm / (std_vol * fact);
+    // triplets per simplex, then a row-wise merge
+    std::vector<int64_t> cnt(static_cast<size_t>(nV) + 1, 0);
+    for (int64_t k = 0; k < static_cast<int64_t>(N) * size; ++k) cnt[S[k] + 1] += size;
+    for (int v = 0; v < nV; ++v) cnt[v + 1] += cnt[v];
+    std::vector<int> tj(static_cast<size_t>(cnt[nV]));
+    std::vector<double> tv(static_cast<size_t>(cnt[nV]));
+    std::vector<int64_t> pos(cnt.begin(), cnt.end() - 1);
+    for (int k = 0; k < N; ++k) {
+        const int* s = S + static_cast<int64_t>(size) * k;
+        double df[3][2];
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < dom; ++j) df[i][j] = V[3 * static_cast<int64_t>(s[j + 1]) + i] - V[3 * static_cast<int64_t>(s[0]) + i];
+        double g[2][2] = {{0, 0}, {0, 0}};
+        for (int a = 0; a < dom; ++a)
+            for (int b = 0; b < dom; ++b)
+                for (int i = 0; i < 3; ++i) g[a][b] += df[i][a] * df[i][b];
+        double a = std_vol, ginv[2][2] = {{0, 0}, {0, 0}};
+        if (dom == 1) {
+            a *= std::sqrt(g[0][0]);
+            ginv[0][0] = 1.0 / g[0][0];
+        } else {
+            const double det = g[0][0] * g[1][1] - g[0][1] * g[1][0];
+            a *= std::sqrt(det);
+            ginv[0][0] = g[1][1] / det;
+            ginv[1][1] = g[0][0] / det;
+            ginv[0][1] = ginv[1][0] = -g[0][1] / det;
+        }
+        double val[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+        const double lf = a * ws;
+        for (int i = 0; i < dom; ++i)
+            for (int j = 0; j < dom; ++j) {
+                const double aij = lf * ginv[i][j];
+                val[0][0] += aij;
+                val[i + 1][0] -= aij;
+                val[0][j + 1] -= aij;
+                val[i + 1][j + 1] = aij;
+            }
+        for (int i = 0; i < size; ++i)
+            for (int j = 0; j < size; ++j) val[i][j] += a * m_factor * (1.0 + (i == j ? 1.0 : 0.0));
+        for (int i = 0; i < size; ++i)
+            for (int j = 0; j < size; ++j) {
+                const int64_t p = pos[s[i]]++;
+                tj[p] = s[j];
+                tv[p] = val[i][j];
+            }
+    }
+    CsrMatrix A;
+    A.n = nV;
+    A.rp.assign(static_cast<size_t>(nV) + 1, 0);
+    std::vector<std::pair<int, double>> row;
+    for (int r = 0; r < nV; ++r) {
+        row.clear();
+        for (int64_t p = cnt[r]; p < cnt[r + 1]; ++p) row.emplace_back(tj[p], tv[p]);
+        std::sort(row.begin(), row.end(), [](const auto& x, const auto& y) { return x.first < y.first; });
+        for (size_t q = 0; q < row.size(); ++q) {
+            if (!A.ci.empty() && static_cast<int64_t>(A.ci.size()) > A.rp[r] && A.ci.back() == row[q].first) {
+                A.val.back() += row[q].second;
+            } else {
+                A.ci.push_back(row[q].first);
+                A.val.push_back(row[q].second);
+            }
+        }
+        A.rp[r + 1] = static_cast<int64_t>(A.ci.size());
+    }
+    return A;
+}
+
+// NestedDissectionOrdering (src/SimplicialMesh/NestedDissectionOrdering.hpp:3-207): at
+// each tree level the vertices of a cluster's range are grouped into those touching
+// only left-child primitives, only right-child primitives, and both (separator, last).
+std::vector<int> nested_dissection_ordering(const HostTree& T, const int* S, int nV)
+{
+    const int N = T.N, size = T.size;
+    std::vector<int> perm0(nV), perm1(nV);
+    for (int i = 0; i < nV; ++i) perm0[i] = i;
+    std::vector<int> Vb(T.NC, 0), Ve(T.NC, 0);
+    Vb[0] = 0;
+    Ve[0] = nV;
+    std::vector<int> queue0{0}, queue1;
+    std::vector<unsigned char> vL(N), vR(N), wL(nV), wR(nV);
+    std::vector<signed char> type(nV);
+    while (!queue0.empty()) {
+        queue1.clear();
+        perm1 = perm0;
+        std::fill(vL.begin(), vL.end(), 0);
+        std::fill(vR.begin(), vR.end(), 0);
+        for (int C : queue0) {
+            const int L = T.C_left[C], R = T.C_right[C];
+            if (L < 0) continue;
+            for (int i = T.C_begin[L]; i < T.C_end[L]; ++i) vL[i] = 1;
+            for (int i = T.C_begin[R]; i < T.C_end[R]; ++i) vR[i] = 1;
+        }
+        std::fill(wL.begin(), wL.end(), 0);
+        std::fill(wR.begin(), wR.end(), 0);
+        for (int i = 0; i < N; ++i) {
+            if (!vL[i] && !vR[i]) continue;
+            const int* s = S + static_cast<int64_t>(size) * T.perm[i];
+            for (int l = 0; l < size; ++l) {
+                if (vL[i]) wL[s[l]] = 1;
+                if (vR[i]) wR[s[l]] = 1;
+            }
+        }
+        for (int i = 0; i < nV; ++i) {
+            const int j = perm0[i];
+            type[i] = static_cast<signed char>(-1 + (wL[j] ? 1 : 0) + (wR[j] ? 2 : 0));
+        }
+        for (int C : queue0) {
+            const int L = T.C_left[C], R = T.C_right[C];
+            if (L < 0) continue;
+            const int ib = Vb[C], ie = Ve[C];
+            int ctr[3] = {0, 0, 0};
+            for (int i = ib; i < ie; ++i)
+                if (type[i] >= 0) ++ctr[type[i]];
+            int pos[4];
+            pos[0] = ib;
+            pos[1] = pos[0] + ctr[0];
+            pos[2] = pos[1] + ctr[1];
+            pos[3] = pos[2] + ctr[2];
+            if (ctr[0] > 0 && ctr[1] > 0 && pos[3] == ie) {
+                Vb[L] = pos[0]; Ve[L] = pos[1];
+                Vb[R] = pos[1]; Ve[R] = pos[2];
+                queue1.push_back(L);
+                queue1.push_back(R);
+                for (int i = ib; i < ie; ++i) {
+                    const int t = type[i];
+                    if (t >= 0) perm1[pos[t]++] = perm0[i];
+                }
+            }
+        }
+        queue0.swap(queue1);
+        perm0.swap(perm1);
+    }
+    return perm0;
+}
+
+std::string cholesky_factor(const CsrMatrix& A, const std::vector<int>& perm, CholeskyFactor& F)
+{
+    const int n = A.n;
+    std::vector<int> pinv(n);
+    for (int i = 0; i < n; ++i) pinv[perm[i]] = i;
+    // upper triangle of C = P A P^T in CSC (column j: rows i <= j)
+    std::vector<int64_t> Cp(static_cast<size_t>(n) + 1, 0);
+    for (int r = 0; r < n; ++r)
+        for (int64_t p = A.rp[r]; p < A.rp[r + 1]; ++p) {
+            const int i = pinv[r], j = pinv[A.ci[p]];
+            if (i <= j) Cp[j + 1]++;
+        }
+    for (int j = 0; j < n; ++j) Cp[j + 1] += Cp[j];
+    std::vector<int> Ci(static_cast<size_t>(Cp[n]));
+    std::vector<double> Cx(static_cast<size_t>(Cp[n]));
+    {
+        std::vector<int64_t> pos(Cp.begin(), Cp.end() - 1);
+        for (int r = 0; r < n; ++r)
+            for (int64_t p = A.rp[r]; p < A.rp[r + 1]; ++p) {
+                const int i = pinv[r], j = pinv[A.ci[p]];
+                if (i <= j) {
+                    Ci[pos[j]] = i;
+                    Cx[pos[j]++] = A.val[p];
+                }
+            }
+    }
+    // elimination tree
+    std::vector<int> parent(n, -1), ancestor(n, -1);
+    for (int k = 0; k < n; ++k)
+        for (int64_t p = Cp[k]; p < Cp[k + 1]; ++p) {
+            int i = Ci[p];
+            while (i != -1 && i < k) {
+                const int inext = ancestor[i];
+                ancestor[i] = k;
+                if (inext == -1) parent[i] = k;
+                i = inext;
+            }
+        }
+    // row patterns (ereach) -> column counts
+    std::vector<int> mark(n, -1), stack(n);
+    auto ereach = [&](int k, int* s) {
+        int top = n;
+        mark[k] = k;
+        for (int64_t p = Cp[k]; p < Cp[k + 1]; ++p) {
+            int i = Ci[p];
+            if (i > k) continue;
+            int len = 0;
+            for (; mark[i] != k; i = parent[i]) {
+                s[len++] = i;
+                mark[i] = k;
+            }
+            while (len > 0) s[--top] = s[--len];
+        }
+        return top;
+    };
+    std::vector<int64_t> colcount(n, 1);
+    for (int k = 0; k < n; ++k) {
+        const int top = ereach(k, stack.data());
+        for (int q = top; q < n; ++q) colcount[stack[q]]++;
+    }
+    std::vector<int64_t> Lp(static_cast<size_t>(n) + 1, 0);
+    for (int j = 0; j < n; ++j) Lp[j + 1] = Lp[j] + colcount[j];
+    std::vector<int> Li(static_cast<size_t>(Lp[n]));
+    std::vector<double> Lx(static_cast<size_t>(Lp[n]));
+    std::vector<int64_t> c(Lp.begin(), Lp.end() - 1);
+    std::vector<double> x(n, 0.0);
+    std::fill(mark.begin(), mark.end(), -1);
+    for (int k = 0; k < n; ++k) {
+        const int top = ereach(k, stack.data());
+        x[k] = 0.0;
+        for (int64_t p = Cp[k]; p < Cp[k + 1]; ++p)
+            if (Ci[p] <= k) x[Ci[p]] = Cx[p];
+        double d = x[k];
+        x[k] = 0.0;
+        for (int q = top; q < n; ++q) {
+            const int i = stack[q];
+            const double lki = x[i] / Lx[Lp[i]];
+            x[i] = 0.0;
+            for (int64_t p = Lp[i] + 1; p < c[i]; ++p) x[Li[p]] -= Lx[p] * lki;
+            d -= lki * lki;
+            const int64_t p = c[i]++;
+            Li[p] = k;
+            Lx[p] = lki;
+        }
+        if (!(d > 0.0)) return "H1 metric is not positive definite";
+        const int64_t p = c[k]++;
+        Li[p] = k;
+        Lx[p] = std::sqrt(d);
+    }
+    // upper form = columns of L (rows of L^T), diagonal first
+    F = CholeskyFactor();
+    F.n = n;
+    F.perm = perm;
+    F.upper_rp = Lp;
+    F.upper_ci = Li;
+    F.upper_val = Lx;
+    // lower form = rows of L, diagonal last
+    F.lower_rp.assign(static_cast<size_t>(n) + 1, 0);
+    for (int64_t p = 0; p < Lp[n]; ++p) F.lower_rp[Li[p] + 1]++;
+    for (int i = 0; i < n; ++i) F.lower_rp[i + 1] += F.lower_rp[i];
+    F.lower_ci.resize(static_cast<size_t>(Lp[n]));
+    F.lower_val.resize(static_cast<size_t>(Lp[n]));
+    std::vector<int64_t> pos(F.lower_rp.begin(), F.lower_rp.end() - 1);
+    for (int j = 0; j < n; ++j)
+        for (int64_t p = Lp[j]; p < Lp[j + 1]; ++p) {
+            const int i = Li[p];
+            F.lower_ci[pos[i]] = j;
+            F.lower_val[pos[i]++] = Lx[p];
+        }
+    return std::string();
+}
+
+}  // namespace rpb

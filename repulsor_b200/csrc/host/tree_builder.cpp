@@ -1,0 +1,553 @@
+// Host construction of the cluster tree and block cluster tree (see tree_builder.hpp).
+#include "tree_builder.hpp"
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <mutex>
+#include <thread>
+#include <utility>
+
+namespace rpb {
+namespace {
+
+constexpr int AMB = 3;
+
+struct Node {
+    int begin, end;
+    double box[7];
+    int left = -1, right = -1;
+    int desc = 1;
+    int depth = 0;
+};
+
+// --- primitives ------------------------------------------------------------
+// Serialized polytope: [r2, centre(3), hull((dom+1) x 3)], hull in the simplex's own vertex order.
+void serialize_polytope(int size, const double* V, const int* s, double* out)
+{
+    double* c = out + 1;
+    double* h = out + 1 + AMB;
+    for (int j = 0; j < size; ++j)
+        for (int k = 0; k < AMB; ++k) h[AMB * j + k] = V[AMB * static_cast<int64_t>(s[j]) + k];
+    const double w = 1.0 / size;
+    for (int k = 0; k < AMB; ++k) {
+        double acc = h[k];
+        for (int j = 1; j < size; ++j) acc += h[AMB * j + k];
+        c[k] = acc * w;
+    }
+    double r2 = 0;
+    for (int j = 0; j < size; ++j) {
+        double d = h[AMB * j] - c[0];
+        double sq = d * d;
+        for (int k = 1; k < AMB; ++k) {
+            d = h[AMB * j + k] - c[k];
+            sq += d * d;
+        }
+        r2 = std::max(r2, sq);
+    }
+    out[0] = r2;
+}
+
+void aabb_of_range(int size, int ps, const double* P, int begin, int end, double* box)
+{
+    double lo[3], hi[3];
+    for (int k = 0; k < AMB; ++k) {
+        lo[k] = std::numeric_limits<double>::max();
+        hi[k] = std::numeric_limits<double>::lowest();
+    }
+    for (int i = begin; i < end; ++i) {
+        const double* h = P + static_cast<int64_t>(ps) * i + 1 + AMB;
+        for (int j = 0; j < size; ++j)
+            for (int k = 0; k < AMB; ++k) {
+                const double x = h[AMB * j + k];
+                lo[k] = std::min(lo[k], x);
+                hi[k] = std::max(hi[k], x);
+            }
+    }
+    double r2 = 0;
+    for (int k = 0; k < AMB; ++k) {
+        const double half = 0.5 * (hi[k] - lo[k]);
+        r2 += half * half;
+        box[1 + k] = lo[k] + half;
+        box[1 + AMB + k] = half;
+    }
+    box[0] = r2;
+}
+
+struct Splitter {
+    int size, ps;
+    std::vector<int>& ord;
+    std::vector<double>& P;
+    std::vector<double> score;
+    std::vector<int> lperm, linv;
+
+    Splitter(int size_, std::vector<int>& ord_, std::vector<double>& P_)
+        : size(size_), ps(1 + AMB + size_ * AMB), ord(ord_), P(P_), score(ord_.size()), lperm(ord_.size()),
+          linv(ord_.size())
+    {}
+
+    void swap_rows(int a, int b)
+    {
+        if (a == b) return;
+        std::swap(ord[a], ord[b]);
+        std::swap_ranges(P.begin() + static_cast<int64_t>(ps) * a, P.begin() + static_cast<int64_t>(ps) * (a + 1),
+                         P.begin() + static_cast<int64_t>(ps) * b);
+    }
+
+    // Returns the split index; reorders [begin,end) in place.
+    int split(int begin, int end, const double* box)
+    {
+        int dir = 0;
+        double lmax = box[1 + AMB];
+        for (int k = 1; k < AMB; ++k)
+            if (box[1 + AMB + k] > lmax) {
+                lmax = box[1 + AMB + k];
+                dir = k;
+            }
+        const double mid = box[1 + dir];
+        int s = begin;
+        for (int i = begin; i < end; ++i) {
+            if (P[static_cast<int64_t>(ps) * i + 1 + dir] < mid) {
+                swap_rows(s, i);
+                ++s;
+            }
+        }
+        if (s == begin || s == end) {
+            // median fallback with the same permutation cycle walk as the reference
+            s = begin + (end - begin) / 2;
+            for (int i = begin; i < end; ++i) {
+                score[i] = P[static_cast<int64_t>(ps) * i + 1 + dir];
+                lperm[i] = i;
+            }
+            const double* sc = score.data();
+            std::nth_element(lperm.begin() + begin, lperm.begin() + s, lperm.begin() + end,
+                             [sc](int a, int b) { return sc[a] < sc[b]; });
+            for (int i = begin; i < end; ++i) linv[lperm[i]] = i;
+            for (int i = begin; i < end; ++i) {
+                int next = i;
+                while (linv[next] >= 0) {
+                    const int t = linv[next];
+                    swap_rows(i, t);
+                    linv[next] = -1;
+                    next = t;
+                }
+            }
+        }
+        return s;
+    }
+};
+
+// Builds the subtree rooted at nodes[0] (range already set) into `nodes`.
+void build_subtree(Splitter& sp, std::vector<Node>& nodes)
+{
+    // explicit pre-order work list; post-order pass for descendant counts
+    std::vector<int> stack{0};
+    std::vector<int> order;
+    while (!stack.empty()) {
+        const int c = stack.back();
+        stack.pop_back();
+        order.push_back(c);
+        const int b = nodes[c].begin, e = nodes[c].end;
+        if (e - b <= 1) continue;  // split_threshold = 1
+        const int s = sp.split(b, e, nodes[c].box);
+        Node L, R;
+        L.begin = b; L.end = s; L.depth = nodes[c].depth + 1;
+        R.begin = s; R.end = e; R.depth = nodes[c].depth + 1;
+        aabb_of_range(sp.size, sp.ps, sp.P.data(), b, s, L.box);
+        aabb_of_range(sp.size, sp.ps, sp.P.data(), s, e, R.box);
+        const int li = static_cast<int>(nodes.size());
+        nodes.push_back(L);
+        nodes.push_back(R);
+        nodes[c].left = li;
+        nodes[c].right = li + 1;
+        stack.push_back(li + 1);
+        stack.push_back(li);
+    }
+    for (auto it = order.rbegin(); it != order.rend(); ++it) {
+        Node& n = nodes[*it];
+        if (n.left >= 0) n.desc = 1 + nodes[n.left].desc + nodes[n.right].desc;
+    }
+}
+
+// --- exact primitive distances (segments and triangles) ----------------------
+inline double dot(const double* a, const double* b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+
+double segseg2(const double* a0, const double* a1, const double* b0, const double* b1)
+{
+    double u[3], v[3], w[3];
+    for (int k = 0; k < 3; ++k) { u[k] = a1[k] - a0[k]; v[k] = b1[k] - b0[k]; w[k] = a0[k] - b0[k]; }
+    const double A = dot(u, u), B = dot(u, v), C = dot(v, v), D = dot(u, w), E = dot(v, w);
+    auto eval = [&](double s, double t) {
+        double d2 = 0;
+        for (int k = 0; k < 3; ++k) { const double d = w[k] + s * u[k] - t * v[k]; d2 += d * d; }
+        return d2;
+    };
+    double best = std::numeric_limits<double>::max();
+    // interior critical point
+    const double den = A * C - B * B;
+    if (den > 0) {
+        const double s = (B * E - C * D) / den, t = (A * E - B * D) / den;
+        if (s >= 0 && s <= 1 && t >= 0 && t <= 1) best = eval(s, t);
+    }
+    // boundary: s in {0,1} with optimal t, t in {0,1} with optimal s
+    for (int e = 0; e < 2; ++e) {
+        const double s = e;
+        const double t = C > 0 ? std::clamp((B * s + E) / C, 0.0, 1.0) : 0.0;
+        best = std::min(best, eval(s, t));
+        const double t2 = e;
+        const double s2 = A > 0 ? std::clamp((B * t2 - D) / A, 0.0, 1.0) : 0.0;
+        best = std::min(best, eval(s2, t2));
+    }
+    return best;
+}
+
+double pointtri2(const double* p, const double* a, const double* b, const double* c)
+{
+    // projection onto the plane; inside test by barycentric coordinates, else edges
+    double e0[3], e1[3], d[3];
+    for (int k = 0; k < 3; ++k) { e0[k] = b[k] - a[k]; e1[k] = c[k] - a[k]; d[k] = p[k] - a[k]; }
+    const double a00 = dot(e0, e0), a01 = dot(e0, e1), a11 = dot(e1, e1);
+    const double b0 = dot(e0, d), b1 = dot(e1, d);
+    const double det = a00 * a11 - a01 * a01;
+    if (det > 0) {
+        const double s = (a11 * b0 - a01 * b1) / det, t = (a00 * b1 - a01 * b0) / det;
+        if (s >= 0 && t >= 0 && s + t <= 1) {
+            double d2 = 0;
+            for (int k = 0; k < 3; ++k) { const double x = d[k] - s * e0[k] - t * e1[k]; d2 += x * x; }
+            return d2;
+        }
+    }
+    return std::min({segseg2(p, p, a, b), segseg2(p, p, b, c), segseg2(p, p, c, a)});
+}
+
+bool segtri_hit(const double* p, const double* q, const double* a, const double* b, const double* c)
+{
+    double e0[3], e1[3], dir[3], n[3];
+    for (int k = 0; k < 3; ++k) { e0[k] = b[k] - a[k]; e1[k] = c[k] - a[k]; dir[k] = q[k] - p[k]; }
+    n[0] = e0[1] * e1[2] - e0[2] * e1[1];
+    n[1] = e0[2] * e1[0] - e0[0] * e1[2];
+    n[2] = e0[0] * e1[1] - e0[1] * e1[0];
+    const double den = dot(n, dir);
+    if (den == 0) return false;
+    double ap[3];
+    for (int k = 0; k < 3; ++k) ap[k] = a[k] - p[k];
+    const double t = dot(n, ap) / den;
+    if (t < 0 || t > 1) return false;
+    double x[3];
+    for (int k = 0; k < 3; ++k) x[k] = p[k] + t * dir[k] - a[k];
+    const double a00 = dot(e0, e0), a01 = dot(e0, e1), a11 = dot(e1, e1);
+    const double b0 = dot(e0, x), b1 = dot(e1, x);
+    const double det = a00 * a11 - a01 * a01;
+    if (det <= 0) return false;
+    const double s = (a11 * b0 - a01 * b1) / det, u = (a00 * b1 - a01 * b0) / det;
+    return s >= 0 && u >= 0 && s + u <= 1;
+}
+
+double tritri2(const double* A, const double* B)
+{
+    for (int e = 0; e < 3; ++e) {
+        const int f = (e + 1) % 3;
+        if (segtri_hit(A + 3 * e, A + 3 * f, B, B + 3, B + 6)) return 0.0;
+        if (segtri_hit(B + 3 * e, B + 3 * f, A, A + 3, A + 6)) return 0.0;
+    }
+    double best = std::numeric_limits<double>::max();
+    for (int v = 0; v < 3; ++v) {
+        best = std::min(best, pointtri2(A + 3 * v, B, B + 3, B + 6));
+        best = std::min(best, pointtri2(B + 3 * v, A, A + 3, A + 6));
+    }
+    for (int e = 0; e < 3; ++e)
+        for (int f = 0; f < 3; ++f)
+            best = std::min(best, segseg2(A + 3 * e, A + 3 * ((e + 1) % 3), B + 3 * f, B + 3 * ((f + 1) % 3)));
+    return best;
+}
+
+// --- pair traversal --------------------------------------------------------------
+struct PairLists {
+    std::vector<std::pair<int, int>> near, far, verynear, inter;
+};
+
+struct Traversal {
+    const HostTree& T;
+    const std::vector<double>& P;   // permuted polytopes
+    const int* S;                   // original simplices
+    int ps;
+    double far_t2, near_t2;
+
+    bool adjacent(int pi, int pj) const
+    {
+        const int* a = S + static_cast<int64_t>(T.size) * T.perm[pi];
+        const int* b = S + static_cast<int64_t>(T.size) * T.perm[pj];
+        for (int u = 0; u < T.size; ++u)
+            for (int v = 0; v < T.size; ++v)
+                if (a[u] == b[v]) return true;
+        return false;
+    }
+
+    void leaf(int pi, int pj, PairLists& out) const  // pi < pj
+    {
+        if (adjacent(pi, pj)) { out.near.emplace_back(pi, pj); return; }
+        const double* A = P.data() + static_cast<int64_t>(ps) * pi;
+        const double* B = P.data() + static_cast<int64_t>(ps) * pj;
+        const double tol = std::max(A[0], B[0]);
+        // cheap separation certificate from the bounding balls
+        double cc = 0;
+        for (int k = 0; k < AMB; ++k) { const double d = A[1 + k] - B[1 + k]; cc += d * d; }
+        const double lb = std::sqrt(cc) - std::sqrt(A[0]) - std::sqrt(B[0]);
+        if (lb > 0 && near_t2 * lb * lb > tol) { out.near.emplace_back(pi, pj); return; }
+        const double d2 = (T.dom == 1) ? segseg2(A + 4, A + 7, B + 4, B + 7) : tritri2(A + 4, B + 4);
+        if (near_t2 * d2 > tol) { out.near.emplace_back(pi, pj); return; }
+        const double tol_i = std::numeric_limits<double>::epsilon() * std::min(A[0], B[0]);
+        if (near_t2 * d2 <= tol_i) out.inter.emplace_back(pi, pj);
+        else out.verynear.emplace_back(pi, pj);
+    }
+
+    bool admissible(int i, int j) const
+    {
+        if (i == j) return false;
+        const double* a = &T.C_box[7 * static_cast<int64_t>(i)];
+        const double* b = &T.C_box[7 * static_cast<int64_t>(j)];
+        double d2 = 0;
+        for (int k = 0; k < AMB; ++k) {
+            const double lo = std::max(a[1 + k] - a[4 + k], b[1 + k] - b[4 + k]);
+            const double hi = std::min(a[1 + k] + a[4 + k], b[1 + k] + b[4 + k]);
+            const double x = std::max(0.0, lo - hi);
+            d2 += x * x;
+        }
+        return std::max(a[0], b[0]) < far_t2 * d2;
+    }
+
+    // Processes one block pair; pushes children (in the reference's push order) to `next`.
+    template <typename Push>
+    void step(int i, int j, PairLists& out, Push&& push) const
+    {
+        if (admissible(i, j)) {
+            if (i <= j) out.far.emplace_back(i, j); else out.far.emplace_back(j, i);
+            return;
+        }
+        const int Li = T.C_left[i], Lj = T.C_left[j];
+        if (Li >= 0 || Lj >= 0) {
+            const int Ri = T.C_right[i], Rj = T.C_right[j];
+            const double si = Li >= 0 ? T.C_box[7 * static_cast<int64_t>(i)] : 0.0;
+            const double sj = Lj >= 0 ? T.C_box[7 * static_cast<int64_t>(j)] : 0.0;
+            if (si == sj && si > 0) {
+                if (i == j) { push(Li, Rj); push(Ri, Rj); push(Li, Lj); }
+                else { push(Ri, Rj); push(Li, Rj); push(Ri, Lj); push(Li, Lj); }
+            } else if (si > sj) {
+                push(Ri, j); push(Li, j);
+            } else {
+                push(i, Rj); push(i, Lj);
+            }
+            return;
+        }
+        if (i == j) return;
+        const int ii = T.C_begin[i], jj = T.C_begin[j];
+        if (ii < jj) leaf(ii, jj, out); else leaf(jj, ii, out);
+    }
+
+    void dfs(int i0, int j0, PairLists& out) const
+    {
+        std::vector<std::pair<int, int>> stack;
+        stack.reserve(1024);
+        stack.emplace_back(i0, j0);
+        while (!stack.empty()) {
+            auto [i, j] = stack.back();
+            stack.pop_back();
+            step(i, j, out, [&](int a, int b) { stack.emplace_back(a, b); });
+        }
+    }
+};
+
+SymPattern to_pattern(int rows, std::vector<PairLists>& parts, std::vector<std::pair<int, int>> PairLists::*member)
+{
+    SymPattern P;
+    P.rows = rows;
+    P.rp.assign(static_cast<size_t>(rows) + 1, 0);
+    for (auto& pl : parts)
+        for (auto& e : pl.*member) { P.rp[e.first + 1]++; P.rp[e.second + 1]++; }
+    for (int i = 0; i < rows; ++i) P.rp[i + 1] += P.rp[i];
+    P.ci.resize(static_cast<size_t>(P.rp[rows]));
+    std::vector<int64_t> pos(P.rp.begin(), P.rp.end() - 1);
+    for (auto& pl : parts)
+        for (auto& e : pl.*member) {
+            P.ci[pos[e.first]++] = e.second;
+            P.ci[pos[e.second]++] = e.first;
+        }
+    P.diag.resize(rows);
+    for (int i = 0; i < rows; ++i) {
+        auto b = P.ci.begin() + P.rp[i], e = P.ci.begin() + P.rp[i + 1];
+        std::sort(b, e);
+        P.diag[i] = std::upper_bound(b, e, i) - P.ci.begin();
+    }
+    return P;
+}
+
+template <typename F>
+void run_threads(int n, F&& f)
+{
+    if (n <= 1) { f(0); return; }
+    std::vector<std::thread> th;
+    for (int t = 0; t < n; ++t) th.emplace_back([&, t] { f(t); });
+    for (auto& x : th) x.join();
+}
+
+}  // namespace
+
+std::string build_tree(int dom, const double* V, int nV, const int* S, int N, const TreeSettings& set,
+                       HostTree& T)
+{
+    if (dom != 1 && dom != 2) return "domain dimension must be 1 or 2";
+    if (nV <= 0 || N <= 0) return "empty mesh";
+    const int size = dom + 1;
+    for (int64_t k = 0; k < static_cast<int64_t>(N) * size; ++k)
+        if (S[k] < 0 || S[k] >= nV) return "simplex vertex index out of range";
+    for (int64_t k = 0; k < 3 * static_cast<int64_t>(nV); ++k)
+        if (!std::isfinite(V[k])) return "non-finite vertex coordinate";
+    const int threads = std::max(1, set.threads);
+
+    T = HostTree();
+    T.dom = dom;
+    T.size = size;
+    T.nV = nV;
+    T.N = N;
+    const int ps = 1 + AMB + size * AMB;
+    std::vector<double> P(static_cast<size_t>(N) * ps);
+    for (int i = 0; i < N; ++i) serialize_polytope(size, V, S + static_cast<int64_t>(size) * i, &P[static_cast<size_t>(ps) * i]);
+    std::vector<int> ord(N);
+    for (int i = 0; i < N; ++i) ord[i] = i;
+
+    // --- split: top levels breadth-first, then independent subtrees in parallel
+    std::vector<Node> top;
+    top.reserve(256);
+    Node root;
+    root.begin = 0; root.end = N; root.depth = 0;
+    aabb_of_range(size, ps, P.data(), 0, N, root.box);
+    top.push_back(root);
+    Splitter sp0(size, ord, P);
+    std::vector<int> frontier{0};
+    const int want = 8 * threads;
+    while (static_cast<int>(frontier.size()) < want) {
+        std::vector<int> next;
+        bool any = false;
+        for (int c : frontier) {
+            const int b = top[c].begin, e = top[c].end;
+            if (e - b <= 1) { next.push_back(c); continue; }
+            any = true;
+            const int s = sp0.split(b, e, top[c].box);
+            Node L, R;
+            L.begin = b; L.end = s; L.depth = top[c].depth + 1;
+            R.begin = s; R.end = e; R.depth = top[c].depth + 1;
+            aabb_of_range(size, ps, P.data(), b, s, L.box);
+            aabb_of_range(size, ps, P.data(), s, e, R.box);
+            const int li = static_cast<int>(top.size());
+            top.push_back(L);
+            top.push_back(R);
+            top[c].left = li;
+            top[c].right = li + 1;
+            next.push_back(li);
+            next.push_back(li + 1);
+        }
+        frontier.swap(next);
+        if (!any) break;
+    }
+    // subtrees of the frontier nodes
+    std::vector<std::vector<Node>> sub(frontier.size());
+    {
+        std::atomic<int> ticket{0};
+        run_threads(threads, [&](int) {
+            Splitter sp(size, ord, P);
+            for (;;) {
+                const int f = ticket.fetch_add(1);
+                if (f >= static_cast<int>(frontier.size())) break;
+                sub[f].push_back(top[frontier[f]]);
+                build_subtree(sp, sub[f]);
+            }
+        });
+    }
+    // merge into one array: frontier subtree roots replace the frontier nodes
+    std::vector<Node> nodes = top;
+    for (size_t f = 0; f < frontier.size(); ++f) {
+        const int off = static_cast<int>(nodes.size()) - 1;  // local index l>0 -> off + l
+        Node& r = nodes[frontier[f]];
+        const Node& lr = sub[f][0];
+        r.desc = lr.desc;
+        if (lr.left >= 0) { r.left = off + lr.left; r.right = off + lr.right; }
+        for (size_t l = 1; l < sub[f].size(); ++l) {
+            Node n = sub[f][l];
+            if (n.left >= 0) { n.left += off; n.right += off; }
+            nodes.push_back(n);
+        }
+    }
+    // descendant counts of the top levels (children were appended after parents)
+    for (int c = static_cast<int>(top.size()); c-- > 0;) {
+        Node& n = nodes[c];
+        bool is_frontier = std::find(frontier.begin(), frontier.end(), c) != frontier.end();
+        if (!is_frontier && n.left >= 0) n.desc = 1 + nodes[n.left].desc + nodes[n.right].desc;
+    }
+
+    // --- depth-first serialization
+    const int NC = nodes[0].desc;
+    T.NC = NC;
+    T.C_begin.assign(NC, 0); T.C_end.assign(NC, 0); T.C_left.assign(NC, -1); T.C_right.assign(NC, -1);
+    T.C_parent.assign(NC, -1); T.C_depth.assign(NC, 0);
+    T.C_box.assign(static_cast<size_t>(NC) * 7, 0.0);
+    {
+        std::vector<std::pair<int, int>> stack{{0, 0}};  // (node, global id)
+        while (!stack.empty()) {
+            auto [c, g] = stack.back();
+            stack.pop_back();
+            const Node& n = nodes[c];
+            T.C_begin[g] = n.begin;
+            T.C_end[g] = n.end;
+            T.C_depth[g] = n.depth;
+            T.depth = std::max(T.depth, n.depth);
+            std::memcpy(&T.C_box[7 * static_cast<size_t>(g)], n.box, sizeof(n.box));
+            if (n.left >= 0) {
+                const int gl = g + 1, gr = g + 1 + nodes[n.left].desc;
+                T.C_left[g] = gl;
+                T.C_right[g] = gr;
+                T.C_parent[gl] = g;
+                T.C_parent[gr] = g;
+                stack.emplace_back(n.right, gr);
+                stack.emplace_back(n.left, gl);
+            }
+        }
+    }
+    T.perm = ord;
+    T.inv_perm.assign(N, 0);
+    for (int i = 0; i < N; ++i) T.inv_perm[ord[i]] = i;
+    T.leaf_of.assign(N, -1);
+    for (int C = 0; C < NC; ++C)
+        if (T.C_left[C] < 0)
+            for (int i = T.C_begin[C]; i < T.C_end[C]; ++i) T.leaf_of[i] = C;
+
+    // --- block cluster tree
+    Traversal tr{T, P, S, ps, set.theta_far * set.theta_far, set.theta_near * set.theta_near};
+    std::vector<std::pair<int, int>> tasks{{0, 0}};
+    std::vector<PairLists> parts(threads);
+    // breadth-first expansion into enough independent tasks
+    const size_t task_target = static_cast<size_t>(16) * threads;
+    while (!tasks.empty() && tasks.size() < task_target) {
+        std::vector<std::pair<int, int>> next;
+        for (auto [i, j] : tasks) tr.step(i, j, parts[0], [&](int a, int b) { next.emplace_back(a, b); });
+        tasks.swap(next);
+    }
+    {
+        std::atomic<size_t> ticket{0};
+        run_threads(threads, [&](int t) {
+            for (;;) {
+                const size_t k = ticket.fetch_add(1);
+                if (k >= tasks.size()) break;
+                tr.dfs(tasks[k].first, tasks[k].second, parts[t]);
+            }
+        });
+    }
+    T.near = to_pattern(N, parts, &PairLists::near);
+    T.far = to_pattern(NC, parts, &PairLists::far);
+    T.verynear = to_pattern(N, parts, &PairLists::verynear);
+    T.inter = to_pattern(N, parts, &PairLists::inter);
+    return std::string();
+}
+
+}  // namespace rpb

@@ -1,0 +1,55 @@
+// Host-side construction of Repulsor's ClusterTree and BlockClusterTree for the
+// B200 path. The tree and its pair lists are built once per mesh on the host and
+// uploaded; SemiStaticUpdate keeps them fixed (src/ClusterTree.hpp:951-993).
+//
+// Restated behaviour (citations are paths inside HenrikSchumacher/Repulsor):
+//  * primitive serialization: src/Primitives/Polytope.hpp:113-160 (frozen coordinates)
+//  * AABB from primitives:    src/BoundingVolumes/AABB.hpp:155-237
+//  * longest-axis split:      src/BoundingVolumes/AABB_LongestAxisSplit.hpp:134-253
+//    (strict x < mid partition with in-place swaps, median fallback via std::nth_element)
+//  * depth-first numbering:   src/ClusterTree/Serialize_Thread.hpp:273-314
+//  * dual-tree traversal:     src/ClusterTreePairTraversor/Traverse_DepthFirst.hpp:52-258
+//  * split kernel / MACs:     src/BlockClusterTree/BlockSplit_Kernel.hpp:164-251, src/GJK.hpp:1162-1183
+//  * symmetric CSR patterns:  src/BlockClusterTree.hpp:306-326
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace rpb {
+
+struct TreeSettings {
+    double theta_far = 0.5;         // far_field_separation_parameter (src/Settings.hpp:39)
+    double theta_near = 10.0;       // AdaptivitySettings::theta (src/Settings.hpp:52)
+    int max_refinement = 30;        // AdaptivitySettings::max_refinement (src/Settings.hpp:51)
+    int threads = 1;                // host threads for the build
+};
+
+// Full symmetric CSR (both triangles), columns sorted, no diagonal entries.
+struct SymPattern {
+    int rows = 0;
+    std::vector<int64_t> rp;        // rows + 1
+    std::vector<int> ci;            // nnz
+    std::vector<int64_t> diag;      // first position in row i with column > i
+    int64_t nnz() const { return rp.empty() ? 0 : rp.back(); }
+};
+
+struct HostTree {
+    int dom = 2, size = 3;
+    int nV = 0, N = 0, NC = 0, depth = 0;
+    std::vector<int> perm;          // position -> original simplex (P_ordering)
+    std::vector<int> inv_perm;      // original simplex -> position
+    std::vector<int> C_begin, C_end, C_left, C_right, C_parent, C_depth;
+    std::vector<int> leaf_of;       // position -> leaf cluster
+    std::vector<double> C_box;      // NC x 7: r2, centre[3], half-lengths[3]
+    SymPattern near, far, verynear, inter;
+};
+
+// Builds the cluster tree and the four block-cluster-tree patterns.
+// V: nV x 3 (frozen coordinates), S: N x (dom+1) simplices.
+// Returns an empty string on success, otherwise an error message.
+std::string build_tree(int dom, const double* V, int nV, const int* S, int N, const TreeSettings& set,
+                       HostTree& out);
+
+}  // namespace rpb

@@ -1,0 +1,508 @@
+// Tangent-point energy and differential kernels (B200, sm_100a).
+//
+//   k_geometry_upsweep : SimplicialMesh::SemiStaticUpdate -- simplex data
+//                        (src/SimplexDataKernel.hpp:92-203) in tree order, plus the
+//                        ClusterTree moment upsweep (ComputeClusterData_Thread.hpp:50-129)
+//                        as one bottom-up pass with arrival counters.
+//   k_tp0_pairs        : TP0 near-field and far-field pair kernels
+//                        (TP0_Kernel_NF.hpp:140-338, TP0_Kernel_FF.hpp:130-319) over the
+//                        full symmetric CSR patterns, one warp per row; every row
+//                        accumulates only its own derivative, so no scatter/atomics.
+//   k_collect_chain    : CollectFar/NearFieldDerivatives (src/ClusterTree.hpp:1115-1208),
+//                        the percolate-down of the far field and DNearFarToHulls
+//                        (SimplicialMeshDetails.hpp:529-733, :1097-1410) per primitive.
+//   k_gather_vertices  : DerivativeAssembler().Dot (src/SimplicialMesh.hpp:625-674).
+#pragma once
+
+#include <type_traits>
+
+#include "rpb_device.cuh"
+
+namespace rpb {
+
+// ----------------------------------------------------------------------------------------
+// Simplex geometry shared by the data, chain-rule and metric kernels.
+// ----------------------------------------------------------------------------------------
+struct SimplexGeom {
+    double h[3][3];      // hull in the simplex's own vertex order
+    double c[3];         // barycentre
+    double vol;          // |tau| (edges) or |nu|/2 (triangles)
+    double t[3];         // unit tangent (edges) or unit normal (triangles)
+    double len;          // |tau| or |nu|
+    double charge;       // mean vertex charge
+    double diam;         // longest edge
+};
+
+__device__ __forceinline__ void simplex_geometry(int dom, const double* __restrict__ V, const int* __restrict__ s,
+                                                 const double* __restrict__ charge_v, SimplexGeom& g)
+{
+    const int size = dom + 1;
+    g.charge = 0.0;
+    for (int j = 0; j < size; ++j) {
+        const int v = s[j];
+        g.h[j][0] = V[3 * static_cast<int64_t>(v) + 0];
+        g.h[j][1] = V[3 * static_cast<int64_t>(v) + 1];
+        g.h[j][2] = V[3 * static_cast<int64_t>(v) + 2];
+        g.charge += charge_v[v];
+    }
+    g.charge /= size;
+    for (int k = 0; k < 3; ++k) {
+        double acc = g.h[0][k];
+        for (int j = 1; j < size; ++j) acc += g.h[j][k];
+        g.c[k] = acc / size;
+    }
+    if (dom == 1) {
+        double tau[3] = {g.h[1][0] - g.h[0][0], g.h[1][1] - g.h[0][1], g.h[1][2] - g.h[0][2]};
+        g.len = sqrt(tau[0] * tau[0] + tau[1] * tau[1] + tau[2] * tau[2]);
+        g.vol = g.len;
+        for (int k = 0; k < 3; ++k) g.t[k] = tau[k] / g.len;
+        g.diam = g.len;
+    } else {
+        double e1[3], e2[3], e3[3];
+        for (int k = 0; k < 3; ++k) {
+            e1[k] = g.h[1][k] - g.h[0][k];
+            e2[k] = g.h[2][k] - g.h[0][k];
+            e3[k] = g.h[2][k] - g.h[1][k];
+        }
+        double nu[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2], e1[0] * e2[1] - e1[1] * e2[0]};
+        g.len = sqrt(nu[0] * nu[0] + nu[1] * nu[1] + nu[2] * nu[2]);
+        g.vol = 0.5 * g.len;
+        for (int k = 0; k < 3; ++k) g.t[k] = nu[k] / g.len;
+        const double l1 = e1[0] * e1[0] + e1[1] * e1[1] + e1[2] * e1[2];
+        const double l2 = e2[0] * e2[0] + e2[1] * e2[1] + e2[2] * e2[2];
+        const double l3 = e3[0] * e3[0] + e3[1] * e3[1] + e3[2] * e3[2];
+        g.diam = sqrt(fmax(l1, fmax(l2, l3)));
+    }
+}
+
+// Packed normal projector: triangles n n^T, edges I - t t^T.
+__device__ __forceinline__ void projector_packed(int dom, const double* t, double* P6)
+{
+    const double sgn = (dom == 1) ? -1.0 : 1.0;
+    const double id = (dom == 1) ? 1.0 : 0.0;
+    P6[0] = id + sgn * t[0] * t[0];
+    P6[1] = sgn * t[0] * t[1];
+    P6[2] = sgn * t[0] * t[2];
+    P6[3] = id + sgn * t[1] * t[1];
+    P6[4] = sgn * t[1] * t[2];
+    P6[5] = id + sgn * t[2] * t[2];
+}
+
+struct GeomArgs {
+    int dom, N;
+    const double* V;          // nV x 3
+    const int* S;             // N x (dom+1)
+    const double* charge_v;   // nV
+    const int* perm;          // position -> simplex
+    const int* leaf_of;       // position -> leaf cluster
+    const int* C_parent;
+    const int* C_left;
+    const int* C_right;
+    PrimDatum* P_pair;        // N
+    ClusterDatum* C_pair;     // NC
+    double* C_mom;            // NC x 10 (a, centre, P) in FP64
+    unsigned* counter;        // NC arrival counters, all zero between launches
+};
+
+__device__ __forceinline__ void store_cluster(ClusterDatum* base, int i, const double* mom)
+{
+    ClusterDatum d;
+    d.c[0] = mom[1]; d.c[1] = mom[2]; d.c[2] = mom[3];
+    for (int k = 0; k < 6; ++k) d.P[k] = mom[4 + k];
+    d.a = mom[0];
+    store_datum(base, i, d);
+}
+
+// One thread per primitive in tree order. After writing its leaf, a thread walks
+// toward the root; at every internal node the second-arriving child computes the
+// mass-weighted average of both children (fixed left/right order, deterministic).
+static __global__ void k_geometry_upsweep(GeomArgs g)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= g.N) return;
+    const int size = g.dom + 1;
+    const int j = g.perm[i];
+    SimplexGeom sg;
+    simplex_geometry(g.dom, g.V, g.S + static_cast<int64_t>(size) * j, g.charge_v, sg);
+    double mom[10];
+    mom[0] = sg.charge * sg.vol;
+    mom[1] = sg.c[0]; mom[2] = sg.c[1]; mom[3] = sg.c[2];
+    projector_packed(g.dom, sg.t, mom + 4);
+    {
+        PrimDatum d;
+        for (int k = 0; k < 3; ++k) { d.c[k] = sg.c[k]; d.n[k] = sg.t[k]; }
+        d.a = mom[0];
+        d.diam = static_cast<float>(sg.diam);
+        d.pad = 0.0f;
+        store_datum(g.P_pair, i, d);
+    }
+    int C = g.leaf_of[i];
+    for (int k = 0; k < 10; ++k) __stcg(&g.C_mom[10 * static_cast<int64_t>(C) + k], mom[k]);
+    store_cluster(g.C_pair, C, mom);
+    for (;;) {
+        const int parent = g.C_parent[C];
+        if (parent < 0) return;
+        __threadfence();
+        const unsigned prev = atomicAdd(&g.counter[parent], 1u);
+        if (prev == 0u) return;            // sibling not done yet; it will continue
+        __threadfence();
+        g.counter[parent] = 0u;            // re-arm for the next launch
+        const int L = g.C_left[parent], R = g.C_right[parent];
+        const double* mL = g.C_mom + 10 * static_cast<int64_t>(L);
+        const double* mR = g.C_mom + 10 * static_cast<int64_t>(R);
+        double wl = __ldcg(mL), wr = __ldcg(mR);
+        const double mass = wl + wr;
+        const double inv = 1.0 / mass;
+        wl *= inv;
+        wr *= inv;
+        double m[10];
+        m[0] = mass;
+#pragma unroll
+        for (int k = 1; k < 10; ++k) m[k] = __dadd_rn(__dmul_rn(wl, __ldcg(mL + k)), __dmul_rn(wr, __ldcg(mR + k)));
+        for (int k = 0; k < 10; ++k) __stcg(&g.C_mom[10 * static_cast<int64_t>(parent) + k], m[k]);
+        store_cluster(g.C_pair, parent, m);
+        C = parent;
+    }
+}
+
+// ----------------------------------------------------------------------------------------
+// TP0 pair kernel, row side. Evaluates one pair (row x, column y) and accumulates the
+// row's derivative in moment coordinates in the centred form
+//     d0 = sum b (E - q/2 |u|^{q/2-1} u s^{p/2-q/2})   (no dEdv.x term),
+//     dx = -sum b dEdv,   dP = sum b/2 K_xy V,
+// where u = (v^T P v)/|v|^2, s = 1/|v|^2. The reference's DX[0] equals d0 - dx.x
+// (TP0_Kernel_FF.hpp:220-255); the x-term is restored in FP64 during collection.
+// Powers are taken of the bounded ratios u, w and of s, which keeps the FP32 range
+// safe for close pairs (r^-p itself would overflow FP32 near r ~ 1e-3).
+// ----------------------------------------------------------------------------------------
+template <typename R>
+struct PairAcc {
+    R d0, dx[3], dP[6];
+};
+
+// v (row -> column), r2 = |v|^2, cphi = v^T P v, cpsi = v^T Q v, Pv, Qv.
+template <typename R>
+struct Proj {
+    R v[3], r2, cphi, cpsi, Pv[3], Qv[3];
+};
+
+template <typename R, int QH, int PH, bool DIFF>
+__device__ __forceinline__ R tp0_core(const TPExp& ex, const Proj<R>& g, R a, R b, PairAcc<R>& acc)
+{
+    const R s = dev_rcp(g.r2);
+    const R u = g.cphi * s;
+    const R w = g.cpsi * s;
+    R uq1, wq1, se;
+    if constexpr (QH > 0 && PH >= QH) {
+        uq1 = ipow_pos(fabs(u), QH - 1);
+        wq1 = ipow_pos(fabs(w), QH - 1);
+        se = ipow_pos(s, PH - QH);
+    } else {
+        const R qh = static_cast<R>(ex.q * 0.5), ph = static_cast<R>(ex.p * 0.5);
+        uq1 = (fabs(u) > R(0)) ? dev_pow(fabs(u), qh - R(1)) : R(0);
+        wq1 = (fabs(w) > R(0)) ? dev_pow(fabs(w), qh - R(1)) : R(0);
+        se = dev_pow(s, ph - qh);
+    }
+    const R uq = uq1 * u, wq = wq1 * w;
+    const R E = (uq + wq) * se;
+    if constexpr (DIFF) {
+        const R q = static_cast<R>(ex.q), p = static_cast<R>(ex.p);
+        const R se1 = se * s;
+        const R Kxy = q * uq1 * se1;
+        const R Kyx = q * wq1 * se1;
+        const R H = p * (uq + wq) * se1;
+        acc.d0 += b * (E - R(0.5) * q * uq * se);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) acc.dx[k] -= b * (Kxy * g.Pv[k] + Kyx * g.Qv[k] - H * g.v[k]);
+        const R hb = R(0.5) * b * Kxy;
+        acc.dP[0] += hb * g.v[0] * g.v[0];
+        acc.dP[1] += hb * R(2) * g.v[0] * g.v[1];
+        acc.dP[2] += hb * R(2) * g.v[0] * g.v[2];
+        acc.dP[3] += hb * g.v[1] * g.v[1];
+        acc.dP[4] += hb * R(2) * g.v[1] * g.v[2];
+        acc.dP[5] += hb * g.v[2] * g.v[2];
+    }
+    return a * E * b;
+}
+
+// Projection of v = y - x for two primitives. Triangles: P = n n^T, so only n.v is
+// needed (FP64); edges: P v = v - t (t.v) (FP64). Everything downstream of v^T P v is
+// well conditioned and is rounded to R.
+template <typename R>
+__device__ __forceinline__ void project_prims(int dom, const PrimDatum& X, const PrimDatum& Y, Proj<R>& g)
+{
+    const double v0 = Y.c[0] - X.c[0], v1 = Y.c[1] - X.c[1], v2 = Y.c[2] - X.c[2];
+    g.v[0] = static_cast<R>(v0); g.v[1] = static_cast<R>(v1); g.v[2] = static_cast<R>(v2);
+    g.r2 = g.v[0] * g.v[0] + g.v[1] * g.v[1] + g.v[2] * g.v[2];
+    const double xv = X.n[0] * v0 + X.n[1] * v1 + X.n[2] * v2;
+    const double yv = Y.n[0] * v0 + Y.n[1] * v1 + Y.n[2] * v2;
+    if (dom == 2) {
+        g.cphi = static_cast<R>(xv * xv);
+        g.cpsi = static_cast<R>(yv * yv);
+        const R xf = static_cast<R>(xv), yf = static_cast<R>(yv);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            g.Pv[k] = static_cast<R>(X.n[k]) * xf;
+            g.Qv[k] = static_cast<R>(Y.n[k]) * yf;
+        }
+    } else {
+        const double p0 = v0 - X.n[0] * xv, p1 = v1 - X.n[1] * xv, p2 = v2 - X.n[2] * xv;
+        const double q0 = v0 - Y.n[0] * yv, q1 = v1 - Y.n[1] * yv, q2 = v2 - Y.n[2] * yv;
+        g.cphi = static_cast<R>(p0 * p0 + p1 * p1 + p2 * p2);
+        g.cpsi = static_cast<R>(q0 * q0 + q1 * q1 + q2 * q2);
+        g.Pv[0] = static_cast<R>(p0); g.Pv[1] = static_cast<R>(p1); g.Pv[2] = static_cast<R>(p2);
+        g.Qv[0] = static_cast<R>(q0); g.Qv[1] = static_cast<R>(q1); g.Qv[2] = static_cast<R>(q2);
+    }
+}
+
+// Projection for two clusters with averaged projectors (FP64 products).
+template <typename R>
+__device__ __forceinline__ void project_clusters(const ClusterDatum& X, const ClusterDatum& Y, Proj<R>& g)
+{
+    const double v0 = Y.c[0] - X.c[0], v1 = Y.c[1] - X.c[1], v2 = Y.c[2] - X.c[2];
+    g.v[0] = static_cast<R>(v0); g.v[1] = static_cast<R>(v1); g.v[2] = static_cast<R>(v2);
+    g.r2 = g.v[0] * g.v[0] + g.v[1] * g.v[1] + g.v[2] * g.v[2];
+    const double* P = X.P;
+    const double* Q = Y.P;
+    const double p0 = P[0] * v0 + P[1] * v1 + P[2] * v2;
+    const double p1 = P[1] * v0 + P[3] * v1 + P[4] * v2;
+    const double p2 = P[2] * v0 + P[4] * v1 + P[5] * v2;
+    const double q0 = Q[0] * v0 + Q[1] * v1 + Q[2] * v2;
+    const double q1 = Q[1] * v0 + Q[3] * v1 + Q[4] * v2;
+    const double q2 = Q[2] * v0 + Q[4] * v1 + Q[5] * v2;
+    g.cphi = static_cast<R>(v0 * p0 + v1 * p1 + v2 * p2);
+    g.cpsi = static_cast<R>(v0 * q0 + v1 * q1 + v2 * q2);
+    g.Pv[0] = static_cast<R>(p0); g.Pv[1] = static_cast<R>(p1); g.Pv[2] = static_cast<R>(p2);
+    g.Qv[0] = static_cast<R>(q0); g.Qv[1] = static_cast<R>(q1); g.Qv[2] = static_cast<R>(q2);
+}
+
+struct PairArgs {
+    int dom;
+    int rows;
+    const int64_t* rp;
+    const int* ci;
+    const void* data;         // PrimDatum* (near) or ClusterDatum* (far)
+    double* D;                // rows x 10 (d0, dx[3], dP[6]) centred moment derivatives
+    double* block_energy;     // gridDim.x
+    unsigned* done;           // 1 counter, zero between launches
+    double* energy_out;       // 1
+    TPExp ex;
+    float close_factor;       // FP64 path for near pairs with r < close_factor (d_i + d_j)
+};
+
+// One warp per row. FAR: rows are clusters of the Far() pattern; otherwise rows are
+// primitives of the Near() pattern.
+template <bool FAR, int QH, int PH, bool DIFF>
+__global__ void __launch_bounds__(256) k_tp0_pairs(PairArgs A)
+{
+    using Datum = typename std::conditional<FAR, ClusterDatum, PrimDatum>::type;
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    const int i = blockIdx.x * (blockDim.x >> 5) + wib;
+    const Datum* base = static_cast<const Datum*>(A.data);
+    double e_row = 0.0;
+    if (i < A.rows) {
+        const Datum X = load_datum(base, i);
+        PairAcc<float> acc = {};
+        float e_lane = 0.0f;
+        double d64[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+        double e64 = 0.0;
+        bool any64 = false;
+        const int64_t k0 = A.rp[i], k1 = A.rp[i + 1];
+        for (int64_t k = k0 + lane; k < k1; k += 32) {
+            const int j = __ldg(A.ci + k);
+            const Datum Y = load_datum(base, j);
+            Proj<float> g;
+            if constexpr (FAR) project_clusters(X, Y, g);
+            else project_prims(A.dom, X, Y, g);
+            bool close = false;
+            if constexpr (!FAR) {
+                const float dd = A.close_factor * (X.diam + Y.diam);
+                close = g.r2 < dd * dd;
+            }
+            if (close) {
+                // close near-field pair: the same kernel in FP64
+                Proj<double> gd;
+                if constexpr (!FAR) project_prims(A.dom, X, Y, gd);
+                PairAcc<double> a64 = {};
+                const double e = tp0_core<double, QH, PH, DIFF>(A.ex, gd, X.a, Y.a, a64);
+                if (j > i) e64 += e;
+                if (DIFF) {
+                    d64[0] += a64.d0;
+                    for (int m = 0; m < 3; ++m) d64[1 + m] += a64.dx[m];
+                    for (int m = 0; m < 6; ++m) d64[4 + m] += a64.dP[m];
+                }
+                any64 = true;
+            } else {
+                const float e = tp0_core<float, QH, PH, DIFF>(A.ex, g, static_cast<float>(X.a), static_cast<float>(Y.a), acc);
+                if (j > i) e_lane += e;
+            }
+        }
+        // compensated cross-lane reduction; FP64 contributions added exactly
+        e_row = warp_sum_compensated(e_lane);
+        const bool has64 = __any_sync(0xffffffffu, any64);
+        if (has64) e_row += warp_sum_f64(e64);
+        if (DIFF) {
+            double out[10];
+            out[0] = warp_sum_compensated(acc.d0);
+#pragma unroll
+            for (int m = 0; m < 3; ++m) out[1 + m] = warp_sum_compensated(acc.dx[m]);
+#pragma unroll
+            for (int m = 0; m < 6; ++m) out[4 + m] = warp_sum_compensated(acc.dP[m]);
+            if (has64) {
+#pragma unroll
+                for (int m = 0; m < 10; ++m) out[m] += warp_sum_f64(d64[m]);
+            }
+            double* dst = A.D + 10 * static_cast<int64_t>(i);
+            if (lane < 10) {
+                double val = out[0];
+#pragma unroll
+                for (int m = 1; m < 10; ++m) val = (lane == m) ? out[m] : val;
+                dst[lane] = val;
+            }
+        }
+    }
+    // deterministic energy reduction: per-block partial, last block sums all partials
+    __shared__ double sh[32];
+    __shared__ bool last;
+    if (lane == 0) sh[wib] = e_row;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int w = 0; w < (blockDim.x >> 5); ++w) s += sh[w];
+        A.block_energy[blockIdx.x] = s;
+        __threadfence();
+        last = (atomicAdd(A.done, 1u) == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (last) {
+        __threadfence();
+        double s = 0.0;
+        for (int b = threadIdx.x; b < gridDim.x; b += blockDim.x) s += __ldcg(A.block_energy + b);
+        s = warp_sum_f64(s);
+        if (lane == 0) sh[wib] = s;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double t = 0.0;
+            for (int w = 0; w < (blockDim.x >> 5); ++w) t += sh[w];
+            *A.energy_out = t;
+            *A.done = 0u;
+        }
+    }
+}
+
+// ----------------------------------------------------------------------------------------
+// Collection + chain rule. One thread per primitive (tree order).
+// ----------------------------------------------------------------------------------------
+struct CollectArgs {
+    int dom, N;
+    const double* V;
+    const int* S;
+    const double* charge_v;
+    const int* perm;
+    const int* leaf_of;
+    const int* C_parent;
+    const ClusterDatum* C_pair;
+    const double* D_near;      // N x 10 centred
+    const double* D_far;       // NC x 10 centred
+    const double* D_vf;        // N x 16 very-near derivatives (reference layout) or nullptr
+    double* B;                 // N x (dom+1) x 3, original simplex order
+};
+
+static __global__ void k_collect_chain(CollectArgs A)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= A.N) return;
+    const int size = A.dom + 1;
+    const int j = A.perm[i];
+    SimplexGeom g;
+    simplex_geometry(A.dom, A.V, A.S + static_cast<int64_t>(size) * j, A.charge_v, g);
+
+    // near field (centred at the primitive barycentre)
+    const double* dn = A.D_near + 10 * static_cast<int64_t>(i);
+    double alpha = dn[0];
+    double gx[3] = {dn[1], dn[2], dn[3]};
+    double G6[6];
+    for (int k = 0; k < 6; ++k) G6[k] = dn[4 + k];
+    // far field: percolate down = sum over all ancestors of the leaf
+    int C = A.leaf_of[i];
+    while (C >= 0) {
+        const double* df = A.D_far + 10 * static_cast<int64_t>(C);
+        const ClusterDatum cd = load_datum(A.C_pair, C);
+        const double dx0 = df[1], dx1 = df[2], dx2 = df[3];
+        alpha += df[0] + dx0 * (g.c[0] - cd.c[0]) + dx1 * (g.c[1] - cd.c[1]) + dx2 * (g.c[2] - cd.c[2]);
+        gx[0] += dx0; gx[1] += dx1; gx[2] += dx2;
+        for (int k = 0; k < 6; ++k) G6[k] += df[4 + k];
+        C = A.C_parent[C];
+    }
+    double hull_extra[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    if (A.D_vf) {
+        const double* dv = A.D_vf + 16 * static_cast<int64_t>(i);
+        alpha += dv[0];
+        for (int c = 0; c < size; ++c)
+            for (int k = 0; k < 3; ++k) {
+                alpha += dv[1 + 3 * c + k] * g.h[c][k];
+                hull_extra[c][k] = dv[1 + 3 * c + k];
+            }
+        for (int k = 0; k < 6; ++k) G6[k] += dv[1 + 3 * size + k];
+    }
+    double P6[6];
+    projector_packed(A.dom, g.t, P6);
+    for (int k = 0; k < 6; ++k) alpha += G6[k] * P6[k];
+    // symmetric G with halved off-diagonals: G_ab = d/dP_ab of sum_{a<=b} G6 P_ab
+    const double G[3][3] = {{G6[0], 0.5 * G6[1], 0.5 * G6[2]},
+                            {0.5 * G6[1], G6[3], 0.5 * G6[4]},
+                            {0.5 * G6[2], 0.5 * G6[4], G6[5]}};
+    double Gt[3];
+    for (int a = 0; a < 3; ++a) Gt[a] = G[a][0] * g.t[0] + G[a][1] * g.t[1] + G[a][2] * g.t[2];
+    const double tGt = g.t[0] * Gt[0] + g.t[1] * Gt[1] + g.t[2] * Gt[2];
+    double Bc[3][3];
+    if (A.dom == 2) {
+        double w[3];
+        for (int a = 0; a < 3; ++a) w[a] = 2.0 * (Gt[a] - tGt * g.t[a]) / g.len;
+        for (int c = 0; c < 3; ++c) {
+            const int c1 = (c + 1) % 3, c2 = (c + 2) % 3;
+            const double u[3] = {g.h[c1][0] - g.h[c2][0], g.h[c1][1] - g.h[c2][1], g.h[c1][2] - g.h[c2][2]};
+            const double un[3] = {u[1] * g.t[2] - u[2] * g.t[1], u[2] * g.t[0] - u[0] * g.t[2], u[0] * g.t[1] - u[1] * g.t[0]};
+            const double uw[3] = {u[1] * w[2] - u[2] * w[1], u[2] * w[0] - u[0] * w[2], u[0] * w[1] - u[1] * w[0]};
+            for (int k = 0; k < 3; ++k)
+                Bc[c][k] = g.charge * (alpha * 0.5 * un[k] + g.vol * (gx[k] / 3.0 + hull_extra[c][k]) + g.vol * uw[k]);
+        }
+    } else {
+        double gg[3];
+        for (int a = 0; a < 3; ++a) gg[a] = -2.0 * (Gt[a] - tGt * g.t[a]) / g.len;
+        for (int c = 0; c < 2; ++c) {
+            const double sgn = (c == 1) ? 1.0 : -1.0;
+            for (int k = 0; k < 3; ++k)
+                Bc[c][k] = g.charge * (alpha * sgn * g.t[k] + g.vol * (gx[k] * 0.5 + hull_extra[c][k]) + g.vol * sgn * gg[k]);
+        }
+    }
+    double* dst = A.B + static_cast<int64_t>(size) * 3 * j;
+    for (int c = 0; c < size; ++c)
+        for (int k = 0; k < 3; ++k) dst[3 * c + k] = Bc[c][k];
+}
+
+struct GatherArgs {
+    int nV;
+    const int* v_rp;     // nV + 1
+    const int* v_slot;   // slot = simplex * (dom+1) + corner
+    const double* B;     // slots x 3
+    double alpha, beta;
+    double* Y;
+    int ldY;
+};
+
+static __global__ void k_gather_vertices(GatherArgs A)
+{
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= A.nV) return;
+    double acc[3] = {0, 0, 0};
+    for (int k = A.v_rp[v]; k < A.v_rp[v + 1]; ++k) {
+        const double* b = A.B + 3 * static_cast<int64_t>(A.v_slot[k]);
+        acc[0] += b[0]; acc[1] += b[1]; acc[2] += b[2];
+    }
+    double* y = A.Y + static_cast<int64_t>(A.ldY) * v;
+    for (int k = 0; k < 3; ++k) y[k] = A.alpha * acc[k] + (A.beta == 0.0 ? 0.0 : A.beta * y[k]);
+}
+
+}  // namespace rpb

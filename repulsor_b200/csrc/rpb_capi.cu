@@ -1,0 +1,577 @@
+// C ABI of the B200 tangent-point path: mesh lifetime, tree upload, energy and
+// differential. Metric and solver entry points live in rpb_metric.cu / rpb_solver.cu.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <thread>
+
+#include "../../include/repulsor_b200.h"
+#include "host/sparse_cholesky.hpp"
+#include "kernels_energy.cuh"
+#include "rpb_internal.cuh"
+#include "rpb_mesh.cuh"
+
+namespace rpb {
+
+static thread_local std::string g_last_error;
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+
+}  // namespace rpb
+
+using namespace rpb;
+
+#define RPB_CUDA(call)                                                                        \
+    do {                                                                                      \
+        cudaError_t e_ = (call);                                                              \
+        if (e_ != cudaSuccess) {                                                              \
+            set_error(std::string("CUDA error: ") + cudaGetErrorString(e_) + " at " #call);   \
+            return e_ == cudaErrorMemoryAllocation ? RPB_ENOMEM : RPB_ECUDA;                  \
+        }                                                                                     \
+    } while (0)
+
+int64_t rpb_mesh::device_bytes() const
+{
+    int64_t b = 0;
+    b += V.bytes() + charge_v.bytes() + S.bytes() + perm.bytes() + leaf_of.bytes() + C_parent.bytes() +
+         C_left.bytes() + C_right.bytes();
+    b += near.rp.bytes() + near.ci.bytes() + far.rp.bytes() + far.ci.bytes() + verynear.rp.bytes() +
+         verynear.ci.bytes();
+    b += P_pair.bytes() + C_pair.bytes() + C_mom.bytes() + counter.bytes() + P_near.bytes();
+    b += D_near.bytes() + D_far.bytes() + D_vf.bytes() + B.bytes() + v_rp.bytes() + v_slot.bytes() + Y.bytes();
+    b += block_energy.bytes() + energy.bytes() + done.bytes();
+    b += pre_cols.bytes() + pre_vals.bytes() + vp_rp.bytes() + vp_slot.bytes();
+    b += buf_Pin64.bytes() + buf_Cin64.bytes() + buf_Pout.bytes() + buf_Cout.bytes() + buf_Z.bytes() + X.bytes() +
+         Yb.bytes();
+    b += metric.nf.bytes() + metric.ff.bytes() + metric.vf.bytes() + metric.nf_diag.bytes() +
+         metric.ff_diag.bytes() + metric.vf_diag.bytes();
+    b += plap.nf.bytes() + plap.ff.bytes() + plap.vf.bytes() + plap.nf_diag.bytes() + plap.ff_diag.bytes() +
+         plap.vf_diag.bytes();
+    return b;
+}
+
+namespace rpb {
+
+template <typename T>
+static rpb_status upload(DevBuf<T>& d, const T* h, size_t n, cudaStream_t s)
+{
+    RPB_CUDA(d.alloc(n));
+    if (n) RPB_CUDA(cudaMemcpyAsync(d.ptr, h, sizeof(T) * n, cudaMemcpyHostToDevice, s));
+    return RPB_OK;
+}
+
+static rpb_status upload_pattern(Csr& d, const SymPattern& P, cudaStream_t s)
+{
+    d.rows = P.rows;
+    d.nnz = P.nnz();
+    rpb_status st = upload(d.rp, P.rp.data(), P.rp.size(), s);
+    if (st != RPB_OK) return st;
+    return upload(d.ci, P.ci.data(), P.ci.size(), s);
+}
+
+TPExp make_exp(int dom, double q, double p)
+{
+    TPExp e;
+    e.q = q;
+    e.p = p;
+    const double s = (p - dom) / q;
+    e.s_exp_metric = -0.5 * (2.0 * (s - 1.0) + dom);
+    const double qh = q / 2, ph = p / 2;
+    e.qh = (qh == std::floor(qh)) ? static_cast<int>(qh) : -1;
+    e.ph = (ph == std::floor(ph)) ? static_cast<int>(ph) : -1;
+    return e;
+}
+
+rpb_status check_exponents(double q, double p)
+{
+    if (!(q >= 2.0) || !std::isfinite(q) || !std::isfinite(p) || !(p > 0)) {
+        set_error("tangent-point kernels need q >= 2 and p > 0 (the reference rejects q < 0 and 0 < q < 2)");
+        return RPB_EINVAL;
+    }
+    return RPB_OK;
+}
+
+// SemiStaticUpdate on the device: simplex data + cluster moments.
+rpb_status launch_geometry(rpb_mesh* m)
+{
+    GeomArgs g;
+    g.dom = m->dom;
+    g.N = m->N;
+    g.V = m->V.ptr;
+    g.S = m->S.ptr;
+    g.charge_v = m->charge_v.ptr;
+    g.perm = m->perm.ptr;
+    g.leaf_of = m->leaf_of.ptr;
+    g.C_parent = m->C_parent.ptr;
+    g.C_left = m->C_left.ptr;
+    g.C_right = m->C_right.ptr;
+    g.P_pair = m->P_pair.ptr;
+    g.C_pair = m->C_pair.ptr;
+    g.C_mom = m->C_mom.ptr;
+    g.counter = m->counter.ptr;
+    k_geometry_upsweep<<<(m->N + 255) / 256, 256, 0, m->stream>>>(g);
+    RPB_CUDA(cudaGetLastError());
+    m->geometry_valid = true;
+    m->geometry_version++;
+    m->metric.valid = false;
+    m->plap.valid = false;
+    return RPB_OK;
+}
+
+template <int QH, int PH>
+static void launch_pairs_t(rpb_mesh* m, const PairArgs& An, const PairArgs& Af, bool diff)
+{
+    if (An.rows > 0) {
+        if (diff) k_tp0_pairs<false, QH, PH, true><<<m->near_blocks, 256, 0, m->stream>>>(An);
+        else k_tp0_pairs<false, QH, PH, false><<<m->near_blocks, 256, 0, m->stream>>>(An);
+    }
+    if (Af.rows > 0) {
+        if (diff) k_tp0_pairs<true, QH, PH, true><<<m->far_blocks, 256, 0, m->stream>>>(Af);
+        else k_tp0_pairs<true, QH, PH, false><<<m->far_blocks, 256, 0, m->stream>>>(Af);
+    }
+}
+
+rpb_status launch_pairs(rpb_mesh* m, const TPExp& ex, bool diff)
+{
+    PairArgs An, Af;
+    An.dom = Af.dom = m->dom;
+    An.ex = Af.ex = ex;
+    An.close_factor = Af.close_factor = 0.1f;
+    An.rows = m->near.nnz > 0 ? m->N : 0;
+    An.rp = m->near.rp.ptr; An.ci = m->near.ci.ptr; An.data = m->P_pair.ptr; An.D = m->D_near.ptr;
+    An.block_energy = m->block_energy.ptr; An.done = m->done.ptr; An.energy_out = m->energy.ptr;
+    Af.rows = m->far.nnz > 0 ? m->NC : 0;
+    Af.rp = m->far.rp.ptr; Af.ci = m->far.ci.ptr; Af.data = m->C_pair.ptr; Af.D = m->D_far.ptr;
+    Af.block_energy = m->block_energy.ptr + m->near_blocks; Af.done = m->done.ptr + 1; Af.energy_out = m->energy.ptr + 1;
+    if (An.rows == 0) {
+        RPB_CUDA(cudaMemsetAsync(m->energy.ptr, 0, sizeof(double), m->stream));
+        if (diff) RPB_CUDA(cudaMemsetAsync(m->D_near.ptr, 0, m->D_near.bytes(), m->stream));
+    }
+    if (Af.rows == 0) {
+        RPB_CUDA(cudaMemsetAsync(m->energy.ptr + 1, 0, sizeof(double), m->stream));
+        if (diff) RPB_CUDA(cudaMemsetAsync(m->D_far.ptr, 0, m->D_far.bytes(), m->stream));
+    }
+    if (ex.qh == 3 && ex.ph == 6) launch_pairs_t<3, 6>(m, An, Af, diff);
+    else if (ex.qh == 2 && ex.ph == 4) launch_pairs_t<2, 4>(m, An, Af, diff);
+    else if (ex.qh == 1 && ex.ph == 2) launch_pairs_t<1, 2>(m, An, Af, diff);
+    else launch_pairs_t<-1, -1>(m, An, Af, diff);
+    RPB_CUDA(cudaGetLastError());
+    return RPB_OK;
+}
+
+rpb_status launch_collect_gather(rpb_mesh* m, double alpha, double beta, double* Y, int ldY, bool with_vf)
+{
+    CollectArgs C;
+    C.dom = m->dom;
+    C.N = m->N;
+    C.V = m->V.ptr;
+    C.S = m->S.ptr;
+    C.charge_v = m->charge_v.ptr;
+    C.perm = m->perm.ptr;
+    C.leaf_of = m->leaf_of.ptr;
+    C.C_parent = m->C_parent.ptr;
+    C.C_pair = m->C_pair.ptr;
+    C.D_near = m->D_near.ptr;
+    C.D_far = m->D_far.ptr;
+    C.D_vf = with_vf ? m->D_vf.ptr : nullptr;
+    C.B = m->B.ptr;
+    k_collect_chain<<<(m->N + 255) / 256, 256, 0, m->stream>>>(C);
+    RPB_CUDA(cudaGetLastError());
+    GatherArgs G;
+    G.nV = m->nV;
+    G.v_rp = m->v_rp.ptr;
+    G.v_slot = m->v_slot.ptr;
+    G.B = m->B.ptr;
+    G.alpha = alpha;
+    G.beta = beta;
+    G.Y = Y;
+    G.ldY = ldY;
+    k_gather_vertices<<<(m->nV + 255) / 256, 256, 0, m->stream>>>(G);
+    RPB_CUDA(cudaGetLastError());
+    return RPB_OK;
+}
+
+// Full energy (+ differential into device Y) evaluation on the mesh stream.
+rpb_status evaluate(rpb_mesh* m, double q, double p, bool diff, double alpha, double beta, double* Y_dev, int ldY,
+                    double* energy_host)
+{
+    rpb_status st = check_exponents(q, p);
+    if (st != RPB_OK) return st;
+    RPB_CUDA(cudaSetDevice(m->device));
+    const TPExp ex = make_exp(m->dom, q, p);
+    if (!m->geometry_valid) {
+        st = launch_geometry(m);
+        if (st != RPB_OK) return st;
+    }
+    st = launch_pairs(m, ex, diff);
+    if (st != RPB_OK) return st;
+    const bool with_vf = m->verynear.nnz > 0;
+    if (with_vf) {
+        st = launch_vf(m, ex, diff);
+        if (st != RPB_OK) return st;
+    }
+    if (diff) {
+        st = launch_collect_gather(m, alpha, beta, Y_dev, ldY, with_vf);
+        if (st != RPB_OK) return st;
+    }
+    if (energy_host) {
+        double e[3] = {0, 0, 0};
+        RPB_CUDA(cudaMemcpyAsync(e, m->energy.ptr, sizeof(double) * 3, cudaMemcpyDeviceToHost, m->stream));
+        RPB_CUDA(cudaStreamSynchronize(m->stream));
+        *energy_host = (e[2] + e[0]) + e[1];
+    }
+    return RPB_OK;
+}
+
+}  // namespace rpb
+
+// ============================================================================================
+extern "C" {
+
+rpb_status rpb_default_settings(rpb_settings* s)
+{
+    if (!s) { set_error("null settings"); return RPB_EINVAL; }
+    s->split_threshold = 1;
+    s->far_field_separation = 0.5;
+    s->near_field_separation = 10.0;
+    s->near_field_intersection = 1e10;
+    s->max_refinement = 30;
+    s->thread_count = 0;
+    s->device = 0;
+    return RPB_OK;
+}
+
+const char* rpb_last_error(void) { return g_last_error.c_str(); }
+
+rpb_status rpb_mesh_create(int dom_dim, int amb_dim, const double* Vh, int64_t nV, const int* Sh, int64_t nS,
+                           const double* charges, const rpb_settings* settings, rpb_mesh** out)
+{
+    if (!out) { set_error("out is null"); return RPB_EINVAL; }
+    *out = nullptr;
+    if (amb_dim != 3) { set_error("only ambient dimension 3 is supported"); return RPB_EINVAL; }
+    if (dom_dim != 1 && dom_dim != 2) { set_error("domain dimension must be 1 or 2"); return RPB_EINVAL; }
+    if (!Vh || !Sh || nV <= 0 || nS <= 0) { set_error("empty mesh: (V.Dim(0) <= 0) || (simplices.Dim(0) <= 0)"); return RPB_EINVAL; }
+    if (nV > (1ll << 30) || nS > (1ll << 29)) { set_error("mesh too large for 32-bit indices"); return RPB_EINVAL; }
+    rpb_settings set;
+    rpb_default_settings(&set);
+    if (settings) set = *settings;
+    if (set.split_threshold != 1) { set_error("only split_threshold = 1 is supported"); return RPB_EINVAL; }
+    if (!(set.far_field_separation > 0) || !(set.near_field_separation > 0)) { set_error("separation parameters must be positive"); return RPB_EINVAL; }
+    if (set.max_refinement < 0 || set.max_refinement > 60) { set_error("max_refinement must be in [0, 60]"); return RPB_EINVAL; }
+    int dev_count = 0;
+    if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count <= 0) {
+        set_error("no CUDA device available: the B200 path has no CPU fallback");
+        return RPB_ECUDA;
+    }
+    if (set.device < 0 || set.device >= dev_count) { set_error("device ordinal out of range"); return RPB_EINVAL; }
+
+    auto* m = new rpb_mesh();
+    m->dom = dom_dim;
+    m->size = dom_dim + 1;
+    m->nV = static_cast<int>(nV);
+    m->N = static_cast<int>(nS);
+    m->device = set.device;
+    m->settings.theta_far = set.far_field_separation;
+    m->settings.theta_near = set.near_field_separation;
+    m->settings.max_refinement = set.max_refinement;
+    m->settings.threads = set.thread_count > 0 ? set.thread_count : std::max(1u, std::thread::hardware_concurrency());
+    auto fail = [&](rpb_status st) { delete m; return st; };
+
+    const auto t0 = std::chrono::steady_clock::now();
+    const std::string err = build_tree(dom_dim, Vh, m->nV, Sh, m->N, m->settings, m->tree);
+    if (!err.empty()) { set_error(err); return fail(RPB_EINVAL); }
+    m->build_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    m->NC = m->tree.NC;
+
+    if (cudaSetDevice(m->device) != cudaSuccess) { set_error("cudaSetDevice failed"); return fail(RPB_ECUDA); }
+    if (cudaStreamCreateWithFlags(&m->own_stream, cudaStreamNonBlocking) != cudaSuccess) { set_error("stream creation failed"); return fail(RPB_ECUDA); }
+    m->stream = m->own_stream;
+    cudaStream_t s = m->stream;
+    const HostTree& T = m->tree;
+    std::vector<double> ch(m->nV, 1.0);
+    if (charges) std::copy(charges, charges + m->nV, ch.begin());
+    rpb_status st;
+#define UP(buf, ptr, n) do { st = upload(buf, ptr, n, s); if (st != RPB_OK) return fail(st); } while (0)
+    UP(m->V, Vh, 3 * static_cast<size_t>(m->nV));
+    UP(m->charge_v, ch.data(), ch.size());
+    UP(m->S, Sh, static_cast<size_t>(m->size) * m->N);
+    UP(m->perm, T.perm.data(), T.perm.size());
+    UP(m->leaf_of, T.leaf_of.data(), T.leaf_of.size());
+    UP(m->C_parent, T.C_parent.data(), T.C_parent.size());
+    UP(m->C_left, T.C_left.data(), T.C_left.size());
+    UP(m->C_right, T.C_right.data(), T.C_right.size());
+    if ((st = upload_pattern(m->near, T.near, s)) != RPB_OK) return fail(st);
+    if ((st = upload_pattern(m->far, T.far, s)) != RPB_OK) return fail(st);
+    if ((st = upload_pattern(m->verynear, T.verynear, s)) != RPB_OK) return fail(st);
+    // vertex -> slot incidence (DerivativeAssembler, src/SimplicialMesh.hpp:625-649)
+    {
+        std::vector<int> rp(m->nV + 1, 0), slot(static_cast<size_t>(m->size) * m->N);
+        for (int64_t k = 0; k < static_cast<int64_t>(m->size) * m->N; ++k) rp[Sh[k] + 1]++;
+        for (int v = 0; v < m->nV; ++v) rp[v + 1] += rp[v];
+        std::vector<int> pos(rp.begin(), rp.end() - 1);
+        for (int64_t k = 0; k < static_cast<int64_t>(m->size) * m->N; ++k) slot[pos[Sh[k]]++] = static_cast<int>(k);
+        UP(m->v_rp, rp.data(), rp.size());
+        UP(m->v_slot, slot.data(), slot.size());
+    }
+#undef UP
+    if (m->P_pair.alloc(m->N) || m->C_pair.alloc(m->NC) || m->C_mom.alloc(10 * static_cast<size_t>(m->NC)) ||
+        m->counter.alloc(m->NC) || m->D_near.alloc(10 * static_cast<size_t>(m->N)) ||
+        m->D_far.alloc(10 * static_cast<size_t>(m->NC)) ||
+        m->B.alloc(3 * static_cast<size_t>(m->size) * m->N) || m->Y.alloc(3 * static_cast<size_t>(m->nV)) ||
+        m->energy.alloc(4) || m->done.alloc(4)) {
+        set_error("device allocation failed");
+        return fail(RPB_ENOMEM);
+    }
+    m->near_blocks = (m->N + 7) / 8;
+    m->far_blocks = (m->NC + 7) / 8;
+    if (m->block_energy.alloc(m->near_blocks + m->far_blocks)) { set_error("device allocation failed"); return fail(RPB_ENOMEM); }
+    if (cudaMemsetAsync(m->counter.ptr, 0, m->counter.bytes(), s) != cudaSuccess ||
+        cudaMemsetAsync(m->done.ptr, 0, m->done.bytes(), s) != cudaSuccess ||
+        cudaMemsetAsync(m->energy.ptr, 0, m->energy.bytes(), s) != cudaSuccess) {
+        set_error("memset failed");
+        return fail(RPB_ECUDA);
+    }
+    if (m->verynear.nnz > 0) {
+        if (m->D_vf.alloc(16 * static_cast<size_t>(m->N))) { set_error("device allocation failed"); return fail(RPB_ENOMEM); }
+    }
+    if ((st = launch_geometry(m)) != RPB_OK) return fail(st);
+    if ((st = metric_init(m, Vh, Sh)) != RPB_OK) return fail(st);
+    if (cudaStreamSynchronize(s) != cudaSuccess) { set_error("initial upload failed"); return fail(RPB_ECUDA); }
+    *out = m;
+    return RPB_OK;
+}
+
+rpb_status rpb_mesh_destroy(rpb_mesh* m)
+{
+    if (!m) return RPB_OK;
+    cudaSetDevice(m->device);
+    if (m->stream) cudaStreamSynchronize(m->stream);
+    solver_free(m);
+    cudaStream_t s = m->own_stream;
+    delete m;  // frees device buffers
+    if (s) cudaStreamDestroy(s);
+    return RPB_OK;
+}
+
+rpb_status rpb_mesh_set_stream(rpb_mesh* m, void* stream)
+{
+    if (!m) { set_error("null mesh"); return RPB_EINVAL; }
+    RPB_CUDA(cudaSetDevice(m->device));
+    RPB_CUDA(cudaStreamSynchronize(m->stream));
+    m->stream = stream ? static_cast<cudaStream_t>(stream) : m->own_stream;
+    return RPB_OK;
+}
+
+rpb_status rpb_mesh_get_stream(const rpb_mesh* m, void** stream)
+{
+    if (!m || !stream) { set_error("null argument"); return RPB_EINVAL; }
+    *stream = static_cast<void*>(m->stream);
+    return RPB_OK;
+}
+
+rpb_status rpb_mesh_stats(const rpb_mesh* m, rpb_stats* o)
+{
+    if (!m || !o) { set_error("null argument"); return RPB_EINVAL; }
+    o->vertex_count = m->nV;
+    o->simplex_count = m->N;
+    o->cluster_count = m->NC;
+    o->tree_depth = m->tree.depth;
+    o->near_nnz = m->tree.near.nnz();
+    o->far_nnz = m->tree.far.nnz();
+    o->verynear_nnz = m->tree.verynear.nnz();
+    o->inter_nnz = m->tree.inter.nnz();
+    o->tree_build_seconds = m->build_seconds;
+    o->device_bytes = m->device_bytes();
+    return RPB_OK;
+}
+
+rpb_status rpb_mesh_tree(const rpb_mesh* m, int* perm, int* C_begin, int* C_end, int* C_left, int* C_right)
+{
+    if (!m) { set_error("null mesh"); return RPB_EINVAL; }
+    const HostTree& T = m->tree;
+    if (perm) std::copy(T.perm.begin(), T.perm.end(), perm);
+    if (C_begin) std::copy(T.C_begin.begin(), T.C_begin.end(), C_begin);
+    if (C_end) std::copy(T.C_end.begin(), T.C_end.end(), C_end);
+    if (C_left) std::copy(T.C_left.begin(), T.C_left.end(), C_left);
+    if (C_right) std::copy(T.C_right.begin(), T.C_right.end(), C_right);
+    return RPB_OK;
+}
+
+rpb_status rpb_mesh_pattern(const rpb_mesh* m, int which, int64_t* rowptr, int* colidx)
+{
+    if (!m) { set_error("null mesh"); return RPB_EINVAL; }
+    const SymPattern* P = which == 0 ? &m->tree.near : which == 1 ? &m->tree.far : which == 2 ? &m->tree.verynear
+                        : which == 3 ? &m->tree.inter : nullptr;
+    if (!P) { set_error("pattern id must be 0..3"); return RPB_EINVAL; }
+    if (rowptr) std::copy(P->rp.begin(), P->rp.end(), rowptr);
+    if (colidx) std::copy(P->ci.begin(), P->ci.end(), colidx);
+    return RPB_OK;
+}
+
+struct rpb_host_tree {
+    HostTree tree;
+    double seconds = 0;
+};
+
+rpb_status rpb_tree_build_host(int dom_dim, const double* V, int64_t nV, const int* S, int64_t nS,
+                               const rpb_settings* settings, rpb_host_tree** out)
+{
+    if (!out) { set_error("out is null"); return RPB_EINVAL; }
+    *out = nullptr;
+    if (!V || !S || nV <= 0 || nS <= 0) { set_error("empty mesh"); return RPB_EINVAL; }
+    if (nV > (1ll << 30) || nS > (1ll << 29)) { set_error("mesh too large for 32-bit indices"); return RPB_EINVAL; }
+    rpb_settings set;
+    rpb_default_settings(&set);
+    if (settings) set = *settings;
+    if (set.split_threshold != 1) { set_error("only split_threshold = 1 is supported"); return RPB_EINVAL; }
+    TreeSettings ts;
+    ts.theta_far = set.far_field_separation;
+    ts.theta_near = set.near_field_separation;
+    ts.max_refinement = set.max_refinement;
+    ts.threads = set.thread_count > 0 ? set.thread_count : std::max(1u, std::thread::hardware_concurrency());
+    auto* t = new rpb_host_tree();
+    const auto t0 = std::chrono::steady_clock::now();
+    const std::string err = build_tree(dom_dim, V, static_cast<int>(nV), S, static_cast<int>(nS), ts, t->tree);
+    if (!err.empty()) { delete t; set_error(err); return RPB_EINVAL; }
+    t->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    *out = t;
+    return RPB_OK;
+}
+
+rpb_status rpb_tree_host_stats(const rpb_host_tree* t, rpb_stats* o)
+{
+    if (!t || !o) { set_error("null argument"); return RPB_EINVAL; }
+    const HostTree& T = t->tree;
+    std::memset(o, 0, sizeof(*o));
+    o->vertex_count = T.nV;
+    o->simplex_count = T.N;
+    o->cluster_count = T.NC;
+    o->tree_depth = T.depth;
+    o->near_nnz = T.near.nnz();
+    o->far_nnz = T.far.nnz();
+    o->verynear_nnz = T.verynear.nnz();
+    o->inter_nnz = T.inter.nnz();
+    o->tree_build_seconds = t->seconds;
+    return RPB_OK;
+}
+
+rpb_status rpb_tree_host_arrays(const rpb_host_tree* t, int* perm, int* C_begin, int* C_end, int* C_left,
+                                int* C_right)
+{
+    if (!t) { set_error("null tree"); return RPB_EINVAL; }
+    const HostTree& T = t->tree;
+    if (perm) std::copy(T.perm.begin(), T.perm.end(), perm);
+    if (C_begin) std::copy(T.C_begin.begin(), T.C_begin.end(), C_begin);
+    if (C_end) std::copy(T.C_end.begin(), T.C_end.end(), C_end);
+    if (C_left) std::copy(T.C_left.begin(), T.C_left.end(), C_left);
+    if (C_right) std::copy(T.C_right.begin(), T.C_right.end(), C_right);
+    return RPB_OK;
+}
+
+rpb_status rpb_tree_host_pattern(const rpb_host_tree* t, int which, int64_t* rowptr, int* colidx)
+{
+    if (!t) { set_error("null tree"); return RPB_EINVAL; }
+    const SymPattern* P = which == 0 ? &t->tree.near : which == 1 ? &t->tree.far : which == 2 ? &t->tree.verynear
+                        : which == 3 ? &t->tree.inter : nullptr;
+    if (!P) { set_error("pattern id must be 0..3"); return RPB_EINVAL; }
+    if (rowptr) std::copy(P->rp.begin(), P->rp.end(), rowptr);
+    if (colidx) std::copy(P->ci.begin(), P->ci.end(), colidx);
+    return RPB_OK;
+}
+
+rpb_status rpb_tree_host_destroy(rpb_host_tree* t)
+{
+    delete t;
+    return RPB_OK;
+}
+
+rpb_status rpb_h1_solve_host(const rpb_host_tree* t, const double* V, const int* S, const double* B, double* X,
+                             int nrhs)
+{
+    if (!t || !V || !S || !B || !X || nrhs <= 0) { set_error("null argument"); return RPB_EINVAL; }
+    const HostTree& T = t->tree;
+    const CsrMatrix H = assemble_h1(T.dom, V, T.nV, S, T.N, 1.0, 1.0);
+    const std::vector<int> perm = nested_dissection_ordering(T, S, T.nV);
+    CholeskyFactor F;
+    const std::string err = cholesky_factor(H, perm, F);
+    if (!err.empty()) { set_error(err); return RPB_EINVAL; }
+    const int n = T.nV;
+    std::vector<double> y(n);
+    for (int c = 0; c < nrhs; ++c) {
+        for (int i = 0; i < n; ++i) {  // forward: rows of L, diagonal last
+            double s = B[static_cast<int64_t>(nrhs) * F.perm[i] + c];
+            const int64_t k1 = F.lower_rp[i + 1] - 1;
+            for (int64_t k = F.lower_rp[i]; k < k1; ++k) s -= F.lower_val[k] * y[F.lower_ci[k]];
+            y[i] = s / F.lower_val[k1];
+        }
+        for (int i = n; i-- > 0;) {    // backward: rows of L^T, diagonal first
+            double s = y[i];
+            const int64_t k0 = F.upper_rp[i];
+            for (int64_t k = k0 + 1; k < F.upper_rp[i + 1]; ++k) s -= F.upper_val[k] * y[F.upper_ci[k]];
+            y[i] = s / F.upper_val[k0];
+        }
+        for (int i = 0; i < n; ++i) X[static_cast<int64_t>(nrhs) * F.perm[i] + c] = y[i];
+    }
+    return RPB_OK;
+}
+
+rpb_status rpb_mesh_semistatic_update(rpb_mesh* m, const double* V, int transp)
+{
+    if (!m || !V) { set_error("null argument"); return RPB_EINVAL; }
+    RPB_CUDA(cudaSetDevice(m->device));
+    if (transp) {
+        std::vector<double> t(3 * static_cast<size_t>(m->nV));
+        for (int v = 0; v < m->nV; ++v)
+            for (int k = 0; k < 3; ++k) t[3 * static_cast<size_t>(v) + k] = V[static_cast<size_t>(k) * m->nV + v];
+        RPB_CUDA(cudaMemcpyAsync(m->V.ptr, t.data(), m->V.bytes(), cudaMemcpyHostToDevice, m->stream));
+        RPB_CUDA(cudaStreamSynchronize(m->stream));
+    } else {
+        RPB_CUDA(cudaMemcpyAsync(m->V.ptr, V, m->V.bytes(), cudaMemcpyHostToDevice, m->stream));
+    }
+    return launch_geometry(m);
+}
+
+rpb_status rpb_mesh_semistatic_update_device(rpb_mesh* m, const double* V_dev)
+{
+    if (!m || !V_dev) { set_error("null argument"); return RPB_EINVAL; }
+    RPB_CUDA(cudaSetDevice(m->device));
+    RPB_CUDA(cudaMemcpyAsync(m->V.ptr, V_dev, m->V.bytes(), cudaMemcpyDeviceToDevice, m->stream));
+    return launch_geometry(m);
+}
+
+rpb_status rpb_tpe0_value(rpb_mesh* m, double q, double p, double* energy)
+{
+    if (!m || !energy) { set_error("null argument"); return RPB_EINVAL; }
+    return evaluate(m, q, p, false, 0.0, 0.0, nullptr, 3, energy);
+}
+
+rpb_status rpb_tpe0_differential_device(rpb_mesh* m, double q, double p, double alpha, double beta, double* Y_dev,
+                                        int ldY, double* energy)
+{
+    if (!m || !Y_dev) { set_error("null argument"); return RPB_EINVAL; }
+    if (ldY < 3) { set_error("ldY must be >= AMB_DIM = 3"); return RPB_EINVAL; }
+    return evaluate(m, q, p, true, alpha, beta, Y_dev, ldY, energy);
+}
+
+rpb_status rpb_tpe0_differential(rpb_mesh* m, double q, double p, double alpha, double beta, double* Y, int ldY,
+                                 double* energy)
+{
+    if (!m || !Y) { set_error("null argument"); return RPB_EINVAL; }
+    if (ldY < 3) { set_error("ldY must be >= AMB_DIM = 3"); return RPB_EINVAL; }
+    RPB_CUDA(cudaSetDevice(m->device));
+    if (beta != 0.0)
+        RPB_CUDA(cudaMemcpy2DAsync(m->Y.ptr, 3 * sizeof(double), Y, ldY * sizeof(double), 3 * sizeof(double), m->nV,
+                                   cudaMemcpyHostToDevice, m->stream));
+    double e = 0;
+    rpb_status st = evaluate(m, q, p, true, alpha, beta, m->Y.ptr, 3, &e);
+    if (st != RPB_OK) return st;
+    RPB_CUDA(cudaMemcpy2DAsync(Y, ldY * sizeof(double), m->Y.ptr, 3 * sizeof(double), 3 * sizeof(double), m->nV,
+                               cudaMemcpyDeviceToHost, m->stream));
+    RPB_CUDA(cudaStreamSynchronize(m->stream));
+    if (energy) *energy = e;
+    return RPB_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,38 @@
+// Internal entry points shared between the translation units of librepulsor_b200.
+#pragma once
+
+#include <string>
+
+#include "../../include/repulsor_b200.h"
+#include "rpb_device.cuh"
+
+struct rpb_mesh;
+
+namespace rpb {
+
+void set_error(const std::string& msg);
+TPExp make_exp(int dom, double q, double p);
+rpb_status check_exponents(double q, double p);
+rpb_status launch_geometry(rpb_mesh* m);
+rpb_status evaluate(rpb_mesh* m, double q, double p, bool diff, double alpha, double beta, double* Y_dev, int ldY,
+                    double* energy_host);
+
+// very-near adaptive quadrature (rpb_verynear.cu)
+rpb_status launch_vf(rpb_mesh* m, const TPExp& ex, bool diff);
+rpb_status launch_vf_metric(rpb_mesh* m, const TPExp& ex, float2* vals, double2* diag);
+
+// metric (rpb_metric.cu)
+rpb_status metric_init(rpb_mesh* m, const double* Vh, const int* Sh);
+rpb_status metric_multiply_dev(rpb_mesh* m, double q, double p, double alpha, const double* X, int ldX, double beta,
+                               double* Y, int ldY, int flags);
+rpb_status plap_multiply_dev(rpb_mesh* m, double s, double alpha, const double* X, int ldX, double beta, double* Y,
+                             int ldY);
+
+// solver (rpb_solver.cu)
+void solver_free(rpb_mesh* m);
+rpb_status reference_precondition(rpb_mesh* m, double q, double p, const double* X, double* Y);
+
+// learned preconditioner (rpb_learned.cu): Z = MLP correction of the residual R (n x 3, device)
+rpb_status learned_precondition(rpb_mesh* m, double q, double p, const double* R, double* Z);
+
+}  // namespace rpb

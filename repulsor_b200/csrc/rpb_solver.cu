@@ -1,0 +1,561 @@
+// MetricBase::Solve and MultiplyPreconditioner on the B200
+// (src/Metrics/MetricDimRestricted.hpp:232-289, src/Metrics/TangentPointMetric0.hpp:88-126).
+//
+// The reference runs left-preconditioned GMRES with P = H1^{-1} L_{2-s} H1^{-1}. Here the
+// metric (symmetric, positive semi-definite; its kernel is the translations) is solved by
+// conjugate gradients with FP64 inner products and residual recurrence, one independent CG
+// per right-hand-side column, with
+//   RPB_PRECOND_NONE       identity,
+//   RPB_PRECOND_REFERENCE  H1^{-1} L_{2-s} H1^{-1}: host Cholesky of the H1 metric (nested-
+//                          dissection order from the cluster tree), GPU triangular solves,
+//                          GPU pseudo-Laplacian,
+//   RPB_PRECOND_LEARNED    per-cluster MLP (rpb_learned.cu) inside flexible CG, falling back
+//                          to REFERENCE when the flexible iteration stalls.
+// Convergence is decided on the true relative residual ||B - A X|| / ||B|| per column.
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "host/sparse_cholesky.hpp"
+#include "rpb_internal.cuh"
+#include "rpb_mesh.cuh"
+#include "rpb_solver.cuh"
+
+namespace rpb {
+
+#define RPB_CUDA(call)                                                                        \
+    do {                                                                                      \
+        cudaError_t e_ = (call);                                                              \
+        if (e_ != cudaSuccess) {                                                              \
+            set_error(std::string("CUDA error: ") + cudaGetErrorString(e_) + " at " #call);   \
+            return e_ == cudaErrorMemoryAllocation ? RPB_ENOMEM : RPB_ECUDA;                  \
+        }                                                                                     \
+    } while (0)
+
+// ------------------------------------------------------------------------------------------
+// Sync-free sparse triangular solves with 3 right-hand sides. Warps take rows in
+// dependency order from a global ticket; a row waits (bounded) on the ready flags of
+// the rows it depends on, which were taken earlier by running warps. Flags carry the
+// launch's epoch so they never need clearing.
+// ------------------------------------------------------------------------------------------
+__device__ __forceinline__ int ld_acquire(const int* p)
+{
+    int v;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void st_release(int* p, int v)
+{
+    asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+constexpr long long kSpinLimit = 1ll << 26;
+
+struct TrsvArgs {
+    int n;
+    const int64_t* rp;
+    const int* ci;
+    const double* val;
+    const double* b;          // right-hand side, n x 3
+    const int* perm_in;       // if set, row i reads b[perm_in[i]]
+    double* y;                // solution in factor order, n x 3
+    double* out;              // if set, out[perm_out[i]] = y_i
+    const int* perm_out;
+    int* flags;
+    int epoch;
+    unsigned* ticket;
+    int* err;
+};
+
+// LOWER: rows ascending, diagonal last in each row. UPPER: rows descending, diagonal first.
+template <bool LOWER>
+__global__ void __launch_bounds__(256) k_trsv(TrsvArgs A)
+{
+    const int lane = threadIdx.x & 31;
+    for (;;) {
+        int t = 0;
+        if (lane == 0) t = static_cast<int>(atomicAdd(A.ticket, 1u));
+        t = __shfl_sync(0xffffffffu, t, 0);
+        if (t >= A.n) return;
+        const int row = LOWER ? t : A.n - 1 - t;
+        const int64_t k0 = A.rp[row], k1 = A.rp[row + 1];
+        const int64_t dpos = LOWER ? k1 - 1 : k0;
+        const int64_t ob = LOWER ? k0 : k0 + 1, oe = LOWER ? k1 - 1 : k1;
+        double s0 = 0, s1 = 0, s2 = 0;
+        for (int64_t k = ob + lane; k < oe; k += 32) {
+            const int j = A.ci[k];
+            long long it = 0;
+            while (ld_acquire(A.flags + j) != A.epoch) {
+                if (++it > kSpinLimit) {
+                    atomicExch(A.err, 1);
+                    break;
+                }
+            }
+            const double v = A.val[k];
+            s0 += v * __ldcg(A.y + 3 * static_cast<int64_t>(j) + 0);
+            s1 += v * __ldcg(A.y + 3 * static_cast<int64_t>(j) + 1);
+            s2 += v * __ldcg(A.y + 3 * static_cast<int64_t>(j) + 2);
+        }
+        s0 = warp_sum_f64(s0);
+        s1 = warp_sum_f64(s1);
+        s2 = warp_sum_f64(s2);
+        if (lane == 0) {
+            const int src = A.perm_in ? A.perm_in[row] : row;
+            const double d = A.val[dpos];
+            const double y0 = (A.b[3 * static_cast<int64_t>(src) + 0] - s0) / d;
+            const double y1 = (A.b[3 * static_cast<int64_t>(src) + 1] - s1) / d;
+            const double y2 = (A.b[3 * static_cast<int64_t>(src) + 2] - s2) / d;
+            __stcg(A.y + 3 * static_cast<int64_t>(row) + 0, y0);
+            __stcg(A.y + 3 * static_cast<int64_t>(row) + 1, y1);
+            __stcg(A.y + 3 * static_cast<int64_t>(row) + 2, y2);
+            if (A.out) {
+                const int dst = A.perm_out[row];
+                A.out[3 * static_cast<int64_t>(dst) + 0] = y0;
+                A.out[3 * static_cast<int64_t>(dst) + 1] = y1;
+                A.out[3 * static_cast<int64_t>(dst) + 2] = y2;
+            }
+            __threadfence();
+            st_release(A.flags + row, A.epoch);
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// CG vector kernels (FP64). Scalars live on the device; per column c:
+//   S_RZ rz, S_RZOLD previous rz, S_PAP (p,Ap), S_RR (r,r), S_ZR_OLD (z, r_old)
+// ------------------------------------------------------------------------------------------
+enum { S_RZ = 0, S_RZOLD = 3, S_PAP = 6, S_RR = 9, S_ZROLD = 12, S_ACTIVE = 15, S_COUNT = 18 };
+
+struct DotArgs {
+    int n;                    // rows (n x 3)
+    const double* a;
+    const double* b;
+    const double* c;          // optional: accumulate (a, b - c) in the second slot
+    double* partials;         // gridDim.x x 6
+    unsigned* done;
+    double* out0;             // 3 results (a, b)
+    double* out1;             // 3 results (a, b - c) if c
+};
+
+__global__ void __launch_bounds__(256) k_dot3(DotArgs A)
+{
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    double s[6] = {0, 0, 0, 0, 0, 0};
+    for (int i = tid; i < A.n; i += gridDim.x * blockDim.x) {
+        for (int c = 0; c < 3; ++c) {
+            const double a = A.a[3 * static_cast<int64_t>(i) + c];
+            const double b = A.b[3 * static_cast<int64_t>(i) + c];
+            s[c] += a * b;
+            if (A.c) s[3 + c] += a * (b - A.c[3 * static_cast<int64_t>(i) + c]);
+        }
+    }
+    __shared__ double sh[8][6];
+    __shared__ bool last;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int k = 0; k < 6; ++k) {
+        const double v = warp_sum_f64(s[k]);
+        if (lane == 0) sh[w][k] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 6) {
+        double v = 0;
+        for (int q = 0; q < (blockDim.x >> 5); ++q) v += sh[q][threadIdx.x];
+        A.partials[6 * blockIdx.x + threadIdx.x] = v;
+        __threadfence();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        last = (atomicAdd(A.done, 1u) == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (last && threadIdx.x < 6) {
+        __threadfence();
+        double v = 0;
+        for (int b = 0; b < static_cast<int>(gridDim.x); ++b) v += __ldcg(A.partials + 6 * b + threadIdx.x);
+        if (threadIdx.x < 3) A.out0[threadIdx.x] = v;
+        else if (A.out1) A.out1[threadIdx.x - 3] = v;
+    }
+    if (last && threadIdx.x == 0) *A.done = 0u;
+}
+
+// x += alpha p, r -= alpha Ap with alpha = rz / (p, Ap) per active column
+__global__ void k_cg_update(int n, const double* S, double* x, double* r, const double* p, const double* Ap)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    for (int c = 0; c < 3; ++c) {
+        if (S[S_ACTIVE + c] == 0.0) continue;
+        const double pap = S[S_PAP + c];
+        const double alpha = pap != 0.0 ? S[S_RZ + c] / pap : 0.0;
+        const int64_t k = 3 * static_cast<int64_t>(i) + c;
+        x[k] += alpha * p[k];
+        r[k] -= alpha * Ap[k];
+    }
+}
+
+// p = z + beta p; beta = rz_new / rz_old (fixed preconditioner) or (z, r - r_old) / rz_old
+// (flexible CG, Polak-Ribiere form).
+__global__ void k_cg_direction(int n, const double* S, bool flexible, const double* z, double* p)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    for (int c = 0; c < 3; ++c) {
+        if (S[S_ACTIVE + c] == 0.0) continue;
+        const double old = S[S_RZOLD + c];
+        const double num = flexible ? S[S_ZROLD + c] : S[S_RZ + c];
+        const double beta = old != 0.0 ? num / old : 0.0;
+        const int64_t k = 3 * static_cast<int64_t>(i) + c;
+        p[k] = z[k] + beta * p[k];
+    }
+}
+
+__global__ void k_axpby3(int n, double alpha, const double* x, double beta, double* y, int ldy)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    for (int c = 0; c < 3; ++c) {
+        double& t = y[static_cast<int64_t>(ldy) * i + c];
+        t = alpha * x[3 * static_cast<int64_t>(i) + c] + (beta == 0.0 ? 0.0 : beta * t);
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// host side
+// ------------------------------------------------------------------------------------------
+Solver::~Solver() {}
+
+static rpb_status ensure_solver(rpb_mesh* m)
+{
+    if (!m->solver) m->solver = new Solver();
+    Solver& s = *m->solver;
+    if (!s.vec.ptr) {
+        const size_t n3 = 3 * static_cast<size_t>(m->nV);
+        RPB_CUDA(s.vec.alloc(Solver::NVEC * n3));
+        RPB_CUDA(s.scal.alloc(S_COUNT));
+        RPB_CUDA(s.partials.alloc(6 * 1024));
+        RPB_CUDA(s.done.alloc(1));
+        RPB_CUDA(s.err.alloc(1));
+        RPB_CUDA(cudaMemsetAsync(s.done.ptr, 0, s.done.bytes(), m->stream));
+        RPB_CUDA(cudaMemsetAsync(s.err.ptr, 0, s.err.bytes(), m->stream));
+        RPB_CUDA(cudaMallocHost(reinterpret_cast<void**>(&s.host_scal), sizeof(double) * S_COUNT));
+    }
+    return RPB_OK;
+}
+
+void solver_free(rpb_mesh* m)
+{
+    if (m->solver) {
+        if (m->solver->host_scal) cudaFreeHost(m->solver->host_scal);
+        delete m->solver;
+        m->solver = nullptr;
+    }
+}
+
+// H1 factor for the current geometry (the reference caches H1Metric/H1Solver on the mesh
+// and clears them with the cache on SemiStaticUpdate, src/SimplicialMesh.hpp:368).
+static rpb_status ensure_h1(rpb_mesh* m)
+{
+    Solver& s = *m->solver;
+    if (s.h1_version == m->geometry_version) return RPB_OK;
+    std::vector<double> V(3 * static_cast<size_t>(m->nV));
+    std::vector<int> S(static_cast<size_t>(m->size) * m->N);
+    RPB_CUDA(cudaMemcpyAsync(V.data(), m->V.ptr, m->V.bytes(), cudaMemcpyDeviceToHost, m->stream));
+    RPB_CUDA(cudaMemcpyAsync(S.data(), m->S.ptr, m->S.bytes(), cudaMemcpyDeviceToHost, m->stream));
+    RPB_CUDA(cudaStreamSynchronize(m->stream));
+    const auto t0 = std::chrono::steady_clock::now();
+    const CsrMatrix H = assemble_h1(m->dom, V.data(), m->nV, S.data(), m->N, 1.0, 1.0);
+    if (s.nd_perm.empty()) s.nd_perm = nested_dissection_ordering(m->tree, S.data(), m->nV);
+    CholeskyFactor F;
+    const std::string err = cholesky_factor(H, s.nd_perm, F);
+    if (!err.empty()) { set_error(err); return RPB_EINVAL; }
+    s.factor_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    s.factor_nnz = F.nnz();
+    cudaStream_t st = m->stream;
+    RPB_CUDA(s.lo_rp.alloc(F.lower_rp.size()));
+    RPB_CUDA(s.lo_ci.alloc(F.lower_ci.size()));
+    RPB_CUDA(s.lo_val.alloc(F.lower_val.size()));
+    RPB_CUDA(s.up_rp.alloc(F.upper_rp.size()));
+    RPB_CUDA(s.up_ci.alloc(F.upper_ci.size()));
+    RPB_CUDA(s.up_val.alloc(F.upper_val.size()));
+    RPB_CUDA(s.perm.alloc(F.perm.size()));
+    RPB_CUDA(s.flags.alloc(m->nV));
+    RPB_CUDA(s.ticket.alloc(4));
+    RPB_CUDA(s.tri.alloc(3 * static_cast<size_t>(m->nV)));
+    RPB_CUDA(s.tmp.alloc(3 * static_cast<size_t>(m->nV)));
+    RPB_CUDA(cudaMemcpyAsync(s.lo_rp.ptr, F.lower_rp.data(), s.lo_rp.bytes(), cudaMemcpyHostToDevice, st));
+    RPB_CUDA(cudaMemcpyAsync(s.lo_ci.ptr, F.lower_ci.data(), s.lo_ci.bytes(), cudaMemcpyHostToDevice, st));
+    RPB_CUDA(cudaMemcpyAsync(s.lo_val.ptr, F.lower_val.data(), s.lo_val.bytes(), cudaMemcpyHostToDevice, st));
+    RPB_CUDA(cudaMemcpyAsync(s.up_rp.ptr, F.upper_rp.data(), s.up_rp.bytes(), cudaMemcpyHostToDevice, st));
+    RPB_CUDA(cudaMemcpyAsync(s.up_ci.ptr, F.upper_ci.data(), s.up_ci.bytes(), cudaMemcpyHostToDevice, st));
+    RPB_CUDA(cudaMemcpyAsync(s.up_val.ptr, F.upper_val.data(), s.up_val.bytes(), cudaMemcpyHostToDevice, st));
+    RPB_CUDA(cudaMemcpyAsync(s.perm.ptr, F.perm.data(), s.perm.bytes(), cudaMemcpyHostToDevice, st));
+    RPB_CUDA(cudaMemsetAsync(s.flags.ptr, 0, s.flags.bytes(), st));
+    RPB_CUDA(cudaStreamSynchronize(st));
+    s.epoch = 0;
+    s.h1_version = m->geometry_version;
+    return RPB_OK;
+}
+
+// out = H1^{-1} b (b, out: n x 3 contiguous, device)
+static rpb_status h1_solve(rpb_mesh* m, const double* b, double* out)
+{
+    Solver& s = *m->solver;
+    const int n = m->nV;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int blocks = std::min((n + 7) / 8, sms * 8);
+    RPB_CUDA(cudaMemsetAsync(s.ticket.ptr, 0, s.ticket.bytes(), m->stream));
+    TrsvArgs A;
+    A.n = n;
+    A.rp = s.lo_rp.ptr; A.ci = s.lo_ci.ptr; A.val = s.lo_val.ptr;
+    A.b = b; A.perm_in = s.perm.ptr; A.y = s.tri.ptr; A.out = nullptr; A.perm_out = nullptr;
+    A.flags = s.flags.ptr; A.epoch = ++s.epoch; A.ticket = s.ticket.ptr; A.err = s.err.ptr;
+    k_trsv<true><<<blocks, 256, 0, m->stream>>>(A);
+    RPB_CUDA(cudaGetLastError());
+    TrsvArgs U = A;
+    U.rp = s.up_rp.ptr; U.ci = s.up_ci.ptr; U.val = s.up_val.ptr;
+    U.b = s.tri.ptr; U.perm_in = nullptr; U.y = s.tmp.ptr; U.out = out; U.perm_out = s.perm.ptr;
+    U.epoch = ++s.epoch; U.ticket = s.ticket.ptr + 1;
+    k_trsv<false><<<blocks, 256, 0, m->stream>>>(U);
+    RPB_CUDA(cudaGetLastError());
+    return RPB_OK;
+}
+
+// Y = H1^{-1} L_{2-s} H1^{-1} X   (X, Y: n x 3 contiguous device; Y may alias X)
+rpb_status reference_precondition(rpb_mesh* m, double q, double p, const double* X, double* Y)
+{
+    rpb_status st;
+    if ((st = ensure_solver(m)) != RPB_OK) return st;
+    if ((st = ensure_h1(m)) != RPB_OK) return st;
+    Solver& s = *m->solver;
+    const double s_tp = (p - m->dom) / q;
+    double* Z = s.vec.ptr + Solver::V_PRE * 3 * static_cast<size_t>(m->nV);
+    if ((st = h1_solve(m, X, Z)) != RPB_OK) return st;
+    if ((st = plap_multiply_dev(m, 2.0 - s_tp, 1.0, Z, 3, 0.0, Z, 3)) != RPB_OK) return st;
+    return h1_solve(m, Z, Y);
+}
+
+static rpb_status read_scalars(rpb_mesh* m)
+{
+    Solver& s = *m->solver;
+    RPB_CUDA(cudaMemcpyAsync(s.host_scal, s.scal.ptr, sizeof(double) * S_COUNT, cudaMemcpyDeviceToHost, m->stream));
+    RPB_CUDA(cudaStreamSynchronize(m->stream));
+    int e = 0;
+    RPB_CUDA(cudaMemcpy(&e, s.err.ptr, sizeof(int), cudaMemcpyDeviceToHost));
+    if (e) {
+        cudaMemset(s.err.ptr, 0, sizeof(int));
+        set_error("a triangular-solve dependency wait exceeded its bound");
+        return RPB_ETIMEOUT;
+    }
+    return RPB_OK;
+}
+
+static rpb_status dot3(rpb_mesh* m, const double* a, const double* b, const double* c, double* out0, double* out1)
+{
+    Solver& s = *m->solver;
+    DotArgs A;
+    A.n = m->nV; A.a = a; A.b = b; A.c = c;
+    A.partials = s.partials.ptr; A.done = s.done.ptr; A.out0 = out0; A.out1 = out1;
+    const int blocks = std::min(1024, (m->nV + 255) / 256);
+    k_dot3<<<blocks, 256, 0, m->stream>>>(A);
+    RPB_CUDA(cudaGetLastError());
+    return RPB_OK;
+}
+
+rpb_status apply_preconditioner(rpb_mesh* m, int kind, double q, double p, const double* R, double* Z);  // below
+
+// Solves A Z = B (device, n x 3) by (flexible) PCG. Returns iterations and true residuals.
+static rpb_status cg_solve(rpb_mesh* m, double q, double p, const double* B, int max_iter, double tol, int precond,
+                           int* iters_out, double* relres_out)
+{
+    rpb_status st;
+    if ((st = ensure_solver(m)) != RPB_OK) return st;
+    Solver& s = *m->solver;
+    const int n = m->nV;
+    const size_t n3 = 3 * static_cast<size_t>(n);
+    double* x = s.vec.ptr + Solver::V_X * n3;
+    double* r = s.vec.ptr + Solver::V_R * n3;
+    double* z = s.vec.ptr + Solver::V_Z * n3;
+    double* pv = s.vec.ptr + Solver::V_P * n3;
+    double* Ap = s.vec.ptr + Solver::V_AP * n3;
+    double* rold = s.vec.ptr + Solver::V_ROLD * n3;
+    double* S = s.scal.ptr;
+    cudaStream_t stream = m->stream;
+    const int eb = (n + 255) / 256;
+    const bool flexible = (precond == RPB_PRECOND_LEARNED);
+    int kind = precond;
+
+    // ||B|| per column
+    RPB_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * n3, stream));
+    if ((st = dot3(m, B, B, nullptr, S + S_RR, nullptr)) != RPB_OK) return st;
+    if ((st = read_scalars(m)) != RPB_OK) return st;
+    double bnorm[3];
+    for (int c = 0; c < 3; ++c) bnorm[c] = std::sqrt(s.host_scal[S_RR + c]);
+    double active[3];
+    for (int c = 0; c < 3; ++c) active[c] = bnorm[c] > 0 ? 1.0 : 0.0;
+    int it = 0;
+    double rel[3] = {0, 0, 0};
+    int restarts = 0;
+    double best[3] = {1e300, 1e300, 1e300};
+    int since_best = 0;
+    bool stalled_flag = false;
+    while (true) {
+        // r = B - A x (true residual), z = M r, p = z
+        if ((st = metric_multiply_dev(m, q, p, -1.0, x, 3, 0.0, r, 3, 7)) != RPB_OK) return st;
+        k_axpby3<<<eb, 256, 0, stream>>>(n, 1.0, B, 1.0, r, 3);
+        RPB_CUDA(cudaGetLastError());
+        if ((st = dot3(m, r, r, nullptr, S + S_RR, nullptr)) != RPB_OK) return st;
+        if ((st = read_scalars(m)) != RPB_OK) return st;
+        bool done = true;
+        for (int c = 0; c < 3; ++c) {
+            rel[c] = bnorm[c] > 0 ? std::sqrt(s.host_scal[S_RR + c]) / bnorm[c] : 0.0;
+            active[c] = rel[c] > tol ? 1.0 : 0.0;
+            if (active[c] != 0.0) done = false;
+        }
+        if (done || it >= max_iter) break;
+        if (stalled_flag && kind == RPB_PRECOND_LEARNED) kind = RPB_PRECOND_REFERENCE;  // fallback on stall
+        stalled_flag = false;
+        ++restarts;
+        RPB_CUDA(cudaMemcpyAsync(S + S_ACTIVE, active, sizeof(active), cudaMemcpyHostToDevice, stream));
+        if ((st = apply_preconditioner(m, kind, q, p, r, z)) != RPB_OK) return st;
+        RPB_CUDA(cudaMemcpyAsync(pv, z, sizeof(double) * n3, cudaMemcpyDeviceToDevice, stream));
+        if ((st = dot3(m, r, z, nullptr, S + S_RZ, nullptr)) != RPB_OK) return st;
+        // inner CG iterations on the recurrence
+        while (it < max_iter) {
+            if ((st = metric_multiply_dev(m, q, p, 1.0, pv, 3, 0.0, Ap, 3, 7)) != RPB_OK) return st;
+            if ((st = dot3(m, pv, Ap, nullptr, S + S_PAP, nullptr)) != RPB_OK) return st;
+            if (flexible) RPB_CUDA(cudaMemcpyAsync(rold, r, sizeof(double) * n3, cudaMemcpyDeviceToDevice, stream));
+            k_cg_update<<<eb, 256, 0, stream>>>(n, S, x, r, pv, Ap);
+            RPB_CUDA(cudaGetLastError());
+            ++it;
+            if ((st = dot3(m, r, r, nullptr, S + S_RR, nullptr)) != RPB_OK) return st;
+            if ((st = read_scalars(m)) != RPB_OK) return st;
+            bool conv = true, stalled = false;
+            for (int c = 0; c < 3; ++c) {
+                if (active[c] == 0.0) continue;
+                const double rc = bnorm[c] > 0 ? std::sqrt(s.host_scal[S_RR + c]) / bnorm[c] : 0.0;
+                if (rc > tol) conv = false;
+                if (rc < 0.9 * best[c]) { best[c] = rc; since_best = 0; }
+            }
+            if (!conv && ++since_best > 60) stalled = true;
+            if (conv || stalled) {
+                stalled_flag = stalled;
+                since_best = 0;
+                break;
+            }
+            RPB_CUDA(cudaMemcpyAsync(S + S_RZOLD, S + S_RZ, 3 * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+            if ((st = apply_preconditioner(m, kind, q, p, r, z)) != RPB_OK) return st;
+            if ((st = dot3(m, z, r, flexible ? rold : nullptr, S + S_RZ, S + S_ZROLD)) != RPB_OK) return st;
+            k_cg_direction<<<eb, 256, 0, stream>>>(n, S, flexible, z, pv);
+            RPB_CUDA(cudaGetLastError());
+        }
+        if (restarts > 50) break;
+    }
+    if (iters_out) *iters_out = it;
+    if (relres_out)
+        for (int c = 0; c < 3; ++c) relres_out[c] = rel[c];
+    bool ok = true;
+    for (int c = 0; c < 3; ++c) ok = ok && !(rel[c] > tol);
+    if (!ok) {
+        set_error("Solve did not reach the tolerance within max_iter iterations");
+        return RPB_ENOTCONV;
+    }
+    return RPB_OK;
+}
+
+rpb_status apply_preconditioner(rpb_mesh* m, int kind, double q, double p, const double* R, double* Z)
+{
+    if (kind == RPB_PRECOND_NONE) {
+        RPB_CUDA(cudaMemcpyAsync(Z, R, sizeof(double) * 3 * static_cast<size_t>(m->nV), cudaMemcpyDeviceToDevice,
+                                 m->stream));
+        return RPB_OK;
+    }
+    if (kind == RPB_PRECOND_LEARNED) return learned_precondition(m, q, p, R, Z);
+    return reference_precondition(m, q, p, R, Z);
+}
+
+}  // namespace rpb
+
+using namespace rpb;
+
+extern "C" {
+
+rpb_status rpb_tpm0_precondition(rpb_mesh* m, double q, double p, double alpha, const double* X, int ldX, double beta,
+                                 double* Y, int ldY, int nrhs)
+{
+    if (!m || !X || !Y) { set_error("null argument"); return RPB_EINVAL; }
+    if (nrhs != 3) {
+        set_error("MultiplyPreconditioner: nrhs = " + std::to_string(nrhs) + " != 3 = AMB_DIM.");
+        return RPB_EINVAL;
+    }
+    if (ldX < 3 || ldY < 3) { set_error("leading dimensions must be >= 3"); return RPB_EINVAL; }
+    rpb_status st = check_exponents(q, p);
+    if (st != RPB_OK) return st;
+    RPB_CUDA(cudaSetDevice(m->device));
+    if ((st = ensure_solver(m)) != RPB_OK) return st;
+    cudaStream_t s = m->stream;
+    const int n = m->nV;
+    RPB_CUDA(cudaMemcpy2DAsync(m->X.ptr, 3 * sizeof(double), X, ldX * sizeof(double), 3 * sizeof(double), n,
+                               cudaMemcpyHostToDevice, s));
+    if (beta != 0.0)
+        RPB_CUDA(cudaMemcpy2DAsync(m->Yb.ptr, 3 * sizeof(double), Y, ldY * sizeof(double), 3 * sizeof(double), n,
+                                   cudaMemcpyHostToDevice, s));
+    double* Z = m->solver->vec.ptr + Solver::V_Z * 3 * static_cast<size_t>(n);
+    if ((st = reference_precondition(m, q, p, m->X.ptr, Z)) != RPB_OK) return st;
+    k_axpby3<<<(n + 255) / 256, 256, 0, s>>>(n, alpha, Z, beta, m->Yb.ptr, 3);
+    RPB_CUDA(cudaGetLastError());
+    RPB_CUDA(cudaMemcpy2DAsync(Y, ldY * sizeof(double), m->Yb.ptr, 3 * sizeof(double), 3 * sizeof(double), n,
+                               cudaMemcpyDeviceToHost, s));
+    RPB_CUDA(cudaStreamSynchronize(s));
+    int e = 0;
+    RPB_CUDA(cudaMemcpy(&e, m->solver->err.ptr, sizeof(int), cudaMemcpyDeviceToHost));
+    if (e) { cudaMemset(m->solver->err.ptr, 0, sizeof(int)); set_error("triangular-solve wait bound exceeded"); return RPB_ETIMEOUT; }
+    return RPB_OK;
+}
+
+rpb_status rpb_tpm0_solve(rpb_mesh* m, double q, double p, double alpha, const double* B, int ldB, double beta,
+                          double* X, int ldX, int nrhs, int max_iter, double tol, int precond, int* iterations,
+                          double* rel_residual)
+{
+    if (!m || !B || !X) { set_error("null argument"); return RPB_EINVAL; }
+    if (nrhs != 3) {
+        set_error("Solve: nrhs = " + std::to_string(nrhs) + " != 3 = AMB_DIM.");
+        return RPB_EINVAL;
+    }
+    if (ldB < 3 || ldX < 3) { set_error("leading dimensions must be >= 3"); return RPB_EINVAL; }
+    if (precond < RPB_PRECOND_NONE || precond > RPB_PRECOND_LEARNED) { set_error("unknown preconditioner kind"); return RPB_EINVAL; }
+    if (!(tol > 0) || max_iter < 0) { set_error("tolerance must be positive and max_iter >= 0"); return RPB_EINVAL; }
+    rpb_status st = check_exponents(q, p);
+    if (st != RPB_OK) return st;
+    RPB_CUDA(cudaSetDevice(m->device));
+    if ((st = ensure_solver(m)) != RPB_OK) return st;
+    cudaStream_t s = m->stream;
+    const int n = m->nV;
+    double* Bd = m->solver->vec.ptr + Solver::V_B * 3 * static_cast<size_t>(n);
+    RPB_CUDA(cudaMemcpy2DAsync(Bd, 3 * sizeof(double), B, ldB * sizeof(double), 3 * sizeof(double), n,
+                               cudaMemcpyHostToDevice, s));
+    int it = 0;
+    double rr[3] = {0, 0, 0};
+    rpb_status cs = cg_solve(m, q, p, Bd, max_iter, tol, precond, &it, rr);
+    if (cs != RPB_OK && cs != RPB_ENOTCONV) return cs;
+    if (iterations) *iterations = it;
+    if (rel_residual)
+        for (int c = 0; c < 3; ++c) rel_residual[c] = rr[c];
+    if (beta != 0.0)
+        RPB_CUDA(cudaMemcpy2DAsync(m->Yb.ptr, 3 * sizeof(double), X, ldX * sizeof(double), 3 * sizeof(double), n,
+                                   cudaMemcpyHostToDevice, s));
+    const double* xs = m->solver->vec.ptr + Solver::V_X * 3 * static_cast<size_t>(n);
+    k_axpby3<<<(n + 255) / 256, 256, 0, s>>>(n, alpha, xs, beta, m->Yb.ptr, 3);
+    RPB_CUDA(cudaGetLastError());
+    RPB_CUDA(cudaMemcpy2DAsync(X, ldX * sizeof(double), m->Yb.ptr, 3 * sizeof(double), 3 * sizeof(double), n,
+                               cudaMemcpyDeviceToHost, s));
+    RPB_CUDA(cudaStreamSynchronize(s));
+    return cs;
+}
+
+}  // extern "C"

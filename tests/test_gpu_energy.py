@@ -1,0 +1,106 @@
+"""TangentPointEnergy0 Value / Differential on the B200 through the C ABI, against
+the FP64 oracle. Tolerances: energy 1e-6 relative; differential 1e-5 relative in
+max norm (||D_gpu - D_ref||_inf / ||D_ref||_inf)."""
+import numpy as np
+import pytest
+
+import oracle
+import repulsor_b200 as rpb
+from repulsor_b200 import meshes
+
+pytestmark = pytest.mark.gpu
+
+E_TOL = 1e-6
+D_TOL = 1e-5
+Q, P = 6.0, 12.0
+
+
+def rel_max(a, b):
+    return float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
+
+
+def _pair(cfg, small):
+    dom, (V, S) = meshes.config_mesh(cfg, small=small)
+    M = rpb.SimplicialMesh(V, S)
+    O = oracle.OracleMesh(dom, V, S, threads=8)
+    return dom, V, S, M, O
+
+
+@pytest.mark.parametrize("cfg", [1, 2, 3])
+@pytest.mark.parametrize("small", [True, False])
+def test_energy_and_differential_match_oracle(cfg, small):
+    dom, V, S, M, O = _pair(cfg, small)
+    tpe = rpb.TangentPointEnergy0(Q, P)
+    E = tpe.Value(M)
+    E_ref = O.energy(Q, P)
+    assert abs(E - E_ref) <= E_TOL * abs(E_ref), (E, E_ref)
+    D = np.zeros((V.shape[0], 3))
+    E2 = tpe.Differential(M, 1.0, 0.0, D)
+    E2_ref, D_ref = O.differential(Q, P)
+    assert abs(E2 - E2_ref) <= E_TOL * abs(E2_ref)
+    assert rel_max(D, D_ref) <= D_TOL, rel_max(D, D_ref)
+
+
+def test_differential_alpha_beta_and_ldY():
+    dom, V, S, M, O = _pair(2, True)
+    tpe = rpb.TangentPointEnergy0(Q, P)
+    _, D_ref = O.differential(Q, P)
+    Y = np.random.default_rng(0).standard_normal((V.shape[0], 5))
+    Y0 = Y.copy()
+    tpe.Differential(M, 0.5, 2.0, Y)
+    assert rel_max(Y[:, :3], 0.5 * D_ref + 2.0 * Y0[:, :3]) <= D_TOL
+    assert np.array_equal(Y[:, 3:], Y0[:, 3:])      # columns beyond AMB_DIM untouched
+
+
+def test_cached_differential_and_value_consistency():
+    dom, V, S, M, O = _pair(1, True)
+    tpe = rpb.TangentPointEnergy0(Q, P)
+    D = tpe.Differential(M)
+    assert D.shape == (V.shape[0], 3)
+    assert tpe.Differential(M) is D                  # cached on the mesh like the reference
+    assert tpe.Value(M) == pytest.approx(O.energy(Q, P), rel=E_TOL)
+
+
+def test_semistatic_update_matches_oracle():
+    dom, V, S, M, O = _pair(3, True)
+    rng = np.random.default_rng(7)
+    V2 = V + 1e-3 * rng.standard_normal(V.shape)
+    M.SemiStaticUpdate(V2)
+    O.semistatic_update(V2)
+    tpe = rpb.TangentPointEnergy0(Q, P)
+    D = np.zeros_like(V2)
+    E = tpe.Differential(M, 1.0, 0.0, D)
+    E_ref, D_ref = O.differential(Q, P)
+    assert abs(E - E_ref) <= E_TOL * abs(E_ref)
+    assert rel_max(D, D_ref) <= D_TOL
+
+
+@pytest.mark.parametrize("cfg", [2, 3])
+def test_full_size_invariants(cfg):
+    """Size-independent properties at the benchmark size: translation invariance
+    sum_v dE/dx_v = 0 and Euler homogeneity sum_v x_v . dE/dx_v = (2n + q - p) E."""
+    dom, (V, S) = meshes.config_mesh(cfg)
+    M = rpb.SimplicialMesh(V, S)
+    tpe = rpb.TangentPointEnergy0(Q, P)
+    D = np.zeros_like(V)
+    E = tpe.Differential(M, 1.0, 0.0, D)
+    scale = np.abs(D).sum()
+    assert np.all(np.abs(D.sum(axis=0)) <= 1e-6 * scale)
+    assert abs((V * D).sum() - (2 * dom + Q - P) * E) <= 1e-5 * abs(E)
+
+
+def test_other_exponents_generic_path():
+    dom, V, S, M, O = _pair(2, True)
+    for q, p in [(4.0, 8.0), (6.0, 13.0), (2.5, 7.0)]:
+        tpe = rpb.TangentPointEnergy0(q, p)
+        D = np.zeros_like(V)
+        E = tpe.Differential(M, 1.0, 0.0, D)
+        E_ref, D_ref = O.differential(q, p)
+        assert abs(E - E_ref) <= 1e-5 * abs(E_ref), (q, p)
+        assert rel_max(D, D_ref) <= 1e-4, (q, p)
+
+
+def test_energy_rejects_bad_exponents():
+    dom, V, S, M, O = _pair(1, True)
+    with pytest.raises(rpb.RepulsorError):
+        rpb.TangentPointEnergy0(1.0, 4.0).Value(M)
