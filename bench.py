@@ -1,0 +1,336 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 tangent-point path (one JSON line on rank 0).
+
+Workload (the configuration the headline metric is quoted on): torus R=1, r=0.4,
+160 x 120 vertex grid (19,200 vertices, 38,400 triangles), normal jitter N(0, 0.002^2),
+q=6, p=12, theta=0.5. A step is one energy + differential evaluation of the mesh at the
+current coordinates: SemiStaticUpdate (simplex data + cluster-moment upsweep) followed
+by TangentPointEnergy0::Differential (near- and far-field pair kernels, collection,
+chain rule, vertex scatter). Synthetic seeded inputs stand in for user meshes.
+
+Timing: W warm-up steps, then K steps, each bracketed by CUDA events on the mesh's
+stream; before every timed step a 256 MiB device buffer is overwritten (outside the
+events) so no step starts with the mesh resident in L2. Multi-GPU runs (torchrun) are
+independent replicas, one mesh per GPU (weak scaling); the reported time is the max
+over ranks.
+
+--impl reference times the CPU restatement of the reference path (oracle/, FP64,
+std::thread) on this host's cores on the same workload.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "energy+grad evals/s; metric-solve ms to 1e-6 res, learned vs plain precond, 1 GPU"
+Q, P = 6.0, 12.0
+# algorithmic flops per unique pair of the energy+differential pair kernel (hand count of
+# TP0_Kernel_FF/NF::Compute with q/2 = 3, p/2 = 6: far-field 165, near-field 185)
+FLOPS_FAR_PAIR = 165.0
+FLOPS_NEAR_PAIR = 185.0
+LAUNCHES_PER_STEP = 5   # geometry+upsweep, near pairs, far pairs, collect+chain rule, vertex gather
+
+
+def workload_mesh():
+    from repulsor_b200 import meshes
+    return meshes.torus(R=1.0, r=0.4, n_major=160, n_minor=120, jitter=0.002, seed=1002)
+
+
+WORKLOAD = {"workload": "torus R=1 r=0.4 160x120 (19,200 vertices, 38,400 triangles), q=6 p=12 theta=0.5",
+            "step": "SemiStaticUpdate + Differential (energy + dE, FP32 pair kernels with FP64 projections)",
+            "l2": "256 MiB buffer overwritten before every timed step"}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ["index", "clocks.sm", "clocks.max.sm", "power.draw", "clocks_event_reasons.active",
+              "clocks_event_reasons.hw_slowdown", "clocks_event_reasons.hw_thermal_slowdown",
+              "clocks_event_reasons.sw_thermal_slowdown", "clocks_event_reasons.sw_power_cap"]
+
+    def __init__(self, device_index):
+        self.path = tempfile.mktemp(suffix=".csv")
+        self.proc = None
+        self.device_index = device_index
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={','.join(self.FIELDS)}", "--format=csv,noheader,nounits",
+                 "-i", str(self.device_index), "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        self.proc.wait()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(V, S, budget_s=20.0, max_evals=30):
+    """CPU restatement of the reference path (oracle port, FP64, std::thread over all
+    host cores) on the same mesh: SemiStaticUpdate + Differential per evaluation."""
+    import numpy as np
+
+    import oracle
+
+    threads = os.cpu_count() or 1
+    O = oracle.OracleMesh(2, V, S, threads=threads)
+    Y = np.zeros_like(V)
+    O.semistatic_update(V)
+    O.differential(Q, P, 1.0, 0.0, Y)   # warm-up
+    n = 0
+    t0 = time.perf_counter()
+    while n < max_evals and time.perf_counter() - t0 < budget_s:
+        O.semistatic_update(V)
+        O.differential(Q, P, 1.0, 0.0, Y)
+        n += 1
+    dt = time.perf_counter() - t0
+    return {"value": n / dt, "unit": "evals/s", "cores": threads, "kind": "port",
+            "sample": f"{n} full evaluations (SemiStaticUpdate + Differential) of the benchmark mesh, "
+                      f"{dt:.1f} s, oracle/tp0_oracle.cpp FP64 with {threads} std::threads"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    V, S = workload_mesh()
+    import numpy as np
+
+    import oracle
+
+    threads = os.cpu_count() or 1
+    O = oracle.OracleMesh(2, V, S, threads=threads)
+    Y = np.zeros_like(V)
+    for _ in range(max(1, args.warmup)):
+        O.semistatic_update(V)
+        O.differential(Q, P, 1.0, 0.0, Y)
+    steps = max(1, min(args.steps, 50))
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        O.semistatic_update(V)
+        O.differential(Q, P, 1.0, 0.0, Y)
+    dt = time.perf_counter() - t0
+    value = steps / dt
+    out = {"impl": "reference", "metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": args.gpus,
+           "steps": steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / steps, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded torus)",
+           "config": dict(WORKLOAD, parallelism="host threads"),
+           "cpu_baseline": {"value": value, "unit": "evals/s", "cores": threads, "kind": "port",
+                            "sample": f"{steps} evaluations of the benchmark mesh (steps capped at 50)"},
+           "e2e": {"value": value, "unit": "evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true")
+    ap.add_argument("--solve", action="store_true", help="also time Solve on the icosphere level-6 mesh")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import numpy as np
+    import torch
+
+    import repulsor_b200 as rpb
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local_rank))
+
+    V, S = workload_mesh()
+    M = rpb.SimplicialMesh(V, S, device=local_rank)
+    tpe = rpb.TangentPointEnergy0(Q, P)
+    st = M.stats()
+    Vd = torch.tensor(V, device="cuda")
+    Yd = torch.zeros((V.shape[0], 3), dtype=torch.float64, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    ext = torch.cuda.ExternalStream(M.stream())
+
+    def step():
+        M.SemiStaticUpdateDevice(Vd.data_ptr())
+        tpe.DifferentialDevice(M, Yd.data_ptr(), 3, 1.0, 0.0)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    sampler = ClockSampler(local_rank)
+    sampler.start()
+    time.sleep(0.3)
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    torch.cuda.synchronize()
+    for k in range(args.steps):
+        with torch.cuda.stream(ext):
+            flush.fill_(k & 0xFF)
+            starts[k].record(ext)
+        step()
+        ends[k].record(ext)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    time.sleep(0.3)
+    clocks = sampler.stop()
+    total_ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
+    if dist:
+        t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * args.steps / (total_ms * 1e-3)
+
+    # end to end through the public API with pinned host buffers (H2D of V, D2H of dE and E)
+    Vh = torch.tensor(V).pin_memory()
+    Yh = torch.zeros((V.shape[0], 3), dtype=torch.float64).pin_memory()
+    Vn, Yn = Vh.numpy(), Yh.numpy()
+    e2e_steps = max(10, min(args.steps, 500))
+    for _ in range(3):
+        M.SemiStaticUpdate(Vn)
+        tpe.Differential(M, 1.0, 0.0, Yn)
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        M.SemiStaticUpdate(Vn)
+        tpe.Differential(M, 1.0, 0.0, Yn)
+    e2e_s = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = {"value": world * e2e_steps / e2e_s, "unit": "evals/s", "h2d_bytes_per_step": V.nbytes,
+           "d2h_bytes_per_step": Yn.nbytes + 8,
+           "how": "SimplicialMesh.SemiStaticUpdate(host V) + TangentPointEnergy0.Differential(M, 1, 0, host Y), "
+                  "pinned host buffers, wall clock per step"}
+
+    out = None
+    if rank == 0:
+        # roofline of the dominant kernel (pair kernels), timed on the launching stream
+        import ctypes
+
+        lib = rpb._capi.load()
+        ms = np.zeros(5)
+        rpb._capi.check(lib.rpb_tpe0_stage_times(M._h, Q, P, 50, 256 << 20, rpb._capi.dptr(ms)), "stage_times")
+        peak = ctypes.c_double()
+        rpb._capi.check(lib.rpb_measure_fp32_peak(local_rank, ctypes.byref(peak)), "fp32_peak")
+        near_pairs = st["near_nnz"] / 2
+        far_pairs = st["far_nnz"] / 2
+        pair_ms = ms[1] + ms[2]
+        flops = FLOPS_NEAR_PAIR * near_pairs + FLOPS_FAR_PAIR * far_pairs
+        achieved = flops / (pair_ms * 1e-3) / 1e12
+        traffic = None
+        tpath = os.path.join(ROOT, "profiles", "traffic.json")
+        if os.path.exists(tpath):
+            traffic = json.load(open(tpath)).get("tp0_pairs_bytes_per_evaluation")
+        roofline = {"bound": "fp32", "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
+                    "frac": achieved / peak.value, "traffic": traffic,
+                    "kernel": "k_tp0_pairs (near + far launches)",
+                    "peak_source": "measured FP32 FMA throughput (rpb_measure_fp32_peak); MEASURED_PEAKS.json "
+                                   "has no FP32 figure",
+                    "flops_per_evaluation": flops,
+                    "stage_ms": {"geometry_upsweep": ms[0], "near_pairs": ms[1], "far_pairs": ms[2],
+                                 "collect_chain_gather": ms[3], "total": ms[4]}}
+        out = {"metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": world, "steps": args.steps,
+               "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+               "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+               "data": "synthetic (seeded torus; no dataset involved)",
+               "config": dict(WORKLOAD, parallelism=f"replicas x{world}", near_nnz=st["near_nnz"],
+                              far_nnz=st["far_nnz"], clusters=st["cluster_count"]),
+               "clocks": clocks, "e2e": e2e, "gpu_launches": LAUNCHES_PER_STEP * args.steps,
+               "roofline": roofline}
+        if not args.no_cpu_baseline:
+            out["cpu_baseline"] = cpu_baseline(V, S)
+        if not args.no_extras:
+            out["extras"] = extras(rpb, torch, args.solve)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if out is not None:
+        print(json.dumps(out))
+    return 0
+
+
+def extras(rpb, torch, with_solve):
+    """Metric matvecs/s and Solve time on the icosphere level-6 configuration."""
+    from repulsor_b200 import meshes
+
+    V, S = meshes.icosphere_sh(level=6, seed=1003)
+    M = rpb.SimplicialMesh(V, S)
+    tpm = rpb.TangentPointMetric0(Q, P)
+    X = torch.randn((V.shape[0], 3), dtype=torch.float64, device="cuda")
+    Y = torch.zeros_like(X)
+    ext = torch.cuda.ExternalStream(M.stream())
+    for _ in range(5):
+        tpm.MultiplyMetricDevice(M, 1.0, X.data_ptr(), 0.0, Y.data_ptr())
+    torch.cuda.synchronize()
+    n = 200
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(ext)
+    for _ in range(n):
+        tpm.MultiplyMetricDevice(M, 1.0, X.data_ptr(), 0.0, Y.data_ptr())
+    b.record(ext)
+    torch.cuda.synchronize()
+    mv_ms = a.elapsed_time(b) / n
+    out = {"metric_matvec": {"workload": "icosphere level 6 (81,920 triangles), nrhs=3",
+                             "matvecs_per_s": 1e3 / mv_ms, "ms": mv_ms}}
+    if not with_solve:
+        return out
+    B = meshes.random_rhs(V.shape[0], seed=1003)
+    solves = {}
+    for name, pc in (("reference_precond_cg", rpb.PRECOND_REFERENCE),):
+        t0 = time.perf_counter()
+        try:
+            tpm.Solve(M, 1.0, B, max_iter=2000, tolerance=1e-6, precond=pc)
+            status = "converged"
+        except rpb.RepulsorError as e:
+            status = str(e)
+        solves[name] = {"ms": 1e3 * (time.perf_counter() - t0), "iterations": tpm.Solver_IterationCount(),
+                        "rel_residual": [float(x) for x in tpm.Solver_RelativeResiduals()], "status": status}
+    out["solve"] = dict(workload="icosphere level 6, RHS N(0,1) projected off translations, tol 1e-6", **solves)
+    return out
+
+
+if __name__ == "__main__":
+    sys.exit(main())

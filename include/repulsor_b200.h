@@ -164,6 +164,20 @@ rpb_status rpb_tpm0_solve(rpb_mesh* m, double q, double p, double alpha, const d
                           double* X, int ldX, int nrhs, int max_iter, double tol, int precond, int* iterations,
                           double* rel_residual);
 
+/* --- measurement (no reference counterpart: Repulsor has no device path) ------------------ */
+
+/* Runs `reps` energy+differential evaluations (SemiStaticUpdate geometry + pair kernels +
+ * collection) on the mesh stream with CUDA events between the stages and returns the
+ * mean milliseconds of each stage: ms[0] geometry/upsweep, ms[1] near-field pairs,
+ * ms[2] far-field pairs, ms[3] collection + chain rule + vertex gather, ms[4] total.
+ * If flush_bytes > 0 a device buffer of that size is overwritten before every
+ * evaluation (outside the timed events) so that no stage starts with a warm L2. */
+rpb_status rpb_tpe0_stage_times(rpb_mesh* m, double q, double p, int reps, int64_t flush_bytes, double* ms);
+
+/* Measured FP32 FMA throughput of the device (TFLOP/s), from a register-resident
+ * kernel of independent FMA chains timed with CUDA events. */
+rpb_status rpb_measure_fp32_peak(int device, double* tflops);
+
 #ifdef __cplusplus
 }
 #endif

@@ -83,6 +83,9 @@ SIGNATURES = {
     "rpb_tpm0_solve": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double, ctypes.c_double, _dp, ctypes.c_int,
                                       ctypes.c_double, _dp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                       ctypes.c_double, ctypes.c_int, _ip, _dp]),
+    "rpb_tpe0_stage_times": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int64,
+                                            _dp]),
+    "rpb_measure_fp32_peak": (ctypes.c_int, [ctypes.c_int, _dp]),
 }
 
 _lib = None

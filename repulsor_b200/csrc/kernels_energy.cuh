@@ -88,20 +88,84 @@ __device__ __forceinline__ void projector_packed(int dom, const double* t, doubl
     P6[5] = id + sgn * t[2] * t[2];
 }
 
+// ----------------------------------------------------------------------------------------
+// Block-wide exclusive scan of W doubles per thread (blockDim.x = SCAN_BLOCK).
+// ----------------------------------------------------------------------------------------
+constexpr int SCAN_BLOCK = 256;
+
+template <int W>
+__device__ __forceinline__ void block_exclusive_scan(double (&v)[W], double (&total)[W])
+{
+    __shared__ double warp_tot[SCAN_BLOCK / 32][W];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    double incl[W];
+#pragma unroll
+    for (int k = 0; k < W; ++k) {
+        double x = v[k];
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const double y = __shfl_up_sync(0xffffffffu, x, off);
+            if (lane >= off) x += y;
+        }
+        incl[k] = x;
+    }
+    if (lane == 31) {
+#pragma unroll
+        for (int k = 0; k < W; ++k) warp_tot[w][k] = incl[k];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < W; ++k) {
+        double before = 0.0, all = 0.0;
+        for (int q = 0; q < SCAN_BLOCK / 32; ++q) {
+            const double t = warp_tot[q][k];
+            if (q < w) before += t;
+            all += t;
+        }
+        v[k] = before + incl[k] - v[k];
+        total[k] = all;
+    }
+    __syncthreads();
+}
+
+// Single-block exclusive scan of `n` rows of W doubles (block sums), in place; row n
+// receives the grand total.
+template <int W>
+__global__ void k_scan_rows(double* rows, int n)
+{
+    __shared__ double carry[W];
+    if (threadIdx.x < W) carry[threadIdx.x] = 0.0;
+    __syncthreads();
+    for (int base = 0; base < n; base += SCAN_BLOCK) {
+        const int i = base + threadIdx.x;
+        double v[W], tot[W];
+#pragma unroll
+        for (int k = 0; k < W; ++k) v[k] = (i < n) ? rows[static_cast<int64_t>(W) * i + k] : 0.0;
+        block_exclusive_scan<W>(v, tot);
+        if (i < n) {
+#pragma unroll
+            for (int k = 0; k < W; ++k) rows[static_cast<int64_t>(W) * i + k] = carry[k] + v[k];
+        }
+        __syncthreads();
+        if (threadIdx.x < W) carry[threadIdx.x] += tot[threadIdx.x];
+        __syncthreads();
+    }
+    if (threadIdx.x < W) rows[static_cast<int64_t>(W) * n + threadIdx.x] = carry[threadIdx.x];
+}
+
 struct GeomArgs {
-    int dom, N;
+    int dom, N, NC;
     const double* V;          // nV x 3
     const int* S;             // N x (dom+1)
     const double* charge_v;   // nV
     const int* perm;          // position -> simplex
-    const int* leaf_of;       // position -> leaf cluster
-    const int* C_parent;
-    const int* C_left;
-    const int* C_right;
+    const int* C_begin;
+    const int* C_end;
     PrimDatum* P_pair;        // N
     ClusterDatum* C_pair;     // NC
     double* C_mom;            // NC x 10 (a, centre, P) in FP64
-    unsigned* counter;        // NC arrival counters, all zero between launches
+    double* local;            // N x 10: exclusive in-block prefix of the moments (a, a c, a P)
+    double* blocks;           // (nblocks + 1) x 10: block sums -> exclusive block prefix
 };
 
 __device__ __forceinline__ void store_cluster(ClusterDatum* base, int i, const double* mom)
@@ -113,56 +177,58 @@ __device__ __forceinline__ void store_cluster(ClusterDatum* base, int i, const d
     store_datum(base, i, d);
 }
 
-// One thread per primitive in tree order. After writing its leaf, a thread walks
-// toward the root; at every internal node the second-arriving child computes the
-// mass-weighted average of both children (fixed left/right order, deterministic).
-static __global__ void k_geometry_upsweep(GeomArgs g)
+// Simplex data in tree order (SimplexDataKernel::ReadSimplex/WriteFar) and the in-block
+// prefix sums of the additive moments (a, a c, a P).
+static __global__ void __launch_bounds__(SCAN_BLOCK) k_geometry_prims(GeomArgs g)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= g.N) return;
-    const int size = g.dom + 1;
-    const int j = g.perm[i];
-    SimplexGeom sg;
-    simplex_geometry(g.dom, g.V, g.S + static_cast<int64_t>(size) * j, g.charge_v, sg);
     double mom[10];
-    mom[0] = sg.charge * sg.vol;
-    mom[1] = sg.c[0]; mom[2] = sg.c[1]; mom[3] = sg.c[2];
-    projector_packed(g.dom, sg.t, mom + 4);
-    {
+    for (int k = 0; k < 10; ++k) mom[k] = 0.0;
+    if (i < g.N) {
+        const int size = g.dom + 1;
+        SimplexGeom sg;
+        simplex_geometry(g.dom, g.V, g.S + static_cast<int64_t>(size) * g.perm[i], g.charge_v, sg);
         PrimDatum d;
         for (int k = 0; k < 3; ++k) { d.c[k] = sg.c[k]; d.n[k] = sg.t[k]; }
-        d.a = mom[0];
+        d.a = sg.charge * sg.vol;
         d.diam = static_cast<float>(sg.diam);
         d.pad = 0.0f;
         store_datum(g.P_pair, i, d);
+        double P6[6];
+        projector_packed(g.dom, sg.t, P6);
+        mom[0] = d.a;
+        for (int k = 0; k < 3; ++k) mom[1 + k] = d.a * sg.c[k];
+        for (int k = 0; k < 6; ++k) mom[4 + k] = d.a * P6[k];
     }
-    int C = g.leaf_of[i];
-    for (int k = 0; k < 10; ++k) __stcg(&g.C_mom[10 * static_cast<int64_t>(C) + k], mom[k]);
-    store_cluster(g.C_pair, C, mom);
-    for (;;) {
-        const int parent = g.C_parent[C];
-        if (parent < 0) return;
-        __threadfence();
-        const unsigned prev = atomicAdd(&g.counter[parent], 1u);
-        if (prev == 0u) return;            // sibling not done yet; it will continue
-        __threadfence();
-        g.counter[parent] = 0u;            // re-arm for the next launch
-        const int L = g.C_left[parent], R = g.C_right[parent];
-        const double* mL = g.C_mom + 10 * static_cast<int64_t>(L);
-        const double* mR = g.C_mom + 10 * static_cast<int64_t>(R);
-        double wl = __ldcg(mL), wr = __ldcg(mR);
-        const double mass = wl + wr;
-        const double inv = 1.0 / mass;
-        wl *= inv;
-        wr *= inv;
-        double m[10];
-        m[0] = mass;
-#pragma unroll
-        for (int k = 1; k < 10; ++k) m[k] = __dadd_rn(__dmul_rn(wl, __ldcg(mL + k)), __dmul_rn(wr, __ldcg(mR + k)));
-        for (int k = 0; k < 10; ++k) __stcg(&g.C_mom[10 * static_cast<int64_t>(parent) + k], m[k]);
-        store_cluster(g.C_pair, parent, m);
-        C = parent;
+    double tot[10];
+    block_exclusive_scan<10>(mom, tot);
+    if (i < g.N)
+        for (int k = 0; k < 10; ++k) g.local[10 * static_cast<int64_t>(i) + k] = mom[k];
+    if (threadIdx.x < 10) g.blocks[10 * static_cast<int64_t>(blockIdx.x) + threadIdx.x] = tot[threadIdx.x];
+}
+
+// ClusterTree moments (ComputeClusterData_Thread.hpp:50-129): a cluster's moments are
+// the sums over its contiguous primitive range, A = S[end] - S[begin], centre and
+// projector = moment / A.
+static __global__ void k_cluster_moments(GeomArgs g)
+{
+    const int C = blockIdx.x * blockDim.x + threadIdx.x;
+    if (C >= g.NC) return;
+    const int b = g.C_begin[C], e = g.C_end[C];
+    double m[10];
+    const double* lb = g.local + 10 * static_cast<int64_t>(b);
+    const double* bb = g.blocks + 10 * static_cast<int64_t>(b / SCAN_BLOCK);
+    const double* be = g.blocks + 10 * static_cast<int64_t>(e / SCAN_BLOCK);
+    for (int k = 0; k < 10; ++k) {
+        const double sb = bb[k] + lb[k];
+        const double se = (e < g.N) ? be[k] + g.local[10 * static_cast<int64_t>(e) + k]
+                                    : g.blocks[10 * static_cast<int64_t>((g.N + SCAN_BLOCK - 1) / SCAN_BLOCK) + k];
+        m[k] = se - sb;
     }
+    const double inv = 1.0 / m[0];
+    for (int k = 1; k < 10; ++k) m[k] *= inv;
+    for (int k = 0; k < 10; ++k) g.C_mom[10 * static_cast<int64_t>(C) + k] = m[k];
+    store_cluster(g.C_pair, C, m);
 }
 
 // ----------------------------------------------------------------------------------------
@@ -281,6 +347,7 @@ struct PairArgs {
     int rows;
     const int64_t* rp;
     const int* ci;
+    const int* order;         // rows in processing order (length-sorted within 256-row chunks)
     const void* data;         // PrimDatum* (near) or ClusterDatum* (far)
     double* D;                // rows x 10 (d0, dx[3], dP[6]) centred moment derivatives
     double* block_energy;     // gridDim.x
@@ -290,26 +357,29 @@ struct PairArgs {
     float close_factor;       // FP64 path for near pairs with r < close_factor (d_i + d_j)
 };
 
-// One warp per row. FAR: rows are clusters of the Far() pattern; otherwise rows are
-// primitives of the Near() pattern.
+constexpr int PAIR_BLOCK = 256;
+constexpr int PAIR_FLUSH = 8;   // FP32 partial sums are carried into FP64 every 8 pairs
+
+// One thread per row. FAR: rows are clusters of the Far() pattern; otherwise rows are
+// primitives of the Near() pattern. A row accumulates only its own derivative; each
+// unordered pair contributes its energy once (from the row with the smaller index).
 template <bool FAR, int QH, int PH, bool DIFF>
-__global__ void __launch_bounds__(256) k_tp0_pairs(PairArgs A)
+__global__ void __launch_bounds__(PAIR_BLOCK) k_tp0_pairs(PairArgs A)
 {
     using Datum = typename std::conditional<FAR, ClusterDatum, PrimDatum>::type;
-    const int lane = threadIdx.x & 31;
-    const int wib = threadIdx.x >> 5;
-    const int i = blockIdx.x * (blockDim.x >> 5) + wib;
     const Datum* base = static_cast<const Datum*>(A.data);
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
     double e_row = 0.0;
-    if (i < A.rows) {
+    if (t < A.rows) {
+        const int i = A.order[t];
         const Datum X = load_datum(base, i);
+        const float ax = static_cast<float>(X.a);
+        double D64[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
         PairAcc<float> acc = {};
-        float e_lane = 0.0f;
-        double d64[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
-        double e64 = 0.0;
-        bool any64 = false;
+        float e32 = 0.0f;
+        int since_flush = 0;
         const int64_t k0 = A.rp[i], k1 = A.rp[i + 1];
-        for (int64_t k = k0 + lane; k < k1; k += 32) {
+        for (int64_t k = k0; k < k1; ++k) {
             const int j = __ldg(A.ci + k);
             const Datum Y = load_datum(base, j);
             Proj<float> g;
@@ -321,50 +391,52 @@ __global__ void __launch_bounds__(256) k_tp0_pairs(PairArgs A)
                 close = g.r2 < dd * dd;
             }
             if (close) {
-                // close near-field pair: the same kernel in FP64
+                // close near-field pair: the same kernel in FP64, added straight into FP64
                 Proj<double> gd;
                 if constexpr (!FAR) project_prims(A.dom, X, Y, gd);
                 PairAcc<double> a64 = {};
                 const double e = tp0_core<double, QH, PH, DIFF>(A.ex, gd, X.a, Y.a, a64);
-                if (j > i) e64 += e;
+                if (j > i) e_row += e;
                 if (DIFF) {
-                    d64[0] += a64.d0;
-                    for (int m = 0; m < 3; ++m) d64[1 + m] += a64.dx[m];
-                    for (int m = 0; m < 6; ++m) d64[4 + m] += a64.dP[m];
+                    D64[0] += a64.d0;
+                    for (int m = 0; m < 3; ++m) D64[1 + m] += a64.dx[m];
+                    for (int m = 0; m < 6; ++m) D64[4 + m] += a64.dP[m];
                 }
-                any64 = true;
             } else {
-                const float e = tp0_core<float, QH, PH, DIFF>(A.ex, g, static_cast<float>(X.a), static_cast<float>(Y.a), acc);
-                if (j > i) e_lane += e;
+                const float e = tp0_core<float, QH, PH, DIFF>(A.ex, g, ax, static_cast<float>(Y.a), acc);
+                if (j > i) e32 += e;
+                if (++since_flush == PAIR_FLUSH) {
+                    since_flush = 0;
+                    e_row += e32;
+                    e32 = 0.0f;
+                    if (DIFF) {
+                        D64[0] += acc.d0;
+#pragma unroll
+                        for (int m = 0; m < 3; ++m) D64[1 + m] += acc.dx[m];
+#pragma unroll
+                        for (int m = 0; m < 6; ++m) D64[4 + m] += acc.dP[m];
+                        acc = PairAcc<float>{};
+                    }
+                }
             }
         }
-        // compensated cross-lane reduction; FP64 contributions added exactly
-        e_row = warp_sum_compensated(e_lane);
-        const bool has64 = __any_sync(0xffffffffu, any64);
-        if (has64) e_row += warp_sum_f64(e64);
+        e_row += e32;
         if (DIFF) {
-            double out[10];
-            out[0] = warp_sum_compensated(acc.d0);
+            D64[0] += acc.d0;
 #pragma unroll
-            for (int m = 0; m < 3; ++m) out[1 + m] = warp_sum_compensated(acc.dx[m]);
+            for (int m = 0; m < 3; ++m) D64[1 + m] += acc.dx[m];
 #pragma unroll
-            for (int m = 0; m < 6; ++m) out[4 + m] = warp_sum_compensated(acc.dP[m]);
-            if (has64) {
-#pragma unroll
-                for (int m = 0; m < 10; ++m) out[m] += warp_sum_f64(d64[m]);
-            }
+            for (int m = 0; m < 6; ++m) D64[4 + m] += acc.dP[m];
             double* dst = A.D + 10 * static_cast<int64_t>(i);
-            if (lane < 10) {
-                double val = out[0];
 #pragma unroll
-                for (int m = 1; m < 10; ++m) val = (lane == m) ? out[m] : val;
-                dst[lane] = val;
-            }
+            for (int m = 0; m < 10; ++m) dst[m] = D64[m];
         }
     }
     // deterministic energy reduction: per-block partial, last block sums all partials
-    __shared__ double sh[32];
+    __shared__ double sh[PAIR_BLOCK / 32];
     __shared__ bool last;
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    e_row = warp_sum_f64(e_row);
     if (lane == 0) sh[wib] = e_row;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -380,12 +452,13 @@ __global__ void __launch_bounds__(256) k_tp0_pairs(PairArgs A)
         double s = 0.0;
         for (int b = threadIdx.x; b < gridDim.x; b += blockDim.x) s += __ldcg(A.block_energy + b);
         s = warp_sum_f64(s);
+        __syncthreads();
         if (lane == 0) sh[wib] = s;
         __syncthreads();
         if (threadIdx.x == 0) {
-            double t = 0.0;
-            for (int w = 0; w < (blockDim.x >> 5); ++w) t += sh[w];
-            *A.energy_out = t;
+            double t2 = 0.0;
+            for (int w = 0; w < (blockDim.x >> 5); ++w) t2 += sh[w];
+            *A.energy_out = t2;
             *A.done = 0u;
         }
     }

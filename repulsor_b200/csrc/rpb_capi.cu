@@ -38,13 +38,14 @@ int64_t rpb_mesh::device_bytes() const
     b += V.bytes() + charge_v.bytes() + S.bytes() + perm.bytes() + leaf_of.bytes() + C_parent.bytes() +
          C_left.bytes() + C_right.bytes();
     b += near.rp.bytes() + near.ci.bytes() + far.rp.bytes() + far.ci.bytes() + verynear.rp.bytes() +
-         verynear.ci.bytes();
-    b += P_pair.bytes() + C_pair.bytes() + C_mom.bytes() + counter.bytes() + P_near.bytes();
+         verynear.ci.bytes() + near_order.bytes() + far_order.bytes();
+    b += P_pair.bytes() + C_pair.bytes() + C_mom.bytes() + counter.bytes() + P_near.bytes() + scan_local.bytes() +
+         scan_blocks.bytes() + C_begin.bytes() + C_end.bytes();
     b += D_near.bytes() + D_far.bytes() + D_vf.bytes() + B.bytes() + v_rp.bytes() + v_slot.bytes() + Y.bytes();
     b += block_energy.bytes() + energy.bytes() + done.bytes();
     b += pre_cols.bytes() + pre_vals.bytes() + vp_rp.bytes() + vp_slot.bytes();
     b += buf_Pin64.bytes() + buf_Cin64.bytes() + buf_Pout.bytes() + buf_Cout.bytes() + buf_Z.bytes() + X.bytes() +
-         Yb.bytes();
+         Yb.bytes() + buf_scan_local.bytes() + buf_scan_blocks.bytes();
     b += metric.nf.bytes() + metric.ff.bytes() + metric.vf.bytes() + metric.nf_diag.bytes() +
          metric.ff_diag.bytes() + metric.vf_diag.bytes();
     b += plap.nf.bytes() + plap.ff.bytes() + plap.vf.bytes() + plap.nf_diag.bytes() + plap.ff_diag.bytes() +
@@ -53,6 +54,22 @@ int64_t rpb_mesh::device_bytes() const
 }
 
 namespace rpb {
+
+// 16 independent FMA chains per thread, fully register resident.
+__global__ void k_fma_peak(float* out, int iters, float m)
+{
+    float r[16];
+#pragma unroll
+    for (int k = 0; k < 16; ++k) r[k] = threadIdx.x * 1e-3f + k;
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int k = 0; k < 16; ++k) r[k] = fmaf(r[k], m, 1e-7f);
+    }
+    float s = 0;
+#pragma unroll
+    for (int k = 0; k < 16; ++k) s += r[k];
+    out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
 
 template <typename T>
 static rpb_status upload(DevBuf<T>& d, const T* h, size_t n, cudaStream_t s)
@@ -99,19 +116,22 @@ rpb_status launch_geometry(rpb_mesh* m)
     GeomArgs g;
     g.dom = m->dom;
     g.N = m->N;
+    g.NC = m->NC;
     g.V = m->V.ptr;
     g.S = m->S.ptr;
     g.charge_v = m->charge_v.ptr;
     g.perm = m->perm.ptr;
-    g.leaf_of = m->leaf_of.ptr;
-    g.C_parent = m->C_parent.ptr;
-    g.C_left = m->C_left.ptr;
-    g.C_right = m->C_right.ptr;
+    g.C_begin = m->C_begin.ptr;
+    g.C_end = m->C_end.ptr;
     g.P_pair = m->P_pair.ptr;
     g.C_pair = m->C_pair.ptr;
     g.C_mom = m->C_mom.ptr;
-    g.counter = m->counter.ptr;
-    k_geometry_upsweep<<<(m->N + 255) / 256, 256, 0, m->stream>>>(g);
+    g.local = m->scan_local.ptr;
+    g.blocks = m->scan_blocks.ptr;
+    const int nb = (m->N + SCAN_BLOCK - 1) / SCAN_BLOCK;
+    k_geometry_prims<<<nb, SCAN_BLOCK, 0, m->stream>>>(g);
+    k_scan_rows<10><<<1, SCAN_BLOCK, 0, m->stream>>>(m->scan_blocks.ptr, nb);
+    k_cluster_moments<<<(m->NC + 255) / 256, 256, 0, m->stream>>>(g);
     RPB_CUDA(cudaGetLastError());
     m->geometry_valid = true;
     m->geometry_version++;
@@ -121,19 +141,20 @@ rpb_status launch_geometry(rpb_mesh* m)
 }
 
 template <int QH, int PH>
-static void launch_pairs_t(rpb_mesh* m, const PairArgs& An, const PairArgs& Af, bool diff)
+static void launch_pairs_t(rpb_mesh* m, const PairArgs& An, const PairArgs& Af, bool diff, cudaEvent_t between)
 {
     if (An.rows > 0) {
-        if (diff) k_tp0_pairs<false, QH, PH, true><<<m->near_blocks, 256, 0, m->stream>>>(An);
-        else k_tp0_pairs<false, QH, PH, false><<<m->near_blocks, 256, 0, m->stream>>>(An);
+        if (diff) k_tp0_pairs<false, QH, PH, true><<<m->near_blocks, PAIR_BLOCK, 0, m->stream>>>(An);
+        else k_tp0_pairs<false, QH, PH, false><<<m->near_blocks, PAIR_BLOCK, 0, m->stream>>>(An);
     }
+    if (between) cudaEventRecord(between, m->stream);
     if (Af.rows > 0) {
-        if (diff) k_tp0_pairs<true, QH, PH, true><<<m->far_blocks, 256, 0, m->stream>>>(Af);
-        else k_tp0_pairs<true, QH, PH, false><<<m->far_blocks, 256, 0, m->stream>>>(Af);
+        if (diff) k_tp0_pairs<true, QH, PH, true><<<m->far_blocks, PAIR_BLOCK, 0, m->stream>>>(Af);
+        else k_tp0_pairs<true, QH, PH, false><<<m->far_blocks, PAIR_BLOCK, 0, m->stream>>>(Af);
     }
 }
 
-rpb_status launch_pairs(rpb_mesh* m, const TPExp& ex, bool diff)
+rpb_status launch_pairs(rpb_mesh* m, const TPExp& ex, bool diff, cudaEvent_t between = nullptr)
 {
     PairArgs An, Af;
     An.dom = Af.dom = m->dom;
@@ -141,9 +162,11 @@ rpb_status launch_pairs(rpb_mesh* m, const TPExp& ex, bool diff)
     An.close_factor = Af.close_factor = 0.1f;
     An.rows = m->near.nnz > 0 ? m->N : 0;
     An.rp = m->near.rp.ptr; An.ci = m->near.ci.ptr; An.data = m->P_pair.ptr; An.D = m->D_near.ptr;
+    An.order = m->near_order.ptr;
     An.block_energy = m->block_energy.ptr; An.done = m->done.ptr; An.energy_out = m->energy.ptr;
     Af.rows = m->far.nnz > 0 ? m->NC : 0;
     Af.rp = m->far.rp.ptr; Af.ci = m->far.ci.ptr; Af.data = m->C_pair.ptr; Af.D = m->D_far.ptr;
+    Af.order = m->far_order.ptr;
     Af.block_energy = m->block_energy.ptr + m->near_blocks; Af.done = m->done.ptr + 1; Af.energy_out = m->energy.ptr + 1;
     if (An.rows == 0) {
         RPB_CUDA(cudaMemsetAsync(m->energy.ptr, 0, sizeof(double), m->stream));
@@ -153,10 +176,10 @@ rpb_status launch_pairs(rpb_mesh* m, const TPExp& ex, bool diff)
         RPB_CUDA(cudaMemsetAsync(m->energy.ptr + 1, 0, sizeof(double), m->stream));
         if (diff) RPB_CUDA(cudaMemsetAsync(m->D_far.ptr, 0, m->D_far.bytes(), m->stream));
     }
-    if (ex.qh == 3 && ex.ph == 6) launch_pairs_t<3, 6>(m, An, Af, diff);
-    else if (ex.qh == 2 && ex.ph == 4) launch_pairs_t<2, 4>(m, An, Af, diff);
-    else if (ex.qh == 1 && ex.ph == 2) launch_pairs_t<1, 2>(m, An, Af, diff);
-    else launch_pairs_t<-1, -1>(m, An, Af, diff);
+    if (ex.qh == 3 && ex.ph == 6) launch_pairs_t<3, 6>(m, An, Af, diff, between);
+    else if (ex.qh == 2 && ex.ph == 4) launch_pairs_t<2, 4>(m, An, Af, diff, between);
+    else if (ex.qh == 1 && ex.ph == 2) launch_pairs_t<1, 2>(m, An, Af, diff, between);
+    else launch_pairs_t<-1, -1>(m, An, Af, diff, between);
     RPB_CUDA(cudaGetLastError());
     return RPB_OK;
 }
@@ -302,6 +325,8 @@ rpb_status rpb_mesh_create(int dom_dim, int amb_dim, const double* Vh, int64_t n
     UP(m->C_parent, T.C_parent.data(), T.C_parent.size());
     UP(m->C_left, T.C_left.data(), T.C_left.size());
     UP(m->C_right, T.C_right.data(), T.C_right.size());
+    UP(m->C_begin, T.C_begin.data(), T.C_begin.size());
+    UP(m->C_end, T.C_end.data(), T.C_end.size());
     if ((st = upload_pattern(m->near, T.near, s)) != RPB_OK) return fail(st);
     if ((st = upload_pattern(m->far, T.far, s)) != RPB_OK) return fail(st);
     if ((st = upload_pattern(m->verynear, T.verynear, s)) != RPB_OK) return fail(st);
@@ -318,14 +343,34 @@ rpb_status rpb_mesh_create(int dom_dim, int amb_dim, const double* Vh, int64_t n
 #undef UP
     if (m->P_pair.alloc(m->N) || m->C_pair.alloc(m->NC) || m->C_mom.alloc(10 * static_cast<size_t>(m->NC)) ||
         m->counter.alloc(m->NC) || m->D_near.alloc(10 * static_cast<size_t>(m->N)) ||
+        m->scan_local.alloc(10 * static_cast<size_t>(m->N)) ||
+        m->scan_blocks.alloc(10 * static_cast<size_t>((m->N + SCAN_BLOCK - 1) / SCAN_BLOCK + 1)) ||
         m->D_far.alloc(10 * static_cast<size_t>(m->NC)) ||
         m->B.alloc(3 * static_cast<size_t>(m->size) * m->N) || m->Y.alloc(3 * static_cast<size_t>(m->nV)) ||
         m->energy.alloc(4) || m->done.alloc(4)) {
         set_error("device allocation failed");
         return fail(RPB_ENOMEM);
     }
-    m->near_blocks = (m->N + 7) / 8;
-    m->far_blocks = (m->NC + 7) / 8;
+    m->near_blocks = (m->N + PAIR_BLOCK - 1) / PAIR_BLOCK;
+    m->far_blocks = (m->NC + PAIR_BLOCK - 1) / PAIR_BLOCK;
+    {
+        // rows of each 256-row chunk sorted by decreasing length: threads of a warp see
+        // similar trip counts while the chunk keeps the tree-order locality of its columns
+        auto order_of = [](const SymPattern& P) {
+            std::vector<int> o(P.rows);
+            for (int i = 0; i < P.rows; ++i) o[i] = i;
+            for (int c0 = 0; c0 < P.rows; c0 += PAIR_BLOCK) {
+                const int c1 = std::min(P.rows, c0 + PAIR_BLOCK);
+                std::stable_sort(o.begin() + c0, o.begin() + c1, [&](int a, int b) {
+                    return (P.rp[a + 1] - P.rp[a]) > (P.rp[b + 1] - P.rp[b]);
+                });
+            }
+            return o;
+        };
+        const std::vector<int> no = order_of(T.near), fo = order_of(T.far);
+        if ((st = upload(m->near_order, no.data(), no.size(), s)) != RPB_OK) return fail(st);
+        if ((st = upload(m->far_order, fo.data(), fo.size(), s)) != RPB_OK) return fail(st);
+    }
     if (m->block_energy.alloc(m->near_blocks + m->far_blocks)) { set_error("device allocation failed"); return fail(RPB_ENOMEM); }
     if (cudaMemsetAsync(m->counter.ptr, 0, m->counter.bytes(), s) != cudaSuccess ||
         cudaMemsetAsync(m->done.ptr, 0, m->done.bytes(), s) != cudaSuccess ||
@@ -571,6 +616,69 @@ rpb_status rpb_tpe0_differential(rpb_mesh* m, double q, double p, double alpha, 
                                cudaMemcpyDeviceToHost, m->stream));
     RPB_CUDA(cudaStreamSynchronize(m->stream));
     if (energy) *energy = e;
+    return RPB_OK;
+}
+
+rpb_status rpb_tpe0_stage_times(rpb_mesh* m, double q, double p, int reps, int64_t flush_bytes, double* ms)
+{
+    if (!m || !ms || reps <= 0) { set_error("bad argument"); return RPB_EINVAL; }
+    rpb_status st = check_exponents(q, p);
+    if (st != RPB_OK) return st;
+    RPB_CUDA(cudaSetDevice(m->device));
+    const TPExp ex = make_exp(m->dom, q, p);
+    cudaEvent_t ev[5];
+    for (auto& e : ev) RPB_CUDA(cudaEventCreate(&e));
+    DevBuf<char> flush;
+    if (flush_bytes > 0) RPB_CUDA(flush.alloc(static_cast<size_t>(flush_bytes)));
+    double acc[5] = {0, 0, 0, 0, 0};
+    const bool with_vf = m->verynear.nnz > 0;
+    for (int r = 0; r < reps; ++r) {
+        if (flush.ptr) RPB_CUDA(cudaMemsetAsync(flush.ptr, r & 0xff, flush.bytes(), m->stream));
+        RPB_CUDA(cudaEventRecord(ev[0], m->stream));
+        if ((st = launch_geometry(m)) != RPB_OK) return st;
+        RPB_CUDA(cudaEventRecord(ev[1], m->stream));
+        // near rows | far rows (+ very-near) | collection
+        if ((st = launch_pairs(m, ex, true, ev[2])) != RPB_OK) return st;
+        if (with_vf && (st = launch_vf(m, ex, true)) != RPB_OK) return st;
+        RPB_CUDA(cudaEventRecord(ev[3], m->stream));
+        if ((st = launch_collect_gather(m, 1.0, 0.0, m->Y.ptr, 3, with_vf)) != RPB_OK) return st;
+        RPB_CUDA(cudaEventRecord(ev[4], m->stream));
+        RPB_CUDA(cudaEventSynchronize(ev[4]));
+        float t;
+        cudaEventElapsedTime(&t, ev[0], ev[1]); acc[0] += t;
+        cudaEventElapsedTime(&t, ev[1], ev[2]); acc[1] += t;
+        cudaEventElapsedTime(&t, ev[2], ev[3]); acc[2] += t;
+        cudaEventElapsedTime(&t, ev[3], ev[4]); acc[3] += t;
+        cudaEventElapsedTime(&t, ev[0], ev[4]); acc[4] += t;
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    for (int k = 0; k < 5; ++k) ms[k] = acc[k] / reps;
+    return RPB_OK;
+}
+
+rpb_status rpb_measure_fp32_peak(int device, double* tflops)
+{
+    if (!tflops) { set_error("null argument"); return RPB_EINVAL; }
+    RPB_CUDA(cudaSetDevice(device));
+    int sms = 0;
+    RPB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    const int blocks = sms * 8, threads = 256, iters = 8192;
+    DevBuf<float> out;
+    RPB_CUDA(out.alloc(static_cast<size_t>(blocks) * threads));
+    cudaEvent_t a, b;
+    RPB_CUDA(cudaEventCreate(&a));
+    RPB_CUDA(cudaEventCreate(&b));
+    k_fma_peak<<<blocks, threads>>>(out.ptr, iters, 1.0001f);
+    RPB_CUDA(cudaEventRecord(a));
+    k_fma_peak<<<blocks, threads>>>(out.ptr, iters, 1.0001f);
+    RPB_CUDA(cudaEventRecord(b));
+    RPB_CUDA(cudaEventSynchronize(b));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    const double flops = 2.0 * 16.0 * iters * static_cast<double>(blocks) * threads;
+    *tflops = flops / (ms * 1e-3) / 1e12;
     return RPB_OK;
 }
 

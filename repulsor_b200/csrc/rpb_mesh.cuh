@@ -77,12 +77,14 @@ struct rpb_mesh {
     rpb::DevBuf<double> V, charge_v;
     rpb::DevBuf<int> S;
     // tree
-    rpb::DevBuf<int> perm, leaf_of, C_parent, C_left, C_right;
+    rpb::DevBuf<int> perm, leaf_of, C_parent, C_left, C_right, C_begin, C_end;
     rpb::Csr near, far, verynear;
+    rpb::DevBuf<int> near_order, far_order;     // pair-kernel row order (length-sorted per chunk)
     // geometry state
     rpb::DevBuf<rpb::PrimDatum> P_pair;
     rpb::DevBuf<rpb::ClusterDatum> C_pair;
     rpb::DevBuf<double> C_mom;
+    rpb::DevBuf<double> scan_local, scan_blocks;   // prefix sums of the moment upsweep
     rpb::DevBuf<unsigned> counter;
     // near-hull data for very-near quadrature (N x (1 + 3 size + 6), FP64)
     rpb::DevBuf<double> P_near;
@@ -97,7 +99,7 @@ struct rpb_mesh {
     rpb::DevBuf<int> pre_cols;
     rpb::DevBuf<double> pre_vals;
     rpb::DevBuf<int> vp_rp, vp_slot;        // vertex -> (primitive position * size + corner)
-    rpb::DevBuf<double> buf_Pin64, buf_Cin64, buf_Pout, buf_Cout, buf_Z;
+    rpb::DevBuf<double> buf_Pin64, buf_Cin64, buf_Pout, buf_Cout, buf_Z, buf_scan_local, buf_scan_blocks;
     rpb::DevBuf<double> X, Yb;              // staging for host-pointer calls (nV x 3)
     rpb::MetricCache metric;
     rpb::PseudoLapCache plap;

@@ -114,64 +114,68 @@ static void launch_values(rpb_mesh* m, bool pl, float s_exp, float2* nf, double2
 // ------------------------------------------------------------------------------------------
 template <int BD>
 struct PreArgs {
-    int N, size;
+    int N, NC, size;
     const int* pre_cols;      // N x size
     const double* pre_vals;   // N x 4 x size
     const double* X;
     int ldX;
-    const int* leaf_of;
-    const int* C_parent;
-    const int* C_left;
-    const int* C_right;
-    unsigned* counter;
+    const int* C_begin;
+    const int* C_end;
     double* Pin;              // N x BD
     double* Cin;              // NC x BD
+    double* local;            // N x BD in-block exclusive prefix
+    double* blocks;           // (nblocks + 1) x BD
 };
 
+// Pre operator per primitive (mi_pre / lo_pre rows, src/ClusterTree.hpp:410-639) and the
+// in-block prefix sums that give PrimitivesToClusters + PercolateUp as range sums.
 template <int BD>
-__device__ __forceinline__ void store_row(double* d, int64_t row, const double* x)
-{
-#pragma unroll
-    for (int k = 0; k < BD; ++k) __stcg(d + BD * row + k, x[k]);
-}
-
-template <int BD>
-__global__ void k_pre(PreArgs<BD> A)
+__global__ void __launch_bounds__(SCAN_BLOCK) k_pre(PreArgs<BD> A)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= A.N) return;
     constexpr int ROWS = BD / 3;  // 4 (mixed order) or 1 (low order)
     double x[BD];
 #pragma unroll
     for (int k = 0; k < BD; ++k) x[k] = 0.0;
-    for (int l = 0; l < A.size; ++l) {
-        const int v = A.pre_cols[A.size * i + l];
-        const double* xv = A.X + static_cast<int64_t>(A.ldX) * v;
-        const double X0 = xv[0], X1 = xv[1], X2 = xv[2];
+    if (i < A.N) {
+        for (int l = 0; l < A.size; ++l) {
+            const int v = A.pre_cols[A.size * i + l];
+            const double* xv = A.X + static_cast<int64_t>(A.ldX) * v;
+            const double X0 = xv[0], X1 = xv[1], X2 = xv[2];
 #pragma unroll
-        for (int r = 0; r < ROWS; ++r) {
-            const double w = A.pre_vals[(4 * static_cast<int64_t>(i) + r) * A.size + l];
-            x[3 * r + 0] += w * X0;
-            x[3 * r + 1] += w * X1;
-            x[3 * r + 2] += w * X2;
+            for (int r = 0; r < ROWS; ++r) {
+                const double w = A.pre_vals[(4 * static_cast<int64_t>(i) + r) * A.size + l];
+                x[3 * r + 0] += w * X0;
+                x[3 * r + 1] += w * X1;
+                x[3 * r + 2] += w * X2;
+            }
         }
-    }
-    store_row<BD>(A.Pin, i, x);
-    int C = A.leaf_of[i];
-    store_row<BD>(A.Cin, C, x);
-    for (;;) {
-        const int parent = A.C_parent[C];
-        if (parent < 0) return;
-        __threadfence();
-        if (atomicAdd(&A.counter[parent], 1u) == 0u) return;
-        __threadfence();
-        A.counter[parent] = 0u;
-        const double* l = A.Cin + BD * static_cast<int64_t>(A.C_left[parent]);
-        const double* r = A.Cin + BD * static_cast<int64_t>(A.C_right[parent]);
 #pragma unroll
-        for (int k = 0; k < BD; ++k) x[k] = __ldcg(l + k) + __ldcg(r + k);
-        store_row<BD>(A.Cin, parent, x);
-        C = parent;
+        for (int k = 0; k < BD; ++k) A.Pin[BD * static_cast<int64_t>(i) + k] = x[k];
+    }
+    double tot[BD];
+    block_exclusive_scan<BD>(x, tot);
+    if (i < A.N) {
+#pragma unroll
+        for (int k = 0; k < BD; ++k) A.local[BD * static_cast<int64_t>(i) + k] = x[k];
+    }
+    if (threadIdx.x < BD) A.blocks[BD * static_cast<int64_t>(blockIdx.x) + threadIdx.x] = tot[threadIdx.x];
+}
+
+template <int BD>
+__global__ void k_cluster_sums(PreArgs<BD> A)
+{
+    const int C = blockIdx.x * blockDim.x + threadIdx.x;
+    if (C >= A.NC) return;
+    const int b = A.C_begin[C], e = A.C_end[C];
+    const int nb = (A.N + SCAN_BLOCK - 1) / SCAN_BLOCK;
+#pragma unroll
+    for (int k = 0; k < BD; ++k) {
+        const double sb = A.blocks[BD * static_cast<int64_t>(b / SCAN_BLOCK) + k] + A.local[BD * static_cast<int64_t>(b) + k];
+        const double se = (e < A.N) ? A.blocks[BD * static_cast<int64_t>(e / SCAN_BLOCK) + k] +
+                                          A.local[BD * static_cast<int64_t>(e) + k]
+                                    : A.blocks[BD * static_cast<int64_t>(nb) + k];
+        A.Cin[BD * static_cast<int64_t>(C) + k] = se - sb;
     }
 }
 
@@ -382,6 +386,8 @@ rpb_status metric_init(rpb_mesh* m, const double* Vh, const int* Sh)
     RPB_CUDA(cudaMemcpyAsync(m->vp_rp.ptr, rp.data(), m->vp_rp.bytes(), cudaMemcpyHostToDevice, s));
     RPB_CUDA(cudaMemcpyAsync(m->vp_slot.ptr, slot.data(), m->vp_slot.bytes(), cudaMemcpyHostToDevice, s));
     RPB_CUDA(m->buf_Pin64.alloc(12 * static_cast<size_t>(N)));
+    RPB_CUDA(m->buf_scan_local.alloc(12 * static_cast<size_t>(N)));
+    RPB_CUDA(m->buf_scan_blocks.alloc(12 * static_cast<size_t>((N + SCAN_BLOCK - 1) / SCAN_BLOCK + 1)));
     RPB_CUDA(m->buf_Cin64.alloc(12 * static_cast<size_t>(m->NC)));
     RPB_CUDA(m->buf_Pout.alloc(12 * static_cast<size_t>(N)));
     RPB_CUDA(m->buf_Cout.alloc(12 * static_cast<size_t>(m->NC)));
@@ -456,13 +462,16 @@ static rpb_status apply_operator(rpb_mesh* m, const float2* nf, const double2* n
 {
     cudaStream_t s = m->stream;
     PreArgs<BD> pa;
-    pa.N = m->N; pa.size = m->size;
+    pa.N = m->N; pa.NC = m->NC; pa.size = m->size;
     pa.pre_cols = m->pre_cols.ptr; pa.pre_vals = m->pre_vals.ptr;
     pa.X = X; pa.ldX = ldX;
-    pa.leaf_of = m->leaf_of.ptr; pa.C_parent = m->C_parent.ptr; pa.C_left = m->C_left.ptr; pa.C_right = m->C_right.ptr;
-    pa.counter = m->counter.ptr;
+    pa.C_begin = m->C_begin.ptr; pa.C_end = m->C_end.ptr;
     pa.Pin = m->buf_Pin64.ptr; pa.Cin = m->buf_Cin64.ptr;
-    k_pre<BD><<<(m->N + 255) / 256, 256, 0, s>>>(pa);
+    pa.local = m->buf_scan_local.ptr; pa.blocks = m->buf_scan_blocks.ptr;
+    const int nb = (m->N + SCAN_BLOCK - 1) / SCAN_BLOCK;
+    k_pre<BD><<<nb, SCAN_BLOCK, 0, s>>>(pa);
+    k_scan_rows<BD><<<1, SCAN_BLOCK, 0, s>>>(m->buf_scan_blocks.ptr, nb);
+    k_cluster_sums<BD><<<(m->NC + 255) / 256, 256, 0, s>>>(pa);
     RPB_CUDA(cudaGetLastError());
 
     const bool NF = (flags & 2) && m->near.nnz > 0;

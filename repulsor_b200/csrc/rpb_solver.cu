@@ -52,7 +52,7 @@ __device__ __forceinline__ void st_release(int* p, int v)
     asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-constexpr long long kSpinLimit = 1ll << 26;
+constexpr long long kSpinLimit = 1ll << 24;   // with the 512 ns backoff cap: a few seconds at most
 
 struct TrsvArgs {
     int n;
@@ -88,11 +88,14 @@ __global__ void __launch_bounds__(256) k_trsv(TrsvArgs A)
         for (int64_t k = ob + lane; k < oe; k += 32) {
             const int j = A.ci[k];
             long long it = 0;
+            unsigned backoff = 32;
             while (ld_acquire(A.flags + j) != A.epoch) {
                 if (++it > kSpinLimit) {
                     atomicExch(A.err, 1);
                     break;
                 }
+                __nanosleep(backoff);
+                backoff = backoff < 256 ? 2 * backoff : 256;
             }
             const double v = A.val[k];
             s0 += v * __ldcg(A.y + 3 * static_cast<int64_t>(j) + 0);
@@ -308,7 +311,7 @@ static rpb_status h1_solve(rpb_mesh* m, const double* b, double* out)
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int blocks = std::min((n + 7) / 8, sms * 8);
+    const int blocks = std::min((n + 7) / 8, sms * 2);
     RPB_CUDA(cudaMemsetAsync(s.ticket.ptr, 0, s.ticket.bytes(), m->stream));
     TrsvArgs A;
     A.n = n;
@@ -442,7 +445,9 @@ static rpb_status cg_solve(rpb_mesh* m, double q, double p, const double* B, int
                 if (rc > tol) conv = false;
                 if (rc < 0.9 * best[c]) { best[c] = rc; since_best = 0; }
             }
-            if (!conv && ++since_best > 60) stalled = true;
+            // stall detection only guards the flexible (learned) iteration, which then falls
+            // back to the reference preconditioner; fixed-preconditioner CG is never restarted
+            if (flexible && kind == RPB_PRECOND_LEARNED && !conv && ++since_best > 60) stalled = true;
             if (conv || stalled) {
                 stalled_flag = stalled;
                 since_best = 0;
@@ -454,7 +459,7 @@ static rpb_status cg_solve(rpb_mesh* m, double q, double p, const double* B, int
             k_cg_direction<<<eb, 256, 0, stream>>>(n, S, flexible, z, pv);
             RPB_CUDA(cudaGetLastError());
         }
-        if (restarts > 50) break;
+        if (restarts > 20) break;
     }
     if (iters_out) *iters_out = it;
     if (relres_out)
