@@ -164,6 +164,24 @@ rpb_status rpb_tpm0_solve(rpb_mesh* m, double q, double p, double alpha, const d
                           double* X, int ldX, int nrhs, int max_iter, double tol, int precond, int* iterations,
                           double* rel_residual);
 
+/* --- energy without device allocation -------------------------------------------------- */
+
+/* No counterpart in the reference (Repulsor has no device path). TangentPointEnergy0
+ * Value for callers that cannot allocate device memory when they need the energy (inside
+ * CUDA graph capture, under a fixed memory arena, in loops that forbid allocation). All
+ * pointers are device pointers the caller owns: V (nV x 3), S (nS x (dom_dim+1)), the tree
+ * (perm: nS, C_begin/C_end: nC) and the full symmetric near/far patterns as returned by
+ * rpb_mesh_tree/rpb_mesh_pattern; the energy (1 double) is written asynchronously on
+ * `stream`. Unit charges; the very-near list must be empty. Scratch lives in one static
+ * device array of about 12.4 MB (at most 40,960 simplices, larger meshes give RPB_EINVAL)
+ * held by every device that loads the library; the first call on a device looks up its
+ * address and should come before any stream capture; calls that overlap on the GPU race
+ * on the shared scratch. Allocates nothing. */
+rpb_status rpb_tpe0_value_noalloc(int dom_dim, const double* V, int64_t nV, const int* S, int64_t nS,
+                                  const int* perm, const int* C_begin, const int* C_end, int64_t nC,
+                                  const int64_t* near_rowptr, const int* near_colidx, const int64_t* far_rowptr,
+                                  const int* far_colidx, double q, double p, double* energy, void* stream);
+
 /* --- measurement (no reference counterpart: Repulsor has no device path) ------------------ */
 
 /* Runs `reps` energy+differential evaluations (SemiStaticUpdate geometry + pair kernels +

@@ -86,6 +86,9 @@ SIGNATURES = {
     "rpb_tpe0_stage_times": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int64,
                                             _dp]),
     "rpb_measure_fp32_peak": (ctypes.c_int, [ctypes.c_int, _dp]),
+    "rpb_tpe0_value_noalloc": (ctypes.c_int, [ctypes.c_int, _vp, ctypes.c_int64, _vp, ctypes.c_int64, _vp, _vp, _vp,
+                                              ctypes.c_int64, _vp, _vp, _vp, _vp, ctypes.c_double, ctypes.c_double,
+                                              _vp, _vp]),
 }
 
 _lib = None

@@ -43,7 +43,7 @@ __device__ __forceinline__ void simplex_geometry(int dom, const double* __restri
         g.h[j][0] = V[3 * static_cast<int64_t>(v) + 0];
         g.h[j][1] = V[3 * static_cast<int64_t>(v) + 1];
         g.h[j][2] = V[3 * static_cast<int64_t>(v) + 2];
-        g.charge += charge_v[v];
+        g.charge += charge_v ? charge_v[v] : 1.0;   // no charges: unit charges
     }
     g.charge /= size;
     for (int k = 0; k < 3; ++k) {
@@ -227,7 +227,8 @@ static __global__ void k_cluster_moments(GeomArgs g)
     }
     const double inv = 1.0 / m[0];
     for (int k = 1; k < 10; ++k) m[k] *= inv;
-    for (int k = 0; k < 10; ++k) g.C_mom[10 * static_cast<int64_t>(C) + k] = m[k];
+    if (g.C_mom)
+        for (int k = 0; k < 10; ++k) g.C_mom[10 * static_cast<int64_t>(C) + k] = m[k];
     store_cluster(g.C_pair, C, m);
 }
 
@@ -371,7 +372,7 @@ __global__ void __launch_bounds__(PAIR_BLOCK) k_tp0_pairs(PairArgs A)
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     double e_row = 0.0;
     if (t < A.rows) {
-        const int i = A.order[t];
+        const int i = A.order ? A.order[t] : t;
         const Datum X = load_datum(base, i);
         const float ax = static_cast<float>(X.a);
         double D64[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
@@ -463,6 +464,9 @@ __global__ void __launch_bounds__(PAIR_BLOCK) k_tp0_pairs(PairArgs A)
         }
     }
 }
+
+// energy = near-field part + far-field part (the order evaluate() uses on the host)
+static __global__ void k_add_pair(const double* e2, double* out) { *out = e2[0] + e2[1]; }
 
 // ----------------------------------------------------------------------------------------
 // Collection + chain rule. One thread per primitive (tree order).
