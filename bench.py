@@ -35,7 +35,9 @@ Q, P = 6.0, 12.0
 # TP0_Kernel_FF/NF::Compute with q/2 = 3, p/2 = 6: far-field 165, near-field 185)
 FLOPS_FAR_PAIR = 165.0
 FLOPS_NEAR_PAIR = 185.0
-LAUNCHES_PER_STEP = 5   # geometry+upsweep, near pairs, far pairs, collect+chain rule, vertex gather
+# geometry (primitive data + in-block scans), block scan, cluster moments, near pairs,
+# far pairs, collect + chain rule, vertex gather
+LAUNCHES_PER_STEP = 7
 
 
 def workload_mesh():
@@ -158,7 +160,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true")
-    ap.add_argument("--solve", action="store_true", help="also time Solve on the icosphere level-6 mesh")
+    ap.add_argument("--no-solve", action="store_true", help="skip the Solve timings on the icosphere level-6 mesh")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -283,7 +285,7 @@ def main():
         if not args.no_cpu_baseline:
             out["cpu_baseline"] = cpu_baseline(V, S)
         if not args.no_extras:
-            out["extras"] = extras(rpb, torch, args.solve)
+            out["extras"] = extras(rpb, torch, not args.no_solve)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -317,19 +319,47 @@ def extras(rpb, torch, with_solve):
                              "matvecs_per_s": 1e3 / mv_ms, "ms": mv_ms}}
     if not with_solve:
         return out
-    B = meshes.random_rhs(V.shape[0], seed=1003)
-    solves = {}
-    for name, pc in (("reference_precond_cg", rpb.PRECOND_REFERENCE),):
-        t0 = time.perf_counter()
-        try:
-            tpm.Solve(M, 1.0, B, max_iter=2000, tolerance=1e-6, precond=pc)
-            status = "converged"
-        except rpb.RepulsorError as e:
-            status = str(e)
-        solves[name] = {"ms": 1e3 * (time.perf_counter() - t0), "iterations": tpm.Solver_IterationCount(),
-                        "rel_residual": [float(x) for x in tpm.Solver_RelativeResiduals()], "status": status}
-    out["solve"] = dict(workload="icosphere level 6, RHS N(0,1) projected off translations, tol 1e-6", **solves)
+    out["solve"] = solve_extras(rpb, M, tpm, V)
     return out
+
+
+def solve_extras(rpb, M, tpm, V):
+    """Solve to 1e-6 relative residual on the icosphere level-6 mesh: plain CG, CG with the
+    reference preconditioner, and flexible CG with the learned preconditioner trained on
+    the GPU (pairs from plain solves on seeded icospheres of levels 4 and 5; training
+    time reported separately)."""
+    from repulsor_b200 import meshes
+    from repulsor_b200.learned import LearnedPreconditioner, train, training_pairs
+
+    t0 = time.perf_counter()
+    data = []
+    for lvl, seed in ((4, 2001), (5, 2002)):
+        Vt, St = meshes.icosphere_sh(level=lvl, seed=seed)
+        Mt = rpb.SimplicialMesh(Vt, St)
+        R, E = training_pairs(Mt, tpm, n_rhs=4, checkpoints=(0, 4, 16, 48, 128), seed=seed, exact_tol=1e-9)
+        data.append((Mt, R, E))
+    t1 = time.perf_counter()
+    net = LearnedPreconditioner(seed=1)
+    hist = train(net, tpm, data, epochs=30, lr=1e-3, batch=4, seed=0)
+    t2 = time.perf_counter()
+    net.attach(M)
+    B = meshes.random_rhs(V.shape[0], seed=1003)
+    res = {"workload": "icosphere level 6 (40,962 vertices), RHS N(0,1) projected off translations, tol 1e-6 "
+                       "(true residual of the plain metric operator)",
+           "training": {"meshes": "icosphere_sh levels 4 and 5 (seeds 2001, 2002), 4 RHS each, CG checkpoints "
+                                  "0/4/16/48/128", "pairs": int(sum(d[1].shape[0] for d in data)),
+                        "pair_generation_s": t1 - t0, "training_s": t2 - t1, "epochs": len(hist),
+                        "loss_first_epoch": hist[0], "loss_last_epoch": hist[-1]}}
+    for name, pc, max_iter in (("plain_cg", rpb.PRECOND_NONE, 20000),
+                               ("learned_fcg", rpb.PRECOND_LEARNED, 20000),
+                               ("reference_precond_cg", rpb.PRECOND_REFERENCE, 2000)):
+        t = time.perf_counter()
+        tpm.Solve(M, 1.0, B, max_iter=max_iter, tolerance=1e-6, precond=pc, strict=False)
+        ms = 1e3 * (time.perf_counter() - t)
+        rr = [float(x) for x in tpm.Solver_RelativeResiduals()]
+        res[name] = {"ms": ms, "iterations": tpm.Solver_IterationCount(), "rel_residual": rr,
+                     "converged": bool(max(rr) <= 1e-6)}
+    return res
 
 
 if __name__ == "__main__":

@@ -164,6 +164,43 @@ rpb_status rpb_tpm0_solve(rpb_mesh* m, double q, double p, double alpha, const d
                           double* X, int ldX, int nrhs, int max_iter, double tol, int precond, int* iterations,
                           double* rel_residual);
 
+/* --- learned preconditioner ------------------------------------------------------------ */
+
+/* No counterpart in the reference: a per-cluster MLP (16 -> 64 -> 64 -> 3, GELU, BF16
+ * weights, FP32 accumulation) that maps a residual r (n_v x 3) to a correction z. Every
+ * cluster C reads 16 features of r and of its geometry (residual moment
+ * R_C = sum_{i in C} a_i mean(r), barycentre, averaged normal, area, diameter, tree level,
+ * 4 child-residual norms) and emits gains g_C = exp(clamp(o_C, +-3)); z is the multilevel
+ * sum over the clusters containing each primitive of g_C R_C / A_C, gathered to the
+ * vertices with the weights a_i/(n+1), minus the column means. rpb_tpm0_solve with
+ * RPB_PRECOND_LEARNED uses it inside flexible CG and switches to the reference
+ * preconditioner (MultiplyPreconditioner) when the residual stalls. */
+typedef struct rpb_mlp rpb_mlp;
+
+/* Number of FP32 parameters (W1 64x16, b1 64, W2 64x64, b2 64, W3 3x64, b3 3 = 5443). */
+int rpb_mlp_param_count(void);
+/* New network on `device`, Xavier-uniform weights from `seed`, zero biases. */
+rpb_status rpb_mlp_create(int device, uint64_t seed, rpb_mlp** out);
+rpb_status rpb_mlp_destroy(rpb_mlp* mlp);
+/* FP32 master parameters (host arrays of rpb_mlp_param_count() floats); set resets Adam. */
+rpb_status rpb_mlp_get_params(const rpb_mlp* mlp, float* params);
+rpb_status rpb_mlp_set_params(rpb_mlp* mlp, const float* params);
+/* Network on n feature rows F (n x 16, host): O (n x 3). With dO (n x 3) and grad
+ * (param_count) non-NULL also grad = d(sum dO . O)/d(params) (for gradient checks). */
+rpb_status rpb_mlp_eval(rpb_mlp* mlp, const float* F, int64_t n, const float* dO, float* O, float* grad);
+/* One Adam step (lr <= 0: none) on npairs (residual R_k, correction E_k) pairs of mesh m
+ * (host, n_v x 3 each, consecutive; A E_k = R_k for the metric A of exponents q, p):
+ * loss = mean_k 1 - (z_k.R_k)^2 / ((z_k.A z_k)(E_k.R_k)) with z_k = M(R_k), the share of
+ * the error energy ||E_k||_A^2 that the best step along z_k leaves. `loss` and `grad`
+ * (param_count floats; either may be NULL) receive the loss and its gradient before the step. */
+rpb_status rpb_mlp_train_step(rpb_mlp* mlp, rpb_mesh* m, double q, double p, const double* R, const double* E,
+                              int npairs, double lr, double* loss, float* grad);
+/* Attach (mlp non-NULL) or detach the network used by RPB_PRECOND_LEARNED on this mesh;
+ * the mesh keeps the pointer, the caller keeps ownership. */
+rpb_status rpb_mesh_set_learned(rpb_mesh* m, rpb_mlp* mlp);
+/* Z = M(R) for one residual (host arrays, n_v x 3, row-major). */
+rpb_status rpb_tpm0_learned_apply(rpb_mesh* m, const double* R, double* Z);
+
 /* --- energy without device allocation -------------------------------------------------- */
 
 /* No counterpart in the reference (Repulsor has no device path). TangentPointEnergy0

@@ -78,6 +78,7 @@ class SimplicialMesh:
               "SimplicialMesh")
         self._h = h
         self._V = V
+        self._S = S
         self._cache = {}
 
     def __del__(self):
@@ -319,8 +320,13 @@ class TangentPointMetric0:
               "MultiplyPreconditioner")
         return Y
 
-    def Solve(self, M, alpha, B, beta=0.0, X=None, max_iter=1000, tolerance=1e-6, precond=PRECOND_REFERENCE):
-        """X = alpha * A^{-1} B + beta * X (src/Metrics/MetricDimRestricted.hpp:232-289)."""
+    def Solve(self, M, alpha, B, beta=0.0, X=None, max_iter=1000, tolerance=1e-6, precond=PRECOND_REFERENCE,
+              strict=True):
+        """X = alpha * A^{-1} B + beta * X (src/Metrics/MetricDimRestricted.hpp:232-289).
+
+        The iterate after max_iter iterations is returned in every case; with strict=True
+        a missed tolerance raises RepulsorError (RPB_ENOTCONV) after the statistics
+        (Solver_IterationCount, Solver_RelativeResiduals) have been recorded."""
         M = _as_mesh(M)
         B = np.ascontiguousarray(B, dtype=np.float64)
         self._check_nrhs(B.shape[1], "Solve")
@@ -328,11 +334,13 @@ class TangentPointMetric0:
             X = np.zeros((M.nV, 3))
         it = ctypes.c_int()
         rr = np.zeros(3)
-        check(_capi.load().rpb_tpm0_solve(M._h, self.q, self.p, float(alpha), dptr(B), B.shape[1], float(beta),
-                                          dptr(X), X.shape[1], B.shape[1], int(max_iter), float(tolerance),
-                                          int(precond), ctypes.byref(it), dptr(rr)), "Solve")
+        st = _capi.load().rpb_tpm0_solve(M._h, self.q, self.p, float(alpha), dptr(B), B.shape[1], float(beta),
+                                         dptr(X), X.shape[1], B.shape[1], int(max_iter), float(tolerance),
+                                         int(precond), ctypes.byref(it), dptr(rr))
         self.iter = it.value
         self.rel_residuals = rr
+        if st != _capi.RPB_ENOTCONV or strict:
+            check(st, "Solve")
         return X
 
     def Solver_IterationCount(self):

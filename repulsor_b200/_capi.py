@@ -21,6 +21,7 @@ PRECOND_NONE, PRECOND_REFERENCE, PRECOND_LEARNED = 0, 1, 2
 _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int)
 _lp = ctypes.POINTER(ctypes.c_int64)
+_fp = ctypes.POINTER(ctypes.c_float)
 _vp = ctypes.c_void_p
 
 
@@ -89,6 +90,16 @@ SIGNATURES = {
     "rpb_tpe0_value_noalloc": (ctypes.c_int, [ctypes.c_int, _vp, ctypes.c_int64, _vp, ctypes.c_int64, _vp, _vp, _vp,
                                               ctypes.c_int64, _vp, _vp, _vp, _vp, ctypes.c_double, ctypes.c_double,
                                               _vp, _vp]),
+    "rpb_mlp_param_count": (ctypes.c_int, []),
+    "rpb_mlp_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_uint64, ctypes.POINTER(_vp)]),
+    "rpb_mlp_destroy": (ctypes.c_int, [_vp]),
+    "rpb_mlp_get_params": (ctypes.c_int, [_vp, _fp]),
+    "rpb_mlp_set_params": (ctypes.c_int, [_vp, _fp]),
+    "rpb_mlp_eval": (ctypes.c_int, [_vp, _fp, ctypes.c_int64, _fp, _fp, _fp]),
+    "rpb_mlp_train_step": (ctypes.c_int, [_vp, _vp, ctypes.c_double, ctypes.c_double, _dp, _dp, ctypes.c_int,
+                                          ctypes.c_double, _dp, _fp]),
+    "rpb_mesh_set_learned": (ctypes.c_int, [_vp, _vp]),
+    "rpb_tpm0_learned_apply": (ctypes.c_int, [_vp, _dp, _dp]),
 }
 
 _lib = None
@@ -132,3 +143,7 @@ def iptr(a):
 
 def lptr(a):
     return a.ctypes.data_as(_lp)
+
+
+def fptr(a):
+    return a.ctypes.data_as(_fp)

@@ -153,6 +153,40 @@ __global__ void k_scan_rows(double* rows, int n)
     if (threadIdx.x < W) rows[static_cast<int64_t>(W) * n + threadIdx.x] = carry[threadIdx.x];
 }
 
+// Range sums over clusters of a per-primitive W-vector: in-block scans, block scan
+// (k_scan_rows), then out_C = S[end] - S[begin].
+template <int W>
+__global__ void __launch_bounds__(SCAN_BLOCK) k_block_scan_rows(int N, const double* vals, double* local, double* blocks)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double v[W], tot[W];
+#pragma unroll
+    for (int k = 0; k < W; ++k) v[k] = (i < N) ? vals[static_cast<int64_t>(W) * i + k] : 0.0;
+    block_exclusive_scan<W>(v, tot);
+    if (i < N) {
+#pragma unroll
+        for (int k = 0; k < W; ++k) local[static_cast<int64_t>(W) * i + k] = v[k];
+    }
+    if (threadIdx.x < W) blocks[static_cast<int64_t>(W) * blockIdx.x + threadIdx.x] = tot[threadIdx.x];
+}
+
+template <int W>
+__global__ void k_range_sums(int N, int NC, const int* C_begin, const int* C_end, const double* local,
+                             const double* blocks, double* out)
+{
+    const int C = blockIdx.x * blockDim.x + threadIdx.x;
+    if (C >= NC) return;
+    const int b = C_begin[C], e = C_end[C];
+    const int nb = (N + SCAN_BLOCK - 1) / SCAN_BLOCK;
+#pragma unroll
+    for (int k = 0; k < W; ++k) {
+        const double sb = blocks[static_cast<int64_t>(W) * (b / SCAN_BLOCK) + k] + local[static_cast<int64_t>(W) * b + k];
+        const double se = (e < N) ? blocks[static_cast<int64_t>(W) * (e / SCAN_BLOCK) + k] + local[static_cast<int64_t>(W) * e + k]
+                                  : blocks[static_cast<int64_t>(W) * nb + k];
+        out[static_cast<int64_t>(W) * C + k] = se - sb;
+    }
+}
+
 struct GeomArgs {
     int dom, N, NC;
     const double* V;          // nV x 3

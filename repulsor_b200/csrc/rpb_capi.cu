@@ -394,6 +394,7 @@ rpb_status rpb_mesh_destroy(rpb_mesh* m)
     cudaSetDevice(m->device);
     if (m->stream) cudaStreamSynchronize(m->stream);
     solver_free(m);
+    learned_free(m);
     cudaStream_t s = m->own_stream;
     delete m;  // frees device buffers
     if (s) cudaStreamDestroy(s);

@@ -34,5 +34,6 @@ rpb_status reference_precondition(rpb_mesh* m, double q, double p, const double*
 
 // learned preconditioner (rpb_learned.cu): Z = MLP correction of the residual R (n x 3, device)
 rpb_status learned_precondition(rpb_mesh* m, double q, double p, const double* R, double* Z);
+void learned_free(rpb_mesh* m);
 
 }  // namespace rpb

@@ -1,16 +1,807 @@
-// Learned per-cluster preconditioner (filled in by the MLP implementation).
+// Learned per-cluster preconditioner for the metric Solve (flexible CG).
+//
+// For a residual r (vertices x 3) the preconditioner returns z = M(r):
+//   1. cluster residual moments R_C = sum_{i in C} a_i mean(r over simplex i): row 0 of
+//      the Pre operator (src/ClusterTree.hpp:770-857) followed by the upward sums over
+//      the tree, done as range sums over prefix sums (clusters are contiguous ranges),
+//   2. 16 features per cluster: R_C / (A_C s) (3, s = RMS of r), centre relative to the
+//      root / root diameter (3), averaged unit normal sum(a n)/A (3), log(A_C/A_root)/10,
+//      log(d_C/d_root)/10, depth / max depth, and the 4 child-residual norms
+//      |R_L|/(A_L s), |R_R|/(A_R s), |R_LL + R_LR|/(A_L s), |R_RL + R_RR|/(A_R s)
+//      (zero where the children do not exist),
+//   3. an MLP 16 -> 64 -> 64 -> 3 with GELU, BF16 weights and FP32 accumulation gives
+//      o_C; the per-component gains g_C = exp(clamp(o_C, +-3)) scale the multilevel
+//      coefficient c_C = g_C * R_C / A_C,
+//   4. every primitive gets Z_i = sum over the clusters containing i of c_C
+//      (PercolateDown + ClustersToPrimitives, src/ClusterTree.hpp:706-768) and every
+//      vertex z_v = sum_{i at v} a_i/(n+1) Z_i (the transpose of step 1), minus the
+//      column means (translations are the kernel of the metric).
+// With all gains 1 this is the fixed symmetric positive definite multilevel operator
+// W^T E diag(1/A_C) E^T W; the gains make it nonlinear but homogeneous of degree one in r,
+// and z . r > 0 always, so flexible CG cannot break down on it.
+//
+// Training (rpb_mlp_train_step) on (residual r, correction e) pairs with A e = r: the loss
+// 1 - (z.r)^2 / ((z.Az)(e.r)) is the share of ||e||_A^2 that the best step along z = M(r)
+// leaves; one metric product Az per pair. Its adjoint runs steps 4 -> 1 backwards
+// (primitive moments and range sums again), then the MLP backward pass; weight gradients
+// are split-K reductions over the clusters; Adam on FP32 master weights that are rounded
+// to the BF16 copy the kernels read.
+#include <cmath>
+#include <cstring>
+#include <random>
 #include <string>
+#include <vector>
 
+#include <cuda_bf16.h>
+
+#include "kernels_energy.cuh"
 #include "rpb_internal.cuh"
 #include "rpb_mesh.cuh"
+#include "rpb_solver.cuh"
 
 namespace rpb {
 
-rpb_status learned_precondition(rpb_mesh* m, double, double, const double*, double*)
+#define RPB_CUDA(call)                                                                        \
+    do {                                                                                      \
+        cudaError_t e_ = (call);                                                              \
+        if (e_ != cudaSuccess) {                                                              \
+            set_error(std::string("CUDA error: ") + cudaGetErrorString(e_) + " at " #call);   \
+            return e_ == cudaErrorMemoryAllocation ? RPB_ENOMEM : RPB_ECUDA;                  \
+        }                                                                                     \
+    } while (0)
+
+constexpr int NF = 16, NH = 64, NO = 3;
+constexpr int OFF_W1 = 0;                     // NH x NF
+constexpr int OFF_B1 = OFF_W1 + NH * NF;      // NH
+constexpr int OFF_W2 = OFF_B1 + NH;           // NH x NH
+constexpr int OFF_B2 = OFF_W2 + NH * NH;      // NH
+constexpr int OFF_W3 = OFF_B2 + NH;           // NO x NH
+constexpr int OFF_B3 = OFF_W3 + NO * NH;      // NO
+constexpr int NPARAM = OFF_B3 + NO;           // 5443
+
+__device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f)); }
+__device__ __forceinline__ float gelu_grad(float x)
 {
-    (void)m;
-    set_error("the learned preconditioner has not been trained for this mesh");
-    return RPB_EINVAL;
+    return 0.5f * (1.0f + erff(x * 0.70710678118654752f)) + x * 0.39894228040143268f * expf(-0.5f * x * x);
+}
+
+// ------------------------------------------------------------------------------------------
+// MLP forward / backward, one thread per cluster; weights staged in shared memory as FP32
+// from their BF16 copies.
+// ------------------------------------------------------------------------------------------
+__device__ void stage_weights(const __nv_bfloat16* w, float* sw)
+{
+    for (int k = threadIdx.x; k < NPARAM; k += blockDim.x) sw[k] = __bfloat162float(w[k]);
+    __syncthreads();
+}
+
+struct MlpArgs {
+    int n;
+    const __nv_bfloat16* w;   // NPARAM BF16 weights
+    const float* F;           // n x NF
+    float* O;                 // n x NO
+    float* pre1;              // n x NH (training only)
+    float* pre2;              // n x NH (training only)
+};
+
+__global__ void __launch_bounds__(128) k_mlp_forward(MlpArgs A)
+{
+    extern __shared__ float sw[];
+    stage_weights(A.w, sw);
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= A.n) return;
+    float f[NF];
+#pragma unroll
+    for (int k = 0; k < NF; ++k) f[k] = A.F[NF * static_cast<int64_t>(c) + k];
+    float h1[NH];
+#pragma unroll 4
+    for (int j = 0; j < NH; ++j) {
+        float s = sw[OFF_B1 + j];
+#pragma unroll
+        for (int k = 0; k < NF; ++k) s = fmaf(sw[OFF_W1 + NF * j + k], f[k], s);
+        if (A.pre1) A.pre1[NH * static_cast<int64_t>(c) + j] = s;
+        h1[j] = gelu(s);
+    }
+    float o[NO] = {sw[OFF_B3 + 0], sw[OFF_B3 + 1], sw[OFF_B3 + 2]};
+    for (int j = 0; j < NH; ++j) {
+        float s = sw[OFF_B2 + j];
+#pragma unroll
+        for (int k = 0; k < NH; ++k) s = fmaf(sw[OFF_W2 + NH * j + k], h1[k], s);
+        if (A.pre2) A.pre2[NH * static_cast<int64_t>(c) + j] = s;
+        const float h2 = gelu(s);
+#pragma unroll
+        for (int q = 0; q < NO; ++q) o[q] = fmaf(sw[OFF_W3 + NH * q + j], h2, o[q]);
+    }
+#pragma unroll
+    for (int q = 0; q < NO; ++q) A.O[NO * static_cast<int64_t>(c) + q] = o[q];
+}
+
+struct MlpBackArgs {
+    int n;
+    const __nv_bfloat16* w;
+    const float* dO;          // n x NO
+    const float* pre1;
+    const float* pre2;
+    float* d2;                // n x NH: dL/dpre2
+    float* d1;                // n x NH: dL/dpre1
+};
+
+__global__ void __launch_bounds__(128) k_mlp_backward(MlpBackArgs A)
+{
+    extern __shared__ float sw[];
+    stage_weights(A.w, sw);
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= A.n) return;
+    const float do0 = A.dO[NO * static_cast<int64_t>(c)], do1 = A.dO[NO * static_cast<int64_t>(c) + 1],
+                do2 = A.dO[NO * static_cast<int64_t>(c) + 2];
+    float g2[NH];
+#pragma unroll 4
+    for (int j = 0; j < NH; ++j) {
+        const float dh2 = sw[OFF_W3 + j] * do0 + sw[OFF_W3 + NH + j] * do1 + sw[OFF_W3 + 2 * NH + j] * do2;
+        g2[j] = dh2 * gelu_grad(A.pre2[NH * static_cast<int64_t>(c) + j]);
+        A.d2[NH * static_cast<int64_t>(c) + j] = g2[j];
+    }
+    for (int k = 0; k < NH; ++k) {
+        float s = 0.0f;
+#pragma unroll
+        for (int j = 0; j < NH; ++j) s = fmaf(sw[OFF_W2 + NH * j + k], g2[j], s);
+        A.d1[NH * static_cast<int64_t>(c) + k] = s * gelu_grad(A.pre1[NH * static_cast<int64_t>(c) + k]);
+    }
+}
+
+// Split-K weight gradient: partial[b][p][q] = sum_{n in chunk b} G[n][p] * act(X[n][q]),
+// with act = identity (X = features) or GELU (X = pre-activations); column p = P means the
+// bias gradient (sum of G). P <= 64, Q <= 64.
+constexpr int WG_CHUNK = 1024;
+
+__global__ void __launch_bounds__(256) k_weight_grad(int n, const float* G, int P, const float* X, int Q, bool gelu_x,
+                                                     float* partial)
+{
+    __shared__ float sg[32][65];
+    __shared__ float sx[32][65];
+    const int n0 = blockIdx.x * WG_CHUNK, n1 = min(n, n0 + WG_CHUNK);
+    constexpr int OUT_PER_THREAD = (65 * 64 + 255) / 256;
+    float acc[OUT_PER_THREAD];
+#pragma unroll
+    for (int t = 0; t < OUT_PER_THREAD; ++t) acc[t] = 0.0f;
+    const int total = P * (Q + 1);
+    for (int base = n0; base < n1; base += 32) {
+        for (int e = threadIdx.x; e < 32 * 64; e += blockDim.x) {
+            const int r = e / 64, col = e % 64, row = base + r;
+            sg[r][col] = (row < n1 && col < P) ? G[static_cast<int64_t>(P) * row + col] : 0.0f;
+            float x = (row < n1 && col < Q) ? X[static_cast<int64_t>(Q) * row + col] : 0.0f;
+            if (gelu_x && row < n1 && col < Q) x = gelu(x);
+            sx[r][col] = x;
+        }
+        if (threadIdx.x < 32) sx[threadIdx.x][Q] = (base + threadIdx.x < n1) ? 1.0f : 0.0f;  // bias column
+        __syncthreads();
+#pragma unroll
+        for (int t = 0; t < OUT_PER_THREAD; ++t) {
+            const int o = threadIdx.x + 256 * t;
+            if (o < total) {
+                const int p = o / (Q + 1), q = o % (Q + 1);
+                float s = acc[t];
+#pragma unroll 8
+                for (int r = 0; r < 32; ++r) s = fmaf(sg[r][p], sx[r][q], s);
+                acc[t] = s;
+            }
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int t = 0; t < OUT_PER_THREAD; ++t) {
+        const int o = threadIdx.x + 256 * t;
+        if (o < total) partial[static_cast<int64_t>(blockIdx.x) * total + o] = acc[t];
+    }
+}
+
+// grad[p][q] (weights) and grad_b[p] (bias) = sum over blocks of the partials (fixed order)
+__global__ void k_reduce_grad(int nblocks, int P, int Q, const float* partial, float* gW, float* gb)
+{
+    const int o = blockIdx.x * blockDim.x + threadIdx.x;
+    const int total = P * (Q + 1);
+    if (o >= total) return;
+    float s = 0.0f;
+    for (int b = 0; b < nblocks; ++b) s += partial[static_cast<int64_t>(b) * total + o];
+    const int p = o / (Q + 1), q = o % (Q + 1);
+    if (q < Q) gW[Q * p + q] = s;
+    else gb[p] = s;
+}
+
+__global__ void k_adam(int n, float* theta, __nv_bfloat16* w16, const float* g, float* m, float* v, float lr,
+                       float b1, float b2, float eps, float bc1, float bc2)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const float gk = g[k];
+    const float mk = b1 * m[k] + (1.0f - b1) * gk;
+    const float vk = b2 * v[k] + (1.0f - b2) * gk * gk;
+    m[k] = mk;
+    v[k] = vk;
+    const float t = theta[k] - lr * (mk / bc1) / (sqrtf(vk / bc2) + eps);
+    theta[k] = t;
+    w16[k] = __float2bfloat16_rn(t);
+}
+
+// ------------------------------------------------------------------------------------------
+// features, correction and the adjoint of the correction
+// ------------------------------------------------------------------------------------------
+struct FeatArgs {
+    int NC, max_depth;
+    const ClusterDatum* C_pair;
+    const double* C_an;       // NC x 3: sum of a n over the cluster
+    const double* Rc;         // NC x 3: cluster residual moments
+    const int* C_left;
+    const int* C_right;
+    const int* C_depth;
+    const float* C_diam;
+    const double* scale;      // global RMS residual s
+    float* F;                 // NC x NF
+};
+
+__global__ void k_features(FeatArgs A)
+{
+    const int C = blockIdx.x * blockDim.x + threadIdx.x;
+    if (C >= A.NC) return;
+    const double s = fmax(*A.scale, 1e-300);
+    const ClusterDatum cd = load_datum(A.C_pair, C);
+    const ClusterDatum root = load_datum(A.C_pair, 0);
+    const double dr = fmax(static_cast<double>(A.C_diam[0]), 1e-300);
+    float f[NF];
+    const double* R = A.Rc + 3 * static_cast<int64_t>(C);
+    for (int k = 0; k < 3; ++k) f[k] = static_cast<float>(R[k] / (cd.a * s));
+    for (int k = 0; k < 3; ++k) f[3 + k] = static_cast<float>((cd.c[k] - root.c[k]) / dr);
+    for (int k = 0; k < 3; ++k) f[6 + k] = static_cast<float>(A.C_an[3 * static_cast<int64_t>(C) + k] / cd.a);
+    f[9] = static_cast<float>(log(cd.a / root.a) / 10.0);
+    f[10] = static_cast<float>(log(fmax(static_cast<double>(A.C_diam[C]), 1e-300) / dr) / 10.0);
+    f[11] = static_cast<float>(A.C_depth[C]) / static_cast<float>(max(A.max_depth, 1));
+    for (int k = 12; k < 16; ++k) f[k] = 0.0f;
+    const int L = A.C_left[C], Rr = A.C_right[C];
+    auto nrm = [&](int X) {
+        const double* q = A.Rc + 3 * static_cast<int64_t>(X);
+        return sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2]);
+    };
+    auto nrm2 = [&](int X, int Y) {
+        const double* q = A.Rc + 3 * static_cast<int64_t>(X);
+        const double* t = A.Rc + 3 * static_cast<int64_t>(Y);
+        const double a0 = q[0] + t[0], a1 = q[1] + t[1], a2 = q[2] + t[2];
+        return sqrt(a0 * a0 + a1 * a1 + a2 * a2);
+    };
+    if (L >= 0) {
+        const double aL = load_datum(A.C_pair, L).a, aR = load_datum(A.C_pair, Rr).a;
+        f[12] = static_cast<float>(nrm(L) / (aL * s));
+        f[13] = static_cast<float>(nrm(Rr) / (aR * s));
+        if (A.C_left[L] >= 0) f[14] = static_cast<float>(nrm2(A.C_left[L], A.C_right[L]) / (aL * s));
+        if (A.C_left[Rr] >= 0) f[15] = static_cast<float>(nrm2(A.C_left[Rr], A.C_right[Rr]) / (aR * s));
+    }
+    for (int k = 0; k < NF; ++k) A.F[NF * static_cast<int64_t>(C) + k] = f[k];
+}
+
+// Gains g_C = exp(clamp(o_C)) keep z . r > 0 for every residual (flexible CG never meets
+// r . z <= 0) and bound the nonlinearity of the preconditioner to [e^-3, e^3] times the
+// fixed multilevel operator.
+constexpr float GAIN_CLAMP = 3.0f;
+
+// c_C = g_C * R_C / A_C per component
+__global__ void k_cluster_coeffs(int NC, const float* O, const double* Rc, const ClusterDatum* C_pair, double* c)
+{
+    const int C = blockIdx.x * blockDim.x + threadIdx.x;
+    if (C >= NC) return;
+    const double inv_a = 1.0 / load_datum(C_pair, C).a;
+    for (int q = 0; q < 3; ++q) {
+        const float o = fminf(fmaxf(O[3 * static_cast<int64_t>(C) + q], -GAIN_CLAMP), GAIN_CLAMP);
+        c[3 * static_cast<int64_t>(C) + q] = exp(static_cast<double>(o)) * Rc[3 * static_cast<int64_t>(C) + q] * inv_a;
+    }
+}
+
+// Z_i = sum over the clusters containing primitive i of c_C (PercolateDown + ClustersToPrimitives)
+__global__ void k_expand_clusters(int N, const int* leaf_of, const int* C_parent, const double* c, double* Z)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    double z0 = 0, z1 = 0, z2 = 0;
+    for (int C = leaf_of[i]; C >= 0; C = C_parent[C]) {
+        z0 += c[3 * static_cast<int64_t>(C)];
+        z1 += c[3 * static_cast<int64_t>(C) + 1];
+        z2 += c[3 * static_cast<int64_t>(C) + 2];
+    }
+    Z[3 * static_cast<int64_t>(i)] = z0;
+    Z[3 * static_cast<int64_t>(i) + 1] = z1;
+    Z[3 * static_cast<int64_t>(i) + 2] = z2;
+}
+
+// z_v = sum_{(i,l) at v} w_il Z_i  (w = a/(n+1), the averaging row of Pre: the transpose
+// of the primitive moments, so that the fixed part of M is symmetric)
+__global__ void k_vertex_sum(int nV, int size, const int* vp_rp, const int* vp_slot, const double* pre_vals,
+                             const double* Z, double* z)
+{
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= nV) return;
+    double a0 = 0, a1 = 0, a2 = 0;
+    for (int k = vp_rp[v]; k < vp_rp[v + 1]; ++k) {
+        const int slot = vp_slot[k];
+        const int i = slot / size, l = slot - i * size;
+        const double w = pre_vals[(4 * static_cast<int64_t>(i)) * size + l];
+        a0 += w * Z[3 * static_cast<int64_t>(i)];
+        a1 += w * Z[3 * static_cast<int64_t>(i) + 1];
+        a2 += w * Z[3 * static_cast<int64_t>(i) + 2];
+    }
+    z[3 * static_cast<int64_t>(v)] = a0;
+    z[3 * static_cast<int64_t>(v) + 1] = a1;
+    z[3 * static_cast<int64_t>(v) + 2] = a2;
+}
+
+// per-primitive a*n (3) for the averaged-normal feature
+__global__ void k_prim_an(int N, const PrimDatum* P, double* an)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const PrimDatum d = load_datum(P, i);
+    for (int k = 0; k < 3; ++k) an[3 * static_cast<int64_t>(i) + k] = d.a * d.n[k];
+}
+
+// translation projection helpers: v -= mean (per column); mean from a device sum
+__global__ void k_sub_mean(int n, double* v, const double* sums)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    for (int c = 0; c < 3; ++c) v[3 * static_cast<int64_t>(i) + c] -= sums[c] / n;
+}
+
+__global__ void k_scale_from_dot(int n, const double* rr, double* scale)
+{
+    *scale = sqrt((rr[0] + rr[1] + rr[2]) / (3.0 * n));
+}
+
+// Energy-norm loss of one preconditioner application: with e the exact correction (A e = r),
+// loss = 1 - (z.r)^2 / ((z.Az)(e.r)) = 1 - cos^2_A(z, e), the share of ||e||_A^2 that the
+// best step along z leaves. Gradient wrt z: -2 (z.r)/((z.Az)(e.r)) r + 2 (z.r)^2/((z.Az)^2 (e.r)) Az.
+// dots: [0..2] z.r, [3..5] z.Az, [6..8] e.r per column.
+__global__ void k_loss_grad(int n, const double* r, const double* Az, const double* dots, double* g, double* loss_acc)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const double zr = dots[0] + dots[1] + dots[2];
+    const double zAz = fmax(dots[3] + dots[4] + dots[5], 1e-300);
+    const double er = fmax(dots[6] + dots[7] + dots[8], 1e-300);
+    const double c1 = -2.0 * zr / (zAz * er), c2 = 2.0 * zr * zr / (zAz * zAz * er);
+    if (i < n)
+        for (int c = 0; c < 3; ++c)
+            g[3 * static_cast<int64_t>(i) + c] = c1 * r[3 * static_cast<int64_t>(i) + c] + c2 * Az[3 * static_cast<int64_t>(i) + c];
+    if (i == 0) *loss_acc += 1.0 - zr * zr / (zAz * er);
+}
+
+// dL/do_C = sum_q gc_Cq R_Cq / A_C * g_Cq (zero where the clamp is active)
+__global__ void k_cluster_out_grad(int NC, const double* gc, const float* O, const double* Rc, const ClusterDatum* C_pair,
+                                   float* dO)
+{
+    const int C = blockIdx.x * blockDim.x + threadIdx.x;
+    if (C >= NC) return;
+    const double inv_a = 1.0 / load_datum(C_pair, C).a;
+    for (int q = 0; q < 3; ++q) {
+        const int64_t k = 3 * static_cast<int64_t>(C) + q;
+        const float o = O[k];
+        const bool inside = o > -GAIN_CLAMP && o < GAIN_CLAMP;
+        dO[k] = inside ? static_cast<float>(gc[k] * Rc[k] * inv_a * exp(static_cast<double>(o))) : 0.0f;
+    }
+}
+
+// out[c] = sum_i a[3i+c] * b[3i+c] (b == nullptr: column sums); one block, fixed order
+__global__ void __launch_bounds__(512) k_dot3_single(int n, const double* a, const double* b, double* out)
+{
+    __shared__ double sh[16][3];
+    double acc[3] = {0, 0, 0};
+    for (int i = threadIdx.x; i < n; i += blockDim.x)
+        for (int c = 0; c < 3; ++c) acc[c] += a[3 * static_cast<int64_t>(i) + c] * (b ? b[3 * static_cast<int64_t>(i) + c] : 1.0);
+    for (int c = 0; c < 3; ++c) acc[c] = warp_sum_f64(acc[c]);
+    if ((threadIdx.x & 31) == 0)
+        for (int c = 0; c < 3; ++c) sh[threadIdx.x >> 5][c] = acc[c];
+    __syncthreads();
+    if (threadIdx.x < 3) {
+        double t = 0;
+        for (int w = 0; w < (blockDim.x >> 5); ++w) t += sh[w][threadIdx.x];
+        out[threadIdx.x] = t;
+    }
+}
+
+// per-primitive residual moment a_i * mean(r over the simplex) (row 0 of the Pre operator)
+__global__ void k_prim_moments(int N, int size, const int* pre_cols, const double* pre_vals, const double* R, double* out)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    double a0 = 0, a1 = 0, a2 = 0;
+    for (int l = 0; l < size; ++l) {
+        const int v = pre_cols[size * i + l];
+        const double w = pre_vals[(4 * static_cast<int64_t>(i)) * size + l];
+        a0 += w * R[3 * static_cast<int64_t>(v)];
+        a1 += w * R[3 * static_cast<int64_t>(v) + 1];
+        a2 += w * R[3 * static_cast<int64_t>(v) + 2];
+    }
+    out[3 * static_cast<int64_t>(i)] = a0;
+    out[3 * static_cast<int64_t>(i) + 1] = a1;
+    out[3 * static_cast<int64_t>(i) + 2] = a2;
+}
+
+// dO_C = s * dL/dc_C (float), from the FP64 cluster sums of gZ
+__global__ void k_cluster_out_grad(int NC, const double* gc, const double* scale, float* dO)
+{
+    const int C = blockIdx.x * blockDim.x + threadIdx.x;
+    if (C >= NC) return;
+    const double s = *scale;
+    for (int q = 0; q < 3; ++q) dO[3 * static_cast<int64_t>(C) + q] = static_cast<float>(s * gc[3 * static_cast<int64_t>(C) + q]);
 }
 
 }  // namespace rpb
+
+// ==========================================================================================
+// host side
+// ==========================================================================================
+struct rpb_mlp {
+    int device = 0;
+    rpb::DevBuf<float> theta, grad, m, v, partial;
+    rpb::DevBuf<__nv_bfloat16> w16;
+    int64_t step = 0;
+};
+
+namespace rpb {
+
+struct LearnedState {
+    rpb_mlp* mlp = nullptr;
+    int64_t geometry_version = -1;
+    int max_depth = 0;
+    DevBuf<double> C_an, tmp3, Rc, c, Z, scale, sums, loss, gc, dots, g, r, z, e, Az;
+    DevBuf<float> F, O, dO, pre1, pre2, d1, d2, C_diam;
+    DevBuf<int> C_depth;
+};
+
+static rpb_status range_sums3(rpb_mesh* m, const double* prim3, double* out3)
+{
+    const int nb = (m->N + SCAN_BLOCK - 1) / SCAN_BLOCK;
+    k_block_scan_rows<3><<<nb, SCAN_BLOCK, 0, m->stream>>>(m->N, prim3, m->buf_scan_local.ptr, m->buf_scan_blocks.ptr);
+    k_scan_rows<3><<<1, SCAN_BLOCK, 0, m->stream>>>(m->buf_scan_blocks.ptr, nb);
+    k_range_sums<3><<<(m->NC + 255) / 256, 256, 0, m->stream>>>(m->N, m->NC, m->C_begin.ptr, m->C_end.ptr,
+                                                                m->buf_scan_local.ptr, m->buf_scan_blocks.ptr, out3);
+    RPB_CUDA(cudaGetLastError());
+    return RPB_OK;
+}
+
+static rpb_status ensure_learned(rpb_mesh* m)
+{
+    if (!m->learned) m->learned = new LearnedState();
+    LearnedState& L = *m->learned;
+    const size_t NC = m->NC, N = m->N, nV = m->nV;
+    if (!L.F.ptr) {
+        RPB_CUDA(L.C_an.alloc(3 * NC));
+        RPB_CUDA(L.tmp3.alloc(3 * N));
+        RPB_CUDA(L.Rc.alloc(3 * NC));
+        RPB_CUDA(L.c.alloc(3 * NC));
+        RPB_CUDA(L.Z.alloc(3 * N));
+        RPB_CUDA(L.scale.alloc(1));
+        RPB_CUDA(L.sums.alloc(4));
+        RPB_CUDA(L.loss.alloc(1));
+        RPB_CUDA(L.gc.alloc(3 * NC));
+        RPB_CUDA(L.dots.alloc(9));
+        RPB_CUDA(L.g.alloc(3 * nV));
+        RPB_CUDA(L.r.alloc(3 * nV));
+        RPB_CUDA(L.z.alloc(3 * nV));
+        RPB_CUDA(L.e.alloc(3 * nV));
+        RPB_CUDA(L.Az.alloc(3 * nV));
+        RPB_CUDA(L.F.alloc(NF * NC));
+        RPB_CUDA(L.O.alloc(NO * NC));
+        RPB_CUDA(L.dO.alloc(NO * NC));
+        RPB_CUDA(L.C_diam.alloc(NC));
+        RPB_CUDA(L.C_depth.alloc(NC));
+        std::vector<float> diam(NC);
+        for (size_t C = 0; C < NC; ++C) diam[C] = static_cast<float>(2.0 * std::sqrt(m->tree.C_box[7 * C]));
+        RPB_CUDA(cudaMemcpyAsync(L.C_diam.ptr, diam.data(), L.C_diam.bytes(), cudaMemcpyHostToDevice, m->stream));
+        RPB_CUDA(cudaMemcpyAsync(L.C_depth.ptr, m->tree.C_depth.data(), L.C_depth.bytes(), cudaMemcpyHostToDevice,
+                                 m->stream));
+        L.max_depth = m->tree.depth;
+        RPB_CUDA(cudaStreamSynchronize(m->stream));
+    }
+    if (L.geometry_version != m->geometry_version) {
+        k_prim_an<<<(m->N + 255) / 256, 256, 0, m->stream>>>(m->N, m->P_pair.ptr, L.tmp3.ptr);
+        rpb_status st = range_sums3(m, L.tmp3.ptr, L.C_an.ptr);
+        if (st != RPB_OK) return st;
+        L.geometry_version = m->geometry_version;
+    }
+    return RPB_OK;
+}
+
+void learned_free(rpb_mesh* m)
+{
+    delete m->learned;
+    m->learned = nullptr;
+}
+
+static rpb_status ensure_training_buffers(rpb_mesh* m)
+{
+    LearnedState& L = *m->learned;
+    if (!L.pre1.ptr) {
+        const size_t NC = m->NC;
+        RPB_CUDA(L.pre1.alloc(NH * NC));
+        RPB_CUDA(L.pre2.alloc(NH * NC));
+        RPB_CUDA(L.d1.alloc(NH * NC));
+        RPB_CUDA(L.d2.alloc(NH * NC));
+    }
+    return RPB_OK;
+}
+
+static rpb_status dot3_dev(rpb_mesh* m, const double* a, const double* b, double* out)
+{
+    k_dot3_single<<<1, 512, 0, m->stream>>>(m->nV, a, b, out);
+    RPB_CUDA(cudaGetLastError());
+    return RPB_OK;
+}
+
+// R_C = sum over the cluster's primitives of a_i mean(r) (Pre row 0, then range sums)
+static rpb_status cluster_moments(rpb_mesh* m, const double* R, double* Rc)
+{
+    k_prim_moments<<<(m->N + 255) / 256, 256, 0, m->stream>>>(m->N, m->size, m->pre_cols.ptr, m->pre_vals.ptr, R,
+                                                              m->learned->tmp3.ptr);
+    RPB_CUDA(cudaGetLastError());
+    return range_sums3(m, m->learned->tmp3.ptr, Rc);
+}
+
+// z = M_learned(R) (device, n_v x 3); with `training` the activations are kept.
+static rpb_status learned_forward(rpb_mesh* m, rpb_mlp* mlp, const double* R, double* z, bool training)
+{
+    LearnedState& L = *m->learned;
+    cudaStream_t s = m->stream;
+    rpb_status st;
+    if ((st = dot3_dev(m, R, R, L.sums.ptr)) != RPB_OK) return st;
+    k_scale_from_dot<<<1, 1, 0, s>>>(m->nV, L.sums.ptr, L.scale.ptr);
+    if ((st = cluster_moments(m, R, L.Rc.ptr)) != RPB_OK) return st;
+    FeatArgs fa;
+    fa.NC = m->NC; fa.max_depth = L.max_depth;
+    fa.C_pair = m->C_pair.ptr; fa.C_an = L.C_an.ptr; fa.Rc = L.Rc.ptr;
+    fa.C_left = m->C_left.ptr; fa.C_right = m->C_right.ptr; fa.C_depth = L.C_depth.ptr; fa.C_diam = L.C_diam.ptr;
+    fa.scale = L.scale.ptr; fa.F = L.F.ptr;
+    k_features<<<(m->NC + 255) / 256, 256, 0, s>>>(fa);
+    MlpArgs ma;
+    ma.n = m->NC; ma.w = mlp->w16.ptr; ma.F = L.F.ptr; ma.O = L.O.ptr;
+    ma.pre1 = training ? L.pre1.ptr : nullptr;
+    ma.pre2 = training ? L.pre2.ptr : nullptr;
+    k_mlp_forward<<<(m->NC + 127) / 128, 128, NPARAM * sizeof(float), s>>>(ma);
+    k_cluster_coeffs<<<(m->NC + 255) / 256, 256, 0, s>>>(m->NC, L.O.ptr, L.Rc.ptr, m->C_pair.ptr, L.c.ptr);
+    k_expand_clusters<<<(m->N + 255) / 256, 256, 0, s>>>(m->N, m->leaf_of.ptr, m->C_parent.ptr, L.c.ptr, L.Z.ptr);
+    k_vertex_sum<<<(m->nV + 255) / 256, 256, 0, s>>>(m->nV, m->size, m->vp_rp.ptr, m->vp_slot.ptr, m->pre_vals.ptr,
+                                                     L.Z.ptr, z);
+    RPB_CUDA(cudaGetLastError());
+    // remove the translation component (the kernel of the metric)
+    if ((st = dot3_dev(m, z, nullptr, L.sums.ptr)) != RPB_OK) return st;
+    k_sub_mean<<<(m->nV + 255) / 256, 256, 0, s>>>(m->nV, z, L.sums.ptr);
+    RPB_CUDA(cudaGetLastError());
+    return RPB_OK;
+}
+
+rpb_status learned_precondition(rpb_mesh* m, double, double, const double* R, double* Z)
+{
+    if (!m->learned || !m->learned->mlp) {
+        set_error("no learned preconditioner is attached to this mesh (rpb_mesh_set_learned)");
+        return RPB_EINVAL;
+    }
+    rpb_status st = ensure_learned(m);
+    if (st != RPB_OK) return st;
+    return learned_forward(m, m->learned->mlp, R, Z, false);
+}
+
+static rpb_status weight_grads(rpb_mlp* mlp, int n, const float* G, int P, const float* X, int Q, bool gelu_x,
+                               float* gW, float* gb, cudaStream_t s)
+{
+    const int nblocks = (n + WG_CHUNK - 1) / WG_CHUNK;
+    const size_t need = static_cast<size_t>(nblocks) * P * (Q + 1);
+    if (mlp->partial.n < need) RPB_CUDA(mlp->partial.alloc(need));
+    k_weight_grad<<<nblocks, 256, 0, s>>>(n, G, P, X, Q, gelu_x, mlp->partial.ptr);
+    k_reduce_grad<<<(P * (Q + 1) + 255) / 256, 256, 0, s>>>(nblocks, P, Q, mlp->partial.ptr, gW, gb);
+    RPB_CUDA(cudaGetLastError());
+    return RPB_OK;
+}
+
+// gradient of the MLP parameters for given cluster output gradients dO (all clusters)
+static rpb_status mlp_backward(rpb_mlp* mlp, int n, const float* F, const float* pre1, const float* pre2,
+                               const float* dO, float* d1, float* d2, float* grad, cudaStream_t s)
+{
+    MlpBackArgs ba;
+    ba.n = n; ba.w = mlp->w16.ptr; ba.dO = dO; ba.pre1 = pre1; ba.pre2 = pre2; ba.d2 = d2; ba.d1 = d1;
+    k_mlp_backward<<<(n + 127) / 128, 128, NPARAM * sizeof(float), s>>>(ba);
+    RPB_CUDA(cudaGetLastError());
+    rpb_status st;
+    if ((st = weight_grads(mlp, n, dO, NO, pre2, NH, true, grad + OFF_W3, grad + OFF_B3, s)) != RPB_OK) return st;
+    if ((st = weight_grads(mlp, n, d2, NH, pre1, NH, true, grad + OFF_W2, grad + OFF_B2, s)) != RPB_OK) return st;
+    if ((st = weight_grads(mlp, n, d1, NH, F, NF, false, grad + OFF_W1, grad + OFF_B1, s)) != RPB_OK) return st;
+    return RPB_OK;
+}
+
+__global__ void k_accumulate(int n, float* dst, const float* src)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) dst[k] += src[k];
+}
+
+}  // namespace rpb
+
+using namespace rpb;
+
+extern "C" {
+
+int rpb_mlp_param_count(void) { return NPARAM; }
+
+rpb_status rpb_mlp_create(int device, uint64_t seed, rpb_mlp** out)
+{
+    if (!out) { set_error("null argument"); return RPB_EINVAL; }
+    *out = nullptr;
+    RPB_CUDA(cudaSetDevice(device));
+    auto* mlp = new rpb_mlp();
+    mlp->device = device;
+    // Xavier-uniform weights, zero biases, a small output layer: all gains start near 1
+    std::vector<float> th(NPARAM, 0.0f);
+    std::mt19937_64 rng(seed);
+    auto fill = [&](int off, int fan_out, int fan_in, float gain) {
+        const float a = gain * std::sqrt(6.0f / (fan_in + fan_out));
+        std::uniform_real_distribution<float> U(-a, a);
+        for (int k = 0; k < fan_out * fan_in; ++k) th[off + k] = U(rng);
+    };
+    fill(OFF_W1, NH, NF, 1.0f);
+    fill(OFF_W2, NH, NH, 1.0f);
+    fill(OFF_W3, NO, NH, 0.01f);
+    if (mlp->theta.alloc(NPARAM) || mlp->grad.alloc(NPARAM) || mlp->m.alloc(NPARAM) || mlp->v.alloc(NPARAM) ||
+        mlp->w16.alloc(NPARAM)) {
+        delete mlp;
+        set_error("device allocation failed");
+        return RPB_ENOMEM;
+    }
+    rpb_status st = rpb_mlp_set_params(mlp, th.data());
+    if (st != RPB_OK) { delete mlp; return st; }
+    *out = mlp;
+    return RPB_OK;
+}
+
+rpb_status rpb_mlp_destroy(rpb_mlp* mlp)
+{
+    delete mlp;
+    return RPB_OK;
+}
+
+rpb_status rpb_mlp_get_params(const rpb_mlp* mlp, float* params)
+{
+    if (!mlp || !params) { set_error("null argument"); return RPB_EINVAL; }
+    RPB_CUDA(cudaSetDevice(mlp->device));
+    RPB_CUDA(cudaMemcpy(params, mlp->theta.ptr, mlp->theta.bytes(), cudaMemcpyDeviceToHost));
+    return RPB_OK;
+}
+
+rpb_status rpb_mlp_set_params(rpb_mlp* mlp, const float* params)
+{
+    if (!mlp || !params) { set_error("null argument"); return RPB_EINVAL; }
+    RPB_CUDA(cudaSetDevice(mlp->device));
+    std::vector<__nv_bfloat16> w(NPARAM);
+    for (int k = 0; k < NPARAM; ++k) w[k] = __float2bfloat16_rn(params[k]);
+    RPB_CUDA(cudaMemcpy(mlp->theta.ptr, params, mlp->theta.bytes(), cudaMemcpyHostToDevice));
+    RPB_CUDA(cudaMemcpy(mlp->w16.ptr, w.data(), mlp->w16.bytes(), cudaMemcpyHostToDevice));
+    RPB_CUDA(cudaMemset(mlp->m.ptr, 0, mlp->m.bytes()));
+    RPB_CUDA(cudaMemset(mlp->v.ptr, 0, mlp->v.bytes()));
+    mlp->step = 0;
+    return RPB_OK;
+}
+
+rpb_status rpb_mlp_eval(rpb_mlp* mlp, const float* F, int64_t n, const float* dO, float* O, float* grad)
+{
+    if (!mlp || !F || !O || n <= 0) { set_error("null or empty argument"); return RPB_EINVAL; }
+    RPB_CUDA(cudaSetDevice(mlp->device));
+    DevBuf<float> dF, dOut, p1, p2, g1, g2, ddO, gr;
+    RPB_CUDA(dF.alloc(NF * n));
+    RPB_CUDA(dOut.alloc(NO * n));
+    RPB_CUDA(p1.alloc(NH * n));
+    RPB_CUDA(p2.alloc(NH * n));
+    RPB_CUDA(cudaMemcpy(dF.ptr, F, dF.bytes(), cudaMemcpyHostToDevice));
+    MlpArgs ma;
+    ma.n = static_cast<int>(n); ma.w = mlp->w16.ptr; ma.F = dF.ptr; ma.O = dOut.ptr; ma.pre1 = p1.ptr; ma.pre2 = p2.ptr;
+    k_mlp_forward<<<static_cast<unsigned>((n + 127) / 128), 128, NPARAM * sizeof(float)>>>(ma);
+    RPB_CUDA(cudaGetLastError());
+    RPB_CUDA(cudaMemcpy(O, dOut.ptr, dOut.bytes(), cudaMemcpyDeviceToHost));
+    if (dO && grad) {
+        RPB_CUDA(g1.alloc(NH * n));
+        RPB_CUDA(g2.alloc(NH * n));
+        RPB_CUDA(ddO.alloc(NO * n));
+        RPB_CUDA(gr.alloc(NPARAM));
+        RPB_CUDA(cudaMemcpy(ddO.ptr, dO, ddO.bytes(), cudaMemcpyHostToDevice));
+        rpb_status st = mlp_backward(mlp, static_cast<int>(n), dF.ptr, p1.ptr, p2.ptr, ddO.ptr, g1.ptr, g2.ptr, gr.ptr, 0);
+        if (st != RPB_OK) return st;
+        RPB_CUDA(cudaMemcpy(grad, gr.ptr, gr.bytes(), cudaMemcpyDeviceToHost));
+    }
+    return RPB_OK;
+}
+
+rpb_status rpb_mesh_set_learned(rpb_mesh* m, rpb_mlp* mlp)
+{
+    if (!m) { set_error("null mesh"); return RPB_EINVAL; }
+    if (mlp && mlp->device != m->device) { set_error("network and mesh live on different devices"); return RPB_EINVAL; }
+    RPB_CUDA(cudaSetDevice(m->device));
+    rpb_status st = ensure_learned(m);
+    if (st != RPB_OK) return st;
+    m->learned->mlp = mlp;
+    return RPB_OK;
+}
+
+rpb_status rpb_tpm0_learned_apply(rpb_mesh* m, const double* R, double* Z)
+{
+    if (!m || !R || !Z) { set_error("null argument"); return RPB_EINVAL; }
+    RPB_CUDA(cudaSetDevice(m->device));
+    rpb_status st = ensure_learned(m);
+    if (st != RPB_OK) return st;
+    if (!m->learned->mlp) { set_error("no learned preconditioner attached"); return RPB_EINVAL; }
+    LearnedState& L = *m->learned;
+    RPB_CUDA(cudaMemcpyAsync(L.r.ptr, R, 3 * sizeof(double) * m->nV, cudaMemcpyHostToDevice, m->stream));
+    if ((st = learned_forward(m, L.mlp, L.r.ptr, L.z.ptr, false)) != RPB_OK) return st;
+    RPB_CUDA(cudaMemcpyAsync(Z, L.z.ptr, 3 * sizeof(double) * m->nV, cudaMemcpyDeviceToHost, m->stream));
+    RPB_CUDA(cudaStreamSynchronize(m->stream));
+    return RPB_OK;
+}
+
+rpb_status rpb_mlp_train_step(rpb_mlp* mlp, rpb_mesh* m, double q, double p, const double* R, const double* E,
+                              int npairs, double lr, double* loss, float* grad)
+{
+    if (!mlp || !m || !R || !E || npairs <= 0) { set_error("null or empty argument"); return RPB_EINVAL; }
+    if (mlp->device != m->device) { set_error("network and mesh live on different devices"); return RPB_EINVAL; }
+    rpb_status st = check_exponents(q, p);
+    if (st != RPB_OK) return st;
+    RPB_CUDA(cudaSetDevice(m->device));
+    if ((st = ensure_learned(m)) != RPB_OK) return st;
+    if ((st = ensure_training_buffers(m)) != RPB_OK) return st;
+    LearnedState& L = *m->learned;
+    cudaStream_t s = m->stream;
+    const int nV = m->nV;
+    const int eb = (nV + 255) / 256;
+    const size_t n3 = 3 * static_cast<size_t>(nV);
+    DevBuf<float> gsum;
+    RPB_CUDA(gsum.alloc(NPARAM));
+    RPB_CUDA(cudaMemsetAsync(gsum.ptr, 0, gsum.bytes(), s));
+    RPB_CUDA(cudaMemsetAsync(L.loss.ptr, 0, sizeof(double), s));
+    for (int k = 0; k < npairs; ++k) {
+        RPB_CUDA(cudaMemcpyAsync(L.r.ptr, R + k * n3, n3 * sizeof(double), cudaMemcpyHostToDevice, s));
+        RPB_CUDA(cudaMemcpyAsync(L.e.ptr, E + k * n3, n3 * sizeof(double), cudaMemcpyHostToDevice, s));
+        if ((st = learned_forward(m, mlp, L.r.ptr, L.z.ptr, true)) != RPB_OK) return st;
+        if ((st = metric_multiply_dev(m, q, p, 1.0, L.z.ptr, 3, 0.0, L.Az.ptr, 3, 7)) != RPB_OK) return st;
+        if ((st = dot3_dev(m, L.z.ptr, L.r.ptr, L.dots.ptr)) != RPB_OK) return st;
+        if ((st = dot3_dev(m, L.z.ptr, L.Az.ptr, L.dots.ptr + 3)) != RPB_OK) return st;
+        if ((st = dot3_dev(m, L.e.ptr, L.r.ptr, L.dots.ptr + 6)) != RPB_OK) return st;
+        k_loss_grad<<<eb, 256, 0, s>>>(nV, L.r.ptr, L.Az.ptr, L.dots.ptr, L.g.ptr, L.loss.ptr);
+        // back through the mean removal, the vertex sum and the cluster expansion (the
+        // transposes: primitive moments and range sums)
+        if ((st = dot3_dev(m, L.g.ptr, nullptr, L.sums.ptr)) != RPB_OK) return st;
+        k_sub_mean<<<eb, 256, 0, s>>>(nV, L.g.ptr, L.sums.ptr);
+        if ((st = cluster_moments(m, L.g.ptr, L.gc.ptr)) != RPB_OK) return st;
+        k_cluster_out_grad<<<(m->NC + 255) / 256, 256, 0, s>>>(m->NC, L.gc.ptr, L.O.ptr, L.Rc.ptr, m->C_pair.ptr,
+                                                               L.dO.ptr);
+        RPB_CUDA(cudaGetLastError());
+        if ((st = mlp_backward(mlp, m->NC, L.F.ptr, L.pre1.ptr, L.pre2.ptr, L.dO.ptr, L.d1.ptr, L.d2.ptr, mlp->grad.ptr,
+                               s)) != RPB_OK)
+            return st;
+        k_accumulate<<<(NPARAM + 255) / 256, 256, 0, s>>>(NPARAM, gsum.ptr, mlp->grad.ptr);
+    }
+    std::vector<float> gh;
+    if (grad) {
+        gh.resize(NPARAM);
+        RPB_CUDA(cudaMemcpyAsync(gh.data(), gsum.ptr, gsum.bytes(), cudaMemcpyDeviceToHost, s));
+    }
+    // Adam on the mean gradient (the bias corrections carry the 1/npairs)
+    mlp->step += 1;
+    const float b1 = 0.9f, b2 = 0.999f;
+    const float bc1 = 1.0f - std::pow(b1, static_cast<float>(mlp->step));
+    const float bc2 = 1.0f - std::pow(b2, static_cast<float>(mlp->step));
+    const float np = static_cast<float>(npairs);
+    if (lr > 0.0)
+        k_adam<<<(NPARAM + 255) / 256, 256, 0, s>>>(NPARAM, mlp->theta.ptr, mlp->w16.ptr, gsum.ptr, mlp->m.ptr, mlp->v.ptr,
+                                                    static_cast<float>(lr), b1, b2, 1e-8f, bc1 * np, bc2 * np * np);
+    RPB_CUDA(cudaGetLastError());
+    double l = 0;
+    RPB_CUDA(cudaMemcpyAsync(&l, L.loss.ptr, sizeof(double), cudaMemcpyDeviceToHost, s));
+    RPB_CUDA(cudaStreamSynchronize(s));
+    if (lr <= 0.0) mlp->step -= 1;
+    if (loss) *loss = l / npairs;
+    if (grad)
+        for (int k = 0; k < NPARAM; ++k) grad[k] = gh[k] / np;
+    return RPB_OK;
+}
+
+}  // extern "C"

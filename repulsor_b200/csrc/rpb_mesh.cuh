@@ -13,6 +13,7 @@
 namespace rpb {
 
 struct Solver;
+struct LearnedState;
 void set_error(const std::string& msg);
 
 template <typename T>
@@ -108,6 +109,8 @@ struct rpb_mesh {
 
     // solver state (allocated on first solve)
     rpb::Solver* solver = nullptr;
+    // learned preconditioner state (allocated on first use)
+    rpb::LearnedState* learned = nullptr;
 
     int64_t device_bytes() const;
 };

@@ -391,6 +391,8 @@ static rpb_status cg_solve(rpb_mesh* m, double q, double p, const double* B, int
     cudaStream_t stream = m->stream;
     const int eb = (n + 255) / 256;
     const bool flexible = (precond == RPB_PRECOND_LEARNED);
+    // iterations without a 10% drop of the best residual that count as a stall
+    constexpr int kStallWindow = 100;
     int kind = precond;
 
     // ||B|| per column
@@ -447,7 +449,7 @@ static rpb_status cg_solve(rpb_mesh* m, double q, double p, const double* B, int
             }
             // stall detection only guards the flexible (learned) iteration, which then falls
             // back to the reference preconditioner; fixed-preconditioner CG is never restarted
-            if (flexible && kind == RPB_PRECOND_LEARNED && !conv && ++since_best > 60) stalled = true;
+            if (flexible && kind == RPB_PRECOND_LEARNED && !conv && ++since_best > kStallWindow) stalled = true;
             if (conv || stalled) {
                 stalled_flag = stalled;
                 since_best = 0;

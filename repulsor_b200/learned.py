@@ -1,0 +1,172 @@
+"""Learned per-cluster preconditioner for TangentPointMetric0.Solve.
+
+The network (16 -> 64 -> 64 -> 3, GELU, BF16 weights with FP32 accumulation) lives on
+the device and is trained there by the library's own forward/backward/Adam kernels
+(``rpb_mlp_*`` in include/repulsor_b200.h) on (residual, solve-correction) pairs that
+plain CG solves of the metric produce:
+
+    for a right-hand side b with exact solution x* = A^{-1} b (a tight plain CG solve)
+    and a CG iterate x_k, the pair is r_k = b - A x_k and e_k = x* - x_k, so that
+    A e_k = r_k.
+
+``Solve(..., precond=PRECOND_LEARNED)`` then runs flexible CG with z = M(r); when the
+residual stops decreasing it switches to the reference preconditioner
+(MultiplyPreconditioner) for the rest of the solve.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _capi
+from ._capi import PRECOND_NONE, RepulsorError, check, dptr, fptr
+
+__all__ = ["LearnedPreconditioner", "training_pairs", "train"]
+
+
+class LearnedPreconditioner:
+    """One MLP on a CUDA device; attach it to meshes with ``attach``."""
+
+    def __init__(self, seed: int = 0, device: int = 0, params=None):
+        lib = _capi.load()
+        h = ctypes.c_void_p()
+        check(lib.rpb_mlp_create(int(device), ctypes.c_uint64(seed), ctypes.byref(h)), "rpb_mlp_create")
+        self._h = h
+        self.device = device
+        if params is not None:
+            self.set_params(params)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h and _capi is not None and _capi._lib is not None:
+            _capi._lib.rpb_mlp_destroy(h)
+            self._h = None
+
+    @staticmethod
+    def param_count() -> int:
+        return _capi.load().rpb_mlp_param_count()
+
+    def get_params(self) -> np.ndarray:
+        out = np.zeros(self.param_count(), np.float32)
+        check(_capi.load().rpb_mlp_get_params(self._h, fptr(out)), "rpb_mlp_get_params")
+        return out
+
+    def set_params(self, params):
+        params = np.ascontiguousarray(params, dtype=np.float32)
+        if params.size != self.param_count():
+            raise RepulsorError(_capi.RPB_EINVAL, f"expected {self.param_count()} parameters, got {params.size}")
+        check(_capi.load().rpb_mlp_set_params(self._h, fptr(params)), "rpb_mlp_set_params")
+
+    def save(self, path):
+        np.save(path, self.get_params())
+
+    @classmethod
+    def load(cls, path, device: int = 0):
+        return cls(device=device, params=np.load(path))
+
+    def eval(self, F, dO=None):
+        """MLP outputs O (n x 3) for features F (n x 16); with dO also d(sum dO*O)/dparams."""
+        F = np.ascontiguousarray(F, dtype=np.float32)
+        n = F.shape[0]
+        O = np.zeros((n, 3), np.float32)
+        grad = None
+        if dO is not None:
+            dO = np.ascontiguousarray(dO, dtype=np.float32)
+            grad = np.zeros(self.param_count(), np.float32)
+        check(_capi.load().rpb_mlp_eval(self._h, fptr(F), n, None if dO is None else fptr(dO), fptr(O),
+                                        None if grad is None else fptr(grad)), "rpb_mlp_eval")
+        return O if dO is None else (O, grad)
+
+    def attach(self, M):
+        check(_capi.load().rpb_mesh_set_learned(M._h, self._h), "rpb_mesh_set_learned")
+        M._learned = self          # keep the network alive while the mesh uses it
+
+    @staticmethod
+    def detach(M):
+        check(_capi.load().rpb_mesh_set_learned(M._h, None), "rpb_mesh_set_learned")
+        M._learned = None
+
+    def apply(self, M, R):
+        """z = M(R) on mesh M (attaches the network to M)."""
+        self.attach(M)
+        R = np.ascontiguousarray(R, dtype=np.float64)
+        Z = np.zeros_like(R)
+        check(_capi.load().rpb_tpm0_learned_apply(M._h, dptr(R), dptr(Z)), "rpb_tpm0_learned_apply")
+        return Z
+
+    def train_step(self, M, metric, R, E, lr=1e-3, want_grad=False):
+        """One Adam step (none for lr <= 0) on the pairs (R[k], E[k]) of mesh M and the
+        metric's exponents; returns the loss before the step (and its gradient with
+        want_grad)."""
+        R = np.ascontiguousarray(R, dtype=np.float64)
+        E = np.ascontiguousarray(E, dtype=np.float64)
+        if R.ndim == 2:
+            R, E = R[None], E[None]
+        loss = ctypes.c_double()
+        grad = np.zeros(self.param_count(), np.float32) if want_grad else None
+        check(_capi.load().rpb_mlp_train_step(self._h, M._h, metric.q, metric.p, dptr(R), dptr(E), R.shape[0], float(lr),
+                                              ctypes.byref(loss), None if grad is None else fptr(grad)),
+              "rpb_mlp_train_step")
+        return (loss.value, grad) if want_grad else loss.value
+
+
+def training_pairs(M, metric, n_rhs=4, checkpoints=(0, 4, 16, 48, 128), seed=0, exact_tol=1e-9,
+                   exact_max_iter=20000, smooth=0):
+    """(R, E) pairs from plain CG solves of metric on mesh M.
+
+    For each of n_rhs seeded right-hand sides b (column means removed, optionally
+    smoothed by `smooth` passes of vertex averaging over the simplices), x* is solved
+    by plain CG to exact_tol; every checkpoint k gives the CG iterate x_k after k
+    iterations and the pair (b - A x_k, x* - x_k)."""
+    from . import meshes
+
+    V = M.VertexCoordinates()
+    nV = V.shape[0]
+    Rs, Es = [], []
+    for j in range(n_rhs):
+        b = meshes.random_rhs(nV, seed=seed + j, project=True)
+        for _ in range(smooth):
+            b = _smooth(M, b)
+        xs = metric.Solve(M, 1.0, b, max_iter=exact_max_iter, tolerance=exact_tol, precond=PRECOND_NONE,
+                          strict=False)
+        for k in checkpoints:
+            if k == 0:
+                xk = np.zeros_like(b)
+            else:
+                xk = metric.Solve(M, 1.0, b, max_iter=k, tolerance=1e-30, precond=PRECOND_NONE, strict=False)
+            r = b - metric.MultiplyMetric(M, 1.0, xk)
+            Rs.append(r)
+            Es.append(xs - xk)
+    return np.stack(Rs), np.stack(Es)
+
+
+def _smooth(M, b):
+    S = M._S if hasattr(M, "_S") else None
+    if S is None:
+        return b
+    acc = np.zeros_like(b)
+    cnt = np.zeros(b.shape[0])
+    for l in range(S.shape[1]):
+        np.add.at(acc, S[:, l], b[S].mean(1))
+        np.add.at(cnt, S[:, l], 1.0)
+    out = acc / np.maximum(cnt, 1.0)[:, None]
+    return out - out.mean(0)
+
+
+def train(net: LearnedPreconditioner, metric, data, epochs=200, lr=1e-3, batch=4, seed=0, log=None):
+    """Adam over the (mesh, R, E) sets in `data`, `batch` pairs per step. Returns the loss
+    history (one mean per epoch)."""
+    rng = np.random.default_rng(seed)
+    hist = []
+    for ep in range(epochs):
+        losses = []
+        for M, R, E in data:
+            order = rng.permutation(R.shape[0])
+            for s in range(0, len(order), batch):
+                idx = order[s:s + batch]
+                losses.append(net.train_step(M, metric, R[idx], E[idx], lr=lr))
+        hist.append(float(np.mean(losses)))
+        if log is not None:
+            log(ep, hist[-1])
+    return hist
