@@ -357,8 +357,13 @@ def solve_extras(rpb, M, tpm, V):
         tpm.Solve(M, 1.0, B, max_iter=max_iter, tolerance=1e-6, precond=pc, strict=False)
         ms = 1e3 * (time.perf_counter() - t)
         rr = [float(x) for x in tpm.Solver_RelativeResiduals()]
+        info = tpm.SolveInfo(M)
         res[name] = {"ms": ms, "iterations": tpm.Solver_IterationCount(), "rel_residual": rr,
-                     "converged": bool(max(rr) <= 1e-6)}
+                     "converged": bool(max(rr) <= 1e-6), "ms_per_iteration": ms / max(1, info["iterations"]),
+                     "fallback_iteration": info["fallback_iteration"]}
+        if pc == rpb.PRECOND_REFERENCE:
+            res[name].update(h1_factor_seconds=info["factor_seconds"], h1_factor_nnz=info["factor_nnz"],
+                             supernode_levels=info["supernode_levels"])
     return res
 
 

@@ -164,6 +164,19 @@ rpb_status rpb_tpm0_solve(rpb_mesh* m, double q, double p, double alpha, const d
                           double* X, int ldX, int nrhs, int max_iter, double tol, int precond, int* iterations,
                           double* rel_residual);
 
+/* Statistics of the last rpb_tpm0_solve on this mesh (the reference's Solver_IterationCount
+ * plus what the B200 solver adds). */
+typedef struct rpb_solve_info {
+    int     iterations;          /* CG iterations (all columns advance together) */
+    int     restarts;            /* recurrences restarted from the true residual */
+    int     fallback_iteration;  /* iteration at which LEARNED switched to REFERENCE, or -1 */
+    int     supernode_levels;    /* launches per triangular solve of the H1 factor (0: none built) */
+    double  factor_seconds;      /* host H1 assembly + ordering + Cholesky time of the current factor */
+    int64_t factor_nnz;          /* nonzeros of the H1 Cholesky factor */
+} rpb_solve_info;
+
+rpb_status rpb_tpm0_solve_info(const rpb_mesh* m, rpb_solve_info* info);
+
 /* --- learned preconditioner ------------------------------------------------------------ */
 
 /* No counterpart in the reference: a per-cluster MLP (16 -> 64 -> 64 -> 3, GELU, BF16

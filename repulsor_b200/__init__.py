@@ -346,6 +346,14 @@ class TangentPointMetric0:
     def Solver_IterationCount(self):
         return self.iter
 
+    @staticmethod
+    def SolveInfo(M) -> dict:
+        """Statistics of the last Solve on M: iterations, restarts, fallback_iteration (-1: the
+        learned preconditioner never fell back), supernode_levels, factor_seconds, factor_nnz."""
+        info = _capi.SolveInfo()
+        check(_capi.load().rpb_tpm0_solve_info(_as_mesh(M)._h, ctypes.byref(info)), "rpb_tpm0_solve_info")
+        return {name: getattr(info, name) for name, _ in _capi.SolveInfo._fields_}
+
     def Solver_RelativeResiduals(self):
         return self.rel_residuals
 

@@ -48,6 +48,15 @@ class Stats(ctypes.Structure):
                 ("device_bytes", ctypes.c_int64)]
 
 
+class SolveInfo(ctypes.Structure):
+    _fields_ = [("iterations", ctypes.c_int),
+                ("restarts", ctypes.c_int),
+                ("fallback_iteration", ctypes.c_int),
+                ("supernode_levels", ctypes.c_int),
+                ("factor_seconds", ctypes.c_double),
+                ("factor_nnz", ctypes.c_int64)]
+
+
 # name -> (restype, argtypes); every exported symbol of include/repulsor_b200.h
 SIGNATURES = {
     "rpb_default_settings": (ctypes.c_int, [ctypes.POINTER(Settings)]),
@@ -90,6 +99,7 @@ SIGNATURES = {
     "rpb_tpe0_value_noalloc": (ctypes.c_int, [ctypes.c_int, _vp, ctypes.c_int64, _vp, ctypes.c_int64, _vp, _vp, _vp,
                                               ctypes.c_int64, _vp, _vp, _vp, _vp, ctypes.c_double, ctypes.c_double,
                                               _vp, _vp]),
+    "rpb_tpm0_solve_info": (ctypes.c_int, [_vp, ctypes.POINTER(SolveInfo)]),
     "rpb_mlp_param_count": (ctypes.c_int, []),
     "rpb_mlp_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_uint64, ctypes.POINTER(_vp)]),
     "rpb_mlp_destroy": (ctypes.c_int, [_vp]),

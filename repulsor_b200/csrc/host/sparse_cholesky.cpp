@@ -260,4 +260,141 @@ std::string cholesky_factor(const CsrMatrix& A, const std::vector<int>& perm, Ch
     return std::string();
 }
 
+namespace {
+
+// groups supernodes by level (levels[s] in 0..L-1) in ascending supernode order
+void group_levels(const std::vector<int>& levels, const std::vector<int>& sn_begin, std::vector<int>& ptr,
+                  std::vector<int>& sns, std::vector<int>& width)
+{
+    const int nsn = static_cast<int>(levels.size());
+    int L = 0;
+    for (int s = 0; s < nsn; ++s) L = std::max(L, levels[s] + 1);
+    ptr.assign(static_cast<size_t>(L) + 1, 0);
+    width.assign(static_cast<size_t>(L), 0);
+    for (int s = 0; s < nsn; ++s) {
+        ptr[levels[s] + 1]++;
+        width[levels[s]] = std::max(width[levels[s]], sn_begin[s + 1] - sn_begin[s]);
+    }
+    for (int l = 0; l < L; ++l) ptr[l + 1] += ptr[l];
+    sns.resize(static_cast<size_t>(nsn));
+    std::vector<int> pos(ptr.begin(), ptr.end() - 1);
+    for (int s = 0; s < nsn; ++s) sns[pos[levels[s]]++] = s;
+}
+
+}  // namespace
+
+std::string supernodal_schedule(const CholeskyFactor& F, int max_width, SupernodalSchedule& out)
+{
+    const int n = F.n;
+    if (n <= 0) return "empty factor";
+    max_width = std::max(1, max_width);
+    // elimination tree and column counts from the column form (diagonal first)
+    std::vector<int> parent(n, -1), nchild(n, 0), cc(n);
+    for (int j = 0; j < n; ++j) {
+        cc[j] = static_cast<int>(F.upper_rp[j + 1] - F.upper_rp[j]);
+        if (cc[j] > 1) parent[j] = F.upper_ci[F.upper_rp[j] + 1];
+    }
+    for (int j = 0; j < n; ++j)
+        if (parent[j] >= 0) nchild[parent[j]]++;
+    // fundamental supernodes
+    std::vector<int> fb;
+    for (int j = 0; j < n; ++j) {
+        const bool merge = j > 0 && parent[j - 1] == j && nchild[j] == 1 && cc[j - 1] == cc[j] + 1;
+        if (!merge) fb.push_back(j);
+    }
+    fb.push_back(n);
+    const int nf = static_cast<int>(fb.size()) - 1;
+    // single-child chains: supernode s+1 whose only child is s (contiguous in postorder)
+    std::vector<int> fsn_of(n);
+    for (int s = 0; s < nf; ++s)
+        for (int j = fb[s]; j < fb[s + 1]; ++j) fsn_of[j] = s;
+    std::vector<int> fparent(nf, -1), fnchild(nf, 0);
+    for (int s = 0; s < nf; ++s) {
+        const int p = parent[fb[s + 1] - 1];
+        if (p >= 0) {
+            fparent[s] = fsn_of[p];
+            fnchild[fparent[s]]++;
+        }
+    }
+    std::vector<int> sb;
+    for (int s = 0; s < nf; ++s) {
+        const bool chain = s > 0 && fparent[s - 1] == s && fnchild[s] == 1;
+        if (!chain || fb[s + 1] - sb.back() > max_width) sb.push_back(fb[s]);
+    }
+    sb.push_back(n);
+    // split ranges wider than max_width
+    std::vector<int> begin;
+    for (size_t s = 0; s + 1 < sb.size(); ++s)
+        for (int c = sb[s]; c < sb[s + 1]; c += max_width) begin.push_back(c);
+    begin.push_back(n);
+    const int nsn = static_cast<int>(begin.size()) - 1;
+    std::vector<int> sn_of(n);
+    int maxw = 0;
+    for (int s = 0; s < nsn; ++s) {
+        for (int j = begin[s]; j < begin[s + 1]; ++j) sn_of[j] = s;
+        maxw = std::max(maxw, begin[s + 1] - begin[s]);
+    }
+    // levels from the actual dependencies: forward reads columns < c0 of its rows of L,
+    // backward reads rows >= c1 of its columns of L
+    std::vector<int> lf(nsn, 0), lb(nsn, 0);
+    for (int s = 0; s < nsn; ++s)
+        for (int r = begin[s]; r < begin[s + 1]; ++r)
+            for (int64_t k = F.lower_rp[r]; k < F.lower_rp[r + 1]; ++k) {
+                const int j = F.lower_ci[k];
+                if (j < begin[s]) lf[s] = std::max(lf[s], lf[sn_of[j]] + 1);
+            }
+    for (int s = nsn - 1; s >= 0; --s)
+        for (int c = begin[s]; c < begin[s + 1]; ++c)
+            for (int64_t k = F.upper_rp[c]; k < F.upper_rp[c + 1]; ++k) {
+                const int r = F.upper_ci[k];
+                if (r >= begin[s + 1]) lb[s] = std::max(lb[s], lb[sn_of[r]] + 1);
+            }
+    out = SupernodalSchedule();
+    out.n = n;
+    out.nsn = nsn;
+    out.max_width = maxw;
+    out.sn_begin = begin;
+    group_levels(lf, begin, out.fwd_level_ptr, out.fwd_level_sn, out.fwd_level_width);
+    group_levels(lb, begin, out.bwd_level_ptr, out.bwd_level_sn, out.bwd_level_width);
+    // inverses of the dense diagonal blocks
+    out.dinv_off.assign(static_cast<size_t>(nsn) + 1, 0);
+    for (int s = 0; s < nsn; ++s) {
+        const int64_t w = begin[s + 1] - begin[s];
+        out.dinv_off[s + 1] = out.dinv_off[s] + w * (w + 1) / 2;
+    }
+    out.dinv.assign(static_cast<size_t>(out.dinv_off[nsn]), 0.0);
+    out.dinvT.assign(static_cast<size_t>(out.dinv_off[nsn]), 0.0);
+    std::vector<double> D, X;
+    for (int s = 0; s < nsn; ++s) {
+        const int c0 = begin[s], w = begin[s + 1] - c0;
+        D.assign(static_cast<size_t>(w) * w, 0.0);
+        for (int r = 0; r < w; ++r)
+            for (int64_t k = F.lower_rp[c0 + r]; k < F.lower_rp[c0 + r + 1]; ++k) {
+                const int j = F.lower_ci[k];
+                if (j >= c0) D[static_cast<size_t>(r) * w + (j - c0)] = F.lower_val[k];
+            }
+        // X = D^{-1} by forward substitution, one unit column at a time (X lower triangular)
+        X.assign(static_cast<size_t>(w) * w, 0.0);
+        for (int c = 0; c < w; ++c) {
+            for (int r = c; r < w; ++r) {
+                double acc = (r == c) ? 1.0 : 0.0;
+                const double* Dr = &D[static_cast<size_t>(r) * w];
+                for (int k = c; k < r; ++k) acc -= Dr[k] * X[static_cast<size_t>(k) * w + c];
+                if (!(Dr[r] > 0.0)) return "zero pivot in a supernode diagonal block";
+                X[static_cast<size_t>(r) * w + c] = acc / Dr[r];
+            }
+        }
+        double* Li = &out.dinv[static_cast<size_t>(out.dinv_off[s])];
+        double* Ui = &out.dinvT[static_cast<size_t>(out.dinv_off[s])];
+        for (int r = 0; r < w; ++r)
+            for (int c = 0; c <= r; ++c) Li[static_cast<int64_t>(r) * (r + 1) / 2 + c] = X[static_cast<size_t>(r) * w + c];
+        // row c of D^{-T} = column c of D^{-1}: entries r = c .. w-1, starting at c w - c (c-1) / 2
+        for (int c = 0; c < w; ++c) {
+            const int64_t o = static_cast<int64_t>(c) * w - static_cast<int64_t>(c) * (c - 1) / 2;
+            for (int r = c; r < w; ++r) Ui[o + (r - c)] = X[static_cast<size_t>(r) * w + c];
+        }
+    }
+    return std::string();
+}
+
 }  // namespace rpb

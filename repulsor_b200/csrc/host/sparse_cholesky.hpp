@@ -43,4 +43,27 @@ struct CholeskyFactor {
 
 std::string cholesky_factor(const CsrMatrix& A, const std::vector<int>& perm, CholeskyFactor& out);
 
+// Level schedule of the triangular solves by supernodes. Supernodes are contiguous column
+// ranges of L: fundamental supernodes (column j+1 is the only child of column j and their
+// structures nest), then single-child chains merged into one range, then ranges wider
+// than max_width split into consecutive pieces. Within a supernode the dense diagonal
+// block D (explicit zeros included) is inverted once on the host, so a supernode is
+// solved as t = b - (external part of its rows) followed by y = D^{-1} t. A supernode's
+// level is one more than the highest level it reads from: all supernodes of one level
+// are independent, and a level is one kernel launch.
+struct SupernodalSchedule {
+    int n = 0, nsn = 0, max_width = 0;
+    std::vector<int> sn_begin;                 // nsn + 1 column offsets
+    // forward (L) and backward (L^T) schedules: supernodes grouped by level
+    std::vector<int> fwd_level_ptr, fwd_level_sn, fwd_level_width;
+    std::vector<int> bwd_level_ptr, bwd_level_sn, bwd_level_width;
+    std::vector<int64_t> dinv_off;             // nsn + 1: w (w + 1) / 2 entries per supernode
+    std::vector<double> dinv;                  // D^{-1}, packed lower triangle by rows
+    std::vector<double> dinvT;                 // D^{-T}, packed upper triangle by rows
+    int fwd_levels() const { return static_cast<int>(fwd_level_ptr.size()) - 1; }
+    int bwd_levels() const { return static_cast<int>(bwd_level_ptr.size()) - 1; }
+};
+
+std::string supernodal_schedule(const CholeskyFactor& F, int max_width, SupernodalSchedule& out);
+
 }  // namespace rpb

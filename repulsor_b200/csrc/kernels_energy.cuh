@@ -394,27 +394,39 @@ struct PairArgs {
 
 constexpr int PAIR_BLOCK = 256;
 constexpr int PAIR_FLUSH = 8;   // FP32 partial sums are carried into FP64 every 8 pairs
+// Threads per CSR row: a row's nonzeros are strided over LANES consecutive lanes and the
+// partial sums combined by an xor-butterfly of warp shuffles (fixed order, deterministic).
+// Near rows (~60 nonzeros at theta = 0.5) take 4 lanes, far rows (~30) take 2, which puts
+// enough rows in flight to fill all SMs at the benchmark sizes.
+constexpr int NEAR_LANES = 4;
+constexpr int FAR_LANES = 2;
 
-// One thread per row. FAR: rows are clusters of the Far() pattern; otherwise rows are
+constexpr int pair_blocks(int rows, int lanes) { return (rows * lanes + PAIR_BLOCK - 1) / PAIR_BLOCK; }
+
+// LANES threads per row. FAR: rows are clusters of the Far() pattern; otherwise rows are
 // primitives of the Near() pattern. A row accumulates only its own derivative; each
 // unordered pair contributes its energy once (from the row with the smaller index).
-template <bool FAR, int QH, int PH, bool DIFF>
+template <bool FAR, int QH, int PH, bool DIFF, int LANES>
 __global__ void __launch_bounds__(PAIR_BLOCK) k_tp0_pairs(PairArgs A)
 {
+    static_assert(LANES == 1 || LANES == 2 || LANES == 4 || LANES == 8, "LANES must divide a warp");
     using Datum = typename std::conditional<FAR, ClusterDatum, PrimDatum>::type;
     const Datum* base = static_cast<const Datum*>(A.data);
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int slot = t / LANES, sub = t & (LANES - 1);
+    const bool active = slot < A.rows;
     double e_row = 0.0;
-    if (t < A.rows) {
-        const int i = A.order ? A.order[t] : t;
+    double D64[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    int i = 0;
+    if (active) {
+        i = A.order ? A.order[slot] : slot;
         const Datum X = load_datum(base, i);
         const float ax = static_cast<float>(X.a);
-        double D64[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
         PairAcc<float> acc = {};
         float e32 = 0.0f;
         int since_flush = 0;
         const int64_t k0 = A.rp[i], k1 = A.rp[i + 1];
-        for (int64_t k = k0; k < k1; ++k) {
+        for (int64_t k = k0 + sub; k < k1; k += LANES) {
             const int j = __ldg(A.ci + k);
             const Datum Y = load_datum(base, j);
             Proj<float> g;
@@ -462,11 +474,23 @@ __global__ void __launch_bounds__(PAIR_BLOCK) k_tp0_pairs(PairArgs A)
             for (int m = 0; m < 3; ++m) D64[1 + m] += acc.dx[m];
 #pragma unroll
             for (int m = 0; m < 6; ++m) D64[4 + m] += acc.dP[m];
-            double* dst = A.D + 10 * static_cast<int64_t>(i);
-#pragma unroll
-            for (int m = 0; m < 10; ++m) dst[m] = D64[m];
         }
     }
+    // combine the LANES partial sums of a row (every lane of the warp takes part)
+#pragma unroll
+    for (int off = 1; off < LANES; off <<= 1) {
+        e_row += __shfl_xor_sync(0xffffffffu, e_row, off);
+        if (DIFF) {
+#pragma unroll
+            for (int m = 0; m < 10; ++m) D64[m] += __shfl_xor_sync(0xffffffffu, D64[m], off);
+        }
+    }
+    if (DIFF && active && sub == 0) {
+        double* dst = A.D + 10 * static_cast<int64_t>(i);
+#pragma unroll
+        for (int m = 0; m < 10; ++m) dst[m] = D64[m];
+    }
+    if (sub != 0) e_row = 0.0;
     // deterministic energy reduction: per-block partial, last block sums all partials
     __shared__ double sh[PAIR_BLOCK / 32];
     __shared__ bool last;

@@ -144,13 +144,13 @@ template <int QH, int PH>
 static void launch_pairs_t(rpb_mesh* m, const PairArgs& An, const PairArgs& Af, bool diff, cudaEvent_t between)
 {
     if (An.rows > 0) {
-        if (diff) k_tp0_pairs<false, QH, PH, true><<<m->near_blocks, PAIR_BLOCK, 0, m->stream>>>(An);
-        else k_tp0_pairs<false, QH, PH, false><<<m->near_blocks, PAIR_BLOCK, 0, m->stream>>>(An);
+        if (diff) k_tp0_pairs<false, QH, PH, true, NEAR_LANES><<<m->near_blocks, PAIR_BLOCK, 0, m->stream>>>(An);
+        else k_tp0_pairs<false, QH, PH, false, NEAR_LANES><<<m->near_blocks, PAIR_BLOCK, 0, m->stream>>>(An);
     }
     if (between) cudaEventRecord(between, m->stream);
     if (Af.rows > 0) {
-        if (diff) k_tp0_pairs<true, QH, PH, true><<<m->far_blocks, PAIR_BLOCK, 0, m->stream>>>(Af);
-        else k_tp0_pairs<true, QH, PH, false><<<m->far_blocks, PAIR_BLOCK, 0, m->stream>>>(Af);
+        if (diff) k_tp0_pairs<true, QH, PH, true, FAR_LANES><<<m->far_blocks, PAIR_BLOCK, 0, m->stream>>>(Af);
+        else k_tp0_pairs<true, QH, PH, false, FAR_LANES><<<m->far_blocks, PAIR_BLOCK, 0, m->stream>>>(Af);
     }
 }
 
@@ -351,8 +351,8 @@ rpb_status rpb_mesh_create(int dom_dim, int amb_dim, const double* Vh, int64_t n
         set_error("device allocation failed");
         return fail(RPB_ENOMEM);
     }
-    m->near_blocks = (m->N + PAIR_BLOCK - 1) / PAIR_BLOCK;
-    m->far_blocks = (m->NC + PAIR_BLOCK - 1) / PAIR_BLOCK;
+    m->near_blocks = pair_blocks(m->N, NEAR_LANES);
+    m->far_blocks = pair_blocks(m->NC, FAR_LANES);
     {
         // rows of each 256-row chunk sorted by decreasing length: threads of a warp see
         // similar trip counts while the chunk keeps the tree-order locality of its columns

@@ -166,14 +166,20 @@ __global__ void __launch_bounds__(256) k_weight_grad(int n, const float* G, int 
     for (int t = 0; t < OUT_PER_THREAD; ++t) acc[t] = 0.0f;
     const int total = P * (Q + 1);
     for (int base = n0; base < n1; base += 32) {
-        for (int e = threadIdx.x; e < 32 * 64; e += blockDim.x) {
-            const int r = e / 64, col = e % 64, row = base + r;
-            sg[r][col] = (row < n1 && col < P) ? G[static_cast<int64_t>(P) * row + col] : 0.0f;
-            float x = (row < n1 && col < Q) ? X[static_cast<int64_t>(Q) * row + col] : 0.0f;
-            if (gelu_x && row < n1 && col < Q) x = gelu(x);
+        // columns 0..Q-1: activations, column Q: 1 (the bias), beyond: 0
+        for (int e = threadIdx.x; e < 32 * 65; e += blockDim.x) {
+            const int r = e / 65, col = e % 65, row = base + r;
+            const bool valid = row < n1;
+            if (col < 64) sg[r][col] = (valid && col < P) ? G[static_cast<int64_t>(P) * row + col] : 0.0f;
+            float x = 0.0f;
+            if (valid && col < Q) {
+                x = X[static_cast<int64_t>(Q) * row + col];
+                if (gelu_x) x = gelu(x);
+            } else if (valid && col == Q) {
+                x = 1.0f;
+            }
             sx[r][col] = x;
         }
-        if (threadIdx.x < 32) sx[threadIdx.x][Q] = (base + threadIdx.x < n1) ? 1.0f : 0.0f;  // bias column
         __syncthreads();
 #pragma unroll
         for (int t = 0; t < OUT_PER_THREAD; ++t) {

@@ -31,7 +31,8 @@ namespace {
 constexpr int kMaxSimplices = 40960;
 constexpr int kMaxClusters = 2 * kMaxSimplices - 1;
 constexpr int kMaxBlocksN = (kMaxSimplices + SCAN_BLOCK - 1) / SCAN_BLOCK;
-constexpr int kMaxBlocksC = (kMaxClusters + PAIR_BLOCK - 1) / PAIR_BLOCK;
+constexpr int kMaxPairBlocksN = pair_blocks(kMaxSimplices, NEAR_LANES);
+constexpr int kMaxPairBlocksC = pair_blocks(kMaxClusters, FAR_LANES);
 
 // byte offsets inside the scratch array (each region 256-byte aligned)
 constexpr size_t align256(size_t x) { return (x + 255) & ~static_cast<size_t>(255); }
@@ -40,7 +41,7 @@ constexpr size_t kOffClus = align256(kOffPrim + sizeof(PrimDatum) * kMaxSimplice
 constexpr size_t kOffLocal = align256(kOffClus + sizeof(ClusterDatum) * kMaxClusters);
 constexpr size_t kOffBlocks = align256(kOffLocal + sizeof(double) * 10 * kMaxSimplices);
 constexpr size_t kOffPartials = align256(kOffBlocks + sizeof(double) * 10 * (kMaxBlocksN + 1));
-constexpr size_t kOffEnergy = align256(kOffPartials + sizeof(double) * (kMaxBlocksN + kMaxBlocksC));
+constexpr size_t kOffEnergy = align256(kOffPartials + sizeof(double) * (kMaxPairBlocksN + kMaxPairBlocksC));
 constexpr size_t kOffDone = align256(kOffEnergy + sizeof(double) * 2);
 constexpr size_t kScratchBytes = align256(kOffDone + sizeof(unsigned) * 2);
 
@@ -75,8 +76,8 @@ rpb_status scratch_on_current_device(unsigned char** out)
 template <int QH, int PH>
 void launch_energy_pairs(const PairArgs& An, const PairArgs& Af, int nb_near, int nb_far, cudaStream_t s)
 {
-    if (An.rows > 0) k_tp0_pairs<false, QH, PH, false><<<nb_near, PAIR_BLOCK, 0, s>>>(An);
-    if (Af.rows > 0) k_tp0_pairs<true, QH, PH, false><<<nb_far, PAIR_BLOCK, 0, s>>>(Af);
+    if (An.rows > 0) k_tp0_pairs<false, QH, PH, false, NEAR_LANES><<<nb_near, PAIR_BLOCK, 0, s>>>(An);
+    if (Af.rows > 0) k_tp0_pairs<true, QH, PH, false, FAR_LANES><<<nb_far, PAIR_BLOCK, 0, s>>>(Af);
 }
 
 }  // namespace
@@ -128,7 +129,7 @@ extern "C" rpb_status rpb_tpe0_value_noalloc(int dom_dim, const double* V, int64
     k_scan_rows<10><<<1, SCAN_BLOCK, 0, s>>>(blocks, nb);
     k_cluster_moments<<<(NC + 255) / 256, 256, 0, s>>>(g);
     const TPExp ex = make_exp(dom_dim, q, p);
-    const int nb_near = (N + PAIR_BLOCK - 1) / PAIR_BLOCK, nb_far = (NC + PAIR_BLOCK - 1) / PAIR_BLOCK;
+    const int nb_near = pair_blocks(N, NEAR_LANES), nb_far = pair_blocks(NC, FAR_LANES);
     PairArgs An, Af;
     An.dom = Af.dom = dom_dim;
     An.ex = Af.ex = ex;

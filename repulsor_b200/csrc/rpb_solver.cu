@@ -7,8 +7,8 @@
 // per right-hand-side column, with
 //   RPB_PRECOND_NONE       identity,
 //   RPB_PRECOND_REFERENCE  H1^{-1} L_{2-s} H1^{-1}: host Cholesky of the H1 metric (nested-
-//                          dissection order from the cluster tree), GPU triangular solves,
-//                          GPU pseudo-Laplacian,
+//                          dissection order from the cluster tree), GPU triangular solves
+//                          level-scheduled by supernodes, GPU pseudo-Laplacian,
 //   RPB_PRECOND_LEARNED    per-cluster MLP (rpb_learned.cu) inside flexible CG, falling back
 //                          to REFERENCE when the flexible iteration stalls.
 // Convergence is decided on the true relative residual ||B - A X|| / ||B|| per column.
@@ -35,93 +35,91 @@ namespace rpb {
     } while (0)
 
 // ------------------------------------------------------------------------------------------
-// Sync-free sparse triangular solves with 3 right-hand sides. Warps take rows in
-// dependency order from a global ticket; a row waits (bounded) on the ready flags of
-// the rows it depends on, which were taken earlier by running warps. Flags carry the
-// launch's epoch so they never need clearing.
+// Level-scheduled supernodal triangular solves with 3 right-hand sides. One launch per
+// level of the supernode schedule (host/sparse_cholesky.cpp), one CTA per supernode:
+//   phase 1 (warp per row):  t_r = b_r - sum over the row's entries outside the supernode
+//                            (all written by earlier levels, i.e. earlier launches),
+//   phase 2 (warp per row):  y = D^{-1} t with the inverse of the dense diagonal block.
+// Forward: rows of L, external columns < c0, D^{-1} packed lower. Backward: rows of L^T,
+// external columns >= c1, D^{-T} packed upper. No inter-CTA waits of any kind.
 // ------------------------------------------------------------------------------------------
-__device__ __forceinline__ int ld_acquire(const int* p)
-{
-    int v;
-    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
-
-__device__ __forceinline__ void st_release(int* p, int v)
-{
-    asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
-
-constexpr long long kSpinLimit = 1ll << 24;   // with the 512 ns backoff cap: a few seconds at most
-
-struct TrsvArgs {
-    int n;
+struct SnArgs {
+    const int* level_sn;      // supernodes of this level
+    const int* sn_begin;
     const int64_t* rp;
     const int* ci;
     const double* val;
+    const int64_t* dinv_off;
+    const double* dinv;
     const double* b;          // right-hand side, n x 3
     const int* perm_in;       // if set, row i reads b[perm_in[i]]
     double* y;                // solution in factor order, n x 3
     double* out;              // if set, out[perm_out[i]] = y_i
     const int* perm_out;
-    int* flags;
-    int epoch;
-    unsigned* ticket;
-    int* err;
 };
 
-// LOWER: rows ascending, diagonal last in each row. UPPER: rows descending, diagonal first.
+constexpr int SN_BLOCK = 256;
+// widest supernode (3 x 8 bytes of shared memory per row: 24 KB at 1024)
+constexpr int kMaxSupernodeWidth = 1024;
+
 template <bool LOWER>
-__global__ void __launch_bounds__(256) k_trsv(TrsvArgs A)
+__global__ void __launch_bounds__(SN_BLOCK) k_sn_solve(SnArgs A)
 {
-    const int lane = threadIdx.x & 31;
-    for (;;) {
-        int t = 0;
-        if (lane == 0) t = static_cast<int>(atomicAdd(A.ticket, 1u));
-        t = __shfl_sync(0xffffffffu, t, 0);
-        if (t >= A.n) return;
-        const int row = LOWER ? t : A.n - 1 - t;
-        const int64_t k0 = A.rp[row], k1 = A.rp[row + 1];
-        const int64_t dpos = LOWER ? k1 - 1 : k0;
-        const int64_t ob = LOWER ? k0 : k0 + 1, oe = LOWER ? k1 - 1 : k1;
+    extern __shared__ double t[];   // w x 3
+    const int s = A.level_sn[blockIdx.x];
+    const int c0 = A.sn_begin[s], c1 = A.sn_begin[s + 1], w = c1 - c0;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    for (int r = warp; r < w; r += nw) {
+        const int row = c0 + r;
         double s0 = 0, s1 = 0, s2 = 0;
-        for (int64_t k = ob + lane; k < oe; k += 32) {
+        for (int64_t k = A.rp[row] + lane; k < A.rp[row + 1]; k += 32) {
             const int j = A.ci[k];
-            long long it = 0;
-            unsigned backoff = 32;
-            while (ld_acquire(A.flags + j) != A.epoch) {
-                if (++it > kSpinLimit) {
-                    atomicExch(A.err, 1);
-                    break;
-                }
-                __nanosleep(backoff);
-                backoff = backoff < 256 ? 2 * backoff : 256;
+            if (LOWER ? (j < c0) : (j >= c1)) {
+                const double v = A.val[k];
+                s0 += v * A.y[3 * static_cast<int64_t>(j) + 0];
+                s1 += v * A.y[3 * static_cast<int64_t>(j) + 1];
+                s2 += v * A.y[3 * static_cast<int64_t>(j) + 2];
             }
-            const double v = A.val[k];
-            s0 += v * __ldcg(A.y + 3 * static_cast<int64_t>(j) + 0);
-            s1 += v * __ldcg(A.y + 3 * static_cast<int64_t>(j) + 1);
-            s2 += v * __ldcg(A.y + 3 * static_cast<int64_t>(j) + 2);
         }
         s0 = warp_sum_f64(s0);
         s1 = warp_sum_f64(s1);
         s2 = warp_sum_f64(s2);
         if (lane == 0) {
             const int src = A.perm_in ? A.perm_in[row] : row;
-            const double d = A.val[dpos];
-            const double y0 = (A.b[3 * static_cast<int64_t>(src) + 0] - s0) / d;
-            const double y1 = (A.b[3 * static_cast<int64_t>(src) + 1] - s1) / d;
-            const double y2 = (A.b[3 * static_cast<int64_t>(src) + 2] - s2) / d;
-            __stcg(A.y + 3 * static_cast<int64_t>(row) + 0, y0);
-            __stcg(A.y + 3 * static_cast<int64_t>(row) + 1, y1);
-            __stcg(A.y + 3 * static_cast<int64_t>(row) + 2, y2);
+            t[3 * r + 0] = A.b[3 * static_cast<int64_t>(src) + 0] - s0;
+            t[3 * r + 1] = A.b[3 * static_cast<int64_t>(src) + 1] - s1;
+            t[3 * r + 2] = A.b[3 * static_cast<int64_t>(src) + 2] - s2;
+        }
+    }
+    __syncthreads();
+    const double* D = A.dinv + A.dinv_off[s];
+    for (int r = warp; r < w; r += nw) {
+        // LOWER: row r of D^{-1} holds columns 0..r; UPPER: row r of D^{-T} holds columns r..w-1
+        const int64_t o = LOWER ? static_cast<int64_t>(r) * (r + 1) / 2
+                                : static_cast<int64_t>(r) * w - static_cast<int64_t>(r) * (r - 1) / 2;
+        const int cb = LOWER ? 0 : r, len = LOWER ? r + 1 : w - r;
+        double s0 = 0, s1 = 0, s2 = 0;
+        for (int c = lane; c < len; c += 32) {
+            const double d = D[o + c];
+            const int tc = 3 * (cb + c);
+            s0 += d * t[tc + 0];
+            s1 += d * t[tc + 1];
+            s2 += d * t[tc + 2];
+        }
+        s0 = warp_sum_f64(s0);
+        s1 = warp_sum_f64(s1);
+        s2 = warp_sum_f64(s2);
+        if (lane == 0) {
+            const int row = c0 + r;
+            A.y[3 * static_cast<int64_t>(row) + 0] = s0;
+            A.y[3 * static_cast<int64_t>(row) + 1] = s1;
+            A.y[3 * static_cast<int64_t>(row) + 2] = s2;
             if (A.out) {
                 const int dst = A.perm_out[row];
-                A.out[3 * static_cast<int64_t>(dst) + 0] = y0;
-                A.out[3 * static_cast<int64_t>(dst) + 1] = y1;
-                A.out[3 * static_cast<int64_t>(dst) + 2] = y2;
+                A.out[3 * static_cast<int64_t>(dst) + 0] = s0;
+                A.out[3 * static_cast<int64_t>(dst) + 1] = s1;
+                A.out[3 * static_cast<int64_t>(dst) + 2] = s2;
             }
-            __threadfence();
-            st_release(A.flags + row, A.epoch);
         }
     }
 }
@@ -241,9 +239,7 @@ static rpb_status ensure_solver(rpb_mesh* m)
         RPB_CUDA(s.scal.alloc(S_COUNT));
         RPB_CUDA(s.partials.alloc(6 * 1024));
         RPB_CUDA(s.done.alloc(1));
-        RPB_CUDA(s.err.alloc(1));
         RPB_CUDA(cudaMemsetAsync(s.done.ptr, 0, s.done.bytes(), m->stream));
-        RPB_CUDA(cudaMemsetAsync(s.err.ptr, 0, s.err.bytes(), m->stream));
         RPB_CUDA(cudaMallocHost(reinterpret_cast<void**>(&s.host_scal), sizeof(double) * S_COUNT));
     }
     return RPB_OK;
@@ -277,54 +273,66 @@ static rpb_status ensure_h1(rpb_mesh* m)
     if (!err.empty()) { set_error(err); return RPB_EINVAL; }
     s.factor_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     s.factor_nnz = F.nnz();
+    SupernodalSchedule SS;
+    const std::string serr = supernodal_schedule(F, kMaxSupernodeWidth, SS);
+    if (!serr.empty()) { set_error(serr); return RPB_EINVAL; }
+    s.sn_levels_fwd = SS.fwd_levels();
+    s.sn_levels_bwd = SS.bwd_levels();
+    s.fwd_level_ptr = SS.fwd_level_ptr;
+    s.bwd_level_ptr = SS.bwd_level_ptr;
+    s.fwd_level_width = SS.fwd_level_width;
+    s.bwd_level_width = SS.bwd_level_width;
     cudaStream_t st = m->stream;
-    RPB_CUDA(s.lo_rp.alloc(F.lower_rp.size()));
-    RPB_CUDA(s.lo_ci.alloc(F.lower_ci.size()));
-    RPB_CUDA(s.lo_val.alloc(F.lower_val.size()));
-    RPB_CUDA(s.up_rp.alloc(F.upper_rp.size()));
-    RPB_CUDA(s.up_ci.alloc(F.upper_ci.size()));
-    RPB_CUDA(s.up_val.alloc(F.upper_val.size()));
-    RPB_CUDA(s.perm.alloc(F.perm.size()));
-    RPB_CUDA(s.flags.alloc(m->nV));
-    RPB_CUDA(s.ticket.alloc(4));
+    auto up = [st](auto& dst, const auto& src) -> cudaError_t {
+        cudaError_t e = dst.alloc(src.size());
+        if (e != cudaSuccess) return e;
+        return cudaMemcpyAsync(dst.ptr, src.data(), dst.bytes(), cudaMemcpyHostToDevice, st);
+    };
+    RPB_CUDA(up(s.lo_rp, F.lower_rp));
+    RPB_CUDA(up(s.lo_ci, F.lower_ci));
+    RPB_CUDA(up(s.lo_val, F.lower_val));
+    RPB_CUDA(up(s.up_rp, F.upper_rp));
+    RPB_CUDA(up(s.up_ci, F.upper_ci));
+    RPB_CUDA(up(s.up_val, F.upper_val));
+    RPB_CUDA(up(s.perm, F.perm));
+    RPB_CUDA(up(s.sn_begin, SS.sn_begin));
+    RPB_CUDA(up(s.fwd_level_sn, SS.fwd_level_sn));
+    RPB_CUDA(up(s.bwd_level_sn, SS.bwd_level_sn));
+    RPB_CUDA(up(s.dinv_off, SS.dinv_off));
+    RPB_CUDA(up(s.dinv, SS.dinv));
+    RPB_CUDA(up(s.dinvT, SS.dinvT));
     RPB_CUDA(s.tri.alloc(3 * static_cast<size_t>(m->nV)));
     RPB_CUDA(s.tmp.alloc(3 * static_cast<size_t>(m->nV)));
-    RPB_CUDA(cudaMemcpyAsync(s.lo_rp.ptr, F.lower_rp.data(), s.lo_rp.bytes(), cudaMemcpyHostToDevice, st));
-    RPB_CUDA(cudaMemcpyAsync(s.lo_ci.ptr, F.lower_ci.data(), s.lo_ci.bytes(), cudaMemcpyHostToDevice, st));
-    RPB_CUDA(cudaMemcpyAsync(s.lo_val.ptr, F.lower_val.data(), s.lo_val.bytes(), cudaMemcpyHostToDevice, st));
-    RPB_CUDA(cudaMemcpyAsync(s.up_rp.ptr, F.upper_rp.data(), s.up_rp.bytes(), cudaMemcpyHostToDevice, st));
-    RPB_CUDA(cudaMemcpyAsync(s.up_ci.ptr, F.upper_ci.data(), s.up_ci.bytes(), cudaMemcpyHostToDevice, st));
-    RPB_CUDA(cudaMemcpyAsync(s.up_val.ptr, F.upper_val.data(), s.up_val.bytes(), cudaMemcpyHostToDevice, st));
-    RPB_CUDA(cudaMemcpyAsync(s.perm.ptr, F.perm.data(), s.perm.bytes(), cudaMemcpyHostToDevice, st));
-    RPB_CUDA(cudaMemsetAsync(s.flags.ptr, 0, s.flags.bytes(), st));
     RPB_CUDA(cudaStreamSynchronize(st));
-    s.epoch = 0;
     s.h1_version = m->geometry_version;
     return RPB_OK;
 }
 
-// out = H1^{-1} b (b, out: n x 3 contiguous, device)
+// out = H1^{-1} b (b, out: n x 3 contiguous, device): forward levels on L, backward
+// levels on L^T, one launch per level
 static rpb_status h1_solve(rpb_mesh* m, const double* b, double* out)
 {
     Solver& s = *m->solver;
-    const int n = m->nV;
-    int dev = 0, sms = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int blocks = std::min((n + 7) / 8, sms * 2);
-    RPB_CUDA(cudaMemsetAsync(s.ticket.ptr, 0, s.ticket.bytes(), m->stream));
-    TrsvArgs A;
-    A.n = n;
-    A.rp = s.lo_rp.ptr; A.ci = s.lo_ci.ptr; A.val = s.lo_val.ptr;
+    SnArgs A;
+    A.sn_begin = s.sn_begin.ptr; A.dinv_off = s.dinv_off.ptr;
+    A.rp = s.lo_rp.ptr; A.ci = s.lo_ci.ptr; A.val = s.lo_val.ptr; A.dinv = s.dinv.ptr;
     A.b = b; A.perm_in = s.perm.ptr; A.y = s.tri.ptr; A.out = nullptr; A.perm_out = nullptr;
-    A.flags = s.flags.ptr; A.epoch = ++s.epoch; A.ticket = s.ticket.ptr; A.err = s.err.ptr;
-    k_trsv<true><<<blocks, 256, 0, m->stream>>>(A);
+    for (int l = 0; l < s.sn_levels_fwd; ++l) {
+        A.level_sn = s.fwd_level_sn.ptr + s.fwd_level_ptr[l];
+        const int nsn = s.fwd_level_ptr[l + 1] - s.fwd_level_ptr[l];
+        const size_t smem = 3 * sizeof(double) * static_cast<size_t>(s.fwd_level_width[l]);
+        k_sn_solve<true><<<nsn, SN_BLOCK, smem, m->stream>>>(A);
+    }
     RPB_CUDA(cudaGetLastError());
-    TrsvArgs U = A;
-    U.rp = s.up_rp.ptr; U.ci = s.up_ci.ptr; U.val = s.up_val.ptr;
+    SnArgs U = A;
+    U.rp = s.up_rp.ptr; U.ci = s.up_ci.ptr; U.val = s.up_val.ptr; U.dinv = s.dinvT.ptr;
     U.b = s.tri.ptr; U.perm_in = nullptr; U.y = s.tmp.ptr; U.out = out; U.perm_out = s.perm.ptr;
-    U.epoch = ++s.epoch; U.ticket = s.ticket.ptr + 1;
-    k_trsv<false><<<blocks, 256, 0, m->stream>>>(U);
+    for (int l = 0; l < s.sn_levels_bwd; ++l) {
+        U.level_sn = s.bwd_level_sn.ptr + s.bwd_level_ptr[l];
+        const int nsn = s.bwd_level_ptr[l + 1] - s.bwd_level_ptr[l];
+        const size_t smem = 3 * sizeof(double) * static_cast<size_t>(s.bwd_level_width[l]);
+        k_sn_solve<false><<<nsn, SN_BLOCK, smem, m->stream>>>(U);
+    }
     RPB_CUDA(cudaGetLastError());
     return RPB_OK;
 }
@@ -348,13 +356,6 @@ static rpb_status read_scalars(rpb_mesh* m)
     Solver& s = *m->solver;
     RPB_CUDA(cudaMemcpyAsync(s.host_scal, s.scal.ptr, sizeof(double) * S_COUNT, cudaMemcpyDeviceToHost, m->stream));
     RPB_CUDA(cudaStreamSynchronize(m->stream));
-    int e = 0;
-    RPB_CUDA(cudaMemcpy(&e, s.err.ptr, sizeof(int), cudaMemcpyDeviceToHost));
-    if (e) {
-        cudaMemset(s.err.ptr, 0, sizeof(int));
-        set_error("a triangular-solve dependency wait exceeded its bound");
-        return RPB_ETIMEOUT;
-    }
     return RPB_OK;
 }
 
@@ -392,7 +393,7 @@ static rpb_status cg_solve(rpb_mesh* m, double q, double p, const double* B, int
     const int eb = (n + 255) / 256;
     const bool flexible = (precond == RPB_PRECOND_LEARNED);
     // iterations without a 10% drop of the best residual that count as a stall
-    constexpr int kStallWindow = 100;
+    constexpr int kStallWindow = 400;
     int kind = precond;
 
     // ||B|| per column
@@ -406,6 +407,7 @@ static rpb_status cg_solve(rpb_mesh* m, double q, double p, const double* B, int
     int it = 0;
     double rel[3] = {0, 0, 0};
     int restarts = 0;
+    s.last_fallback_iteration = -1;
     double best[3] = {1e300, 1e300, 1e300};
     int since_best = 0;
     bool stalled_flag = false;
@@ -423,7 +425,10 @@ static rpb_status cg_solve(rpb_mesh* m, double q, double p, const double* B, int
             if (active[c] != 0.0) done = false;
         }
         if (done || it >= max_iter) break;
-        if (stalled_flag && kind == RPB_PRECOND_LEARNED) kind = RPB_PRECOND_REFERENCE;  // fallback on stall
+        if (stalled_flag && kind == RPB_PRECOND_LEARNED) {
+            kind = RPB_PRECOND_REFERENCE;  // fallback on stall
+            s.last_fallback_iteration = it;
+        }
         stalled_flag = false;
         ++restarts;
         RPB_CUDA(cudaMemcpyAsync(S + S_ACTIVE, active, sizeof(active), cudaMemcpyHostToDevice, stream));
@@ -463,6 +468,8 @@ static rpb_status cg_solve(rpb_mesh* m, double q, double p, const double* B, int
         }
         if (restarts > 20) break;
     }
+    s.last_iterations = it;
+    s.last_restarts = restarts;
     if (iters_out) *iters_out = it;
     if (relres_out)
         for (int c = 0; c < 3; ++c) relres_out[c] = rel[c];
@@ -519,9 +526,6 @@ rpb_status rpb_tpm0_precondition(rpb_mesh* m, double q, double p, double alpha, 
     RPB_CUDA(cudaMemcpy2DAsync(Y, ldY * sizeof(double), m->Yb.ptr, 3 * sizeof(double), 3 * sizeof(double), n,
                                cudaMemcpyDeviceToHost, s));
     RPB_CUDA(cudaStreamSynchronize(s));
-    int e = 0;
-    RPB_CUDA(cudaMemcpy(&e, m->solver->err.ptr, sizeof(int), cudaMemcpyDeviceToHost));
-    if (e) { cudaMemset(m->solver->err.ptr, 0, sizeof(int)); set_error("triangular-solve wait bound exceeded"); return RPB_ETIMEOUT; }
     return RPB_OK;
 }
 
@@ -563,6 +567,18 @@ rpb_status rpb_tpm0_solve(rpb_mesh* m, double q, double p, double alpha, const d
                                cudaMemcpyDeviceToHost, s));
     RPB_CUDA(cudaStreamSynchronize(s));
     return cs;
+}
+
+rpb_status rpb_tpm0_solve_info(const rpb_mesh* m, rpb_solve_info* info)
+{
+    if (!m || !info) { set_error("null argument"); return RPB_EINVAL; }
+    info->iterations = m->solver ? m->solver->last_iterations : 0;
+    info->restarts = m->solver ? m->solver->last_restarts : 0;
+    info->fallback_iteration = m->solver ? m->solver->last_fallback_iteration : -1;
+    info->factor_seconds = m->solver ? m->solver->factor_seconds : 0.0;
+    info->factor_nnz = m->solver ? m->solver->factor_nnz : 0;
+    info->supernode_levels = m->solver ? m->solver->sn_levels_fwd : 0;
+    return RPB_OK;
 }
 
 }  // extern "C"

@@ -17,18 +17,19 @@ struct Solver {
     DevBuf<double> scal;          // per-column CG scalars
     DevBuf<double> partials;      // block partials of the dot products
     DevBuf<unsigned> done;
-    DevBuf<int> err;              // set when a bounded device wait gives up
     double* host_scal = nullptr;  // pinned readback of the scalars
-    // H1 Cholesky factor (reference preconditioner)
+    // H1 Cholesky factor (reference preconditioner) and its supernodal level schedule
     int64_t h1_version = -1;
     std::vector<int> nd_perm;
-    DevBuf<int64_t> lo_rp, up_rp;
-    DevBuf<int> lo_ci, up_ci, perm, flags;
-    DevBuf<double> lo_val, up_val, tri, tmp;
-    DevBuf<unsigned> ticket;
-    int epoch = 0;
+    DevBuf<int64_t> lo_rp, up_rp, dinv_off;
+    DevBuf<int> lo_ci, up_ci, perm, sn_begin, fwd_level_sn, bwd_level_sn;
+    DevBuf<double> lo_val, up_val, dinv, dinvT, tri, tmp;
+    int sn_levels_fwd = 0, sn_levels_bwd = 0;
+    std::vector<int> fwd_level_ptr, bwd_level_ptr, fwd_level_width, bwd_level_width;
     double factor_seconds = 0;
     int64_t factor_nnz = 0;
+    // statistics of the last Solve
+    int last_iterations = 0, last_restarts = 0, last_fallback_iteration = -1;
 };
 
 }  // namespace rpb

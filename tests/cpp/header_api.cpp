@@ -1,0 +1,63 @@
+// Drives the header-only C++20 mirror (include/repulsor_b200/Repulsor.hpp) the way
+// Repulsor's own drivers use the reference API (Example/main.cpp): build a mesh, evaluate
+// TangentPointEnergy0 Value/Differential, multiply the metric, solve. Input: a mesh file
+// "nV nS dom" followed by the coordinates and simplices; output: energy, |dE|_max,
+// sum(A dE), iterations and the relative residual, one per line.
+#include <cmath>
+#include <cstdio>
+#include <fstream>
+#include <vector>
+
+#include "repulsor_b200/Repulsor.hpp"
+
+namespace Repulsor = Repulsor_B200;
+
+template <int DOM>
+int run(const std::vector<double>& V, const std::vector<int>& S, int nV, int nS)
+{
+    using Mesh_T = Repulsor::SimplicialMesh<DOM, 3>;
+    Mesh_T M(V.data(), nV, S.data(), nS, 4);
+    M.block_cluster_tree_settings.far_field_separation_parameter = 0.5;
+    M.adaptivity_settings.theta = 10.0;
+    Repulsor::TangentPointEnergy0<Mesh_T> tpe(6.0, 12.0);
+    Repulsor::TangentPointMetric0<Mesh_T> tpm(6.0, 12.0);
+    const double E = tpe.Value(M);
+    const std::vector<double>& D = tpe.Differential(M);
+    if (D.size() != static_cast<size_t>(3 * nV)) return 2;
+    double dmax = 0;
+    for (double d : D) dmax = std::fmax(dmax, std::fabs(d));
+    std::vector<double> Y(3 * nV, 0.0), X(3 * nV, 0.0);
+    tpm.MultiplyMetric(M, 1.0, D.data(), 3, 0.0, Y.data(), 3, 3);
+    double ysum = 0;
+    for (double y : Y) ysum += y;
+    // right-hand side: the differential without its column means (the metric's kernel)
+    std::vector<double> B(D);
+    for (int k = 0; k < 3; ++k) {
+        double m = 0;
+        for (int v = 0; v < nV; ++v) m += B[3 * v + k];
+        for (int v = 0; v < nV; ++v) B[3 * v + k] -= m / nV;
+    }
+    tpm.SetPreconditioner(RPB_PRECOND_NONE);
+    tpm.Solve(M, 1.0, B.data(), 3, 0.0, X.data(), 3, 3, 20000, 1e-6);
+    const std::vector<double> rr = tpm.Solver_RelativeResiduals();
+    double rmax = 0;
+    for (double r : rr) rmax = std::fmax(rmax, r);
+    std::printf("%.17g\n%.17g\n%.17g\n%d\n%.6g\n", E, dmax, ysum, static_cast<int>(tpm.Solver_IterationCount()), rmax);
+    // errors follow the reference: print and do nothing
+    tpm.MultiplyMetric(M, 1.0, D.data(), 3, 0.0, Y.data(), 3, 2);
+    return 0;
+}
+
+int main(int argc, char** argv)
+{
+    if (argc < 2) return 1;
+    std::ifstream in(argv[1]);
+    int nV = 0, nS = 0, dom = 0;
+    in >> nV >> nS >> dom;
+    std::vector<double> V(3 * nV);
+    std::vector<int> S((dom + 1) * nS);
+    for (double& x : V) in >> x;
+    for (int& s : S) in >> s;
+    if (!in) return 1;
+    return dom == 1 ? run<1>(V, S, nV, nS) : run<2>(V, S, nV, nS);
+}
