@@ -114,6 +114,13 @@ rpb_status rpb_tree_host_arrays(const rpb_host_tree* t, int* perm, int* C_begin,
 rpb_status rpb_tree_host_pattern(const rpb_host_tree* t, int which, int64_t* rowptr, int* colidx);
 rpb_status rpb_tree_host_destroy(rpb_host_tree* t);
 
+/* The obstacle lists of rpb_mesh_load_obstacle on the host only: counts[4] = sizes of
+ * [near, far, very near, intersecting]; rowptr/colidx (may be NULL) receive list `which`.
+ * V, S and VO, SO are the coordinates and simplices the two trees were built from. */
+rpb_status rpb_tree_host_obstacle_pattern(const rpb_host_tree* mesh, const double* V, const int* S,
+                                          const rpb_host_tree* obstacle, const double* VO, const int* SO, int which,
+                                          int64_t* counts, int64_t* rowptr, int* colidx);
+
 /* SimplicialMesh::H1Solver().Solve on the host (src/SimplicialMesh/H1Metric.hpp:208-257):
  * X = H1^{-1} B with H1 = stiffness + mass of the given coordinates, factorized by the
  * same nested-dissection-ordered sparse Cholesky the GPU preconditioner uploads.
@@ -176,6 +183,34 @@ typedef struct rpb_solve_info {
 } rpb_solve_info;
 
 rpb_status rpb_tpm0_solve_info(const rpb_mesh* m, rpb_solve_info* info);
+
+/* --- obstacle energy --------------------------------------------------------------------- */
+
+/* SimplicialMesh::LoadObstacle (src/SimplicialMesh.hpp:697-719): m takes ownership of the
+ * obstacle mesh (destroyed with m or when another obstacle is loaded; the caller must not
+ * destroy it). Builds the non-symmetric block cluster tree of (m's tree, the obstacle's
+ * tree) (GetObstacleBlockClusterTree, src/SimplicialMesh.hpp:741-756) once, from the
+ * coordinates both trees were built from. Both meshes must have the same domain
+ * dimension and live on the same device. */
+rpb_status rpb_mesh_load_obstacle(rpb_mesh* m, rpb_mesh* obstacle);
+
+/* Sizes [near, far, very near, intersecting] of the obstacle lists (rows are m's
+ * primitives, or clusters for far; columns the obstacle's). */
+rpb_status rpb_mesh_obstacle_stats(const rpb_mesh* m, int64_t* counts);
+
+/* One obstacle list as CSR (rowptr: rows + 1, colidx: nnz); which as for rpb_mesh_pattern. */
+rpb_status rpb_mesh_obstacle_pattern(const rpb_mesh* m, int which, int64_t* rowptr, int* colidx);
+
+/* TangentPointObstacleEnergy (src/Energies/TangentPointObstacleEnergy.hpp:62-96): the
+ * tangent-point energy of every (mesh, obstacle) pair with the symmetry factor 1/2 of a
+ * non-symmetric block cluster tree; 0 without an obstacle. The differential (Y = alpha dE +
+ * beta Y) is taken with respect to m's vertices only. */
+rpb_status rpb_tpoe_value(rpb_mesh* m, double q, double p, double* energy);
+rpb_status rpb_tpoe_differential(rpb_mesh* m, double q, double p, double alpha, double beta, double* Y, int ldY,
+                                 double* energy);
+/* Same with Y on the device (asynchronous on the mesh stream; energy may be NULL). */
+rpb_status rpb_tpoe_differential_device(rpb_mesh* m, double q, double p, double alpha, double beta, double* Y_dev,
+                                        int ldY, double* energy);
 
 /* --- learned preconditioner ------------------------------------------------------------ */
 

@@ -62,6 +62,16 @@ def _load():
     lib.oracle_h1_triplet_count.restype = ctypes.c_int64
     lib.oracle_h1_triplet_count.argtypes = [ctypes.c_void_p]
     lib.oracle_h1_triplets.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double, _ip, _ip, _dp]
+    lib.oracle_load_obstacle.restype = ctypes.c_int
+    lib.oracle_load_obstacle.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+    lib.oracle_obstacle_counts.argtypes = [ctypes.c_void_p, _lp]
+    lib.oracle_obstacle_pattern.argtypes = [ctypes.c_void_p, ctypes.c_int, _lp, _ip]
+    for name in ("oracle_obstacle_energy", "oracle_obstacle_allpairs_energy"):
+        getattr(lib, name).restype = ctypes.c_double
+        getattr(lib, name).argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double]
+    lib.oracle_obstacle_differential.restype = ctypes.c_double
+    lib.oracle_obstacle_differential.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                                 ctypes.c_double, _dp, ctypes.c_int]
     _lib = lib
     return lib
 
@@ -104,6 +114,38 @@ class OracleMesh:
 
     def set_threads(self, threads):
         _load().oracle_set_threads(self._h, int(threads))
+
+    # --- obstacle (TangentPointObstacleEnergy) -------------------------------------------
+    def load_obstacle(self, obstacle):
+        """Non-symmetric block cluster tree against another OracleMesh (kept referenced)."""
+        if _load().oracle_load_obstacle(self._h, obstacle._h) != 0:
+            raise ValueError("obstacle domain dimension differs from the mesh's")
+        self._obstacle = obstacle
+
+    def obstacle_counts(self):
+        out = np.zeros(4, dtype=np.int64)
+        _load().oracle_obstacle_counts(self._h, _l(out))
+        return dict(zip(["near", "far", "verynear", "inter"], out.tolist()))
+
+    def obstacle_pattern(self, which):
+        w = {"near": 0, "far": 1, "verynear": 2, "inter": 3}[which]
+        rows = self.counts()["clusters"] if which == "far" else self.nS
+        nnz = self.obstacle_counts()[which]
+        rp = np.zeros(rows + 1, dtype=np.int64)
+        ci = np.zeros(max(nnz, 1), dtype=np.int32)
+        _load().oracle_obstacle_pattern(self._h, w, _l(rp), _i(ci))
+        return rp, ci[:nnz]
+
+    def obstacle_energy(self, q=6.0, p=12.0):
+        return _load().oracle_obstacle_energy(self._h, q, p)
+
+    def obstacle_differential(self, q=6.0, p=12.0, alpha=1.0, beta=0.0, Y=None):
+        Y = np.zeros((self.nV, 3)) if Y is None else Y
+        en = _load().oracle_obstacle_differential(self._h, q, p, alpha, beta, _d(Y), 3)
+        return en, Y
+
+    def obstacle_allpairs_energy(self, q=6.0, p=12.0):
+        return _load().oracle_obstacle_allpairs_energy(self._h, q, p)
 
     def counts(self):
         out = np.zeros(7, dtype=np.int64)

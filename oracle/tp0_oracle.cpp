@@ -942,6 +942,41 @@ static void vf_quadrature(const Mesh& M, Int i, Int j, Emit&& emit)
 // ----------------------------------------------------------------------------
 struct EvalResult { double energy; };
 
+// CollectFarFieldDerivatives (src/ClusterTree.hpp:1164-1208), PercolateDown and
+// ClustersToPrimitives, CollectNearFieldDerivatives (src/ClusterTree.hpp:1115-1161):
+// per-thread buffers summed, far field pushed to the primitives, both unpermuted.
+static void collect_derivatives(Mesh& M, const std::vector<std::vector<double>>& tDn,
+                                const std::vector<std::vector<double>>& tDf, int threads, int nd)
+{
+        // CollectFarFieldDerivatives (src/ClusterTree.hpp:1164-1208)
+    std::vector<double> C_out(static_cast<size_t>(M.NC) * FAR_DIM, 0.0);
+    for (int t = 0; t < threads; ++t)
+        for (size_t k = 0; k < C_out.size(); ++k) C_out[k] += tDf[t][k];
+    for (Int C = 0; C < M.NC; ++C) {  // PercolateDown: parents before children in DFS order
+        const Int L = M.C_left[C];
+        if (L >= 0) {
+            const Int R = M.C_right[C];
+            for (int k = 0; k < FAR_DIM; ++k) {
+                C_out[FAR_DIM * static_cast<size_t>(L) + k] += C_out[FAR_DIM * static_cast<size_t>(C) + k];
+                C_out[FAR_DIM * static_cast<size_t>(R) + k] += C_out[FAR_DIM * static_cast<size_t>(C) + k];
+            }
+        }
+    }
+    std::vector<double> P_out(static_cast<size_t>(M.nS) * FAR_DIM, 0.0);
+    for (Int C = 0; C < M.NC; ++C)
+        if (M.C_left[C] < 0)
+            for (Int i = M.C_begin[C]; i < M.C_end[C]; ++i)
+                for (int k = 0; k < FAR_DIM; ++k) P_out[FAR_DIM * static_cast<size_t>(i) + k] = C_out[FAR_DIM * static_cast<size_t>(C) + k];
+    M.P_D_far.assign(static_cast<size_t>(M.nS) * FAR_DIM, 0.0);
+    M.P_D_near.assign(static_cast<size_t>(M.nS) * nd, 0.0);
+    for (Int i = 0; i < M.nS; ++i) {
+        const Int pi = M.inv_perm[i];
+        for (int k = 0; k < FAR_DIM; ++k) M.P_D_far[FAR_DIM * static_cast<size_t>(i) + k] = P_out[FAR_DIM * static_cast<size_t>(pi) + k];
+        for (int t = 0; t < threads; ++t)
+            for (int k = 0; k < nd; ++k) M.P_D_near[nd * static_cast<size_t>(i) + k] += tDn[t][nd * static_cast<size_t>(pi) + k];
+    }
+    }
+
 static double tp0_evaluate(Mesh& M, double q, double p, bool diff)
 {
     const TPParams T(q, p, M.dom);
@@ -1082,35 +1117,7 @@ static double tp0_evaluate(Mesh& M, double q, double p, bool diff)
         for (double v : part) en += v;
     }
 
-    if (diff) {
-        // CollectFarFieldDerivatives (src/ClusterTree.hpp:1164-1208)
-        std::vector<double> C_out(static_cast<size_t>(M.NC) * FAR_DIM, 0.0);
-        for (int t = 0; t < threads; ++t)
-            for (size_t k = 0; k < C_out.size(); ++k) C_out[k] += tDf[t][k];
-        for (Int C = 0; C < M.NC; ++C) {  // PercolateDown: parents before children in DFS order
-            const Int L = M.C_left[C];
-            if (L >= 0) {
-                const Int R = M.C_right[C];
-                for (int k = 0; k < FAR_DIM; ++k) {
-                    C_out[FAR_DIM * static_cast<size_t>(L) + k] += C_out[FAR_DIM * static_cast<size_t>(C) + k];
-                    C_out[FAR_DIM * static_cast<size_t>(R) + k] += C_out[FAR_DIM * static_cast<size_t>(C) + k];
-                }
-            }
-        }
-        std::vector<double> P_out(static_cast<size_t>(M.nS) * FAR_DIM, 0.0);
-        for (Int C = 0; C < M.NC; ++C)
-            if (M.C_left[C] < 0)
-                for (Int i = M.C_begin[C]; i < M.C_end[C]; ++i)
-                    for (int k = 0; k < FAR_DIM; ++k) P_out[FAR_DIM * static_cast<size_t>(i) + k] = C_out[FAR_DIM * static_cast<size_t>(C) + k];
-        M.P_D_far.assign(static_cast<size_t>(M.nS) * FAR_DIM, 0.0);
-        M.P_D_near.assign(static_cast<size_t>(M.nS) * nd, 0.0);
-        for (Int i = 0; i < M.nS; ++i) {
-            const Int pi = M.inv_perm[i];
-            for (int k = 0; k < FAR_DIM; ++k) M.P_D_far[FAR_DIM * static_cast<size_t>(i) + k] = P_out[FAR_DIM * static_cast<size_t>(pi) + k];
-            for (int t = 0; t < threads; ++t)
-                for (int k = 0; k < nd; ++k) M.P_D_near[nd * static_cast<size_t>(i) + k] += tDn[t][nd * static_cast<size_t>(pi) + k];
-        }
-    }
+    if (diff) collect_derivatives(M, tDn, tDf, threads, nd);
     return en;
 }
 
@@ -1636,6 +1643,202 @@ static double allpairs_energy(const Mesh& M, double q, double p)
     return en;
 }
 
+// ----------------------------------------------------------------------------
+// TangentPointObstacleEnergy (src/Energies/TangentPointObstacleEnergy.hpp:62-96): the TP
+// energy/differential kernels (src/Energies/TangentPointEnergy/TP_Kernel_FF.hpp:130-260,
+// TP_Kernel_NF.hpp, identical to TP0's for energy and differential) over the
+// non-symmetric block cluster tree of (mesh tree, obstacle tree)
+// (src/SimplicialMesh.hpp:741-756, BlockClusterTree<...,false>; traversal
+// src/ClusterTreePairTraversor/Traverse_DepthFirst.hpp:52-258 with symmetricQ = false).
+// Every (mesh, obstacle) pair is visited once with the symmetry factor 1/2
+// (src/FMM/FMM_Kernel.hpp:43) on energy and derivatives; only the mesh side's derivatives
+// are assembled (the obstacle does not move).
+// ----------------------------------------------------------------------------
+struct CrossPattern {
+    Int rows = 0;
+    std::vector<LInt> rp;
+    std::vector<Int> ci;
+    LInt nnz() const { return rp.empty() ? 0 : rp.back(); }
+};
+
+static CrossPattern make_cross_pattern(Int rows, std::vector<std::pair<Int, Int>>& pairs)
+{
+    std::sort(pairs.begin(), pairs.end());
+    CrossPattern P;
+    P.rows = rows;
+    P.rp.assign(static_cast<size_t>(rows) + 1, 0);
+    for (auto& e : pairs) P.rp[e.first + 1]++;
+    for (Int i = 0; i < rows; ++i) P.rp[i + 1] += P.rp[i];
+    P.ci.resize(pairs.size());
+    for (size_t k = 0; k < pairs.size(); ++k) P.ci[k] = pairs[k].second;
+    return P;
+}
+
+struct ObstacleLists {
+    CrossPattern near, far, verynear, inter;
+};
+
+static void build_obstacle_block_cluster_tree(const Mesh& M, const Mesh& O, ObstacleLists& L)
+{
+    const double far_t2 = M.set.theta_far * M.set.theta_far;
+    const double near_t2 = M.set.theta_near * M.set.theta_near;
+    const double eps2 = std::numeric_limits<double>::epsilon();
+    const int psM = M.poly_size(), psO = O.poly_size();
+    std::vector<std::pair<Int, Int>> near_l, far_l, vn_l, inter_l;
+    auto leaf = [&](Int pi, Int pj) {
+        const double* A = &M.P_poly[psM * static_cast<size_t>(pi)];
+        const double* B = &O.P_poly[psO * static_cast<size_t>(pj)];
+        const double d2 = poly_sqdist(M.dom, A + 1 + AMB, B + 1 + AMB);
+        const double tol = std::max(A[0], B[0]);
+        if (near_t2 * d2 > tol) { near_l.emplace_back(pi, pj); return; }
+        const double tol_i = eps2 * std::min(A[0], B[0]);
+        if (near_t2 * d2 <= tol_i) inter_l.emplace_back(pi, pj);
+        else vn_l.emplace_back(pi, pj);
+    };
+    std::vector<std::pair<Int, Int>> stack;
+    stack.emplace_back(0, 0);
+    while (!stack.empty()) {
+        auto [i, j] = stack.back();
+        stack.pop_back();
+        const double* Bi = &M.C_box[7 * static_cast<size_t>(i)];
+        const double* Bj = &O.C_box[7 * static_cast<size_t>(j)];
+        if (std::max(Bi[0], Bj[0]) < far_t2 * aabb_sq_dist(Bi, Bj)) {
+            far_l.emplace_back(i, j);
+            continue;
+        }
+        const Int Li = M.C_left[i], Lj = O.C_left[j];
+        if (Li >= 0 || Lj >= 0) {
+            const Int Ri = M.C_right[i], Rj = O.C_right[j];
+            const double si = (Li >= 0) ? Bi[0] : 0.0;
+            const double sj = (Lj >= 0) ? Bj[0] : 0.0;
+            if (si == sj && si > 0) {
+                stack.emplace_back(Ri, Rj);
+                stack.emplace_back(Li, Rj);
+                stack.emplace_back(Ri, Lj);
+                stack.emplace_back(Li, Lj);
+            } else if (si > sj) {
+                stack.emplace_back(Ri, j);
+                stack.emplace_back(Li, j);
+            } else {
+                stack.emplace_back(i, Rj);
+                stack.emplace_back(i, Lj);
+            }
+        } else {
+            leaf(M.C_begin[i], O.C_begin[j]);
+        }
+    }
+    L.near = make_cross_pattern(M.nS, near_l);
+    L.far = make_cross_pattern(M.NC, far_l);
+    L.verynear = make_cross_pattern(M.nS, vn_l);
+    L.inter = make_cross_pattern(M.nS, inter_l);
+}
+
+static double obstacle_evaluate(Mesh& M, const Mesh& O, const ObstacleLists& L, double q, double p, bool diff)
+{
+    const TPParams T(q, p, M.dom);
+    const int nd = near_dim(M.dom);
+    const int SIZE = M.SIZE;
+    const int threads = std::max(1, M.set.threads);
+    const double S_scale = 1.0 / SIZE;
+    const double sf = 0.5;   // symmetry factor of a non-symmetric block cluster tree
+    std::vector<std::vector<double>> tDn, tDf;
+    if (diff) {
+        tDn.assign(threads, std::vector<double>(static_cast<size_t>(M.nS) * nd, 0.0));
+        tDf.assign(threads, std::vector<double>(static_cast<size_t>(M.NC) * FAR_DIM, 0.0));
+    }
+    double en = 0;
+    auto center = [&](const Mesh& X, Int i, double* c) {
+        const double* D = &X.P_near[near_dim(X.dom) * static_cast<size_t>(i)];
+        for (int k = 0; k < 3; ++k) {
+            c[k] = 0;
+            for (int v = 0; v < X.SIZE; ++v) c[k] += D[1 + AMB * v + k] / X.SIZE;
+        }
+    };
+    {   // NF
+        const CrossPattern& Pt = L.near;
+        std::vector<double> part(threads, 0.0);
+        parallel_do(threads, [&](int t) {
+            double local = 0;
+            for (Int i = job_pointer(M.nS, threads, t); i < job_pointer(M.nS, threads, t + 1); ++i) {
+                const double* Xi = &M.P_near[nd * static_cast<size_t>(i)];
+                double x[3];
+                center(M, i, x);
+                for (LInt k = Pt.rp[i]; k < Pt.rp[i + 1]; ++k) {
+                    const Int j = Pt.ci[k];
+                    const double* Yj = &O.P_near[near_dim(O.dom) * static_cast<size_t>(j)];
+                    double y[3];
+                    center(O, j, y);
+                    PairOut o;
+                    tp0_pair(T, Xi[0], x, Xi + 1 + AMB * SIZE, Yj[0], y, Yj + 1 + AMB * O.SIZE, diff, false, o);
+                    local += sf * o.energy;
+                    if (diff) {
+                        double* DX = &tDn[t][nd * static_cast<size_t>(i)];
+                        DX[0] += sf * o.DX[0];
+                        for (int v = 0; v < SIZE; ++v)
+                            for (int kk = 0; kk < 3; ++kk) DX[1 + 3 * v + kk] += sf * S_scale * o.DX[1 + kk];
+                        for (int kk = 0; kk < 6; ++kk) DX[1 + AMB * SIZE + kk] += sf * o.DX[4 + kk];
+                    }
+                }
+            }
+            part[t] = local;
+        });
+        for (double v : part) en += v;
+    }
+    {   // FF
+        const CrossPattern& Pt = L.far;
+        std::vector<double> part(threads, 0.0);
+        parallel_do(threads, [&](int t) {
+            double local = 0;
+            for (Int i = job_pointer(M.NC, threads, t); i < job_pointer(M.NC, threads, t + 1); ++i) {
+                const double* Xi = &M.C_far[FAR_DIM * static_cast<size_t>(i)];
+                for (LInt k = Pt.rp[i]; k < Pt.rp[i + 1]; ++k) {
+                    const Int j = Pt.ci[k];
+                    const double* Yj = &O.C_far[FAR_DIM * static_cast<size_t>(j)];
+                    PairOut o;
+                    tp0_pair(T, Xi[0], Xi + 1, Xi + 4, Yj[0], Yj + 1, Yj + 4, diff, false, o);
+                    local += sf * o.energy;
+                    if (diff) {
+                        double* DX = &tDf[t][FAR_DIM * static_cast<size_t>(i)];
+                        for (int kk = 0; kk < 10; ++kk) DX[kk] += sf * o.DX[kk];
+                    }
+                }
+            }
+            part[t] = local;
+        });
+        for (double v : part) en += v;
+    }
+    if (diff) collect_derivatives(M, tDn, tDf, threads, nd);
+    return en;
+}
+
+// 1/2 sum over all (mesh primitive, obstacle primitive) pairs of a E b at the barycentres
+static double obstacle_allpairs_energy(const Mesh& M, const Mesh& O, double q, double p)
+{
+    const TPParams T(q, p, M.dom);
+    const int threads = std::max(1, M.set.threads);
+    std::vector<double> part(threads, 0.0);
+    parallel_do(threads, [&](int t) {
+        double local = 0;
+        for (Int i = job_pointer(M.nS, threads, t); i < job_pointer(M.nS, threads, t + 1); ++i) {
+            const double* X = &M.P_near[near_dim(M.dom) * static_cast<size_t>(i)];
+            double x[3];
+            for (int k = 0; k < 3; ++k) { x[k] = 0; for (int v = 0; v < M.SIZE; ++v) x[k] += X[1 + 3 * v + k] / M.SIZE; }
+            for (Int j = 0; j < O.nS; ++j) {
+                const double* Y = &O.P_near[near_dim(O.dom) * static_cast<size_t>(j)];
+                double y[3];
+                for (int k = 0; k < 3; ++k) { y[k] = 0; for (int v = 0; v < O.SIZE; ++v) y[k] += Y[1 + 3 * v + k] / O.SIZE; }
+                PairOut o;
+                tp0_pair(T, X[0], x, X + 1 + AMB * M.SIZE, Y[0], y, Y + 1 + AMB * O.SIZE, false, false, o);
+                local += 0.5 * o.energy;
+            }
+        }
+        part[t] = local;
+    });
+    double en = 0;
+    for (double v : part) en += v;
+    return en;
+}
+
 }  // namespace oracle
 
 // ============================================================================
@@ -1645,6 +1848,8 @@ using namespace oracle;
 
 struct OracleHandle {
     Mesh M;
+    const Mesh* obstacle = nullptr;   // not owned
+    ObstacleLists ob;
     MetricValues mv;
     bool mv_valid = false;
     double mv_q = 0, mv_p = 0;
@@ -1808,6 +2013,57 @@ int64_t oracle_h1_triplet_count(void* h)
 void oracle_h1_triplets(void* h, double ws, double wm, int* I, int* J, double* A)
 {
     h1_triplets(static_cast<OracleHandle*>(h)->M, ws, wm, I, J, A);
+}
+
+
+// Obstacle (the obstacle handle must outlive its use by h). Returns 0, or -1 if the
+// domain dimensions differ.
+int oracle_load_obstacle(void* h, void* obstacle)
+{
+    auto* H = static_cast<OracleHandle*>(h);
+    const Mesh& O = static_cast<OracleHandle*>(obstacle)->M;
+    if (O.dom != H->M.dom) return -1;
+    H->obstacle = &O;
+    build_obstacle_block_cluster_tree(H->M, O, H->ob);
+    return 0;
+}
+
+// [near, far, verynear, inter] nnz of the obstacle lists
+void oracle_obstacle_counts(void* h, int64_t* out)
+{
+    const auto* H = static_cast<OracleHandle*>(h);
+    out[0] = H->ob.near.nnz(); out[1] = H->ob.far.nnz(); out[2] = H->ob.verynear.nnz(); out[3] = H->ob.inter.nnz();
+}
+
+void oracle_obstacle_pattern(void* h, int which, int64_t* rp, int* ci)
+{
+    const auto* H = static_cast<OracleHandle*>(h);
+    const CrossPattern& P = which == 0 ? H->ob.near : which == 1 ? H->ob.far : which == 2 ? H->ob.verynear : H->ob.inter;
+    for (size_t k = 0; k < P.rp.size(); ++k) rp[k] = static_cast<int64_t>(P.rp[k]);
+    for (size_t k = 0; k < P.ci.size(); ++k) ci[k] = P.ci[k];
+}
+
+double oracle_obstacle_energy(void* h, double q, double p)
+{
+    auto* H = static_cast<OracleHandle*>(h);
+    if (!H->obstacle) return 0.0;
+    return obstacle_evaluate(H->M, *H->obstacle, H->ob, q, p, false);
+}
+
+double oracle_obstacle_differential(void* h, double q, double p, double alpha, double beta, double* Y, int ldY)
+{
+    auto* H = static_cast<OracleHandle*>(h);
+    if (!H->obstacle) return 0.0;
+    const double en = obstacle_evaluate(H->M, *H->obstacle, H->ob, q, p, true);
+    assemble_derivatives(H->M, alpha, beta, Y, ldY);
+    return en;
+}
+
+double oracle_obstacle_allpairs_energy(void* h, double q, double p)
+{
+    auto* H = static_cast<OracleHandle*>(h);
+    if (!H->obstacle) return 0.0;
+    return obstacle_allpairs_energy(H->M, *H->obstacle, q, p);
 }
 
 }  // extern "C"

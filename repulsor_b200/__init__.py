@@ -31,6 +31,7 @@ __all__ = [
     "HostTree",
     "TangentPointEnergy0",
     "TangentPointMetric0",
+    "TangentPointObstacleEnergy",
     "TangentPointEnergy0_Factory",
     "TangentPointMetric0_Factory",
     "RepulsorError",
@@ -83,7 +84,7 @@ class SimplicialMesh:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h and _capi is not None and _capi._lib is not None:
+        if h and getattr(self, "_owned", True) and _capi is not None and _capi._lib is not None:
             _capi._lib.rpb_mesh_destroy(h)
             self._h = None
 
@@ -118,6 +119,29 @@ class SimplicialMesh:
         check(_capi.load().rpb_mesh_semistatic_update_device(self._h, ctypes.c_void_p(V_dev_ptr)),
               "SemiStaticUpdateDevice")
         self._cache.clear()
+
+    def LoadObstacle(self, obstacle: "SimplicialMesh"):
+        """SimplicialMesh::LoadObstacle (src/SimplicialMesh.hpp:697-719): the mesh takes the
+        obstacle over (the obstacle object stays usable for reading, the mesh destroys it)."""
+        check(_capi.load().rpb_mesh_load_obstacle(self._h, obstacle._h), "LoadObstacle")
+        obstacle._owned = False
+        self._obstacle = obstacle
+        self._cache.clear()
+
+    def obstacle_stats(self) -> dict:
+        c = np.zeros(4, np.int64)
+        check(_capi.load().rpb_mesh_obstacle_stats(self._h, lptr(c)), "rpb_mesh_obstacle_stats")
+        return dict(zip(["near_nnz", "far_nnz", "verynear_nnz", "inter_nnz"], c.tolist()))
+
+    def obstacle_pattern(self, which: str):
+        """'near' | 'far' | 'verynear' | 'inter' -> (rowptr int64, colidx int32) of the obstacle lists."""
+        w = {"near": 0, "far": 1, "verynear": 2, "inter": 3}[which]
+        rows = self.stats()["cluster_count"] if which == "far" else self.nS
+        nnz = self.obstacle_stats()[which + "_nnz"]
+        rp = np.zeros(rows + 1, np.int64)
+        ci = np.zeros(max(nnz, 1), np.int32)
+        check(_capi.load().rpb_mesh_obstacle_pattern(self._h, w, lptr(rp), iptr(ci)), "rpb_mesh_obstacle_pattern")
+        return rp, ci[:nnz]
 
     # --- B200 extras ---------------------------------------------------------------------
     def stats(self) -> dict:
@@ -197,6 +221,26 @@ class HostTree:
         check(_capi.load().rpb_tree_host_pattern(self._h, w, lptr(rp), iptr(ci)), "rpb_tree_host_pattern")
         return rp, ci[:nnz]
 
+    def obstacle_pattern(self, V, S, obstacle: "HostTree", VO, SO, which: str):
+        """Obstacle list `which` of this tree (built from V, S) against `obstacle` (built
+        from VO, SO), as rpb_mesh_load_obstacle builds it: (rowptr, colidx, counts)."""
+        lib = _capi.load()
+        w = {"near": 0, "far": 1, "verynear": 2, "inter": 3}[which]
+        V = np.ascontiguousarray(V, dtype=np.float64)
+        S = np.ascontiguousarray(S, dtype=np.int32)
+        VO = np.ascontiguousarray(VO, dtype=np.float64)
+        SO = np.ascontiguousarray(SO, dtype=np.int32)
+        counts = np.zeros(4, np.int64)
+        args = (self._h, dptr(V), iptr(S), obstacle._h, dptr(VO), iptr(SO), w, lptr(counts))
+        check(lib.rpb_tree_host_obstacle_pattern(*args, None, None), "rpb_tree_host_obstacle_pattern")
+        st = self.stats()
+        rows = st["cluster_count"] if which == "far" else st["simplex_count"]
+        nnz = int(counts[w])
+        rp = np.zeros(rows + 1, np.int64)
+        ci = np.zeros(max(nnz, 1), np.int32)
+        check(lib.rpb_tree_host_obstacle_pattern(*args, lptr(rp), iptr(ci)), "rpb_tree_host_obstacle_pattern")
+        return rp, ci[:nnz], dict(zip(["near", "far", "verynear", "inter"], counts.tolist()))
+
     def h1_solve(self, V, S, B):
         """X = H1^{-1} B on the host (nested-dissection sparse Cholesky)."""
         V = np.ascontiguousarray(V, dtype=np.float64)
@@ -266,6 +310,59 @@ class TangentPointEnergy0:
         """Y (device pointer, n_v x ldY float64) = alpha dE + beta Y on the mesh stream."""
         e = ctypes.c_double()
         check(_capi.load().rpb_tpe0_differential_device(M._h, self.q, self.p, float(alpha), float(beta),
+                                                        ctypes.c_void_p(Y_dev_ptr), ldY, ctypes.byref(e)),
+              "DifferentialDevice")
+        return e.value
+
+
+class TangentPointObstacleEnergy:
+    """TangentPointObstacleEnergy(q, p) of a mesh against its loaded obstacle
+    (src/Energies/TangentPointObstacleEnergy.hpp:48-96); 0 without an obstacle."""
+
+    def __init__(self, q, p=None):
+        if p is None:
+            q, p = float(q), 2.0 * float(q)
+        self.q = float(q)
+        self.p = float(p)
+
+    def ClassName(self):
+        return f"TangentPointObstacleEnergy({self.q},{self.p})"
+
+    def Value(self, M: SimplicialMesh) -> float:
+        M = _as_mesh(M)
+        tag = self.ClassName() + "::Value"
+        if tag not in M._cache:
+            e = ctypes.c_double()
+            check(_capi.load().rpb_tpoe_value(M._h, self.q, self.p, ctypes.byref(e)), "Value")
+            M._cache[tag] = e.value
+        return M._cache[tag]
+
+    def Differential(self, M: SimplicialMesh, alpha=None, beta=0.0, Y=None):
+        """As TangentPointEnergy0.Differential; derivatives with respect to M's vertices."""
+        M = _as_mesh(M)
+        lib = _capi.load()
+        if alpha is None:
+            tag = self.ClassName() + "::Differential"
+            if tag not in M._cache:
+                D = np.zeros((M.nV, 3))
+                e = ctypes.c_double()
+                check(lib.rpb_tpoe_differential(M._h, self.q, self.p, 1.0, 0.0, dptr(D), 3, ctypes.byref(e)),
+                      "Differential")
+                M._cache[tag] = D
+                M._cache.setdefault(self.ClassName() + "::Value", e.value)
+            return M._cache[tag]
+        if Y is None:
+            Y = np.zeros((M.nV, 3))
+        if Y.dtype != np.float64 or not Y.flags.c_contiguous or Y.shape[0] != M.nV or Y.shape[1] < 3:
+            raise RepulsorError(_capi.RPB_EINVAL, "Differential: Y must be a C-contiguous float64 (n_v, ldY>=3) array")
+        e = ctypes.c_double()
+        check(lib.rpb_tpoe_differential(M._h, self.q, self.p, float(alpha), float(beta), dptr(Y), Y.shape[1],
+                                        ctypes.byref(e)), "Differential")
+        return e.value
+
+    def DifferentialDevice(self, M: SimplicialMesh, Y_dev_ptr: int, ldY: int = 3, alpha=1.0, beta=0.0) -> float:
+        e = ctypes.c_double()
+        check(_capi.load().rpb_tpoe_differential_device(M._h, self.q, self.p, float(alpha), float(beta),
                                                         ctypes.c_void_p(Y_dev_ptr), ldY, ctypes.byref(e)),
               "DifferentialDevice")
         return e.value

@@ -77,6 +77,7 @@ SIGNATURES = {
     "rpb_tree_host_arrays": (ctypes.c_int, [_vp, _ip, _ip, _ip, _ip, _ip]),
     "rpb_tree_host_pattern": (ctypes.c_int, [_vp, ctypes.c_int, _lp, _ip]),
     "rpb_tree_host_destroy": (ctypes.c_int, [_vp]),
+    "rpb_tree_host_obstacle_pattern": (ctypes.c_int, [_vp, _dp, _ip, _vp, _dp, _ip, ctypes.c_int, _lp, _lp, _ip]),
     "rpb_h1_solve_host": (ctypes.c_int, [_vp, _dp, _ip, _dp, _dp, ctypes.c_int]),
     "rpb_tpe0_value": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double, _dp]),
     "rpb_tpe0_differential": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double, ctypes.c_double,
@@ -100,6 +101,14 @@ SIGNATURES = {
                                               ctypes.c_int64, _vp, _vp, _vp, _vp, ctypes.c_double, ctypes.c_double,
                                               _vp, _vp]),
     "rpb_tpm0_solve_info": (ctypes.c_int, [_vp, ctypes.POINTER(SolveInfo)]),
+    "rpb_mesh_load_obstacle": (ctypes.c_int, [_vp, _vp]),
+    "rpb_mesh_obstacle_stats": (ctypes.c_int, [_vp, _lp]),
+    "rpb_mesh_obstacle_pattern": (ctypes.c_int, [_vp, ctypes.c_int, _lp, _ip]),
+    "rpb_tpoe_value": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double, _dp]),
+    "rpb_tpoe_differential": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                             _dp, ctypes.c_int, _dp]),
+    "rpb_tpoe_differential_device": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                                    ctypes.c_double, _vp, ctypes.c_int, _dp]),
     "rpb_mlp_param_count": (ctypes.c_int, []),
     "rpb_mlp_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_uint64, ctypes.POINTER(_vp)]),
     "rpb_mlp_destroy": (ctypes.c_int, [_vp]),

@@ -550,4 +550,134 @@ std::string build_tree(int dom, const double* V, int nV, const int* S, int N, co
     return std::string();
 }
 
+namespace {
+
+CrossPattern to_cross(int rows, std::vector<std::vector<std::pair<int, int>>>& parts)
+{
+    CrossPattern P;
+    P.rows = rows;
+    P.rp.assign(static_cast<size_t>(rows) + 1, 0);
+    for (auto& v : parts)
+        for (auto& e : v) P.rp[e.first + 1]++;
+    for (int i = 0; i < rows; ++i) P.rp[i + 1] += P.rp[i];
+    P.ci.resize(static_cast<size_t>(P.rp[rows]));
+    std::vector<int64_t> pos(P.rp.begin(), P.rp.end() - 1);
+    for (auto& v : parts)
+        for (auto& e : v) P.ci[pos[e.first]++] = e.second;
+    for (int i = 0; i < rows; ++i) std::sort(P.ci.begin() + P.rp[i], P.ci.begin() + P.rp[i + 1]);
+    return P;
+}
+
+std::vector<double> permuted_polytopes(const HostTree& T, const double* V, const int* S)
+{
+    const int ps = 1 + AMB + T.size * AMB;
+    std::vector<double> P(static_cast<size_t>(T.N) * ps);
+    for (int i = 0; i < T.N; ++i)
+        serialize_polytope(T.size, V, S + static_cast<int64_t>(T.size) * T.perm[i], &P[static_cast<size_t>(ps) * i]);
+    return P;
+}
+
+struct CrossTraversal {
+    const HostTree& A;
+    const HostTree& B;
+    const std::vector<double>& PA;
+    const std::vector<double>& PB;
+    int psA, psB;
+    double far_t2, near_t2;
+
+    struct Out {
+        std::vector<std::pair<int, int>> near, far, verynear, inter;
+    };
+
+    void leaf(int pi, int pj, Out& out) const
+    {
+        const double* X = PA.data() + static_cast<int64_t>(psA) * pi;
+        const double* Y = PB.data() + static_cast<int64_t>(psB) * pj;
+        const double tol = std::max(X[0], Y[0]);
+        double cc = 0;
+        for (int k = 0; k < AMB; ++k) { const double d = X[1 + k] - Y[1 + k]; cc += d * d; }
+        const double lb = std::sqrt(cc) - std::sqrt(X[0]) - std::sqrt(Y[0]);
+        if (lb > 0 && near_t2 * lb * lb > tol) { out.near.emplace_back(pi, pj); return; }
+        const double d2 = (A.dom == 1) ? segseg2(X + 4, X + 7, Y + 4, Y + 7) : tritri2(X + 4, Y + 4);
+        if (near_t2 * d2 > tol) { out.near.emplace_back(pi, pj); return; }
+        const double tol_i = std::numeric_limits<double>::epsilon() * std::min(X[0], Y[0]);
+        if (near_t2 * d2 <= tol_i) out.inter.emplace_back(pi, pj);
+        else out.verynear.emplace_back(pi, pj);
+    }
+
+    template <typename Push>
+    void step(int i, int j, Out& out, Push&& push) const
+    {
+        const double* a = &A.C_box[7 * static_cast<int64_t>(i)];
+        const double* b = &B.C_box[7 * static_cast<int64_t>(j)];
+        double d2 = 0;
+        for (int k = 0; k < AMB; ++k) {
+            const double lo = std::max(a[1 + k] - a[4 + k], b[1 + k] - b[4 + k]);
+            const double hi = std::min(a[1 + k] + a[4 + k], b[1 + k] + b[4 + k]);
+            const double x = std::max(0.0, lo - hi);
+            d2 += x * x;
+        }
+        if (std::max(a[0], b[0]) < far_t2 * d2) { out.far.emplace_back(i, j); return; }
+        const int Li = A.C_left[i], Lj = B.C_left[j];
+        if (Li >= 0 || Lj >= 0) {
+            const int Ri = A.C_right[i], Rj = B.C_right[j];
+            const double si = Li >= 0 ? a[0] : 0.0;
+            const double sj = Lj >= 0 ? b[0] : 0.0;
+            if (si == sj && si > 0) { push(Ri, Rj); push(Li, Rj); push(Ri, Lj); push(Li, Lj); }
+            else if (si > sj) { push(Ri, j); push(Li, j); }
+            else { push(i, Rj); push(i, Lj); }
+            return;
+        }
+        leaf(A.C_begin[i], B.C_begin[j], out);
+    }
+};
+
+}  // namespace
+
+std::string build_cross_lists(const HostTree& S, const double* VS, const int* SS, const HostTree& T,
+                              const double* VT, const int* ST, const TreeSettings& set, CrossLists& out)
+{
+    if (S.dom != T.dom) return "the obstacle's domain dimension differs from the mesh's";
+    if (S.NC <= 0 || T.NC <= 0) return "empty tree";
+    const std::vector<double> PA = permuted_polytopes(S, VS, SS), PB = permuted_polytopes(T, VT, ST);
+    CrossTraversal tr{S, T, PA, PB, 1 + AMB + S.size * AMB, 1 + AMB + T.size * AMB,
+                      set.theta_far * set.theta_far, set.theta_near * set.theta_near};
+    const int threads = std::max(1, set.threads);
+    // expand the root block breadth-first into independent tasks, then depth-first in parallel
+    CrossTraversal::Out top;
+    std::vector<std::pair<int, int>> tasks{{0, 0}};
+    while (!tasks.empty() && static_cast<int>(tasks.size()) < 16 * threads) {
+        std::vector<std::pair<int, int>> next;
+        for (auto [i, j] : tasks) tr.step(i, j, top, [&](int a, int b) { next.emplace_back(a, b); });
+        tasks.swap(next);
+    }
+    std::vector<CrossTraversal::Out> parts(tasks.size());
+    std::atomic<int> ticket{0};
+    run_threads(threads, [&](int) {
+        std::vector<std::pair<int, int>> stack;
+        for (;;) {
+            const int t = ticket.fetch_add(1);
+            if (t >= static_cast<int>(tasks.size())) break;
+            stack.assign(1, tasks[t]);
+            while (!stack.empty()) {
+                auto [i, j] = stack.back();
+                stack.pop_back();
+                tr.step(i, j, parts[t], [&](int a, int b) { stack.emplace_back(a, b); });
+            }
+        }
+    });
+    auto gather = [&](std::vector<std::pair<int, int>> CrossTraversal::Out::*mem, int rows) {
+        std::vector<std::vector<std::pair<int, int>>> v;
+        v.push_back(std::move(top.*mem));
+        for (auto& p : parts) v.push_back(std::move(p.*mem));
+        return to_cross(rows, v);
+    };
+    out = CrossLists();
+    out.near = gather(&CrossTraversal::Out::near, S.N);
+    out.far = gather(&CrossTraversal::Out::far, S.NC);
+    out.verynear = gather(&CrossTraversal::Out::verynear, S.N);
+    out.inter = gather(&CrossTraversal::Out::inter, S.N);
+    return std::string();
+}
+
 }  // namespace rpb

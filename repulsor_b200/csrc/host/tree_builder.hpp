@@ -52,4 +52,23 @@ struct HostTree {
 std::string build_tree(int dom, const double* V, int nV, const int* S, int N, const TreeSettings& set,
                        HostTree& out);
 
+// Rectangular CSR (rows of one tree, columns of another), columns sorted.
+struct CrossPattern {
+    int rows = 0;
+    std::vector<int64_t> rp;
+    std::vector<int> ci;
+    int64_t nnz() const { return rp.empty() ? 0 : rp.back(); }
+};
+
+// Non-symmetric block cluster tree of a mesh tree S against an obstacle tree T
+// (BlockClusterTree<..., false>, src/SimplicialMesh.hpp:741-756): every (S, T) block
+// pair is visited once, the larger cluster (by squared radius) is split, both when the
+// radii are equal. near/verynear/inter rows are S primitives, far rows are S clusters.
+struct CrossLists {
+    CrossPattern near, far, verynear, inter;
+};
+
+std::string build_cross_lists(const HostTree& S, const double* VS, const int* SS, const HostTree& T,
+                              const double* VT, const int* ST, const TreeSettings& set, CrossLists& out);
+
 }  // namespace rpb

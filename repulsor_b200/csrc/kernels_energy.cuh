@@ -384,6 +384,7 @@ struct PairArgs {
     const int* ci;
     const int* order;         // rows in processing order (length-sorted within 256-row chunks)
     const void* data;         // PrimDatum* (near) or ClusterDatum* (far)
+    const void* col_data;     // CROSS: the obstacle's data the columns index
     double* D;                // rows x 10 (d0, dx[3], dP[6]) centred moment derivatives
     double* block_energy;     // gridDim.x
     unsigned* done;           // 1 counter, zero between launches
@@ -406,12 +407,16 @@ constexpr int pair_blocks(int rows, int lanes) { return (rows * lanes + PAIR_BLO
 // LANES threads per row. FAR: rows are clusters of the Far() pattern; otherwise rows are
 // primitives of the Near() pattern. A row accumulates only its own derivative; each
 // unordered pair contributes its energy once (from the row with the smaller index).
-template <bool FAR, int QH, int PH, bool DIFF, int LANES>
+// CROSS: rows are the mesh's, columns the obstacle's (a non-symmetric block cluster tree):
+// every pair counts, energy and derivatives carry the symmetry factor 1/2
+// (src/FMM/FMM_Kernel.hpp:43) and the obstacle's derivatives are not formed.
+template <bool FAR, int QH, int PH, bool DIFF, int LANES, bool CROSS = false>
 __global__ void __launch_bounds__(PAIR_BLOCK) k_tp0_pairs(PairArgs A)
 {
     static_assert(LANES == 1 || LANES == 2 || LANES == 4 || LANES == 8, "LANES must divide a warp");
     using Datum = typename std::conditional<FAR, ClusterDatum, PrimDatum>::type;
     const Datum* base = static_cast<const Datum*>(A.data);
+    const Datum* cols = CROSS ? static_cast<const Datum*>(A.col_data) : base;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int slot = t / LANES, sub = t & (LANES - 1);
     const bool active = slot < A.rows;
@@ -428,7 +433,7 @@ __global__ void __launch_bounds__(PAIR_BLOCK) k_tp0_pairs(PairArgs A)
         const int64_t k0 = A.rp[i], k1 = A.rp[i + 1];
         for (int64_t k = k0 + sub; k < k1; k += LANES) {
             const int j = __ldg(A.ci + k);
-            const Datum Y = load_datum(base, j);
+            const Datum Y = load_datum(cols, j);
             Proj<float> g;
             if constexpr (FAR) project_clusters(X, Y, g);
             else project_prims(A.dom, X, Y, g);
@@ -443,7 +448,7 @@ __global__ void __launch_bounds__(PAIR_BLOCK) k_tp0_pairs(PairArgs A)
                 if constexpr (!FAR) project_prims(A.dom, X, Y, gd);
                 PairAcc<double> a64 = {};
                 const double e = tp0_core<double, QH, PH, DIFF>(A.ex, gd, X.a, Y.a, a64);
-                if (j > i) e_row += e;
+                if (CROSS || j > i) e_row += e;
                 if (DIFF) {
                     D64[0] += a64.d0;
                     for (int m = 0; m < 3; ++m) D64[1 + m] += a64.dx[m];
@@ -451,7 +456,7 @@ __global__ void __launch_bounds__(PAIR_BLOCK) k_tp0_pairs(PairArgs A)
                 }
             } else {
                 const float e = tp0_core<float, QH, PH, DIFF>(A.ex, g, ax, static_cast<float>(Y.a), acc);
-                if (j > i) e32 += e;
+                if (CROSS || j > i) e32 += e;
                 if (++since_flush == PAIR_FLUSH) {
                     since_flush = 0;
                     e_row += e32;
@@ -475,6 +480,11 @@ __global__ void __launch_bounds__(PAIR_BLOCK) k_tp0_pairs(PairArgs A)
 #pragma unroll
             for (int m = 0; m < 6; ++m) D64[4 + m] += acc.dP[m];
         }
+    }
+    if constexpr (CROSS) {
+        e_row *= 0.5;
+#pragma unroll
+        for (int m = 0; m < 10; ++m) D64[m] *= 0.5;
     }
     // combine the LANES partial sums of a row (every lane of the warp takes part)
 #pragma unroll

@@ -157,6 +157,7 @@ static void launch_pairs_t(rpb_mesh* m, const PairArgs& An, const PairArgs& Af, 
 rpb_status launch_pairs(rpb_mesh* m, const TPExp& ex, bool diff, cudaEvent_t between = nullptr)
 {
     PairArgs An, Af;
+    An.col_data = Af.col_data = nullptr;
     An.dom = Af.dom = m->dom;
     An.ex = Af.ex = ex;
     An.close_factor = Af.close_factor = 0.1f;
@@ -184,7 +185,8 @@ rpb_status launch_pairs(rpb_mesh* m, const TPExp& ex, bool diff, cudaEvent_t bet
     return RPB_OK;
 }
 
-rpb_status launch_collect_gather(rpb_mesh* m, double alpha, double beta, double* Y, int ldY, bool with_vf)
+rpb_status launch_collect_gather(rpb_mesh* m, double alpha, double beta, double* Y, int ldY, bool with_vf,
+                                 const double* D_near, const double* D_far)
 {
     CollectArgs C;
     C.dom = m->dom;
@@ -196,8 +198,8 @@ rpb_status launch_collect_gather(rpb_mesh* m, double alpha, double beta, double*
     C.leaf_of = m->leaf_of.ptr;
     C.C_parent = m->C_parent.ptr;
     C.C_pair = m->C_pair.ptr;
-    C.D_near = m->D_near.ptr;
-    C.D_far = m->D_far.ptr;
+    C.D_near = D_near ? D_near : m->D_near.ptr;
+    C.D_far = D_far ? D_far : m->D_far.ptr;
     C.D_vf = with_vf ? m->D_vf.ptr : nullptr;
     C.B = m->B.ptr;
     k_collect_chain<<<(m->N + 255) / 256, 256, 0, m->stream>>>(C);
@@ -236,7 +238,7 @@ rpb_status evaluate(rpb_mesh* m, double q, double p, bool diff, double alpha, do
         if (st != RPB_OK) return st;
     }
     if (diff) {
-        st = launch_collect_gather(m, alpha, beta, Y_dev, ldY, with_vf);
+        st = launch_collect_gather(m, alpha, beta, Y_dev, ldY, with_vf, nullptr, nullptr);
         if (st != RPB_OK) return st;
     }
     if (energy_host) {
@@ -307,6 +309,8 @@ rpb_status rpb_mesh_create(int dom_dim, int amb_dim, const double* Vh, int64_t n
     if (!err.empty()) { set_error(err); return fail(RPB_EINVAL); }
     m->build_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     m->NC = m->tree.NC;
+    m->V_frozen.assign(Vh, Vh + 3 * static_cast<size_t>(m->nV));
+    m->S_host.assign(Sh, Sh + static_cast<size_t>(m->size) * m->N);
 
     if (cudaSetDevice(m->device) != cudaSuccess) { set_error("cudaSetDevice failed"); return fail(RPB_ECUDA); }
     if (cudaStreamCreateWithFlags(&m->own_stream, cudaStreamNonBlocking) != cudaSuccess) { set_error("stream creation failed"); return fail(RPB_ECUDA); }
@@ -395,6 +399,7 @@ rpb_status rpb_mesh_destroy(rpb_mesh* m)
     if (m->stream) cudaStreamSynchronize(m->stream);
     solver_free(m);
     learned_free(m);
+    obstacle_free(m);
     cudaStream_t s = m->own_stream;
     delete m;  // frees device buffers
     if (s) cudaStreamDestroy(s);
@@ -458,6 +463,7 @@ rpb_status rpb_mesh_pattern(const rpb_mesh* m, int which, int64_t* rowptr, int* 
 
 struct rpb_host_tree {
     HostTree tree;
+    TreeSettings settings;
     double seconds = 0;
 };
 
@@ -478,6 +484,7 @@ rpb_status rpb_tree_build_host(int dom_dim, const double* V, int64_t nV, const i
     ts.max_refinement = set.max_refinement;
     ts.threads = set.thread_count > 0 ? set.thread_count : std::max(1u, std::thread::hardware_concurrency());
     auto* t = new rpb_host_tree();
+    t->settings = ts;
     const auto t0 = std::chrono::steady_clock::now();
     const std::string err = build_tree(dom_dim, V, static_cast<int>(nV), S, static_cast<int>(nS), ts, t->tree);
     if (!err.empty()) { delete t; set_error(err); return RPB_EINVAL; }
@@ -530,6 +537,22 @@ rpb_status rpb_tree_host_pattern(const rpb_host_tree* t, int which, int64_t* row
 rpb_status rpb_tree_host_destroy(rpb_host_tree* t)
 {
     delete t;
+    return RPB_OK;
+}
+
+rpb_status rpb_tree_host_obstacle_pattern(const rpb_host_tree* mesh, const double* V, const int* S,
+                                          const rpb_host_tree* obstacle, const double* VO, const int* SO, int which,
+                                          int64_t* counts, int64_t* rowptr, int* colidx)
+{
+    if (!mesh || !obstacle || !V || !S || !VO || !SO || !counts) { set_error("null argument"); return RPB_EINVAL; }
+    if (which < 0 || which > 3) { set_error("pattern id must be 0..3"); return RPB_EINVAL; }
+    CrossLists L;
+    const std::string err = build_cross_lists(mesh->tree, V, S, obstacle->tree, VO, SO, mesh->settings, L);
+    if (!err.empty()) { set_error(err); return RPB_EINVAL; }
+    counts[0] = L.near.nnz(); counts[1] = L.far.nnz(); counts[2] = L.verynear.nnz(); counts[3] = L.inter.nnz();
+    const CrossPattern& P = which == 0 ? L.near : which == 1 ? L.far : which == 2 ? L.verynear : L.inter;
+    if (rowptr) std::copy(P.rp.begin(), P.rp.end(), rowptr);
+    if (colidx) std::copy(P.ci.begin(), P.ci.end(), colidx);
     return RPB_OK;
 }
 
@@ -642,7 +665,7 @@ rpb_status rpb_tpe0_stage_times(rpb_mesh* m, double q, double p, int reps, int64
         if ((st = launch_pairs(m, ex, true, ev[2])) != RPB_OK) return st;
         if (with_vf && (st = launch_vf(m, ex, true)) != RPB_OK) return st;
         RPB_CUDA(cudaEventRecord(ev[3], m->stream));
-        if ((st = launch_collect_gather(m, 1.0, 0.0, m->Y.ptr, 3, with_vf)) != RPB_OK) return st;
+        if ((st = launch_collect_gather(m, 1.0, 0.0, m->Y.ptr, 3, with_vf, nullptr, nullptr)) != RPB_OK) return st;
         RPB_CUDA(cudaEventRecord(ev[4], m->stream));
         RPB_CUDA(cudaEventSynchronize(ev[4]));
         float t;

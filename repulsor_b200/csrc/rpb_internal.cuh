@@ -14,6 +14,9 @@ void set_error(const std::string& msg);
 TPExp make_exp(int dom, double q, double p);
 rpb_status check_exponents(double q, double p);
 rpb_status launch_geometry(rpb_mesh* m);
+// near/far moment derivatives (mesh buffers when null) -> chain rule -> Y = alpha dE + beta Y
+rpb_status launch_collect_gather(rpb_mesh* m, double alpha, double beta, double* Y, int ldY, bool with_vf,
+                                 const double* D_near, const double* D_far);
 rpb_status evaluate(rpb_mesh* m, double q, double p, bool diff, double alpha, double beta, double* Y_dev, int ldY,
                     double* energy_host);
 
@@ -35,5 +38,8 @@ rpb_status reference_precondition(rpb_mesh* m, double q, double p, const double*
 // learned preconditioner (rpb_learned.cu): Z = MLP correction of the residual R (n x 3, device)
 rpb_status learned_precondition(rpb_mesh* m, double q, double p, const double* R, double* Z);
 void learned_free(rpb_mesh* m);
+
+// obstacle (rpb_obstacle.cu)
+void obstacle_free(rpb_mesh* m);
 
 }  // namespace rpb

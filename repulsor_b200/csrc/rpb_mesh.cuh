@@ -14,6 +14,7 @@ namespace rpb {
 
 struct Solver;
 struct LearnedState;
+struct ObstacleState;
 void set_error(const std::string& msg);
 
 template <typename T>
@@ -111,6 +112,11 @@ struct rpb_mesh {
     rpb::Solver* solver = nullptr;
     // learned preconditioner state (allocated on first use)
     rpb::LearnedState* learned = nullptr;
+    // obstacle of TangentPointObstacleEnergy (owned, with its cross block cluster tree)
+    rpb::ObstacleState* obstacle = nullptr;
+    // frozen coordinates and simplices on the host (the tree was built from them)
+    std::vector<double> V_frozen;
+    std::vector<int> S_host;
 
     int64_t device_bytes() const;
 };

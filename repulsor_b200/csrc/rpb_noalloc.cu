@@ -131,6 +131,7 @@ extern "C" rpb_status rpb_tpe0_value_noalloc(int dom_dim, const double* V, int64
     const TPExp ex = make_exp(dom_dim, q, p);
     const int nb_near = pair_blocks(N, NEAR_LANES), nb_far = pair_blocks(NC, FAR_LANES);
     PairArgs An, Af;
+    An.col_data = Af.col_data = nullptr;
     An.dom = Af.dom = dom_dim;
     An.ex = Af.ex = ex;
     An.close_factor = Af.close_factor = 0.1f;
