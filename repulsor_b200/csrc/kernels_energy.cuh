@@ -14,7 +14,11 @@
 //   k_gather_vertices  : DerivativeAssembler().Dot (src/SimplicialMesh.hpp:625-674).
 #pragma once
 
+#include <algorithm>
+#include <map>
+#include <mutex>
 #include <type_traits>
+#include <utility>
 
 #include "rpb_device.cuh"
 
@@ -388,6 +392,7 @@ struct PairArgs {
     double* D;                // rows x 10 (d0, dx[3], dP[6]) centred moment derivatives
     double* block_energy;     // gridDim.x
     unsigned* done;           // 1 counter, zero between launches
+    unsigned* rows_taken;     // 1 counter, zero between launches (dynamic row distribution)
     double* energy_out;       // 1
     TPExp ex;
     float close_factor;       // FP64 path for near pairs with r < close_factor (d_i + d_j)
@@ -410,103 +415,115 @@ constexpr int pair_blocks(int rows, int lanes) { return (rows * lanes + PAIR_BLO
 // CROSS: rows are the mesh's, columns the obstacle's (a non-symmetric block cluster tree):
 // every pair counts, energy and derivatives carry the symmetry factor 1/2
 // (src/FMM/FMM_Kernel.hpp:43) and the obstacle's derivatives are not formed.
+// The grid is the resident set (pair_grid): warps take the next 32/LANES rows of the
+// processing order from a global counter until none are left, so long and short rows
+// balance across the SMs and no block waits on a slow sibling at its end.
 template <bool FAR, int QH, int PH, bool DIFF, int LANES, bool CROSS = false>
 __global__ void __launch_bounds__(PAIR_BLOCK) k_tp0_pairs(PairArgs A)
 {
     static_assert(LANES == 1 || LANES == 2 || LANES == 4 || LANES == 8, "LANES must divide a warp");
+    constexpr int ROWS_PER_WARP = 32 / LANES;
     using Datum = typename std::conditional<FAR, ClusterDatum, PrimDatum>::type;
     const Datum* base = static_cast<const Datum*>(A.data);
     const Datum* cols = CROSS ? static_cast<const Datum*>(A.col_data) : base;
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    const int slot = t / LANES, sub = t & (LANES - 1);
-    const bool active = slot < A.rows;
-    double e_row = 0.0;
-    double D64[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
-    int i = 0;
-    if (active) {
-        i = A.order ? A.order[slot] : slot;
-        const Datum X = load_datum(base, i);
-        const float ax = static_cast<float>(X.a);
-        PairAcc<float> acc = {};
-        float e32 = 0.0f;
-        int since_flush = 0;
-        const int64_t k0 = A.rp[i], k1 = A.rp[i + 1];
-        for (int64_t k = k0 + sub; k < k1; k += LANES) {
-            const int j = __ldg(A.ci + k);
-            const Datum Y = load_datum(cols, j);
-            Proj<float> g;
-            if constexpr (FAR) project_clusters(X, Y, g);
-            else project_prims(A.dom, X, Y, g);
-            bool close = false;
-            if constexpr (!FAR) {
-                const float dd = A.close_factor * (X.diam + Y.diam);
-                close = g.r2 < dd * dd;
-            }
-            if (close) {
-                // close near-field pair: the same kernel in FP64, added straight into FP64
-                Proj<double> gd;
-                if constexpr (!FAR) project_prims(A.dom, X, Y, gd);
-                PairAcc<double> a64 = {};
-                const double e = tp0_core<double, QH, PH, DIFF>(A.ex, gd, X.a, Y.a, a64);
-                if (CROSS || j > i) e_row += e;
-                if (DIFF) {
-                    D64[0] += a64.d0;
-                    for (int m = 0; m < 3; ++m) D64[1 + m] += a64.dx[m];
-                    for (int m = 0; m < 6; ++m) D64[4 + m] += a64.dP[m];
+    const int lane = threadIdx.x & 31;
+    const int grp = lane / LANES, sub = lane & (LANES - 1);
+    double e_acc = 0.0;
+    for (;;) {
+        int first = 0;
+        if (lane == 0) first = static_cast<int>(atomicAdd(A.rows_taken, static_cast<unsigned>(ROWS_PER_WARP)));
+        first = __shfl_sync(0xffffffffu, first, 0);
+        if (first >= A.rows) break;
+        const int slot = first + grp;
+        const bool active = slot < A.rows;
+        double e_row = 0.0;
+        double D64[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+        int i = 0;
+        if (active) {
+            i = A.order ? A.order[slot] : slot;
+            const Datum X = load_datum(base, i);
+            const float ax = static_cast<float>(X.a);
+            PairAcc<float> acc = {};
+            float e32 = 0.0f;
+            int since_flush = 0;
+            const int64_t k0 = A.rp[i], k1 = A.rp[i + 1];
+            for (int64_t k = k0 + sub; k < k1; k += LANES) {
+                const int j = __ldg(A.ci + k);
+                const Datum Y = load_datum(cols, j);
+                Proj<float> g;
+                if constexpr (FAR) project_clusters(X, Y, g);
+                else project_prims(A.dom, X, Y, g);
+                bool close = false;
+                if constexpr (!FAR) {
+                    const float dd = A.close_factor * (X.diam + Y.diam);
+                    close = g.r2 < dd * dd;
                 }
-            } else {
-                const float e = tp0_core<float, QH, PH, DIFF>(A.ex, g, ax, static_cast<float>(Y.a), acc);
-                if (CROSS || j > i) e32 += e;
-                if (++since_flush == PAIR_FLUSH) {
-                    since_flush = 0;
-                    e_row += e32;
-                    e32 = 0.0f;
+                if (close) {
+                    // close near-field pair: the same kernel in FP64, added straight into FP64
+                    Proj<double> gd;
+                    if constexpr (!FAR) project_prims(A.dom, X, Y, gd);
+                    PairAcc<double> a64 = {};
+                    const double e = tp0_core<double, QH, PH, DIFF>(A.ex, gd, X.a, Y.a, a64);
+                    if (CROSS || j > i) e_row += e;
                     if (DIFF) {
-                        D64[0] += acc.d0;
+                        D64[0] += a64.d0;
+                        for (int m = 0; m < 3; ++m) D64[1 + m] += a64.dx[m];
+                        for (int m = 0; m < 6; ++m) D64[4 + m] += a64.dP[m];
+                    }
+                } else {
+                    const float e = tp0_core<float, QH, PH, DIFF>(A.ex, g, ax, static_cast<float>(Y.a), acc);
+                    if (CROSS || j > i) e32 += e;
+                    if (++since_flush == PAIR_FLUSH) {
+                        since_flush = 0;
+                        e_row += e32;
+                        e32 = 0.0f;
+                        if (DIFF) {
+                            D64[0] += acc.d0;
 #pragma unroll
-                        for (int m = 0; m < 3; ++m) D64[1 + m] += acc.dx[m];
+                            for (int m = 0; m < 3; ++m) D64[1 + m] += acc.dx[m];
 #pragma unroll
-                        for (int m = 0; m < 6; ++m) D64[4 + m] += acc.dP[m];
-                        acc = PairAcc<float>{};
+                            for (int m = 0; m < 6; ++m) D64[4 + m] += acc.dP[m];
+                            acc = PairAcc<float>{};
+                        }
                     }
                 }
             }
+            e_row += e32;
+            if (DIFF) {
+                D64[0] += acc.d0;
+#pragma unroll
+                for (int m = 0; m < 3; ++m) D64[1 + m] += acc.dx[m];
+#pragma unroll
+                for (int m = 0; m < 6; ++m) D64[4 + m] += acc.dP[m];
+            }
         }
-        e_row += e32;
-        if (DIFF) {
-            D64[0] += acc.d0;
+        if constexpr (CROSS) {
+            e_row *= 0.5;
 #pragma unroll
-            for (int m = 0; m < 3; ++m) D64[1 + m] += acc.dx[m];
-#pragma unroll
-            for (int m = 0; m < 6; ++m) D64[4 + m] += acc.dP[m];
+            for (int m = 0; m < 10; ++m) D64[m] *= 0.5;
         }
-    }
-    if constexpr (CROSS) {
-        e_row *= 0.5;
+        // combine the LANES partial sums of a row (every lane of the warp takes part)
 #pragma unroll
-        for (int m = 0; m < 10; ++m) D64[m] *= 0.5;
-    }
-    // combine the LANES partial sums of a row (every lane of the warp takes part)
+        for (int off = 1; off < LANES; off <<= 1) {
+            e_row += __shfl_xor_sync(0xffffffffu, e_row, off);
+            if (DIFF) {
 #pragma unroll
-    for (int off = 1; off < LANES; off <<= 1) {
-        e_row += __shfl_xor_sync(0xffffffffu, e_row, off);
-        if (DIFF) {
-#pragma unroll
-            for (int m = 0; m < 10; ++m) D64[m] += __shfl_xor_sync(0xffffffffu, D64[m], off);
+                for (int m = 0; m < 10; ++m) D64[m] += __shfl_xor_sync(0xffffffffu, D64[m], off);
+            }
         }
-    }
-    if (DIFF && active && sub == 0) {
-        double* dst = A.D + 10 * static_cast<int64_t>(i);
+        if (DIFF && active && sub == 0) {
+            double* dst = A.D + 10 * static_cast<int64_t>(i);
 #pragma unroll
-        for (int m = 0; m < 10; ++m) dst[m] = D64[m];
+            for (int m = 0; m < 10; ++m) dst[m] = D64[m];
+        }
+        if (sub == 0) e_acc += e_row;
     }
-    if (sub != 0) e_row = 0.0;
     // deterministic energy reduction: per-block partial, last block sums all partials
     __shared__ double sh[PAIR_BLOCK / 32];
     __shared__ bool last;
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    e_row = warp_sum_f64(e_row);
-    if (lane == 0) sh[wib] = e_row;
+    const int wib = threadIdx.x >> 5;
+    double e_w = warp_sum_f64(e_acc);
+    if (lane == 0) sh[wib] = e_w;
     __syncthreads();
     if (threadIdx.x == 0) {
         double s = 0.0;
@@ -529,8 +546,34 @@ __global__ void __launch_bounds__(PAIR_BLOCK) k_tp0_pairs(PairArgs A)
             for (int w = 0; w < (blockDim.x >> 5); ++w) t2 += sh[w];
             *A.energy_out = t2;
             *A.done = 0u;
+            *A.rows_taken = 0u;
         }
     }
+}
+
+// Resident grid of a pair kernel: blocks per SM at its register use times the SM count,
+// no more than the rows need. Computed once per kernel and device.
+inline int pair_grid(const void* kernel, int rows, int lanes)
+{
+    static std::mutex mu;
+    static std::map<std::pair<const void*, int>, int> resident;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    int r = 0;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        auto it = resident.find({kernel, dev});
+        if (it != resident.end()) r = it->second;
+    }
+    if (r == 0) {
+        int per_sm = 0, sms = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, PAIR_BLOCK, 0);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        r = std::max(1, per_sm) * std::max(1, sms);
+        std::lock_guard<std::mutex> lock(mu);
+        resident[{kernel, dev}] = r;
+    }
+    return std::max(1, std::min(r, pair_blocks(rows, lanes)));
 }
 
 // energy = near-field part + far-field part (the order evaluate() uses on the host)

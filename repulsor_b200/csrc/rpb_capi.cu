@@ -144,13 +144,23 @@ template <int QH, int PH>
 static void launch_pairs_t(rpb_mesh* m, const PairArgs& An, const PairArgs& Af, bool diff, cudaEvent_t between)
 {
     if (An.rows > 0) {
-        if (diff) k_tp0_pairs<false, QH, PH, true, NEAR_LANES><<<m->near_blocks, PAIR_BLOCK, 0, m->stream>>>(An);
-        else k_tp0_pairs<false, QH, PH, false, NEAR_LANES><<<m->near_blocks, PAIR_BLOCK, 0, m->stream>>>(An);
+        if (diff) {
+            auto k = k_tp0_pairs<false, QH, PH, true, NEAR_LANES>;
+            k<<<pair_grid(reinterpret_cast<const void*>(k), An.rows, NEAR_LANES), PAIR_BLOCK, 0, m->stream>>>(An);
+        } else {
+            auto k = k_tp0_pairs<false, QH, PH, false, NEAR_LANES>;
+            k<<<pair_grid(reinterpret_cast<const void*>(k), An.rows, NEAR_LANES), PAIR_BLOCK, 0, m->stream>>>(An);
+        }
     }
     if (between) cudaEventRecord(between, m->stream);
     if (Af.rows > 0) {
-        if (diff) k_tp0_pairs<true, QH, PH, true, FAR_LANES><<<m->far_blocks, PAIR_BLOCK, 0, m->stream>>>(Af);
-        else k_tp0_pairs<true, QH, PH, false, FAR_LANES><<<m->far_blocks, PAIR_BLOCK, 0, m->stream>>>(Af);
+        if (diff) {
+            auto k = k_tp0_pairs<true, QH, PH, true, FAR_LANES>;
+            k<<<pair_grid(reinterpret_cast<const void*>(k), Af.rows, FAR_LANES), PAIR_BLOCK, 0, m->stream>>>(Af);
+        } else {
+            auto k = k_tp0_pairs<true, QH, PH, false, FAR_LANES>;
+            k<<<pair_grid(reinterpret_cast<const void*>(k), Af.rows, FAR_LANES), PAIR_BLOCK, 0, m->stream>>>(Af);
+        }
     }
 }
 
@@ -165,10 +175,12 @@ rpb_status launch_pairs(rpb_mesh* m, const TPExp& ex, bool diff, cudaEvent_t bet
     An.rp = m->near.rp.ptr; An.ci = m->near.ci.ptr; An.data = m->P_pair.ptr; An.D = m->D_near.ptr;
     An.order = m->near_order.ptr;
     An.block_energy = m->block_energy.ptr; An.done = m->done.ptr; An.energy_out = m->energy.ptr;
+    An.rows_taken = m->done.ptr + 2;
     Af.rows = m->far.nnz > 0 ? m->NC : 0;
     Af.rp = m->far.rp.ptr; Af.ci = m->far.ci.ptr; Af.data = m->C_pair.ptr; Af.D = m->D_far.ptr;
     Af.order = m->far_order.ptr;
     Af.block_energy = m->block_energy.ptr + m->near_blocks; Af.done = m->done.ptr + 1; Af.energy_out = m->energy.ptr + 1;
+    Af.rows_taken = m->done.ptr + 3;
     if (An.rows == 0) {
         RPB_CUDA(cudaMemsetAsync(m->energy.ptr, 0, sizeof(double), m->stream));
         if (diff) RPB_CUDA(cudaMemsetAsync(m->D_near.ptr, 0, m->D_near.bytes(), m->stream));

@@ -87,12 +87,12 @@ void launch_cross(rpb_mesh* m, const PairArgs& An, const PairArgs& Af, bool diff
 {
     ObstacleState& O = *m->obstacle;
     if (An.rows > 0) {
-        if (diff) k_tp0_pairs<false, QH, PH, true, NEAR_LANES, true><<<O.near_blocks, PAIR_BLOCK, 0, m->stream>>>(An);
-        else k_tp0_pairs<false, QH, PH, false, NEAR_LANES, true><<<O.near_blocks, PAIR_BLOCK, 0, m->stream>>>(An);
+        auto k = diff ? k_tp0_pairs<false, QH, PH, true, NEAR_LANES, true> : k_tp0_pairs<false, QH, PH, false, NEAR_LANES, true>;
+        k<<<std::min(O.near_blocks, pair_grid(reinterpret_cast<const void*>(k), An.rows, NEAR_LANES)), PAIR_BLOCK, 0, m->stream>>>(An);
     }
     if (Af.rows > 0) {
-        if (diff) k_tp0_pairs<true, QH, PH, true, FAR_LANES, true><<<O.far_blocks, PAIR_BLOCK, 0, m->stream>>>(Af);
-        else k_tp0_pairs<true, QH, PH, false, FAR_LANES, true><<<O.far_blocks, PAIR_BLOCK, 0, m->stream>>>(Af);
+        auto k = diff ? k_tp0_pairs<true, QH, PH, true, FAR_LANES, true> : k_tp0_pairs<true, QH, PH, false, FAR_LANES, true>;
+        k<<<std::min(O.far_blocks, pair_grid(reinterpret_cast<const void*>(k), Af.rows, FAR_LANES)), PAIR_BLOCK, 0, m->stream>>>(Af);
     }
 }
 
@@ -129,10 +129,12 @@ rpb_status evaluate_obstacle(rpb_mesh* m, double q, double p, bool diff, double 
     An.rp = O.near.rp.ptr; An.ci = O.near.ci.ptr; An.order = O.near_order.ptr;
     An.data = m->P_pair.ptr; An.col_data = O.mesh->P_pair.ptr; An.D = O.D_near.ptr;
     An.block_energy = O.block_energy.ptr; An.done = O.done.ptr; An.energy_out = O.energy.ptr;
+    An.rows_taken = O.done.ptr + 2;
     Af.rows = O.far.nnz > 0 ? m->NC : 0;
     Af.rp = O.far.rp.ptr; Af.ci = O.far.ci.ptr; Af.order = O.far_order.ptr;
     Af.data = m->C_pair.ptr; Af.col_data = O.mesh->C_pair.ptr; Af.D = O.D_far.ptr;
     Af.block_energy = O.block_energy.ptr + O.near_blocks; Af.done = O.done.ptr + 1; Af.energy_out = O.energy.ptr + 1;
+    Af.rows_taken = O.done.ptr + 3;
     if (An.rows == 0) {
         RPB_CUDA(cudaMemsetAsync(O.energy.ptr, 0, sizeof(double), m->stream));
         if (diff) RPB_CUDA(cudaMemsetAsync(O.D_near.ptr, 0, O.D_near.bytes(), m->stream));
@@ -194,7 +196,7 @@ rpb_status rpb_mesh_load_obstacle(rpb_mesh* m, rpb_mesh* obstacle)
     O->near_blocks = pair_blocks(m->N, NEAR_LANES);
     O->far_blocks = pair_blocks(m->NC, FAR_LANES);
     if (O->D_near.alloc(10 * static_cast<size_t>(m->N)) || O->D_far.alloc(10 * static_cast<size_t>(m->NC)) ||
-        O->block_energy.alloc(O->near_blocks + O->far_blocks) || O->energy.alloc(2) || O->done.alloc(2)) {
+        O->block_energy.alloc(O->near_blocks + O->far_blocks) || O->energy.alloc(2) || O->done.alloc(4)) {
         set_error("device allocation failed");
         return fail(RPB_ENOMEM);
     }

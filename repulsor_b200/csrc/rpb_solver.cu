@@ -61,6 +61,8 @@ struct SnArgs {
 constexpr int SN_BLOCK = 256;
 // widest supernode (3 x 8 bytes of shared memory per row: 24 KB at 1024)
 constexpr int kMaxSupernodeWidth = 1024;
+// levels with fewer supernodes than this are spread over their rows (two launches)
+constexpr int kSplitBelow = 64;
 
 template <bool LOWER>
 __global__ void __launch_bounds__(SN_BLOCK) k_sn_solve(SnArgs A)
@@ -120,6 +122,91 @@ __global__ void __launch_bounds__(SN_BLOCK) k_sn_solve(SnArgs A)
                 A.out[3 * static_cast<int64_t>(dst) + 1] = s1;
                 A.out[3 * static_cast<int64_t>(dst) + 2] = s2;
             }
+        }
+    }
+}
+
+// Levels with few, wide supernodes run as two launches over all their rows instead
+// (one warp per row, many CTAs): the external part into t (global), then y = D^{-1} t.
+struct SnSplitArgs {
+    const int* rows;          // rows of the level (factor order)
+    int nrows;
+    const int* sn_of;         // column -> supernode
+    const int* sn_begin;
+    const int64_t* rp;
+    const int* ci;
+    const double* val;
+    const int64_t* dinv_off;
+    const double* dinv;
+    const double* b;
+    const int* perm_in;
+    double* t;                // n x 3 scratch
+    double* y;
+    double* out;
+    const int* perm_out;
+};
+
+template <bool LOWER>
+__global__ void __launch_bounds__(SN_BLOCK) k_sn_external(SnSplitArgs A)
+{
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (w >= A.nrows) return;
+    const int row = A.rows[w];
+    const int s = A.sn_of[row];
+    const int c0 = A.sn_begin[s], c1 = A.sn_begin[s + 1];
+    double s0 = 0, s1 = 0, s2 = 0;
+    for (int64_t k = A.rp[row] + lane; k < A.rp[row + 1]; k += 32) {
+        const int j = A.ci[k];
+        if (LOWER ? (j < c0) : (j >= c1)) {
+            const double v = A.val[k];
+            s0 += v * A.y[3 * static_cast<int64_t>(j) + 0];
+            s1 += v * A.y[3 * static_cast<int64_t>(j) + 1];
+            s2 += v * A.y[3 * static_cast<int64_t>(j) + 2];
+        }
+    }
+    s0 = warp_sum_f64(s0);
+    s1 = warp_sum_f64(s1);
+    s2 = warp_sum_f64(s2);
+    if (lane == 0) {
+        const int src = A.perm_in ? A.perm_in[row] : row;
+        A.t[3 * static_cast<int64_t>(row) + 0] = A.b[3 * static_cast<int64_t>(src) + 0] - s0;
+        A.t[3 * static_cast<int64_t>(row) + 1] = A.b[3 * static_cast<int64_t>(src) + 1] - s1;
+        A.t[3 * static_cast<int64_t>(row) + 2] = A.b[3 * static_cast<int64_t>(src) + 2] - s2;
+    }
+}
+
+template <bool LOWER>
+__global__ void __launch_bounds__(SN_BLOCK) k_sn_dense(SnSplitArgs A)
+{
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (w >= A.nrows) return;
+    const int row = A.rows[w];
+    const int s = A.sn_of[row];
+    const int c0 = A.sn_begin[s], wd = A.sn_begin[s + 1] - c0, r = row - c0;
+    const double* D = A.dinv + A.dinv_off[s];
+    const int64_t o = LOWER ? static_cast<int64_t>(r) * (r + 1) / 2
+                            : static_cast<int64_t>(r) * wd - static_cast<int64_t>(r) * (r - 1) / 2;
+    const int cb = LOWER ? 0 : r, len = LOWER ? r + 1 : wd - r;
+    double s0 = 0, s1 = 0, s2 = 0;
+    for (int c = lane; c < len; c += 32) {
+        const double d = D[o + c];
+        const int64_t tc = 3 * static_cast<int64_t>(c0 + cb + c);
+        s0 += d * A.t[tc + 0];
+        s1 += d * A.t[tc + 1];
+        s2 += d * A.t[tc + 2];
+    }
+    s0 = warp_sum_f64(s0);
+    s1 = warp_sum_f64(s1);
+    s2 = warp_sum_f64(s2);
+    if (lane == 0) {
+        A.y[3 * static_cast<int64_t>(row) + 0] = s0;
+        A.y[3 * static_cast<int64_t>(row) + 1] = s1;
+        A.y[3 * static_cast<int64_t>(row) + 2] = s2;
+        if (A.out) {
+            const int dst = A.perm_out[row];
+            A.out[3 * static_cast<int64_t>(dst) + 0] = s0;
+            A.out[3 * static_cast<int64_t>(dst) + 1] = s1;
+            A.out[3 * static_cast<int64_t>(dst) + 2] = s2;
         }
     }
 }
@@ -301,8 +388,31 @@ static rpb_status ensure_h1(rpb_mesh* m)
     RPB_CUDA(up(s.dinv_off, SS.dinv_off));
     RPB_CUDA(up(s.dinv, SS.dinv));
     RPB_CUDA(up(s.dinvT, SS.dinvT));
+    // levels with fewer supernodes than kSplitBelow run split over their rows
+    std::vector<int> sn_of(m->nV);
+    for (int sn = 0; sn < SS.nsn; ++sn)
+        for (int c = SS.sn_begin[sn]; c < SS.sn_begin[sn + 1]; ++c) sn_of[c] = sn;
+    auto split_rows = [&](const std::vector<int>& lptr, const std::vector<int>& lsn, std::vector<int>& rptr,
+                          std::vector<int>& rows) {
+        const int L = static_cast<int>(lptr.size()) - 1;
+        rptr.assign(static_cast<size_t>(L) + 1, 0);
+        rows.clear();
+        for (int l = 0; l < L; ++l) {
+            if (lptr[l + 1] - lptr[l] < kSplitBelow)
+                for (int q = lptr[l]; q < lptr[l + 1]; ++q)
+                    for (int c = SS.sn_begin[lsn[q]]; c < SS.sn_begin[lsn[q] + 1]; ++c) rows.push_back(c);
+            rptr[l + 1] = static_cast<int>(rows.size());
+        }
+    };
+    std::vector<int> frows, brows;
+    split_rows(SS.fwd_level_ptr, SS.fwd_level_sn, s.fwd_split_ptr, frows);
+    split_rows(SS.bwd_level_ptr, SS.bwd_level_sn, s.bwd_split_ptr, brows);
+    RPB_CUDA(up(s.sn_of, sn_of));
+    RPB_CUDA(up(s.fwd_split_rows, frows));
+    RPB_CUDA(up(s.bwd_split_rows, brows));
     RPB_CUDA(s.tri.alloc(3 * static_cast<size_t>(m->nV)));
     RPB_CUDA(s.tmp.alloc(3 * static_cast<size_t>(m->nV)));
+    RPB_CUDA(s.tbuf.alloc(3 * static_cast<size_t>(m->nV)));
     RPB_CUDA(cudaStreamSynchronize(st));
     s.h1_version = m->geometry_version;
     return RPB_OK;
@@ -317,22 +427,41 @@ static rpb_status h1_solve(rpb_mesh* m, const double* b, double* out)
     A.sn_begin = s.sn_begin.ptr; A.dinv_off = s.dinv_off.ptr;
     A.rp = s.lo_rp.ptr; A.ci = s.lo_ci.ptr; A.val = s.lo_val.ptr; A.dinv = s.dinv.ptr;
     A.b = b; A.perm_in = s.perm.ptr; A.y = s.tri.ptr; A.out = nullptr; A.perm_out = nullptr;
-    for (int l = 0; l < s.sn_levels_fwd; ++l) {
-        A.level_sn = s.fwd_level_sn.ptr + s.fwd_level_ptr[l];
-        const int nsn = s.fwd_level_ptr[l + 1] - s.fwd_level_ptr[l];
-        const size_t smem = 3 * sizeof(double) * static_cast<size_t>(s.fwd_level_width[l]);
-        k_sn_solve<true><<<nsn, SN_BLOCK, smem, m->stream>>>(A);
-    }
+    SnSplitArgs P;
+    P.sn_of = s.sn_of.ptr; P.sn_begin = s.sn_begin.ptr; P.dinv_off = s.dinv_off.ptr; P.t = s.tbuf.ptr;
+    auto level = [&](const SnArgs& a, const int* level_sn, int nsn, int width, const int* rows, int nrows, bool lower) {
+        if (nrows > 0) {
+            P.rows = rows; P.nrows = nrows;
+            P.rp = a.rp; P.ci = a.ci; P.val = a.val; P.dinv = a.dinv;
+            P.b = a.b; P.perm_in = a.perm_in; P.y = a.y; P.out = a.out; P.perm_out = a.perm_out;
+            const int grid = (nrows + SN_BLOCK / 32 - 1) / (SN_BLOCK / 32);
+            if (lower) {
+                k_sn_external<true><<<grid, SN_BLOCK, 0, m->stream>>>(P);
+                k_sn_dense<true><<<grid, SN_BLOCK, 0, m->stream>>>(P);
+            } else {
+                k_sn_external<false><<<grid, SN_BLOCK, 0, m->stream>>>(P);
+                k_sn_dense<false><<<grid, SN_BLOCK, 0, m->stream>>>(P);
+            }
+            return;
+        }
+        SnArgs a2 = a;
+        a2.level_sn = level_sn;
+        const size_t smem = 3 * sizeof(double) * static_cast<size_t>(width);
+        if (lower) k_sn_solve<true><<<nsn, SN_BLOCK, smem, m->stream>>>(a2);
+        else k_sn_solve<false><<<nsn, SN_BLOCK, smem, m->stream>>>(a2);
+    };
+    for (int l = 0; l < s.sn_levels_fwd; ++l)
+        level(A, s.fwd_level_sn.ptr + s.fwd_level_ptr[l], s.fwd_level_ptr[l + 1] - s.fwd_level_ptr[l],
+              s.fwd_level_width[l], s.fwd_split_rows.ptr + s.fwd_split_ptr[l],
+              s.fwd_split_ptr[l + 1] - s.fwd_split_ptr[l], true);
     RPB_CUDA(cudaGetLastError());
     SnArgs U = A;
     U.rp = s.up_rp.ptr; U.ci = s.up_ci.ptr; U.val = s.up_val.ptr; U.dinv = s.dinvT.ptr;
     U.b = s.tri.ptr; U.perm_in = nullptr; U.y = s.tmp.ptr; U.out = out; U.perm_out = s.perm.ptr;
-    for (int l = 0; l < s.sn_levels_bwd; ++l) {
-        U.level_sn = s.bwd_level_sn.ptr + s.bwd_level_ptr[l];
-        const int nsn = s.bwd_level_ptr[l + 1] - s.bwd_level_ptr[l];
-        const size_t smem = 3 * sizeof(double) * static_cast<size_t>(s.bwd_level_width[l]);
-        k_sn_solve<false><<<nsn, SN_BLOCK, smem, m->stream>>>(U);
-    }
+    for (int l = 0; l < s.sn_levels_bwd; ++l)
+        level(U, s.bwd_level_sn.ptr + s.bwd_level_ptr[l], s.bwd_level_ptr[l + 1] - s.bwd_level_ptr[l],
+              s.bwd_level_width[l], s.bwd_split_rows.ptr + s.bwd_split_ptr[l],
+              s.bwd_split_ptr[l + 1] - s.bwd_split_ptr[l], false);
     RPB_CUDA(cudaGetLastError());
     return RPB_OK;
 }

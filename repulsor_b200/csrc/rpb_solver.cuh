@@ -22,10 +22,11 @@ struct Solver {
     int64_t h1_version = -1;
     std::vector<int> nd_perm;
     DevBuf<int64_t> lo_rp, up_rp, dinv_off;
-    DevBuf<int> lo_ci, up_ci, perm, sn_begin, fwd_level_sn, bwd_level_sn;
-    DevBuf<double> lo_val, up_val, dinv, dinvT, tri, tmp;
+    DevBuf<int> lo_ci, up_ci, perm, sn_begin, fwd_level_sn, bwd_level_sn, sn_of, fwd_split_rows, bwd_split_rows;
+    DevBuf<double> lo_val, up_val, dinv, dinvT, tri, tmp, tbuf;
     int sn_levels_fwd = 0, sn_levels_bwd = 0;
     std::vector<int> fwd_level_ptr, bwd_level_ptr, fwd_level_width, bwd_level_width;
+    std::vector<int> fwd_split_ptr, bwd_split_ptr;   // per level: rows of split levels (empty range: fused)
     double factor_seconds = 0;
     int64_t factor_nnz = 0;
     // statistics of the last Solve
