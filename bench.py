@@ -161,10 +161,14 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true")
     ap.add_argument("--no-solve", action="store_true", help="skip the Solve timings on the icosphere level-6 mesh")
+    ap.add_argument("--flow", action="store_true",
+                    help="only the full flow step on two linked tori (1,228,800 triangles) with an obstacle")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
         return run_reference(args)
+    if args.flow:
+        return run_flow(args)
 
     import numpy as np
     import torch
@@ -342,7 +346,6 @@ def solve_extras(rpb, M, tpm, V):
     net = LearnedPreconditioner(seed=1)
     hist = train(net, tpm, data, epochs=30, lr=1e-3, batch=4, seed=0)
     t2 = time.perf_counter()
-    net.attach(M)
     B = meshes.random_rhs(V.shape[0], seed=1003)
     res = {"workload": "icosphere level 6 (40,962 vertices), RHS N(0,1) projected off translations, tol 1e-6 "
                        "(true residual of the plain metric operator)",
@@ -350,9 +353,19 @@ def solve_extras(rpb, M, tpm, V):
                                   "0/4/16/48/128", "pairs": int(sum(d[1].shape[0] for d in data)),
                         "pair_generation_s": t1 - t0, "training_s": t2 - t1, "epochs": len(hist),
                         "loss_first_epoch": hist[0], "loss_last_epoch": hist[-1]}}
+    from repulsor_b200.learned import NPARAM_OUTPUT_OFFSET
+    prior = LearnedPreconditioner(seed=1)
+    p0 = prior.get_params()
+    p0[NPARAM_OUTPUT_OFFSET:] = 0.0          # output layer zero: every gain 1 (the untrained multilevel operator)
+    prior.set_params(p0)
     for name, pc, max_iter in (("plain_cg", rpb.PRECOND_NONE, 20000),
+                               ("multilevel_prior_fcg", rpb.PRECOND_LEARNED, 20000),
                                ("learned_fcg", rpb.PRECOND_LEARNED, 20000),
                                ("reference_precond_cg", rpb.PRECOND_REFERENCE, 2000)):
+        if name == "multilevel_prior_fcg":
+            prior.attach(M)
+        elif name == "learned_fcg":
+            net.attach(M)
         t = time.perf_counter()
         tpm.Solve(M, 1.0, B, max_iter=max_iter, tolerance=1e-6, precond=pc, strict=False)
         ms = 1e3 * (time.perf_counter() - t)
@@ -365,6 +378,67 @@ def solve_extras(rpb, M, tpm, V):
             res[name].update(h1_factor_seconds=info["factor_seconds"], h1_factor_nnz=info["factor_nnz"],
                              supernode_levels=info["supernode_levels"])
     return res
+
+
+def run_flow(args):
+    """Full flow step at scale: two linked tori (R=1, r=0.3, 480 x 640 grids, 1,228,800
+    triangles) with an icosphere level-5 obstacle of radius 0.3 at (0, 0, 2): energy +
+    differential (TangentPointEnergy0 + TangentPointObstacleEnergy), then the metric Solve
+    of the differential to 1e-6 by learned-preconditioned flexible CG (network trained on
+    seeded icospheres, time reported separately) with the reference preconditioner as
+    fallback. One step; times are wall clock around each public call."""
+    import numpy as np
+    import torch
+
+    import repulsor_b200 as rpb
+    from repulsor_b200 import meshes
+    from repulsor_b200.learned import LearnedPreconditioner, train, training_pairs
+
+    torch.cuda.set_device(0)
+    out = {"metric": "full flow step (energy+grad, learned FCG solve to 1e-6)", "unit": "s",
+           "workload": "two linked tori 480x640 (614,400 vertices, 1,228,800 triangles) + icosphere L5 obstacle "
+                       "r=0.3 at (0,0,2), q=6 p=12 theta=0.5"}
+    t = time.perf_counter()
+    V, S = meshes.linked_tori()
+    M = rpb.SimplicialMesh(V, S)
+    Vo, So = meshes.icosphere(level=5, radius=0.3, centre=(0.0, 0.0, 2.0))
+    M.LoadObstacle(rpb.SimplicialMesh(Vo, So))
+    out["setup_s"] = time.perf_counter() - t
+    st = M.stats()
+    out["mesh"] = {k: st[k] for k in ("cluster_count", "near_nnz", "far_nnz", "tree_build_seconds", "device_bytes")}
+    out["obstacle"] = M.obstacle_stats()
+    tpe, tpo = rpb.TangentPointEnergy0(Q, P), rpb.TangentPointObstacleEnergy(Q, P)
+    tpm = rpb.TangentPointMetric0(Q, P)
+    D = np.zeros_like(V)
+    for _ in range(2):
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        E = tpe.Differential(M, 1.0, 0.0, D)
+        E += tpo.Differential(M, 1.0, 1.0, D)
+        out["energy_grad_s"] = time.perf_counter() - t
+    out["energy"] = E
+    t = time.perf_counter()
+    data = []
+    for lvl, seed in ((4, 2001), (5, 2002)):
+        Vt, St = meshes.icosphere_sh(level=lvl, seed=seed)
+        Mt = rpb.SimplicialMesh(Vt, St)
+        R, Er = training_pairs(Mt, tpm, n_rhs=4, checkpoints=(0, 4, 16, 48, 128), seed=seed, exact_tol=1e-9)
+        data.append((Mt, R, Er))
+    net = LearnedPreconditioner(seed=1)
+    train(net, tpm, data, epochs=30, lr=1e-3, batch=4, seed=0)
+    out["training_s"] = time.perf_counter() - t
+    net.attach(M)
+    B = D - D.mean(0)
+    t = time.perf_counter()
+    tpm.Solve(M, 1.0, B, max_iter=20000, tolerance=1e-6,
+              precond=rpb.PRECOND_LEARNED, strict=False)
+    out["solve_s"] = time.perf_counter() - t
+    info = tpm.SolveInfo(M)
+    out["solve"] = {"iterations": info["iterations"], "fallback_iteration": info["fallback_iteration"],
+                    "rel_residual": [float(x) for x in tpm.Solver_RelativeResiduals()]}
+    out["value"] = out["energy_grad_s"] + out["solve_s"]
+    print(json.dumps(out))
+    return 0
 
 
 if __name__ == "__main__":

@@ -15,10 +15,9 @@
 #pragma once
 
 #include <algorithm>
-#include <map>
-#include <mutex>
+#include <cstdint>
 #include <type_traits>
-#include <utility>
+#include <vector>
 
 #include "rpb_device.cuh"
 
@@ -392,7 +391,7 @@ struct PairArgs {
     double* D;                // rows x 10 (d0, dx[3], dP[6]) centred moment derivatives
     double* block_energy;     // gridDim.x
     unsigned* done;           // 1 counter, zero between launches
-    unsigned* rows_taken;     // 1 counter, zero between launches (dynamic row distribution)
+    const int* block_rows;    // gridDim.x + 1 slot ranges of the blocks (null: PAIR_BLOCK / LANES slots each)
     double* energy_out;       // 1
     TPExp ex;
     float close_factor;       // FP64 path for near pairs with r < close_factor (d_i + d_j)
@@ -415,9 +414,10 @@ constexpr int pair_blocks(int rows, int lanes) { return (rows * lanes + PAIR_BLO
 // CROSS: rows are the mesh's, columns the obstacle's (a non-symmetric block cluster tree):
 // every pair counts, energy and derivatives carry the symmetry factor 1/2
 // (src/FMM/FMM_Kernel.hpp:43) and the obstacle's derivatives are not formed.
-// The grid is the resident set (pair_grid): warps take the next 32/LANES rows of the
-// processing order from a global counter until none are left, so long and short rows
-// balance across the SMs and no block waits on a slow sibling at its end.
+// Block b takes the contiguous slot range block_rows[b] .. block_rows[b+1] of the processing
+// order (ranges of equal nonzero count, so blocks carry equal work and an SM's rows stay
+// neighbours in tree order); inside a block, warps take the next 32/LANES rows from a
+// shared counter, so long and short rows balance across the block's warps.
 template <bool FAR, int QH, int PH, bool DIFF, int LANES, bool CROSS = false>
 __global__ void __launch_bounds__(PAIR_BLOCK) k_tp0_pairs(PairArgs A)
 {
@@ -428,14 +428,19 @@ __global__ void __launch_bounds__(PAIR_BLOCK) k_tp0_pairs(PairArgs A)
     const Datum* cols = CROSS ? static_cast<const Datum*>(A.col_data) : base;
     const int lane = threadIdx.x & 31;
     const int grp = lane / LANES, sub = lane & (LANES - 1);
+    const int slot_begin = A.block_rows ? A.block_rows[blockIdx.x] : blockIdx.x * (PAIR_BLOCK / LANES);
+    const int slot_end = A.block_rows ? A.block_rows[blockIdx.x + 1] : min(A.rows, slot_begin + PAIR_BLOCK / LANES);
+    __shared__ int next_slot;
+    if (threadIdx.x == 0) next_slot = slot_begin;
+    __syncthreads();
     double e_acc = 0.0;
     for (;;) {
         int first = 0;
-        if (lane == 0) first = static_cast<int>(atomicAdd(A.rows_taken, static_cast<unsigned>(ROWS_PER_WARP)));
+        if (lane == 0) first = atomicAdd(&next_slot, ROWS_PER_WARP);
         first = __shfl_sync(0xffffffffu, first, 0);
-        if (first >= A.rows) break;
+        if (first >= slot_end) break;
         const int slot = first + grp;
-        const bool active = slot < A.rows;
+        const bool active = slot < slot_end;
         double e_row = 0.0;
         double D64[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
         int i = 0;
@@ -447,9 +452,20 @@ __global__ void __launch_bounds__(PAIR_BLOCK) k_tp0_pairs(PairArgs A)
             float e32 = 0.0f;
             int since_flush = 0;
             const int64_t k0 = A.rp[i], k1 = A.rp[i + 1];
+            // software pipeline: the next column's datum is in flight while this pair computes
+            int j_next = 0;
+            Datum Y_next;
+            if (k0 + sub < k1) {
+                j_next = __ldg(A.ci + k0 + sub);
+                Y_next = load_datum(cols, j_next);
+            }
             for (int64_t k = k0 + sub; k < k1; k += LANES) {
-                const int j = __ldg(A.ci + k);
-                const Datum Y = load_datum(cols, j);
+                const int j = j_next;
+                const Datum Y = Y_next;
+                if (k + LANES < k1) {
+                    j_next = __ldg(A.ci + k + LANES);
+                    Y_next = load_datum(cols, j_next);
+                }
                 Proj<float> g;
                 if constexpr (FAR) project_clusters(X, Y, g);
                 else project_prims(A.dom, X, Y, g);
@@ -546,34 +562,32 @@ __global__ void __launch_bounds__(PAIR_BLOCK) k_tp0_pairs(PairArgs A)
             for (int w = 0; w < (blockDim.x >> 5); ++w) t2 += sh[w];
             *A.energy_out = t2;
             *A.done = 0u;
-            *A.rows_taken = 0u;
         }
     }
 }
 
-// Resident grid of a pair kernel: blocks per SM at its register use times the SM count,
-// no more than the rows need. Computed once per kernel and device.
-inline int pair_grid(const void* kernel, int rows, int lanes)
+// Slot ranges of the pair-kernel blocks: the rows in processing order (row lengths
+// `len`) cut into contiguous ranges of about equal nonzero count, about
+// PAIR_BLOCK / lanes * mean row length nonzeros each. Returns blocks + 1 offsets.
+inline std::vector<int> pair_block_ranges(const std::vector<int64_t>& len, int lanes)
 {
-    static std::mutex mu;
-    static std::map<std::pair<const void*, int>, int> resident;
-    int dev = 0;
-    cudaGetDevice(&dev);
-    int r = 0;
-    {
-        std::lock_guard<std::mutex> lock(mu);
-        auto it = resident.find({kernel, dev});
-        if (it != resident.end()) r = it->second;
+    const int rows = static_cast<int>(len.size());
+    int64_t nnz = 0;
+    for (int64_t x : len) nnz += x;
+    std::vector<int> r{0};
+    if (rows == 0) return r;
+    const int64_t rows_per_block = PAIR_BLOCK / lanes;
+    const int64_t per = std::max<int64_t>(1, (nnz * rows_per_block + rows - 1) / rows);
+    int64_t acc = 0;
+    for (int i = 0; i < rows; ++i) {
+        acc += std::max<int64_t>(len[i], 1);
+        if (acc >= per && i + 1 < rows) {
+            r.push_back(i + 1);
+            acc = 0;
+        }
     }
-    if (r == 0) {
-        int per_sm = 0, sms = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, PAIR_BLOCK, 0);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        r = std::max(1, per_sm) * std::max(1, sms);
-        std::lock_guard<std::mutex> lock(mu);
-        resident[{kernel, dev}] = r;
-    }
-    return std::max(1, std::min(r, pair_blocks(rows, lanes)));
+    r.push_back(rows);
+    return r;
 }
 
 // energy = near-field part + far-field part (the order evaluate() uses on the host)

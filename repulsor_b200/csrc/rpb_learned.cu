@@ -84,6 +84,33 @@ struct MlpArgs {
     float* pre2;              // n x NH (training only)
 };
 
+// o = MLP(f) with the FP32 copy of the weights in shared memory; the pre-activations are
+// written to pre1/pre2 when those are non-null (training)
+__device__ __forceinline__ void mlp_eval(const float* sw, const float* f, float* o, float* pre1, float* pre2)
+{
+    float h1[NH];
+#pragma unroll 4
+    for (int j = 0; j < NH; ++j) {
+        float s = sw[OFF_B1 + j];
+#pragma unroll
+        for (int k = 0; k < NF; ++k) s = fmaf(sw[OFF_W1 + NF * j + k], f[k], s);
+        if (pre1) pre1[j] = s;
+        h1[j] = gelu(s);
+    }
+    o[0] = sw[OFF_B3 + 0];
+    o[1] = sw[OFF_B3 + 1];
+    o[2] = sw[OFF_B3 + 2];
+    for (int j = 0; j < NH; ++j) {
+        float s = sw[OFF_B2 + j];
+#pragma unroll
+        for (int k = 0; k < NH; ++k) s = fmaf(sw[OFF_W2 + NH * j + k], h1[k], s);
+        if (pre2) pre2[j] = s;
+        const float h2 = gelu(s);
+#pragma unroll
+        for (int q = 0; q < NO; ++q) o[q] = fmaf(sw[OFF_W3 + NH * q + j], h2, o[q]);
+    }
+}
+
 __global__ void __launch_bounds__(128) k_mlp_forward(MlpArgs A)
 {
     extern __shared__ float sw[];
@@ -93,25 +120,9 @@ __global__ void __launch_bounds__(128) k_mlp_forward(MlpArgs A)
     float f[NF];
 #pragma unroll
     for (int k = 0; k < NF; ++k) f[k] = A.F[NF * static_cast<int64_t>(c) + k];
-    float h1[NH];
-#pragma unroll 4
-    for (int j = 0; j < NH; ++j) {
-        float s = sw[OFF_B1 + j];
-#pragma unroll
-        for (int k = 0; k < NF; ++k) s = fmaf(sw[OFF_W1 + NF * j + k], f[k], s);
-        if (A.pre1) A.pre1[NH * static_cast<int64_t>(c) + j] = s;
-        h1[j] = gelu(s);
-    }
-    float o[NO] = {sw[OFF_B3 + 0], sw[OFF_B3 + 1], sw[OFF_B3 + 2]};
-    for (int j = 0; j < NH; ++j) {
-        float s = sw[OFF_B2 + j];
-#pragma unroll
-        for (int k = 0; k < NH; ++k) s = fmaf(sw[OFF_W2 + NH * j + k], h1[k], s);
-        if (A.pre2) A.pre2[NH * static_cast<int64_t>(c) + j] = s;
-        const float h2 = gelu(s);
-#pragma unroll
-        for (int q = 0; q < NO; ++q) o[q] = fmaf(sw[OFF_W3 + NH * q + j], h2, o[q]);
-    }
+    float o[NO];
+    mlp_eval(sw, f, o, A.pre1 ? A.pre1 + NH * static_cast<int64_t>(c) : nullptr,
+             A.pre2 ? A.pre2 + NH * static_cast<int64_t>(c) : nullptr);
 #pragma unroll
     for (int q = 0; q < NO; ++q) A.O[NO * static_cast<int64_t>(c) + q] = o[q];
 }
@@ -230,96 +241,237 @@ __global__ void k_adam(int n, float* theta, __nv_bfloat16* w16, const float* g, 
 }
 
 // ------------------------------------------------------------------------------------------
-// features, correction and the adjoint of the correction
+// The preconditioner application in four launches:
+//   k_prim_scan     primitive moments a_i mean(r) -> in-block prefix sums; sum of |r|^2
+//   k_scan_totals   prefix sums of the block totals; the global sum of |r|^2
+//   k_cluster_mlp   per cluster: R_C (and its children's) as prefix-sum differences,
+//                   16 features, the MLP, gains, c_C = g_C R_C / A_C; sum_C A_C c_C
+//   k_vertex_expand z_v = sum_{i at v} w_i sum_{C containing i} c_C - mean(z)
 // ------------------------------------------------------------------------------------------
-struct FeatArgs {
-    int NC, max_depth;
-    const ClusterDatum* C_pair;
-    const double* C_an;       // NC x 3: sum of a n over the cluster
-    const double* Rc;         // NC x 3: cluster residual moments
-    const int* C_left;
-    const int* C_right;
-    const int* C_depth;
-    const float* C_diam;
-    const double* scale;      // global RMS residual s
-    float* F;                 // NC x NF
-};
-
-__global__ void k_features(FeatArgs A)
-{
-    const int C = blockIdx.x * blockDim.x + threadIdx.x;
-    if (C >= A.NC) return;
-    const double s = fmax(*A.scale, 1e-300);
-    const ClusterDatum cd = load_datum(A.C_pair, C);
-    const ClusterDatum root = load_datum(A.C_pair, 0);
-    const double dr = fmax(static_cast<double>(A.C_diam[0]), 1e-300);
-    float f[NF];
-    const double* R = A.Rc + 3 * static_cast<int64_t>(C);
-    for (int k = 0; k < 3; ++k) f[k] = static_cast<float>(R[k] / (cd.a * s));
-    for (int k = 0; k < 3; ++k) f[3 + k] = static_cast<float>((cd.c[k] - root.c[k]) / dr);
-    for (int k = 0; k < 3; ++k) f[6 + k] = static_cast<float>(A.C_an[3 * static_cast<int64_t>(C) + k] / cd.a);
-    f[9] = static_cast<float>(log(cd.a / root.a) / 10.0);
-    f[10] = static_cast<float>(log(fmax(static_cast<double>(A.C_diam[C]), 1e-300) / dr) / 10.0);
-    f[11] = static_cast<float>(A.C_depth[C]) / static_cast<float>(max(A.max_depth, 1));
-    for (int k = 12; k < 16; ++k) f[k] = 0.0f;
-    const int L = A.C_left[C], Rr = A.C_right[C];
-    auto nrm = [&](int X) {
-        const double* q = A.Rc + 3 * static_cast<int64_t>(X);
-        return sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2]);
-    };
-    auto nrm2 = [&](int X, int Y) {
-        const double* q = A.Rc + 3 * static_cast<int64_t>(X);
-        const double* t = A.Rc + 3 * static_cast<int64_t>(Y);
-        const double a0 = q[0] + t[0], a1 = q[1] + t[1], a2 = q[2] + t[2];
-        return sqrt(a0 * a0 + a1 * a1 + a2 * a2);
-    };
-    if (L >= 0) {
-        const double aL = load_datum(A.C_pair, L).a, aR = load_datum(A.C_pair, Rr).a;
-        f[12] = static_cast<float>(nrm(L) / (aL * s));
-        f[13] = static_cast<float>(nrm(Rr) / (aR * s));
-        if (A.C_left[L] >= 0) f[14] = static_cast<float>(nrm2(A.C_left[L], A.C_right[L]) / (aL * s));
-        if (A.C_left[Rr] >= 0) f[15] = static_cast<float>(nrm2(A.C_left[Rr], A.C_right[Rr]) / (aR * s));
-    }
-    for (int k = 0; k < NF; ++k) A.F[NF * static_cast<int64_t>(C) + k] = f[k];
-}
-
+constexpr int GAIN_BLOCK = 128;
 // Gains g_C = exp(clamp(o_C)) keep z . r > 0 for every residual (flexible CG never meets
 // r . z <= 0) and bound the nonlinearity of the preconditioner to [e^-3, e^3] times the
 // fixed multilevel operator.
 constexpr float GAIN_CLAMP = 3.0f;
 
-// c_C = g_C * R_C / A_C per component
-__global__ void k_cluster_coeffs(int NC, const float* O, const double* Rc, const ClusterDatum* C_pair, double* c)
-{
-    const int C = blockIdx.x * blockDim.x + threadIdx.x;
-    if (C >= NC) return;
-    const double inv_a = 1.0 / load_datum(C_pair, C).a;
-    for (int q = 0; q < 3; ++q) {
-        const float o = fminf(fmaxf(O[3 * static_cast<int64_t>(C) + q], -GAIN_CLAMP), GAIN_CLAMP);
-        c[3 * static_cast<int64_t>(C) + q] = exp(static_cast<double>(o)) * Rc[3 * static_cast<int64_t>(C) + q] * inv_a;
-    }
-}
+struct PrimScanArgs {
+    int N, nV, size;
+    const int* pre_cols;
+    const double* pre_vals;
+    const double* R;          // n_v x 3
+    double* local;            // N x 3 in-block exclusive prefix sums
+    double* blocks;           // (nb + 1) x 3 block totals -> exclusive prefix (row nb: total)
+    double* sq_part;          // nb partial sums of |r|^2
+};
 
-// Z_i = sum over the clusters containing primitive i of c_C (PercolateDown + ClustersToPrimitives)
-__global__ void k_expand_clusters(int N, const int* leaf_of, const int* C_parent, const double* c, double* Z)
+__global__ void __launch_bounds__(SCAN_BLOCK) k_prim_scan(PrimScanArgs A)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= N) return;
-    double z0 = 0, z1 = 0, z2 = 0;
-    for (int C = leaf_of[i]; C >= 0; C = C_parent[C]) {
-        z0 += c[3 * static_cast<int64_t>(C)];
-        z1 += c[3 * static_cast<int64_t>(C) + 1];
-        z2 += c[3 * static_cast<int64_t>(C) + 2];
+    double v[3] = {0, 0, 0}, tot[3];
+    if (i < A.N)
+        for (int l = 0; l < A.size; ++l) {
+            const int u = A.pre_cols[A.size * i + l];
+            const double w = A.pre_vals[(4 * static_cast<int64_t>(i)) * A.size + l];
+            v[0] += w * A.R[3 * static_cast<int64_t>(u)];
+            v[1] += w * A.R[3 * static_cast<int64_t>(u) + 1];
+            v[2] += w * A.R[3 * static_cast<int64_t>(u) + 2];
+        }
+    block_exclusive_scan<3>(v, tot);
+    if (i < A.N)
+        for (int k = 0; k < 3; ++k) A.local[3 * static_cast<int64_t>(i) + k] = v[k];
+    if (threadIdx.x < 3) A.blocks[3 * static_cast<int64_t>(blockIdx.x) + threadIdx.x] = tot[threadIdx.x];
+    // |r|^2 over the vertices, grid-strided
+    double sq = 0;
+    for (int u = i; u < A.nV; u += gridDim.x * blockDim.x)
+        for (int k = 0; k < 3; ++k) {
+            const double x = A.R[3 * static_cast<int64_t>(u) + k];
+            sq += x * x;
+        }
+    __shared__ double sh[SCAN_BLOCK / 32];
+    sq = warp_sum_f64(sq);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = sq;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0;
+        for (int w = 0; w < SCAN_BLOCK / 32; ++w) t += sh[w];
+        A.sq_part[blockIdx.x] = t;
     }
-    Z[3 * static_cast<int64_t>(i)] = z0;
-    Z[3 * static_cast<int64_t>(i) + 1] = z1;
-    Z[3 * static_cast<int64_t>(i) + 2] = z2;
 }
 
-// z_v = sum_{(i,l) at v} w_il Z_i  (w = a/(n+1), the averaging row of Pre: the transpose
-// of the primitive moments, so that the fixed part of M is symmetric)
-__global__ void k_vertex_sum(int nV, int size, const int* vp_rp, const int* vp_slot, const double* pre_vals,
-                             const double* Z, double* z)
+// one block: exclusive prefix of the nb block totals (row nb: the total) and the scale
+// s = sqrt(sum |r|^2 / (3 n_v))
+__global__ void __launch_bounds__(SCAN_BLOCK) k_scan_totals(int nb, int nV, double* blocks, const double* sq_part,
+                                                            double* scale)
+{
+    double sq = 0;
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) sq += sq_part[b];
+    __shared__ double sh[SCAN_BLOCK / 32];
+    sq = warp_sum_f64(sq);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = sq;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0;
+        for (int w = 0; w < SCAN_BLOCK / 32; ++w) t += sh[w];
+        *scale = sqrt(t / (3.0 * nV));
+    }
+    __syncthreads();
+    __shared__ double carry[3];
+    if (threadIdx.x < 3) carry[threadIdx.x] = 0.0;
+    __syncthreads();
+    for (int base = 0; base < nb; base += SCAN_BLOCK) {
+        const int i = base + threadIdx.x;
+        double v[3], tot[3];
+        for (int k = 0; k < 3; ++k) v[k] = (i < nb) ? blocks[3 * static_cast<int64_t>(i) + k] : 0.0;
+        block_exclusive_scan<3>(v, tot);
+        if (i < nb)
+            for (int k = 0; k < 3; ++k) blocks[3 * static_cast<int64_t>(i) + k] = carry[k] + v[k];
+        __syncthreads();
+        if (threadIdx.x < 3) carry[threadIdx.x] += tot[threadIdx.x];
+        __syncthreads();
+    }
+    if (threadIdx.x < 3) blocks[3 * static_cast<int64_t>(nb) + threadIdx.x] = carry[threadIdx.x];
+}
+
+struct ClusterMlpArgs {
+    int N, NC, nV, max_depth;
+    const __nv_bfloat16* w;
+    const ClusterDatum* C_pair;
+    const double* C_an;       // NC x 3: sum of a n over the cluster
+    const int* C_begin;
+    const int* C_end;
+    const int* C_left;
+    const int* C_right;
+    const int* C_depth;
+    const float* C_diam;
+    const double* local;      // prefix sums of the primitive moments (k_prim_scan / k_scan_totals)
+    const double* blocks;
+    const double* scale;
+    double* c;                // NC x 3: coefficients
+    double* csum_part;        // gridDim.x x 3: partial sums of A_C c_C
+    unsigned* done;           // last-block counter (zero between launches)
+    double* zmean;            // 3: sum_C A_C c_C / n_v = mean of z before its removal
+    // training only (may be null)
+    float* F;                 // NC x NF
+    float* O;                 // NC x NO
+    float* pre1;              // NC x NH
+    float* pre2;              // NC x NH
+    double* Rc;               // NC x 3
+};
+
+__device__ __forceinline__ void prefix_at(const double* local, const double* blocks, int N, int k, double* out)
+{
+    const int nb = (N + SCAN_BLOCK - 1) / SCAN_BLOCK;
+    if (k < N) {
+        for (int q = 0; q < 3; ++q) out[q] = blocks[3 * static_cast<int64_t>(k / SCAN_BLOCK) + q] + local[3 * static_cast<int64_t>(k) + q];
+    } else {
+        for (int q = 0; q < 3; ++q) out[q] = blocks[3 * static_cast<int64_t>(nb) + q];
+    }
+}
+
+__device__ __forceinline__ void cluster_moment(const ClusterMlpArgs& A, int C, double* R)
+{
+    double sb[3], se[3];
+    prefix_at(A.local, A.blocks, A.N, A.C_begin[C], sb);
+    prefix_at(A.local, A.blocks, A.N, A.C_end[C], se);
+    for (int q = 0; q < 3; ++q) R[q] = se[q] - sb[q];
+}
+
+__global__ void __launch_bounds__(GAIN_BLOCK) k_cluster_mlp(ClusterMlpArgs A)
+{
+    extern __shared__ float sw[];
+    stage_weights(A.w, sw);
+    const int C = blockIdx.x * blockDim.x + threadIdx.x;
+    double cs[3] = {0, 0, 0};
+    if (C < A.NC) {
+        const double s = fmax(*A.scale, 1e-300);
+        const ClusterDatum cd = load_datum(A.C_pair, C);
+        const ClusterDatum root = load_datum(A.C_pair, 0);
+        const double dr = fmax(static_cast<double>(A.C_diam[0]), 1e-300);
+        double R[3];
+        cluster_moment(A, C, R);
+        float f[NF];
+        for (int k = 0; k < 3; ++k) f[k] = static_cast<float>(R[k] / (cd.a * s));
+        for (int k = 0; k < 3; ++k) f[3 + k] = static_cast<float>((cd.c[k] - root.c[k]) / dr);
+        for (int k = 0; k < 3; ++k) f[6 + k] = static_cast<float>(A.C_an[3 * static_cast<int64_t>(C) + k] / cd.a);
+        f[9] = static_cast<float>(log(cd.a / root.a) / 10.0);
+        f[10] = static_cast<float>(log(fmax(static_cast<double>(A.C_diam[C]), 1e-300) / dr) / 10.0);
+        f[11] = static_cast<float>(A.C_depth[C]) / static_cast<float>(max(A.max_depth, 1));
+        for (int k = 12; k < 16; ++k) f[k] = 0.0f;
+        const int L = A.C_left[C], Rr = A.C_right[C];
+        if (L >= 0) {
+            const double aL = load_datum(A.C_pair, L).a, aR = load_datum(A.C_pair, Rr).a;
+            double q[3];
+            cluster_moment(A, L, q);
+            f[12] = static_cast<float>(sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2]) / (aL * s));
+            cluster_moment(A, Rr, q);
+            f[13] = static_cast<float>(sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2]) / (aR * s));
+            // children of L together span L: R_LL + R_LR = R_L (as in the reference tree, a
+            // cluster is the union of its children); the grandchildren feature uses them
+            if (A.C_left[L] >= 0) {
+                double a[3], b[3];
+                cluster_moment(A, A.C_left[L], a);
+                cluster_moment(A, A.C_right[L], b);
+                f[14] = static_cast<float>(sqrt((a[0] + b[0]) * (a[0] + b[0]) + (a[1] + b[1]) * (a[1] + b[1]) +
+                                                (a[2] + b[2]) * (a[2] + b[2])) / (aL * s));
+            }
+            if (A.C_left[Rr] >= 0) {
+                double a[3], b[3];
+                cluster_moment(A, A.C_left[Rr], a);
+                cluster_moment(A, A.C_right[Rr], b);
+                f[15] = static_cast<float>(sqrt((a[0] + b[0]) * (a[0] + b[0]) + (a[1] + b[1]) * (a[1] + b[1]) +
+                                                (a[2] + b[2]) * (a[2] + b[2])) / (aR * s));
+            }
+        }
+        float o[NO];
+        mlp_eval(sw, f, o, A.pre1 ? A.pre1 + NH * static_cast<int64_t>(C) : nullptr,
+                 A.pre2 ? A.pre2 + NH * static_cast<int64_t>(C) : nullptr);
+        const double inv_a = 1.0 / cd.a;
+        for (int q = 0; q < 3; ++q) {
+            const float oc = fminf(fmaxf(o[q], -GAIN_CLAMP), GAIN_CLAMP);
+            const double cq = exp(static_cast<double>(oc)) * R[q] * inv_a;
+            A.c[3 * static_cast<int64_t>(C) + q] = cq;
+            cs[q] = cd.a * cq;
+        }
+        if (A.F)
+            for (int k = 0; k < NF; ++k) A.F[NF * static_cast<int64_t>(C) + k] = f[k];
+        if (A.O)
+            for (int q = 0; q < NO; ++q) A.O[NO * static_cast<int64_t>(C) + q] = o[q];
+        if (A.Rc)
+            for (int q = 0; q < 3; ++q) A.Rc[3 * static_cast<int64_t>(C) + q] = R[q];
+    }
+    // sum_C A_C c_C: block partials, the last block adds them in block order
+    __shared__ double sh[GAIN_BLOCK / 32][3];
+    __shared__ bool last;
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    for (int q = 0; q < 3; ++q) {
+        const double v = warp_sum_f64(cs[q]);
+        if (lane == 0) sh[wib][q] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int q = 0; q < 3; ++q) {
+            double t = 0;
+            for (int w = 0; w < GAIN_BLOCK / 32; ++w) t += sh[w][q];
+            A.csum_part[3 * static_cast<int64_t>(blockIdx.x) + q] = t;
+        }
+        __threadfence();
+        last = (atomicAdd(A.done, 1u) == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (last && threadIdx.x < 3) {
+        __threadfence();
+        double t = 0;
+        for (int b = 0; b < static_cast<int>(gridDim.x); ++b) t += __ldcg(A.csum_part + 3 * static_cast<int64_t>(b) + threadIdx.x);
+        A.zmean[threadIdx.x] = t / A.nV;
+        if (threadIdx.x == 0) *A.done = 0u;
+    }
+}
+
+// z_v = sum over the primitives i at v of w_i * (sum over the clusters containing i of c_C),
+// minus the mean of z (translations are the kernel of the metric)
+__global__ void k_vertex_expand(int nV, int size, const int* vp_rp, const int* vp_slot, const double* pre_vals,
+                                const int* leaf_of, const int* C_parent, const double* c, const double* zmean,
+                                double* z)
 {
     const int v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= nV) return;
@@ -328,13 +480,19 @@ __global__ void k_vertex_sum(int nV, int size, const int* vp_rp, const int* vp_s
         const int slot = vp_slot[k];
         const int i = slot / size, l = slot - i * size;
         const double w = pre_vals[(4 * static_cast<int64_t>(i)) * size + l];
-        a0 += w * Z[3 * static_cast<int64_t>(i)];
-        a1 += w * Z[3 * static_cast<int64_t>(i) + 1];
-        a2 += w * Z[3 * static_cast<int64_t>(i) + 2];
+        double z0 = 0, z1 = 0, z2 = 0;
+        for (int C = leaf_of[i]; C >= 0; C = C_parent[C]) {
+            z0 += c[3 * static_cast<int64_t>(C)];
+            z1 += c[3 * static_cast<int64_t>(C) + 1];
+            z2 += c[3 * static_cast<int64_t>(C) + 2];
+        }
+        a0 += w * z0;
+        a1 += w * z1;
+        a2 += w * z2;
     }
-    z[3 * static_cast<int64_t>(v)] = a0;
-    z[3 * static_cast<int64_t>(v) + 1] = a1;
-    z[3 * static_cast<int64_t>(v) + 2] = a2;
+    z[3 * static_cast<int64_t>(v)] = a0 - zmean[0];
+    z[3 * static_cast<int64_t>(v) + 1] = a1 - zmean[1];
+    z[3 * static_cast<int64_t>(v) + 2] = a2 - zmean[2];
 }
 
 // per-primitive a*n (3) for the averaged-normal feature
@@ -352,11 +510,6 @@ __global__ void k_sub_mean(int n, double* v, const double* sums)
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     for (int c = 0; c < 3; ++c) v[3 * static_cast<int64_t>(i) + c] -= sums[c] / n;
-}
-
-__global__ void k_scale_from_dot(int n, const double* rr, double* scale)
-{
-    *scale = sqrt((rr[0] + rr[1] + rr[2]) / (3.0 * n));
 }
 
 // Energy-norm loss of one preconditioner application: with e the exact correction (A e = r),
@@ -427,15 +580,6 @@ __global__ void k_prim_moments(int N, int size, const int* pre_cols, const doubl
     out[3 * static_cast<int64_t>(i) + 2] = a2;
 }
 
-// dO_C = s * dL/dc_C (float), from the FP64 cluster sums of gZ
-__global__ void k_cluster_out_grad(int NC, const double* gc, const double* scale, float* dO)
-{
-    const int C = blockIdx.x * blockDim.x + threadIdx.x;
-    if (C >= NC) return;
-    const double s = *scale;
-    for (int q = 0; q < 3; ++q) dO[3 * static_cast<int64_t>(C) + q] = static_cast<float>(s * gc[3 * static_cast<int64_t>(C) + q]);
-}
-
 }  // namespace rpb
 
 // ==========================================================================================
@@ -454,7 +598,9 @@ struct LearnedState {
     rpb_mlp* mlp = nullptr;
     int64_t geometry_version = -1;
     int max_depth = 0;
-    DevBuf<double> C_an, tmp3, Rc, c, Z, scale, sums, loss, gc, dots, g, r, z, e, Az;
+    DevBuf<double> C_an, tmp3, Rc, c, scale, sums, loss, gc, dots, g, r, z, e, Az;
+    DevBuf<double> local, blocks, sq_part, csum_part, zmean;
+    DevBuf<unsigned> done;
     DevBuf<float> F, O, dO, pre1, pre2, d1, d2, C_diam;
     DevBuf<int> C_depth;
 };
@@ -480,7 +626,14 @@ static rpb_status ensure_learned(rpb_mesh* m)
         RPB_CUDA(L.tmp3.alloc(3 * N));
         RPB_CUDA(L.Rc.alloc(3 * NC));
         RPB_CUDA(L.c.alloc(3 * NC));
-        RPB_CUDA(L.Z.alloc(3 * N));
+        const size_t nb = (N + SCAN_BLOCK - 1) / SCAN_BLOCK;
+        RPB_CUDA(L.local.alloc(3 * N));
+        RPB_CUDA(L.blocks.alloc(3 * (nb + 1)));
+        RPB_CUDA(L.sq_part.alloc(nb));
+        RPB_CUDA(L.csum_part.alloc(3 * ((NC + GAIN_BLOCK - 1) / GAIN_BLOCK)));
+        RPB_CUDA(L.zmean.alloc(3));
+        RPB_CUDA(L.done.alloc(1));
+        RPB_CUDA(cudaMemsetAsync(L.done.ptr, 0, L.done.bytes(), m->stream));
         RPB_CUDA(L.scale.alloc(1));
         RPB_CUDA(L.sums.alloc(4));
         RPB_CUDA(L.loss.alloc(1));
@@ -548,34 +701,34 @@ static rpb_status cluster_moments(rpb_mesh* m, const double* R, double* Rc)
     return range_sums3(m, m->learned->tmp3.ptr, Rc);
 }
 
-// z = M_learned(R) (device, n_v x 3); with `training` the activations are kept.
+// z = M_learned(R) (device, n_v x 3) in four launches; with `training` the features,
+// activations, outputs and cluster moments are kept for the backward pass.
 static rpb_status learned_forward(rpb_mesh* m, rpb_mlp* mlp, const double* R, double* z, bool training)
 {
     LearnedState& L = *m->learned;
     cudaStream_t s = m->stream;
-    rpb_status st;
-    if ((st = dot3_dev(m, R, R, L.sums.ptr)) != RPB_OK) return st;
-    k_scale_from_dot<<<1, 1, 0, s>>>(m->nV, L.sums.ptr, L.scale.ptr);
-    if ((st = cluster_moments(m, R, L.Rc.ptr)) != RPB_OK) return st;
-    FeatArgs fa;
-    fa.NC = m->NC; fa.max_depth = L.max_depth;
-    fa.C_pair = m->C_pair.ptr; fa.C_an = L.C_an.ptr; fa.Rc = L.Rc.ptr;
-    fa.C_left = m->C_left.ptr; fa.C_right = m->C_right.ptr; fa.C_depth = L.C_depth.ptr; fa.C_diam = L.C_diam.ptr;
-    fa.scale = L.scale.ptr; fa.F = L.F.ptr;
-    k_features<<<(m->NC + 255) / 256, 256, 0, s>>>(fa);
-    MlpArgs ma;
-    ma.n = m->NC; ma.w = mlp->w16.ptr; ma.F = L.F.ptr; ma.O = L.O.ptr;
-    ma.pre1 = training ? L.pre1.ptr : nullptr;
-    ma.pre2 = training ? L.pre2.ptr : nullptr;
-    k_mlp_forward<<<(m->NC + 127) / 128, 128, NPARAM * sizeof(float), s>>>(ma);
-    k_cluster_coeffs<<<(m->NC + 255) / 256, 256, 0, s>>>(m->NC, L.O.ptr, L.Rc.ptr, m->C_pair.ptr, L.c.ptr);
-    k_expand_clusters<<<(m->N + 255) / 256, 256, 0, s>>>(m->N, m->leaf_of.ptr, m->C_parent.ptr, L.c.ptr, L.Z.ptr);
-    k_vertex_sum<<<(m->nV + 255) / 256, 256, 0, s>>>(m->nV, m->size, m->vp_rp.ptr, m->vp_slot.ptr, m->pre_vals.ptr,
-                                                     L.Z.ptr, z);
-    RPB_CUDA(cudaGetLastError());
-    // remove the translation component (the kernel of the metric)
-    if ((st = dot3_dev(m, z, nullptr, L.sums.ptr)) != RPB_OK) return st;
-    k_sub_mean<<<(m->nV + 255) / 256, 256, 0, s>>>(m->nV, z, L.sums.ptr);
+    const int nb = (m->N + SCAN_BLOCK - 1) / SCAN_BLOCK;
+    PrimScanArgs ps;
+    ps.N = m->N; ps.nV = m->nV; ps.size = m->size;
+    ps.pre_cols = m->pre_cols.ptr; ps.pre_vals = m->pre_vals.ptr; ps.R = R;
+    ps.local = L.local.ptr; ps.blocks = L.blocks.ptr; ps.sq_part = L.sq_part.ptr;
+    k_prim_scan<<<nb, SCAN_BLOCK, 0, s>>>(ps);
+    k_scan_totals<<<1, SCAN_BLOCK, 0, s>>>(nb, m->nV, L.blocks.ptr, L.sq_part.ptr, L.scale.ptr);
+    ClusterMlpArgs ca;
+    ca.N = m->N; ca.NC = m->NC; ca.nV = m->nV; ca.max_depth = L.max_depth;
+    ca.w = mlp->w16.ptr; ca.C_pair = m->C_pair.ptr; ca.C_an = L.C_an.ptr;
+    ca.C_begin = m->C_begin.ptr; ca.C_end = m->C_end.ptr; ca.C_left = m->C_left.ptr; ca.C_right = m->C_right.ptr;
+    ca.C_depth = L.C_depth.ptr; ca.C_diam = L.C_diam.ptr;
+    ca.local = L.local.ptr; ca.blocks = L.blocks.ptr; ca.scale = L.scale.ptr;
+    ca.c = L.c.ptr; ca.csum_part = L.csum_part.ptr; ca.done = L.done.ptr; ca.zmean = L.zmean.ptr;
+    ca.F = training ? L.F.ptr : nullptr;
+    ca.O = training ? L.O.ptr : nullptr;
+    ca.pre1 = training ? L.pre1.ptr : nullptr;
+    ca.pre2 = training ? L.pre2.ptr : nullptr;
+    ca.Rc = training ? L.Rc.ptr : nullptr;
+    k_cluster_mlp<<<(m->NC + GAIN_BLOCK - 1) / GAIN_BLOCK, GAIN_BLOCK, NPARAM * sizeof(float), s>>>(ca);
+    k_vertex_expand<<<(m->nV + 255) / 256, 256, 0, s>>>(m->nV, m->size, m->vp_rp.ptr, m->vp_slot.ptr, m->pre_vals.ptr,
+                                                        m->leaf_of.ptr, m->C_parent.ptr, L.c.ptr, L.zmean.ptr, z);
     RPB_CUDA(cudaGetLastError());
     return RPB_OK;
 }

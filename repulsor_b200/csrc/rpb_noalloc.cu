@@ -76,14 +76,8 @@ rpb_status scratch_on_current_device(unsigned char** out)
 template <int QH, int PH>
 void launch_energy_pairs(const PairArgs& An, const PairArgs& Af, int nb_near, int nb_far, cudaStream_t s)
 {
-    if (An.rows > 0) {
-        auto k = k_tp0_pairs<false, QH, PH, false, NEAR_LANES>;
-        k<<<std::min(nb_near, pair_grid(reinterpret_cast<const void*>(k), An.rows, NEAR_LANES)), PAIR_BLOCK, 0, s>>>(An);
-    }
-    if (Af.rows > 0) {
-        auto k = k_tp0_pairs<true, QH, PH, false, FAR_LANES>;
-        k<<<std::min(nb_far, pair_grid(reinterpret_cast<const void*>(k), Af.rows, FAR_LANES)), PAIR_BLOCK, 0, s>>>(Af);
-    }
+    if (An.rows > 0) k_tp0_pairs<false, QH, PH, false, NEAR_LANES><<<nb_near, PAIR_BLOCK, 0, s>>>(An);
+    if (Af.rows > 0) k_tp0_pairs<true, QH, PH, false, FAR_LANES><<<nb_far, PAIR_BLOCK, 0, s>>>(Af);
 }
 
 }  // namespace
@@ -142,10 +136,10 @@ extern "C" rpb_status rpb_tpe0_value_noalloc(int dom_dim, const double* V, int64
     An.ex = Af.ex = ex;
     An.close_factor = Af.close_factor = 0.1f;
     An.rows = near_colidx ? N : 0; An.rp = near_rowptr; An.ci = near_colidx; An.order = nullptr; An.data = P_pair;
-    An.D = nullptr; An.block_energy = partials; An.done = done; An.energy_out = e2; An.rows_taken = done + 2;
+    An.D = nullptr; An.block_energy = partials; An.done = done; An.energy_out = e2; An.block_rows = nullptr;
     Af.rows = far_colidx ? NC : 0; Af.rp = far_rowptr; Af.ci = far_colidx; Af.order = nullptr; Af.data = C_pair;
     Af.D = nullptr; Af.block_energy = partials + nb_near; Af.done = done + 1; Af.energy_out = e2 + 1;
-    Af.rows_taken = done + 3;
+    Af.block_rows = nullptr;
     if (ex.qh == 3 && ex.ph == 6) launch_energy_pairs<3, 6>(An, Af, nb_near, nb_far, s);
     else launch_energy_pairs<-1, -1>(An, Af, nb_near, nb_far, s);
     k_add_pair<<<1, 1, 0, s>>>(e2, energy);

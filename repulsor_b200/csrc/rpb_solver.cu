@@ -522,7 +522,7 @@ static rpb_status cg_solve(rpb_mesh* m, double q, double p, const double* B, int
     const int eb = (n + 255) / 256;
     const bool flexible = (precond == RPB_PRECOND_LEARNED);
     // iterations without a 10% drop of the best residual that count as a stall
-    constexpr int kStallWindow = 400;
+    constexpr int kStallWindow = 500;
     int kind = precond;
 
     // ||B|| per column

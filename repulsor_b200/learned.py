@@ -22,7 +22,10 @@ import numpy as np
 from . import _capi
 from ._capi import PRECOND_NONE, RepulsorError, check, dptr, fptr
 
-__all__ = ["LearnedPreconditioner", "training_pairs", "train"]
+__all__ = ["LearnedPreconditioner", "training_pairs", "train", "NPARAM_OUTPUT_OFFSET"]
+
+# offset of the output layer (W3, b3) in the parameter vector: W1 64x16, b1 64, W2 64x64, b2 64
+NPARAM_OUTPUT_OFFSET = 64 * 16 + 64 + 64 * 64 + 64
 
 
 class LearnedPreconditioner:
