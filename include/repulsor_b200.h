@@ -239,10 +239,12 @@ rpb_status rpb_mlp_eval(rpb_mlp* mlp, const float* F, int64_t n, const float* dO
 /* One Adam step (lr <= 0: none) on npairs (residual R_k, correction E_k) pairs of mesh m
  * (host, n_v x 3 each, consecutive; A E_k = R_k for the metric A of exponents q, p):
  * loss = mean_k 1 - (z_k.R_k)^2 / ((z_k.A z_k)(E_k.R_k)) with z_k = M(R_k), the share of
- * the error energy ||E_k||_A^2 that the best step along z_k leaves. `loss` and `grad`
- * (param_count floats; either may be NULL) receive the loss and its gradient before the step. */
+ * the error energy ||E_k||_A^2 that the best step along z_k leaves, plus reg * mean over
+ * clusters and components of o_C^2 (keeps the gains near the multilevel operator's 1).
+ * `loss` (without the penalty) and `grad` (param_count floats, with it; either may be
+ * NULL) are taken before the step. */
 rpb_status rpb_mlp_train_step(rpb_mlp* mlp, rpb_mesh* m, double q, double p, const double* R, const double* E,
-                              int npairs, double lr, double* loss, float* grad);
+                              int npairs, double lr, double reg, double* loss, float* grad);
 /* Attach (mlp non-NULL) or detach the network used by RPB_PRECOND_LEARNED on this mesh;
  * the mesh keeps the pointer, the caller keeps ownership. */
 rpb_status rpb_mesh_set_learned(rpb_mesh* m, rpb_mlp* mlp);

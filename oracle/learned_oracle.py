@@ -203,9 +203,10 @@ class LearnedGeometry:
             return z, (cache, O32, gain, Rc)
         return z
 
-    def loss_and_grad(self, theta, R, E, apply_A, quantize=True):
+    def loss_and_grad(self, theta, R, E, apply_A, quantize=True, reg=0.0):
         """Energy-norm loss 1 - (z.R)^2 / ((z.Az)(E.R)) of z = M(R) and its parameter
-        gradient; apply_A is the metric product."""
+        gradient (the gradient includes the gain penalty reg * mean(o^2), the returned loss
+        does not); apply_A is the metric product."""
         R = np.asarray(R, np.float64)
         z, (cache, O32, gain, Rc) = self.apply(theta, R, return_cache=True, quantize=quantize)
         Az = apply_A(z)
@@ -215,7 +216,7 @@ class LearnedGeometry:
         g -= g.mean(0)
         gc = self.range_sums(self.prim_from_vertices(g))
         inside = np.abs(O32) < GAIN_CLAMP
-        dO = gc * Rc * gain * inside
+        dO = gc * Rc * gain * inside + 2.0 * reg * O32 / (3.0 * self.NC)
         if quantize:
             dO = dO.astype(np.float32).astype(np.float64)
         return loss, mlp_backward(theta, cache, dO, quantize)

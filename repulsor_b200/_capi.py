@@ -116,7 +116,7 @@ SIGNATURES = {
     "rpb_mlp_set_params": (ctypes.c_int, [_vp, _fp]),
     "rpb_mlp_eval": (ctypes.c_int, [_vp, _fp, ctypes.c_int64, _fp, _fp, _fp]),
     "rpb_mlp_train_step": (ctypes.c_int, [_vp, _vp, ctypes.c_double, ctypes.c_double, _dp, _dp, ctypes.c_int,
-                                          ctypes.c_double, _dp, _fp]),
+                                          ctypes.c_double, ctypes.c_double, _dp, _fp]),
     "rpb_mesh_set_learned": (ctypes.c_int, [_vp, _vp]),
     "rpb_tpm0_learned_apply": (ctypes.c_int, [_vp, _dp, _dp]),
 }

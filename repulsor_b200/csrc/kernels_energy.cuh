@@ -397,7 +397,9 @@ struct PairArgs {
     float close_factor;       // FP64 path for near pairs with r < close_factor (d_i + d_j)
 };
 
-constexpr int PAIR_BLOCK = 256;
+constexpr int PAIR_BLOCK = 128;
+// 4 resident blocks of 128 threads per SM (at most 128 registers per thread)
+constexpr int PAIR_MIN_BLOCKS = 4;
 constexpr int PAIR_FLUSH = 8;   // FP32 partial sums are carried into FP64 every 8 pairs
 // Threads per CSR row: a row's nonzeros are strided over LANES consecutive lanes and the
 // partial sums combined by an xor-butterfly of warp shuffles (fixed order, deterministic).
@@ -419,7 +421,7 @@ constexpr int pair_blocks(int rows, int lanes) { return (rows * lanes + PAIR_BLO
 // neighbours in tree order); inside a block, warps take the next 32/LANES rows from a
 // shared counter, so long and short rows balance across the block's warps.
 template <bool FAR, int QH, int PH, bool DIFF, int LANES, bool CROSS = false>
-__global__ void __launch_bounds__(PAIR_BLOCK) k_tp0_pairs(PairArgs A)
+__global__ void __launch_bounds__(PAIR_BLOCK, PAIR_MIN_BLOCKS) k_tp0_pairs(PairArgs A)
 {
     static_assert(LANES == 1 || LANES == 2 || LANES == 4 || LANES == 8, "LANES must divide a warp");
     constexpr int ROWS_PER_WARP = 32 / LANES;
@@ -452,20 +454,9 @@ __global__ void __launch_bounds__(PAIR_BLOCK) k_tp0_pairs(PairArgs A)
             float e32 = 0.0f;
             int since_flush = 0;
             const int64_t k0 = A.rp[i], k1 = A.rp[i + 1];
-            // software pipeline: the next column's datum is in flight while this pair computes
-            int j_next = 0;
-            Datum Y_next;
-            if (k0 + sub < k1) {
-                j_next = __ldg(A.ci + k0 + sub);
-                Y_next = load_datum(cols, j_next);
-            }
             for (int64_t k = k0 + sub; k < k1; k += LANES) {
-                const int j = j_next;
-                const Datum Y = Y_next;
-                if (k + LANES < k1) {
-                    j_next = __ldg(A.ci + k + LANES);
-                    Y_next = load_datum(cols, j_next);
-                }
+                const int j = __ldg(A.ci + k);
+                const Datum Y = load_datum(cols, j);
                 Proj<float> g;
                 if constexpr (FAR) project_clusters(X, Y, g);
                 else project_prims(A.dom, X, Y, g);

@@ -529,9 +529,10 @@ __global__ void k_loss_grad(int n, const double* r, const double* Az, const doub
     if (i == 0) *loss_acc += 1.0 - zr * zr / (zAz * er);
 }
 
-// dL/do_C = sum_q gc_Cq R_Cq / A_C * g_Cq (zero where the clamp is active)
+// dL/do_C = sum_q gc_Cq R_Cq / A_C * g_Cq (zero where the clamp is active), plus the
+// gradient 2 reg o_C / (3 N_C) of the gain penalty reg * mean(o^2)
 __global__ void k_cluster_out_grad(int NC, const double* gc, const float* O, const double* Rc, const ClusterDatum* C_pair,
-                                   float* dO)
+                                   float reg, float* dO)
 {
     const int C = blockIdx.x * blockDim.x + threadIdx.x;
     if (C >= NC) return;
@@ -540,7 +541,8 @@ __global__ void k_cluster_out_grad(int NC, const double* gc, const float* O, con
         const int64_t k = 3 * static_cast<int64_t>(C) + q;
         const float o = O[k];
         const bool inside = o > -GAIN_CLAMP && o < GAIN_CLAMP;
-        dO[k] = inside ? static_cast<float>(gc[k] * Rc[k] * inv_a * exp(static_cast<double>(o))) : 0.0f;
+        dO[k] = (inside ? static_cast<float>(gc[k] * Rc[k] * inv_a * exp(static_cast<double>(o))) : 0.0f) +
+                2.0f * reg * o / (3.0f * NC);
     }
 }
 
@@ -898,7 +900,7 @@ rpb_status rpb_tpm0_learned_apply(rpb_mesh* m, const double* R, double* Z)
 }
 
 rpb_status rpb_mlp_train_step(rpb_mlp* mlp, rpb_mesh* m, double q, double p, const double* R, const double* E,
-                              int npairs, double lr, double* loss, float* grad)
+                              int npairs, double lr, double reg, double* loss, float* grad)
 {
     if (!mlp || !m || !R || !E || npairs <= 0) { set_error("null or empty argument"); return RPB_EINVAL; }
     if (mlp->device != m->device) { set_error("network and mesh live on different devices"); return RPB_EINVAL; }
@@ -931,7 +933,7 @@ rpb_status rpb_mlp_train_step(rpb_mlp* mlp, rpb_mesh* m, double q, double p, con
         k_sub_mean<<<eb, 256, 0, s>>>(nV, L.g.ptr, L.sums.ptr);
         if ((st = cluster_moments(m, L.g.ptr, L.gc.ptr)) != RPB_OK) return st;
         k_cluster_out_grad<<<(m->NC + 255) / 256, 256, 0, s>>>(m->NC, L.gc.ptr, L.O.ptr, L.Rc.ptr, m->C_pair.ptr,
-                                                               L.dO.ptr);
+                                                               static_cast<float>(reg), L.dO.ptr);
         RPB_CUDA(cudaGetLastError());
         if ((st = mlp_backward(mlp, m->NC, L.F.ptr, L.pre1.ptr, L.pre2.ptr, L.dO.ptr, L.d1.ptr, L.d2.ptr, mlp->grad.ptr,
                                s)) != RPB_OK)

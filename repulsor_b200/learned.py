@@ -98,7 +98,7 @@ class LearnedPreconditioner:
         check(_capi.load().rpb_tpm0_learned_apply(M._h, dptr(R), dptr(Z)), "rpb_tpm0_learned_apply")
         return Z
 
-    def train_step(self, M, metric, R, E, lr=1e-3, want_grad=False):
+    def train_step(self, M, metric, R, E, lr=1e-3, want_grad=False, reg=0.0):
         """One Adam step (none for lr <= 0) on the pairs (R[k], E[k]) of mesh M and the
         metric's exponents; returns the loss before the step (and its gradient with
         want_grad)."""
@@ -109,7 +109,7 @@ class LearnedPreconditioner:
         loss = ctypes.c_double()
         grad = np.zeros(self.param_count(), np.float32) if want_grad else None
         check(_capi.load().rpb_mlp_train_step(self._h, M._h, metric.q, metric.p, dptr(R), dptr(E), R.shape[0], float(lr),
-                                              ctypes.byref(loss), None if grad is None else fptr(grad)),
+                                              float(reg), ctypes.byref(loss), None if grad is None else fptr(grad)),
               "rpb_mlp_train_step")
         return (loss.value, grad) if want_grad else loss.value
 
@@ -157,9 +157,9 @@ def _smooth(M, b):
     return out - out.mean(0)
 
 
-def train(net: LearnedPreconditioner, metric, data, epochs=200, lr=1e-3, batch=4, seed=0, log=None):
-    """Adam over the (mesh, R, E) sets in `data`, `batch` pairs per step. Returns the loss
-    history (one mean per epoch)."""
+def train(net: LearnedPreconditioner, metric, data, epochs=200, lr=1e-3, batch=4, seed=0, log=None, reg=1.0):
+    """Adam over the (mesh, R, E) sets in `data`, `batch` pairs per step, with the gain
+    penalty reg * mean(o^2). Returns the loss history (one mean per epoch, penalty excluded)."""
     rng = np.random.default_rng(seed)
     hist = []
     for ep in range(epochs):
@@ -168,7 +168,7 @@ def train(net: LearnedPreconditioner, metric, data, epochs=200, lr=1e-3, batch=4
             order = rng.permutation(R.shape[0])
             for s in range(0, len(order), batch):
                 idx = order[s:s + batch]
-                losses.append(net.train_step(M, metric, R[idx], E[idx], lr=lr))
+                losses.append(net.train_step(M, metric, R[idx], E[idx], lr=lr, reg=reg))
         hist.append(float(np.mean(losses)))
         if log is not None:
             log(ep, hist[-1])
