@@ -14,10 +14,7 @@
 //   k_gather_vertices  : DerivativeAssembler().Dot (src/SimplicialMesh.hpp:625-674).
 #pragma once
 
-#include <algorithm>
-#include <cstdint>
 #include <type_traits>
-#include <vector>
 
 #include "rpb_device.cuh"
 
@@ -391,15 +388,12 @@ struct PairArgs {
     double* D;                // rows x 10 (d0, dx[3], dP[6]) centred moment derivatives
     double* block_energy;     // gridDim.x
     unsigned* done;           // 1 counter, zero between launches
-    const int* block_rows;    // gridDim.x + 1 slot ranges of the blocks (null: PAIR_BLOCK / LANES slots each)
     double* energy_out;       // 1
     TPExp ex;
     float close_factor;       // FP64 path for near pairs with r < close_factor (d_i + d_j)
 };
 
-constexpr int PAIR_BLOCK = 128;
-// 4 resident blocks of 128 threads per SM (at most 128 registers per thread)
-constexpr int PAIR_MIN_BLOCKS = 4;
+constexpr int PAIR_BLOCK = 256;
 constexpr int PAIR_FLUSH = 8;   // FP32 partial sums are carried into FP64 every 8 pairs
 // Threads per CSR row: a row's nonzeros are strided over LANES consecutive lanes and the
 // partial sums combined by an xor-butterfly of warp shuffles (fixed order, deterministic).
@@ -416,121 +410,103 @@ constexpr int pair_blocks(int rows, int lanes) { return (rows * lanes + PAIR_BLO
 // CROSS: rows are the mesh's, columns the obstacle's (a non-symmetric block cluster tree):
 // every pair counts, energy and derivatives carry the symmetry factor 1/2
 // (src/FMM/FMM_Kernel.hpp:43) and the obstacle's derivatives are not formed.
-// Block b takes the contiguous slot range block_rows[b] .. block_rows[b+1] of the processing
-// order (ranges of equal nonzero count, so blocks carry equal work and an SM's rows stay
-// neighbours in tree order); inside a block, warps take the next 32/LANES rows from a
-// shared counter, so long and short rows balance across the block's warps.
 template <bool FAR, int QH, int PH, bool DIFF, int LANES, bool CROSS = false>
-__global__ void __launch_bounds__(PAIR_BLOCK, PAIR_MIN_BLOCKS) k_tp0_pairs(PairArgs A)
+__global__ void __launch_bounds__(PAIR_BLOCK) k_tp0_pairs(PairArgs A)
 {
     static_assert(LANES == 1 || LANES == 2 || LANES == 4 || LANES == 8, "LANES must divide a warp");
-    constexpr int ROWS_PER_WARP = 32 / LANES;
     using Datum = typename std::conditional<FAR, ClusterDatum, PrimDatum>::type;
     const Datum* base = static_cast<const Datum*>(A.data);
     const Datum* cols = CROSS ? static_cast<const Datum*>(A.col_data) : base;
-    const int lane = threadIdx.x & 31;
-    const int grp = lane / LANES, sub = lane & (LANES - 1);
-    const int slot_begin = A.block_rows ? A.block_rows[blockIdx.x] : blockIdx.x * (PAIR_BLOCK / LANES);
-    const int slot_end = A.block_rows ? A.block_rows[blockIdx.x + 1] : min(A.rows, slot_begin + PAIR_BLOCK / LANES);
-    __shared__ int next_slot;
-    if (threadIdx.x == 0) next_slot = slot_begin;
-    __syncthreads();
-    double e_acc = 0.0;
-    for (;;) {
-        int first = 0;
-        if (lane == 0) first = atomicAdd(&next_slot, ROWS_PER_WARP);
-        first = __shfl_sync(0xffffffffu, first, 0);
-        if (first >= slot_end) break;
-        const int slot = first + grp;
-        const bool active = slot < slot_end;
-        double e_row = 0.0;
-        double D64[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
-        int i = 0;
-        if (active) {
-            i = A.order ? A.order[slot] : slot;
-            const Datum X = load_datum(base, i);
-            const float ax = static_cast<float>(X.a);
-            PairAcc<float> acc = {};
-            float e32 = 0.0f;
-            int since_flush = 0;
-            const int64_t k0 = A.rp[i], k1 = A.rp[i + 1];
-            for (int64_t k = k0 + sub; k < k1; k += LANES) {
-                const int j = __ldg(A.ci + k);
-                const Datum Y = load_datum(cols, j);
-                Proj<float> g;
-                if constexpr (FAR) project_clusters(X, Y, g);
-                else project_prims(A.dom, X, Y, g);
-                bool close = false;
-                if constexpr (!FAR) {
-                    const float dd = A.close_factor * (X.diam + Y.diam);
-                    close = g.r2 < dd * dd;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int slot = t / LANES, sub = t & (LANES - 1);
+    const bool active = slot < A.rows;
+    double e_row = 0.0;
+    double D64[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    int i = 0;
+    if (active) {
+        i = A.order ? A.order[slot] : slot;
+        const Datum X = load_datum(base, i);
+        const float ax = static_cast<float>(X.a);
+        PairAcc<float> acc = {};
+        float e32 = 0.0f;
+        int since_flush = 0;
+        const int64_t k0 = A.rp[i], k1 = A.rp[i + 1];
+        for (int64_t k = k0 + sub; k < k1; k += LANES) {
+            const int j = __ldg(A.ci + k);
+            const Datum Y = load_datum(cols, j);
+            Proj<float> g;
+            if constexpr (FAR) project_clusters(X, Y, g);
+            else project_prims(A.dom, X, Y, g);
+            bool close = false;
+            if constexpr (!FAR) {
+                const float dd = A.close_factor * (X.diam + Y.diam);
+                close = g.r2 < dd * dd;
+            }
+            if (close) {
+                // close near-field pair: the same kernel in FP64, added straight into FP64
+                Proj<double> gd;
+                if constexpr (!FAR) project_prims(A.dom, X, Y, gd);
+                PairAcc<double> a64 = {};
+                const double e = tp0_core<double, QH, PH, DIFF>(A.ex, gd, X.a, Y.a, a64);
+                if (CROSS || j > i) e_row += e;
+                if (DIFF) {
+                    D64[0] += a64.d0;
+                    for (int m = 0; m < 3; ++m) D64[1 + m] += a64.dx[m];
+                    for (int m = 0; m < 6; ++m) D64[4 + m] += a64.dP[m];
                 }
-                if (close) {
-                    // close near-field pair: the same kernel in FP64, added straight into FP64
-                    Proj<double> gd;
-                    if constexpr (!FAR) project_prims(A.dom, X, Y, gd);
-                    PairAcc<double> a64 = {};
-                    const double e = tp0_core<double, QH, PH, DIFF>(A.ex, gd, X.a, Y.a, a64);
-                    if (CROSS || j > i) e_row += e;
+            } else {
+                const float e = tp0_core<float, QH, PH, DIFF>(A.ex, g, ax, static_cast<float>(Y.a), acc);
+                if (CROSS || j > i) e32 += e;
+                if (++since_flush == PAIR_FLUSH) {
+                    since_flush = 0;
+                    e_row += e32;
+                    e32 = 0.0f;
                     if (DIFF) {
-                        D64[0] += a64.d0;
-                        for (int m = 0; m < 3; ++m) D64[1 + m] += a64.dx[m];
-                        for (int m = 0; m < 6; ++m) D64[4 + m] += a64.dP[m];
-                    }
-                } else {
-                    const float e = tp0_core<float, QH, PH, DIFF>(A.ex, g, ax, static_cast<float>(Y.a), acc);
-                    if (CROSS || j > i) e32 += e;
-                    if (++since_flush == PAIR_FLUSH) {
-                        since_flush = 0;
-                        e_row += e32;
-                        e32 = 0.0f;
-                        if (DIFF) {
-                            D64[0] += acc.d0;
+                        D64[0] += acc.d0;
 #pragma unroll
-                            for (int m = 0; m < 3; ++m) D64[1 + m] += acc.dx[m];
+                        for (int m = 0; m < 3; ++m) D64[1 + m] += acc.dx[m];
 #pragma unroll
-                            for (int m = 0; m < 6; ++m) D64[4 + m] += acc.dP[m];
-                            acc = PairAcc<float>{};
-                        }
+                        for (int m = 0; m < 6; ++m) D64[4 + m] += acc.dP[m];
+                        acc = PairAcc<float>{};
                     }
                 }
             }
-            e_row += e32;
-            if (DIFF) {
-                D64[0] += acc.d0;
-#pragma unroll
-                for (int m = 0; m < 3; ++m) D64[1 + m] += acc.dx[m];
-#pragma unroll
-                for (int m = 0; m < 6; ++m) D64[4 + m] += acc.dP[m];
-            }
         }
-        if constexpr (CROSS) {
-            e_row *= 0.5;
+        e_row += e32;
+        if (DIFF) {
+            D64[0] += acc.d0;
 #pragma unroll
-            for (int m = 0; m < 10; ++m) D64[m] *= 0.5;
+            for (int m = 0; m < 3; ++m) D64[1 + m] += acc.dx[m];
+#pragma unroll
+            for (int m = 0; m < 6; ++m) D64[4 + m] += acc.dP[m];
         }
-        // combine the LANES partial sums of a row (every lane of the warp takes part)
-#pragma unroll
-        for (int off = 1; off < LANES; off <<= 1) {
-            e_row += __shfl_xor_sync(0xffffffffu, e_row, off);
-            if (DIFF) {
-#pragma unroll
-                for (int m = 0; m < 10; ++m) D64[m] += __shfl_xor_sync(0xffffffffu, D64[m], off);
-            }
-        }
-        if (DIFF && active && sub == 0) {
-            double* dst = A.D + 10 * static_cast<int64_t>(i);
-#pragma unroll
-            for (int m = 0; m < 10; ++m) dst[m] = D64[m];
-        }
-        if (sub == 0) e_acc += e_row;
     }
+    if constexpr (CROSS) {
+        e_row *= 0.5;
+#pragma unroll
+        for (int m = 0; m < 10; ++m) D64[m] *= 0.5;
+    }
+    // combine the LANES partial sums of a row (every lane of the warp takes part)
+#pragma unroll
+    for (int off = 1; off < LANES; off <<= 1) {
+        e_row += __shfl_xor_sync(0xffffffffu, e_row, off);
+        if (DIFF) {
+#pragma unroll
+            for (int m = 0; m < 10; ++m) D64[m] += __shfl_xor_sync(0xffffffffu, D64[m], off);
+        }
+    }
+    if (DIFF && active && sub == 0) {
+        double* dst = A.D + 10 * static_cast<int64_t>(i);
+#pragma unroll
+        for (int m = 0; m < 10; ++m) dst[m] = D64[m];
+    }
+    if (sub != 0) e_row = 0.0;
     // deterministic energy reduction: per-block partial, last block sums all partials
     __shared__ double sh[PAIR_BLOCK / 32];
     __shared__ bool last;
-    const int wib = threadIdx.x >> 5;
-    double e_w = warp_sum_f64(e_acc);
-    if (lane == 0) sh[wib] = e_w;
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    e_row = warp_sum_f64(e_row);
+    if (lane == 0) sh[wib] = e_row;
     __syncthreads();
     if (threadIdx.x == 0) {
         double s = 0.0;
@@ -555,30 +531,6 @@ __global__ void __launch_bounds__(PAIR_BLOCK, PAIR_MIN_BLOCKS) k_tp0_pairs(PairA
             *A.done = 0u;
         }
     }
-}
-
-// Slot ranges of the pair-kernel blocks: the rows in processing order (row lengths
-// `len`) cut into contiguous ranges of about equal nonzero count, about
-// PAIR_BLOCK / lanes * mean row length nonzeros each. Returns blocks + 1 offsets.
-inline std::vector<int> pair_block_ranges(const std::vector<int64_t>& len, int lanes)
-{
-    const int rows = static_cast<int>(len.size());
-    int64_t nnz = 0;
-    for (int64_t x : len) nnz += x;
-    std::vector<int> r{0};
-    if (rows == 0) return r;
-    const int64_t rows_per_block = PAIR_BLOCK / lanes;
-    const int64_t per = std::max<int64_t>(1, (nnz * rows_per_block + rows - 1) / rows);
-    int64_t acc = 0;
-    for (int i = 0; i < rows; ++i) {
-        acc += std::max<int64_t>(len[i], 1);
-        if (acc >= per && i + 1 < rows) {
-            r.push_back(i + 1);
-            acc = 0;
-        }
-    }
-    r.push_back(rows);
-    return r;
 }
 
 // energy = near-field part + far-field part (the order evaluate() uses on the host)

@@ -165,12 +165,12 @@ rpb_status launch_pairs(rpb_mesh* m, const TPExp& ex, bool diff, cudaEvent_t bet
     An.rp = m->near.rp.ptr; An.ci = m->near.ci.ptr; An.data = m->P_pair.ptr; An.D = m->D_near.ptr;
     An.order = m->near_order.ptr;
     An.block_energy = m->block_energy.ptr; An.done = m->done.ptr; An.energy_out = m->energy.ptr;
-    An.block_rows = m->near_block_rows.ptr;
+
     Af.rows = m->far.nnz > 0 ? m->NC : 0;
     Af.rp = m->far.rp.ptr; Af.ci = m->far.ci.ptr; Af.data = m->C_pair.ptr; Af.D = m->D_far.ptr;
     Af.order = m->far_order.ptr;
     Af.block_energy = m->block_energy.ptr + m->near_blocks; Af.done = m->done.ptr + 1; Af.energy_out = m->energy.ptr + 1;
-    Af.block_rows = m->far_block_rows.ptr;
+
     if (An.rows == 0) {
         RPB_CUDA(cudaMemsetAsync(m->energy.ptr, 0, sizeof(double), m->stream));
         if (diff) RPB_CUDA(cudaMemsetAsync(m->D_near.ptr, 0, m->D_near.bytes(), m->stream));
@@ -374,17 +374,8 @@ rpb_status rpb_mesh_create(int dom_dim, int amb_dim, const double* Vh, int64_t n
         const std::vector<int> no = order_of(T.near), fo = order_of(T.far);
         if ((st = upload(m->near_order, no.data(), no.size(), s)) != RPB_OK) return fail(st);
         if ((st = upload(m->far_order, fo.data(), fo.size(), s)) != RPB_OK) return fail(st);
-        // blocks over contiguous slot ranges of equal nonzero count
-        auto ranges = [](const SymPattern& P, const std::vector<int>& o, int lanes) {
-            std::vector<int64_t> len(o.size());
-            for (size_t k = 0; k < o.size(); ++k) len[k] = P.rp[o[k] + 1] - P.rp[o[k]];
-            return pair_block_ranges(len, lanes);
-        };
-        const std::vector<int> nr = ranges(T.near, no, NEAR_LANES), fr = ranges(T.far, fo, FAR_LANES);
-        m->near_blocks = static_cast<int>(nr.size()) - 1;
-        m->far_blocks = static_cast<int>(fr.size()) - 1;
-        if ((st = upload(m->near_block_rows, nr.data(), nr.size(), s)) != RPB_OK) return fail(st);
-        if ((st = upload(m->far_block_rows, fr.data(), fr.size(), s)) != RPB_OK) return fail(st);
+        m->near_blocks = pair_blocks(m->N, NEAR_LANES);
+        m->far_blocks = pair_blocks(m->NC, FAR_LANES);
     }
     if (m->block_energy.alloc(m->near_blocks + m->far_blocks)) { set_error("device allocation failed"); return fail(RPB_ENOMEM); }
     if (cudaMemsetAsync(m->counter.ptr, 0, m->counter.bytes(), s) != cudaSuccess ||

@@ -82,7 +82,6 @@ struct rpb_mesh {
     rpb::DevBuf<int> perm, leaf_of, C_parent, C_left, C_right, C_begin, C_end;
     rpb::Csr near, far, verynear;
     rpb::DevBuf<int> near_order, far_order;             // pair-kernel row order (length-sorted per chunk)
-    rpb::DevBuf<int> near_block_rows, far_block_rows;   // slot ranges of the pair-kernel blocks
     // geometry state
     rpb::DevBuf<rpb::PrimDatum> P_pair;
     rpb::DevBuf<rpb::ClusterDatum> C_pair;

@@ -136,10 +136,9 @@ extern "C" rpb_status rpb_tpe0_value_noalloc(int dom_dim, const double* V, int64
     An.ex = Af.ex = ex;
     An.close_factor = Af.close_factor = 0.1f;
     An.rows = near_colidx ? N : 0; An.rp = near_rowptr; An.ci = near_colidx; An.order = nullptr; An.data = P_pair;
-    An.D = nullptr; An.block_energy = partials; An.done = done; An.energy_out = e2; An.block_rows = nullptr;
+    An.D = nullptr; An.block_energy = partials; An.done = done; An.energy_out = e2;
     Af.rows = far_colidx ? NC : 0; Af.rp = far_rowptr; Af.ci = far_colidx; Af.order = nullptr; Af.data = C_pair;
     Af.D = nullptr; Af.block_energy = partials + nb_near; Af.done = done + 1; Af.energy_out = e2 + 1;
-    Af.block_rows = nullptr;
     if (ex.qh == 3 && ex.ph == 6) launch_energy_pairs<3, 6>(An, Af, nb_near, nb_far, s);
     else launch_energy_pairs<-1, -1>(An, Af, nb_near, nb_far, s);
     k_add_pair<<<1, 1, 0, s>>>(e2, energy);

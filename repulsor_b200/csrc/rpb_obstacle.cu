@@ -32,7 +32,7 @@ namespace rpb {
 struct ObstacleState {
     rpb_mesh* mesh = nullptr;      // the obstacle (owned)
     Csr near, far;
-    DevBuf<int> near_order, far_order, near_block_rows, far_block_rows;
+    DevBuf<int> near_order, far_order;
     int64_t verynear_nnz = 0, inter_nnz = 0;
     CrossLists lists;              // host copy (patterns for inspection)
     DevBuf<double> D_near, D_far, block_energy, energy;
@@ -129,12 +129,12 @@ rpb_status evaluate_obstacle(rpb_mesh* m, double q, double p, bool diff, double 
     An.rp = O.near.rp.ptr; An.ci = O.near.ci.ptr; An.order = O.near_order.ptr;
     An.data = m->P_pair.ptr; An.col_data = O.mesh->P_pair.ptr; An.D = O.D_near.ptr;
     An.block_energy = O.block_energy.ptr; An.done = O.done.ptr; An.energy_out = O.energy.ptr;
-    An.block_rows = O.near_block_rows.ptr;
+
     Af.rows = O.far.nnz > 0 ? m->NC : 0;
     Af.rp = O.far.rp.ptr; Af.ci = O.far.ci.ptr; Af.order = O.far_order.ptr;
     Af.data = m->C_pair.ptr; Af.col_data = O.mesh->C_pair.ptr; Af.D = O.D_far.ptr;
     Af.block_energy = O.block_energy.ptr + O.near_blocks; Af.done = O.done.ptr + 1; Af.energy_out = O.energy.ptr + 1;
-    Af.block_rows = O.far_block_rows.ptr;
+
     if (An.rows == 0) {
         RPB_CUDA(cudaMemsetAsync(O.energy.ptr, 0, sizeof(double), m->stream));
         if (diff) RPB_CUDA(cudaMemsetAsync(O.D_near.ptr, 0, O.D_near.bytes(), m->stream));
@@ -188,18 +188,11 @@ rpb_status rpb_mesh_load_obstacle(rpb_mesh* m, rpb_mesh* obstacle)
     O->verynear_nnz = L.verynear.nnz();
     O->inter_nnz = L.inter.nnz();
     const std::vector<int> no = chunk_order(L.near), fo = chunk_order(L.far);
-    auto ranges = [](const CrossPattern& P, const std::vector<int>& o, int lanes) {
-        std::vector<int64_t> len(o.size());
-        for (size_t k = 0; k < o.size(); ++k) len[k] = P.rp[o[k] + 1] - P.rp[o[k]];
-        return pair_block_ranges(len, lanes);
-    };
-    const std::vector<int> nr = ranges(L.near, no, NEAR_LANES), fr = ranges(L.far, fo, FAR_LANES);
-    O->near_blocks = static_cast<int>(nr.size()) - 1;
-    O->far_blocks = static_cast<int>(fr.size()) - 1;
+    O->near_blocks = pair_blocks(m->N, NEAR_LANES);
+    O->far_blocks = pair_blocks(m->NC, FAR_LANES);
     if (upload_vec(O->near.rp, L.near.rp, s) || upload_vec(O->near.ci, L.near.ci, s) ||
         upload_vec(O->far.rp, L.far.rp, s) || upload_vec(O->far.ci, L.far.ci, s) ||
-        upload_vec(O->near_order, no, s) || upload_vec(O->far_order, fo, s) ||
-        upload_vec(O->near_block_rows, nr, s) || upload_vec(O->far_block_rows, fr, s)) {
+        upload_vec(O->near_order, no, s) || upload_vec(O->far_order, fo, s)) {
         set_error("obstacle list upload failed");
         return fail(RPB_ENOMEM);
     }
