@@ -40,6 +40,17 @@ FLOPS_NEAR_PAIR = 185.0
 LAUNCHES_PER_STEP = 7
 
 
+def pair_traffic_from_profile():
+    """DRAM bytes (read + write) of the two pair launches of one evaluation, from the ncu
+    capture summarised in profiles/k_tp0_pairs_torus160x120.md (null if absent)."""
+    import re
+    path = os.path.join(ROOT, "profiles", "k_tp0_pairs_torus160x120.md")
+    if not os.path.exists(path):
+        return None
+    m = re.search(r"DRAM bytes per evaluation[^:]*:\s*([0-9,]+)", open(path).read(), re.IGNORECASE)
+    return int(m.group(1).replace(",", "")) if m else None
+
+
 def workload_mesh():
     from repulsor_b200 import meshes
     return meshes.torus(R=1.0, r=0.4, n_major=160, n_minor=120, jitter=0.002, seed=1002)
@@ -266,10 +277,7 @@ def main():
         pair_ms = ms[1] + ms[2]
         flops = FLOPS_NEAR_PAIR * near_pairs + FLOPS_FAR_PAIR * far_pairs
         achieved = flops / (pair_ms * 1e-3) / 1e12
-        traffic = None
-        tpath = os.path.join(ROOT, "profiles", "traffic.json")
-        if os.path.exists(tpath):
-            traffic = json.load(open(tpath)).get("tp0_pairs_bytes_per_evaluation")
+        traffic = pair_traffic_from_profile()
         roofline = {"bound": "fp32", "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
                     "frac": achieved / peak.value, "traffic": traffic,
                     "kernel": "k_tp0_pairs (near + far launches)",

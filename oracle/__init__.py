@@ -62,6 +62,9 @@ def _load():
     lib.oracle_h1_triplet_count.restype = ctypes.c_int64
     lib.oracle_h1_triplet_count.argtypes = [ctypes.c_void_p]
     lib.oracle_h1_triplets.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double, _ip, _ip, _dp]
+    for name in ("oracle_simplex_densities", "oracle_vertex_densities"):
+        getattr(lib, name).restype = ctypes.c_double
+        getattr(lib, name).argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double, _dp]
     lib.oracle_load_obstacle.restype = ctypes.c_int
     lib.oracle_load_obstacle.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
     lib.oracle_obstacle_counts.argtypes = [ctypes.c_void_p, _lp]
@@ -205,6 +208,16 @@ class OracleMesh:
         Df = np.zeros((self.nS, 10))
         _load().oracle_moment_derivatives(self._h, _d(Dn), _d(Df))
         return Dn, Df
+
+    def simplex_densities(self, q=6.0, p=12.0):
+        out = np.zeros(self.nS)
+        en = _load().oracle_simplex_densities(self._h, q, p, _d(out))
+        return en, out
+
+    def vertex_densities(self, q=6.0, p=12.0):
+        out = np.zeros(self.nV)
+        en = _load().oracle_vertex_densities(self._h, q, p, _d(out))
+        return en, out
 
     def allpairs_energy(self, q=6.0, p=12.0):
         return _load().oracle_allpairs_energy(self._h, q, p)

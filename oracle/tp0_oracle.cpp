@@ -750,6 +750,8 @@ static inline double pow_c(const TPParams& T, double c_abs)
 struct PairOut {
     double E;          // energy density E (without a*b)
     double energy;     // a*E*b
+    double dens_x;     // density contribution at x: b |Pv|^q / |v|^p (TP0_Kernel_FF.hpp:214-218)
+    double dens_y;     // density contribution at y: a |Qv|^q / |v|^p
     double DX[10], DY[10];
     double a0, a1;     // metric block
 };
@@ -780,6 +782,8 @@ static inline void tp0_pair(const TPParams& T, double a, const double* x, const 
     const double E = Num * rmp;
     o.E = E;
     o.energy = a * E * b;
+    o.dens_x = b * cphi_q * rmp;
+    o.dens_y = a * cpsi_q * rmp;
     if (diff) {
         const double factor = T.q * rmp;
         const double Kxy = factor * cphi_qm2;
@@ -1839,6 +1843,65 @@ static double obstacle_allpairs_energy(const Mesh& M, const Mesh& O, double q, d
     return en;
 }
 
+// Energy densities (EnergyBase::SimplexDensities / VertexDensities,
+// src/Energies/EnergyBase.hpp:129-150; CollectPrimitiveDensities / CollectVertexDensities,
+// src/ClusterTree/ClusterTreeBase.hpp:601-729): per pair, x receives b |Pv|^q / |v|^p and
+// y receives a |Qv|^q / |v|^p; far-field cluster densities are pushed down to the
+// primitives (sum over the ancestors). Sum_i a_i rho_i equals the energy. Returns the
+// energy; rho in original simplex order. The very-near list must be empty.
+static double tp0_densities(const Mesh& M, double q, double p, std::vector<double>& rho)
+{
+    const TPParams T(q, p, M.dom);
+    const int nd = near_dim(M.dom), SIZE = M.SIZE;
+    std::vector<double> rn(M.nS, 0.0), rf(M.NC, 0.0);
+    double en = 0;
+    auto center = [&](Int i, double* c) {
+        const double* D = &M.P_near[nd * static_cast<size_t>(i)];
+        for (int k = 0; k < 3; ++k) {
+            c[k] = 0;
+            for (int v = 0; v < SIZE; ++v) c[k] += D[1 + AMB * v + k] / SIZE;
+        }
+    };
+    for (Int i = 0; i < M.nS; ++i) {
+        const double* Xi = &M.P_near[nd * static_cast<size_t>(i)];
+        double x[3];
+        center(i, x);
+        for (LInt k = M.near.diag[i]; k < M.near.rp[i + 1]; ++k) {
+            const Int j = M.near.ci[k];
+            const double* Yj = &M.P_near[nd * static_cast<size_t>(j)];
+            double y[3];
+            center(j, y);
+            PairOut o;
+            tp0_pair(T, Xi[0], x, Xi + 1 + AMB * SIZE, Yj[0], y, Yj + 1 + AMB * SIZE, false, false, o);
+            en += o.energy;
+            rn[i] += o.dens_x;
+            rn[j] += o.dens_y;
+        }
+    }
+    for (Int i = 0; i < M.NC; ++i) {
+        const double* Xi = &M.C_far[FAR_DIM * static_cast<size_t>(i)];
+        for (LInt k = M.far.diag[i]; k < M.far.rp[i + 1]; ++k) {
+            const Int j = M.far.ci[k];
+            const double* Yj = &M.C_far[FAR_DIM * static_cast<size_t>(j)];
+            PairOut o;
+            tp0_pair(T, Xi[0], Xi + 1, Xi + 4, Yj[0], Yj + 1, Yj + 4, false, false, o);
+            en += o.energy;
+            rf[i] += o.dens_x;
+            rf[j] += o.dens_y;
+        }
+    }
+    for (Int C = 0; C < M.NC; ++C)   // PercolateDown (parents precede children)
+        if (M.C_left[C] >= 0) {
+            rf[M.C_left[C]] += rf[C];
+            rf[M.C_right[C]] += rf[C];
+        }
+    rho.assign(M.nS, 0.0);
+    for (Int C = 0; C < M.NC; ++C)
+        if (M.C_left[C] < 0)
+            for (Int i = M.C_begin[C]; i < M.C_end[C]; ++i) rho[M.perm[i]] = rn[i] + rf[C];
+    return en;
+}
+
 }  // namespace oracle
 
 // ============================================================================
@@ -2064,6 +2127,38 @@ double oracle_obstacle_allpairs_energy(void* h, double q, double p)
     auto* H = static_cast<OracleHandle*>(h);
     if (!H->obstacle) return 0.0;
     return obstacle_allpairs_energy(H->M, *H->obstacle, q, p);
+}
+
+
+// SimplexDensities (rho per simplex, original order); returns the energy
+double oracle_simplex_densities(void* h, double q, double p, double* out)
+{
+    const Mesh& M = static_cast<OracleHandle*>(h)->M;
+    std::vector<double> rho;
+    const double en = tp0_densities(M, q, p, rho);
+    std::copy(rho.begin(), rho.end(), out);
+    return en;
+}
+
+// VertexDensities: sum over the simplices at v of (a_i/(n+1)) rho_i, divided by the same sum
+// of a_i/(n+1) (the dual volume); a_i = mean vertex charge * volume
+double oracle_vertex_densities(void* h, double q, double p, double* out)
+{
+    const Mesh& M = static_cast<OracleHandle*>(h)->M;
+    std::vector<double> rho;
+    const double en = tp0_densities(M, q, p, rho);
+    std::vector<double> num(M.nV, 0.0), den(M.nV, 0.0);
+    for (Int i = 0; i < M.nS; ++i) {
+        const Int pi = M.inv_perm[i];
+        const double w = M.pre_vals[4 * static_cast<size_t>(pi) * M.SIZE];   // row 0: a_i / (n+1)
+        for (int c = 0; c < M.SIZE; ++c) {
+            const Int v = M.S[M.SIZE * static_cast<size_t>(i) + c];
+            num[v] += w * rho[i];
+            den[v] += w;
+        }
+    }
+    for (Int v = 0; v < M.nV; ++v) out[v] = den[v] > 0 ? num[v] / den[v] : 0.0;
+    return en;
 }
 
 }  // extern "C"
