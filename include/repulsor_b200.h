@@ -184,6 +184,14 @@ typedef struct rpb_solve_info {
 
 rpb_status rpb_tpm0_solve_info(const rpb_mesh* m, rpb_solve_info* info);
 
+/* EnergyBase::SimplexDensities / VertexDensities (src/Energies/EnergyBase.hpp:129-150):
+ * energy densities per simplex (original order, n_s values) or per vertex (n_v values; the
+ * simplex densities averaged with the weights a_i/(n+1) and divided by the dual volume);
+ * sum_i a_i rho_i is the energy, which `energy` (may be NULL) receives. Not built for
+ * meshes with very-near primitive pairs. */
+rpb_status rpb_tpe0_simplex_densities(rpb_mesh* m, double q, double p, double* density, double* energy);
+rpb_status rpb_tpe0_vertex_densities(rpb_mesh* m, double q, double p, double* density, double* energy);
+
 /* --- obstacle energy --------------------------------------------------------------------- */
 
 /* SimplicialMesh::LoadObstacle (src/SimplicialMesh.hpp:697-719): m takes ownership of the

@@ -306,6 +306,29 @@ class TangentPointEnergy0:
                                         ctypes.byref(e)), "Differential")
         return e.value
 
+    def SimplexDensities(self, M: SimplicialMesh, density=None):
+        """Energy density per simplex into `density` (n_s, original order); returns the
+        energy (src/Energies/EnergyBase.hpp:129-137). Without `density`, returns
+        (energy, densities)."""
+        return self._densities(M, density, "simplex")
+
+    def VertexDensities(self, M: SimplicialMesh, density=None):
+        """Energy density per vertex into `density` (n_v); returns the energy
+        (src/Energies/EnergyBase.hpp:140-148). Without `density`, returns (energy, densities)."""
+        return self._densities(M, density, "vertex")
+
+    def _densities(self, M, density, kind):
+        M = _as_mesh(M)
+        n = M.nS if kind == "simplex" else M.nV
+        given = density is not None
+        out = density if given else np.zeros(n)
+        if out.dtype != np.float64 or not out.flags.c_contiguous or out.size != n:
+            raise RepulsorError(_capi.RPB_EINVAL, f"{kind} densities need a contiguous float64 array of {n} values")
+        e = ctypes.c_double()
+        fn = _capi.load().rpb_tpe0_simplex_densities if kind == "simplex" else _capi.load().rpb_tpe0_vertex_densities
+        check(fn(M._h, self.q, self.p, dptr(out), ctypes.byref(e)), f"{kind.capitalize()}Densities")
+        return e.value if given else (e.value, out)
+
     def DifferentialDevice(self, M: SimplicialMesh, Y_dev_ptr: int, ldY: int = 3, alpha=1.0, beta=0.0) -> float:
         """Y (device pointer, n_v x ldY float64) = alpha dE + beta Y on the mesh stream."""
         e = ctypes.c_double()

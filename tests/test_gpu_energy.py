@@ -104,3 +104,24 @@ def test_energy_rejects_bad_exponents():
     dom, V, S, M, O = _pair(1, True)
     with pytest.raises(rpb.RepulsorError):
         rpb.TangentPointEnergy0(1.0, 4.0).Value(M)
+
+
+@pytest.mark.parametrize("cfg", [1, 2, 3])
+def test_densities_match_oracle(cfg):
+    """EnergyBase::SimplexDensities / VertexDensities against the oracle; the simplex
+    densities weighted by the simplex weights sum to the energy."""
+    dom, (V, S) = meshes.config_mesh(cfg, small=True)
+    M = rpb.SimplicialMesh(V, S)
+    om = oracle.OracleMesh(dom, V, S, threads=8)
+    tpe = rpb.TangentPointEnergy0(6.0, 12.0)
+    E, rho = tpe.SimplexDensities(M)
+    E_ref, rho_ref = om.simplex_densities()
+    assert abs(E - E_ref) <= E_TOL * abs(E_ref)
+    assert np.abs(rho - rho_ref).max() <= D_TOL * np.abs(rho_ref).max()
+    Ev, rv = tpe.VertexDensities(M)
+    _, rv_ref = om.vertex_densities()
+    assert np.abs(rv - rv_ref).max() <= D_TOL * np.abs(rv_ref).max()
+    Pn, _ = om.primitive_data()
+    a = np.zeros(S.shape[0])
+    a[om.tree()["perm"]] = Pn[:, 0]
+    assert abs((a * rho).sum() - E) <= 1e-6 * abs(E)

@@ -112,3 +112,18 @@ def test_golden_fixtures(name):
     assert np.max(np.abs(O.metric_multiply(g["X"]) - g["AX"])) <= 1e-11 * np.max(np.abs(g["AX"]))
     assert np.max(np.abs(O.precondition(g["X"]) - g["PX"])) <= 1e-9 * np.max(np.abs(g["PX"]))
     assert O.allpairs_energy(Q, P) == pytest.approx(float(g["allpairs_energy"]), rel=1e-12)
+
+
+@pytest.mark.parametrize("cfg", [1, 2])
+def test_oracle_densities_integrate_to_the_energy(cfg):
+    """Sum over simplices of a_i * rho_i is the energy (every ordered pair once)."""
+    dom, (V, S) = meshes.config_mesh(cfg, small=True)
+    om = oracle.OracleMesh(dom, V, S, threads=8)
+    en, rho = om.simplex_densities()
+    Pn, _ = om.primitive_data()
+    a = np.zeros(S.shape[0])
+    a[om.tree()["perm"]] = Pn[:, 0]
+    assert abs((a * rho).sum() - en) <= 1e-12 * abs(en)
+    assert abs(en - om.energy()) <= 1e-12 * abs(en)
+    ev, rv = om.vertex_densities()
+    assert rv.shape == (V.shape[0],) and np.all(rv > 0)
