@@ -17,8 +17,9 @@ follow the reference's ClusterTree conventions:
   src/ClusterTree.hpp:706-768), and the transpose of Pre (Post,
   src/ClusterTree.hpp:860-870).
 
-The MLP reads BF16-rounded weights (round to nearest even) and is evaluated here in FP64,
-so GPU-vs-oracle differences come from the FP32 accumulation of the device kernels only.
+The MLP reads BF16-rounded weights (round to nearest even) and BF16-rounded layer inputs,
+as the device's tensor-core pass does, and is evaluated here in FP64; GPU-vs-oracle
+differences come from the FP32 accumulation and from activations that round differently.
 """
 from __future__ import annotations
 
@@ -58,19 +59,24 @@ def gelu_grad(x):
 
 
 def mlp_forward(theta, F, quantize=True):
+    """With quantize (the device's arithmetic): BF16 weights, BF16 layer inputs (features
+    and GELU outputs), FP32-or-better accumulation (FP64 here)."""
     W1, b1, W2, b2, W3, b3 = unpack(theta, quantize)
-    F = np.asarray(F, np.float64)
-    pre1 = F @ W1.T + b1
-    pre2 = gelu(pre1) @ W2.T + b2
-    O = gelu(pre2) @ W3.T + b3
-    return O, (F, pre1, pre2)
+    q = bf16_round if quantize else (lambda x: np.asarray(x, np.float64))
+    Fq = q(np.asarray(F, np.float64))
+    pre1 = Fq @ W1.T + b1
+    h1 = q(gelu(pre1))
+    pre2 = h1 @ W2.T + b2
+    h2 = q(gelu(pre2))
+    O = h2 @ W3.T + b3
+    return O, (Fq, pre1, pre2, h1, h2)
 
 
 def mlp_backward(theta, cache, dO, quantize=True):
-    """Gradient of sum(dO * O) with respect to the (BF16-rounded) parameters."""
+    """Gradient of sum(dO * O) with respect to the (BF16-rounded) parameters; the BF16
+    rounding of the activations passes gradients straight through."""
     W1, b1, W2, b2, W3, b3 = unpack(theta, quantize)
-    F, pre1, pre2 = cache
-    h1, h2 = gelu(pre1), gelu(pre2)
+    F, pre1, pre2, h1, h2 = cache
     g = np.zeros(NPARAM)
     g[OFF_W3:OFF_B3] = (dO.T @ h2).ravel()
     g[OFF_B3:NPARAM] = dO.sum(0)

@@ -84,47 +84,156 @@ struct MlpArgs {
     float* pre2;              // n x NH (training only)
 };
 
-// o = MLP(f) with the FP32 copy of the weights in shared memory; the pre-activations are
-// written to pre1/pre2 when those are non-null (training)
-__device__ __forceinline__ void mlp_eval(const float* sw, const float* f, float* o, float* pre1, float* pre2)
+// ------------------------------------------------------------------------------------------
+// Forward pass on the tensor cores: a block of 4 warps takes 128 clusters, each warp two
+// 16-row tiles; mma.sync m16n8k16 with BF16 operands and FP32 accumulation. Activations
+// enter each layer as BF16 (features, GELU outputs), pre-activations and outputs stay FP32.
+// Weights are staged to shared memory as BF16 with padded row strides, so that the
+// fragment loads of a warp hit 32 distinct banks.
+// ------------------------------------------------------------------------------------------
+constexpr int MLP_TILE = 128;
+constexpr int SF_LD = 24, SH_LD = 72, W1_LD = 24, W2_LD = 72, W3_LD = 72;
+
+struct MlpSmem {
+    __nv_bfloat16 W1[NH * W1_LD];
+    __nv_bfloat16 W2[NH * W2_LD];
+    __nv_bfloat16 W3[8 * W3_LD];          // rows 3..7 zero
+    float b1[NH], b2[NH], b3[8];
+    __nv_bfloat16 F[MLP_TILE * SF_LD];
+    __nv_bfloat16 H[MLP_TILE * SH_LD];
+    float O[MLP_TILE * 4];
+};
+
+__device__ void stage_mlp_weights(const __nv_bfloat16* w, MlpSmem& sm)
 {
-    float h1[NH];
-#pragma unroll 4
-    for (int j = 0; j < NH; ++j) {
-        float s = sw[OFF_B1 + j];
-#pragma unroll
-        for (int k = 0; k < NF; ++k) s = fmaf(sw[OFF_W1 + NF * j + k], f[k], s);
-        if (pre1) pre1[j] = s;
-        h1[j] = gelu(s);
+    const __nv_bfloat16 zero = __float2bfloat16_rn(0.0f);
+    for (int k = threadIdx.x; k < NH * NF; k += blockDim.x) sm.W1[(k / NF) * W1_LD + k % NF] = w[OFF_W1 + k];
+    for (int k = threadIdx.x; k < NH * NH; k += blockDim.x) sm.W2[(k / NH) * W2_LD + k % NH] = w[OFF_W2 + k];
+    for (int k = threadIdx.x; k < 8 * NH; k += blockDim.x)
+        sm.W3[(k / NH) * W3_LD + k % NH] = (k < NO * NH) ? w[OFF_W3 + k] : zero;
+    for (int k = threadIdx.x; k < NH; k += blockDim.x) {
+        sm.b1[k] = __bfloat162float(w[OFF_B1 + k]);
+        sm.b2[k] = __bfloat162float(w[OFF_B2 + k]);
     }
-    o[0] = sw[OFF_B3 + 0];
-    o[1] = sw[OFF_B3 + 1];
-    o[2] = sw[OFF_B3 + 2];
-    for (int j = 0; j < NH; ++j) {
-        float s = sw[OFF_B2 + j];
-#pragma unroll
-        for (int k = 0; k < NH; ++k) s = fmaf(sw[OFF_W2 + NH * j + k], h1[k], s);
-        if (pre2) pre2[j] = s;
-        const float h2 = gelu(s);
-#pragma unroll
-        for (int q = 0; q < NO; ++q) o[q] = fmaf(sw[OFF_W3 + NH * q + j], h2, o[q]);
-    }
+    if (threadIdx.x < 8) sm.b3[threadIdx.x] = threadIdx.x < NO ? __bfloat162float(w[OFF_B3 + threadIdx.x]) : 0.0f;
 }
 
-__global__ void __launch_bounds__(128) k_mlp_forward(MlpArgs A)
+__device__ __forceinline__ uint32_t ld_bf16x2(const __nv_bfloat16* p) { return *reinterpret_cast<const uint32_t*>(p); }
+
+__device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi)
 {
-    extern __shared__ float sw[];
-    stage_weights(A.w, sw);
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= A.n) return;
-    float f[NF];
+    __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<uint32_t*>(&v);
+}
+
+__device__ __forceinline__ void mma_16816(float* c, const uint32_t* a, const uint32_t* b)
+{
+    asm volatile("mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+                 "{%0,%1,%2,%3};\n"
+                 : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+                 : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+// One warp: rows 32 w .. 32 w + 31 of the tile (features in sm.F) -> outputs in sm.O;
+// pre1/pre2 (training, may be null) receive the FP32 pre-activations of the valid rows
+// (global row = row0 + tile row, valid below n).
+__device__ void mlp_tile(MlpSmem& sm, int row0, int n, float* pre1, float* pre2)
+{
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+    float acc[2][8][4];
+    // layer 1: [32 x 16] x [16 x 64]
 #pragma unroll
-    for (int k = 0; k < NF; ++k) f[k] = A.F[NF * static_cast<int64_t>(c) + k];
-    float o[NO];
-    mlp_eval(sw, f, o, A.pre1 ? A.pre1 + NH * static_cast<int64_t>(c) : nullptr,
-             A.pre2 ? A.pre2 + NH * static_cast<int64_t>(c) : nullptr);
+    for (int mt = 0; mt < 2; ++mt) {
+        const int r = 32 * w + 16 * mt + g;
+        uint32_t a[4] = {ld_bf16x2(sm.F + r * SF_LD + 2 * t), ld_bf16x2(sm.F + (r + 8) * SF_LD + 2 * t),
+                         ld_bf16x2(sm.F + r * SF_LD + 2 * t + 8), ld_bf16x2(sm.F + (r + 8) * SF_LD + 2 * t + 8)};
 #pragma unroll
-    for (int q = 0; q < NO; ++q) A.O[NO * static_cast<int64_t>(c) + q] = o[q];
+        for (int nt = 0; nt < 8; ++nt) {
+            const int col = 8 * nt + g;
+            const uint32_t bb[2] = {ld_bf16x2(sm.W1 + col * W1_LD + 2 * t), ld_bf16x2(sm.W1 + col * W1_LD + 2 * t + 8)};
+            acc[mt][nt][0] = acc[mt][nt][1] = acc[mt][nt][2] = acc[mt][nt][3] = 0.0f;
+            mma_16816(acc[mt][nt], a, bb);
+        }
+    }
+    auto epilogue = [&](const float* bias, float* pre) {
+        __syncwarp();
+#pragma unroll
+        for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+            for (int nt = 0; nt < 8; ++nt) {
+                const int r = 32 * w + 16 * mt + g, col = 8 * nt + 2 * t;
+                const float v00 = acc[mt][nt][0] + bias[col], v01 = acc[mt][nt][1] + bias[col + 1];
+                const float v10 = acc[mt][nt][2] + bias[col], v11 = acc[mt][nt][3] + bias[col + 1];
+                if (pre) {
+                    if (row0 + r < n) *reinterpret_cast<float2*>(pre + NH * static_cast<int64_t>(row0 + r) + col) = make_float2(v00, v01);
+                    if (row0 + r + 8 < n) *reinterpret_cast<float2*>(pre + NH * static_cast<int64_t>(row0 + r + 8) + col) = make_float2(v10, v11);
+                }
+                *reinterpret_cast<uint32_t*>(sm.H + r * SH_LD + col) = pack_bf16x2(gelu(v00), gelu(v01));
+                *reinterpret_cast<uint32_t*>(sm.H + (r + 8) * SH_LD + col) = pack_bf16x2(gelu(v10), gelu(v11));
+            }
+        __syncwarp();
+    };
+    epilogue(sm.b1, pre1);
+    // layer 2: [32 x 64] x [64 x 64]
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < 8; ++nt) acc[mt][nt][0] = acc[mt][nt][1] = acc[mt][nt][2] = acc[mt][nt][3] = 0.0f;
+#pragma unroll
+    for (int ks = 0; ks < 4; ++ks)
+#pragma unroll
+        for (int mt = 0; mt < 2; ++mt) {
+            const int r = 32 * w + 16 * mt + g, k0 = 16 * ks + 2 * t;
+            uint32_t a[4] = {ld_bf16x2(sm.H + r * SH_LD + k0), ld_bf16x2(sm.H + (r + 8) * SH_LD + k0),
+                             ld_bf16x2(sm.H + r * SH_LD + k0 + 8), ld_bf16x2(sm.H + (r + 8) * SH_LD + k0 + 8)};
+#pragma unroll
+            for (int nt = 0; nt < 8; ++nt) {
+                const int col = 8 * nt + g;
+                const uint32_t bb[2] = {ld_bf16x2(sm.W2 + col * W2_LD + k0), ld_bf16x2(sm.W2 + col * W2_LD + k0 + 8)};
+                mma_16816(acc[mt][nt], a, bb);
+            }
+        }
+    epilogue(sm.b2, pre2);
+    // layer 3: [32 x 64] x [64 x 8] (3 outputs)
+    float o[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
+#pragma unroll
+    for (int ks = 0; ks < 4; ++ks)
+#pragma unroll
+        for (int mt = 0; mt < 2; ++mt) {
+            const int r = 32 * w + 16 * mt + g, k0 = 16 * ks + 2 * t;
+            uint32_t a[4] = {ld_bf16x2(sm.H + r * SH_LD + k0), ld_bf16x2(sm.H + (r + 8) * SH_LD + k0),
+                             ld_bf16x2(sm.H + r * SH_LD + k0 + 8), ld_bf16x2(sm.H + (r + 8) * SH_LD + k0 + 8)};
+            const uint32_t bb[2] = {ld_bf16x2(sm.W3 + g * W3_LD + k0), ld_bf16x2(sm.W3 + g * W3_LD + k0 + 8)};
+            mma_16816(o[mt], a, bb);
+        }
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt) {
+        const int r = 32 * w + 16 * mt + g, col = 2 * t;
+        if (col < NO) {
+            sm.O[r * 4 + col] = o[mt][0] + sm.b3[col];
+            sm.O[(r + 8) * 4 + col] = o[mt][2] + sm.b3[col];
+        }
+        if (col + 1 < NO) {
+            sm.O[r * 4 + col + 1] = o[mt][1] + sm.b3[col + 1];
+            sm.O[(r + 8) * 4 + col + 1] = o[mt][3] + sm.b3[col + 1];
+        }
+    }
+    __syncwarp();
+}
+
+__global__ void __launch_bounds__(MLP_TILE) k_mlp_forward(MlpArgs A)
+{
+    __shared__ MlpSmem sm;
+    stage_mlp_weights(A.w, sm);
+    const int row0 = blockIdx.x * MLP_TILE;
+    const int c = row0 + threadIdx.x;
+    for (int k = 0; k < NF; ++k)
+        sm.F[threadIdx.x * SF_LD + k] = __float2bfloat16_rn(c < A.n ? A.F[NF * static_cast<int64_t>(c) + k] : 0.0f);
+    __syncthreads();
+    mlp_tile(sm, row0, A.n, A.pre1, A.pre2);
+    __syncthreads();
+    if (c < A.n)
+        for (int q = 0; q < NO; ++q) A.O[NO * static_cast<int64_t>(c) + q] = sm.O[threadIdx.x * 4 + q];
 }
 
 struct MlpBackArgs {
@@ -165,6 +274,8 @@ __global__ void __launch_bounds__(128) k_mlp_backward(MlpBackArgs A)
 // bias gradient (sum of G). P <= 64, Q <= 64.
 constexpr int WG_CHUNK = 1024;
 
+// The forward pass feeds each layer BF16 activations, so X (or GELU(X)) is rounded to BF16
+// here as well.
 __global__ void __launch_bounds__(256) k_weight_grad(int n, const float* G, int P, const float* X, int Q, bool gelu_x,
                                                      float* partial)
 {
@@ -186,6 +297,7 @@ __global__ void __launch_bounds__(256) k_weight_grad(int n, const float* G, int 
             if (valid && col < Q) {
                 x = X[static_cast<int64_t>(Q) * row + col];
                 if (gelu_x) x = gelu(x);
+                x = __bfloat162float(__float2bfloat16_rn(x));
             } else if (valid && col == Q) {
                 x = 1.0f;
             }
@@ -378,18 +490,22 @@ __device__ __forceinline__ void cluster_moment(const ClusterMlpArgs& A, int C, d
 
 __global__ void __launch_bounds__(GAIN_BLOCK) k_cluster_mlp(ClusterMlpArgs A)
 {
-    extern __shared__ float sw[];
-    stage_weights(A.w, sw);
-    const int C = blockIdx.x * blockDim.x + threadIdx.x;
+    static_assert(GAIN_BLOCK == MLP_TILE, "one MLP tile per block");
+    __shared__ MlpSmem sm;
+    stage_mlp_weights(A.w, sm);
+    const int row0 = blockIdx.x * GAIN_BLOCK;
+    const int C = row0 + threadIdx.x;
     double cs[3] = {0, 0, 0};
+    float f[NF];
+    for (int k = 0; k < NF; ++k) f[k] = 0.0f;
+    double R[3] = {0, 0, 0};
+    ClusterDatum cd{};
     if (C < A.NC) {
         const double s = fmax(*A.scale, 1e-300);
-        const ClusterDatum cd = load_datum(A.C_pair, C);
+        cd = load_datum(A.C_pair, C);
         const ClusterDatum root = load_datum(A.C_pair, 0);
         const double dr = fmax(static_cast<double>(A.C_diam[0]), 1e-300);
-        double R[3];
         cluster_moment(A, C, R);
-        float f[NF];
         for (int k = 0; k < 3; ++k) f[k] = static_cast<float>(R[k] / (cd.a * s));
         for (int k = 0; k < 3; ++k) f[3 + k] = static_cast<float>((cd.c[k] - root.c[k]) / dr);
         for (int k = 0; k < 3; ++k) f[6 + k] = static_cast<float>(A.C_an[3 * static_cast<int64_t>(C) + k] / cd.a);
@@ -422,9 +538,14 @@ __global__ void __launch_bounds__(GAIN_BLOCK) k_cluster_mlp(ClusterMlpArgs A)
                                                 (a[2] + b[2]) * (a[2] + b[2])) / (aR * s));
             }
         }
+    }
+    for (int k = 0; k < NF; ++k) sm.F[threadIdx.x * SF_LD + k] = __float2bfloat16_rn(f[k]);
+    __syncthreads();
+    mlp_tile(sm, row0, A.NC, A.pre1, A.pre2);
+    __syncthreads();
+    if (C < A.NC) {
         float o[NO];
-        mlp_eval(sw, f, o, A.pre1 ? A.pre1 + NH * static_cast<int64_t>(C) : nullptr,
-                 A.pre2 ? A.pre2 + NH * static_cast<int64_t>(C) : nullptr);
+        for (int q = 0; q < NO; ++q) o[q] = sm.O[threadIdx.x * 4 + q];
         const double inv_a = 1.0 / cd.a;
         for (int q = 0; q < 3; ++q) {
             const float oc = fminf(fmaxf(o[q], -GAIN_CLAMP), GAIN_CLAMP);
@@ -728,7 +849,7 @@ static rpb_status learned_forward(rpb_mesh* m, rpb_mlp* mlp, const double* R, do
     ca.pre1 = training ? L.pre1.ptr : nullptr;
     ca.pre2 = training ? L.pre2.ptr : nullptr;
     ca.Rc = training ? L.Rc.ptr : nullptr;
-    k_cluster_mlp<<<(m->NC + GAIN_BLOCK - 1) / GAIN_BLOCK, GAIN_BLOCK, NPARAM * sizeof(float), s>>>(ca);
+    k_cluster_mlp<<<(m->NC + GAIN_BLOCK - 1) / GAIN_BLOCK, GAIN_BLOCK, 0, s>>>(ca);
     k_vertex_expand<<<(m->nV + 255) / 256, 256, 0, s>>>(m->nV, m->size, m->vp_rp.ptr, m->vp_slot.ptr, m->pre_vals.ptr,
                                                         m->leaf_of.ptr, m->C_parent.ptr, L.c.ptr, L.zmean.ptr, z);
     RPB_CUDA(cudaGetLastError());
@@ -857,7 +978,7 @@ rpb_status rpb_mlp_eval(rpb_mlp* mlp, const float* F, int64_t n, const float* dO
     RPB_CUDA(cudaMemcpy(dF.ptr, F, dF.bytes(), cudaMemcpyHostToDevice));
     MlpArgs ma;
     ma.n = static_cast<int>(n); ma.w = mlp->w16.ptr; ma.F = dF.ptr; ma.O = dOut.ptr; ma.pre1 = p1.ptr; ma.pre2 = p2.ptr;
-    k_mlp_forward<<<static_cast<unsigned>((n + 127) / 128), 128, NPARAM * sizeof(float)>>>(ma);
+    k_mlp_forward<<<static_cast<unsigned>((n + MLP_TILE - 1) / MLP_TILE), MLP_TILE>>>(ma);
     RPB_CUDA(cudaGetLastError());
     RPB_CUDA(cudaMemcpy(O, dOut.ptr, dOut.bytes(), cudaMemcpyDeviceToHost));
     if (dO && grad) {

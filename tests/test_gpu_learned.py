@@ -13,9 +13,12 @@ from repulsor_b200.learned import LearnedPreconditioner, train, training_pairs
 
 pytestmark = pytest.mark.gpu
 
-O_TOL = 1e-4        # MLP outputs: FP32 accumulation vs FP64, relative to max |O|
-G_TOL = 1e-3        # parameter gradients, relative in the 2-norm
-Z_TOL = 1e-4        # preconditioner output, relative in the max norm
+# The device MLP runs on the tensor cores with BF16 layer inputs and FP32 accumulation; the
+# oracle rounds the same activations in FP64 arithmetic, so an activation can round to the
+# neighbouring BF16 value (relative step 2^-8) where the FP32 and FP64 sums straddle a tie.
+O_TOL = 5e-3        # MLP outputs, relative to max |O|
+G_TOL = 1e-2        # parameter gradients, relative in the 2-norm
+Z_TOL = 2e-3        # preconditioner output, relative in the max norm
 Q, P = 6.0, 12.0
 
 
