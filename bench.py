@@ -172,6 +172,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true")
     ap.add_argument("--no-solve", action="store_true", help="skip the Solve timings on the icosphere level-6 mesh")
+    ap.add_argument("--flow-max-iter", type=int, default=3000, help="iteration limit of the full-flow Solve")
     ap.add_argument("--flow", action="store_true",
                     help="only the full flow step on two linked tori (1,228,800 triangles) with an obstacle")
     args = ap.parse_args()
@@ -438,8 +439,7 @@ def run_flow(args):
     net.attach(M)
     B = D - D.mean(0)
     t = time.perf_counter()
-    tpm.Solve(M, 1.0, B, max_iter=20000, tolerance=1e-6,
-              precond=rpb.PRECOND_LEARNED, strict=False)
+    tpm.Solve(M, 1.0, B, max_iter=args.flow_max_iter, tolerance=1e-6, precond=rpb.PRECOND_LEARNED, strict=False)
     out["solve_s"] = time.perf_counter() - t
     info = tpm.SolveInfo(M)
     out["solve"] = {"iterations": info["iterations"], "fallback_iteration": info["fallback_iteration"],

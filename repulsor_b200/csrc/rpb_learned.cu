@@ -353,12 +353,13 @@ __global__ void k_adam(int n, float* theta, __nv_bfloat16* w16, const float* g, 
 }
 
 // ------------------------------------------------------------------------------------------
-// The preconditioner application in four launches:
+// The preconditioner application in five launches:
 //   k_prim_scan     primitive moments a_i mean(r) -> in-block prefix sums; sum of |r|^2
 //   k_scan_totals   prefix sums of the block totals; the global sum of |r|^2
 //   k_cluster_mlp   per cluster: R_C (and its children's) as prefix-sum differences,
 //                   16 features, the MLP, gains, c_C = g_C R_C / A_C; sum_C A_C c_C
-//   k_vertex_expand z_v = sum_{i at v} w_i sum_{C containing i} c_C - mean(z)
+//   k_prim_expand   Z_i = sum_{C containing i} c_C
+//   k_vertex_expand z_v = sum_{i at v} w_i Z_i - mean(z)
 // ------------------------------------------------------------------------------------------
 constexpr int GAIN_BLOCK = 128;
 // Gains g_C = exp(clamp(o_C)) keep z . r > 0 for every residual (flexible CG never meets
@@ -588,11 +589,27 @@ __global__ void __launch_bounds__(GAIN_BLOCK) k_cluster_mlp(ClusterMlpArgs A)
     }
 }
 
-// z_v = sum over the primitives i at v of w_i * (sum over the clusters containing i of c_C),
-// minus the mean of z (translations are the kernel of the metric)
+// Z_i = sum over the clusters containing primitive i of c_C (PercolateDown +
+// ClustersToPrimitives as an ancestor walk)
+__global__ void k_prim_expand(int N, const int* leaf_of, const int* C_parent, const double* c, double* Z)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    double z0 = 0, z1 = 0, z2 = 0;
+    for (int C = leaf_of[i]; C >= 0; C = C_parent[C]) {
+        z0 += c[3 * static_cast<int64_t>(C)];
+        z1 += c[3 * static_cast<int64_t>(C) + 1];
+        z2 += c[3 * static_cast<int64_t>(C) + 2];
+    }
+    Z[3 * static_cast<int64_t>(i)] = z0;
+    Z[3 * static_cast<int64_t>(i) + 1] = z1;
+    Z[3 * static_cast<int64_t>(i) + 2] = z2;
+}
+
+// z_v = sum over the primitives i at v of w_i Z_i, minus the mean of z (translations are
+// the kernel of the metric)
 __global__ void k_vertex_expand(int nV, int size, const int* vp_rp, const int* vp_slot, const double* pre_vals,
-                                const int* leaf_of, const int* C_parent, const double* c, const double* zmean,
-                                double* z)
+                                const double* Z, const double* zmean, double* z)
 {
     const int v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= nV) return;
@@ -601,15 +618,9 @@ __global__ void k_vertex_expand(int nV, int size, const int* vp_rp, const int* v
         const int slot = vp_slot[k];
         const int i = slot / size, l = slot - i * size;
         const double w = pre_vals[(4 * static_cast<int64_t>(i)) * size + l];
-        double z0 = 0, z1 = 0, z2 = 0;
-        for (int C = leaf_of[i]; C >= 0; C = C_parent[C]) {
-            z0 += c[3 * static_cast<int64_t>(C)];
-            z1 += c[3 * static_cast<int64_t>(C) + 1];
-            z2 += c[3 * static_cast<int64_t>(C) + 2];
-        }
-        a0 += w * z0;
-        a1 += w * z1;
-        a2 += w * z2;
+        a0 += w * Z[3 * static_cast<int64_t>(i)];
+        a1 += w * Z[3 * static_cast<int64_t>(i) + 1];
+        a2 += w * Z[3 * static_cast<int64_t>(i) + 2];
     }
     z[3 * static_cast<int64_t>(v)] = a0 - zmean[0];
     z[3 * static_cast<int64_t>(v) + 1] = a1 - zmean[1];
@@ -824,7 +835,7 @@ static rpb_status cluster_moments(rpb_mesh* m, const double* R, double* Rc)
     return range_sums3(m, m->learned->tmp3.ptr, Rc);
 }
 
-// z = M_learned(R) (device, n_v x 3) in four launches; with `training` the features,
+// z = M_learned(R) (device, n_v x 3) in five launches; with `training` the features,
 // activations, outputs and cluster moments are kept for the backward pass.
 static rpb_status learned_forward(rpb_mesh* m, rpb_mlp* mlp, const double* R, double* z, bool training)
 {
@@ -850,8 +861,9 @@ static rpb_status learned_forward(rpb_mesh* m, rpb_mlp* mlp, const double* R, do
     ca.pre2 = training ? L.pre2.ptr : nullptr;
     ca.Rc = training ? L.Rc.ptr : nullptr;
     k_cluster_mlp<<<(m->NC + GAIN_BLOCK - 1) / GAIN_BLOCK, GAIN_BLOCK, 0, s>>>(ca);
+    k_prim_expand<<<(m->N + 255) / 256, 256, 0, s>>>(m->N, m->leaf_of.ptr, m->C_parent.ptr, L.c.ptr, L.tmp3.ptr);
     k_vertex_expand<<<(m->nV + 255) / 256, 256, 0, s>>>(m->nV, m->size, m->vp_rp.ptr, m->vp_slot.ptr, m->pre_vals.ptr,
-                                                        m->leaf_of.ptr, m->C_parent.ptr, L.c.ptr, L.zmean.ptr, z);
+                                                        L.tmp3.ptr, L.zmean.ptr, z);
     RPB_CUDA(cudaGetLastError());
     return RPB_OK;
 }

@@ -1,11 +1,14 @@
 // Drives the header-only C++20 mirror (include/repulsor_b200/Repulsor.hpp) the way
 // Repulsor's own drivers use the reference API (Example/main.cpp): build a mesh, evaluate
-// TangentPointEnergy0 Value/Differential, multiply the metric, solve. Input: a mesh file
-// "nV nS dom" followed by the coordinates and simplices; output: energy, |dE|_max,
-// sum(A dE), iterations and the relative residual, one per line.
+// TangentPointEnergy0 Value/Differential/SimplexDensities, multiply the metric, solve, load
+// an obstacle and evaluate TangentPointObstacleEnergy. Input: a mesh file "nV nS dom"
+// followed by the coordinates and simplices; output: energy, |dE|_max, sum(A dE),
+// iterations, the relative residual, the energy from the densities call and the obstacle
+// energy, one per line.
 #include <cmath>
 #include <cstdio>
 #include <fstream>
+#include <memory>
 #include <vector>
 
 #include "repulsor_b200/Repulsor.hpp"
@@ -42,7 +45,16 @@ int run(const std::vector<double>& V, const std::vector<int>& S, int nV, int nS)
     const std::vector<double> rr = tpm.Solver_RelativeResiduals();
     double rmax = 0;
     for (double r : rr) rmax = std::fmax(rmax, r);
-    std::printf("%.17g\n%.17g\n%.17g\n%d\n%.6g\n", E, dmax, ysum, static_cast<int>(tpm.Solver_IterationCount()), rmax);
+    std::vector<double> rho(nS);
+    const double Ed = tpe.SimplexDensities(M, rho.data());
+    // an obstacle: the mesh shifted by 3 along z, loaded into the mesh
+    std::vector<double> VO(V);
+    for (int v = 0; v < nV; ++v) VO[3 * v + 2] += 3.0;
+    M.LoadObstacle(std::make_unique<Mesh_T>(VO.data(), nV, S.data(), nS, 4));
+    Repulsor::TangentPointObstacleEnergy<Mesh_T> tpo(6.0, 12.0);
+    const double Eo = tpo.Value(M);
+    std::printf("%.17g\n%.17g\n%.17g\n%d\n%.6g\n%.17g\n%.17g\n", E, dmax, ysum,
+                static_cast<int>(tpm.Solver_IterationCount()), rmax, Ed, Eo);
     // errors follow the reference: print and do nothing
     tpm.MultiplyMetric(M, 1.0, D.data(), 3, 0.0, Y.data(), 3, 2);
     return 0;

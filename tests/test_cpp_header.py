@@ -46,6 +46,7 @@ def test_header_driver_matches_python_mirror(tmp_path, cfg):
     out = subprocess.run([exe, mesh_file], check=True, capture_output=True, text=True)
     lines = out.stdout.split()
     E, dmax, ysum, iters, rmax = float(lines[0]), float(lines[1]), float(lines[2]), int(lines[3]), float(lines[4])
+    Ed, Eo = float(lines[5]), float(lines[6])
     assert "nrhs = 2 != 3 = AMB_DIM" in out.stderr          # print-and-return error path
 
     M = rpb.SimplicialMesh(V, S)
@@ -61,3 +62,10 @@ def test_header_driver_matches_python_mirror(tmp_path, cfg):
     assert abs(ysum - Y.sum()) <= 1e-9 * np.abs(Y).sum()
     assert iters == tpm.Solver_IterationCount()
     assert rmax <= 1e-6
+    assert abs(Ed - E_py) <= 1e-6 * abs(E_py)          # the densities kernel sums in another order
+    Mo = rpb.SimplicialMesh(V, S)
+    VO = V.copy()
+    VO[:, 2] += 3.0
+    Mo.LoadObstacle(rpb.SimplicialMesh(VO, S))
+    Eo_py = rpb.TangentPointObstacleEnergy(6.0, 12.0).Value(Mo)
+    assert Eo > 0 and abs(Eo - Eo_py) <= 1e-12 * abs(Eo_py)
