@@ -40,6 +40,23 @@ FLOPS_NEAR_PAIR = 185.0
 LAUNCHES_PER_STEP = 7
 
 
+def max_over_ranks(x, dist, device):
+    """The slowest rank's time (replicas run the same work; the job ends with the slowest)."""
+    if not dist:
+        return x
+    import torch
+
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(world, steps_per_rank, max_ms):
+    """Whole-job evaluations per second: every rank evaluates its own mesh `steps_per_rank`
+    times; the job takes the slowest rank's `max_ms`."""
+    return world * steps_per_rank / (max_ms * 1e-3)
+
+
 def pair_traffic_from_profile():
     """DRAM bytes (read + write) of the two pair launches of one evaluation, from the ncu
     capture summarised in profiles/k_tp0_pairs_torus160x120.md (null if absent)."""
@@ -234,12 +251,8 @@ def main():
         dist.barrier()
     time.sleep(0.3)
     clocks = sampler.stop()
-    total_ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
-    if dist:
-        t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-    value = world * args.steps / (total_ms * 1e-3)
+    total_ms = max_over_ranks(sum(s.elapsed_time(e) for s, e in zip(starts, ends)), dist, "cuda")
+    value = replica_throughput(world, args.steps, total_ms)
 
     # end to end through the public API with pinned host buffers (H2D of V, D2H of dE and E)
     Vh = torch.tensor(V).pin_memory()
@@ -253,12 +266,8 @@ def main():
     for _ in range(e2e_steps):
         M.SemiStaticUpdate(Vn)
         tpe.Differential(M, 1.0, 0.0, Yn)
-    e2e_s = time.perf_counter() - t0
-    if dist:
-        t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e = {"value": world * e2e_steps / e2e_s, "unit": "evals/s", "h2d_bytes_per_step": V.nbytes,
+    e2e_s = max_over_ranks(time.perf_counter() - t0, dist, "cuda")
+    e2e = {"value": replica_throughput(world, e2e_steps, e2e_s * 1e3), "unit": "evals/s", "h2d_bytes_per_step": V.nbytes,
            "d2h_bytes_per_step": Yn.nbytes + 8,
            "how": "SimplicialMesh.SemiStaticUpdate(host V) + TangentPointEnergy0.Differential(M, 1, 0, host Y), "
                   "pinned host buffers, wall clock per step"}
