@@ -190,52 +190,89 @@ struct SpmmArgs {
     bool accumulate;          // y += (very-near add-in) instead of y =
 };
 
-// One warp per row, lanes over the row's blocks. Input rows are gathered in FP64
-// (the operator's result cancels strongly for smooth fields: with the diagonal built
-// from the same stored values, FP64 keeps that cancellation exact to ~1e-15).
+// SPMM_LANES lanes per row, striding over the row's blocks (rows hold ~30-60 blocks at
+// theta = 0.5). Input rows are gathered in FP64 (the operator's result cancels strongly for
+// smooth fields: with the diagonal built from the same stored values, FP64 keeps that
+// cancellation exact to ~1e-15). The lanes of a row combine their partial sums by a
+// reduce-scatter (BD = 12: 6 + 3 shuffles, each lane ends with 3 of the 12 outputs) or an
+// xor butterfly (BD = 3), in a fixed order.
+constexpr int SPMM_LANES = 4;
+
 template <int BD>
 __global__ void __launch_bounds__(256) k_block_spmm(SpmmArgs<BD> A)
 {
-    const int lane = threadIdx.x & 31;
-    const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    if (row >= A.rows0 + A.rows1) return;
+    static_assert(BD == 12 || BD == 3, "block width 12 (metric) or 3 (pseudo-Laplacian)");
+    const int sub = threadIdx.x & (SPMM_LANES - 1);
+    const int row = (blockIdx.x * blockDim.x + threadIdx.x) / SPMM_LANES;
+    const bool active = row < A.rows0 + A.rows1;
     const bool first = row < A.rows0;
     const int i = first ? row : row - A.rows0;
-    const int64_t* rp = first ? A.rp0 : A.rp1;
-    const int* ci = first ? A.ci0 : A.ci1;
-    const float2* vals = first ? A.v0 : A.v1;
     const double* x = first ? A.x0 : A.x1;
     double acc[BD];
 #pragma unroll
     for (int c = 0; c < BD; ++c) acc[c] = 0.0;
-    for (int64_t k = rp[i] + lane; k < rp[i + 1]; k += 32) {
-        const int j = __ldg(ci + k);
-        const float2 a = __ldg(vals + k);
-        const double ax = a.x, ay = a.y;
-        if constexpr (BD % 2 == 0) {
-            const double2* xp = reinterpret_cast<const double2*>(x + BD * static_cast<int64_t>(j));
+    if (active) {
+        const int64_t* rp = first ? A.rp0 : A.rp1;
+        const int* ci = first ? A.ci0 : A.ci1;
+        const float2* vals = first ? A.v0 : A.v1;
+        for (int64_t k = rp[i] + sub; k < rp[i + 1]; k += SPMM_LANES) {
+            const int j = __ldg(ci + k);
+            const float2 a = __ldg(vals + k);
+            const double ax = a.x, ay = a.y;
+            if constexpr (BD == 12) {
+                const double2* xp = reinterpret_cast<const double2*>(x + BD * static_cast<int64_t>(j));
 #pragma unroll
-            for (int q = 0; q < BD / 2; ++q) {
-                const double2 t = __ldg(xp + q);
-                acc[2 * q] += (2 * q < 3 ? ax : ay) * t.x;
-                acc[2 * q + 1] += (2 * q + 1 < 3 ? ax : ay) * t.y;
+                for (int q = 0; q < BD / 2; ++q) {
+                    const double2 t = __ldg(xp + q);
+                    acc[2 * q] += (2 * q < 3 ? ax : ay) * t.x;
+                    acc[2 * q + 1] += (2 * q + 1 < 3 ? ax : ay) * t.y;
+                }
+            } else {
+#pragma unroll
+                for (int c = 0; c < BD; ++c) acc[c] += ax * __ldg(x + BD * static_cast<int64_t>(j) + c);
             }
-        } else {
-#pragma unroll
-            for (int c = 0; c < BD; ++c) acc[c] += (c < 3 ? ax : ay) * __ldg(x + BD * static_cast<int64_t>(j) + c);
         }
     }
-    double out[BD];
+    const double2 dg = active ? (first ? A.d0 : A.d1)[i] : make_double2(0.0, 0.0);
+    double* y = active ? (first ? A.y0 : A.y1) + BD * static_cast<int64_t>(i) : nullptr;
+    if constexpr (BD == 12) {
+        // reduce-scatter over the 4 lanes: lane (b1, b0) ends with outputs 6 b1 + 3 b0 .. +2
+        const bool b1 = sub & 2, b0 = sub & 1;
+        double h[6];
 #pragma unroll
-    for (int c = 0; c < BD; ++c) out[c] = warp_sum_f64(acc[c]);
-    if (lane < BD) {
-        const double2 dg = (first ? A.d0 : A.d1)[i];
-        double* y = (first ? A.y0 : A.y1) + BD * static_cast<int64_t>(i);
-        double val = out[0];
+        for (int q = 0; q < 6; ++q) {
+            const double send = b1 ? acc[q] : acc[q + 6];
+            const double keep = b1 ? acc[q + 6] : acc[q];
+            h[q] = keep + __shfl_xor_sync(0xffffffffu, send, 2);
+        }
+        double f[3];
 #pragma unroll
-        for (int c = 1; c < BD; ++c) val = (lane == c) ? out[c] : val;
-        val += (lane < 3 ? dg.x : dg.y) * x[BD * static_cast<int64_t>(i) + lane];
-        y[lane] = A.accumulate ? y[lane] + val : val;
+        for (int q = 0; q < 3; ++q) {
+            const double send = b0 ? h[q] : h[q + 3];
+            const double keep = b0 ? h[q + 3] : h[q];
+            f[q] = keep + __shfl_xor_sync(0xffffffffu, send, 1);
+        }
+        if (active) {
+            const int base = 6 * (b1 ? 1 : 0) + 3 * (b0 ? 1 : 0);
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+                const int c = base + q;
+                const double val = f[q] + (c < 3 ? dg.x : dg.y) * x[BD * static_cast<int64_t>(i) + c];
+                y[c] = A.accumulate ? y[c] + val : val;
+            }
+        }
+    } else {
+#pragma unroll
+        for (int off = 1; off < SPMM_LANES; off <<= 1)
+#pragma unroll
+            for (int c = 0; c < BD; ++c) acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], off);
+        if (active && sub < BD) {
+            double val = acc[0];
+#pragma unroll
+            for (int c = 1; c < BD; ++c) val = (sub == c) ? acc[c] : val;
+            val += dg.x * x[BD * static_cast<int64_t>(i) + sub];
+            y[sub] = A.accumulate ? y[sub] + val : val;
+        }
     }
 }
 
@@ -489,7 +526,7 @@ static rpb_status apply_operator(rpb_mesh* m, const float2* nf, const double2* n
         sa.rp1 = m->far.rp.ptr; sa.ci1 = m->far.ci.ptr; sa.v1 = ff; sa.d1 = ffd;
         sa.x1 = m->buf_Cin64.ptr; sa.y1 = m->buf_Cout.ptr;
         sa.accumulate = false;
-        k_block_spmm<BD><<<(sa.rows0 + sa.rows1 + 7) / 8, 256, 0, s>>>(sa);
+        k_block_spmm<BD><<<((sa.rows0 + sa.rows1) * SPMM_LANES + 255) / 256, 256, 0, s>>>(sa);
         RPB_CUDA(cudaGetLastError());
     }
     if (VF) {
@@ -499,7 +536,7 @@ static rpb_status apply_operator(rpb_mesh* m, const float2* nf, const double2* n
         sa.rp0 = m->verynear.rp.ptr; sa.ci0 = m->verynear.ci.ptr; sa.v0 = vf; sa.d0 = vfd;
         sa.x0 = m->buf_Pin64.ptr; sa.y0 = m->buf_Pout.ptr;
         sa.accumulate = true;
-        k_block_spmm<BD><<<(sa.rows0 + 7) / 8, 256, 0, s>>>(sa);
+        k_block_spmm<BD><<<(sa.rows0 * SPMM_LANES + 255) / 256, 256, 0, s>>>(sa);
         RPB_CUDA(cudaGetLastError());
     }
     PostArgs<BD> po;
