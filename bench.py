@@ -74,7 +74,8 @@ def workload_mesh():
 
 
 WORKLOAD = {"workload": "torus R=1 r=0.4 160x120 (19,200 vertices, 38,400 triangles), q=6 p=12 theta=0.5",
-            "step": "SemiStaticUpdate + Differential (energy + dE, FP32 pair kernels with FP64 projections)",
+            "step": "SemiStaticUpdate + Differential (energy + dE, FP32 pair kernels with FP64 near-field projections), "
+                    "one CUDA graph per step",
             "l2": "256 MiB buffer overwritten before every timed step"}
 
 
@@ -189,6 +190,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true")
     ap.add_argument("--no-solve", action="store_true", help="skip the Solve timings on the icosphere level-6 mesh")
+    ap.add_argument("--no-graph", action="store_true", help="time direct launches instead of a captured CUDA graph")
     ap.add_argument("--flow-max-iter", type=int, default=3000, help="iteration limit of the full-flow Solve")
     ap.add_argument("--flow", action="store_true",
                     help="only the full flow step on two linked tori (1,228,800 triangles) with an obstacle")
@@ -223,14 +225,36 @@ def main():
     Vd = torch.tensor(V, device="cuda")
     Yd = torch.zeros((V.shape[0], 3), dtype=torch.float64, device="cuda")
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
-    ext = torch.cuda.ExternalStream(M.stream())
+    # the mesh works on a torch stream so that a step can be captured into a CUDA graph
+    ext = torch.cuda.Stream()
+    M.set_stream(ext.cuda_stream)
 
     def step():
+        # the energy stays on the device (no host read per step); e2e below reads it back
         M.SemiStaticUpdateDevice(Vd.data_ptr())
-        tpe.DifferentialDevice(M, Yd.data_ptr(), 3, 1.0, 0.0)
+        tpe.DifferentialDevice(M, Yd.data_ptr(), 3, 1.0, 0.0, want_energy=False)
 
     for _ in range(args.warmup):
         step()
+    torch.cuda.synchronize()
+    # one step as a CUDA graph (8 nodes: the coordinate copy and the seven kernels), replayed
+    # per timed step; direct launches if capture is not possible
+    graph = None
+    if not args.no_graph:
+        try:
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g, stream=ext):
+                step()
+            torch.cuda.synchronize()
+            graph = g
+        except Exception as exc:   # noqa: BLE001 - capture is an optimisation only
+            print(f"CUDA graph capture failed ({exc}); timing direct launches", file=sys.stderr)
+            graph = None
+        M.set_stream(ext.cuda_stream)
+    run_step = graph.replay if graph is not None else step
+    for _ in range(args.warmup):
+        with torch.cuda.stream(ext):
+            run_step()
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
@@ -244,8 +268,8 @@ def main():
         with torch.cuda.stream(ext):
             flush.fill_(k & 0xFF)
             starts[k].record(ext)
-        step()
-        ends[k].record(ext)
+            run_step()
+            ends[k].record(ext)
     torch.cuda.synchronize()
     if dist:
         dist.barrier()

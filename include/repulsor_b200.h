@@ -138,7 +138,10 @@ rpb_status rpb_tpe0_value(rpb_mesh* m, double q, double p, double* energy);
 rpb_status rpb_tpe0_differential(rpb_mesh* m, double q, double p, double alpha, double beta, double* Y, int ldY,
                                  double* energy);
 
-/* Same with Y a device pointer (nV x ldY) on the mesh stream; energy written to host. */
+/* Same with Y a device pointer (nV x ldY) on the mesh stream. With `energy` non-NULL the
+ * energy is read back (synchronizing the stream); with NULL nothing synchronizes and the
+ * call (like rpb_mesh_semistatic_update_device) may be captured into a CUDA graph;
+ * rpb_tpe0_energy_device then places the energy in device memory. */
 rpb_status rpb_tpe0_differential_device(rpb_mesh* m, double q, double p, double alpha, double beta, double* Y_dev,
                                         int ldY, double* energy);
 
@@ -183,6 +186,10 @@ typedef struct rpb_solve_info {
 } rpb_solve_info;
 
 rpb_status rpb_tpm0_solve_info(const rpb_mesh* m, rpb_solve_info* info);
+
+/* The energy of the last evaluation on this mesh (Value / Differential), written to the
+ * device double `energy_dev` asynchronously on the mesh stream (graph-capturable). */
+rpb_status rpb_tpe0_energy_device(rpb_mesh* m, double* energy_dev);
 
 /* EnergyBase::SimplexDensities / VertexDensities (src/Energies/EnergyBase.hpp:129-150):
  * energy densities per simplex (original order, n_s values) or per vertex (n_v values; the

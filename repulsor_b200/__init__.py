@@ -329,13 +329,17 @@ class TangentPointEnergy0:
         check(fn(M._h, self.q, self.p, dptr(out), ctypes.byref(e)), f"{kind.capitalize()}Densities")
         return e.value if given else (e.value, out)
 
-    def DifferentialDevice(self, M: SimplicialMesh, Y_dev_ptr: int, ldY: int = 3, alpha=1.0, beta=0.0) -> float:
-        """Y (device pointer, n_v x ldY float64) = alpha dE + beta Y on the mesh stream."""
+    def DifferentialDevice(self, M: SimplicialMesh, Y_dev_ptr: int, ldY: int = 3, alpha=1.0, beta=0.0,
+                           want_energy: bool = True):
+        """Y (device pointer, n_v x ldY float64) = alpha dE + beta Y on the mesh stream.
+        Returns the energy (synchronizing) or, with want_energy=False, None without any
+        synchronization (the call can then be captured into a CUDA graph)."""
         e = ctypes.c_double()
         check(_capi.load().rpb_tpe0_differential_device(M._h, self.q, self.p, float(alpha), float(beta),
-                                                        ctypes.c_void_p(Y_dev_ptr), ldY, ctypes.byref(e)),
+                                                        ctypes.c_void_p(Y_dev_ptr), ldY,
+                                                        ctypes.byref(e) if want_energy else None),
               "DifferentialDevice")
-        return e.value
+        return e.value if want_energy else None
 
 
 class TangentPointObstacleEnergy:

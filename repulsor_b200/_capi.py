@@ -101,6 +101,7 @@ SIGNATURES = {
                                               ctypes.c_int64, _vp, _vp, _vp, _vp, ctypes.c_double, ctypes.c_double,
                                               _vp, _vp]),
     "rpb_tpm0_solve_info": (ctypes.c_int, [_vp, ctypes.POINTER(SolveInfo)]),
+    "rpb_tpe0_energy_device": (ctypes.c_int, [_vp, _vp]),
     "rpb_tpe0_simplex_densities": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double, _dp, _dp]),
     "rpb_tpe0_vertex_densities": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double, _dp, _dp]),
     "rpb_mesh_load_obstacle": (ctypes.c_int, [_vp, _vp]),

@@ -220,6 +220,9 @@ rpb_status launch_collect_gather(rpb_mesh* m, double alpha, double beta, double*
     return RPB_OK;
 }
 
+// (very-near + near) + far, the order evaluate() uses on the host
+static __global__ void k_sum_energy_parts(const double* e, double* out) { *out = (e[2] + e[0]) + e[1]; }
+
 // Full energy (+ differential into device Y) evaluation on the mesh stream.
 rpb_status evaluate(rpb_mesh* m, double q, double p, bool diff, double alpha, double beta, double* Y_dev, int ldY,
                     double* energy_host)
@@ -624,6 +627,15 @@ rpb_status rpb_tpe0_differential_device(rpb_mesh* m, double q, double p, double 
     if (!m || !Y_dev) { set_error("null argument"); return RPB_EINVAL; }
     if (ldY < 3) { set_error("ldY must be >= AMB_DIM = 3"); return RPB_EINVAL; }
     return evaluate(m, q, p, true, alpha, beta, Y_dev, ldY, energy);
+}
+
+rpb_status rpb_tpe0_energy_device(rpb_mesh* m, double* energy_dev)
+{
+    if (!m || !energy_dev) { set_error("null argument"); return RPB_EINVAL; }
+    RPB_CUDA(cudaSetDevice(m->device));
+    k_sum_energy_parts<<<1, 1, 0, m->stream>>>(m->energy.ptr, energy_dev);
+    RPB_CUDA(cudaGetLastError());
+    return RPB_OK;
 }
 
 rpb_status rpb_tpe0_differential(rpb_mesh* m, double q, double p, double alpha, double beta, double* Y, int ldY,

@@ -1,6 +1,8 @@
 """TangentPointEnergy0 Value / Differential on the B200 through the C ABI, against
 the FP64 oracle. Tolerances: energy 1e-6 relative; differential 1e-5 relative in
 max norm (||D_gpu - D_ref||_inf / ||D_ref||_inf)."""
+import ctypes
+
 import numpy as np
 import pytest
 
@@ -125,3 +127,41 @@ def test_densities_match_oracle(cfg):
     a = np.zeros(S.shape[0])
     a[om.tree()["perm"]] = Pn[:, 0]
     assert abs((a * rho).sum() - E) <= 1e-6 * abs(E)
+
+
+def test_differential_in_a_cuda_graph_matches_direct_call():
+    """SemiStaticUpdateDevice + DifferentialDevice without an energy readback capture into
+    a CUDA graph; replaying it (and rpb_tpe0_energy_device) gives the direct results."""
+    torch = pytest.importorskip("torch")
+    from repulsor_b200 import _capi
+
+    dom, (V, S) = meshes.config_mesh(2, small=True)
+    M = rpb.SimplicialMesh(V, S)
+    tpe = rpb.TangentPointEnergy0(6.0, 12.0)
+    D_ref = np.zeros_like(V)
+    E_ref = tpe.Differential(M, 1.0, 0.0, D_ref)
+    s = torch.cuda.Stream()
+    M.set_stream(s.cuda_stream)
+    Vd = torch.tensor(V * 1.0, device="cuda")
+    Yd = torch.zeros((V.shape[0], 3), dtype=torch.float64, device="cuda")
+    Ed = torch.zeros(1, dtype=torch.float64, device="cuda")
+    lib = _capi.load()
+
+    def step():
+        M.SemiStaticUpdateDevice(Vd.data_ptr())
+        tpe.DifferentialDevice(M, Yd.data_ptr(), 3, 1.0, 0.0, want_energy=False)
+        _capi.check(lib.rpb_tpe0_energy_device(M._h, ctypes.c_void_p(Ed.data_ptr())), "energy_device")
+
+    with torch.cuda.stream(s):
+        step()
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=s):
+        step()
+    Yd.zero_()
+    Ed.zero_()
+    with torch.cuda.stream(s):
+        g.replay()
+    torch.cuda.synchronize()
+    assert abs(float(Ed.item()) - E_ref) <= 1e-12 * abs(E_ref)
+    np.testing.assert_allclose(Yd.cpu().numpy(), D_ref, rtol=0, atol=1e-12 * np.abs(D_ref).max())
