@@ -206,8 +206,9 @@ __device__ __forceinline__ void store_cluster(ClusterDatum* base, int i, const d
 {
     ClusterDatum d;
     d.c[0] = mom[1]; d.c[1] = mom[2]; d.c[2] = mom[3];
-    for (int k = 0; k < 6; ++k) d.P[k] = mom[4 + k];
+    for (int k = 0; k < 6; ++k) d.P[k] = static_cast<float>(mom[4 + k]);
     d.a = mom[0];
+    d.pad[0] = d.pad[1] = 0.0f;
     store_datum(base, i, d);
 }
 

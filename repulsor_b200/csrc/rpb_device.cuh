@@ -22,14 +22,16 @@ struct __align__(16) PrimDatum {
 };
 static_assert(sizeof(PrimDatum) == 64, "PrimDatum must be 64 bytes");
 
-// Pair data of a cluster: centre of mass, averaged projector (packed upper
-// triangle (0,0),(0,1),(0,2),(1,1),(1,2),(2,2)) in FP64, and the weight. 80 bytes.
+// Pair data of a cluster: centre of mass (FP64), averaged projector (packed upper
+// triangle (0,0),(0,1),(0,2),(1,1),(1,2),(2,2)) in FP32 — far pairs project in FP32 —,
+// and the weight. 64 bytes: four 16-byte loads per gather.
 struct __align__(16) ClusterDatum {
     double c[3];
-    double P[6];
+    float P[6];
     double a;
+    float pad[2];
 };
-static_assert(sizeof(ClusterDatum) == 80, "ClusterDatum must be 80 bytes");
+static_assert(sizeof(ClusterDatum) == 64, "ClusterDatum must be 64 bytes");
 
 // Tangent-point exponents of one evaluation. q = numerator, p = denominator.
 struct TPExp {
