@@ -215,7 +215,8 @@ __global__ void __launch_bounds__(SN_BLOCK) k_sn_dense(SnSplitArgs A)
 // CG vector kernels (FP64). Scalars live on the device; per column c:
 //   S_RZ rz, S_RZOLD previous rz, S_PAP (p,Ap), S_RR (r,r), S_ZR_OLD (z, r_old)
 // ------------------------------------------------------------------------------------------
-enum { S_RZ = 0, S_RZOLD = 3, S_PAP = 6, S_RR = 9, S_ZROLD = 12, S_ACTIVE = 15, S_COUNT = 18 };
+enum { S_RZ = 0, S_RZOLD = 3, S_PAP = 6, S_RR = 9, S_ZROLD = 12, S_ACTIVE = 15, S_BB = 18, S_CONV_IT = 21, S_IT = 24,
+       S_COUNT = 25 };
 
 struct DotArgs {
     int n;                    // rows (n x 3)
@@ -299,6 +300,18 @@ __global__ void k_cg_direction(int n, const double* S, bool flexible, const doub
         const int64_t k = 3 * static_cast<int64_t>(i) + c;
         p[k] = z[k] + beta * p[k];
     }
+}
+
+// After an iteration: count it, and freeze the columns whose recurrence residual met the
+// tolerance (||r_c||^2 <= tol^2 ||b_c||^2), recording the iteration at which they did.
+__global__ void k_cg_check(double* S, double tol2)
+{
+    S[S_IT] += 1.0;
+    for (int c = 0; c < 3; ++c)
+        if (S[S_ACTIVE + c] != 0.0 && S[S_RR + c] <= tol2 * S[S_BB + c]) {
+            S[S_ACTIVE + c] = 0.0;
+            S[S_CONV_IT + c] = S[S_IT];
+        }
 }
 
 __global__ void k_axpby3(int n, double alpha, const double* x, double beta, double* y, int ldy)
@@ -523,14 +536,20 @@ static rpb_status cg_solve(rpb_mesh* m, double q, double p, const double* B, int
     const bool flexible = (precond == RPB_PRECOND_LEARNED);
     // iterations without a 10% drop of the best residual that count as a stall
     constexpr int kStallWindow = 500;
+    // iterations per captured graph between host checks of the residuals
+    constexpr int kGraphIters = 8;
     int kind = precond;
 
     // ||B|| per column
     RPB_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * n3, stream));
     if ((st = dot3(m, B, B, nullptr, S + S_RR, nullptr)) != RPB_OK) return st;
     if ((st = read_scalars(m)) != RPB_OK) return st;
-    double bnorm[3];
-    for (int c = 0; c < 3; ++c) bnorm[c] = std::sqrt(s.host_scal[S_RR + c]);
+    double bnorm[3], bb[3];
+    for (int c = 0; c < 3; ++c) {
+        bb[c] = s.host_scal[S_RR + c];
+        bnorm[c] = std::sqrt(bb[c]);
+    }
+    RPB_CUDA(cudaMemcpyAsync(S + S_BB, bb, sizeof(bb), cudaMemcpyHostToDevice, stream));
     double active[3];
     for (int c = 0; c < 3; ++c) active[c] = bnorm[c] > 0 ? 1.0 : 0.0;
     int it = 0;
@@ -540,13 +559,38 @@ static rpb_status cg_solve(rpb_mesh* m, double q, double p, const double* B, int
     double best[3] = {1e300, 1e300, 1e300};
     int since_best = 0;
     bool stalled_flag = false;
+    const double tol2 = tol * tol;
+    // One CG iteration from a search direction p: A p, step, residual, convergence flags,
+    // then the next preconditioned direction. Only launches and device-to-device copies,
+    // so K of them are captured into one CUDA graph and replayed between host checks.
+    auto iteration = [&](int k) -> rpb_status {
+        rpb_status e;
+        if ((e = metric_multiply_dev(m, q, p, 1.0, pv, 3, 0.0, Ap, 3, 7)) != RPB_OK) return e;
+        if ((e = dot3(m, pv, Ap, nullptr, S + S_PAP, nullptr)) != RPB_OK) return e;
+        if (flexible) RPB_CUDA(cudaMemcpyAsync(rold, r, sizeof(double) * n3, cudaMemcpyDeviceToDevice, stream));
+        k_cg_update<<<eb, 256, 0, stream>>>(n, S, x, r, pv, Ap);
+        if ((e = dot3(m, r, r, nullptr, S + S_RR, nullptr)) != RPB_OK) return e;
+        k_cg_check<<<1, 1, 0, stream>>>(S, tol2);
+        RPB_CUDA(cudaMemcpyAsync(S + S_RZOLD, S + S_RZ, 3 * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+        if ((e = apply_preconditioner(m, k, q, p, r, z)) != RPB_OK) return e;
+        if ((e = dot3(m, z, r, flexible ? rold : nullptr, S + S_RZ, S + S_ZROLD)) != RPB_OK) return e;
+        k_cg_direction<<<eb, 256, 0, stream>>>(n, S, flexible, z, pv);
+        RPB_CUDA(cudaGetLastError());
+        return RPB_OK;
+    };
+    cudaGraphExec_t graph = nullptr;
+    int graph_kind = -1;
+    auto drop_graph = [&]() {
+        if (graph) cudaGraphExecDestroy(graph);
+        graph = nullptr;
+    };
     while (true) {
         // r = B - A x (true residual), z = M r, p = z
-        if ((st = metric_multiply_dev(m, q, p, -1.0, x, 3, 0.0, r, 3, 7)) != RPB_OK) return st;
+        if ((st = metric_multiply_dev(m, q, p, -1.0, x, 3, 0.0, r, 3, 7)) != RPB_OK) { drop_graph(); return st; }
         k_axpby3<<<eb, 256, 0, stream>>>(n, 1.0, B, 1.0, r, 3);
         RPB_CUDA(cudaGetLastError());
-        if ((st = dot3(m, r, r, nullptr, S + S_RR, nullptr)) != RPB_OK) return st;
-        if ((st = read_scalars(m)) != RPB_OK) return st;
+        if ((st = dot3(m, r, r, nullptr, S + S_RR, nullptr)) != RPB_OK) { drop_graph(); return st; }
+        if ((st = read_scalars(m)) != RPB_OK) { drop_graph(); return st; }
         bool done = true;
         for (int c = 0; c < 3; ++c) {
             rel[c] = bnorm[c] > 0 ? std::sqrt(s.host_scal[S_RR + c]) / bnorm[c] : 0.0;
@@ -560,43 +604,64 @@ static rpb_status cg_solve(rpb_mesh* m, double q, double p, const double* B, int
         }
         stalled_flag = false;
         ++restarts;
+        double it_conv[4] = {-1.0, -1.0, -1.0, static_cast<double>(it)};
         RPB_CUDA(cudaMemcpyAsync(S + S_ACTIVE, active, sizeof(active), cudaMemcpyHostToDevice, stream));
-        if ((st = apply_preconditioner(m, kind, q, p, r, z)) != RPB_OK) return st;
+        RPB_CUDA(cudaMemcpyAsync(S + S_CONV_IT, it_conv, sizeof(it_conv), cudaMemcpyHostToDevice, stream));
+        if ((st = apply_preconditioner(m, kind, q, p, r, z)) != RPB_OK) { drop_graph(); return st; }
         RPB_CUDA(cudaMemcpyAsync(pv, z, sizeof(double) * n3, cudaMemcpyDeviceToDevice, stream));
-        if ((st = dot3(m, r, z, nullptr, S + S_RZ, nullptr)) != RPB_OK) return st;
-        // inner CG iterations on the recurrence
+        if ((st = dot3(m, r, z, nullptr, S + S_RZ, nullptr)) != RPB_OK) { drop_graph(); return st; }
+        // batches of kGraphIters iterations as one graph; the remainder launched directly
+        // (and everything when the mesh works on the legacy default stream, which cannot
+        // be captured)
+        const bool use_graph = stream != nullptr;
+        if (use_graph && graph_kind != kind) {
+            drop_graph();
+            cudaGraph_t g = nullptr;
+            RPB_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+            rpb_status cst = RPB_OK;
+            for (int k = 0; k < kGraphIters && cst == RPB_OK; ++k) cst = iteration(kind);
+            const cudaError_t ce = cudaStreamEndCapture(stream, &g);
+            if (cst != RPB_OK) { if (g) cudaGraphDestroy(g); return cst; }
+            RPB_CUDA(ce);
+            const cudaError_t ie = cudaGraphInstantiate(&graph, g, 0);
+            cudaGraphDestroy(g);
+            RPB_CUDA(ie);
+            graph_kind = kind;
+        }
         while (it < max_iter) {
-            if ((st = metric_multiply_dev(m, q, p, 1.0, pv, 3, 0.0, Ap, 3, 7)) != RPB_OK) return st;
-            if ((st = dot3(m, pv, Ap, nullptr, S + S_PAP, nullptr)) != RPB_OK) return st;
-            if (flexible) RPB_CUDA(cudaMemcpyAsync(rold, r, sizeof(double) * n3, cudaMemcpyDeviceToDevice, stream));
-            k_cg_update<<<eb, 256, 0, stream>>>(n, S, x, r, pv, Ap);
-            RPB_CUDA(cudaGetLastError());
-            ++it;
-            if ((st = dot3(m, r, r, nullptr, S + S_RR, nullptr)) != RPB_OK) return st;
-            if ((st = read_scalars(m)) != RPB_OK) return st;
+            int batch = std::min(kGraphIters, max_iter - it);
+            if (use_graph && batch == kGraphIters) {
+                RPB_CUDA(cudaGraphLaunch(graph, stream));
+            } else {
+                for (int k = 0; k < batch; ++k)
+                    if ((st = iteration(kind)) != RPB_OK) { drop_graph(); return st; }
+            }
+            if ((st = read_scalars(m)) != RPB_OK) { drop_graph(); return st; }
+            const int done_it = static_cast<int>(s.host_scal[S_IT]);
             bool conv = true, stalled = false;
+            int last_conv = 0;
             for (int c = 0; c < 3; ++c) {
                 if (active[c] == 0.0) continue;
+                const double ci = s.host_scal[S_CONV_IT + c];
+                if (ci < 0.0) conv = false;
+                else last_conv = std::max(last_conv, static_cast<int>(ci));
                 const double rc = bnorm[c] > 0 ? std::sqrt(s.host_scal[S_RR + c]) / bnorm[c] : 0.0;
-                if (rc > tol) conv = false;
-                if (rc < 0.9 * best[c]) { best[c] = rc; since_best = 0; }
+                if (ci < 0.0 && rc < 0.9 * best[c]) { best[c] = rc; since_best = 0; }
             }
+            it = conv ? last_conv : done_it;
             // stall detection only guards the flexible (learned) iteration, which then falls
             // back to the reference preconditioner; fixed-preconditioner CG is never restarted
-            if (flexible && kind == RPB_PRECOND_LEARNED && !conv && ++since_best > kStallWindow) stalled = true;
+            since_best += batch;
+            if (flexible && kind == RPB_PRECOND_LEARNED && !conv && since_best > kStallWindow) stalled = true;
             if (conv || stalled) {
                 stalled_flag = stalled;
                 since_best = 0;
                 break;
             }
-            RPB_CUDA(cudaMemcpyAsync(S + S_RZOLD, S + S_RZ, 3 * sizeof(double), cudaMemcpyDeviceToDevice, stream));
-            if ((st = apply_preconditioner(m, kind, q, p, r, z)) != RPB_OK) return st;
-            if ((st = dot3(m, z, r, flexible ? rold : nullptr, S + S_RZ, S + S_ZROLD)) != RPB_OK) return st;
-            k_cg_direction<<<eb, 256, 0, stream>>>(n, S, flexible, z, pv);
-            RPB_CUDA(cudaGetLastError());
         }
         if (restarts > 20) break;
     }
+    drop_graph();
     s.last_iterations = it;
     s.last_restarts = restarts;
     if (iters_out) *iters_out = it;
