@@ -680,4 +680,70 @@ std::string build_cross_lists(const HostTree& S, const double* VS, const int* SS
     return std::string();
 }
 
+void build_row_tiles(const int64_t* rp, const int* ci, int rows, int ncols, int max_rows, int max_union, int threads,
+                     RowTiles& out)
+{
+    out = RowTiles();
+    max_union = std::min(max_union, 65535);
+    for (int i = 0; i < rows; ++i)
+        if (rp[i + 1] - rp[i] > max_union) return;
+    // chunks of rows (a whole number of full tiles) are tiled independently
+    max_rows = std::max(1, max_rows);
+    const int chunk = max_rows * ((4096 + max_rows - 1) / max_rows);
+    const int nchunks = (rows + chunk - 1) / chunk;
+    struct Part {
+        std::vector<int> row0, cols_rp, cols, order;
+        int max_union = 0;
+    };
+    std::vector<Part> parts(nchunks);
+    out.slot.assign(static_cast<size_t>(rows > 0 ? rp[rows] : 0), 0);
+    std::atomic<int> ticket{0};
+    run_threads(std::max(1, std::min(threads, nchunks)), [&](int) {
+        std::vector<int> pos(ncols, -1), U;
+        for (;;) {
+            const int c = ticket.fetch_add(1);
+            if (c >= nchunks) break;
+            Part& P = parts[c];
+            const int r_end = std::min(rows, (c + 1) * chunk);
+            int r = c * chunk;
+            while (r < r_end) {
+                const int t0 = r;
+                U.clear();
+                while (r < r_end && r - t0 < max_rows) {
+                    int fresh = 0;
+                    for (int64_t k = rp[r]; k < rp[r + 1]; ++k) fresh += (pos[ci[k]] < 0);
+                    if (r > t0 && static_cast<int>(U.size()) + fresh > max_union) break;
+                    for (int64_t k = rp[r]; k < rp[r + 1]; ++k)
+                        if (pos[ci[k]] < 0) { pos[ci[k]] = 0; U.push_back(ci[k]); }
+                    ++r;
+                }
+                std::sort(U.begin(), U.end());
+                for (size_t u = 0; u < U.size(); ++u) pos[U[u]] = static_cast<int>(u);
+                for (int i = t0; i < r; ++i)
+                    for (int64_t k = rp[i]; k < rp[i + 1]; ++k) out.slot[k] = static_cast<uint16_t>(pos[ci[k]]);
+                P.row0.push_back(t0);
+                P.cols_rp.push_back(static_cast<int>(U.size()));
+                P.cols.insert(P.cols.end(), U.begin(), U.end());
+                P.max_union = std::max(P.max_union, static_cast<int>(U.size()));
+                const size_t o0 = P.order.size();
+                for (int i = t0; i < r; ++i) P.order.push_back(i);
+                std::stable_sort(P.order.begin() + o0, P.order.end(),
+                                 [&](int a, int b) { return (rp[a + 1] - rp[a]) > (rp[b + 1] - rp[b]); });
+                for (int u : U) pos[u] = -1;
+            }
+        }
+    });
+    out.row0.reserve(rows + 1);
+    out.cols_rp.push_back(0);
+    for (const Part& P : parts) {
+        out.row0.insert(out.row0.end(), P.row0.begin(), P.row0.end());
+        for (int n : P.cols_rp) out.cols_rp.push_back(out.cols_rp.back() + n);
+        out.cols.insert(out.cols.end(), P.cols.begin(), P.cols.end());
+        out.order.insert(out.order.end(), P.order.begin(), P.order.end());
+        out.max_union = std::max(out.max_union, P.max_union);
+    }
+    out.row0.push_back(rows);
+    out.valid = true;
+}
+
 }  // namespace rpb

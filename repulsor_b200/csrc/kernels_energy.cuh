@@ -1,13 +1,15 @@
 // Tangent-point energy and differential kernels (B200, sm_100a).
 //
-//   k_geometry_upsweep : SimplicialMesh::SemiStaticUpdate -- simplex data
-//                        (src/SimplexDataKernel.hpp:92-203) in tree order, plus the
-//                        ClusterTree moment upsweep (ComputeClusterData_Thread.hpp:50-129)
-//                        as one bottom-up pass with arrival counters.
-//   k_tp0_pairs        : TP0 near-field and far-field pair kernels
-//                        (TP0_Kernel_NF.hpp:140-338, TP0_Kernel_FF.hpp:130-319) over the
-//                        full symmetric CSR patterns, one warp per row; every row
-//                        accumulates only its own derivative, so no scatter/atomics.
+//   k_geometry_prims,  : SimplicialMesh::SemiStaticUpdate -- simplex data
+//   k_cluster_moments    (src/SimplexDataKernel.hpp:92-203) in tree order, plus the
+//                        ClusterTree moments (ComputeClusterData_Thread.hpp:50-129) as
+//                        prefix-sum range differences.
+//   k_tp0_pairs_tiled  : TP0 near-field and far-field pair kernels
+//   k_tp0_pairs          (TP0_Kernel_NF.hpp:140-338, TP0_Kernel_FF.hpp:130-319) over the
+//                        full symmetric CSR patterns, LANES threads per row; every row
+//                        accumulates only its own derivative, so no scatter/atomics. The
+//                        tiled form stages each row tile's column data in shared memory;
+//                        the gather form reads it through L1/L2.
 //   k_collect_chain    : CollectFar/NearFieldDerivatives (src/ClusterTree.hpp:1115-1208),
 //                        the percolate-down of the far field and DNearFarToHulls
 //                        (SimplicialMeshDetails.hpp:529-733, :1097-1410) per primitive.
@@ -413,9 +415,154 @@ constexpr int FAR_LANES = 2;
 
 constexpr int pair_blocks(int rows, int lanes) { return (rows * lanes + PAIR_BLOCK - 1) / PAIR_BLOCK; }
 
-// LANES threads per row. FAR: rows are clusters of the Far() pattern; otherwise rows are
-// primitives of the Near() pattern. A row accumulates only its own derivative; each
-// unordered pair contributes its energy once (from the row with the smaller index).
+// Row tiles of the shared-memory kernels: threads per block (PAIR_TILE_THREADS / LANES rows
+// at most per tile, two blocks per SM) and the largest column union a tile may stage
+// (64-byte data + a 4-byte id per column). The host sizes the tiles so that their count
+// is a whole number of waves of resident blocks.
+constexpr int PAIR_TILE_THREADS = 288;
+constexpr int NEAR_TILE_UNION = 1024;
+constexpr int FAR_TILE_UNION = 1536;
+
+// One lane's share of a row: the row's entries k = k0 + sub, k0 + sub + LANES, ... with the
+// column handle u = index(k) and the column datum from datum(u, j, Y) (j: the column's
+// tree position). The next entry's handle (PREFETCH: and its datum) is requested before
+// the current pair is evaluated. A row accumulates only its own derivative; each
+// unordered pair contributes its energy once (from the row with the smaller index),
+// CROSS pairs always.
+template <bool FAR, int QH, int PH, bool DIFF, int LANES, bool CROSS, bool PREFETCH, typename Datum, typename Index,
+          typename Fetch>
+__device__ __forceinline__ void pair_row(const PairArgs& A, const Datum& X, int i, int sub, Index index, Fetch datum,
+                                         double& e_row, double (&D64)[10])
+{
+    const float ax = static_cast<float>(X.a);
+    PairAcc<float> acc = {};
+    float e32 = 0.0f;
+    int since_flush = 0;
+    const int64_t k0 = A.rp[i], k1 = A.rp[i + 1];
+    int64_t k = k0 + sub;
+    int un = (k < k1) ? index(k) : 0;
+    int jn = 0;
+    Datum Yn;
+    if (PREFETCH && k < k1) datum(un, jn, Yn);
+    for (; k < k1; k += LANES) {
+        int j;
+        Datum Y;
+        if constexpr (PREFETCH) {
+            j = jn;
+            Y = Yn;
+            if (k + LANES < k1) datum(index(k + LANES), jn, Yn);
+        } else {
+            datum(un, j, Y);
+            if (k + LANES < k1) un = index(k + LANES);
+        }
+        Proj<float> g;
+        if constexpr (FAR) project_clusters(X, Y, g);
+        else project_prims(A.dom, X, Y, g);
+        bool close = false;
+        if constexpr (!FAR) {
+            const float dd = A.close_factor * (X.diam + Y.diam);
+            close = g.r2 < dd * dd;
+        }
+        if (close) {
+            // close near-field pair: the same kernel in FP64, added straight into FP64
+            Proj<double> gd;
+            if constexpr (!FAR) project_prims(A.dom, X, Y, gd);
+            PairAcc<double> a64 = {};
+            const double e = tp0_core<double, QH, PH, DIFF>(A.ex, gd, X.a, Y.a, a64);
+            if (CROSS || j > i) e_row += e;
+            if (DIFF) {
+                D64[0] += a64.d0;
+                for (int m = 0; m < 3; ++m) D64[1 + m] += a64.dx[m];
+                for (int m = 0; m < 6; ++m) D64[4 + m] += a64.dP[m];
+            }
+        } else {
+            const float e = tp0_core<float, QH, PH, DIFF>(A.ex, g, ax, static_cast<float>(Y.a), acc);
+            if (CROSS || j > i) e32 += e;
+            if (++since_flush == PAIR_FLUSH) {
+                since_flush = 0;
+                e_row += e32;
+                e32 = 0.0f;
+                if (DIFF) {
+                    D64[0] += acc.d0;
+#pragma unroll
+                    for (int m = 0; m < 3; ++m) D64[1 + m] += acc.dx[m];
+#pragma unroll
+                    for (int m = 0; m < 6; ++m) D64[4 + m] += acc.dP[m];
+                    acc = PairAcc<float>{};
+                }
+            }
+        }
+    }
+    e_row += e32;
+    if (DIFF) {
+        D64[0] += acc.d0;
+#pragma unroll
+        for (int m = 0; m < 3; ++m) D64[1 + m] += acc.dx[m];
+#pragma unroll
+        for (int m = 0; m < 6; ++m) D64[4 + m] += acc.dP[m];
+    }
+}
+
+// Combines the LANES partial sums of a row (xor butterfly, every lane of the warp takes
+// part), writes the row's derivative, and reduces the energy deterministically: one
+// partial per block, the last block to finish sums the partials in block order.
+template <bool DIFF, int LANES, bool CROSS>
+__device__ __forceinline__ void pair_epilogue(const PairArgs& A, bool active, int i, int sub, double e_row,
+                                              double (&D64)[10])
+{
+    if constexpr (CROSS) {
+        e_row *= 0.5;
+#pragma unroll
+        for (int m = 0; m < 10; ++m) D64[m] *= 0.5;
+    }
+#pragma unroll
+    for (int off = 1; off < LANES; off <<= 1) {
+        e_row += __shfl_xor_sync(0xffffffffu, e_row, off);
+        if (DIFF) {
+#pragma unroll
+            for (int m = 0; m < 10; ++m) D64[m] += __shfl_xor_sync(0xffffffffu, D64[m], off);
+        }
+    }
+    if (DIFF && active && sub == 0) {
+        double* dst = A.D + 10 * static_cast<int64_t>(i);
+#pragma unroll
+        for (int m = 0; m < 10; ++m) dst[m] = D64[m];
+    }
+    if (sub != 0) e_row = 0.0;
+    __shared__ double sh[32];
+    __shared__ bool last;
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int nw = blockDim.x >> 5;
+    e_row = warp_sum_f64(e_row);
+    if (lane == 0) sh[wib] = e_row;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int w = 0; w < nw; ++w) s += sh[w];
+        A.block_energy[blockIdx.x] = s;
+        __threadfence();
+        last = (atomicAdd(A.done, 1u) == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (last) {
+        __threadfence();
+        double s = 0.0;
+        for (int b = threadIdx.x; b < gridDim.x; b += blockDim.x) s += __ldcg(A.block_energy + b);
+        s = warp_sum_f64(s);
+        __syncthreads();
+        if (lane == 0) sh[wib] = s;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double t2 = 0.0;
+            for (int w = 0; w < nw; ++w) t2 += sh[w];
+            *A.energy_out = t2;
+            *A.done = 0u;
+        }
+    }
+}
+
+// LANES threads per row, column data gathered from global memory (L1/L2). FAR: rows are
+// clusters of the Far() pattern; otherwise rows are primitives of the Near() pattern.
 // CROSS: rows are the mesh's, columns the obstacle's (a non-symmetric block cluster tree):
 // every pair counts, energy and derivatives carry the symmetry factor 1/2
 // (src/FMM/FMM_Kernel.hpp:43) and the obstacle's derivatives are not formed.
@@ -435,111 +582,90 @@ __global__ void __launch_bounds__(PAIR_BLOCK) k_tp0_pairs(PairArgs A)
     if (active) {
         i = A.order ? A.order[slot] : slot;
         const Datum X = load_datum(base, i);
-        const float ax = static_cast<float>(X.a);
-        PairAcc<float> acc = {};
-        float e32 = 0.0f;
-        int since_flush = 0;
-        const int64_t k0 = A.rp[i], k1 = A.rp[i + 1];
-        for (int64_t k = k0 + sub; k < k1; k += LANES) {
-            const int j = __ldg(A.ci + k);
-            const Datum Y = load_datum(cols, j);
-            Proj<float> g;
-            if constexpr (FAR) project_clusters(X, Y, g);
-            else project_prims(A.dom, X, Y, g);
-            bool close = false;
-            if constexpr (!FAR) {
-                const float dd = A.close_factor * (X.diam + Y.diam);
-                close = g.r2 < dd * dd;
-            }
-            if (close) {
-                // close near-field pair: the same kernel in FP64, added straight into FP64
-                Proj<double> gd;
-                if constexpr (!FAR) project_prims(A.dom, X, Y, gd);
-                PairAcc<double> a64 = {};
-                const double e = tp0_core<double, QH, PH, DIFF>(A.ex, gd, X.a, Y.a, a64);
-                if (CROSS || j > i) e_row += e;
-                if (DIFF) {
-                    D64[0] += a64.d0;
-                    for (int m = 0; m < 3; ++m) D64[1 + m] += a64.dx[m];
-                    for (int m = 0; m < 6; ++m) D64[4 + m] += a64.dP[m];
-                }
-            } else {
-                const float e = tp0_core<float, QH, PH, DIFF>(A.ex, g, ax, static_cast<float>(Y.a), acc);
-                if (CROSS || j > i) e32 += e;
-                if (++since_flush == PAIR_FLUSH) {
-                    since_flush = 0;
-                    e_row += e32;
-                    e32 = 0.0f;
-                    if (DIFF) {
-                        D64[0] += acc.d0;
-#pragma unroll
-                        for (int m = 0; m < 3; ++m) D64[1 + m] += acc.dx[m];
-#pragma unroll
-                        for (int m = 0; m < 6; ++m) D64[4 + m] += acc.dP[m];
-                        acc = PairAcc<float>{};
-                    }
-                }
-            }
-        }
-        e_row += e32;
-        if (DIFF) {
-            D64[0] += acc.d0;
-#pragma unroll
-            for (int m = 0; m < 3; ++m) D64[1 + m] += acc.dx[m];
-#pragma unroll
-            for (int m = 0; m < 6; ++m) D64[4 + m] += acc.dP[m];
-        }
+        auto index = [&](int64_t k) { return __ldg(A.ci + k); };
+        auto datum = [&](int u, int& j, Datum& Y) {
+            j = u;
+            Y = load_datum(cols, u);
+        };
+        pair_row<FAR, QH, PH, DIFF, LANES, CROSS, true>(A, X, i, sub, index, datum, e_row, D64);
     }
-    if constexpr (CROSS) {
-        e_row *= 0.5;
+    pair_epilogue<DIFF, LANES, CROSS>(A, active, i, sub, e_row, D64);
+}
+
+// Row tiles (build_row_tiles): block b owns the rows order[row0[b] .. row0[b+1]) and
+// stages the data of the union of their columns, cols[cols_rp[b] .. cols_rp[b+1]), in
+// shared memory with asynchronous 16-byte copies; entry k then reads its column datum
+// from shared-memory slot slot[k]. The 16-byte pieces of a datum are rotated by the slot
+// index, so that the lanes of a warp spread their shared-memory reads over all banks.
+struct PairTiles {
+    const int* row0;
+    const int* cols_rp;
+    const int* cols;
+    const uint16_t* slot;
+    const int* order;
+};
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem)
+{
+    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+template <typename Datum>
+__device__ __forceinline__ Datum load_datum_rot(const float4* sdat, int u)
+{
+    Datum d;
+    float4* o = reinterpret_cast<float4*>(&d);
 #pragma unroll
-        for (int m = 0; m < 10; ++m) D64[m] *= 0.5;
+    for (int q = 0; q < 4; ++q) o[q] = sdat[4 * u + ((q + u) & 3)];
+    return d;
+}
+
+// dynamic shared memory per tile of union size n: the data, then the column ids
+__host__ __device__ constexpr size_t pair_tile_smem(int n) { return static_cast<size_t>(n) * (64 + 4); }
+
+template <bool FAR, int QH, int PH, bool DIFF, int LANES>
+__global__ void __launch_bounds__(PAIR_TILE_THREADS, 2) k_tp0_pairs_tiled(PairArgs A, PairTiles T)
+{
+    static_assert(LANES == 1 || LANES == 2 || LANES == 4 || LANES == 8, "LANES must divide a warp");
+    using Datum = typename std::conditional<FAR, ClusterDatum, PrimDatum>::type;
+    static_assert(sizeof(Datum) == 64, "64-byte data");
+    extern __shared__ float4 tile_smem[];
+    const Datum* base = static_cast<const Datum*>(A.data);
+    const int b = blockIdx.x;
+    const int u0 = T.cols_rp[b], un = T.cols_rp[b + 1] - u0;
+    float4* sdat = tile_smem;
+    int* sid = reinterpret_cast<int*>(tile_smem + 4 * static_cast<size_t>(un));
+    for (int idx = threadIdx.x; idx < 4 * un; idx += blockDim.x) {
+        const int u = idx >> 2, q = idx & 3;
+        const float4* src = reinterpret_cast<const float4*>(base + __ldg(T.cols + u0 + u)) + q;
+        cp_async16(sdat + 4 * u + ((q + u) & 3), src);
     }
-    // combine the LANES partial sums of a row (every lane of the warp takes part)
-#pragma unroll
-    for (int off = 1; off < LANES; off <<= 1) {
-        e_row += __shfl_xor_sync(0xffffffffu, e_row, off);
-        if (DIFF) {
-#pragma unroll
-            for (int m = 0; m < 10; ++m) D64[m] += __shfl_xor_sync(0xffffffffu, D64[m], off);
-        }
+    for (int u = threadIdx.x; u < un; u += blockDim.x) sid[u] = __ldg(T.cols + u0 + u);
+    const int r0 = T.row0[b], nrows = T.row0[b + 1] - r0;
+    const int slot = threadIdx.x / LANES, sub = threadIdx.x & (LANES - 1);
+    const bool active = slot < nrows;
+    int i = 0;
+    Datum X;
+    if (active) {
+        i = T.order[r0 + slot];
+        X = load_datum(base, i);
     }
-    if (DIFF && active && sub == 0) {
-        double* dst = A.D + 10 * static_cast<int64_t>(i);
-#pragma unroll
-        for (int m = 0; m < 10; ++m) dst[m] = D64[m];
-    }
-    if (sub != 0) e_row = 0.0;
-    // deterministic energy reduction: per-block partial, last block sums all partials
-    __shared__ double sh[PAIR_BLOCK / 32];
-    __shared__ bool last;
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    e_row = warp_sum_f64(e_row);
-    if (lane == 0) sh[wib] = e_row;
+    cp_async_wait_all();
     __syncthreads();
-    if (threadIdx.x == 0) {
-        double s = 0.0;
-        for (int w = 0; w < (blockDim.x >> 5); ++w) s += sh[w];
-        A.block_energy[blockIdx.x] = s;
-        __threadfence();
-        last = (atomicAdd(A.done, 1u) == gridDim.x - 1);
+    double e_row = 0.0;
+    double D64[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    if (active) {
+        auto index = [&](int64_t k) { return static_cast<int>(__ldg(T.slot + k)); };
+        auto datum = [&](int u, int& j, Datum& Y) {
+            Y = load_datum_rot<Datum>(sdat, u);
+            j = sid[u];
+        };
+        pair_row<FAR, QH, PH, DIFF, LANES, false, false>(A, X, i, sub, index, datum, e_row, D64);
     }
-    __syncthreads();
-    if (last) {
-        __threadfence();
-        double s = 0.0;
-        for (int b = threadIdx.x; b < gridDim.x; b += blockDim.x) s += __ldcg(A.block_energy + b);
-        s = warp_sum_f64(s);
-        __syncthreads();
-        if (lane == 0) sh[wib] = s;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            double t2 = 0.0;
-            for (int w = 0; w < (blockDim.x >> 5); ++w) t2 += sh[w];
-            *A.energy_out = t2;
-            *A.done = 0u;
-        }
-    }
+    pair_epilogue<DIFF, LANES, false>(A, active, i, sub, e_row, D64);
 }
 
 // energy = near-field part + far-field part (the order evaluate() uses on the host)

@@ -4,6 +4,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <thread>
 
@@ -39,6 +40,8 @@ int64_t rpb_mesh::device_bytes() const
          C_left.bytes() + C_right.bytes();
     b += near.rp.bytes() + near.ci.bytes() + far.rp.bytes() + far.ci.bytes() + verynear.rp.bytes() +
          verynear.ci.bytes() + near_order.bytes() + far_order.bytes();
+    for (const rpb::TileBufs* t : {&near_tiles, &far_tiles})
+        b += t->row0.bytes() + t->cols_rp.bytes() + t->cols.bytes() + t->order.bytes() + t->slot.bytes();
     b += P_pair.bytes() + C_pair.bytes() + C_mom.bytes() + counter.bytes() + P_near.bytes() + scan_local.bytes() +
          scan_blocks.bytes() + C_begin.bytes() + C_end.bytes();
     b += D_near.bytes() + D_far.bytes() + D_vf.bytes() + B.bytes() + v_rp.bytes() + v_slot.bytes() + Y.bytes();
@@ -140,16 +143,65 @@ rpb_status launch_geometry(rpb_mesh* m)
     return RPB_OK;
 }
 
+// Largest dynamic shared memory a tiled pair kernel may ask for, set once per device for
+// every instantiation (the attribute only permits; each launch asks for its tiles' need).
+template <int QH, int PH>
+static cudaError_t allow_tile_smem_t()
+{
+    const int nb = static_cast<int>(pair_tile_smem(NEAR_TILE_UNION)), fb = static_cast<int>(pair_tile_smem(FAR_TILE_UNION));
+    cudaError_t e = cudaSuccess;
+    auto set = [&](const void* f, int bytes) {
+        const cudaError_t r = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        if (e == cudaSuccess) e = r;
+    };
+    set(reinterpret_cast<const void*>(k_tp0_pairs_tiled<false, QH, PH, true, NEAR_LANES>), nb);
+    set(reinterpret_cast<const void*>(k_tp0_pairs_tiled<false, QH, PH, false, NEAR_LANES>), nb);
+    set(reinterpret_cast<const void*>(k_tp0_pairs_tiled<true, QH, PH, true, FAR_LANES>), fb);
+    set(reinterpret_cast<const void*>(k_tp0_pairs_tiled<true, QH, PH, false, FAR_LANES>), fb);
+    return e;
+}
+
+static rpb_status allow_tile_smem(int device)
+{
+    static std::mutex mu;
+    static std::vector<int> done;
+    std::lock_guard<std::mutex> lock(mu);
+    if (std::find(done.begin(), done.end(), device) != done.end()) return RPB_OK;
+    RPB_CUDA((allow_tile_smem_t<3, 6>()));
+    RPB_CUDA((allow_tile_smem_t<2, 4>()));
+    RPB_CUDA((allow_tile_smem_t<1, 2>()));
+    RPB_CUDA((allow_tile_smem_t<-1, -1>()));
+    done.push_back(device);
+    return RPB_OK;
+}
+
+static PairTiles tiles_view(const TileBufs& t)
+{
+    return PairTiles{t.row0.ptr, t.cols_rp.ptr, t.cols.ptr, t.slot.ptr, t.order.ptr};
+}
+
 template <int QH, int PH>
 static void launch_pairs_t(rpb_mesh* m, const PairArgs& An, const PairArgs& Af, bool diff, cudaEvent_t between)
 {
     if (An.rows > 0) {
-        if (diff) k_tp0_pairs<false, QH, PH, true, NEAR_LANES><<<m->near_blocks, PAIR_BLOCK, 0, m->stream>>>(An);
+        const TileBufs& t = m->near_tiles;
+        if (t.valid) {
+            const size_t smem = pair_tile_smem(t.max_union);
+            const int threads = PAIR_TILE_THREADS;
+            if (diff) k_tp0_pairs_tiled<false, QH, PH, true, NEAR_LANES><<<t.tiles, threads, smem, m->stream>>>(An, tiles_view(t));
+            else k_tp0_pairs_tiled<false, QH, PH, false, NEAR_LANES><<<t.tiles, threads, smem, m->stream>>>(An, tiles_view(t));
+        } else if (diff) k_tp0_pairs<false, QH, PH, true, NEAR_LANES><<<m->near_blocks, PAIR_BLOCK, 0, m->stream>>>(An);
         else k_tp0_pairs<false, QH, PH, false, NEAR_LANES><<<m->near_blocks, PAIR_BLOCK, 0, m->stream>>>(An);
     }
     if (between) cudaEventRecord(between, m->stream);
     if (Af.rows > 0) {
-        if (diff) k_tp0_pairs<true, QH, PH, true, FAR_LANES><<<m->far_blocks, PAIR_BLOCK, 0, m->stream>>>(Af);
+        const TileBufs& t = m->far_tiles;
+        if (t.valid) {
+            const size_t smem = pair_tile_smem(t.max_union);
+            const int threads = PAIR_TILE_THREADS;
+            if (diff) k_tp0_pairs_tiled<true, QH, PH, true, FAR_LANES><<<t.tiles, threads, smem, m->stream>>>(Af, tiles_view(t));
+            else k_tp0_pairs_tiled<true, QH, PH, false, FAR_LANES><<<t.tiles, threads, smem, m->stream>>>(Af, tiles_view(t));
+        } else if (diff) k_tp0_pairs<true, QH, PH, true, FAR_LANES><<<m->far_blocks, PAIR_BLOCK, 0, m->stream>>>(Af);
         else k_tp0_pairs<true, QH, PH, false, FAR_LANES><<<m->far_blocks, PAIR_BLOCK, 0, m->stream>>>(Af);
     }
 }
@@ -379,6 +431,44 @@ rpb_status rpb_mesh_create(int dom_dim, int amb_dim, const double* Vh, int64_t n
         if ((st = upload(m->far_order, fo.data(), fo.size(), s)) != RPB_OK) return fail(st);
         m->near_blocks = pair_blocks(m->N, NEAR_LANES);
         m->far_blocks = pair_blocks(m->NC, FAR_LANES);
+        // shared-memory row tiles; the kernels' grids are then one block per tile
+        // Tiles hold at most PAIR_TILE_THREADS / LANES rows; their row count is chosen so
+        // that the tiles fill a whole number of waves of resident blocks (no partial last
+        // wave, whose few blocks would run while the other SMs idle).
+        int sms = 0;
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, m->device) != cudaSuccess) sms = 0;
+        auto tile = [&](const SymPattern& P, int ncols, int lanes, const void* kernel, int cap, TileBufs& d,
+                        int& blocks) {
+            d.valid = false;
+            int per_sm = 0;
+            if (sms <= 0 || P.nnz() == 0 ||
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, PAIR_TILE_THREADS, pair_tile_smem(cap)) !=
+                    cudaSuccess || per_sm <= 0)
+                return RPB_OK;
+            const int64_t slots = static_cast<int64_t>(per_sm) * sms, groups = PAIR_TILE_THREADS / lanes;
+            const int64_t waves = std::max<int64_t>(1, (P.rows + slots * groups - 1) / (slots * groups));
+            const int rows_per_tile = static_cast<int>((P.rows + waves * slots - 1) / (waves * slots));
+            RowTiles R;
+            build_row_tiles(P.rp.data(), P.ci.data(), P.rows, ncols, rows_per_tile, cap,
+                            std::max(1, m->settings.threads), R);
+            if (!R.valid || R.tiles() == 0) return RPB_OK;
+            rpb_status e;
+            if ((e = upload(d.row0, R.row0.data(), R.row0.size(), s)) != RPB_OK) return e;
+            if ((e = upload(d.cols_rp, R.cols_rp.data(), R.cols_rp.size(), s)) != RPB_OK) return e;
+            if ((e = upload(d.cols, R.cols.data(), R.cols.size(), s)) != RPB_OK) return e;
+            if ((e = upload(d.order, R.order.data(), R.order.size(), s)) != RPB_OK) return e;
+            if ((e = upload(d.slot, R.slot.data(), R.slot.size(), s)) != RPB_OK) return e;
+            d.tiles = R.tiles();
+            d.max_union = R.max_union;
+            d.valid = true;
+            blocks = d.tiles;
+            return RPB_OK;
+        };
+        if ((st = allow_tile_smem(m->device)) != RPB_OK) return fail(st);
+        const void* kn = reinterpret_cast<const void*>(k_tp0_pairs_tiled<false, 3, 6, true, NEAR_LANES>);
+        const void* kf = reinterpret_cast<const void*>(k_tp0_pairs_tiled<true, 3, 6, true, FAR_LANES>);
+        if ((st = tile(T.near, m->N, NEAR_LANES, kn, NEAR_TILE_UNION, m->near_tiles, m->near_blocks)) != RPB_OK) return fail(st);
+        if ((st = tile(T.far, m->NC, FAR_LANES, kf, FAR_TILE_UNION, m->far_tiles, m->far_blocks)) != RPB_OK) return fail(st);
     }
     if (m->block_energy.alloc(m->near_blocks + m->far_blocks)) { set_error("device allocation failed"); return fail(RPB_ENOMEM); }
     if (cudaMemsetAsync(m->counter.ptr, 0, m->counter.bytes(), s) != cudaSuccess ||

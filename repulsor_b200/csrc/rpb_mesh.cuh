@@ -64,6 +64,14 @@ struct PseudoLapCache {
     DevBuf<double> nf_diag, ff_diag, vf_diag;
 };
 
+// Device copy of a pattern's row tiles (RowTiles); valid == false: the gather kernels run.
+struct TileBufs {
+    DevBuf<int> row0, cols_rp, cols, order;
+    DevBuf<uint16_t> slot;
+    int tiles = 0, max_union = 0;
+    bool valid = false;
+};
+
 }  // namespace rpb
 
 struct rpb_mesh {
@@ -82,6 +90,7 @@ struct rpb_mesh {
     rpb::DevBuf<int> perm, leaf_of, C_parent, C_left, C_right, C_begin, C_end;
     rpb::Csr near, far, verynear;
     rpb::DevBuf<int> near_order, far_order;             // pair-kernel row order (length-sorted per chunk)
+    rpb::TileBufs near_tiles, far_tiles;                // shared-memory row tiles of the two patterns
     // geometry state
     rpb::DevBuf<rpb::PrimDatum> P_pair;
     rpb::DevBuf<rpb::ClusterDatum> C_pair;

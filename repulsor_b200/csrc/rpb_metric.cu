@@ -198,6 +198,54 @@ struct SpmmArgs {
 // xor butterfly (BD = 3), in a fixed order.
 constexpr int SPMM_LANES = 4;
 
+// reduce-scatter / butterfly of the SPMM_LANES partial sums of a row, diagonal term, store
+template <int BD>
+__device__ __forceinline__ void spmm_finish(const double (&acc)[BD], int sub, bool active, double2 dg,
+                                            const double* xi, double* y, bool accumulate)
+{
+    if constexpr (BD == 12) {
+        const bool b1 = sub & 2, b0 = sub & 1;
+        double h[6];
+#pragma unroll
+        for (int q = 0; q < 6; ++q) {
+            const double send = b1 ? acc[q] : acc[q + 6];
+            const double keep = b1 ? acc[q + 6] : acc[q];
+            h[q] = keep + __shfl_xor_sync(0xffffffffu, send, 2);
+        }
+        double f[3];
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            const double send = b0 ? h[q] : h[q + 3];
+            const double keep = b0 ? h[q + 3] : h[q];
+            f[q] = keep + __shfl_xor_sync(0xffffffffu, send, 1);
+        }
+        if (active) {
+            const int base = 6 * (b1 ? 1 : 0) + 3 * (b0 ? 1 : 0);
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+                const int c = base + q;
+                const double val = f[q] + (c < 3 ? dg.x : dg.y) * xi[c];
+                y[c] = accumulate ? y[c] + val : val;
+            }
+        }
+    } else {
+        double a[BD];
+#pragma unroll
+        for (int c = 0; c < BD; ++c) a[c] = acc[c];
+#pragma unroll
+        for (int off = 1; off < SPMM_LANES; off <<= 1)
+#pragma unroll
+            for (int c = 0; c < BD; ++c) a[c] += __shfl_xor_sync(0xffffffffu, a[c], off);
+        if (active && sub < BD) {
+            double val = a[0];
+#pragma unroll
+            for (int c = 1; c < BD; ++c) val = (sub == c) ? a[c] : val;
+            val += dg.x * xi[sub];
+            y[sub] = accumulate ? y[sub] + val : val;
+        }
+    }
+}
+
 template <int BD>
 __global__ void __launch_bounds__(256) k_block_spmm(SpmmArgs<BD> A)
 {
@@ -234,46 +282,8 @@ __global__ void __launch_bounds__(256) k_block_spmm(SpmmArgs<BD> A)
         }
     }
     const double2 dg = active ? (first ? A.d0 : A.d1)[i] : make_double2(0.0, 0.0);
-    double* y = active ? (first ? A.y0 : A.y1) + BD * static_cast<int64_t>(i) : nullptr;
-    if constexpr (BD == 12) {
-        // reduce-scatter over the 4 lanes: lane (b1, b0) ends with outputs 6 b1 + 3 b0 .. +2
-        const bool b1 = sub & 2, b0 = sub & 1;
-        double h[6];
-#pragma unroll
-        for (int q = 0; q < 6; ++q) {
-            const double send = b1 ? acc[q] : acc[q + 6];
-            const double keep = b1 ? acc[q + 6] : acc[q];
-            h[q] = keep + __shfl_xor_sync(0xffffffffu, send, 2);
-        }
-        double f[3];
-#pragma unroll
-        for (int q = 0; q < 3; ++q) {
-            const double send = b0 ? h[q] : h[q + 3];
-            const double keep = b0 ? h[q + 3] : h[q];
-            f[q] = keep + __shfl_xor_sync(0xffffffffu, send, 1);
-        }
-        if (active) {
-            const int base = 6 * (b1 ? 1 : 0) + 3 * (b0 ? 1 : 0);
-#pragma unroll
-            for (int q = 0; q < 3; ++q) {
-                const int c = base + q;
-                const double val = f[q] + (c < 3 ? dg.x : dg.y) * x[BD * static_cast<int64_t>(i) + c];
-                y[c] = A.accumulate ? y[c] + val : val;
-            }
-        }
-    } else {
-#pragma unroll
-        for (int off = 1; off < SPMM_LANES; off <<= 1)
-#pragma unroll
-            for (int c = 0; c < BD; ++c) acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], off);
-        if (active && sub < BD) {
-            double val = acc[0];
-#pragma unroll
-            for (int c = 1; c < BD; ++c) val = (sub == c) ? acc[c] : val;
-            val += dg.x * x[BD * static_cast<int64_t>(i) + sub];
-            y[sub] = A.accumulate ? y[sub] + val : val;
-        }
-    }
+    double* y = (first ? A.y0 : A.y1) + BD * static_cast<int64_t>(i);
+    spmm_finish<BD>(acc, sub, active, dg, x + BD * static_cast<int64_t>(i), y, A.accumulate);
 }
 
 // ------------------------------------------------------------------------------------------
