@@ -329,11 +329,38 @@ __device__ __forceinline__ R tp0_core(const TPExp& ex, const Proj<R>& g, R a, R 
     return a * E * b;
 }
 
-// Projection of v = y - x for two primitives. Triangles: P = n n^T, so only n.v is
-// needed (FP64); edges: P v = v - t (t.v) (FP64). Everything downstream of v^T P v is
-// well conditioned and is rounded to R.
+// A primitive's pair data as the tiled near-field kernel keeps it in shared memory: the
+// 64-byte PrimDatum plus FP32 copies of the normal and the weight, converted once when the
+// tile is staged instead of once per pair (80 bytes: consecutive data start on different
+// shared-memory banks).
+struct __align__(16) PrimTile {
+    double c[3];
+    double n[3];
+    double a;
+    float diam;
+    float af;
+    float nf[3];
+    float pad;
+};
+static_assert(sizeof(PrimTile) == 80, "PrimTile must be 80 bytes");
+
 template <typename R>
-__device__ __forceinline__ void project_prims(int dom, const PrimDatum& X, const PrimDatum& Y, Proj<R>& g)
+__device__ __forceinline__ R col_normal(const PrimDatum& Y, int k) { return static_cast<R>(Y.n[k]); }
+template <typename R>
+__device__ __forceinline__ R col_normal(const PrimTile& Y, int k)
+{
+    if constexpr (std::is_same<R, float>::value) return Y.nf[k];
+    else return Y.n[k];
+}
+__device__ __forceinline__ float weight_f(const PrimDatum& Y) { return static_cast<float>(Y.a); }
+__device__ __forceinline__ float weight_f(const PrimTile& Y) { return Y.af; }
+__device__ __forceinline__ float weight_f(const ClusterDatum& Y) { return static_cast<float>(Y.a); }
+
+// Projection of v = y - x for two primitives. Triangles: P = n n^T, so only n.v is
+// needed (FP64); edges: P v = v - t (t.v) (FP64). Everything downstream of n.v (or of
+// P v) is well conditioned and is rounded to R.
+template <typename R, typename YD>
+__device__ __forceinline__ void project_prims(int dom, const PrimDatum& X, const YD& Y, Proj<R>& g)
 {
     const double v0 = Y.c[0] - X.c[0], v1 = Y.c[1] - X.c[1], v2 = Y.c[2] - X.c[2];
     g.v[0] = static_cast<R>(v0); g.v[1] = static_cast<R>(v1); g.v[2] = static_cast<R>(v2);
@@ -341,13 +368,13 @@ __device__ __forceinline__ void project_prims(int dom, const PrimDatum& X, const
     const double xv = X.n[0] * v0 + X.n[1] * v1 + X.n[2] * v2;
     const double yv = Y.n[0] * v0 + Y.n[1] * v1 + Y.n[2] * v2;
     if (dom == 2) {
-        g.cphi = static_cast<R>(xv * xv);
-        g.cpsi = static_cast<R>(yv * yv);
         const R xf = static_cast<R>(xv), yf = static_cast<R>(yv);
+        g.cphi = xf * xf;
+        g.cpsi = yf * yf;
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
             g.Pv[k] = static_cast<R>(X.n[k]) * xf;
-            g.Qv[k] = static_cast<R>(Y.n[k]) * yf;
+            g.Qv[k] = col_normal<R>(Y, k) * yf;
         }
     } else {
         const double p0 = v0 - X.n[0] * xv, p1 = v1 - X.n[1] * xv, p2 = v2 - X.n[2] * xv;
@@ -429,8 +456,8 @@ constexpr int FAR_TILE_UNION = 1536;
 // the current pair is evaluated. A row accumulates only its own derivative; each
 // unordered pair contributes its energy once (from the row with the smaller index),
 // CROSS pairs always.
-template <bool FAR, int QH, int PH, bool DIFF, int LANES, bool CROSS, bool PREFETCH, typename Datum, typename Index,
-          typename Fetch>
+template <bool FAR, int QH, int PH, bool DIFF, int LANES, bool CROSS, bool PREFETCH, typename ColDatum,
+          typename Datum, typename Index, typename Fetch>
 __device__ __forceinline__ void pair_row(const PairArgs& A, const Datum& X, int i, int sub, Index index, Fetch datum,
                                          double& e_row, double (&D64)[10])
 {
@@ -442,11 +469,11 @@ __device__ __forceinline__ void pair_row(const PairArgs& A, const Datum& X, int 
     int64_t k = k0 + sub;
     int un = (k < k1) ? index(k) : 0;
     int jn = 0;
-    Datum Yn;
+    ColDatum Yn;
     if (PREFETCH && k < k1) datum(un, jn, Yn);
     for (; k < k1; k += LANES) {
         int j;
-        Datum Y;
+        ColDatum Y;
         if constexpr (PREFETCH) {
             j = jn;
             Y = Yn;
@@ -476,7 +503,7 @@ __device__ __forceinline__ void pair_row(const PairArgs& A, const Datum& X, int 
                 for (int m = 0; m < 6; ++m) D64[4 + m] += a64.dP[m];
             }
         } else {
-            const float e = tp0_core<float, QH, PH, DIFF>(A.ex, g, ax, static_cast<float>(Y.a), acc);
+            const float e = tp0_core<float, QH, PH, DIFF>(A.ex, g, ax, weight_f(Y), acc);
             if (CROSS || j > i) e32 += e;
             if (++since_flush == PAIR_FLUSH) {
                 since_flush = 0;
@@ -587,16 +614,17 @@ __global__ void __launch_bounds__(PAIR_BLOCK) k_tp0_pairs(PairArgs A)
             j = u;
             Y = load_datum(cols, u);
         };
-        pair_row<FAR, QH, PH, DIFF, LANES, CROSS, true>(A, X, i, sub, index, datum, e_row, D64);
+        pair_row<FAR, QH, PH, DIFF, LANES, CROSS, true, Datum>(A, X, i, sub, index, datum, e_row, D64);
     }
     pair_epilogue<DIFF, LANES, CROSS>(A, active, i, sub, e_row, D64);
 }
 
 // Row tiles (build_row_tiles): block b owns the rows order[row0[b] .. row0[b+1]) and
 // stages the data of the union of their columns, cols[cols_rp[b] .. cols_rp[b+1]), in
-// shared memory with asynchronous 16-byte copies; entry k then reads its column datum
-// from shared-memory slot slot[k]. The 16-byte pieces of a datum are rotated by the slot
-// index, so that the lanes of a warp spread their shared-memory reads over all banks.
+// shared memory; entry k then reads its column datum from shared-memory slot slot[k].
+// Far tiles are copied with asynchronous 16-byte copies whose pieces are rotated by the
+// slot (the lanes of a warp then spread their reads over all banks); near tiles are
+// expanded to PrimTile on the way in.
 struct PairTiles {
     const int* row0;
     const int* cols_rp;
@@ -613,35 +641,57 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem)
 
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
-template <typename Datum>
-__device__ __forceinline__ Datum load_datum_rot(const float4* sdat, int u)
+__device__ __forceinline__ ClusterDatum load_cluster_rot(const float4* sdat, int u)
 {
-    Datum d;
+    ClusterDatum d;
     float4* o = reinterpret_cast<float4*>(&d);
 #pragma unroll
     for (int q = 0; q < 4; ++q) o[q] = sdat[4 * u + ((q + u) & 3)];
     return d;
 }
 
-// dynamic shared memory per tile of union size n: the data, then the column ids
-__host__ __device__ constexpr size_t pair_tile_smem(int n) { return static_cast<size_t>(n) * (64 + 4); }
+// dynamic shared memory per tile of union size n: the data (PrimTile 80 bytes, ClusterDatum
+// 64 bytes), then the column ids
+__host__ __device__ constexpr size_t pair_tile_smem(int n, bool far)
+{
+    return static_cast<size_t>(n) * ((far ? sizeof(ClusterDatum) : sizeof(PrimTile)) + sizeof(int));
+}
 
 template <bool FAR, int QH, int PH, bool DIFF, int LANES>
 __global__ void __launch_bounds__(PAIR_TILE_THREADS, 2) k_tp0_pairs_tiled(PairArgs A, PairTiles T)
 {
     static_assert(LANES == 1 || LANES == 2 || LANES == 4 || LANES == 8, "LANES must divide a warp");
     using Datum = typename std::conditional<FAR, ClusterDatum, PrimDatum>::type;
-    static_assert(sizeof(Datum) == 64, "64-byte data");
+    using ColDatum = typename std::conditional<FAR, ClusterDatum, PrimTile>::type;
     extern __shared__ float4 tile_smem[];
     const Datum* base = static_cast<const Datum*>(A.data);
     const int b = blockIdx.x;
     const int u0 = T.cols_rp[b], un = T.cols_rp[b + 1] - u0;
     float4* sdat = tile_smem;
-    int* sid = reinterpret_cast<int*>(tile_smem + 4 * static_cast<size_t>(un));
-    for (int idx = threadIdx.x; idx < 4 * un; idx += blockDim.x) {
-        const int u = idx >> 2, q = idx & 3;
-        const float4* src = reinterpret_cast<const float4*>(base + __ldg(T.cols + u0 + u)) + q;
-        cp_async16(sdat + 4 * u + ((q + u) & 3), src);
+    int* sid = reinterpret_cast<int*>(reinterpret_cast<char*>(tile_smem) + sizeof(ColDatum) * static_cast<size_t>(un));
+    if constexpr (FAR) {
+        for (int idx = threadIdx.x; idx < 4 * un; idx += blockDim.x) {
+            const int u = idx >> 2, q = idx & 3;
+            const float4* src = reinterpret_cast<const float4*>(base + __ldg(T.cols + u0 + u)) + q;
+            cp_async16(sdat + 4 * u + ((q + u) & 3), src);
+        }
+    } else {
+        PrimTile* st = reinterpret_cast<PrimTile*>(tile_smem);
+        for (int u = threadIdx.x; u < un; u += blockDim.x) {
+            const PrimDatum d = load_datum(base, __ldg(T.cols + u0 + u));
+            PrimTile t;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                t.c[k] = d.c[k];
+                t.n[k] = d.n[k];
+                t.nf[k] = static_cast<float>(d.n[k]);
+            }
+            t.a = d.a;
+            t.af = static_cast<float>(d.a);
+            t.diam = d.diam;
+            t.pad = 0.0f;
+            st[u] = t;
+        }
     }
     for (int u = threadIdx.x; u < un; u += blockDim.x) sid[u] = __ldg(T.cols + u0 + u);
     const int r0 = T.row0[b], nrows = T.row0[b + 1] - r0;
@@ -653,17 +703,18 @@ __global__ void __launch_bounds__(PAIR_TILE_THREADS, 2) k_tp0_pairs_tiled(PairAr
         i = T.order[r0 + slot];
         X = load_datum(base, i);
     }
-    cp_async_wait_all();
+    if constexpr (FAR) cp_async_wait_all();
     __syncthreads();
     double e_row = 0.0;
     double D64[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
     if (active) {
         auto index = [&](int64_t k) { return static_cast<int>(__ldg(T.slot + k)); };
-        auto datum = [&](int u, int& j, Datum& Y) {
-            Y = load_datum_rot<Datum>(sdat, u);
+        auto datum = [&](int u, int& j, ColDatum& Y) {
+            if constexpr (FAR) Y = load_cluster_rot(sdat, u);
+            else Y = reinterpret_cast<const PrimTile*>(tile_smem)[u];
             j = sid[u];
         };
-        pair_row<FAR, QH, PH, DIFF, LANES, false, false>(A, X, i, sub, index, datum, e_row, D64);
+        pair_row<FAR, QH, PH, DIFF, LANES, false, false, ColDatum>(A, X, i, sub, index, datum, e_row, D64);
     }
     pair_epilogue<DIFF, LANES, false>(A, active, i, sub, e_row, D64);
 }

@@ -148,7 +148,8 @@ rpb_status launch_geometry(rpb_mesh* m)
 template <int QH, int PH>
 static cudaError_t allow_tile_smem_t()
 {
-    const int nb = static_cast<int>(pair_tile_smem(NEAR_TILE_UNION)), fb = static_cast<int>(pair_tile_smem(FAR_TILE_UNION));
+    const int nb = static_cast<int>(pair_tile_smem(NEAR_TILE_UNION, false));
+    const int fb = static_cast<int>(pair_tile_smem(FAR_TILE_UNION, true));
     cudaError_t e = cudaSuccess;
     auto set = [&](const void* f, int bytes) {
         const cudaError_t r = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
@@ -186,7 +187,7 @@ static void launch_pairs_t(rpb_mesh* m, const PairArgs& An, const PairArgs& Af, 
     if (An.rows > 0) {
         const TileBufs& t = m->near_tiles;
         if (t.valid) {
-            const size_t smem = pair_tile_smem(t.max_union);
+            const size_t smem = pair_tile_smem(t.max_union, false);
             const int threads = PAIR_TILE_THREADS;
             if (diff) k_tp0_pairs_tiled<false, QH, PH, true, NEAR_LANES><<<t.tiles, threads, smem, m->stream>>>(An, tiles_view(t));
             else k_tp0_pairs_tiled<false, QH, PH, false, NEAR_LANES><<<t.tiles, threads, smem, m->stream>>>(An, tiles_view(t));
@@ -197,7 +198,7 @@ static void launch_pairs_t(rpb_mesh* m, const PairArgs& An, const PairArgs& Af, 
     if (Af.rows > 0) {
         const TileBufs& t = m->far_tiles;
         if (t.valid) {
-            const size_t smem = pair_tile_smem(t.max_union);
+            const size_t smem = pair_tile_smem(t.max_union, true);
             const int threads = PAIR_TILE_THREADS;
             if (diff) k_tp0_pairs_tiled<true, QH, PH, true, FAR_LANES><<<t.tiles, threads, smem, m->stream>>>(Af, tiles_view(t));
             else k_tp0_pairs_tiled<true, QH, PH, false, FAR_LANES><<<t.tiles, threads, smem, m->stream>>>(Af, tiles_view(t));
@@ -437,21 +438,33 @@ rpb_status rpb_mesh_create(int dom_dim, int amb_dim, const double* Vh, int64_t n
         // wave, whose few blocks would run while the other SMs idle).
         int sms = 0;
         if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, m->device) != cudaSuccess) sms = 0;
-        auto tile = [&](const SymPattern& P, int ncols, int lanes, const void* kernel, int cap, TileBufs& d,
+        auto tile = [&](const SymPattern& P, int ncols, int lanes, bool far, const void* kernel, int cap, TileBufs& d,
                         int& blocks) {
             d.valid = false;
-            int per_sm = 0;
-            if (sms <= 0 || P.nnz() == 0 ||
-                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, PAIR_TILE_THREADS, pair_tile_smem(cap)) !=
-                    cudaSuccess || per_sm <= 0)
-                return RPB_OK;
-            const int64_t slots = static_cast<int64_t>(per_sm) * sms, groups = PAIR_TILE_THREADS / lanes;
-            const int64_t waves = std::max<int64_t>(1, (P.rows + slots * groups - 1) / (slots * groups));
-            const int rows_per_tile = static_cast<int>((P.rows + waves * slots - 1) / (waves * slots));
+            auto resident = [&](int max_union) {
+                int per_sm = 0;
+                if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, PAIR_TILE_THREADS,
+                                                                  pair_tile_smem(max_union, far)) != cudaSuccess)
+                    return 0;
+                return per_sm;
+            };
+            if (sms <= 0 || P.nnz() == 0) return RPB_OK;
+            // resident blocks depend on the tiles' largest union and the tile size on the
+            // resident blocks: start from the cap and re-tile while the count changes
+            int per_sm = resident(cap);
             RowTiles R;
-            build_row_tiles(P.rp.data(), P.ci.data(), P.rows, ncols, rows_per_tile, cap,
-                            std::max(1, m->settings.threads), R);
-            if (!R.valid || R.tiles() == 0) return RPB_OK;
+            for (int pass = 0; pass < 3 && per_sm > 0; ++pass) {
+                const int64_t slots = static_cast<int64_t>(per_sm) * sms, groups = PAIR_TILE_THREADS / lanes;
+                const int64_t waves = std::max<int64_t>(1, (P.rows + slots * groups - 1) / (slots * groups));
+                const int rows_per_tile = static_cast<int>((P.rows + waves * slots - 1) / (waves * slots));
+                build_row_tiles(P.rp.data(), P.ci.data(), P.rows, ncols, rows_per_tile, cap,
+                                std::max(1, m->settings.threads), R);
+                if (!R.valid) break;
+                const int now = resident(R.max_union);
+                if (now == per_sm) break;
+                per_sm = now;
+            }
+            if (per_sm <= 0 || !R.valid || R.tiles() == 0) return RPB_OK;
             rpb_status e;
             if ((e = upload(d.row0, R.row0.data(), R.row0.size(), s)) != RPB_OK) return e;
             if ((e = upload(d.cols_rp, R.cols_rp.data(), R.cols_rp.size(), s)) != RPB_OK) return e;
@@ -467,8 +480,10 @@ rpb_status rpb_mesh_create(int dom_dim, int amb_dim, const double* Vh, int64_t n
         if ((st = allow_tile_smem(m->device)) != RPB_OK) return fail(st);
         const void* kn = reinterpret_cast<const void*>(k_tp0_pairs_tiled<false, 3, 6, true, NEAR_LANES>);
         const void* kf = reinterpret_cast<const void*>(k_tp0_pairs_tiled<true, 3, 6, true, FAR_LANES>);
-        if ((st = tile(T.near, m->N, NEAR_LANES, kn, NEAR_TILE_UNION, m->near_tiles, m->near_blocks)) != RPB_OK) return fail(st);
-        if ((st = tile(T.far, m->NC, FAR_LANES, kf, FAR_TILE_UNION, m->far_tiles, m->far_blocks)) != RPB_OK) return fail(st);
+        if ((st = tile(T.near, m->N, NEAR_LANES, false, kn, NEAR_TILE_UNION, m->near_tiles, m->near_blocks)) != RPB_OK)
+            return fail(st);
+        if ((st = tile(T.far, m->NC, FAR_LANES, true, kf, FAR_TILE_UNION, m->far_tiles, m->far_blocks)) != RPB_OK)
+            return fail(st);
     }
     if (m->block_energy.alloc(m->near_blocks + m->far_blocks)) { set_error("device allocation failed"); return fail(RPB_ENOMEM); }
     if (cudaMemsetAsync(m->counter.ptr, 0, m->counter.bytes(), s) != cudaSuccess ||
