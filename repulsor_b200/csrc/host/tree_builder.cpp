@@ -680,69 +680,109 @@ std::string build_cross_lists(const HostTree& S, const double* VS, const int* SS
     return std::string();
 }
 
-void build_row_tiles(const int64_t* rp, const int* ci, int rows, int ncols, int max_rows, int max_union, int threads,
-                     RowTiles& out)
+void build_row_tiles(const int64_t* rp, const int* ci, int rows, int ncols, int block_lanes, int64_t target_entries,
+                     int max_union, int threads, RowTiles& out)
 {
     out = RowTiles();
     max_union = std::min(max_union, 65535);
+    if (block_lanes < 1 || block_lanes % 32 != 0) return;
     for (int i = 0; i < rows; ++i)
         if (rp[i + 1] - rp[i] > max_union) return;
-    // chunks of rows (a whole number of full tiles) are tiled independently
-    max_rows = std::max(1, max_rows);
-    const int chunk = max_rows * ((4096 + max_rows - 1) / max_rows);
-    const int nchunks = (rows + chunk - 1) / chunk;
-    struct Part {
-        std::vector<int> row0, cols_rp, cols, order;
-        int max_union = 0;
-    };
-    std::vector<Part> parts(nchunks);
+    target_entries = std::max<int64_t>(1, target_entries);
+    out.block_lanes = block_lanes;
+    // tile boundaries (sequential): add rows until the tile holds target_entries entries,
+    // block_lanes rows, or the column union would exceed the cap
+    {
+        std::vector<char> mark(ncols, 0);
+        std::vector<int> U;
+        int r = 0;
+        while (r < rows) {
+            const int t0 = r;
+            int64_t entries = 0;
+            U.clear();
+            while (r < rows && entries < target_entries && r - t0 < block_lanes) {
+                int fresh = 0;
+                for (int64_t k = rp[r]; k < rp[r + 1]; ++k) fresh += !mark[ci[k]];
+                if (r > t0 && static_cast<int>(U.size()) + fresh > max_union) break;
+                for (int64_t k = rp[r]; k < rp[r + 1]; ++k)
+                    if (!mark[ci[k]]) { mark[ci[k]] = 1; U.push_back(ci[k]); }
+                entries += rp[r + 1] - rp[r];
+                ++r;
+            }
+            for (int u : U) mark[u] = 0;
+            out.row0.push_back(t0);
+            out.cols_rp.push_back(static_cast<int>(U.size()));   // sizes for now
+        }
+        out.row0.push_back(rows);
+    }
+    const int nt = out.tiles();
+    {
+        std::vector<int> sizes(out.cols_rp.begin(), out.cols_rp.end());
+        out.cols_rp.assign(nt + 1, 0);
+        for (int b = 0; b < nt; ++b) {
+            out.cols_rp[b + 1] = out.cols_rp[b] + sizes[b];
+            out.max_union = std::max(out.max_union, sizes[b]);
+        }
+    }
+    out.cols.assign(out.cols_rp[nt], 0);
     out.slot.assign(static_cast<size_t>(rows > 0 ? rp[rows] : 0), 0);
+    out.order.assign(rows, 0);
+    out.lane_map.assign(static_cast<size_t>(nt) * block_lanes, -1);
+    // per tile (parallel): sorted union, slots, lane groups, row order, lane map
     std::atomic<int> ticket{0};
-    run_threads(std::max(1, std::min(threads, nchunks)), [&](int) {
-        std::vector<int> pos(ncols, -1), U;
+    run_threads(std::max(1, std::min(threads, nt)), [&](int) {
+        std::vector<int> pos(ncols, -1), U, size, idx;
         for (;;) {
-            const int c = ticket.fetch_add(1);
-            if (c >= nchunks) break;
-            Part& P = parts[c];
-            const int r_end = std::min(rows, (c + 1) * chunk);
-            int r = c * chunk;
-            while (r < r_end) {
-                const int t0 = r;
-                U.clear();
-                while (r < r_end && r - t0 < max_rows) {
-                    int fresh = 0;
-                    for (int64_t k = rp[r]; k < rp[r + 1]; ++k) fresh += (pos[ci[k]] < 0);
-                    if (r > t0 && static_cast<int>(U.size()) + fresh > max_union) break;
-                    for (int64_t k = rp[r]; k < rp[r + 1]; ++k)
-                        if (pos[ci[k]] < 0) { pos[ci[k]] = 0; U.push_back(ci[k]); }
-                    ++r;
-                }
-                std::sort(U.begin(), U.end());
-                for (size_t u = 0; u < U.size(); ++u) pos[U[u]] = static_cast<int>(u);
-                for (int i = t0; i < r; ++i)
-                    for (int64_t k = rp[i]; k < rp[i + 1]; ++k) out.slot[k] = static_cast<uint16_t>(pos[ci[k]]);
-                P.row0.push_back(t0);
-                P.cols_rp.push_back(static_cast<int>(U.size()));
-                P.cols.insert(P.cols.end(), U.begin(), U.end());
-                P.max_union = std::max(P.max_union, static_cast<int>(U.size()));
-                const size_t o0 = P.order.size();
-                for (int i = t0; i < r; ++i) P.order.push_back(i);
-                std::stable_sort(P.order.begin() + o0, P.order.end(),
-                                 [&](int a, int b) { return (rp[a + 1] - rp[a]) > (rp[b + 1] - rp[b]); });
-                for (int u : U) pos[u] = -1;
+            const int b = ticket.fetch_add(1);
+            if (b >= nt) break;
+            const int t0 = out.row0[b], t1 = out.row0[b + 1], R = t1 - t0;
+            U.clear();
+            for (int64_t k = rp[t0]; k < rp[t1]; ++k)
+                if (pos[ci[k]] < 0) { pos[ci[k]] = 0; U.push_back(ci[k]); }
+            std::sort(U.begin(), U.end());
+            for (size_t u = 0; u < U.size(); ++u) {
+                pos[U[u]] = static_cast<int>(u);
+                out.cols[out.cols_rp[b] + u] = U[u];
+            }
+            for (int64_t k = rp[t0]; k < rp[t1]; ++k) out.slot[k] = static_cast<uint16_t>(pos[ci[k]]);
+            for (int u : U) pos[u] = -1;
+            // lane groups: every row starts with one lane; the row with the most entries per
+            // lane doubles its group while the block has lanes left (groups of at most 32)
+            auto len = [&](int q) { return rp[t0 + q + 1] - rp[t0 + q]; };
+            auto load = [&](int q) { return (len(q) + size[q] - 1) / size[q]; };
+            size.assign(R, 1);
+            int used = R;
+            auto cmp = [&](int x, int y) { return load(x) < load(y) || (load(x) == load(y) && x > y); };
+            std::vector<int> heap(R);
+            for (int q = 0; q < R; ++q) heap[q] = q;
+            std::make_heap(heap.begin(), heap.end(), cmp);
+            while (!heap.empty()) {
+                std::pop_heap(heap.begin(), heap.end(), cmp);
+                const int q = heap.back();
+                if (size[q] >= 32 || used + size[q] > block_lanes || len(q) <= size[q]) break;
+                used += size[q];
+                size[q] *= 2;
+                std::push_heap(heap.begin(), heap.end(), cmp);
+            }
+            // groups in decreasing size (then decreasing length) start at multiples of their
+            // size and never straddle a warp
+            idx.resize(R);
+            for (int q = 0; q < R; ++q) idx[q] = q;
+            std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) {
+                return size[x] > size[y] || (size[x] == size[y] && len(x) > len(y));
+            });
+            int lane = 0;
+            for (int pos_in_tile = 0; pos_in_tile < R; ++pos_in_tile) {
+                const int q = idx[pos_in_tile];
+                out.order[t0 + pos_in_tile] = t0 + q;
+                int lg = 0;
+                while ((1 << lg) < size[q]) ++lg;
+                for (int sub = 0; sub < size[q]; ++sub)
+                    out.lane_map[static_cast<size_t>(b) * block_lanes + lane + sub] = (pos_in_tile << 8) | (lg << 5) | sub;
+                lane += size[q];
             }
         }
     });
-    out.row0.reserve(rows + 1);
-    out.cols_rp.push_back(0);
-    for (const Part& P : parts) {
-        out.row0.insert(out.row0.end(), P.row0.begin(), P.row0.end());
-        for (int n : P.cols_rp) out.cols_rp.push_back(out.cols_rp.back() + n);
-        out.cols.insert(out.cols.end(), P.cols.begin(), P.cols.end());
-        out.order.insert(out.order.end(), P.order.begin(), P.order.end());
-        out.max_union = std::max(out.max_union, P.max_union);
-    }
-    out.row0.push_back(rows);
     out.valid = true;
 }
 

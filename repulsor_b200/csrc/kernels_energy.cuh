@@ -442,24 +442,24 @@ constexpr int FAR_LANES = 2;
 
 constexpr int pair_blocks(int rows, int lanes) { return (rows * lanes + PAIR_BLOCK - 1) / PAIR_BLOCK; }
 
-// Row tiles of the shared-memory kernels: threads per block (PAIR_TILE_THREADS / LANES rows
-// at most per tile, two blocks per SM) and the largest column union a tile may stage
-// (64-byte data + a 4-byte id per column). The host sizes the tiles so that their count
-// is a whole number of waves of resident blocks.
+// Row tiles of the shared-memory kernels: threads per block (two blocks per SM), the mean
+// rows per tile the host aims below, and the largest column union a tile may stage. The
+// host sizes the tiles so that their count is a whole number of waves of resident blocks.
 constexpr int PAIR_TILE_THREADS = 288;
+constexpr int TILE_ROWS = 144;
 constexpr int NEAR_TILE_UNION = 1024;
 constexpr int FAR_TILE_UNION = 1536;
 
-// One lane's share of a row: the row's entries k = k0 + sub, k0 + sub + LANES, ... with the
+// One lane's share of a row: the row's entries k = k0 + sub, k0 + sub + stride, ... with the
 // column handle u = index(k) and the column datum from datum(u, j, Y) (j: the column's
 // tree position). The next entry's handle (PREFETCH: and its datum) is requested before
 // the current pair is evaluated. A row accumulates only its own derivative; each
 // unordered pair contributes its energy once (from the row with the smaller index),
 // CROSS pairs always.
-template <bool FAR, int QH, int PH, bool DIFF, int LANES, bool CROSS, bool PREFETCH, typename ColDatum,
-          typename Datum, typename Index, typename Fetch>
-__device__ __forceinline__ void pair_row(const PairArgs& A, const Datum& X, int i, int sub, Index index, Fetch datum,
-                                         double& e_row, double (&D64)[10])
+template <bool FAR, int QH, int PH, bool DIFF, bool CROSS, bool PREFETCH, typename ColDatum, typename Datum,
+          typename Index, typename Fetch>
+__device__ __forceinline__ void pair_row(const PairArgs& A, const Datum& X, int i, int sub, int stride, Index index,
+                                         Fetch datum, double& e_row, double (&D64)[10])
 {
     const float ax = static_cast<float>(X.a);
     PairAcc<float> acc = {};
@@ -471,16 +471,16 @@ __device__ __forceinline__ void pair_row(const PairArgs& A, const Datum& X, int 
     int jn = 0;
     ColDatum Yn;
     if (PREFETCH && k < k1) datum(un, jn, Yn);
-    for (; k < k1; k += LANES) {
+    for (; k < k1; k += stride) {
         int j;
         ColDatum Y;
         if constexpr (PREFETCH) {
             j = jn;
             Y = Yn;
-            if (k + LANES < k1) datum(index(k + LANES), jn, Yn);
+            if (k + stride < k1) datum(index(k + stride), jn, Yn);
         } else {
             datum(un, j, Y);
-            if (k + LANES < k1) un = index(k + LANES);
+            if (k + stride < k1) un = index(k + stride);
         }
         Proj<float> g;
         if constexpr (FAR) project_clusters(X, Y, g);
@@ -530,24 +530,30 @@ __device__ __forceinline__ void pair_row(const PairArgs& A, const Datum& X, int 
     }
 }
 
-// Combines the LANES partial sums of a row (xor butterfly, every lane of the warp takes
-// part), writes the row's derivative, and reduces the energy deterministically: one
-// partial per block, the last block to finish sums the partials in block order.
-template <bool DIFF, int LANES, bool CROSS>
-__device__ __forceinline__ void pair_epilogue(const PairArgs& A, bool active, int i, int sub, double e_row,
-                                              double (&D64)[10])
+// Combines the partial sums of a row's lane group (size lanes, aligned: an xor butterfly
+// over offsets below the warp's largest group, every lane of the warp takes part, a lane
+// adds only offsets inside its group), writes the row's derivative, and reduces the
+// energy deterministically: one partial per block, the last block to finish sums the
+// partials in block order.
+template <bool DIFF, bool CROSS>
+__device__ __forceinline__ void pair_epilogue(const PairArgs& A, bool active, int i, int sub, int size, int warp_size_max,
+                                              double e_row, double (&D64)[10])
 {
     if constexpr (CROSS) {
         e_row *= 0.5;
 #pragma unroll
         for (int m = 0; m < 10; ++m) D64[m] *= 0.5;
     }
-#pragma unroll
-    for (int off = 1; off < LANES; off <<= 1) {
-        e_row += __shfl_xor_sync(0xffffffffu, e_row, off);
+    for (int off = 1; off < warp_size_max; off <<= 1) {
+        const bool in = off < size;
+        const double e = __shfl_xor_sync(0xffffffffu, e_row, off);
+        if (in) e_row += e;
         if (DIFF) {
 #pragma unroll
-            for (int m = 0; m < 10; ++m) D64[m] += __shfl_xor_sync(0xffffffffu, D64[m], off);
+            for (int m = 0; m < 10; ++m) {
+                const double d = __shfl_xor_sync(0xffffffffu, D64[m], off);
+                if (in) D64[m] += d;
+            }
         }
     }
     if (DIFF && active && sub == 0) {
@@ -614,9 +620,9 @@ __global__ void __launch_bounds__(PAIR_BLOCK) k_tp0_pairs(PairArgs A)
             j = u;
             Y = load_datum(cols, u);
         };
-        pair_row<FAR, QH, PH, DIFF, LANES, CROSS, true, Datum>(A, X, i, sub, index, datum, e_row, D64);
+        pair_row<FAR, QH, PH, DIFF, CROSS, true, Datum>(A, X, i, sub, LANES, index, datum, e_row, D64);
     }
-    pair_epilogue<DIFF, LANES, CROSS>(A, active, i, sub, e_row, D64);
+    pair_epilogue<DIFF, CROSS>(A, active, i, sub, LANES, LANES, e_row, D64);
 }
 
 // Row tiles (build_row_tiles): block b owns the rows order[row0[b] .. row0[b+1]) and
@@ -624,13 +630,15 @@ __global__ void __launch_bounds__(PAIR_BLOCK) k_tp0_pairs(PairArgs A)
 // shared memory; entry k then reads its column datum from shared-memory slot slot[k].
 // Far tiles are copied with asynchronous 16-byte copies whose pieces are rotated by the
 // slot (the lanes of a warp then spread their reads over all banks); near tiles are
-// expanded to PrimTile on the way in.
+// expanded to PrimTile on the way in. Each thread's row, group size and lane in the
+// group come from the tile's lane map, so long rows get more lanes.
 struct PairTiles {
     const int* row0;
     const int* cols_rp;
     const int* cols;
     const uint16_t* slot;
     const int* order;
+    const int* lane_map;      // tiles x PAIR_TILE_THREADS (RowTiles::lane_map)
 };
 
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem)
@@ -657,10 +665,9 @@ __host__ __device__ constexpr size_t pair_tile_smem(int n, bool far)
     return static_cast<size_t>(n) * ((far ? sizeof(ClusterDatum) : sizeof(PrimTile)) + sizeof(int));
 }
 
-template <bool FAR, int QH, int PH, bool DIFF, int LANES>
+template <bool FAR, int QH, int PH, bool DIFF>
 __global__ void __launch_bounds__(PAIR_TILE_THREADS, 2) k_tp0_pairs_tiled(PairArgs A, PairTiles T)
 {
-    static_assert(LANES == 1 || LANES == 2 || LANES == 4 || LANES == 8, "LANES must divide a warp");
     using Datum = typename std::conditional<FAR, ClusterDatum, PrimDatum>::type;
     using ColDatum = typename std::conditional<FAR, ClusterDatum, PrimTile>::type;
     extern __shared__ float4 tile_smem[];
@@ -694,13 +701,15 @@ __global__ void __launch_bounds__(PAIR_TILE_THREADS, 2) k_tp0_pairs_tiled(PairAr
         }
     }
     for (int u = threadIdx.x; u < un; u += blockDim.x) sid[u] = __ldg(T.cols + u0 + u);
-    const int r0 = T.row0[b], nrows = T.row0[b + 1] - r0;
-    const int slot = threadIdx.x / LANES, sub = threadIdx.x & (LANES - 1);
-    const bool active = slot < nrows;
+    const int r0 = T.row0[b];
+    const int lm = __ldg(T.lane_map + static_cast<int64_t>(b) * PAIR_TILE_THREADS + threadIdx.x);
+    const bool active = lm >= 0;
+    const int sub = active ? (lm & 31) : 0, size = active ? (1 << ((lm >> 5) & 7)) : 1;
+    const int warp_size_max = __reduce_max_sync(0xffffffffu, size);
     int i = 0;
     Datum X;
     if (active) {
-        i = T.order[r0 + slot];
+        i = T.order[r0 + (lm >> 8)];
         X = load_datum(base, i);
     }
     if constexpr (FAR) cp_async_wait_all();
@@ -714,9 +723,9 @@ __global__ void __launch_bounds__(PAIR_TILE_THREADS, 2) k_tp0_pairs_tiled(PairAr
             else Y = reinterpret_cast<const PrimTile*>(tile_smem)[u];
             j = sid[u];
         };
-        pair_row<FAR, QH, PH, DIFF, LANES, false, false, ColDatum>(A, X, i, sub, index, datum, e_row, D64);
+        pair_row<FAR, QH, PH, DIFF, false, false, ColDatum>(A, X, i, sub, size, index, datum, e_row, D64);
     }
-    pair_epilogue<DIFF, LANES, false>(A, active, i, sub, e_row, D64);
+    pair_epilogue<DIFF, false>(A, active, i, sub, size, warp_size_max, e_row, D64);
 }
 
 // energy = near-field part + far-field part (the order evaluate() uses on the host)

@@ -41,7 +41,8 @@ int64_t rpb_mesh::device_bytes() const
     b += near.rp.bytes() + near.ci.bytes() + far.rp.bytes() + far.ci.bytes() + verynear.rp.bytes() +
          verynear.ci.bytes() + near_order.bytes() + far_order.bytes();
     for (const rpb::TileBufs* t : {&near_tiles, &far_tiles})
-        b += t->row0.bytes() + t->cols_rp.bytes() + t->cols.bytes() + t->order.bytes() + t->slot.bytes();
+        b += t->row0.bytes() + t->cols_rp.bytes() + t->cols.bytes() + t->order.bytes() + t->slot.bytes() +
+             t->lane_map.bytes();
     b += P_pair.bytes() + C_pair.bytes() + C_mom.bytes() + counter.bytes() + P_near.bytes() + scan_local.bytes() +
          scan_blocks.bytes() + C_begin.bytes() + C_end.bytes();
     b += D_near.bytes() + D_far.bytes() + D_vf.bytes() + B.bytes() + v_rp.bytes() + v_slot.bytes() + Y.bytes();
@@ -155,10 +156,10 @@ static cudaError_t allow_tile_smem_t()
         const cudaError_t r = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
         if (e == cudaSuccess) e = r;
     };
-    set(reinterpret_cast<const void*>(k_tp0_pairs_tiled<false, QH, PH, true, NEAR_LANES>), nb);
-    set(reinterpret_cast<const void*>(k_tp0_pairs_tiled<false, QH, PH, false, NEAR_LANES>), nb);
-    set(reinterpret_cast<const void*>(k_tp0_pairs_tiled<true, QH, PH, true, FAR_LANES>), fb);
-    set(reinterpret_cast<const void*>(k_tp0_pairs_tiled<true, QH, PH, false, FAR_LANES>), fb);
+    set(reinterpret_cast<const void*>(k_tp0_pairs_tiled<false, QH, PH, true>), nb);
+    set(reinterpret_cast<const void*>(k_tp0_pairs_tiled<false, QH, PH, false>), nb);
+    set(reinterpret_cast<const void*>(k_tp0_pairs_tiled<true, QH, PH, true>), fb);
+    set(reinterpret_cast<const void*>(k_tp0_pairs_tiled<true, QH, PH, false>), fb);
     return e;
 }
 
@@ -178,7 +179,7 @@ static rpb_status allow_tile_smem(int device)
 
 static PairTiles tiles_view(const TileBufs& t)
 {
-    return PairTiles{t.row0.ptr, t.cols_rp.ptr, t.cols.ptr, t.slot.ptr, t.order.ptr};
+    return PairTiles{t.row0.ptr, t.cols_rp.ptr, t.cols.ptr, t.slot.ptr, t.order.ptr, t.lane_map.ptr};
 }
 
 template <int QH, int PH>
@@ -189,8 +190,8 @@ static void launch_pairs_t(rpb_mesh* m, const PairArgs& An, const PairArgs& Af, 
         if (t.valid) {
             const size_t smem = pair_tile_smem(t.max_union, false);
             const int threads = PAIR_TILE_THREADS;
-            if (diff) k_tp0_pairs_tiled<false, QH, PH, true, NEAR_LANES><<<t.tiles, threads, smem, m->stream>>>(An, tiles_view(t));
-            else k_tp0_pairs_tiled<false, QH, PH, false, NEAR_LANES><<<t.tiles, threads, smem, m->stream>>>(An, tiles_view(t));
+            if (diff) k_tp0_pairs_tiled<false, QH, PH, true><<<t.tiles, threads, smem, m->stream>>>(An, tiles_view(t));
+            else k_tp0_pairs_tiled<false, QH, PH, false><<<t.tiles, threads, smem, m->stream>>>(An, tiles_view(t));
         } else if (diff) k_tp0_pairs<false, QH, PH, true, NEAR_LANES><<<m->near_blocks, PAIR_BLOCK, 0, m->stream>>>(An);
         else k_tp0_pairs<false, QH, PH, false, NEAR_LANES><<<m->near_blocks, PAIR_BLOCK, 0, m->stream>>>(An);
     }
@@ -200,8 +201,8 @@ static void launch_pairs_t(rpb_mesh* m, const PairArgs& An, const PairArgs& Af, 
         if (t.valid) {
             const size_t smem = pair_tile_smem(t.max_union, true);
             const int threads = PAIR_TILE_THREADS;
-            if (diff) k_tp0_pairs_tiled<true, QH, PH, true, FAR_LANES><<<t.tiles, threads, smem, m->stream>>>(Af, tiles_view(t));
-            else k_tp0_pairs_tiled<true, QH, PH, false, FAR_LANES><<<t.tiles, threads, smem, m->stream>>>(Af, tiles_view(t));
+            if (diff) k_tp0_pairs_tiled<true, QH, PH, true><<<t.tiles, threads, smem, m->stream>>>(Af, tiles_view(t));
+            else k_tp0_pairs_tiled<true, QH, PH, false><<<t.tiles, threads, smem, m->stream>>>(Af, tiles_view(t));
         } else if (diff) k_tp0_pairs<true, QH, PH, true, FAR_LANES><<<m->far_blocks, PAIR_BLOCK, 0, m->stream>>>(Af);
         else k_tp0_pairs<true, QH, PH, false, FAR_LANES><<<m->far_blocks, PAIR_BLOCK, 0, m->stream>>>(Af);
     }
@@ -433,13 +434,12 @@ rpb_status rpb_mesh_create(int dom_dim, int amb_dim, const double* Vh, int64_t n
         m->near_blocks = pair_blocks(m->N, NEAR_LANES);
         m->far_blocks = pair_blocks(m->NC, FAR_LANES);
         // shared-memory row tiles; the kernels' grids are then one block per tile
-        // Tiles hold at most PAIR_TILE_THREADS / LANES rows; their row count is chosen so
-        // that the tiles fill a whole number of waves of resident blocks (no partial last
-        // wave, whose few blocks would run while the other SMs idle).
+        // Tiles are balanced by entries and their count is a whole number of waves of
+        // resident blocks (no partial last wave, whose few blocks would run while the
+        // other SMs idle); about TILE_ROWS rows per tile.
         int sms = 0;
         if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, m->device) != cudaSuccess) sms = 0;
-        auto tile = [&](const SymPattern& P, int ncols, int lanes, bool far, const void* kernel, int cap, TileBufs& d,
-                        int& blocks) {
+        auto tile = [&](const SymPattern& P, int ncols, bool far, const void* kernel, int cap, TileBufs& d, int& blocks) {
             d.valid = false;
             auto resident = [&](int max_union) {
                 int per_sm = 0;
@@ -454,10 +454,10 @@ rpb_status rpb_mesh_create(int dom_dim, int amb_dim, const double* Vh, int64_t n
             int per_sm = resident(cap);
             RowTiles R;
             for (int pass = 0; pass < 3 && per_sm > 0; ++pass) {
-                const int64_t slots = static_cast<int64_t>(per_sm) * sms, groups = PAIR_TILE_THREADS / lanes;
-                const int64_t waves = std::max<int64_t>(1, (P.rows + slots * groups - 1) / (slots * groups));
-                const int rows_per_tile = static_cast<int>((P.rows + waves * slots - 1) / (waves * slots));
-                build_row_tiles(P.rp.data(), P.ci.data(), P.rows, ncols, rows_per_tile, cap,
+                const int64_t slots = static_cast<int64_t>(per_sm) * sms;
+                const int64_t waves = std::max<int64_t>(1, (P.rows + slots * TILE_ROWS - 1) / (slots * TILE_ROWS));
+                const int64_t target = (P.nnz() + waves * slots - 1) / (waves * slots);
+                build_row_tiles(P.rp.data(), P.ci.data(), P.rows, ncols, PAIR_TILE_THREADS, target, cap,
                                 std::max(1, m->settings.threads), R);
                 if (!R.valid) break;
                 const int now = resident(R.max_union);
@@ -471,6 +471,7 @@ rpb_status rpb_mesh_create(int dom_dim, int amb_dim, const double* Vh, int64_t n
             if ((e = upload(d.cols, R.cols.data(), R.cols.size(), s)) != RPB_OK) return e;
             if ((e = upload(d.order, R.order.data(), R.order.size(), s)) != RPB_OK) return e;
             if ((e = upload(d.slot, R.slot.data(), R.slot.size(), s)) != RPB_OK) return e;
+            if ((e = upload(d.lane_map, R.lane_map.data(), R.lane_map.size(), s)) != RPB_OK) return e;
             d.tiles = R.tiles();
             d.max_union = R.max_union;
             d.valid = true;
@@ -478,11 +479,11 @@ rpb_status rpb_mesh_create(int dom_dim, int amb_dim, const double* Vh, int64_t n
             return RPB_OK;
         };
         if ((st = allow_tile_smem(m->device)) != RPB_OK) return fail(st);
-        const void* kn = reinterpret_cast<const void*>(k_tp0_pairs_tiled<false, 3, 6, true, NEAR_LANES>);
-        const void* kf = reinterpret_cast<const void*>(k_tp0_pairs_tiled<true, 3, 6, true, FAR_LANES>);
-        if ((st = tile(T.near, m->N, NEAR_LANES, false, kn, NEAR_TILE_UNION, m->near_tiles, m->near_blocks)) != RPB_OK)
+        const void* kn = reinterpret_cast<const void*>(k_tp0_pairs_tiled<false, 3, 6, true>);
+        const void* kf = reinterpret_cast<const void*>(k_tp0_pairs_tiled<true, 3, 6, true>);
+        if ((st = tile(T.near, m->N, false, kn, NEAR_TILE_UNION, m->near_tiles, m->near_blocks)) != RPB_OK)
             return fail(st);
-        if ((st = tile(T.far, m->NC, FAR_LANES, true, kf, FAR_TILE_UNION, m->far_tiles, m->far_blocks)) != RPB_OK)
+        if ((st = tile(T.far, m->NC, true, kf, FAR_TILE_UNION, m->far_tiles, m->far_blocks)) != RPB_OK)
             return fail(st);
     }
     if (m->block_energy.alloc(m->near_blocks + m->far_blocks)) { set_error("device allocation failed"); return fail(RPB_ENOMEM); }

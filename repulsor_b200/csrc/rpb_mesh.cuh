@@ -66,7 +66,7 @@ struct PseudoLapCache {
 
 // Device copy of a pattern's row tiles (RowTiles); valid == false: the gather kernels run.
 struct TileBufs {
-    DevBuf<int> row0, cols_rp, cols, order;
+    DevBuf<int> row0, cols_rp, cols, order, lane_map;
     DevBuf<uint16_t> slot;
     int tiles = 0, max_union = 0;
     bool valid = false;

@@ -1,7 +1,9 @@
 // Invariants of build_row_tiles on seeded random banded symmetric patterns: tiles cover
-// the rows in order, every union is sorted, unique and within the cap, every entry's slot
-// names its column, each tile's order is a permutation of its rows by decreasing length,
-// and a row longer than the cap disables the tiles. Prints "ok" or the first violation.
+// the rows in order and stay within the row, entry and union bounds, every union is
+// sorted and unique, every entry's slot names its column, each tile's order is a
+// permutation of its rows, and the lane map gives every row one aligned power-of-two
+// group inside a warp (each lane at most once). A row longer than the cap disables the
+// tiles. Prints "ok" or the first violation.
 #include <algorithm>
 #include <cstdio>
 #include <random>
@@ -9,7 +11,7 @@
 
 #include "host/tree_builder.hpp"
 
-static int check(int rows, int band, int max_rows, int cap, int threads, unsigned seed)
+static int check(int rows, int band, int lanes, int cap, int threads, unsigned seed)
 {
     std::mt19937 rng(seed);
     std::vector<std::vector<int>> adj(rows);
@@ -28,7 +30,8 @@ static int check(int rows, int band, int max_rows, int cap, int threads, unsigne
         rp[i + 1] = static_cast<int64_t>(ci.size());
     }
     rpb::RowTiles T;
-    rpb::build_row_tiles(rp.data(), ci.data(), rows, rows, max_rows, cap, threads, T);
+    const int64_t target = std::max<int64_t>(1, rp[rows] / std::max(1, rows / 100));
+    rpb::build_row_tiles(rp.data(), ci.data(), rows, rows, lanes, target, cap, threads, T);
     int64_t longest = 0;
     for (int i = 0; i < rows; ++i) longest = std::max(longest, rp[i + 1] - rp[i]);
     if (longest > cap) {
@@ -37,24 +40,39 @@ static int check(int rows, int band, int max_rows, int cap, int threads, unsigne
     }
     if (!T.valid) { std::printf("tiles invalid\n"); return 1; }
     if (T.row0.front() != 0 || T.row0.back() != rows) { std::printf("row range\n"); return 1; }
+    if (static_cast<int>(T.lane_map.size()) != T.tiles() * lanes) { std::printf("lane map size\n"); return 1; }
     for (int b = 0; b < T.tiles(); ++b) {
         const int r0 = T.row0[b], r1 = T.row0[b + 1];
-        if (r1 <= r0 || r1 - r0 > max_rows) { std::printf("tile %d rows %d..%d\n", b, r0, r1); return 1; }
+        if (r1 <= r0 || r1 - r0 > lanes) { std::printf("tile %d rows %d..%d\n", b, r0, r1); return 1; }
+        if (rp[r1 - 1] - rp[r0] >= target && r1 - r0 > 1) { std::printf("tile %d over the entry target\n", b); return 1; }
         const int u0 = T.cols_rp[b], un = T.cols_rp[b + 1] - u0;
         if (un > cap || un > T.max_union) { std::printf("tile %d union %d\n", b, un); return 1; }
         for (int u = 1; u < un; ++u)
             if (T.cols[u0 + u] <= T.cols[u0 + u - 1]) { std::printf("tile %d union not ascending\n", b); return 1; }
-        std::vector<int> seen(rows, 0);
+        std::vector<int> seen(rows, 0), group_size(r1 - r0, 0);
+        std::vector<int64_t> group_lanes(r1 - r0, 0);
         for (int k = r0; k < r1; ++k) {
             const int i = T.order[k];
             if (i < r0 || i >= r1 || seen[i]++) { std::printf("tile %d order\n", b); return 1; }
-            if (k > r0) {
-                const int h = T.order[k - 1];
-                if (rp[h + 1] - rp[h] < rp[i + 1] - rp[i]) { std::printf("tile %d order not by length\n", b); return 1; }
-            }
             for (int64_t e = rp[i]; e < rp[i + 1]; ++e)
                 if (T.slot[e] >= un || T.cols[u0 + T.slot[e]] != ci[e]) { std::printf("slot of entry %ld\n", (long)e); return 1; }
         }
+        for (int t = 0; t < lanes; ++t) {
+            const int m = T.lane_map[static_cast<size_t>(b) * lanes + t];
+            if (m < 0) continue;
+            const int q = m >> 8, lg = (m >> 5) & 7, sub = m & 31, size = 1 << lg;
+            if (q >= r1 - r0 || lg > 5 || sub >= size) { std::printf("tile %d lane %d map\n", b, t); return 1; }
+            const int start = t - sub;
+            if (start % size != 0 || start / 32 != (start + size - 1) / 32) { std::printf("tile %d group alignment\n", b); return 1; }
+            if (group_size[q] == 0) group_size[q] = size;
+            else if (group_size[q] != size) { std::printf("tile %d group size\n", b); return 1; }
+            group_lanes[q] += int64_t(1) << sub;   // each lane of the group exactly once
+        }
+        for (int q = 0; q < r1 - r0; ++q)
+            if (group_size[q] == 0 || group_lanes[q] != static_cast<int64_t>((1ull << group_size[q]) - 1)) {
+                std::printf("tile %d row %d lanes\n", b, q);
+                return 1;
+            }
     }
     return 0;
 }
@@ -62,11 +80,12 @@ static int check(int rows, int band, int max_rows, int cap, int threads, unsigne
 int main()
 {
     int bad = 0;
-    bad |= check(10000, 40, 64, 1024, 4, 1u);
-    bad |= check(10000, 40, 64, 60, 3, 2u);          // small cap: tiles close early
-    bad |= check(5000, 200, 128, 150, 2, 3u);        // rows longer than the cap: tiles off
-    bad |= check(1, 1, 64, 1024, 1, 4u);             // a single row without entries
-    bad |= check(70000, 12, 128, 1536, 8, 5u);       // several chunks of 4096 rows
+    bad |= check(10000, 40, 288, 1024, 4, 1u);
+    bad |= check(10000, 40, 288, 60, 3, 2u);         // small cap: tiles close early
+    bad |= check(5000, 200, 288, 150, 2, 3u);        // rows longer than the cap: tiles off
+    bad |= check(1, 1, 288, 1024, 1, 4u);            // a single row without entries
+    bad |= check(70000, 12, 256, 1536, 8, 5u);       // many tiles, short rows
+    bad |= check(3000, 120, 64, 4096, 2, 6u);        // long rows, few lanes
     if (!bad) std::printf("ok\n");
     return bad;
 }
