@@ -314,7 +314,7 @@ def main():
         traffic = pair_traffic_from_profile()
         roofline = {"bound": "fp32", "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
                     "frac": achieved / peak.value, "traffic": traffic,
-                    "kernel": "k_tp0_pairs (near + far launches)",
+                    "kernel": "k_tp0_pairs_tiled (near + far launches)",
                     "peak_source": "measured FP32 FMA throughput (rpb_measure_fp32_peak); MEASURED_PEAKS.json "
                                    "has no FP32 figure",
                     "flops_per_evaluation": flops,

@@ -446,7 +446,8 @@ constexpr int pair_blocks(int rows, int lanes) { return (rows * lanes + PAIR_BLO
 // rows per tile the host aims below, and the largest column union a tile may stage. The
 // host sizes the tiles so that their count is a whole number of waves of resident blocks.
 constexpr int PAIR_TILE_THREADS = 288;
-constexpr int TILE_ROWS = 144;
+constexpr int NEAR_TILE_ROWS = 288;
+constexpr int FAR_TILE_ROWS = 144;
 constexpr int NEAR_TILE_UNION = 1024;
 constexpr int FAR_TILE_UNION = 1536;
 

@@ -436,7 +436,7 @@ rpb_status rpb_mesh_create(int dom_dim, int amb_dim, const double* Vh, int64_t n
         // shared-memory row tiles; the kernels' grids are then one block per tile
         // Tiles are balanced by entries and their count is a whole number of waves of
         // resident blocks (no partial last wave, whose few blocks would run while the
-        // other SMs idle); about TILE_ROWS rows per tile.
+        // other SMs idle); at most NEAR_TILE_ROWS / FAR_TILE_ROWS rows per tile on average.
         int sms = 0;
         if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, m->device) != cudaSuccess) sms = 0;
         auto tile = [&](const SymPattern& P, int ncols, bool far, const void* kernel, int cap, TileBufs& d, int& blocks) {
@@ -455,7 +455,8 @@ rpb_status rpb_mesh_create(int dom_dim, int amb_dim, const double* Vh, int64_t n
             RowTiles R;
             for (int pass = 0; pass < 3 && per_sm > 0; ++pass) {
                 const int64_t slots = static_cast<int64_t>(per_sm) * sms;
-                const int64_t waves = std::max<int64_t>(1, (P.rows + slots * TILE_ROWS - 1) / (slots * TILE_ROWS));
+                const int64_t tile_rows = far ? FAR_TILE_ROWS : NEAR_TILE_ROWS;
+                const int64_t waves = std::max<int64_t>(1, (P.rows + slots * tile_rows - 1) / (slots * tile_rows));
                 const int64_t target = (P.nnz() + waves * slots - 1) / (waves * slots);
                 build_row_tiles(P.rp.data(), P.ci.data(), P.rows, ncols, PAIR_TILE_THREADS, target, cap,
                                 std::max(1, m->settings.threads), R);
