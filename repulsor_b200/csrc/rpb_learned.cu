@@ -59,7 +59,18 @@ constexpr int OFF_W3 = OFF_B2 + NH;           // NO x NH
 constexpr int OFF_B3 = OFF_W3 + NO * NH;      // NO
 constexpr int NPARAM = OFF_B3 + NO;           // 5443
 
-__device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f)); }
+// GELU x Phi(x), Phi from the complementary error function of Abramowitz & Stegun 7.1.26
+// (absolute error <= 1.5e-7): Phi(-|x|) = 0.5 t P(t) exp(-x^2 / 2), t = 1 / (1 + p |x| / sqrt 2).
+// Two MUFU operations (reciprocal, exponential); the activations are rounded to BF16 next.
+__device__ __forceinline__ float gelu(float x)
+{
+    const float z = fabsf(x) * 0.70710678118654752f;
+    const float t = __fdividef(1.0f, fmaf(0.3275911f, z, 1.0f));
+    const float poly =
+        t * fmaf(t, fmaf(t, fmaf(t, fmaf(t, 1.061405429f, -1.453152027f), 1.421413741f), -0.284496736f), 0.254829592f);
+    const float h = 0.5f * poly * __expf(-z * z);
+    return x * (x < 0.0f ? h : 1.0f - h);
+}
 __device__ __forceinline__ float gelu_grad(float x)
 {
     return 0.5f * (1.0f + erff(x * 0.70710678118654752f)) + x * 0.39894228040143268f * expf(-0.5f * x * x);
@@ -460,8 +471,9 @@ struct ClusterMlpArgs {
     const double* blocks;
     const double* scale;
     double* c;                // NC x 3: coefficients
-    double* csum_part;        // gridDim.x x 3: partial sums of A_C c_C
-    unsigned* done;           // last-block counter (zero between launches)
+    const float* Fs;          // NC x NFS: the geometric features 3..11 (k_static_features)
+    double* csum_part;        // units x 3: partial sums of A_C c_C per 32-cluster unit
+    unsigned* done;           // [0] last-block counter, [1] unit counter (zero between launches)
     double* zmean;            // 3: sum_C A_C c_C / n_v = mean of z before its removal
     // training only (may be null)
     float* F;                 // NC x NF
@@ -489,103 +501,138 @@ __device__ __forceinline__ void cluster_moment(const ClusterMlpArgs& A, int C, d
     for (int q = 0; q < 3; ++q) R[q] = se[q] - sb[q];
 }
 
-__global__ void __launch_bounds__(GAIN_BLOCK) k_cluster_mlp(ClusterMlpArgs A)
+// Geometric features of the clusters (3..11 of the 16), once per geometry: centre
+// relative to the root over the root diameter, averaged normal, log area ratio, log
+// diameter ratio, depth.
+constexpr int NFS = 9;
+__global__ void k_static_features(int NC, int max_depth, const ClusterDatum* C_pair, const double* C_an,
+                                  const float* C_diam, const int* C_depth, float* Fs)
+{
+    const int C = blockIdx.x * blockDim.x + threadIdx.x;
+    if (C >= NC) return;
+    const ClusterDatum cd = load_datum(C_pair, C);
+    const ClusterDatum root = load_datum(C_pair, 0);
+    const double dr = fmax(static_cast<double>(C_diam[0]), 1e-300);
+    float* f = Fs + NFS * static_cast<int64_t>(C);
+    for (int k = 0; k < 3; ++k) f[k] = static_cast<float>((cd.c[k] - root.c[k]) / dr);
+    for (int k = 0; k < 3; ++k) f[3 + k] = static_cast<float>(C_an[3 * static_cast<int64_t>(C) + k] / cd.a);
+    f[6] = static_cast<float>(log(cd.a / root.a) / 10.0);
+    f[7] = static_cast<float>(log(fmax(static_cast<double>(C_diam[C]), 1e-300) / dr) / 10.0);
+    f[8] = static_cast<float>(C_depth[C]) / static_cast<float>(max(max_depth, 1));
+}
+
+// Persistent: every block stages the weights once, then each of its warps takes units of
+// 32 clusters from a global counter (lane = cluster) until none are left: features, the
+// MLP on the warp's own 32 rows of the shared tile, gains and coefficients. Per-unit
+// partial sums of A_C c_C are added by the last block in unit order (deterministic
+// whatever warp took which unit); it also resets both counters.
+__global__ void __launch_bounds__(GAIN_BLOCK, 4) k_cluster_mlp(ClusterMlpArgs A)
 {
     static_assert(GAIN_BLOCK == MLP_TILE, "one MLP tile per block");
     __shared__ MlpSmem sm;
-    stage_mlp_weights(A.w, sm);
-    const int row0 = blockIdx.x * GAIN_BLOCK;
-    const int C = row0 + threadIdx.x;
-    double cs[3] = {0, 0, 0};
-    float f[NF];
-    for (int k = 0; k < NF; ++k) f[k] = 0.0f;
-    double R[3] = {0, 0, 0};
-    ClusterDatum cd{};
-    if (C < A.NC) {
-        const double s = fmax(*A.scale, 1e-300);
-        cd = load_datum(A.C_pair, C);
-        const ClusterDatum root = load_datum(A.C_pair, 0);
-        const double dr = fmax(static_cast<double>(A.C_diam[0]), 1e-300);
-        cluster_moment(A, C, R);
-        for (int k = 0; k < 3; ++k) f[k] = static_cast<float>(R[k] / (cd.a * s));
-        for (int k = 0; k < 3; ++k) f[3 + k] = static_cast<float>((cd.c[k] - root.c[k]) / dr);
-        for (int k = 0; k < 3; ++k) f[6 + k] = static_cast<float>(A.C_an[3 * static_cast<int64_t>(C) + k] / cd.a);
-        f[9] = static_cast<float>(log(cd.a / root.a) / 10.0);
-        f[10] = static_cast<float>(log(fmax(static_cast<double>(A.C_diam[C]), 1e-300) / dr) / 10.0);
-        f[11] = static_cast<float>(A.C_depth[C]) / static_cast<float>(max(A.max_depth, 1));
-        for (int k = 12; k < 16; ++k) f[k] = 0.0f;
-        const int L = A.C_left[C], Rr = A.C_right[C];
-        if (L >= 0) {
-            const double aL = load_datum(A.C_pair, L).a, aR = load_datum(A.C_pair, Rr).a;
-            double q[3];
-            cluster_moment(A, L, q);
-            f[12] = static_cast<float>(sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2]) / (aL * s));
-            cluster_moment(A, Rr, q);
-            f[13] = static_cast<float>(sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2]) / (aR * s));
-            // children of L together span L: R_LL + R_LR = R_L (as in the reference tree, a
-            // cluster is the union of its children); the grandchildren feature uses them
-            if (A.C_left[L] >= 0) {
-                double a[3], b[3];
-                cluster_moment(A, A.C_left[L], a);
-                cluster_moment(A, A.C_right[L], b);
-                f[14] = static_cast<float>(sqrt((a[0] + b[0]) * (a[0] + b[0]) + (a[1] + b[1]) * (a[1] + b[1]) +
-                                                (a[2] + b[2]) * (a[2] + b[2])) / (aL * s));
-            }
-            if (A.C_left[Rr] >= 0) {
-                double a[3], b[3];
-                cluster_moment(A, A.C_left[Rr], a);
-                cluster_moment(A, A.C_right[Rr], b);
-                f[15] = static_cast<float>(sqrt((a[0] + b[0]) * (a[0] + b[0]) + (a[1] + b[1]) * (a[1] + b[1]) +
-                                                (a[2] + b[2]) * (a[2] + b[2])) / (aR * s));
-            }
-        }
-    }
-    for (int k = 0; k < NF; ++k) sm.F[threadIdx.x * SF_LD + k] = __float2bfloat16_rn(f[k]);
-    __syncthreads();
-    mlp_tile(sm, row0, A.NC, A.pre1, A.pre2);
-    __syncthreads();
-    if (C < A.NC) {
-        float o[NO];
-        for (int q = 0; q < NO; ++q) o[q] = sm.O[threadIdx.x * 4 + q];
-        const double inv_a = 1.0 / cd.a;
-        for (int q = 0; q < 3; ++q) {
-            const float oc = fminf(fmaxf(o[q], -GAIN_CLAMP), GAIN_CLAMP);
-            const double cq = exp(static_cast<double>(oc)) * R[q] * inv_a;
-            A.c[3 * static_cast<int64_t>(C) + q] = cq;
-            cs[q] = cd.a * cq;
-        }
-        if (A.F)
-            for (int k = 0; k < NF; ++k) A.F[NF * static_cast<int64_t>(C) + k] = f[k];
-        if (A.O)
-            for (int q = 0; q < NO; ++q) A.O[NO * static_cast<int64_t>(C) + q] = o[q];
-        if (A.Rc)
-            for (int q = 0; q < 3; ++q) A.Rc[3 * static_cast<int64_t>(C) + q] = R[q];
-    }
-    // sum_C A_C c_C: block partials, the last block adds them in block order
-    __shared__ double sh[GAIN_BLOCK / 32][3];
     __shared__ bool last;
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    for (int q = 0; q < 3; ++q) {
-        const double v = warp_sum_f64(cs[q]);
-        if (lane == 0) sh[wib][q] = v;
+    stage_mlp_weights(A.w, sm);
+    __syncthreads();
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int units = (A.NC + 31) / 32;
+    const double s = fmax(*A.scale, 1e-300);
+    for (;;) {
+        int u = 0;
+        if (lane == 0) u = static_cast<int>(atomicAdd(A.done + 1, 1u));
+        u = __shfl_sync(0xffffffffu, u, 0);
+        if (u >= units) break;
+        const int C = 32 * u + lane;
+        double cs[3] = {0, 0, 0};
+        float f[NF];
+        for (int k = 0; k < NF; ++k) f[k] = 0.0f;
+        double R[3] = {0, 0, 0};
+        double ca = 1.0;
+        if (C < A.NC) {
+            ca = __ldg(&A.C_pair[C].a);
+            cluster_moment(A, C, R);
+            for (int k = 0; k < 3; ++k) f[k] = static_cast<float>(R[k] / (ca * s));
+            const float* fs = A.Fs + NFS * static_cast<int64_t>(C);
+            for (int k = 0; k < NFS; ++k) f[3 + k] = __ldg(fs + k);
+            const int L = A.C_left[C], Rr = A.C_right[C];
+            if (L >= 0) {
+                const double aL = __ldg(&A.C_pair[L].a), aR = __ldg(&A.C_pair[Rr].a);
+                double q[3];
+                cluster_moment(A, L, q);
+                f[12] = static_cast<float>(sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2]) / (aL * s));
+                cluster_moment(A, Rr, q);
+                f[13] = static_cast<float>(sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2]) / (aR * s));
+                // children of L together span L: R_LL + R_LR = R_L (as in the reference tree, a
+                // cluster is the union of its children); the grandchildren feature uses them
+                if (A.C_left[L] >= 0) {
+                    double a[3], b[3];
+                    cluster_moment(A, A.C_left[L], a);
+                    cluster_moment(A, A.C_right[L], b);
+                    f[14] = static_cast<float>(sqrt((a[0] + b[0]) * (a[0] + b[0]) + (a[1] + b[1]) * (a[1] + b[1]) +
+                                                    (a[2] + b[2]) * (a[2] + b[2])) / (aL * s));
+                }
+                if (A.C_left[Rr] >= 0) {
+                    double a[3], b[3];
+                    cluster_moment(A, A.C_left[Rr], a);
+                    cluster_moment(A, A.C_right[Rr], b);
+                    f[15] = static_cast<float>(sqrt((a[0] + b[0]) * (a[0] + b[0]) + (a[1] + b[1]) * (a[1] + b[1]) +
+                                                    (a[2] + b[2]) * (a[2] + b[2])) / (aR * s));
+                }
+            }
+        }
+        const int row = 32 * w + lane;
+        for (int k = 0; k < NF; ++k) sm.F[row * SF_LD + k] = __float2bfloat16_rn(f[k]);
+        __syncwarp();
+        mlp_tile(sm, 32 * u - 32 * w, A.NC, A.pre1, A.pre2);
+        if (C < A.NC) {
+            float o[NO];
+            for (int q = 0; q < NO; ++q) o[q] = sm.O[row * 4 + q];
+            const double inv_a = 1.0 / ca;
+            for (int q = 0; q < 3; ++q) {
+                const float oc = fminf(fmaxf(o[q], -GAIN_CLAMP), GAIN_CLAMP);
+                const double cq = exp(static_cast<double>(oc)) * R[q] * inv_a;
+                A.c[3 * static_cast<int64_t>(C) + q] = cq;
+                cs[q] = ca * cq;
+            }
+            if (A.F)
+                for (int k = 0; k < NF; ++k) A.F[NF * static_cast<int64_t>(C) + k] = f[k];
+            if (A.O)
+                for (int q = 0; q < NO; ++q) A.O[NO * static_cast<int64_t>(C) + q] = o[q];
+            if (A.Rc)
+                for (int q = 0; q < 3; ++q) A.Rc[3 * static_cast<int64_t>(C) + q] = R[q];
+        }
+        for (int q = 0; q < 3; ++q) {
+            const double v = warp_sum_f64(cs[q]);
+            if (lane == 0) A.csum_part[3 * static_cast<int64_t>(u) + q] = v;
+        }
+        __syncwarp();
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        for (int q = 0; q < 3; ++q) {
-            double t = 0;
-            for (int w = 0; w < GAIN_BLOCK / 32; ++w) t += sh[w][q];
-            A.csum_part[3 * static_cast<int64_t>(blockIdx.x) + q] = t;
-        }
         __threadfence();
         last = (atomicAdd(A.done, 1u) == gridDim.x - 1);
     }
     __syncthreads();
-    if (last && threadIdx.x < 3) {
+    if (last) {
         __threadfence();
-        double t = 0;
-        for (int b = 0; b < static_cast<int>(gridDim.x); ++b) t += __ldcg(A.csum_part + 3 * static_cast<int64_t>(b) + threadIdx.x);
-        A.zmean[threadIdx.x] = t / A.nV;
-        if (threadIdx.x == 0) *A.done = 0u;
+        // thread t adds units t, t + GAIN_BLOCK, ... ; then a fixed tree over the threads
+        double t3[3] = {0, 0, 0};
+        for (int v = threadIdx.x; v < units; v += GAIN_BLOCK)
+            for (int q = 0; q < 3; ++q) t3[q] += __ldcg(A.csum_part + 3 * static_cast<int64_t>(v) + q);
+        __shared__ double sh[GAIN_BLOCK / 32][3];
+        for (int q = 0; q < 3; ++q) {
+            const double v = warp_sum_f64(t3[q]);
+            if (lane == 0) sh[w][q] = v;
+        }
+        __syncthreads();
+        if (threadIdx.x < 3) {
+            double t = 0;
+            for (int k = 0; k < GAIN_BLOCK / 32; ++k) t += sh[k][threadIdx.x];
+            A.zmean[threadIdx.x] = t / A.nV;
+        }
+        if (threadIdx.x == 0) {
+            A.done[0] = 0u;
+            A.done[1] = 0u;
+        }
     }
 }
 
@@ -737,6 +784,8 @@ struct LearnedState {
     DevBuf<unsigned> done;
     DevBuf<float> F, O, dO, pre1, pre2, d1, d2, C_diam;
     DevBuf<int> C_depth;
+    DevBuf<float> Fs;         // NC x NFS geometric features
+    int mlp_grid = 0;         // resident blocks of k_cluster_mlp on the device
 };
 
 static rpb_status range_sums3(rpb_mesh* m, const double* prim3, double* out3)
@@ -764,9 +813,14 @@ static rpb_status ensure_learned(rpb_mesh* m)
         RPB_CUDA(L.local.alloc(3 * N));
         RPB_CUDA(L.blocks.alloc(3 * (nb + 1)));
         RPB_CUDA(L.sq_part.alloc(nb));
-        RPB_CUDA(L.csum_part.alloc(3 * ((NC + GAIN_BLOCK - 1) / GAIN_BLOCK)));
+        RPB_CUDA(L.csum_part.alloc(3 * ((NC + 31) / 32)));
         RPB_CUDA(L.zmean.alloc(3));
-        RPB_CUDA(L.done.alloc(1));
+        RPB_CUDA(L.done.alloc(2));
+        RPB_CUDA(L.Fs.alloc(NFS * NC));
+        int per_sm = 0, sms = 0;
+        RPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cluster_mlp, GAIN_BLOCK, 0));
+        RPB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, m->device));
+        L.mlp_grid = std::max(1, per_sm * sms);
         RPB_CUDA(cudaMemsetAsync(L.done.ptr, 0, L.done.bytes(), m->stream));
         RPB_CUDA(L.scale.alloc(1));
         RPB_CUDA(L.sums.alloc(4));
@@ -795,6 +849,9 @@ static rpb_status ensure_learned(rpb_mesh* m)
         k_prim_an<<<(m->N + 255) / 256, 256, 0, m->stream>>>(m->N, m->P_pair.ptr, L.tmp3.ptr);
         rpb_status st = range_sums3(m, L.tmp3.ptr, L.C_an.ptr);
         if (st != RPB_OK) return st;
+        k_static_features<<<(m->NC + 255) / 256, 256, 0, m->stream>>>(m->NC, L.max_depth, m->C_pair.ptr, L.C_an.ptr,
+                                                                      L.C_diam.ptr, L.C_depth.ptr, L.Fs.ptr);
+        RPB_CUDA(cudaGetLastError());
         L.geometry_version = m->geometry_version;
     }
     return RPB_OK;
@@ -855,12 +912,13 @@ static rpb_status learned_forward(rpb_mesh* m, rpb_mlp* mlp, const double* R, do
     ca.C_depth = L.C_depth.ptr; ca.C_diam = L.C_diam.ptr;
     ca.local = L.local.ptr; ca.blocks = L.blocks.ptr; ca.scale = L.scale.ptr;
     ca.c = L.c.ptr; ca.csum_part = L.csum_part.ptr; ca.done = L.done.ptr; ca.zmean = L.zmean.ptr;
+    ca.Fs = L.Fs.ptr;
     ca.F = training ? L.F.ptr : nullptr;
     ca.O = training ? L.O.ptr : nullptr;
     ca.pre1 = training ? L.pre1.ptr : nullptr;
     ca.pre2 = training ? L.pre2.ptr : nullptr;
     ca.Rc = training ? L.Rc.ptr : nullptr;
-    k_cluster_mlp<<<(m->NC + GAIN_BLOCK - 1) / GAIN_BLOCK, GAIN_BLOCK, 0, s>>>(ca);
+    k_cluster_mlp<<<std::min(L.mlp_grid, (m->NC + GAIN_BLOCK - 1) / GAIN_BLOCK), GAIN_BLOCK, 0, s>>>(ca);
     k_prim_expand<<<(m->N + 255) / 256, 256, 0, s>>>(m->N, m->leaf_of.ptr, m->C_parent.ptr, L.c.ptr, L.tmp3.ptr);
     k_vertex_expand<<<(m->nV + 255) / 256, 256, 0, s>>>(m->nV, m->size, m->vp_rp.ptr, m->vp_slot.ptr, m->pre_vals.ptr,
                                                         L.tmp3.ptr, L.zmean.ptr, z);

@@ -246,6 +246,62 @@ __device__ __forceinline__ void spmm_finish(const double (&acc)[BD], int sub, bo
     }
 }
 
+// BD = 12: six lanes per row (five rows per warp, two lanes idle); lane s owns outputs
+// 2s, 2s+1 and reads the 16-byte piece s of every column row, so one load instruction
+// covers five whole 96-byte input rows. Each lane walks all of the row's blocks, four at a
+// time with the loads issued first; no cross-lane combination.
+constexpr int SPMM6_ROWS_PER_WARP = 5;
+__global__ void __launch_bounds__(256) k_block_spmm12_rows6(SpmmArgs<12> A)
+{
+    const int lane = threadIdx.x & 31, grp = lane / 6, sub = lane - 6 * grp;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int row = warp * SPMM6_ROWS_PER_WARP + grp;
+    if (grp >= SPMM6_ROWS_PER_WARP || row >= A.rows0 + A.rows1) return;
+    const bool first = row < A.rows0;
+    const int i = first ? row : row - A.rows0;
+    const double2* x = reinterpret_cast<const double2*>(first ? A.x0 : A.x1) + sub;
+    const int64_t* rp = first ? A.rp0 : A.rp1;
+    const int* ci = first ? A.ci0 : A.ci1;
+    const float2* vals = first ? A.v0 : A.v1;
+    const bool lo_x = 2 * sub < 3, hi_x = 2 * sub + 1 < 3;
+    double acc0 = 0.0, acc1 = 0.0;
+    const int64_t k1 = rp[i + 1];
+    int64_t k = rp[i];
+    for (; k + 4 <= k1; k += 4) {
+        int j[4];
+        float2 a[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            j[q] = __ldg(ci + k + q);
+            a[q] = __ldg(vals + k + q);
+        }
+        double2 t[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) t[q] = __ldg(x + 6 * static_cast<int64_t>(j[q]));
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            acc0 += static_cast<double>(lo_x ? a[q].x : a[q].y) * t[q].x;
+            acc1 += static_cast<double>(hi_x ? a[q].x : a[q].y) * t[q].y;
+        }
+    }
+    for (; k < k1; ++k) {
+        const int j = __ldg(ci + k);
+        const float2 a = __ldg(vals + k);
+        const double2 t = __ldg(x + 6 * static_cast<int64_t>(j));
+        acc0 += static_cast<double>(lo_x ? a.x : a.y) * t.x;
+        acc1 += static_cast<double>(hi_x ? a.x : a.y) * t.y;
+    }
+    const double2 dg = (first ? A.d0 : A.d1)[i];
+    const double2 xi = x[6 * static_cast<int64_t>(i)];
+    double* y = (first ? A.y0 : A.y1) + 12 * static_cast<int64_t>(i) + 2 * sub;
+    const double v0 = acc0 + (lo_x ? dg.x : dg.y) * xi.x, v1 = acc1 + (hi_x ? dg.x : dg.y) * xi.y;
+    if (A.accumulate) {
+        y[0] += v0; y[1] += v1;
+    } else {
+        y[0] = v0; y[1] = v1;
+    }
+}
+
 template <int BD>
 __global__ void __launch_bounds__(256) k_block_spmm(SpmmArgs<BD> A)
 {
@@ -536,7 +592,11 @@ static rpb_status apply_operator(rpb_mesh* m, const float2* nf, const double2* n
         sa.rp1 = m->far.rp.ptr; sa.ci1 = m->far.ci.ptr; sa.v1 = ff; sa.d1 = ffd;
         sa.x1 = m->buf_Cin64.ptr; sa.y1 = m->buf_Cout.ptr;
         sa.accumulate = false;
-        k_block_spmm<BD><<<((sa.rows0 + sa.rows1) * SPMM_LANES + 255) / 256, 256, 0, s>>>(sa);
+        if constexpr (BD == 12) {
+            const int warps = (sa.rows0 + sa.rows1 + SPMM6_ROWS_PER_WARP - 1) / SPMM6_ROWS_PER_WARP;
+            k_block_spmm12_rows6<<<(warps + 7) / 8, 256, 0, s>>>(sa);
+        } else
+            k_block_spmm<BD><<<((sa.rows0 + sa.rows1) * SPMM_LANES + 255) / 256, 256, 0, s>>>(sa);
         RPB_CUDA(cudaGetLastError());
     }
     if (VF) {

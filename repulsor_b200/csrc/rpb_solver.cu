@@ -261,14 +261,26 @@ __global__ void __launch_bounds__(256) k_dot3(DotArgs A)
         last = (atomicAdd(A.done, 1u) == gridDim.x - 1);
     }
     __syncthreads();
-    if (last && threadIdx.x < 6) {
+    if (last) {
+        // every thread adds the partials of blocks t, t + blockDim.x, ..., then a fixed
+        // tree over warps: deterministic, and no serial chain over the blocks
         __threadfence();
-        double v = 0;
-        for (int b = 0; b < static_cast<int>(gridDim.x); ++b) v += __ldcg(A.partials + 6 * b + threadIdx.x);
-        if (threadIdx.x < 3) A.out0[threadIdx.x] = v;
-        else if (A.out1) A.out1[threadIdx.x - 3] = v;
+        double v[6] = {0, 0, 0, 0, 0, 0};
+        for (int b = threadIdx.x; b < static_cast<int>(gridDim.x); b += blockDim.x)
+            for (int k = 0; k < 6; ++k) v[k] += __ldcg(A.partials + 6 * b + k);
+        for (int k = 0; k < 6; ++k) {
+            const double t = warp_sum_f64(v[k]);
+            if (lane == 0) sh[w][k] = t;
+        }
+        __syncthreads();
+        if (threadIdx.x < 6) {
+            double t = 0;
+            for (int q = 0; q < (blockDim.x >> 5); ++q) t += sh[q][threadIdx.x];
+            if (threadIdx.x < 3) A.out0[threadIdx.x] = t;
+            else if (A.out1) A.out1[threadIdx.x - 3] = t;
+        }
+        if (threadIdx.x == 0) *A.done = 0u;
     }
-    if (last && threadIdx.x == 0) *A.done = 0u;
 }
 
 // x += alpha p, r -= alpha Ap with alpha = rz / (p, Ap) per active column
