@@ -191,6 +191,32 @@ rpb_status rpb_tpm0_solve_info(const rpb_mesh* m, rpb_solve_info* info);
  * device double `energy_dev` asynchronously on the mesh stream (graph-capturable). */
 rpb_status rpb_tpe0_energy_device(rpb_mesh* m, double* energy_dev);
 
+/* --- row sharding of one evaluation over several GPUs ------------------------------------- */
+/* The reference splits the rows of the Near() and Far() lists over host threads by nonzero
+ * count and adds the per-thread derivative slices (src/FMM/FMM_Traversor.hpp:56-147,
+ * src/ClusterTree.hpp:1115-1208). Here each of `shards` processes (one per GPU, the same
+ * mesh at the same coordinates on every one) evaluates a contiguous range of row tiles,
+ * the partial buffers are summed across processes (one all-reduce, e.g. NCCL), and every
+ * process applies the chain rule to the sum.
+ *
+ * rpb_mesh_set_shards regroups the row tiles so that every shard owns whole waves of
+ * resident blocks (synchronizes the mesh stream; call before any capture). */
+rpb_status rpb_mesh_set_shards(rpb_mesh* m, int shards);
+/* Rows [near_rows[0], near_rows[1]) of Near() and [far_rows[0], far_rows[1]) of Far() (tree
+ * order) that shard `shard` evaluates. */
+rpb_status rpb_mesh_shard_rows(const rpb_mesh* m, int shard, int64_t near_rows[2], int64_t far_rows[2]);
+/* Number of doubles of a shard buffer: 10 N (near moment derivatives) + 10 N_C (far) + 1
+ * (energy part). */
+rpb_status rpb_mesh_shard_buffer_doubles(const rpb_mesh* m, int64_t* doubles);
+/* Pair kernels of shard `shard` on the mesh stream into the device buffer `buf`: the
+ * centred moment derivatives of the shard's rows (zero elsewhere) and its energy part.
+ * Meshes with very-near pairs are rejected. */
+rpb_status rpb_tpe0_pairs_shard(rpb_mesh* m, double q, double p, int shard, double* buf);
+/* Collection, chain rule and vertex gather from the sum of all shards' buffers:
+ * Y_dev = alpha dE + beta Y_dev (n_v x ldY, device); the energy is buf[10 N + 10 N_C]. */
+rpb_status rpb_tpe0_collect_shards(rpb_mesh* m, const double* buf, double alpha, double beta, double* Y_dev,
+                                   int ldY);
+
 /* EnergyBase::SimplexDensities / VertexDensities (src/Energies/EnergyBase.hpp:129-150):
  * energy densities per simplex (original order, n_s values) or per vertex (n_v values; the
  * simplex densities averaged with the weights a_i/(n+1) and divided by the dual volume);

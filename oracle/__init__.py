@@ -52,6 +52,10 @@ def _load():
     lib.oracle_differential.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                         ctypes.c_double, _dp, ctypes.c_int]
     lib.oracle_moment_derivatives.argtypes = [ctypes.c_void_p, _dp, _dp]
+    lib.oracle_partial_derivatives.restype = ctypes.c_double
+    lib.oracle_partial_derivatives.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                               ctypes.c_int, _dp, _dp]
+    lib.oracle_collect.argtypes = [ctypes.c_void_p, _dp, _dp, ctypes.c_double, ctypes.c_double, _dp, ctypes.c_int]
     lib.oracle_allpairs_energy.restype = ctypes.c_double
     lib.oracle_allpairs_energy.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double]
     lib.oracle_metric_values.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double, _dp, _dp, _dp, _dp]
@@ -201,6 +205,25 @@ class OracleMesh:
             Y = np.zeros((self.nV, 3))
         en = _load().oracle_differential(self._h, q, p, alpha, beta, _d(Y), Y.shape[1])
         return en, Y
+
+    def partial_derivatives(self, shard, shards, q=6.0, p=12.0):
+        """Shard `shard` of `shards` (upper-triangle rows split like the reference's
+        threads): its near (N x NEAR_DIM) and far (N_C x 10) derivative slices in tree
+        order before collection, and its energy part."""
+        nd = 1 + (self.dom + 1) * 3 + 6
+        Dn = np.zeros((self.nS, nd))
+        Df = np.zeros((self.counts()["clusters"], 10))
+        e = _load().oracle_partial_derivatives(self._h, q, p, shard, shards, _d(Dn), _d(Df))
+        return Dn, Df, e
+
+    def collect(self, Dn, Df, alpha=1.0, beta=0.0, Y=None):
+        """Y = alpha dE + beta Y from summed derivative slices (collection, chain rule,
+        vertex scatter)."""
+        Y = np.zeros((self.nV, 3)) if Y is None else Y
+        Dn = np.ascontiguousarray(Dn, dtype=np.float64)
+        Df = np.ascontiguousarray(Df, dtype=np.float64)
+        _load().oracle_collect(self._h, _d(Dn), _d(Df), alpha, beta, _d(Y), Y.shape[1])
+        return Y
 
     def moment_derivatives(self):
         nd = 1 + (self.dom + 1) * 3 + 6

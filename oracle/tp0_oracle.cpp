@@ -981,12 +981,17 @@ static void collect_derivatives(Mesh& M, const std::vector<std::vector<double>>&
     }
     }
 
-static double tp0_evaluate(Mesh& M, double q, double p, bool diff)
+// Full evaluation (only < 0), or the slice of one "thread" of `shards` (only >= 0): the
+// upper-triangle rows job_pointer(only)..job_pointer(only + 1) of every list, the way the
+// reference splits rows over threads (src/FMM/FMM_Traversor.hpp:65-101); the slice's
+// derivatives are left in tDn_out / tDf_out (tree order) instead of being collected.
+static double tp0_evaluate(Mesh& M, double q, double p, bool diff, int shards = 0, int only = -1,
+                           std::vector<double>* tDn_out = nullptr, std::vector<double>* tDf_out = nullptr)
 {
     const TPParams T(q, p, M.dom);
     const int nd = near_dim(M.dom);
     const int SIZE = M.SIZE;
-    const int threads = std::max(1, M.set.threads);
+    const int threads = shards > 0 ? shards : std::max(1, M.set.threads);
     const double S_scale = 1.0 / SIZE;
 
     std::vector<std::vector<double>> tDn, tDf;   // thread_P_D_near, thread_C_D_far
@@ -1002,6 +1007,7 @@ static double tp0_evaluate(Mesh& M, double q, double p, bool diff)
         std::vector<double> part(threads, 0.0);
         auto jp = upper_job_ptr(Pt, threads);
         parallel_do(threads, [&](int t) {
+            if (only >= 0 && t != only) return;
             double local = 0;
             for (Int i = jp[t]; i < jp[t + 1]; ++i)
                 for (LInt k = Pt.diag[i]; k < Pt.rp[i + 1]; ++k) {
@@ -1043,6 +1049,7 @@ static double tp0_evaluate(Mesh& M, double q, double p, bool diff)
         std::vector<double> part(threads, 0.0);
         auto jp = upper_job_ptr(Pt, threads);
         parallel_do(threads, [&](int t) {
+            if (only >= 0 && t != only) return;
             double local = 0;
             for (Int i = jp[t]; i < jp[t + 1]; ++i) {
                 if (Pt.rp[i + 1] <= Pt.diag[i]) continue;
@@ -1095,6 +1102,7 @@ static double tp0_evaluate(Mesh& M, double q, double p, bool diff)
         std::vector<double> part(threads, 0.0);
         auto jp = upper_job_ptr(Pt, threads);
         parallel_do(threads, [&](int t) {
+            if (only >= 0 && t != only) return;
             double local = 0;
             for (Int i = jp[t]; i < jp[t + 1]; ++i) {
                 if (Pt.rp[i + 1] <= Pt.diag[i]) continue;
@@ -1121,7 +1129,12 @@ static double tp0_evaluate(Mesh& M, double q, double p, bool diff)
         for (double v : part) en += v;
     }
 
-    if (diff) collect_derivatives(M, tDn, tDf, threads, nd);
+    if (diff && only >= 0) {
+        if (tDn_out) *tDn_out = tDn[only];
+        if (tDf_out) *tDf_out = tDf[only];
+    } else if (diff) {
+        collect_derivatives(M, tDn, tDf, threads, nd);
+    }
     return en;
 }
 
@@ -2017,6 +2030,31 @@ double oracle_differential(void* h, double q, double p, double alpha, double bet
     const double en = tp0_evaluate(M, q, p, true);
     assemble_derivatives(M, alpha, beta, Y, ldY);
     return en;
+}
+
+// One row shard of `shards` (the upper-triangle rows split like the reference's threads):
+// its thread slice of near derivatives (N x NEAR_DIM) and far derivatives (N_C x FAR_DIM),
+// tree order, before collection; returns the shard's energy part.
+double oracle_partial_derivatives(void* h, double q, double p, int shard, int shards, double* D_near, double* D_far)
+{
+    Mesh& M = static_cast<OracleHandle*>(h)->M;
+    std::vector<double> dn, df;
+    const double en = tp0_evaluate(M, q, p, true, shards, shard, &dn, &df);
+    std::memcpy(D_near, dn.data(), sizeof(double) * dn.size());
+    std::memcpy(D_far, df.data(), sizeof(double) * df.size());
+    return en;
+}
+
+// Collection (percolate-down, primitive copy, unpermute), chain rule and vertex scatter
+// from summed slices: Y = alpha dE + beta Y.
+void oracle_collect(void* h, const double* D_near, const double* D_far, double alpha, double beta, double* Y, int ldY)
+{
+    Mesh& M = static_cast<OracleHandle*>(h)->M;
+    const int nd = near_dim(M.dom);
+    std::vector<std::vector<double>> tDn(1, std::vector<double>(D_near, D_near + static_cast<size_t>(M.nS) * nd));
+    std::vector<std::vector<double>> tDf(1, std::vector<double>(D_far, D_far + static_cast<size_t>(M.NC) * FAR_DIM));
+    collect_derivatives(M, tDn, tDf, 1, nd);
+    assemble_derivatives(M, alpha, beta, Y, ldY);
 }
 
 // moment-coordinate derivatives after collection (original order)

@@ -102,6 +102,11 @@ SIGNATURES = {
                                               _vp, _vp]),
     "rpb_tpm0_solve_info": (ctypes.c_int, [_vp, ctypes.POINTER(SolveInfo)]),
     "rpb_tpe0_energy_device": (ctypes.c_int, [_vp, _vp]),
+    "rpb_mesh_set_shards": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "rpb_mesh_shard_rows": (ctypes.c_int, [_vp, ctypes.c_int, _lp, _lp]),
+    "rpb_mesh_shard_buffer_doubles": (ctypes.c_int, [_vp, _lp]),
+    "rpb_tpe0_pairs_shard": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double, ctypes.c_int, _vp]),
+    "rpb_tpe0_collect_shards": (ctypes.c_int, [_vp, _vp, ctypes.c_double, ctypes.c_double, _vp, ctypes.c_int]),
     "rpb_tpe0_simplex_densities": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double, _dp, _dp]),
     "rpb_tpe0_vertex_densities": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double, _dp, _dp]),
     "rpb_mesh_load_obstacle": (ctypes.c_int, [_vp, _vp]),

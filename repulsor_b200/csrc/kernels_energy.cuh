@@ -640,6 +640,7 @@ struct PairTiles {
     const uint16_t* slot;
     const int* order;
     const int* lane_map;      // tiles x PAIR_TILE_THREADS (RowTiles::lane_map)
+    int tile_base;            // block b takes tile tile_base + b (a row shard's first tile)
 };
 
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem)
@@ -673,7 +674,7 @@ __global__ void __launch_bounds__(PAIR_TILE_THREADS, 2) k_tp0_pairs_tiled(PairAr
     using ColDatum = typename std::conditional<FAR, ClusterDatum, PrimTile>::type;
     extern __shared__ float4 tile_smem[];
     const Datum* base = static_cast<const Datum*>(A.data);
-    const int b = blockIdx.x;
+    const int b = T.tile_base + blockIdx.x;
     const int u0 = T.cols_rp[b], un = T.cols_rp[b + 1] - u0;
     float4* sdat = tile_smem;
     int* sid = reinterpret_cast<int*>(reinterpret_cast<char*>(tile_smem) + sizeof(ColDatum) * static_cast<size_t>(un));

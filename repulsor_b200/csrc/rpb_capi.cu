@@ -177,21 +177,100 @@ static rpb_status allow_tile_smem(int device)
     return RPB_OK;
 }
 
-static PairTiles tiles_view(const TileBufs& t)
+// Tiles [first, first + count) of shard `shard` of `shards` (all tiles for shard < 0).
+static void shard_tiles(const TileBufs& t, int shard, int shards, int& first, int& count)
 {
-    return PairTiles{t.row0.ptr, t.cols_rp.ptr, t.cols.ptr, t.slot.ptr, t.order.ptr, t.lane_map.ptr};
+    if (shard < 0) { first = 0; count = t.tiles; return; }
+    first = static_cast<int>(static_cast<int64_t>(t.tiles) * shard / shards);
+    count = static_cast<int>(static_cast<int64_t>(t.tiles) * (shard + 1) / shards) - first;
+}
+
+static PairTiles tiles_view(const TileBufs& t, int first)
+{
+    return PairTiles{t.row0.ptr, t.cols_rp.ptr, t.cols.ptr, t.slot.ptr, t.order.ptr, t.lane_map.ptr, first};
+}
+
+// Shared-memory row tiles of the near and far patterns (one kernel block per tile). Tiles
+// are balanced by entries and their count is shards x a whole number of waves of resident
+// blocks (no partial last wave, whose few blocks would run while the other SMs idle), so
+// that each of `shards` GPUs owns whole waves; at most NEAR_TILE_ROWS / FAR_TILE_ROWS rows
+// per tile on average. A pattern whose rows exceed the union cap keeps the gather kernel.
+// Sets the launch grids and sizes the per-block energy partials.
+static rpb_status build_pair_tiles(rpb_mesh* m, int shards)
+{
+    cudaStream_t s = m->stream;
+    rpb_status st;
+    if ((st = allow_tile_smem(m->device)) != RPB_OK) return st;
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, m->device) != cudaSuccess) sms = 0;
+    auto tile = [&](const SymPattern& P, int ncols, bool far, const void* kernel, int cap, TileBufs& d, int& blocks) {
+        d.valid = false;
+        d.tiles = 0;
+        auto resident = [&](int max_union) {
+            int per_sm = 0;
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, PAIR_TILE_THREADS,
+                                                              pair_tile_smem(max_union, far)) != cudaSuccess)
+                return 0;
+            return per_sm;
+        };
+        if (sms <= 0 || P.nnz() == 0) return RPB_OK;
+        // resident blocks depend on the tiles' largest union and the tile size on the
+        // resident blocks: start from the cap and re-tile while the count changes
+        int per_sm = resident(cap);
+        RowTiles R;
+        for (int pass = 0; pass < 3 && per_sm > 0; ++pass) {
+            const int64_t slots = static_cast<int64_t>(per_sm) * sms * shards;
+            const int64_t tile_rows = far ? FAR_TILE_ROWS : NEAR_TILE_ROWS;
+            const int64_t waves = std::max<int64_t>(1, (P.rows + slots * tile_rows - 1) / (slots * tile_rows));
+            const int64_t target = (P.nnz() + waves * slots - 1) / (waves * slots);
+            build_row_tiles(P.rp.data(), P.ci.data(), P.rows, ncols, PAIR_TILE_THREADS, target, cap,
+                            std::max(1, m->settings.threads), R);
+            if (!R.valid) break;
+            const int now = resident(R.max_union);
+            if (now == per_sm) break;
+            per_sm = now;
+        }
+        if (per_sm <= 0 || !R.valid || R.tiles() == 0) return RPB_OK;
+        rpb_status e;
+        if ((e = upload(d.row0, R.row0.data(), R.row0.size(), s)) != RPB_OK) return e;
+        if ((e = upload(d.cols_rp, R.cols_rp.data(), R.cols_rp.size(), s)) != RPB_OK) return e;
+        if ((e = upload(d.cols, R.cols.data(), R.cols.size(), s)) != RPB_OK) return e;
+        if ((e = upload(d.order, R.order.data(), R.order.size(), s)) != RPB_OK) return e;
+        if ((e = upload(d.slot, R.slot.data(), R.slot.size(), s)) != RPB_OK) return e;
+        if ((e = upload(d.lane_map, R.lane_map.data(), R.lane_map.size(), s)) != RPB_OK) return e;
+        d.row0_host = R.row0;
+        d.tiles = R.tiles();
+        d.max_union = R.max_union;
+        d.valid = true;
+        blocks = d.tiles;
+        return RPB_OK;
+    };
+    m->near_blocks = pair_blocks(m->N, NEAR_LANES);
+    m->far_blocks = pair_blocks(m->NC, FAR_LANES);
+    const void* kn = reinterpret_cast<const void*>(k_tp0_pairs_tiled<false, 3, 6, true>);
+    const void* kf = reinterpret_cast<const void*>(k_tp0_pairs_tiled<true, 3, 6, true>);
+    if ((st = tile(m->tree.near, m->N, false, kn, NEAR_TILE_UNION, m->near_tiles, m->near_blocks)) != RPB_OK) return st;
+    if ((st = tile(m->tree.far, m->NC, true, kf, FAR_TILE_UNION, m->far_tiles, m->far_blocks)) != RPB_OK) return st;
+    m->shards = shards;
+    if (m->block_energy.alloc(m->near_blocks + m->far_blocks)) {
+        set_error("device allocation failed");
+        return RPB_ENOMEM;
+    }
+    return RPB_OK;
 }
 
 template <int QH, int PH>
-static void launch_pairs_t(rpb_mesh* m, const PairArgs& An, const PairArgs& Af, bool diff, cudaEvent_t between)
+static void launch_pairs_t(rpb_mesh* m, const PairArgs& An, const PairArgs& Af, bool diff, cudaEvent_t between,
+                           int shard)
 {
     if (An.rows > 0) {
         const TileBufs& t = m->near_tiles;
         if (t.valid) {
+            int first, count;
+            shard_tiles(t, shard, m->shards, first, count);
             const size_t smem = pair_tile_smem(t.max_union, false);
-            const int threads = PAIR_TILE_THREADS;
-            if (diff) k_tp0_pairs_tiled<false, QH, PH, true><<<t.tiles, threads, smem, m->stream>>>(An, tiles_view(t));
-            else k_tp0_pairs_tiled<false, QH, PH, false><<<t.tiles, threads, smem, m->stream>>>(An, tiles_view(t));
+            if (diff) k_tp0_pairs_tiled<false, QH, PH, true><<<count, PAIR_TILE_THREADS, smem, m->stream>>>(An, tiles_view(t, first));
+            else k_tp0_pairs_tiled<false, QH, PH, false><<<count, PAIR_TILE_THREADS, smem, m->stream>>>(An, tiles_view(t, first));
         } else if (diff) k_tp0_pairs<false, QH, PH, true, NEAR_LANES><<<m->near_blocks, PAIR_BLOCK, 0, m->stream>>>(An);
         else k_tp0_pairs<false, QH, PH, false, NEAR_LANES><<<m->near_blocks, PAIR_BLOCK, 0, m->stream>>>(An);
     }
@@ -199,16 +278,21 @@ static void launch_pairs_t(rpb_mesh* m, const PairArgs& An, const PairArgs& Af, 
     if (Af.rows > 0) {
         const TileBufs& t = m->far_tiles;
         if (t.valid) {
+            int first, count;
+            shard_tiles(t, shard, m->shards, first, count);
             const size_t smem = pair_tile_smem(t.max_union, true);
-            const int threads = PAIR_TILE_THREADS;
-            if (diff) k_tp0_pairs_tiled<true, QH, PH, true><<<t.tiles, threads, smem, m->stream>>>(Af, tiles_view(t));
-            else k_tp0_pairs_tiled<true, QH, PH, false><<<t.tiles, threads, smem, m->stream>>>(Af, tiles_view(t));
+            if (diff) k_tp0_pairs_tiled<true, QH, PH, true><<<count, PAIR_TILE_THREADS, smem, m->stream>>>(Af, tiles_view(t, first));
+            else k_tp0_pairs_tiled<true, QH, PH, false><<<count, PAIR_TILE_THREADS, smem, m->stream>>>(Af, tiles_view(t, first));
         } else if (diff) k_tp0_pairs<true, QH, PH, true, FAR_LANES><<<m->far_blocks, PAIR_BLOCK, 0, m->stream>>>(Af);
         else k_tp0_pairs<true, QH, PH, false, FAR_LANES><<<m->far_blocks, PAIR_BLOCK, 0, m->stream>>>(Af);
     }
 }
 
-rpb_status launch_pairs(rpb_mesh* m, const TPExp& ex, bool diff, cudaEvent_t between = nullptr)
+// Near- and far-field pair kernels on the mesh stream. shard >= 0: only that row shard's
+// tiles (both patterns tiled), derivatives into D_near / D_far (zeroed first), energies into
+// energy[0..1]; shard < 0: every row, into the mesh's own buffers.
+rpb_status launch_pairs(rpb_mesh* m, const TPExp& ex, bool diff, cudaEvent_t between = nullptr, int shard = -1,
+                        double* D_near = nullptr, double* D_far = nullptr)
 {
     PairArgs An, Af;
     An.col_data = Af.col_data = nullptr;
@@ -225,18 +309,29 @@ rpb_status launch_pairs(rpb_mesh* m, const TPExp& ex, bool diff, cudaEvent_t bet
     Af.order = m->far_order.ptr;
     Af.block_energy = m->block_energy.ptr + m->near_blocks; Af.done = m->done.ptr + 1; Af.energy_out = m->energy.ptr + 1;
 
+    if (shard >= 0) {
+        An.D = D_near;
+        Af.D = D_far;
+        RPB_CUDA(cudaMemsetAsync(D_near, 0, sizeof(double) * 10 * static_cast<size_t>(m->N), m->stream));
+        RPB_CUDA(cudaMemsetAsync(D_far, 0, sizeof(double) * 10 * static_cast<size_t>(m->NC), m->stream));
+        int first, count;
+        shard_tiles(m->near_tiles, shard, m->shards, first, count);
+        if (count == 0) An.rows = 0;
+        shard_tiles(m->far_tiles, shard, m->shards, first, count);
+        if (count == 0) Af.rows = 0;
+    }
     if (An.rows == 0) {
         RPB_CUDA(cudaMemsetAsync(m->energy.ptr, 0, sizeof(double), m->stream));
-        if (diff) RPB_CUDA(cudaMemsetAsync(m->D_near.ptr, 0, m->D_near.bytes(), m->stream));
+        if (diff && shard < 0) RPB_CUDA(cudaMemsetAsync(m->D_near.ptr, 0, m->D_near.bytes(), m->stream));
     }
     if (Af.rows == 0) {
         RPB_CUDA(cudaMemsetAsync(m->energy.ptr + 1, 0, sizeof(double), m->stream));
-        if (diff) RPB_CUDA(cudaMemsetAsync(m->D_far.ptr, 0, m->D_far.bytes(), m->stream));
+        if (diff && shard < 0) RPB_CUDA(cudaMemsetAsync(m->D_far.ptr, 0, m->D_far.bytes(), m->stream));
     }
-    if (ex.qh == 3 && ex.ph == 6) launch_pairs_t<3, 6>(m, An, Af, diff, between);
-    else if (ex.qh == 2 && ex.ph == 4) launch_pairs_t<2, 4>(m, An, Af, diff, between);
-    else if (ex.qh == 1 && ex.ph == 2) launch_pairs_t<1, 2>(m, An, Af, diff, between);
-    else launch_pairs_t<-1, -1>(m, An, Af, diff, between);
+    if (ex.qh == 3 && ex.ph == 6) launch_pairs_t<3, 6>(m, An, Af, diff, between, shard);
+    else if (ex.qh == 2 && ex.ph == 4) launch_pairs_t<2, 4>(m, An, Af, diff, between, shard);
+    else if (ex.qh == 1 && ex.ph == 2) launch_pairs_t<1, 2>(m, An, Af, diff, between, shard);
+    else launch_pairs_t<-1, -1>(m, An, Af, diff, between, shard);
     RPB_CUDA(cudaGetLastError());
     return RPB_OK;
 }
@@ -433,61 +528,8 @@ rpb_status rpb_mesh_create(int dom_dim, int amb_dim, const double* Vh, int64_t n
         if ((st = upload(m->far_order, fo.data(), fo.size(), s)) != RPB_OK) return fail(st);
         m->near_blocks = pair_blocks(m->N, NEAR_LANES);
         m->far_blocks = pair_blocks(m->NC, FAR_LANES);
-        // shared-memory row tiles; the kernels' grids are then one block per tile
-        // Tiles are balanced by entries and their count is a whole number of waves of
-        // resident blocks (no partial last wave, whose few blocks would run while the
-        // other SMs idle); at most NEAR_TILE_ROWS / FAR_TILE_ROWS rows per tile on average.
-        int sms = 0;
-        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, m->device) != cudaSuccess) sms = 0;
-        auto tile = [&](const SymPattern& P, int ncols, bool far, const void* kernel, int cap, TileBufs& d, int& blocks) {
-            d.valid = false;
-            auto resident = [&](int max_union) {
-                int per_sm = 0;
-                if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, PAIR_TILE_THREADS,
-                                                                  pair_tile_smem(max_union, far)) != cudaSuccess)
-                    return 0;
-                return per_sm;
-            };
-            if (sms <= 0 || P.nnz() == 0) return RPB_OK;
-            // resident blocks depend on the tiles' largest union and the tile size on the
-            // resident blocks: start from the cap and re-tile while the count changes
-            int per_sm = resident(cap);
-            RowTiles R;
-            for (int pass = 0; pass < 3 && per_sm > 0; ++pass) {
-                const int64_t slots = static_cast<int64_t>(per_sm) * sms;
-                const int64_t tile_rows = far ? FAR_TILE_ROWS : NEAR_TILE_ROWS;
-                const int64_t waves = std::max<int64_t>(1, (P.rows + slots * tile_rows - 1) / (slots * tile_rows));
-                const int64_t target = (P.nnz() + waves * slots - 1) / (waves * slots);
-                build_row_tiles(P.rp.data(), P.ci.data(), P.rows, ncols, PAIR_TILE_THREADS, target, cap,
-                                std::max(1, m->settings.threads), R);
-                if (!R.valid) break;
-                const int now = resident(R.max_union);
-                if (now == per_sm) break;
-                per_sm = now;
-            }
-            if (per_sm <= 0 || !R.valid || R.tiles() == 0) return RPB_OK;
-            rpb_status e;
-            if ((e = upload(d.row0, R.row0.data(), R.row0.size(), s)) != RPB_OK) return e;
-            if ((e = upload(d.cols_rp, R.cols_rp.data(), R.cols_rp.size(), s)) != RPB_OK) return e;
-            if ((e = upload(d.cols, R.cols.data(), R.cols.size(), s)) != RPB_OK) return e;
-            if ((e = upload(d.order, R.order.data(), R.order.size(), s)) != RPB_OK) return e;
-            if ((e = upload(d.slot, R.slot.data(), R.slot.size(), s)) != RPB_OK) return e;
-            if ((e = upload(d.lane_map, R.lane_map.data(), R.lane_map.size(), s)) != RPB_OK) return e;
-            d.tiles = R.tiles();
-            d.max_union = R.max_union;
-            d.valid = true;
-            blocks = d.tiles;
-            return RPB_OK;
-        };
-        if ((st = allow_tile_smem(m->device)) != RPB_OK) return fail(st);
-        const void* kn = reinterpret_cast<const void*>(k_tp0_pairs_tiled<false, 3, 6, true>);
-        const void* kf = reinterpret_cast<const void*>(k_tp0_pairs_tiled<true, 3, 6, true>);
-        if ((st = tile(T.near, m->N, false, kn, NEAR_TILE_UNION, m->near_tiles, m->near_blocks)) != RPB_OK)
-            return fail(st);
-        if ((st = tile(T.far, m->NC, true, kf, FAR_TILE_UNION, m->far_tiles, m->far_blocks)) != RPB_OK)
-            return fail(st);
+        if ((st = build_pair_tiles(m, 1)) != RPB_OK) return fail(st);
     }
-    if (m->block_energy.alloc(m->near_blocks + m->far_blocks)) { set_error("device allocation failed"); return fail(RPB_ENOMEM); }
     if (cudaMemsetAsync(m->counter.ptr, 0, m->counter.bytes(), s) != cudaSuccess ||
         cudaMemsetAsync(m->done.ptr, 0, m->done.bytes(), s) != cudaSuccess ||
         cudaMemsetAsync(m->energy.ptr, 0, m->energy.bytes(), s) != cudaSuccess) {
@@ -734,6 +776,80 @@ rpb_status rpb_tpe0_differential_device(rpb_mesh* m, double q, double p, double 
     if (!m || !Y_dev) { set_error("null argument"); return RPB_EINVAL; }
     if (ldY < 3) { set_error("ldY must be >= AMB_DIM = 3"); return RPB_EINVAL; }
     return evaluate(m, q, p, true, alpha, beta, Y_dev, ldY, energy);
+}
+
+rpb_status rpb_mesh_set_shards(rpb_mesh* m, int shards)
+{
+    if (!m) { set_error("null mesh"); return RPB_EINVAL; }
+    if (shards < 1) { set_error("shards must be >= 1"); return RPB_EINVAL; }
+    RPB_CUDA(cudaSetDevice(m->device));
+    RPB_CUDA(cudaStreamSynchronize(m->stream));
+    rpb_status st = build_pair_tiles(m, shards);
+    if (st != RPB_OK) return st;
+    RPB_CUDA(cudaStreamSynchronize(m->stream));
+    return RPB_OK;
+}
+
+rpb_status rpb_mesh_shard_rows(const rpb_mesh* m, int shard, int64_t* near_rows, int64_t* far_rows)
+{
+    if (!m || !near_rows || !far_rows) { set_error("null argument"); return RPB_EINVAL; }
+    if (shard < 0 || shard >= m->shards) { set_error("shard out of range"); return RPB_EINVAL; }
+    const TileBufs* tb[2] = {&m->near_tiles, &m->far_tiles};
+    int64_t* out[2] = {near_rows, far_rows};
+    const int rows[2] = {m->N, m->NC};
+    for (int k = 0; k < 2; ++k) {
+        if (!tb[k]->valid) {
+            out[k][0] = 0; out[k][1] = shard == 0 ? rows[k] : 0;   // untiled (empty) pattern: shard 0
+            continue;
+        }
+        int first, count;
+        shard_tiles(*tb[k], shard, m->shards, first, count);
+        out[k][0] = tb[k]->row0_host[first];
+        out[k][1] = tb[k]->row0_host[first + count];
+    }
+    return RPB_OK;
+}
+
+rpb_status rpb_mesh_shard_buffer_doubles(const rpb_mesh* m, int64_t* doubles)
+{
+    if (!m || !doubles) { set_error("null argument"); return RPB_EINVAL; }
+    *doubles = 10 * static_cast<int64_t>(m->N) + 10 * static_cast<int64_t>(m->NC) + 1;
+    return RPB_OK;
+}
+
+rpb_status rpb_tpe0_pairs_shard(rpb_mesh* m, double q, double p, int shard, double* buf)
+{
+    if (!m || !buf) { set_error("null argument"); return RPB_EINVAL; }
+    if (shard < 0 || shard >= m->shards) { set_error("shard out of range"); return RPB_EINVAL; }
+    if (m->verynear.nnz > 0) {
+        set_error("row-sharded evaluation is not built for meshes with very-near primitive pairs");
+        return RPB_EINVAL;
+    }
+    if ((m->near.nnz > 0 && !m->near_tiles.valid) || (m->far.nnz > 0 && !m->far_tiles.valid)) {
+        set_error("row-sharded evaluation needs row tiles (a row exceeds the tile column cap)");
+        return RPB_EINVAL;
+    }
+    rpb_status st = check_exponents(q, p);
+    if (st != RPB_OK) return st;
+    RPB_CUDA(cudaSetDevice(m->device));
+    if (!m->geometry_valid && (st = launch_geometry(m)) != RPB_OK) return st;
+    double* D_near = buf;
+    double* D_far = buf + 10 * static_cast<int64_t>(m->N);
+    double* e_out = D_far + 10 * static_cast<int64_t>(m->NC);
+    if ((st = launch_pairs(m, make_exp(m->dom, q, p), true, nullptr, shard, D_near, D_far)) != RPB_OK) return st;
+    k_add_pair<<<1, 1, 0, m->stream>>>(m->energy.ptr, e_out);
+    RPB_CUDA(cudaGetLastError());
+    return RPB_OK;
+}
+
+rpb_status rpb_tpe0_collect_shards(rpb_mesh* m, const double* buf, double alpha, double beta, double* Y_dev, int ldY)
+{
+    if (!m || !buf || !Y_dev) { set_error("null argument"); return RPB_EINVAL; }
+    if (ldY < 3) { set_error("ldY must be >= AMB_DIM = 3"); return RPB_EINVAL; }
+    RPB_CUDA(cudaSetDevice(m->device));
+    const double* D_near = buf;
+    const double* D_far = buf + 10 * static_cast<int64_t>(m->N);
+    return launch_collect_gather(m, alpha, beta, Y_dev, ldY, false, D_near, D_far);
 }
 
 rpb_status rpb_tpe0_energy_device(rpb_mesh* m, double* energy_dev)

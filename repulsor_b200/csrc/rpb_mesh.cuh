@@ -68,6 +68,7 @@ struct PseudoLapCache {
 struct TileBufs {
     DevBuf<int> row0, cols_rp, cols, order, lane_map;
     DevBuf<uint16_t> slot;
+    std::vector<int> row0_host;   // tiles + 1: first row of each tile
     int tiles = 0, max_union = 0;
     bool valid = false;
 };
@@ -106,6 +107,7 @@ struct rpb_mesh {
     rpb::DevBuf<double> block_energy, energy;   // energy[0] near, [1] far, [2] very near
     rpb::DevBuf<unsigned> done;                 // last-block counters of the two pair kernels
     int near_blocks = 0, far_blocks = 0;
+    int shards = 1;                             // row shards the tiles are grouped for
     // metric: frozen Pre/Post (per primitive in tree order: sorted vertex ids, 4 x size coefficients)
     rpb::DevBuf<int> pre_cols;
     rpb::DevBuf<double> pre_vals;
