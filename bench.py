@@ -31,10 +31,13 @@ sys.path.insert(0, ROOT)
 
 METRIC = "energy+grad evals/s; metric-solve ms to 1e-6 res, learned vs plain precond, 1 GPU"
 Q, P = 6.0, 12.0
-# algorithmic flops per unique pair of the energy+differential pair kernel (hand count of
-# TP0_Kernel_FF/NF::Compute with q/2 = 3, p/2 = 6: far-field 165, near-field 185)
-FLOPS_FAR_PAIR = 165.0
-FLOPS_NEAR_PAIR = 185.0
+# algorithmic flops per unique pair of the energy+differential traversal with q/2 = 3,
+# p/2 = 6 (TP0_Kernel_FF/NF::Compute and the loop bodies around them), counted by the
+# oracle's operation-counting scalar (oracle.pair_opcounts; tests/test_opcounts.py keeps
+# these equal): far field 56 add + 96 mul + 1 div, near field (triangles) 74 add + 123 mul
+# + 1 div
+FLOPS_FAR_PAIR = 153.0
+FLOPS_NEAR_PAIR = 198.0
 # geometry (primitive data + in-block scans), block scan, cluster moments, near pairs,
 # far pairs, collect + chain rule, vertex gather
 LAUNCHES_PER_STEP = 7
@@ -66,6 +69,15 @@ def pair_traffic_from_profile():
         return None
     m = re.search(r"DRAM bytes per evaluation[^:]*:\s*([0-9,]+)", open(path).read(), re.IGNORECASE)
     return int(m.group(1).replace(",", "")) if m else None
+
+
+def measured_hbm_gbs():
+    """HBM copy bandwidth measured on this pool's B200s (MEASURED_PEAKS.json), else the
+    pool's earlier measurement."""
+    try:
+        return float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"])
+    except (OSError, KeyError, ValueError):
+        return 6650.0
 
 
 def workload_mesh():
@@ -194,12 +206,17 @@ def main():
     ap.add_argument("--flow-max-iter", type=int, default=3000, help="iteration limit of the full-flow Solve")
     ap.add_argument("--flow", action="store_true",
                     help="only the full flow step on two linked tori (1,228,800 triangles) with an obstacle")
+    ap.add_argument("--sharded", action="store_true",
+                    help="strong scaling: one mesh (the two linked tori) row-sharded over the ranks, one NCCL "
+                         "all-reduce of the derivative buffers per evaluation")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
         return run_reference(args)
     if args.flow:
         return run_flow(args)
+    if args.sharded:
+        return run_sharded(args)
 
     import numpy as np
     import torch
@@ -361,8 +378,22 @@ def extras(rpb, torch, with_solve):
     b.record(ext)
     torch.cuda.synchronize()
     mv_ms = a.elapsed_time(b) / n
+    st = M.stats()
+    N, NC, nV = st["simplex_count"], st["cluster_count"], st["vertex_count"]
+    # algorithmic bytes of one product: per full-pattern nonzero two FP32 values and a column
+    # index; row pointers; the FP64 12-wide primitive and cluster buffers read and written;
+    # the Pre/Post operator (3 indices + 12 FP64 coefficients per primitive) applied twice;
+    # the input, output and one intermediate vertex vector
+    mv_bytes = ((st["near_nnz"] + st["far_nnz"]) * 12 + (N + NC) * 8 + (N + NC) * 96 * 2
+                + N * (3 * 4 + 12 * 8) * 2 + nV * 24 * 3)
+    peak = measured_hbm_gbs()
+    achieved = mv_bytes / (mv_ms * 1e-3) / 1e9
     out = {"metric_matvec": {"workload": "icosphere level 6 (81,920 triangles), nrhs=3",
-                             "matvecs_per_s": 1e3 / mv_ms, "ms": mv_ms}}
+                             "matvecs_per_s": 1e3 / mv_ms, "ms": mv_ms,
+                             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                                          "frac": achieved / peak if peak else None, "bytes_per_product": mv_bytes,
+                                          "note": "the block SpMM is bound by L1 request throughput on the "
+                                                  "96-byte input gathers, not by HBM"}}}
     if not with_solve:
         return out
     out["solve"] = solve_extras(rpb, M, tpm, V)
@@ -479,6 +510,72 @@ def run_flow(args):
                     "rel_residual": [float(x) for x in tpm.Solver_RelativeResiduals()]}
     out["value"] = out["energy_grad_s"] + out["solve_s"]
     print(json.dumps(out))
+    return 0
+
+
+def run_sharded(args):
+    """One evaluation (SemiStaticUpdate + Differential) of the two linked tori (1,228,800
+    triangles) per step, its row tiles split over the ranks (repulsor_b200/sharding.py):
+    each GPU evaluates its shard, one NCCL all-reduce sums the (N + N_C) x 10 derivative
+    buffer, every GPU collects. Total work is fixed as N grows (strong scaling); the step
+    time is the slowest rank's CUDA-event time."""
+    import datetime
+
+    import torch
+
+    import repulsor_b200 as rpb
+    from repulsor_b200 import meshes
+    from repulsor_b200.sharding import ShardedDifferential
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local_rank)
+    import torch.distributed as dist
+    os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+    os.environ.setdefault("MASTER_PORT", "29512")
+    dist.init_process_group("nccl", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120),
+                            device_id=torch.device("cuda", local_rank))
+    try:
+        V, S = meshes.linked_tori()
+        M = rpb.SimplicialMesh(V, S, device=local_rank)
+        tpe = rpb.TangentPointEnergy0(Q, P)
+        sd = ShardedDifferential(M, tpe)
+        Vd = torch.tensor(V, device="cuda")
+        Yd = torch.zeros((V.shape[0], 3), dtype=torch.float64, device="cuda")
+        ext = torch.cuda.ExternalStream(M.stream())
+
+        def step():
+            M.SemiStaticUpdateDevice(Vd.data_ptr())
+            sd(Yd.data_ptr(), want_energy=False)
+
+        for _ in range(args.warmup):
+            step()
+        torch.cuda.synchronize()
+        dist.barrier()
+        steps = max(1, min(args.steps, 50))
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(ext)
+        for _ in range(steps):
+            step()
+        b.record(ext)
+        torch.cuda.synchronize()
+        ms = max_over_ranks(a.elapsed_time(b) / steps, dist, "cuda")
+        E = sd(Yd.data_ptr())
+        st = M.stats()
+        if rank == 0:
+            print(json.dumps({"metric": "energy+grad evals/s of one mesh, row-sharded", "value": 1e3 / ms,
+                              "unit": "evals/s", "n_gpus": world, "steps": steps, "warmup": args.warmup,
+                              "ms_per_step": ms, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+                              "dtype": "f32+f64", "data": "synthetic (seeded linked tori)",
+                              "config": {"workload": "two linked tori 480x640 (1,228,800 triangles), q=6 p=12 "
+                                                     "theta=0.5", "parallelism": f"row shards x{world}",
+                                         "near_nnz": st["near_nnz"], "far_nnz": st["far_nnz"],
+                                         "allreduce_bytes": 8 * sd.buf.numel()},
+                              "energy": E}))
+        del sd
+    finally:
+        dist.destroy_process_group()
     return 0
 
 

@@ -55,6 +55,7 @@ def _load():
     lib.oracle_partial_derivatives.restype = ctypes.c_double
     lib.oracle_partial_derivatives.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                                ctypes.c_int, _dp, _dp]
+    lib.oracle_pair_opcounts.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, _lp]
     lib.oracle_collect.argtypes = [ctypes.c_void_p, _dp, _dp, ctypes.c_double, ctypes.c_double, _dp, ctypes.c_int]
     lib.oracle_allpairs_energy.restype = ctypes.c_double
     lib.oracle_allpairs_energy.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double]
@@ -93,6 +94,18 @@ def _i(a):
 
 def _l(a):
     return a.ctypes.data_as(_lp)
+
+
+def pair_opcounts(dom, far, q=6.0, p=12.0):
+    """Arithmetic of one unique pair of the energy + differential traversal (FF loop body
+    if far, else the NF loop body for simplices of dimension dom), counted by the oracle's
+    operation-counting scalar: {"add", "mul", "div", "sqrt", "pow", "flops"} with flops =
+    add + mul + div + sqrt + pow (the source has no fused multiply-adds)."""
+    out = np.zeros(5, dtype=np.int64)
+    _load().oracle_pair_opcounts(int(dom), int(bool(far)), float(q), float(p), _l(out))
+    c = dict(zip(("add", "mul", "div", "sqrt", "pow"), (int(v) for v in out)))
+    c["flops"] = sum(c.values())
+    return c
 
 
 class OracleMesh:

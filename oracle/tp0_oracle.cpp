@@ -707,12 +707,21 @@ static void compute_cluster_data(Mesh& M)
 // Integer powers (Tensors' Power<Real,Int>: exact repeated multiplication,
 // reciprocal for negative exponents).
 // ----------------------------------------------------------------------------
-static inline double ipow(double x, int k)
+template <typename R>
+static inline R ipow(R x, int k)
 {
-    if (k < 0) return 1.0 / ipow(x, -k);
-    double r = 1.0;
-    double b = x;
-    while (k) { if (k & 1) r *= b; b *= b; k >>= 1; }
+    if (k < 0) return R(1.0) / ipow(x, -k);
+    R r = R(1.0);
+    R b = x;
+    bool first = true;
+    while (k) {
+        if (k & 1) {
+            if (first) { r = b; first = false; }   // 1 * b is not an operation
+            else r = r * b;
+        }
+        k >>= 1;
+        if (k) b = b * b;
+    }
     return r;
 }
 
@@ -730,83 +739,119 @@ struct TPParams {
         const double s = (p - dom) / q;
         s_exp_metric = -0.5 * (2.0 * (s - 1.0) + dom);
     }
-    double pow_r2(double r2, double half_exp_plus) const;  // not used
 };
 
+// ----------------------------------------------------------------------------
+// Operation counting (test infrastructure for the roofline's algorithmic flops): a double
+// that counts its arithmetic. add/sub, mul, div, sqrt and pow calls are counted
+// separately; abs and comparisons are not arithmetic.
+// ----------------------------------------------------------------------------
+struct OpCounts { int64_t add = 0, mul = 0, div = 0, sqrt = 0, pow = 0; };
+static thread_local OpCounts g_ops;
+struct FC {
+    double v = 0;
+    FC() = default;
+    FC(double x) : v(x) {}   // NOLINT: implicit from double, as a Real would be
+};
+static inline FC operator+(FC a, FC b) { ++g_ops.add; return FC(a.v + b.v); }
+static inline FC operator-(FC a, FC b) { ++g_ops.add; return FC(a.v - b.v); }
+static inline FC operator*(FC a, FC b) { ++g_ops.mul; return FC(a.v * b.v); }
+static inline FC operator/(FC a, FC b) { ++g_ops.div; return FC(a.v / b.v); }
+static inline FC operator-(FC a) { return FC(-a.v); }
+static inline FC& operator+=(FC& a, FC b) { a = a + b; return a; }
+static inline FC& operator-=(FC& a, FC b) { a = a - b; return a; }
+static inline FC& operator*=(FC& a, FC b) { a = a * b; return a; }
+static inline FC fc_abs(FC a) { return FC(std::fabs(a.v)); }
+static inline double fc_abs(double a) { return std::fabs(a); }
+static inline FC fc_pow(FC a, double e) { ++g_ops.pow; return FC(std::pow(a.v, e)); }
+static inline double fc_pow(double a, double e) { return std::pow(a, e); }
+
 // Power of r2 by (-p/2 - 1), and |c|^(q/2 - 1)
-static inline double pow_r_mp2(const TPParams& T, double r2)
+template <typename R>
+static inline R pow_r_mp2(const TPParams& T, R r2)
 {
-    return T.p_int ? ipow(r2, -T.p_half_int - 1) : std::pow(r2, -T.p / 2 - 1);
+    return T.p_int ? ipow(r2, -T.p_half_int - 1) : fc_pow(r2, -T.p / 2 - 1);
 }
-static inline double pow_c(const TPParams& T, double c_abs)
+template <typename R>
+static inline R pow_c(const TPParams& T, R c_abs)
 {
-    return T.q_int ? ipow(c_abs, T.q_half_int - 1) : std::pow(c_abs, T.q / 2 - 1);
+    return T.q_int ? ipow(c_abs, T.q_half_int - 1) : fc_pow(c_abs, T.q / 2 - 1);
 }
 
 // One pair of the TP0 FF/NF kernels (TP0_Kernel_FF.hpp:130-319, TP0_Kernel_NF.hpp:140-338)
 // in moment coordinates. x,y centres; P,Q packed projectors; a,b weights.
 // Outputs (if non-null): DX/DY in (a, x, P) layout of FF (10 entries). For NF
 // the hull slots are filled from the x-slot by the caller.
-struct PairOut {
-    double E;          // energy density E (without a*b)
-    double energy;     // a*E*b
-    double dens_x;     // density contribution at x: b |Pv|^q / |v|^p (TP0_Kernel_FF.hpp:214-218)
-    double dens_y;     // density contribution at y: a |Qv|^q / |v|^p
-    double DX[10], DY[10];
-    double a0, a1;     // metric block
+template <typename R>
+struct PairOutT {
+    R E;          // energy density E (without a*b)
+    R energy;     // a*E*b
+    R dens_x;     // density contribution at x: b |Pv|^q / |v|^p (TP0_Kernel_FF.hpp:214-218)
+    R dens_y;     // density contribution at y: a |Qv|^q / |v|^p
+    R DX[10], DY[10];
+    R a0, a1;     // metric block
 };
+using PairOut = PairOutT<double>;
 
-static inline void tp0_pair(const TPParams& T, double a, const double* x, const double* P, double b,
-                            const double* y, const double* Q, bool diff, bool metric, PairOut& o)
+template <typename R>
+static inline void tp0_pair(const TPParams& T, R a, const R* x, const R* P, R b, const R* y, const R* Q, bool diff,
+                            bool metric, PairOutT<R>& o)
 {
-    double v[3], Pv[3] = {0, 0, 0}, Qv[3] = {0, 0, 0}, V[6];
-    double r2 = 0, cphi = 0, cpsi = 0;
-    for (int l = 0; l < 3; ++l) { v[l] = y[l] - x[l]; r2 += v[l] * v[l]; }
+    R v[3], Pv[3], Qv[3], V[6];
+    R r2, cphi, cpsi;
+    for (int l = 0; l < 3; ++l) {
+        v[l] = y[l] - x[l];
+        r2 = (l == 0) ? v[l] * v[l] : r2 + v[l] * v[l];
+    }
     for (int i = 0; i < 3; ++i) {
         for (int j = 0; j < 3; ++j) {
             const int k = lin_k(i, j);
-            Pv[i] += P[k] * v[j];
-            Qv[i] += Q[k] * v[j];
-            if (j >= i) V[k] = (1.0 + (i != j ? 1.0 : 0.0)) * v[i] * v[j];
+            Pv[i] = (j == 0) ? P[k] * v[j] : Pv[i] + P[k] * v[j];
+            Qv[i] = (j == 0) ? Q[k] * v[j] : Qv[i] + Q[k] * v[j];
+            if (j > i) V[k] = R(2.0) * v[i] * v[j];
+            else if (j == i) V[k] = v[i] * v[j];
         }
-        cphi += v[i] * Pv[i];
-        cpsi += v[i] * Qv[i];
+        cphi = (i == 0) ? v[i] * Pv[i] : cphi + v[i] * Pv[i];
+        cpsi = (i == 0) ? v[i] * Qv[i] : cpsi + v[i] * Qv[i];
     }
-    const double rmp2 = pow_r_mp2(T, r2);
-    const double rmp = rmp2 * r2;
-    const double cphi_qm2 = pow_c(T, std::abs(cphi));
-    const double cpsi_qm2 = pow_c(T, std::abs(cpsi));
-    const double cphi_q = cphi_qm2 * cphi;
-    const double cpsi_q = cpsi_qm2 * cpsi;
-    const double Num = cphi_q + cpsi_q;
-    const double E = Num * rmp;
+    const R rmp2 = pow_r_mp2(T, r2);
+    const R rmp = rmp2 * r2;
+    const R cphi_qm2 = pow_c(T, fc_abs(cphi));
+    const R cpsi_qm2 = pow_c(T, fc_abs(cpsi));
+    const R cphi_q = cphi_qm2 * cphi;
+    const R cpsi_q = cpsi_qm2 * cpsi;
+    const R Num = cphi_q + cpsi_q;
+    const R E = Num * rmp;
     o.E = E;
     o.energy = a * E * b;
-    o.dens_x = b * cphi_q * rmp;
-    o.dens_y = a * cpsi_q * rmp;
+    o.dens_x = R(0.0);
+    o.dens_y = R(0.0);
+    if (!diff && !metric) {   // densities only where an energy alone is asked for
+        o.dens_x = b * cphi_q * rmp;
+        o.dens_y = a * cpsi_q * rmp;
+    }
     if (diff) {
-        const double factor = T.q * rmp;
-        const double Kxy = factor * cphi_qm2;
-        const double Kyx = factor * cpsi_qm2;
-        const double H = T.p * rmp2 * Num;
-        double dEdvx = 0, dEdvy = 0;
-        for (int k = 0; k < 10; ++k) { o.DX[k] = 0; o.DY[k] = 0; }
+        const R factor = R(T.q) * rmp;
+        const R Kxy = factor * cphi_qm2;
+        const R Kyx = factor * cpsi_qm2;
+        const R H = R(T.p) * rmp2 * Num;
+        R dEdvx, dEdvy;
         for (int i = 0; i < 3; ++i) {
-            const double dEdv = Kxy * Pv[i] + Kyx * Qv[i] - H * v[i];
-            dEdvx += dEdv * x[i];
-            dEdvy += dEdv * y[i];
-            o.DX[1 + i] -= b * dEdv;
-            o.DY[1 + i] += a * dEdv;
+            const R dEdv = Kxy * Pv[i] + Kyx * Qv[i] - H * v[i];
+            dEdvx = (i == 0) ? dEdv * x[i] : dEdvx + dEdv * x[i];
+            dEdvy = (i == 0) ? dEdv * y[i] : dEdvy + dEdv * y[i];
+            o.DX[1 + i] = -(b * dEdv);
+            o.DY[1 + i] = a * dEdv;
         }
-        o.DX[0] += b * (E - 0.5 * factor * cphi_q + dEdvx);
-        o.DY[0] += a * (E - 0.5 * factor * cpsi_q - dEdvy);
-        const double hbK = 0.5 * b * Kxy, haK = 0.5 * a * Kyx;
-        for (int k = 0; k < 6; ++k) { o.DX[4 + k] += hbK * V[k]; o.DY[4 + k] += haK * V[k]; }
+        o.DX[0] = b * (E - R(0.5) * factor * cphi_q + dEdvx);
+        o.DY[0] = a * (E - R(0.5) * factor * cpsi_q - dEdvy);
+        const R hbK = R(0.5) * b * Kxy, haK = R(0.5) * a * Kyx;
+        for (int k = 0; k < 6; ++k) { o.DX[4 + k] = hbK * V[k]; o.DY[4 + k] = haK * V[k]; }
     }
     if (metric) {
-        const double r4 = r2 * r2;
-        const double a1 = -2.0 * std::pow(r2, T.s_exp_metric);
-        const double a0 = 0.5 * (cphi + cpsi) / r4 * a1;
+        const R r4 = r2 * r2;
+        const R a1 = R(-2.0) * fc_pow(r2, T.s_exp_metric);
+        const R a0 = R(0.5) * (cphi + cpsi) / r4 * a1;
         o.a0 = a0;
         o.a1 = a1;
     }
@@ -2055,6 +2100,50 @@ void oracle_collect(void* h, const double* D_near, const double* D_far, double a
     std::vector<std::vector<double>> tDf(1, std::vector<double>(D_far, D_far + static_cast<size_t>(M.NC) * FAR_DIM));
     collect_derivatives(M, tDn, tDf, 1, nd);
     assemble_derivatives(M, alpha, beta, Y, ldY);
+}
+
+// Arithmetic of one unique pair of the energy + differential traversals, counted with
+// FC: far = 1 the FF loop body (tp0_pair + accumulation of DX into the row and DY into
+// the column, TP0_Kernel_FF.hpp:130-319 with FMM_Kernel_FF.hpp:162-217), far = 0 the NF
+// loop body for simplices of dimension dom (column barycentre from the hull, tp0_pair,
+// spreading of dE/dx over the hull slots of row and column, TP0_Kernel_NF.hpp:140-338 with
+// FMM_Kernel_NF.hpp:169-272). Per-row work (row barycentre, row write) is excluded.
+// out: add/sub, mul, div, sqrt, pow.
+void oracle_pair_opcounts(int dom, int far, double q, double p, int64_t* out)
+{
+    const TPParams T(q, p, dom);
+    const int SIZE = dom + 1;
+    const FC S_scale(1.0 / SIZE);
+    FC x[3] = {0.1, 0.2, 0.3}, P[6] = {1, 0, 0, 1, 0, 1}, Q[6] = {1, 0, 0, 1, 0, 1}, hull[9];
+    for (int k = 0; k < 9; ++k) hull[k] = FC(0.5 + 0.1 * k);
+    FC DXs[16], DY[16];
+    for (int k = 0; k < 16; ++k) { DXs[k] = FC(0.0); DY[k] = FC(0.0); }
+    g_ops = OpCounts();
+    PairOutT<FC> o;
+    if (far) {
+        const FC y[3] = {1.1, 1.2, 1.3};
+        tp0_pair<FC>(T, FC(1.0), x, P, FC(2.0), y, Q, true, false, o);
+        for (int k = 0; k < 10; ++k) { DXs[k] += o.DX[k]; DY[k] += o.DY[k]; }
+    } else {
+        FC y[3];
+        for (int k = 0; k < 3; ++k) {
+            y[k] = S_scale * hull[k];
+            for (int v = 1; v < SIZE; ++v) y[k] += S_scale * hull[3 * v + k];
+        }
+        tp0_pair<FC>(T, FC(1.0), x, P, FC(2.0), y, Q, true, false, o);
+        DXs[0] += o.DX[0];
+        DY[0] += o.DY[0];
+        for (int v = 0; v < SIZE; ++v)
+            for (int k = 0; k < 3; ++k) {
+                DXs[1 + 3 * v + k] += S_scale * o.DX[1 + k];
+                DY[1 + 3 * v + k] += S_scale * o.DY[1 + k];
+            }
+        for (int k = 0; k < 6; ++k) {
+            DXs[1 + AMB * SIZE + k] += o.DX[4 + k];
+            DY[1 + AMB * SIZE + k] += o.DY[4 + k];
+        }
+    }
+    out[0] = g_ops.add; out[1] = g_ops.mul; out[2] = g_ops.div; out[3] = g_ops.sqrt; out[4] = g_ops.pow;
 }
 
 // moment-coordinate derivatives after collection (original order)
