@@ -13,6 +13,16 @@ namespace rpb {
 void set_error(const std::string& msg);
 TPExp make_exp(int dom, double q, double p);
 rpb_status check_exponents(double q, double p);
+
+// n rows of 3 doubles between arrays with leading dimensions ld_dst / ld_src (host or
+// device): one contiguous copy when both are 3 (a pitched copy of 24-byte rows from
+// pageable host memory moves row by row, ~100x slower), a pitched copy otherwise.
+inline cudaError_t copy_rows3(void* dst, int ld_dst, const void* src, int ld_src, int64_t n, cudaMemcpyKind kind,
+                              cudaStream_t s)
+{
+    if (ld_dst == 3 && ld_src == 3) return cudaMemcpyAsync(dst, src, sizeof(double) * 3 * n, kind, s);
+    return cudaMemcpy2DAsync(dst, sizeof(double) * ld_dst, src, sizeof(double) * ld_src, sizeof(double) * 3, n, kind, s);
+}
 rpb_status launch_geometry(rpb_mesh* m);
 // near/far moment derivatives (mesh buffers when null) -> chain rule -> Y = alpha dE + beta Y
 rpb_status launch_collect_gather(rpb_mesh* m, double alpha, double beta, double* Y, int ldY, bool with_vf,

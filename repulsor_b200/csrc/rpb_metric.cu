@@ -677,15 +677,12 @@ rpb_status rpb_tpm0_multiply(rpb_mesh* m, double q, double p, double alpha, cons
     if (ldX < 3 || ldY < 3) { set_error("leading dimensions must be >= 3"); return RPB_EINVAL; }
     RPB_CUDA(cudaSetDevice(m->device));
     cudaStream_t s = m->stream;
-    RPB_CUDA(cudaMemcpy2DAsync(m->X.ptr, 3 * sizeof(double), X, ldX * sizeof(double), 3 * sizeof(double), m->nV,
-                               cudaMemcpyHostToDevice, s));
+    RPB_CUDA(copy_rows3(m->X.ptr, 3, X, ldX, m->nV, cudaMemcpyHostToDevice, s));
     if (beta != 0.0)
-        RPB_CUDA(cudaMemcpy2DAsync(m->Yb.ptr, 3 * sizeof(double), Y, ldY * sizeof(double), 3 * sizeof(double), m->nV,
-                                   cudaMemcpyHostToDevice, s));
+        RPB_CUDA(copy_rows3(m->Yb.ptr, 3, Y, ldY, m->nV, cudaMemcpyHostToDevice, s));
     rpb_status st = metric_multiply_dev(m, q, p, alpha, m->X.ptr, 3, beta, m->Yb.ptr, 3, flags);
     if (st != RPB_OK) return st;
-    RPB_CUDA(cudaMemcpy2DAsync(Y, ldY * sizeof(double), m->Yb.ptr, 3 * sizeof(double), 3 * sizeof(double), m->nV,
-                               cudaMemcpyDeviceToHost, s));
+    RPB_CUDA(copy_rows3(Y, ldY, m->Yb.ptr, 3, m->nV, cudaMemcpyDeviceToHost, s));
     RPB_CUDA(cudaStreamSynchronize(s));
     return RPB_OK;
 }

@@ -259,13 +259,11 @@ rpb_status rpb_tpoe_differential(rpb_mesh* m, double q, double p, double alpha, 
     if (ldY < 3) { set_error("ldY must be >= AMB_DIM = 3"); return RPB_EINVAL; }
     RPB_CUDA(cudaSetDevice(m->device));
     if (beta != 0.0)
-        RPB_CUDA(cudaMemcpy2DAsync(m->Y.ptr, 3 * sizeof(double), Y, ldY * sizeof(double), 3 * sizeof(double), m->nV,
-                                   cudaMemcpyHostToDevice, m->stream));
+        RPB_CUDA(copy_rows3(m->Y.ptr, 3, Y, ldY, m->nV, cudaMemcpyHostToDevice, m->stream));
     double e = 0;
     const rpb_status st = evaluate_obstacle(m, q, p, true, alpha, beta, m->Y.ptr, 3, &e);
     if (st != RPB_OK) return st;
-    RPB_CUDA(cudaMemcpy2DAsync(Y, ldY * sizeof(double), m->Y.ptr, 3 * sizeof(double), 3 * sizeof(double), m->nV,
-                               cudaMemcpyDeviceToHost, m->stream));
+    RPB_CUDA(copy_rows3(Y, ldY, m->Y.ptr, 3, m->nV, cudaMemcpyDeviceToHost, m->stream));
     RPB_CUDA(cudaStreamSynchronize(m->stream));
     if (energy) *energy = e;
     return RPB_OK;

@@ -720,17 +720,14 @@ rpb_status rpb_tpm0_precondition(rpb_mesh* m, double q, double p, double alpha, 
     if ((st = ensure_solver(m)) != RPB_OK) return st;
     cudaStream_t s = m->stream;
     const int n = m->nV;
-    RPB_CUDA(cudaMemcpy2DAsync(m->X.ptr, 3 * sizeof(double), X, ldX * sizeof(double), 3 * sizeof(double), n,
-                               cudaMemcpyHostToDevice, s));
+    RPB_CUDA(copy_rows3(m->X.ptr, 3, X, ldX, n, cudaMemcpyHostToDevice, s));
     if (beta != 0.0)
-        RPB_CUDA(cudaMemcpy2DAsync(m->Yb.ptr, 3 * sizeof(double), Y, ldY * sizeof(double), 3 * sizeof(double), n,
-                                   cudaMemcpyHostToDevice, s));
+        RPB_CUDA(copy_rows3(m->Yb.ptr, 3, Y, ldY, n, cudaMemcpyHostToDevice, s));
     double* Z = m->solver->vec.ptr + Solver::V_Z * 3 * static_cast<size_t>(n);
     if ((st = reference_precondition(m, q, p, m->X.ptr, Z)) != RPB_OK) return st;
     k_axpby3<<<(n + 255) / 256, 256, 0, s>>>(n, alpha, Z, beta, m->Yb.ptr, 3);
     RPB_CUDA(cudaGetLastError());
-    RPB_CUDA(cudaMemcpy2DAsync(Y, ldY * sizeof(double), m->Yb.ptr, 3 * sizeof(double), 3 * sizeof(double), n,
-                               cudaMemcpyDeviceToHost, s));
+    RPB_CUDA(copy_rows3(Y, ldY, m->Yb.ptr, 3, n, cudaMemcpyDeviceToHost, s));
     RPB_CUDA(cudaStreamSynchronize(s));
     return RPB_OK;
 }
@@ -754,8 +751,7 @@ rpb_status rpb_tpm0_solve(rpb_mesh* m, double q, double p, double alpha, const d
     cudaStream_t s = m->stream;
     const int n = m->nV;
     double* Bd = m->solver->vec.ptr + Solver::V_B * 3 * static_cast<size_t>(n);
-    RPB_CUDA(cudaMemcpy2DAsync(Bd, 3 * sizeof(double), B, ldB * sizeof(double), 3 * sizeof(double), n,
-                               cudaMemcpyHostToDevice, s));
+    RPB_CUDA(copy_rows3(Bd, 3, B, ldB, n, cudaMemcpyHostToDevice, s));
     int it = 0;
     double rr[3] = {0, 0, 0};
     rpb_status cs = cg_solve(m, q, p, Bd, max_iter, tol, precond, &it, rr);
@@ -764,13 +760,11 @@ rpb_status rpb_tpm0_solve(rpb_mesh* m, double q, double p, double alpha, const d
     if (rel_residual)
         for (int c = 0; c < 3; ++c) rel_residual[c] = rr[c];
     if (beta != 0.0)
-        RPB_CUDA(cudaMemcpy2DAsync(m->Yb.ptr, 3 * sizeof(double), X, ldX * sizeof(double), 3 * sizeof(double), n,
-                                   cudaMemcpyHostToDevice, s));
+        RPB_CUDA(copy_rows3(m->Yb.ptr, 3, X, ldX, n, cudaMemcpyHostToDevice, s));
     const double* xs = m->solver->vec.ptr + Solver::V_X * 3 * static_cast<size_t>(n);
     k_axpby3<<<(n + 255) / 256, 256, 0, s>>>(n, alpha, xs, beta, m->Yb.ptr, 3);
     RPB_CUDA(cudaGetLastError());
-    RPB_CUDA(cudaMemcpy2DAsync(X, ldX * sizeof(double), m->Yb.ptr, 3 * sizeof(double), 3 * sizeof(double), n,
-                               cudaMemcpyDeviceToHost, s));
+    RPB_CUDA(copy_rows3(X, ldX, m->Yb.ptr, 3, n, cudaMemcpyDeviceToHost, s));
     RPB_CUDA(cudaStreamSynchronize(s));
     return cs;
 }
