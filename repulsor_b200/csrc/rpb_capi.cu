@@ -468,6 +468,10 @@ rpb_status rpb_mesh_create(int dom_dim, int amb_dim, const double* Vh, int64_t n
 
     if (cudaSetDevice(m->device) != cudaSuccess) { set_error("cudaSetDevice failed"); return fail(RPB_ECUDA); }
     if (cudaStreamCreateWithFlags(&m->own_stream, cudaStreamNonBlocking) != cudaSuccess) { set_error("stream creation failed"); return fail(RPB_ECUDA); }
+    if (cudaMallocHost(reinterpret_cast<void**>(&m->host_energy), 3 * sizeof(double)) != cudaSuccess) {
+        set_error("pinned host allocation failed");
+        return fail(RPB_ENOMEM);
+    }
     m->stream = m->own_stream;
     cudaStream_t s = m->stream;
     const HostTree& T = m->tree;
@@ -555,7 +559,7 @@ rpb_status rpb_mesh_destroy(rpb_mesh* m)
     learned_free(m);
     obstacle_free(m);
     cudaStream_t s = m->own_stream;
-    delete m;  // frees device buffers
+    delete m;  // frees device buffers and the pinned energy slots
     if (s) cudaStreamDestroy(s);
     return RPB_OK;
 }
@@ -869,12 +873,13 @@ rpb_status rpb_tpe0_differential(rpb_mesh* m, double q, double p, double alpha, 
     RPB_CUDA(cudaSetDevice(m->device));
     if (beta != 0.0)
         RPB_CUDA(copy_rows3(m->Y.ptr, 3, Y, ldY, m->nV, cudaMemcpyHostToDevice, m->stream));
-    double e = 0;
-    rpb_status st = evaluate(m, q, p, true, alpha, beta, m->Y.ptr, 3, &e);
+    // the derivative and the energy parts come back with one synchronization
+    rpb_status st = evaluate(m, q, p, true, alpha, beta, m->Y.ptr, 3, nullptr);
     if (st != RPB_OK) return st;
+    RPB_CUDA(cudaMemcpyAsync(m->host_energy, m->energy.ptr, 3 * sizeof(double), cudaMemcpyDeviceToHost, m->stream));
     RPB_CUDA(copy_rows3(Y, ldY, m->Y.ptr, 3, m->nV, cudaMemcpyDeviceToHost, m->stream));
     RPB_CUDA(cudaStreamSynchronize(m->stream));
-    if (energy) *energy = e;
+    if (energy) *energy = (m->host_energy[2] + m->host_energy[0]) + m->host_energy[1];
     return RPB_OK;
 }
 

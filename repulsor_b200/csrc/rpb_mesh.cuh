@@ -81,6 +81,8 @@ struct rpb_mesh {
     double build_seconds = 0;
     cudaStream_t stream = nullptr;        // stream all work is issued on
     cudaStream_t own_stream = nullptr;    // stream created by the mesh
+    double* host_energy = nullptr;        // 3 pinned doubles: energy parts read back with the results
+    ~rpb_mesh() { if (host_energy) cudaFreeHost(host_energy); }
     rpb::HostTree tree;
     rpb::TreeSettings settings;
 
