@@ -191,6 +191,17 @@ rpb_status rpb_tpm0_solve_info(const rpb_mesh* m, rpb_solve_info* info);
  * device double `energy_dev` asynchronously on the mesh stream (graph-capturable). */
 rpb_status rpb_tpe0_energy_device(rpb_mesh* m, double* energy_dev);
 
+/* --- collision-free step size ---------------------------------------------------------------- */
+
+/* SimplicialMesh::MaximumSafeStepSize(vecs, max_time, TOL) (src/SimplicialMesh.hpp:441-468,
+ * src/CollisionTree.hpp:175-215, src/CollisionFinder.hpp:94-200): the largest t <= max_time
+ * such that the mesh moved by t * velocities (n_v x 3 host doubles) keeps every pair of
+ * primitives without a common vertex apart, up to the relative bisection tolerance `tol`
+ * (the reference's default is 0.0625). As in the reference the test uses the coordinates
+ * the cluster tree was built from. An obstacle, if loaded, is not included. */
+rpb_status rpb_mesh_maximum_safe_step_size(rpb_mesh* m, const double* velocities, double max_time, double tol,
+                                           double* t);
+
 /* --- row sharding of one evaluation over several GPUs ------------------------------------- */
 /* The reference splits the rows of the Near() and Far() lists over host threads by nonzero
  * count and adds the per-thread derivative slices (src/FMM/FMM_Traversor.hpp:56-147,

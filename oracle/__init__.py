@@ -56,6 +56,8 @@ def _load():
     lib.oracle_partial_derivatives.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                                ctypes.c_int, _dp, _dp]
     lib.oracle_pair_opcounts.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, _lp]
+    lib.oracle_maximum_safe_step_size.restype = ctypes.c_double
+    lib.oracle_maximum_safe_step_size.argtypes = [ctypes.c_void_p, _dp, ctypes.c_double, ctypes.c_double]
     lib.oracle_collect.argtypes = [ctypes.c_void_p, _dp, _dp, ctypes.c_double, ctypes.c_double, _dp, ctypes.c_int]
     lib.oracle_allpairs_energy.restype = ctypes.c_double
     lib.oracle_allpairs_energy.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double]
@@ -237,6 +239,12 @@ class OracleMesh:
         Df = np.ascontiguousarray(Df, dtype=np.float64)
         _load().oracle_collect(self._h, _d(Dn), _d(Df), alpha, beta, _d(Y), Y.shape[1])
         return Y
+
+    def maximum_safe_step_size(self, velocities, max_time, tol=0.0625):
+        """Largest step t <= max_time along the vertex velocities (n_v x 3) that keeps
+        non-adjacent primitives of the (construction-time) mesh apart."""
+        vel = np.ascontiguousarray(velocities, dtype=np.float64)
+        return _load().oracle_maximum_safe_step_size(self._h, _d(vel), float(max_time), float(tol))
 
     def moment_derivatives(self):
         nd = 1 + (self.dom + 1) * 3 + 6

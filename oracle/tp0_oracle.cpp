@@ -1967,6 +1967,351 @@ static double tp0_densities(const Mesh& M, double q, double p, std::vector<doubl
 // ============================================================================
 using namespace oracle;
 
+// ----------------------------------------------------------------------------
+// MaximumSafeStepSize (src/SimplicialMesh.hpp:441-468, src/CollisionTree.hpp:175-215):
+// the largest t <= max_time for which the mesh moved by t * (vertex velocities) keeps
+// all non-adjacent primitive pairs apart, found on the frozen (construction) coordinates
+// the cluster tree was built from. Moving simplices as space-time hulls
+// (src/Primitives/MovingPolytope.hpp:148-460), a collision-only GJK in 4 dimensions
+// (src/GJK.hpp:618-797), bisection with a stack (src/CollisionFinder.hpp:94-200), AABB
+// collision time intervals (src/CollisionTree/Compute_AABB_CollisionTimeInterval.hpp)
+// and the symmetric dual traversal with the step-size kernel
+// (src/CollisionTree/MaximumSafeStepSize_Kernel.hpp).
+// ----------------------------------------------------------------------------
+static const double kGjkEps = std::sqrt(std::numeric_limits<double>::epsilon());
+
+struct MovingSimplex {
+    int n = 3;
+    double x[3][3], u[3][3];
+    double c[3], cu[3];
+    double r = 0, v = 0, w = 0;
+    double a = 0, b = 1, T = 1;
+
+    double support(const double d[4], double s[4], bool maximum) const
+    {
+        double best_a = 0, best_b = 0;
+        int ia = 0, ib = 0;
+        for (int i = 0; i < n; ++i) {
+            double va = x[i][0] * d[0] + a * (u[i][0] * d[0]);
+            double vb = x[i][0] * d[0] + b * (u[i][0] * d[0]);
+            for (int j = 1; j < 3; ++j) {
+                const double px = x[i][j] * d[j], py = u[i][j] * d[j];
+                va += px + a * py;
+                vb += px + b * py;
+            }
+            if (i == 0 || (maximum ? va > best_a : va < best_a)) { best_a = va; ia = i; }
+            if (i == 0 || (maximum ? vb > best_b : vb < best_b)) { best_b = vb; ib = i; }
+        }
+        best_a += a * T * d[3];
+        best_b += b * T * d[3];
+        const bool take_a = maximum ? best_a >= best_b : best_a <= best_b;
+        const int i = take_a ? ia : ib;
+        const double t = take_a ? a : b;
+        for (int j = 0; j < 3; ++j) s[j] = x[i][j] + t * u[i][j];
+        s[3] = t * T;
+        return take_a ? best_a : best_b;
+    }
+    void interior(double p[4]) const
+    {
+        const double t = 0.5 * (a + b);
+        for (int k = 0; k < 3; ++k) p[k] = c[k] + t * cu[k];
+        p[3] = t * T;
+    }
+    double sq_radius() const
+    {
+        const double s = 0.5 * std::fabs(b - a);
+        const double X = s * v + r + w * b, Y = s * T;
+        return X * X + Y * Y;
+    }
+};
+
+// Closest point of the convex hull of k <= 5 points in R^4 to the origin: the minimum over
+// the faces whose affine closest point has nonnegative barycentric coordinates. Returns
+// |v|^2, the point in v and the supporting points (reordered to the front) in their count.
+static double closest_on_simplex(double W[5][4], int& k, double v[4])
+{
+    double best = std::numeric_limits<double>::infinity();
+    int best_mask = 0;
+    double best_v[4] = {0, 0, 0, 0};
+    for (int mask = 1; mask < (1 << k); ++mask) {
+        int idx[5], m = 0;
+        for (int i = 0; i < k; ++i)
+            if (mask & (1 << i)) idx[m++] = i;
+        double lam[5];
+        if (m == 1) {
+            lam[0] = 1.0;
+        } else {
+            // (w_i - w_0).(w_j - w_0) mu_j = -(w_i - w_0).w_0, i, j = 1..m-1
+            const int n = m - 1;
+            double G[4][5];
+            for (int i = 0; i < n; ++i) {
+                for (int j = 0; j < n; ++j) {
+                    double g = 0;
+                    for (int q = 0; q < 4; ++q) g += (W[idx[i + 1]][q] - W[idx[0]][q]) * (W[idx[j + 1]][q] - W[idx[0]][q]);
+                    G[i][j] = g;
+                }
+                double rhs = 0;
+                for (int q = 0; q < 4; ++q) rhs -= (W[idx[i + 1]][q] - W[idx[0]][q]) * W[idx[0]][q];
+                G[i][n] = rhs;
+            }
+            bool singular = false;
+            for (int col = 0; col < n && !singular; ++col) {
+                int piv = col;
+                for (int r = col + 1; r < n; ++r)
+                    if (std::fabs(G[r][col]) > std::fabs(G[piv][col])) piv = r;
+                double scale = 0;
+                for (int r = 0; r < n; ++r) scale = std::max(scale, std::fabs(G[r][r]));
+                if (std::fabs(G[piv][col]) <= 1e-14 * std::max(scale, 1e-300)) { singular = true; break; }
+                if (piv != col)
+                    for (int c2 = 0; c2 <= n; ++c2) std::swap(G[piv][c2], G[col][c2]);
+                for (int r = col + 1; r < n; ++r) {
+                    const double f = G[r][col] / G[col][col];
+                    for (int c2 = col; c2 <= n; ++c2) G[r][c2] -= f * G[col][c2];
+                }
+            }
+            if (singular) continue;
+            double mu[4];
+            for (int r = n - 1; r >= 0; --r) {
+                double acc = G[r][n];
+                for (int c2 = r + 1; c2 < n; ++c2) acc -= G[r][c2] * mu[c2];
+                mu[r] = acc / G[r][r];
+            }
+            double s0 = 1.0;
+            for (int i = 0; i < n; ++i) { lam[i + 1] = mu[i]; s0 -= mu[i]; }
+            lam[0] = s0;
+        }
+        bool inside = true;
+        for (int i = 0; i < m; ++i) inside = inside && lam[i] >= 0.0;
+        if (!inside) continue;
+        double p[4] = {0, 0, 0, 0};
+        for (int i = 0; i < m; ++i)
+            for (int q = 0; q < 4; ++q) p[q] += lam[i] * W[idx[i]][q];
+        const double d2 = p[0] * p[0] + p[1] * p[1] + p[2] * p[2] + p[3] * p[3];
+        if (d2 < best) { best = d2; best_mask = mask; for (int q = 0; q < 4; ++q) best_v[q] = p[q]; }
+    }
+    double keep[5][4];
+    int m = 0;
+    for (int i = 0; i < k; ++i)
+        if (best_mask & (1 << i)) { for (int q = 0; q < 4; ++q) keep[m][q] = W[i][q]; ++m; }
+    for (int i = 0; i < m; ++i) for (int q = 0; q < 4; ++q) W[i][q] = keep[i][q];
+    k = m;
+    for (int q = 0; q < 4; ++q) v[q] = best_v[q];
+    return best;
+}
+
+// Collision-only GJK: true if the two space-time hulls come closer than
+// eps * sqrt(min squared radius) (GJK::IntersectingQ with theta = 1).
+static bool gjk_intersecting(const MovingSimplex& P, const MovingSimplex& Q)
+{
+    const double eps = kGjkEps, eps2 = eps * eps;
+    double TOL2 = eps2 * std::min(P.sq_radius(), Q.sq_radius());
+    if (TOL2 <= 0) TOL2 = eps2 * std::max(P.sq_radius(), Q.sq_radius());
+    double v[4], q4[4];
+    P.interior(v);
+    Q.interior(q4);
+    for (int k = 0; k < 4; ++k) v[k] -= q4[k];
+    double W[5][4];
+    int k = 0;
+    double ps[4], qs[4];
+    P.support(v, ps, false);
+    Q.support(v, qs, true);
+    for (int j = 0; j < 4; ++j) W[0][j] = ps[j] - qs[j];
+    k = 1;
+    for (int j = 0; j < 4; ++j) v[j] = W[0][j];
+    double dotvv = v[0] * v[0] + v[1] * v[1] + v[2] * v[2] + v[3] * v[3];
+    bool separated = false;
+    int iter = 0;
+    while (true) {
+        if (dotvv < TOL2) break;
+        if (k >= 5) break;
+        if (iter >= 100) break;
+        ++iter;
+        const double a = P.support(v, ps, false);
+        const double b = Q.support(v, qs, true);
+        const double dotvw = a - b;
+        if (dotvw > 0 && dotvw * dotvw > TOL2) { separated = true; break; }
+        if (std::fabs(dotvv - dotvw) <= eps * dotvv) break;
+        double w[4];
+        for (int j = 0; j < 4; ++j) w[j] = ps[j] - qs[j];
+        bool dup = false;
+        for (int i = 0; i < k && !dup; ++i)
+            dup = W[i][0] == w[0] && W[i][1] == w[1] && W[i][2] == w[2] && W[i][3] == w[3];
+        if (dup) break;
+        for (int j = 0; j < 4; ++j) W[k][j] = w[j];
+        ++k;
+        const double old = dotvv;
+        dotvv = closest_on_simplex(W, k, v);
+        if (std::fabs(old - dotvv) <= eps * dotvv) break;
+    }
+    separated = separated || TOL2 < dotvv;
+    return !separated;
+}
+
+// CollisionFinder::FindMaximumSafeStepSize (src/CollisionFinder.hpp:94-200)
+static double find_max_safe_step(MovingSimplex P, MovingSimplex Q, double tinit, double TOL)
+{
+    double a = 0.0, b = tinit;
+    P.a = Q.a = a; P.b = Q.b = b; P.T = Q.T = 1.0;
+    double pi4[4], qi4[4];
+    P.interior(pi4);
+    Q.interior(qi4);
+    double d2 = 0;
+    for (int k = 0; k < 4; ++k) d2 += (qi4[k] - pi4[k]) * (qi4[k] - pi4[k]);
+    const double T = std::sqrt(d2 + P.sq_radius() + Q.sq_radius()) / tinit;
+    P.T = Q.T = T;
+    constexpr int max_iter = 126;
+    double stack[max_iter + 2];
+    int iter = 0, sp = 0;
+    stack[0] = 0.0;
+    while (b - a > TOL * b && iter < max_iter) {
+        ++iter;
+        if (!gjk_intersecting(P, Q)) {
+            if (sp > 0) {
+                a = b; P.a = Q.a = a;
+                b = stack[sp--]; P.b = Q.b = b;
+            } else {
+                return b;
+            }
+        } else {
+            stack[++sp] = b;
+            b = 0.5 * (a + b);
+            P.b = Q.b = b;
+        }
+    }
+    if (sp >= max_iter || iter >= max_iter) return a;
+    return a <= 0.0 ? b : a;
+}
+
+static void moving_simplex(const Mesh& M, const double* vel, Int i, MovingSimplex& P)
+{
+    const int ps = M.poly_size();
+    const double* poly = &M.P_poly[ps * static_cast<size_t>(i)];
+    const Int* s = &M.S[static_cast<size_t>(M.SIZE) * M.perm[i]];
+    P.n = M.SIZE;
+    P.r = std::sqrt(poly[0]);
+    for (int k = 0; k < 3; ++k) P.c[k] = poly[1 + k];
+    for (int j = 0; j < M.SIZE; ++j)
+        for (int k = 0; k < 3; ++k) { P.x[j][k] = poly[1 + AMB + AMB * j + k]; P.u[j][k] = vel[AMB * s[j] + k]; }
+    for (int k = 0; k < 3; ++k) {
+        P.cu[k] = P.u[0][k];
+        for (int j = 1; j < M.SIZE; ++j) P.cu[k] += P.u[j][k];
+        P.cu[k] *= 1.0 / M.SIZE;
+    }
+    P.v = std::sqrt(P.cu[0] * P.cu[0] + P.cu[1] * P.cu[1] + P.cu[2] * P.cu[2]);
+    double w2 = 0;
+    for (int j = 0; j < M.SIZE; ++j) {
+        double q = 0;
+        for (int k = 0; k < 3; ++k) q += (P.u[j][k] - P.cu[k]) * (P.u[j][k] - P.cu[k]);
+        w2 = std::max(w2, q);
+    }
+    P.w = std::sqrt(w2);
+}
+
+// Compute_AABB_CollisionTimeInterval: the first time in [0, 1] at which the boxes moving
+// linearly from p0 to p1 and from q0 to q1 ([r2, centre, half]) can intersect (1: never).
+static double aabb_collision_start(const double* p0, const double* p1, const double* q0, const double* q1)
+{
+    double t0 = 0.0, t1 = 1.0;
+    for (int k = 0; k < 3; ++k) {
+        const int i = 1 + k, j = 4 + k;
+        const double Pmin0 = p0[i] - p0[j], Pmax0 = p0[i] + p0[j], Pmin1 = p1[i] - p1[j], Pmax1 = p1[i] + p1[j];
+        const double Qmin0 = q0[i] - q0[j], Qmax0 = q0[i] + q0[j], Qmin1 = q1[i] - q1[j], Qmax1 = q1[i] + q1[j];
+        const bool init = (Pmin0 <= Qmax0) && (Qmin0 <= Pmax0);
+        const double m0 = Qmax0 - Qmax1 - Pmin0 + Pmin1, m1 = Pmax0 - Pmax1 - Qmin0 + Qmin1;
+        double A = m0 != 0 ? std::min(1.0, (Qmax0 - Pmin0) / m0) : 1.0;
+        double B = m1 != 0 ? std::min(1.0, (Pmax0 - Qmin0) / m1) : 1.0;
+        if (A > B) std::swap(A, B);
+        double a, b;
+        if (init) { a = 0.0; b = A > 0 ? A : (B <= 0 ? 1.0 : B); }
+        else if (B < 0) { a = 1.0; b = 1.0; }
+        else if (A >= 0) { a = A; b = B; }
+        else { a = B; b = 1.0; }
+        t0 = std::max(t0, a);
+        t1 = std::min(t1, b);
+    }
+    return t1 < t0 ? 1.0 : t0;
+}
+
+static bool primitives_adjacent(const Mesh& M, Int pi, Int pj)
+{
+    const Int* a = &M.S[static_cast<size_t>(M.SIZE) * M.perm[pi]];
+    const Int* b = &M.S[static_cast<size_t>(M.SIZE) * M.perm[pj]];
+    for (int x = 0; x < M.SIZE; ++x)
+        for (int y = 0; y < M.SIZE; ++y)
+            if (a[x] == b[y]) return true;
+    return false;
+}
+
+static double maximum_safe_step_size(const Mesh& M, const double* vel, double max_time, double TOL)
+{
+    const Int N = M.nS, NC = M.NC;
+    std::vector<MovingSimplex> P(N);
+    for (Int i = 0; i < N; ++i) moving_simplex(M, vel, i, P[i]);
+    // cluster boxes at max_time: leaves from the moved simplex, internal clusters merged
+    std::vector<double> lo(3 * static_cast<size_t>(NC)), hi(3 * static_cast<size_t>(NC)), C_up(7 * static_cast<size_t>(NC));
+    for (Int C = NC - 1; C >= 0; --C) {
+        double* l = &lo[3 * static_cast<size_t>(C)];
+        double* h = &hi[3 * static_cast<size_t>(C)];
+        if (M.C_left[C] < 0) {
+            const MovingSimplex& S = P[M.C_begin[C]];
+            for (int k = 0; k < 3; ++k) { l[k] = std::numeric_limits<double>::max(); h[k] = std::numeric_limits<double>::lowest(); }
+            for (int j = 0; j < S.n; ++j)
+                for (int k = 0; k < 3; ++k) {
+                    const double x = S.x[j][k] + max_time * S.u[j][k];
+                    l[k] = std::min(l[k], x);
+                    h[k] = std::max(h[k], x);
+                }
+        } else {
+            const Int L = M.C_left[C], R = M.C_right[C];
+            for (int k = 0; k < 3; ++k) {
+                l[k] = std::min(lo[3 * static_cast<size_t>(L) + k], lo[3 * static_cast<size_t>(R) + k]);
+                h[k] = std::max(hi[3 * static_cast<size_t>(L) + k], hi[3 * static_cast<size_t>(R) + k]);
+            }
+        }
+        double* bx = &C_up[7 * static_cast<size_t>(C)];
+        double r2 = 0;
+        for (int k = 0; k < 3; ++k) {
+            const double half = 0.5 * (h[k] - l[k]);
+            bx[1 + k] = l[k] + half;
+            bx[4 + k] = half;
+            r2 += half * half;
+        }
+        bx[0] = r2;
+    }
+    const double t_init = max_time;
+    double t_max = t_init;
+    std::vector<std::pair<Int, Int>> stack{{0, 0}};
+    while (!stack.empty()) {
+        auto [i, j] = stack.back();
+        stack.pop_back();
+        if (i != j) {
+            const double a = aabb_collision_start(&M.C_box[7 * static_cast<size_t>(i)], &C_up[7 * static_cast<size_t>(i)],
+                                                  &M.C_box[7 * static_cast<size_t>(j)], &C_up[7 * static_cast<size_t>(j)]);
+            if (a * t_init >= t_max) continue;   // admissible: no contact before t_max
+        }
+        const Int Li = M.C_left[i], Lj = M.C_left[j];
+        if (Li >= 0 || Lj >= 0) {
+            const Int Ri = M.C_right[i], Rj = M.C_right[j];
+            const double si = Li >= 0 ? M.C_box[7 * static_cast<size_t>(i)] : 0.0;
+            const double sj = Lj >= 0 ? M.C_box[7 * static_cast<size_t>(j)] : 0.0;
+            if (si == sj && si > 0) {
+                if (i == j) { stack.push_back({Li, Rj}); stack.push_back({Ri, Rj}); stack.push_back({Li, Lj}); }
+                else { stack.push_back({Ri, Rj}); stack.push_back({Li, Rj}); stack.push_back({Ri, Lj}); stack.push_back({Li, Lj}); }
+            } else if (si > sj) {
+                stack.push_back({Ri, j}); stack.push_back({Li, j});
+            } else {
+                stack.push_back({i, Rj}); stack.push_back({i, Lj});
+            }
+            continue;
+        }
+        if (i == j) continue;
+        const Int pi = M.C_begin[i], pj = M.C_begin[j];
+        if (primitives_adjacent(M, pi, pj)) continue;
+        t_max = find_max_safe_step(P[pi], P[pj], t_max, TOL);
+    }
+    return std::min(t_max, t_init);
+}
+
 struct OracleHandle {
     Mesh M;
     const Mesh* obstacle = nullptr;   // not owned
@@ -2144,6 +2489,12 @@ void oracle_pair_opcounts(int dom, int far, double q, double p, int64_t* out)
         }
     }
     out[0] = g_ops.add; out[1] = g_ops.mul; out[2] = g_ops.div; out[3] = g_ops.sqrt; out[4] = g_ops.pow;
+}
+
+// SimplicialMesh::MaximumSafeStepSize(vecs, max_time, TOL) without an obstacle; vel: nV x 3
+double oracle_maximum_safe_step_size(void* h, const double* vel, double max_time, double tol)
+{
+    return maximum_safe_step_size(static_cast<OracleHandle*>(h)->M, vel, max_time, tol);
 }
 
 // moment-coordinate derivatives after collection (original order)

@@ -107,6 +107,19 @@ class SimplicialMesh:
     def ClearCache(self):
         self._cache.clear()
 
+    def MaximumSafeStepSize(self, velocities, max_time: float, TOL: float = 0.0625) -> float:
+        """SimplicialMesh::MaximumSafeStepSize (src/SimplicialMesh.hpp:441-468): the largest
+        t <= max_time for which moving every vertex by t * velocities (n_v x 3) keeps the
+        primitives without a common vertex apart (construction-time coordinates, as the
+        reference's collision tree uses)."""
+        vel = np.ascontiguousarray(velocities, dtype=np.float64)
+        if vel.shape != (self.nV, 3):
+            raise ValueError(f"velocities must be ({self.nV}, 3)")
+        t = ctypes.c_double()
+        check(_capi.load().rpb_mesh_maximum_safe_step_size(self._h, dptr(vel), float(max_time), float(TOL),
+                                                           ctypes.byref(t)), "MaximumSafeStepSize")
+        return t.value
+
     def SemiStaticUpdate(self, V, transp: bool = False):
         """New coordinates with the same tree and pair lists (src/SimplicialMesh.hpp:354-376)."""
         V = np.ascontiguousarray(V, dtype=np.float64)

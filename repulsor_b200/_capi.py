@@ -102,6 +102,7 @@ SIGNATURES = {
                                               _vp, _vp]),
     "rpb_tpm0_solve_info": (ctypes.c_int, [_vp, ctypes.POINTER(SolveInfo)]),
     "rpb_tpe0_energy_device": (ctypes.c_int, [_vp, _vp]),
+    "rpb_mesh_maximum_safe_step_size": (ctypes.c_int, [_vp, _dp, ctypes.c_double, ctypes.c_double, _dp]),
     "rpb_mesh_set_shards": (ctypes.c_int, [_vp, ctypes.c_int]),
     "rpb_mesh_shard_rows": (ctypes.c_int, [_vp, ctypes.c_int, _lp, _lp]),
     "rpb_mesh_shard_buffer_doubles": (ctypes.c_int, [_vp, _lp]),

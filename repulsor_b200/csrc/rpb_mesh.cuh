@@ -110,6 +110,7 @@ struct rpb_mesh {
     rpb::DevBuf<unsigned> done;                 // last-block counters of the two pair kernels
     int near_blocks = 0, far_blocks = 0;
     int shards = 1;                             // row shards the tiles are grouped for
+    int64_t last_step_candidates = 0;           // candidate pairs of the last MaximumSafeStepSize
     // metric: frozen Pre/Post (per primitive in tree order: sorted vertex ids, 4 x size coefficients)
     rpb::DevBuf<int> pre_cols;
     rpb::DevBuf<double> pre_vals;
