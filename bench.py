@@ -394,6 +394,21 @@ def extras(rpb, torch, with_solve):
                                           "frac": achieved / peak if peak else None, "bytes_per_product": mv_bytes,
                                           "note": "the block SpMM is bound by L1 request throughput on the "
                                                   "96-byte input gathers, not by HBM"}}}
+    # collision-free step size along the negative differential of the same mesh, scaled so
+    # that the fastest vertex moves by 5 mean edge lengths at t = 1
+    import numpy as np
+
+    Dd = rpb.TangentPointEnergy0(Q, P).Differential(M)
+    edge = float(np.linalg.norm(V[S[:, 1]] - V[S[:, 0]], axis=1).mean())
+    vel = -Dd * (5.0 * edge / max(float(np.abs(Dd).max()), 1e-300))
+    M.MaximumSafeStepSize(vel, 1.0)
+    t0 = time.perf_counter()
+    reps = 5
+    for _ in range(reps):
+        t_step = M.MaximumSafeStepSize(vel, 1.0)
+    out["step_size"] = {"workload": "icosphere level 6, velocities -dE scaled to 5 mean edge lengths, max_time 1, "
+                                    "TOL 1/16", "ms": 1e3 * (time.perf_counter() - t0) / reps, "t": t_step,
+                        "how": "host candidate traversal + GPU bisections, wall clock per call"}
     if not with_solve:
         return out
     out["solve"] = solve_extras(rpb, M, tpm, V)
@@ -456,10 +471,11 @@ def solve_extras(rpb, M, tpm, V):
 def run_flow(args):
     """Full flow step at scale: two linked tori (R=1, r=0.3, 480 x 640 grids, 1,228,800
     triangles) with an icosphere level-5 obstacle of radius 0.3 at (0, 0, 2): energy +
-    differential (TangentPointEnergy0 + TangentPointObstacleEnergy), then the metric Solve
-    of the differential to 1e-6 by learned-preconditioned flexible CG (network trained on
-    seeded icospheres, time reported separately) with the reference preconditioner as
-    fallback. One step; times are wall clock around each public call."""
+    differential (TangentPointEnergy0 + TangentPointObstacleEnergy), the metric Solve of the
+    differential to 1e-6 by learned-preconditioned flexible CG (network trained on seeded
+    icospheres, time reported separately) with the reference preconditioner as fallback,
+    and the collision-free step size along the solution (MaximumSafeStepSize). One step;
+    times are wall clock around each public call."""
     import numpy as np
     import torch
 
@@ -503,12 +519,19 @@ def run_flow(args):
     net.attach(M)
     B = D - D.mean(0)
     t = time.perf_counter()
-    tpm.Solve(M, 1.0, B, max_iter=args.flow_max_iter, tolerance=1e-6, precond=rpb.PRECOND_LEARNED, strict=False)
+    X = tpm.Solve(M, 1.0, B, max_iter=args.flow_max_iter, tolerance=1e-6, precond=rpb.PRECOND_LEARNED, strict=False)
     out["solve_s"] = time.perf_counter() - t
+    # the flow's next call: the collision-free step along the descent direction -X, scaled so
+    # that the fastest vertex moves by at most the mean edge length at t = 1
+    edge = float(np.linalg.norm(V[S[:, 1]] - V[S[:, 0]], axis=1).mean())
+    vel = -X * (edge / max(float(np.abs(X).max()), 1e-300))
+    t = time.perf_counter()
+    out["step_size"] = M.MaximumSafeStepSize(vel, 1.0)
+    out["step_size_s"] = time.perf_counter() - t
     info = tpm.SolveInfo(M)
     out["solve"] = {"iterations": info["iterations"], "fallback_iteration": info["fallback_iteration"],
                     "rel_residual": [float(x) for x in tpm.Solver_RelativeResiduals()]}
-    out["value"] = out["energy_grad_s"] + out["solve_s"]
+    out["value"] = out["energy_grad_s"] + out["solve_s"] + out["step_size_s"]
     print(json.dumps(out))
     return 0
 

@@ -198,7 +198,7 @@ rpb_status rpb_tpe0_energy_device(rpb_mesh* m, double* energy_dev);
  * such that the mesh moved by t * velocities (n_v x 3 host doubles) keeps every pair of
  * primitives without a common vertex apart, up to the relative bisection tolerance `tol`
  * (the reference's default is 0.0625). As in the reference the test uses the coordinates
- * the cluster tree was built from. An obstacle, if loaded, is not included. */
+ * the cluster tree was built from. A loaded obstacle (at rest) is included. */
 rpb_status rpb_mesh_maximum_safe_step_size(rpb_mesh* m, const double* velocities, double max_time, double tol,
                                            double* t);
 

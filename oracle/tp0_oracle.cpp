@@ -2242,12 +2242,10 @@ static bool primitives_adjacent(const Mesh& M, Int pi, Int pj)
     return false;
 }
 
-static double maximum_safe_step_size(const Mesh& M, const double* vel, double max_time, double TOL)
+// cluster boxes of a tree at max_time: leaves from the moved simplex, internal clusters merged
+static std::vector<double> moved_boxes(const Mesh& M, const std::vector<MovingSimplex>& P, double max_time)
 {
-    const Int N = M.nS, NC = M.NC;
-    std::vector<MovingSimplex> P(N);
-    for (Int i = 0; i < N; ++i) moving_simplex(M, vel, i, P[i]);
-    // cluster boxes at max_time: leaves from the moved simplex, internal clusters merged
+    const Int NC = M.NC;
     std::vector<double> lo(3 * static_cast<size_t>(NC)), hi(3 * static_cast<size_t>(NC)), C_up(7 * static_cast<size_t>(NC));
     for (Int C = NC - 1; C >= 0; --C) {
         double* l = &lo[3 * static_cast<size_t>(C)];
@@ -2278,7 +2276,48 @@ static double maximum_safe_step_size(const Mesh& M, const double* vel, double ma
         }
         bx[0] = r2;
     }
-    const double t_init = max_time;
+    return C_up;
+}
+
+static double maximum_safe_step_size(const Mesh& M, const double* vel, double max_time, double TOL,
+                                     const Mesh* Ob = nullptr)
+{
+    const Int N = M.nS;
+    std::vector<MovingSimplex> P(N);
+    for (Int i = 0; i < N; ++i) moving_simplex(M, vel, i, P[i]);
+    const std::vector<double> C_up = moved_boxes(M, P, max_time);
+    double t = max_time;
+    if (Ob) {
+        // the obstacle's collision tree first (src/SimplicialMesh.hpp:453-461): the obstacle at
+        // rest, mesh x obstacle block pairs from the roots, every leaf pair evaluated
+        std::vector<double> zero(3 * static_cast<size_t>(Ob->nV), 0.0);
+        std::vector<MovingSimplex> Q(Ob->nS);
+        for (Int i = 0; i < Ob->nS; ++i) moving_simplex(*Ob, zero.data(), i, Q[i]);
+        const std::vector<double> O_up = moved_boxes(*Ob, Q, max_time);
+        const double t_init = t;
+        double t_max = t_init;
+        std::vector<std::pair<Int, Int>> st{{0, 0}};
+        while (!st.empty()) {
+            auto [i, j] = st.back();
+            st.pop_back();
+            const double a = aabb_collision_start(&M.C_box[7 * static_cast<size_t>(i)], &C_up[7 * static_cast<size_t>(i)],
+                                                  &Ob->C_box[7 * static_cast<size_t>(j)], &O_up[7 * static_cast<size_t>(j)]);
+            if (a * t_init >= t_max) continue;
+            const Int Li = M.C_left[i], Lj = Ob->C_left[j];
+            if (Li >= 0 || Lj >= 0) {
+                const Int Ri = M.C_right[i], Rj = Ob->C_right[j];
+                const double si = Li >= 0 ? M.C_box[7 * static_cast<size_t>(i)] : 0.0;
+                const double sj = Lj >= 0 ? Ob->C_box[7 * static_cast<size_t>(j)] : 0.0;
+                if (si == sj && si > 0) { st.push_back({Ri, Rj}); st.push_back({Li, Rj}); st.push_back({Ri, Lj}); st.push_back({Li, Lj}); }
+                else if (si > sj) { st.push_back({Ri, j}); st.push_back({Li, j}); }
+                else { st.push_back({i, Rj}); st.push_back({i, Lj}); }
+                continue;
+            }
+            t_max = find_max_safe_step(P[M.C_begin[i]], Q[Ob->C_begin[j]], t_max, TOL);
+        }
+        t = std::min(t_max, t_init);
+    }
+    const double t_init = t;
     double t_max = t_init;
     std::vector<std::pair<Int, Int>> stack{{0, 0}};
     while (!stack.empty()) {
@@ -2491,10 +2530,11 @@ void oracle_pair_opcounts(int dom, int far, double q, double p, int64_t* out)
     out[0] = g_ops.add; out[1] = g_ops.mul; out[2] = g_ops.div; out[3] = g_ops.sqrt; out[4] = g_ops.pow;
 }
 
-// SimplicialMesh::MaximumSafeStepSize(vecs, max_time, TOL) without an obstacle; vel: nV x 3
+// SimplicialMesh::MaximumSafeStepSize(vecs, max_time, TOL), with the loaded obstacle if any; vel: nV x 3
 double oracle_maximum_safe_step_size(void* h, const double* vel, double max_time, double tol)
 {
-    return maximum_safe_step_size(static_cast<OracleHandle*>(h)->M, vel, max_time, tol);
+    const OracleHandle* H = static_cast<OracleHandle*>(h);
+    return maximum_safe_step_size(H->M, vel, max_time, tol, H->obstacle);
 }
 
 // moment-coordinate derivatives after collection (original order)

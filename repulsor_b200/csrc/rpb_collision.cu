@@ -291,14 +291,14 @@ double aabb_collision_start(const Box& p0, const Box& p1, const Box& q0, const B
 
 }  // namespace
 
-// Candidates and moving data on the host, the bisections on the device.
-static rpb_status safe_step(rpb_mesh* m, const double* vel, double max_time, double tol, double* t_out)
+// Moving data of every primitive of a mesh (tree order) on its construction coordinates;
+// vel = nullptr: at rest.
+static void moving_data(const rpb_mesh* m, const double* vel, std::vector<MovingData>& data)
 {
     const HostTree& T = m->tree;
-    const int N = m->N, NC = m->NC, size = m->size;
+    const int N = m->N, size = m->size;
     const double* V = m->V_frozen.data();
-    std::vector<MovingData> data(N);
-    std::vector<Box> up(NC), box(NC);
+    data.resize(N);
     for (int i = 0; i < N; ++i) {
         MovingData& d = data[i];
         const int* s = m->S_host.data() + static_cast<int64_t>(size) * T.perm[i];
@@ -307,7 +307,7 @@ static rpb_status safe_step(rpb_mesh* m, const double* vel, double max_time, dou
             double c = 0, cu = 0;
             for (int j = 0; j < size; ++j) {
                 d.x[j][k] = V[3 * static_cast<int64_t>(s[j]) + k];
-                d.u[j][k] = vel[3 * static_cast<int64_t>(s[j]) + k];
+                d.u[j][k] = vel ? vel[3 * static_cast<int64_t>(s[j]) + k] : 0.0;
                 c += d.x[j][k];
                 cu += d.u[j][k];
             }
@@ -330,7 +330,17 @@ static rpb_status safe_step(rpb_mesh* m, const double* vel, double max_time, dou
         d.v = std::sqrt(d.cu[0] * d.cu[0] + d.cu[1] * d.cu[1] + d.cu[2] * d.cu[2]);
         d.w = std::sqrt(w2);
     }
-    // cluster boxes now (construction) and at max_time (moved leaves, merged upwards)
+}
+
+// Cluster boxes of a mesh's tree now (construction) and at max_time (moved leaves, merged
+// upwards).
+static void moving_boxes(const rpb_mesh* m, const std::vector<MovingData>& data, double max_time, std::vector<Box>& box,
+                         std::vector<Box>& up)
+{
+    const HostTree& T = m->tree;
+    const int NC = m->NC, size = m->size;
+    box.resize(NC);
+    up.resize(NC);
     std::vector<double> lo(3 * static_cast<size_t>(NC)), hi(3 * static_cast<size_t>(NC));
     for (int C = NC - 1; C >= 0; --C) {
         const double* cb = &T.C_box[7 * static_cast<size_t>(C)];
@@ -363,6 +373,17 @@ static rpb_status safe_step(rpb_mesh* m, const double* vel, double max_time, dou
         }
         up[C].r2 = r2;
     }
+}
+
+// Candidates and moving data on the host, the bisections on the device.
+static rpb_status safe_step(rpb_mesh* m, const double* vel, double max_time, double tol, double* t_out)
+{
+    const HostTree& T = m->tree;
+    const int size = m->size;
+    std::vector<MovingData> data;
+    std::vector<Box> up, box;
+    moving_data(m, vel, data);
+    moving_boxes(m, data, max_time, box, up);
     auto adjacent = [&](int pi, int pj) {
         const int* a = m->S_host.data() + static_cast<int64_t>(size) * T.perm[pi];
         const int* b = m->S_host.data() + static_cast<int64_t>(size) * T.perm[pj];
@@ -396,6 +417,39 @@ static rpb_status safe_step(rpb_mesh* m, const double* vel, double max_time, dou
         if (i == j) continue;
         const int pi = T.C_begin[i], pj = T.C_begin[j];
         if (!adjacent(pi, pj)) cand.push_back(make_int2(pi, pj));
+    }
+    // the obstacle at rest (LoadUpdateVectors(nullptr) on the obstacle,
+    // src/SimplicialMesh.hpp:455-460): mesh x obstacle block pairs, the larger box split
+    // (both when equal), every leaf pair a candidate; obstacle data follow the mesh's
+    const rpb_mesh* ob = obstacle_mesh(m);
+    if (ob) {
+        std::vector<MovingData> odata;
+        std::vector<Box> obox, oup;
+        moving_data(ob, nullptr, odata);
+        moving_boxes(ob, odata, max_time, obox, oup);
+        const HostTree& O = ob->tree;
+        const int base = static_cast<int>(data.size());
+        data.insert(data.end(), odata.begin(), odata.end());
+        stack.assign(1, {0, 0});
+        while (!stack.empty()) {
+            const auto [i, j] = stack.back();
+            stack.pop_back();
+            if (aabb_collision_start(box[i], up[i], obox[j], oup[j]) >= 1.0) continue;
+            const int Li = T.C_left[i], Lj = O.C_left[j];
+            if (Li >= 0 || Lj >= 0) {
+                const int Ri = T.C_right[i], Rj = O.C_right[j];
+                const double si = Li >= 0 ? box[i].r2 : 0.0, sj = Lj >= 0 ? obox[j].r2 : 0.0;
+                if (si == sj && si > 0) {
+                    stack.push_back({Ri, Rj}); stack.push_back({Li, Rj}); stack.push_back({Ri, Lj}); stack.push_back({Li, Lj});
+                } else if (si > sj) {
+                    stack.push_back({Ri, j}); stack.push_back({Li, j});
+                } else {
+                    stack.push_back({i, Rj}); stack.push_back({i, Lj});
+                }
+                continue;
+            }
+            cand.push_back(make_int2(T.C_begin[i], base + O.C_begin[j]));
+        }
     }
     *t_out = max_time;
     if (cand.empty()) return RPB_OK;

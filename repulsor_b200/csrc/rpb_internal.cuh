@@ -13,6 +13,8 @@ namespace rpb {
 void set_error(const std::string& msg);
 TPExp make_exp(int dom, double q, double p);
 rpb_status check_exponents(double q, double p);
+// the obstacle loaded into m (rpb_mesh_load_obstacle), or null
+rpb_mesh* obstacle_mesh(const rpb_mesh* m);
 
 // n rows of 3 doubles between arrays with leading dimensions ld_dst / ld_src (host or
 // device): one contiguous copy when both are 3 (a pitched copy of 24-byte rows from

@@ -40,6 +40,8 @@ struct ObstacleState {
     int near_blocks = 0, far_blocks = 0;
 };
 
+rpb_mesh* obstacle_mesh(const rpb_mesh* m) { return m->obstacle ? m->obstacle->mesh : nullptr; }
+
 void obstacle_free(rpb_mesh* m)
 {
     if (!m->obstacle) return;

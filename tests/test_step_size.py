@@ -50,6 +50,26 @@ def test_oracle_two_spheres_known_answer():
     assert O.maximum_safe_step_size(-vel, 1.0, TOL) == 1.0          # moving apart
 
 
+def _sphere_and_obstacle():
+    """An icosphere of radius 0.5 at (-1, 0, 0) moving at unit speed towards a resting
+    obstacle icosphere of radius 0.5 at (1, 0, 0): the gap of 1 closes at t = 1."""
+    V, S = meshes.icosphere(level=2, radius=0.5, centre=(-1.0, 0.0, 0.0))
+    Vo, So = meshes.icosphere(level=2, radius=0.5, centre=(1.0, 0.0, 0.0))
+    vel = np.zeros_like(V)
+    vel[:, 0] = 1.0
+    return V, S, Vo, So, vel
+
+
+def test_oracle_obstacle_known_answer():
+    V, S, Vo, So, vel = _sphere_and_obstacle()
+    O = oracle.OracleMesh(2, V, S, threads=4)
+    Ob = oracle.OracleMesh(2, Vo, So, threads=4)
+    assert O.maximum_safe_step_size(vel, 2.0, TOL) == 2.0           # alone it moves freely
+    O.load_obstacle(Ob)
+    t = O.maximum_safe_step_size(vel, 2.0, TOL)
+    assert 1.0 * (1 - TOL) <= t <= 1.0 + 0.04
+
+
 def test_oracle_step_is_safe_and_tight_on_linked_tori():
     V, S, vel = _linked_tori()
     O = oracle.OracleMesh(2, V, S, threads=4)
@@ -58,6 +78,22 @@ def test_oracle_step_is_safe_and_tight_on_linked_tori():
     # a tighter tolerance refines the same contact from below
     t2 = O.maximum_safe_step_size(vel, 1.0, TOL / 8)
     assert t2 >= t * (1 - TOL) and abs(t2 - t) <= TOL * t2
+
+
+@pytest.mark.gpu
+def test_gpu_step_size_with_obstacle_matches_oracle():
+    import repulsor_b200 as rpb
+
+    V, S, Vo, So, vel = _sphere_and_obstacle()
+    O = oracle.OracleMesh(2, V, S, threads=4)
+    Ob = oracle.OracleMesh(2, Vo, So, threads=4)
+    O.load_obstacle(Ob)
+    M = rpb.SimplicialMesh(V, S)
+    M.LoadObstacle(rpb.SimplicialMesh(Vo, So))
+    t_ref = O.maximum_safe_step_size(vel, 2.0, TOL)
+    t = M.MaximumSafeStepSize(vel, 2.0, TOL)
+    assert abs(t - t_ref) <= TOL * max(t, t_ref), (t, t_ref)
+    assert 1.0 * (1 - TOL) <= t <= 1.04
 
 
 @pytest.mark.gpu
