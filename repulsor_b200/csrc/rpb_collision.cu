@@ -19,9 +19,11 @@
 // starts later pairs from the running minimum, so both results are safe steps that can
 // differ by up to the relative bisection tolerance.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/repulsor_b200.h"
@@ -289,6 +291,18 @@ double aabb_collision_start(const Box& p0, const Box& p1, const Box& q0, const B
     return t1 < t0 ? 1.0 : t0;
 }
 
+template <typename F>
+void parallel_for(int threads, int n, F&& f)
+{
+    threads = std::max(1, std::min(threads, n / 4096 + 1));
+    if (threads == 1) { f(0, n); return; }
+    std::vector<std::thread> th;
+    for (int t = 0; t < threads; ++t)
+        th.emplace_back([&, t] { f(static_cast<int>(static_cast<int64_t>(n) * t / threads),
+                                   static_cast<int>(static_cast<int64_t>(n) * (t + 1) / threads)); });
+    for (auto& x : th) x.join();
+}
+
 }  // namespace
 
 // Moving data of every primitive of a mesh (tree order) on its construction coordinates;
@@ -299,7 +313,8 @@ static void moving_data(const rpb_mesh* m, const double* vel, std::vector<Moving
     const int N = m->N, size = m->size;
     const double* V = m->V_frozen.data();
     data.resize(N);
-    for (int i = 0; i < N; ++i) {
+    parallel_for(std::max(1, m->settings.threads), N, [&](int i0, int i1) {
+    for (int i = i0; i < i1; ++i) {
         MovingData& d = data[i];
         const int* s = m->S_host.data() + static_cast<int64_t>(size) * T.perm[i];
         double r2 = 0;
@@ -330,6 +345,7 @@ static void moving_data(const rpb_mesh* m, const double* vel, std::vector<Moving
         d.v = std::sqrt(d.cu[0] * d.cu[0] + d.cu[1] * d.cu[1] + d.cu[2] * d.cu[2]);
         d.w = std::sqrt(w2);
     }
+    });
 }
 
 // Cluster boxes of a mesh's tree now (construction) and at max_time (moved leaves, merged
@@ -392,31 +408,59 @@ static rpb_status safe_step(rpb_mesh* m, const double* vel, double max_time, dou
                 if (a[x] == b[y]) return true;
         return false;
     };
-    // symmetric dual traversal (the reference's push order), pruned where the moving boxes
-    // cannot meet before max_time
+    // symmetric dual traversal (the reference's split rule), pruned where the moving boxes
+    // cannot meet before max_time; the top levels are expanded breadth first into
+    // independent block pairs that threads then traverse depth first
     std::vector<int2> cand;
-    std::vector<std::pair<int, int>> stack{{0, 0}};
-    while (!stack.empty()) {
-        const auto [i, j] = stack.back();
-        stack.pop_back();
-        if (i != j && aabb_collision_start(box[i], up[i], box[j], up[j]) >= 1.0) continue;
+    std::vector<std::pair<int, int>> stack;
+    auto step = [&](int i, int j, std::vector<int2>& out, std::vector<std::pair<int, int>>& push) {
+        if (i != j && aabb_collision_start(box[i], up[i], box[j], up[j]) >= 1.0) return;
         const int Li = T.C_left[i], Lj = T.C_left[j];
         if (Li >= 0 || Lj >= 0) {
             const int Ri = T.C_right[i], Rj = T.C_right[j];
             const double si = Li >= 0 ? box[i].r2 : 0.0, sj = Lj >= 0 ? box[j].r2 : 0.0;
             if (si == sj && si > 0) {
-                if (i == j) { stack.push_back({Li, Rj}); stack.push_back({Ri, Rj}); stack.push_back({Li, Lj}); }
-                else { stack.push_back({Ri, Rj}); stack.push_back({Li, Rj}); stack.push_back({Ri, Lj}); stack.push_back({Li, Lj}); }
+                if (i == j) { push.push_back({Li, Rj}); push.push_back({Ri, Rj}); push.push_back({Li, Lj}); }
+                else { push.push_back({Ri, Rj}); push.push_back({Li, Rj}); push.push_back({Ri, Lj}); push.push_back({Li, Lj}); }
             } else if (si > sj) {
-                stack.push_back({Ri, j}); stack.push_back({Li, j});
+                push.push_back({Ri, j}); push.push_back({Li, j});
             } else {
-                stack.push_back({i, Rj}); stack.push_back({i, Lj});
+                push.push_back({i, Rj}); push.push_back({i, Lj});
             }
-            continue;
+            return;
         }
-        if (i == j) continue;
+        if (i == j) return;
         const int pi = T.C_begin[i], pj = T.C_begin[j];
-        if (!adjacent(pi, pj)) cand.push_back(make_int2(pi, pj));
+        if (!adjacent(pi, pj)) out.push_back(make_int2(pi, pj));
+    };
+    {
+        const int threads = std::max(1, m->settings.threads);
+        std::vector<std::pair<int, int>> level{{0, 0}}, next;
+        while (!level.empty() && static_cast<int>(level.size()) < 64 * threads) {
+            next.clear();
+            for (const auto& [i, j] : level) step(i, j, cand, next);
+            level.swap(next);
+        }
+        std::vector<std::vector<int2>> part(level.size());
+        std::atomic<int> ticket{0};
+        auto work = [&] {
+            std::vector<std::pair<int, int>> st;
+            for (;;) {
+                const int k = ticket.fetch_add(1);
+                if (k >= static_cast<int>(level.size())) break;
+                st.assign(1, level[k]);
+                while (!st.empty()) {
+                    const auto [i, j] = st.back();
+                    st.pop_back();
+                    step(i, j, part[k], st);
+                }
+            }
+        };
+        std::vector<std::thread> th;
+        for (int t = 1; t < threads && !level.empty(); ++t) th.emplace_back(work);
+        work();
+        for (auto& x : th) x.join();
+        for (auto& p : part) cand.insert(cand.end(), p.begin(), p.end());
     }
     // the obstacle at rest (LoadUpdateVectors(nullptr) on the obstacle,
     // src/SimplicialMesh.hpp:455-460): mesh x obstacle block pairs, the larger box split
