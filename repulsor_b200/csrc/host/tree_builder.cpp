@@ -1,6 +1,8 @@
 // Host construction of the cluster tree and block cluster tree (see tree_builder.hpp).
 #include "tree_builder.hpp"
 
+#include "bct_rules.hpp"
+
 #include <algorithm>
 #include <atomic>
 #include <cmath>
@@ -171,98 +173,7 @@ void build_subtree(Splitter& sp, std::vector<Node>& nodes)
     }
 }
 
-// --- exact primitive distances (segments and triangles) ----------------------
-inline double dot(const double* a, const double* b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
-
-double segseg2(const double* a0, const double* a1, const double* b0, const double* b1)
-{
-    double u[3], v[3], w[3];
-    for (int k = 0; k < 3; ++k) { u[k] = a1[k] - a0[k]; v[k] = b1[k] - b0[k]; w[k] = a0[k] - b0[k]; }
-    const double A = dot(u, u), B = dot(u, v), C = dot(v, v), D = dot(u, w), E = dot(v, w);
-    auto eval = [&](double s, double t) {
-        double d2 = 0;
-        for (int k = 0; k < 3; ++k) { const double d = w[k] + s * u[k] - t * v[k]; d2 += d * d; }
-        return d2;
-    };
-    double best = std::numeric_limits<double>::max();
-    // interior critical point
-    const double den = A * C - B * B;
-    if (den > 0) {
-        const double s = (B * E - C * D) / den, t = (A * E - B * D) / den;
-        if (s >= 0 && s <= 1 && t >= 0 && t <= 1) best = eval(s, t);
-    }
-    // boundary: s in {0,1} with optimal t, t in {0,1} with optimal s
-    for (int e = 0; e < 2; ++e) {
-        const double s = e;
-        const double t = C > 0 ? std::clamp((B * s + E) / C, 0.0, 1.0) : 0.0;
-        best = std::min(best, eval(s, t));
-        const double t2 = e;
-        const double s2 = A > 0 ? std::clamp((B * t2 - D) / A, 0.0, 1.0) : 0.0;
-        best = std::min(best, eval(s2, t2));
-    }
-    return best;
-}
-
-double pointtri2(const double* p, const double* a, const double* b, const double* c)
-{
-    // projection onto the plane; inside test by barycentric coordinates, else edges
-    double e0[3], e1[3], d[3];
-    for (int k = 0; k < 3; ++k) { e0[k] = b[k] - a[k]; e1[k] = c[k] - a[k]; d[k] = p[k] - a[k]; }
-    const double a00 = dot(e0, e0), a01 = dot(e0, e1), a11 = dot(e1, e1);
-    const double b0 = dot(e0, d), b1 = dot(e1, d);
-    const double det = a00 * a11 - a01 * a01;
-    if (det > 0) {
-        const double s = (a11 * b0 - a01 * b1) / det, t = (a00 * b1 - a01 * b0) / det;
-        if (s >= 0 && t >= 0 && s + t <= 1) {
-            double d2 = 0;
-            for (int k = 0; k < 3; ++k) { const double x = d[k] - s * e0[k] - t * e1[k]; d2 += x * x; }
-            return d2;
-        }
-    }
-    return std::min({segseg2(p, p, a, b), segseg2(p, p, b, c), segseg2(p, p, c, a)});
-}
-
-bool segtri_hit(const double* p, const double* q, const double* a, const double* b, const double* c)
-{
-    double e0[3], e1[3], dir[3], n[3];
-    for (int k = 0; k < 3; ++k) { e0[k] = b[k] - a[k]; e1[k] = c[k] - a[k]; dir[k] = q[k] - p[k]; }
-    n[0] = e0[1] * e1[2] - e0[2] * e1[1];
-    n[1] = e0[2] * e1[0] - e0[0] * e1[2];
-    n[2] = e0[0] * e1[1] - e0[1] * e1[0];
-    const double den = dot(n, dir);
-    if (den == 0) return false;
-    double ap[3];
-    for (int k = 0; k < 3; ++k) ap[k] = a[k] - p[k];
-    const double t = dot(n, ap) / den;
-    if (t < 0 || t > 1) return false;
-    double x[3];
-    for (int k = 0; k < 3; ++k) x[k] = p[k] + t * dir[k] - a[k];
-    const double a00 = dot(e0, e0), a01 = dot(e0, e1), a11 = dot(e1, e1);
-    const double b0 = dot(e0, x), b1 = dot(e1, x);
-    const double det = a00 * a11 - a01 * a01;
-    if (det <= 0) return false;
-    const double s = (a11 * b0 - a01 * b1) / det, u = (a00 * b1 - a01 * b0) / det;
-    return s >= 0 && u >= 0 && s + u <= 1;
-}
-
-double tritri2(const double* A, const double* B)
-{
-    for (int e = 0; e < 3; ++e) {
-        const int f = (e + 1) % 3;
-        if (segtri_hit(A + 3 * e, A + 3 * f, B, B + 3, B + 6)) return 0.0;
-        if (segtri_hit(B + 3 * e, B + 3 * f, A, A + 3, A + 6)) return 0.0;
-    }
-    double best = std::numeric_limits<double>::max();
-    for (int v = 0; v < 3; ++v) {
-        best = std::min(best, pointtri2(A + 3 * v, B, B + 3, B + 6));
-        best = std::min(best, pointtri2(B + 3 * v, A, A + 3, A + 6));
-    }
-    for (int e = 0; e < 3; ++e)
-        for (int f = 0; f < 3; ++f)
-            best = std::min(best, segseg2(A + 3 * e, A + 3 * ((e + 1) % 3), B + 3 * f, B + 3 * ((f + 1) % 3)));
-    return best;
-}
-
+// --- exact primitive distances and block decisions: host/bct_rules.hpp -------------------
 // --- pair traversal --------------------------------------------------------------
 struct PairLists {
     std::vector<std::pair<int, int>> near, far, verynear, inter;
@@ -290,32 +201,16 @@ struct Traversal {
         if (adjacent(pi, pj)) { out.near.emplace_back(pi, pj); return; }
         const double* A = P.data() + static_cast<int64_t>(ps) * pi;
         const double* B = P.data() + static_cast<int64_t>(ps) * pj;
-        const double tol = std::max(A[0], B[0]);
-        // cheap separation certificate from the bounding balls
-        double cc = 0;
-        for (int k = 0; k < AMB; ++k) { const double d = A[1 + k] - B[1 + k]; cc += d * d; }
-        const double lb = std::sqrt(cc) - std::sqrt(A[0]) - std::sqrt(B[0]);
-        if (lb > 0 && near_t2 * lb * lb > tol) { out.near.emplace_back(pi, pj); return; }
-        const double d2 = (T.dom == 1) ? segseg2(A + 4, A + 7, B + 4, B + 7) : tritri2(A + 4, B + 4);
-        if (near_t2 * d2 > tol) { out.near.emplace_back(pi, pj); return; }
-        const double tol_i = std::numeric_limits<double>::epsilon() * std::min(A[0], B[0]);
-        if (near_t2 * d2 <= tol_i) out.inter.emplace_back(pi, pj);
-        else out.verynear.emplace_back(pi, pj);
+        const int cls = bct::classify_leaf(T.dom, A, B, near_t2);
+        if (cls == 0) out.near.emplace_back(pi, pj);
+        else if (cls == 1) out.verynear.emplace_back(pi, pj);
+        else out.inter.emplace_back(pi, pj);
     }
 
     bool admissible(int i, int j) const
     {
         if (i == j) return false;
-        const double* a = &T.C_box[7 * static_cast<int64_t>(i)];
-        const double* b = &T.C_box[7 * static_cast<int64_t>(j)];
-        double d2 = 0;
-        for (int k = 0; k < AMB; ++k) {
-            const double lo = std::max(a[1 + k] - a[4 + k], b[1 + k] - b[4 + k]);
-            const double hi = std::min(a[1 + k] + a[4 + k], b[1 + k] + b[4 + k]);
-            const double x = std::max(0.0, lo - hi);
-            d2 += x * x;
-        }
-        return std::max(a[0], b[0]) < far_t2 * d2;
+        return bct::boxes_admissible(&T.C_box[7 * static_cast<int64_t>(i)], &T.C_box[7 * static_cast<int64_t>(j)], far_t2);
     }
 
     // Processes one block pair; pushes children (in the reference's push order) to `next`.
@@ -593,16 +488,10 @@ struct CrossTraversal {
     {
         const double* X = PA.data() + static_cast<int64_t>(psA) * pi;
         const double* Y = PB.data() + static_cast<int64_t>(psB) * pj;
-        const double tol = std::max(X[0], Y[0]);
-        double cc = 0;
-        for (int k = 0; k < AMB; ++k) { const double d = X[1 + k] - Y[1 + k]; cc += d * d; }
-        const double lb = std::sqrt(cc) - std::sqrt(X[0]) - std::sqrt(Y[0]);
-        if (lb > 0 && near_t2 * lb * lb > tol) { out.near.emplace_back(pi, pj); return; }
-        const double d2 = (A.dom == 1) ? segseg2(X + 4, X + 7, Y + 4, Y + 7) : tritri2(X + 4, Y + 4);
-        if (near_t2 * d2 > tol) { out.near.emplace_back(pi, pj); return; }
-        const double tol_i = std::numeric_limits<double>::epsilon() * std::min(X[0], Y[0]);
-        if (near_t2 * d2 <= tol_i) out.inter.emplace_back(pi, pj);
-        else out.verynear.emplace_back(pi, pj);
+        const int cls = bct::classify_leaf(A.dom, X, Y, near_t2);
+        if (cls == 0) out.near.emplace_back(pi, pj);
+        else if (cls == 1) out.verynear.emplace_back(pi, pj);
+        else out.inter.emplace_back(pi, pj);
     }
 
     template <typename Push>

@@ -432,7 +432,7 @@ struct PairArgs {
 };
 
 constexpr int PAIR_BLOCK = 256;
-constexpr int PAIR_FLUSH = 8;   // FP32 partial sums are carried into FP64 every 8 pairs
+constexpr int PAIR_FLUSH = 16;  // FP32 partial sums are carried into FP64 every 16 pairs
 // Threads per CSR row: a row's nonzeros are strided over LANES consecutive lanes and the
 // partial sums combined by an xor-butterfly of warp shuffles (fixed order, deterministic).
 // Near rows (~60 nonzeros at theta = 0.5) take 4 lanes, far rows (~30) take 2, which puts
