@@ -289,8 +289,8 @@ void run_threads(int n, F&& f)
 
 }  // namespace
 
-std::string build_tree(int dom, const double* V, int nV, const int* S, int N, const TreeSettings& set,
-                       HostTree& T)
+std::string build_cluster_tree(int dom, const double* V, int nV, const int* S, int N, const TreeSettings& set,
+                               HostTree& T, std::vector<double>& P)
 {
     if (dom != 1 && dom != 2) return "domain dimension must be 1 or 2";
     if (nV <= 0 || N <= 0) return "empty mesh";
@@ -307,7 +307,7 @@ std::string build_tree(int dom, const double* V, int nV, const int* S, int N, co
     T.nV = nV;
     T.N = N;
     const int ps = 1 + AMB + size * AMB;
-    std::vector<double> P(static_cast<size_t>(N) * ps);
+    P.assign(static_cast<size_t>(N) * ps, 0.0);
     for (int i = 0; i < N; ++i) serialize_polytope(size, V, S + static_cast<int64_t>(size) * i, &P[static_cast<size_t>(ps) * i]);
     std::vector<int> ord(N);
     for (int i = 0; i < N; ++i) ord[i] = i;
@@ -417,6 +417,14 @@ std::string build_tree(int dom, const double* V, int nV, const int* S, int N, co
         if (T.C_left[C] < 0)
             for (int i = T.C_begin[C]; i < T.C_end[C]; ++i) T.leaf_of[i] = C;
 
+    return std::string();
+}
+
+void build_block_cluster_tree(HostTree& T, const std::vector<double>& P, const int* S, const TreeSettings& set)
+{
+    const int threads = std::max(1, set.threads);
+    const int ps = 1 + AMB + T.size * AMB;
+    const int N = T.N, NC = T.NC;
     // --- block cluster tree
     Traversal tr{T, P, S, ps, set.theta_far * set.theta_far, set.theta_near * set.theta_near};
     std::vector<std::pair<int, int>> tasks{{0, 0}};
@@ -442,6 +450,15 @@ std::string build_tree(int dom, const double* V, int nV, const int* S, int N, co
     T.far = to_pattern(NC, parts, &PairLists::far);
     T.verynear = to_pattern(N, parts, &PairLists::verynear);
     T.inter = to_pattern(N, parts, &PairLists::inter);
+}
+
+std::string build_tree(int dom, const double* V, int nV, const int* S, int N, const TreeSettings& set,
+                       HostTree& T)
+{
+    std::vector<double> P;
+    std::string err = build_cluster_tree(dom, V, nV, S, N, set, T, P);
+    if (!err.empty()) return err;
+    build_block_cluster_tree(T, P, S, set);
     return std::string();
 }
 

@@ -52,6 +52,13 @@ struct HostTree {
 std::string build_tree(int dom, const double* V, int nV, const int* S, int N, const TreeSettings& set,
                        HostTree& out);
 
+// The two halves of build_tree: the cluster tree (returns the serialized polytopes
+// [r2, centre, hull] in tree order, which the block cluster tree reads) and the block
+// cluster tree's patterns (host threads; rpb_gputree.cu computes the same on the device).
+std::string build_cluster_tree(int dom, const double* V, int nV, const int* S, int N, const TreeSettings& set,
+                               HostTree& out, std::vector<double>& P);
+void build_block_cluster_tree(HostTree& T, const std::vector<double>& P, const int* S, const TreeSettings& set);
+
 // Rectangular CSR (rows of one tree, columns of another), columns sorted.
 struct CrossPattern {
     int rows = 0;

@@ -458,16 +458,26 @@ rpb_status rpb_mesh_create(int dom_dim, int amb_dim, const double* Vh, int64_t n
     m->settings.threads = set.thread_count > 0 ? set.thread_count : std::max(1u, std::thread::hardware_concurrency());
     auto fail = [&](rpb_status st) { delete m; return st; };
 
+    if (cudaSetDevice(m->device) != cudaSuccess) { set_error("cudaSetDevice failed"); return fail(RPB_ECUDA); }
+    if (cudaStreamCreateWithFlags(&m->own_stream, cudaStreamNonBlocking) != cudaSuccess) { set_error("stream creation failed"); return fail(RPB_ECUDA); }
+    // the cluster tree on the host, the block cluster tree's traversal on the device (the
+    // host traversal if the device one fails; both give the same patterns)
     const auto t0 = std::chrono::steady_clock::now();
-    const std::string err = build_tree(dom_dim, Vh, m->nV, Sh, m->N, m->settings, m->tree);
-    if (!err.empty()) { set_error(err); return fail(RPB_EINVAL); }
+    {
+        std::vector<double> Pser;
+        const std::string err = build_cluster_tree(dom_dim, Vh, m->nV, Sh, m->N, m->settings, m->tree, Pser);
+        if (!err.empty()) { set_error(err); return fail(RPB_EINVAL); }
+        std::string derr;
+        if (!build_block_cluster_tree_device(m->tree, Pser, Sh, m->settings, m->own_stream, derr)) {
+            cudaGetLastError();
+            build_block_cluster_tree(m->tree, Pser, Sh, m->settings);
+        }
+    }
     m->build_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     m->NC = m->tree.NC;
     m->V_frozen.assign(Vh, Vh + 3 * static_cast<size_t>(m->nV));
     m->S_host.assign(Sh, Sh + static_cast<size_t>(m->size) * m->N);
 
-    if (cudaSetDevice(m->device) != cudaSuccess) { set_error("cudaSetDevice failed"); return fail(RPB_ECUDA); }
-    if (cudaStreamCreateWithFlags(&m->own_stream, cudaStreamNonBlocking) != cudaSuccess) { set_error("stream creation failed"); return fail(RPB_ECUDA); }
     if (cudaMallocHost(reinterpret_cast<void**>(&m->host_energy), 3 * sizeof(double)) != cudaSuccess) {
         set_error("pinned host allocation failed");
         return fail(RPB_ENOMEM);

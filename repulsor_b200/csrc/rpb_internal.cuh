@@ -4,6 +4,7 @@
 #include <string>
 
 #include "../../include/repulsor_b200.h"
+#include "host/tree_builder.hpp"
 #include "rpb_device.cuh"
 
 struct rpb_mesh;
@@ -13,6 +14,10 @@ namespace rpb {
 void set_error(const std::string& msg);
 TPExp make_exp(int dom, double q, double p);
 rpb_status check_exponents(double q, double p);
+// the four block-cluster-tree patterns of T on the device (rpb_gputree.cu); false with T
+// untouched and err set if the device work failed
+bool build_block_cluster_tree_device(HostTree& T, const std::vector<double>& P, const int* S, const TreeSettings& set,
+                                     cudaStream_t s, std::string& err);
 // the obstacle loaded into m (rpb_mesh_load_obstacle), or null
 rpb_mesh* obstacle_mesh(const rpb_mesh* m);
 
