@@ -283,18 +283,68 @@ __global__ void __launch_bounds__(256) k_dot3(DotArgs A)
     }
 }
 
-// x += alpha p, r -= alpha Ap with alpha = rz / (p, Ap) per active column
-__global__ void k_cg_update(int n, const double* S, double* x, double* r, const double* p, const double* Ap)
+// x += alpha p, r -= alpha Ap with alpha = rz / (p, Ap) per active column, fused with the
+// copy r_old = r (flexible CG) and the inner products (r, r) per column: grid-stride over the rows, per-block partials, the last block adds them in
+// block order (deterministic) into S[S_RR..].
+__global__ void __launch_bounds__(256) k_cg_update_rr(int n, double* S, double* x, double* r, const double* p,
+                                                      const double* Ap, double* rold, double* partials, unsigned* done)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+    double alpha[3];
+    bool act[3];
     for (int c = 0; c < 3; ++c) {
-        if (S[S_ACTIVE + c] == 0.0) continue;
+        act[c] = S[S_ACTIVE + c] != 0.0;
         const double pap = S[S_PAP + c];
-        const double alpha = pap != 0.0 ? S[S_RZ + c] / pap : 0.0;
-        const int64_t k = 3 * static_cast<int64_t>(i) + c;
-        x[k] += alpha * p[k];
-        r[k] -= alpha * Ap[k];
+        alpha[c] = pap != 0.0 ? S[S_RZ + c] / pap : 0.0;
+    }
+    double s3[3] = {0, 0, 0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        for (int c = 0; c < 3; ++c) {
+            const int64_t k = 3 * static_cast<int64_t>(i) + c;
+            double rk = r[k];
+            if (rold) rold[k] = rk;
+            if (act[c]) {
+                x[k] += alpha[c] * p[k];
+                rk -= alpha[c] * Ap[k];
+                r[k] = rk;
+            }
+            s3[c] += rk * rk;
+        }
+    __shared__ double sh[8][3];
+    __shared__ bool last;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int c = 0; c < 3; ++c) {
+        const double v = warp_sum_f64(s3[c]);
+        if (lane == 0) sh[w][c] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 3) {
+        double v = 0;
+        for (int q = 0; q < (blockDim.x >> 5); ++q) v += sh[q][threadIdx.x];
+        partials[3 * blockIdx.x + threadIdx.x] = v;
+        __threadfence();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        last = (atomicAdd(done, 1u) == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (last) {
+        __threadfence();
+        double v[3] = {0, 0, 0};
+        for (int b = threadIdx.x; b < static_cast<int>(gridDim.x); b += blockDim.x)
+            for (int c = 0; c < 3; ++c) v[c] += __ldcg(partials + 3 * b + c);
+        for (int c = 0; c < 3; ++c) {
+            const double t = warp_sum_f64(v[c]);
+            if (lane == 0) sh[w][c] = t;
+        }
+        __syncthreads();
+        if (threadIdx.x < 3) {
+            double t = 0;
+            for (int q = 0; q < (blockDim.x >> 5); ++q) t += sh[q][threadIdx.x];
+            S[S_RR + threadIdx.x] = t;
+        }
+        if (threadIdx.x == 0) *done = 0u;
     }
 }
 
@@ -316,14 +366,17 @@ __global__ void k_cg_direction(int n, const double* S, bool flexible, const doub
 
 // After an iteration: count it, and freeze the columns whose recurrence residual met the
 // tolerance (||r_c||^2 <= tol^2 ||b_c||^2), recording the iteration at which they did.
+// Also keeps rz as rz_old for the next direction update.
 __global__ void k_cg_check(double* S, double tol2)
 {
     S[S_IT] += 1.0;
-    for (int c = 0; c < 3; ++c)
+    for (int c = 0; c < 3; ++c) {
         if (S[S_ACTIVE + c] != 0.0 && S[S_RR + c] <= tol2 * S[S_BB + c]) {
             S[S_ACTIVE + c] = 0.0;
             S[S_CONV_IT + c] = S[S_IT];
         }
+        S[S_RZOLD + c] = S[S_RZ + c];
+    }
 }
 
 __global__ void k_axpby3(int n, double alpha, const double* x, double beta, double* y, int ldy)
@@ -579,11 +632,9 @@ static rpb_status cg_solve(rpb_mesh* m, double q, double p, const double* B, int
         rpb_status e;
         if ((e = metric_multiply_dev(m, q, p, 1.0, pv, 3, 0.0, Ap, 3, 7)) != RPB_OK) return e;
         if ((e = dot3(m, pv, Ap, nullptr, S + S_PAP, nullptr)) != RPB_OK) return e;
-        if (flexible) RPB_CUDA(cudaMemcpyAsync(rold, r, sizeof(double) * n3, cudaMemcpyDeviceToDevice, stream));
-        k_cg_update<<<eb, 256, 0, stream>>>(n, S, x, r, pv, Ap);
-        if ((e = dot3(m, r, r, nullptr, S + S_RR, nullptr)) != RPB_OK) return e;
+        k_cg_update_rr<<<std::min(1024, eb), 256, 0, stream>>>(n, S, x, r, pv, Ap, flexible ? rold : nullptr,
+                                                               s.partials.ptr, s.done.ptr);
         k_cg_check<<<1, 1, 0, stream>>>(S, tol2);
-        RPB_CUDA(cudaMemcpyAsync(S + S_RZOLD, S + S_RZ, 3 * sizeof(double), cudaMemcpyDeviceToDevice, stream));
         if ((e = apply_preconditioner(m, k, q, p, r, z)) != RPB_OK) return e;
         if ((e = dot3(m, z, r, flexible ? rold : nullptr, S + S_RZ, S + S_ZROLD)) != RPB_OK) return e;
         k_cg_direction<<<eb, 256, 0, stream>>>(n, S, flexible, z, pv);
