@@ -35,139 +35,176 @@ namespace rpb {
     } while (0)
 
 // ------------------------------------------------------------------------------------------
-// Level-scheduled supernodal triangular solves with 3 right-hand sides. One launch per
-// level of the supernode schedule (host/sparse_cholesky.cpp), one CTA per supernode:
-//   phase 1 (warp per row):  t_r = b_r - sum over the row's entries outside the supernode
-//                            (all written by earlier levels, i.e. earlier launches),
-//   phase 2 (warp per row):  y = D^{-1} t with the inverse of the dense diagonal block.
-// Forward: rows of L, external columns < c0, D^{-1} packed lower. Backward: rows of L^T,
-// external columns >= c1, D^{-T} packed upper. No inter-CTA waits of any kind.
+// Level-scheduled supernodal triangular solves with 3 right-hand sides. A supernode c0..c1-1
+// is solved as t = b - (its rows' entries outside the supernode) . y, then y = D^{-1} t with
+// the inverse of its dense diagonal block. Forward: rows of L, external columns < c0,
+// D^{-1} packed lower by rows. Backward: rows of L^T, external columns >= c1, D^{-T} packed
+// upper by rows. The external entries are stored apart from the diagonal blocks (ext_*),
+// so the gathers run without a branch. Every level of the supernode schedule
+// (host/sparse_cholesky.cpp) is either
+//   a warp level (all supernodes at most 32 wide, short external rows): one launch, one
+//     warp per supernode, g = 32 / pow2ceil(w) lanes per row, t passed by shuffles;
+//   a split level: two launches over the level's rows, G lanes per row (G a power of two,
+//     4..256, chosen by the host from the level's longest row): external part into t,
+//     then y = D^{-1} t.
+// No inter-CTA waits of any kind.
 // ------------------------------------------------------------------------------------------
-struct SnArgs {
-    const int* level_sn;      // supernodes of this level
+struct SnTri {
     const int* sn_begin;
-    const int64_t* rp;
-    const int* ci;
-    const double* val;
+    const int* sn_of;         // row -> supernode
+    const int64_t* ext_rp;    // row -> its entries outside its supernode
+    const int* ext_ci;
+    const double* ext_val;
     const int64_t* dinv_off;
     const double* dinv;
     const double* b;          // right-hand side, n x 3
     const int* perm_in;       // if set, row i reads b[perm_in[i]]
+    double* t;                // split levels: n x 3 scratch
     double* y;                // solution in factor order, n x 3
     double* out;              // if set, out[perm_out[i]] = y_i
     const int* perm_out;
 };
 
 constexpr int SN_BLOCK = 256;
-// widest supernode (3 x 8 bytes of shared memory per row: 24 KB at 1024)
+// widest supernode
 constexpr int kMaxSupernodeWidth = 1024;
-// levels with fewer supernodes than this are spread over their rows (two launches)
-constexpr int kSplitBelow = 64;
+// a level runs as a warp level when every external row takes at most this many
+// iterations of its lane group
+constexpr int kWarpExtIters = 8;
 
+// row r of the packed inverse diagonal block of a w-wide supernode: offset, first column, length
 template <bool LOWER>
-__global__ void __launch_bounds__(SN_BLOCK) k_sn_solve(SnArgs A)
+__device__ __forceinline__ void dense_row(int r, int w, int64_t& o, int& cb, int& len)
 {
-    extern __shared__ double t[];   // w x 3
-    const int s = A.level_sn[blockIdx.x];
-    const int c0 = A.sn_begin[s], c1 = A.sn_begin[s + 1], w = c1 - c0;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-    for (int r = warp; r < w; r += nw) {
-        const int row = c0 + r;
-        double s0 = 0, s1 = 0, s2 = 0;
-        for (int64_t k = A.rp[row] + lane; k < A.rp[row + 1]; k += 32) {
-            const int j = A.ci[k];
-            if (LOWER ? (j < c0) : (j >= c1)) {
-                const double v = A.val[k];
-                s0 += v * A.y[3 * static_cast<int64_t>(j) + 0];
-                s1 += v * A.y[3 * static_cast<int64_t>(j) + 1];
-                s2 += v * A.y[3 * static_cast<int64_t>(j) + 2];
-            }
-        }
-        s0 = warp_sum_f64(s0);
-        s1 = warp_sum_f64(s1);
-        s2 = warp_sum_f64(s2);
-        if (lane == 0) {
-            const int src = A.perm_in ? A.perm_in[row] : row;
-            t[3 * r + 0] = A.b[3 * static_cast<int64_t>(src) + 0] - s0;
-            t[3 * r + 1] = A.b[3 * static_cast<int64_t>(src) + 1] - s1;
-            t[3 * r + 2] = A.b[3 * static_cast<int64_t>(src) + 2] - s2;
-        }
-    }
-    __syncthreads();
-    const double* D = A.dinv + A.dinv_off[s];
-    for (int r = warp; r < w; r += nw) {
-        // LOWER: row r of D^{-1} holds columns 0..r; UPPER: row r of D^{-T} holds columns r..w-1
-        const int64_t o = LOWER ? static_cast<int64_t>(r) * (r + 1) / 2
-                                : static_cast<int64_t>(r) * w - static_cast<int64_t>(r) * (r - 1) / 2;
-        const int cb = LOWER ? 0 : r, len = LOWER ? r + 1 : w - r;
-        double s0 = 0, s1 = 0, s2 = 0;
-        for (int c = lane; c < len; c += 32) {
-            const double d = D[o + c];
-            const int tc = 3 * (cb + c);
-            s0 += d * t[tc + 0];
-            s1 += d * t[tc + 1];
-            s2 += d * t[tc + 2];
-        }
-        s0 = warp_sum_f64(s0);
-        s1 = warp_sum_f64(s1);
-        s2 = warp_sum_f64(s2);
-        if (lane == 0) {
-            const int row = c0 + r;
-            A.y[3 * static_cast<int64_t>(row) + 0] = s0;
-            A.y[3 * static_cast<int64_t>(row) + 1] = s1;
-            A.y[3 * static_cast<int64_t>(row) + 2] = s2;
-            if (A.out) {
-                const int dst = A.perm_out[row];
-                A.out[3 * static_cast<int64_t>(dst) + 0] = s0;
-                A.out[3 * static_cast<int64_t>(dst) + 1] = s1;
-                A.out[3 * static_cast<int64_t>(dst) + 2] = s2;
-            }
-        }
+    o = LOWER ? static_cast<int64_t>(r) * (r + 1) / 2 : static_cast<int64_t>(r) * w - static_cast<int64_t>(r) * (r - 1) / 2;
+    cb = LOWER ? 0 : r;
+    len = LOWER ? r + 1 : w - r;
+}
+
+__device__ __forceinline__ void ext_dot(const SnTri& A, int64_t k0, int64_t k1, int step, double& s0, double& s1,
+                                        double& s2)
+{
+#pragma unroll 4
+    for (int64_t k = k0; k < k1; k += step) {
+        const int j = __ldg(A.ext_ci + k);
+        const double v = __ldg(A.ext_val + k);
+        const double* yj = A.y + 3 * static_cast<int64_t>(j);
+        s0 += v * yj[0];
+        s1 += v * yj[1];
+        s2 += v * yj[2];
     }
 }
 
-// Levels with few, wide supernodes run as two launches over all their rows instead
-// (one warp per row, many CTAs): the external part into t (global), then y = D^{-1} t.
-struct SnSplitArgs {
-    const int* rows;          // rows of the level (factor order)
-    int nrows;
-    const int* sn_of;         // column -> supernode
-    const int* sn_begin;
-    const int64_t* rp;
-    const int* ci;
-    const double* val;
-    const int64_t* dinv_off;
-    const double* dinv;
-    const double* b;
-    const int* perm_in;
-    double* t;                // n x 3 scratch
-    double* y;
-    double* out;
-    const int* perm_out;
-};
-
-template <bool LOWER>
-__global__ void __launch_bounds__(SN_BLOCK) k_sn_external(SnSplitArgs A)
+// sum over aligned groups of g lanes (g a power of two, at most 32, uniform in the warp)
+__device__ __forceinline__ double lane_group_sum(double v, int g)
 {
-    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-    if (w >= A.nrows) return;
-    const int row = A.rows[w];
-    const int s = A.sn_of[row];
-    const int c0 = A.sn_begin[s], c1 = A.sn_begin[s + 1];
-    double s0 = 0, s1 = 0, s2 = 0;
-    for (int64_t k = A.rp[row] + lane; k < A.rp[row + 1]; k += 32) {
-        const int j = A.ci[k];
-        if (LOWER ? (j < c0) : (j >= c1)) {
-            const double v = A.val[k];
-            s0 += v * A.y[3 * static_cast<int64_t>(j) + 0];
-            s1 += v * A.y[3 * static_cast<int64_t>(j) + 1];
-            s2 += v * A.y[3 * static_cast<int64_t>(j) + 2];
-        }
+    for (int o = g >> 1; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// sum over aligned groups of G threads (G a power of two up to the block size, uniform in
+// the block; every thread of the block calls it); valid in the group's first thread
+__device__ __forceinline__ void block_group_sum3(double& s0, double& s1, double& s2, int G, double (*sh)[3])
+{
+    if (G <= 32) {
+        s0 = lane_group_sum(s0, G);
+        s1 = lane_group_sum(s1, G);
+        s2 = lane_group_sum(s2, G);
+        return;
     }
     s0 = warp_sum_f64(s0);
     s1 = warp_sum_f64(s1);
     s2 = warp_sum_f64(s2);
-    if (lane == 0) {
+    const int warp = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) {
+        sh[warp][0] = s0;
+        sh[warp][1] = s1;
+        sh[warp][2] = s2;
+    }
+    __syncthreads();
+    if ((threadIdx.x & (G - 1)) == 0) {
+        s0 = s1 = s2 = 0;
+        for (int q = warp; q < warp + G / 32; ++q) {
+            s0 += sh[q][0];
+            s1 += sh[q][1];
+            s2 += sh[q][2];
+        }
+    }
+}
+
+__device__ __forceinline__ void store_solution(const SnTri& A, int row, double s0, double s1, double s2)
+{
+    A.y[3 * static_cast<int64_t>(row) + 0] = s0;
+    A.y[3 * static_cast<int64_t>(row) + 1] = s1;
+    A.y[3 * static_cast<int64_t>(row) + 2] = s2;
+    if (A.out) {
+        const int dst = A.perm_out[row];
+        A.out[3 * static_cast<int64_t>(dst) + 0] = s0;
+        A.out[3 * static_cast<int64_t>(dst) + 1] = s1;
+        A.out[3 * static_cast<int64_t>(dst) + 2] = s2;
+    }
+}
+
+template <bool LOWER>
+__global__ void __launch_bounds__(SN_BLOCK) k_sn_warp(SnTri A, const int* sn_list, int nsn)
+{
+    const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (wid >= nsn) return;   // whole warps
+    const int s = sn_list[wid];
+    const int c0 = A.sn_begin[s], w = A.sn_begin[s + 1] - c0;
+    int p2 = 1;
+    while (p2 < w) p2 <<= 1;
+    const int g = 32 / p2, r = lane / g, sl = lane - r * g;
+    const bool live = r < w;
+    const int rr = live ? r : 0, row = c0 + rr;
+    double s0 = 0, s1 = 0, s2 = 0;
+    if (live) ext_dot(A, A.ext_rp[row] + sl, A.ext_rp[row + 1], g, s0, s1, s2);
+    s0 = lane_group_sum(s0, g);
+    s1 = lane_group_sum(s1, g);
+    s2 = lane_group_sum(s2, g);
+    double t0 = 0, t1 = 0, t2 = 0;
+    if (live) {
+        const int src = A.perm_in ? A.perm_in[row] : row;
+        t0 = A.b[3 * static_cast<int64_t>(src) + 0] - s0;
+        t1 = A.b[3 * static_cast<int64_t>(src) + 1] - s1;
+        t2 = A.b[3 * static_cast<int64_t>(src) + 2] - s2;
+    }
+    // y_r = sum_c Dinv[r][c] t_c; t_c lives in the lanes of row c's group
+    int64_t o;
+    int cb, len;
+    dense_row<LOWER>(rr, w, o, cb, len);
+    const double* D = A.dinv + A.dinv_off[s];
+    double a0 = 0, a1 = 0, a2 = 0;
+    for (int it = 0; it < p2; it += g) {
+        const int c = it + sl, col = cb + c;
+        const int src = (col < w ? col : 0) * g;
+        const double u0 = __shfl_sync(0xffffffffu, t0, src);
+        const double u1 = __shfl_sync(0xffffffffu, t1, src);
+        const double u2 = __shfl_sync(0xffffffffu, t2, src);
+        if (live && c < len) {
+            const double d = D[o + c];
+            a0 += d * u0;
+            a1 += d * u1;
+            a2 += d * u2;
+        }
+    }
+    a0 = lane_group_sum(a0, g);
+    a1 = lane_group_sum(a1, g);
+    a2 = lane_group_sum(a2, g);
+    if (live && sl == 0) store_solution(A, row, a0, a1, a2);
+}
+
+template <bool LOWER>
+__global__ void __launch_bounds__(SN_BLOCK) k_sn_split_ext(SnTri A, const int* rows, int nrows, int G)
+{
+    __shared__ double sh[SN_BLOCK / 32][3];
+    const int q = (blockIdx.x * blockDim.x + threadIdx.x) / G, sl = threadIdx.x & (G - 1);
+    const bool live = q < nrows;
+    const int row = live ? rows[q] : 0;
+    double s0 = 0, s1 = 0, s2 = 0;
+    if (live) ext_dot(A, A.ext_rp[row] + sl, A.ext_rp[row + 1], G, s0, s1, s2);
+    block_group_sum3(s0, s1, s2, G, sh);
+    if (live && sl == 0) {
         const int src = A.perm_in ? A.perm_in[row] : row;
         A.t[3 * static_cast<int64_t>(row) + 0] = A.b[3 * static_cast<int64_t>(src) + 0] - s0;
         A.t[3 * static_cast<int64_t>(row) + 1] = A.b[3 * static_cast<int64_t>(src) + 1] - s1;
@@ -176,39 +213,31 @@ __global__ void __launch_bounds__(SN_BLOCK) k_sn_external(SnSplitArgs A)
 }
 
 template <bool LOWER>
-__global__ void __launch_bounds__(SN_BLOCK) k_sn_dense(SnSplitArgs A)
+__global__ void __launch_bounds__(SN_BLOCK) k_sn_split_dense(SnTri A, const int* rows, int nrows, int G)
 {
-    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-    if (w >= A.nrows) return;
-    const int row = A.rows[w];
-    const int s = A.sn_of[row];
-    const int c0 = A.sn_begin[s], wd = A.sn_begin[s + 1] - c0, r = row - c0;
-    const double* D = A.dinv + A.dinv_off[s];
-    const int64_t o = LOWER ? static_cast<int64_t>(r) * (r + 1) / 2
-                            : static_cast<int64_t>(r) * wd - static_cast<int64_t>(r) * (r - 1) / 2;
-    const int cb = LOWER ? 0 : r, len = LOWER ? r + 1 : wd - r;
+    __shared__ double sh[SN_BLOCK / 32][3];
+    const int q = (blockIdx.x * blockDim.x + threadIdx.x) / G, sl = threadIdx.x & (G - 1);
+    const bool live = q < nrows;
+    const int row = live ? rows[q] : 0;
     double s0 = 0, s1 = 0, s2 = 0;
-    for (int c = lane; c < len; c += 32) {
-        const double d = D[o + c];
-        const int64_t tc = 3 * static_cast<int64_t>(c0 + cb + c);
-        s0 += d * A.t[tc + 0];
-        s1 += d * A.t[tc + 1];
-        s2 += d * A.t[tc + 2];
-    }
-    s0 = warp_sum_f64(s0);
-    s1 = warp_sum_f64(s1);
-    s2 = warp_sum_f64(s2);
-    if (lane == 0) {
-        A.y[3 * static_cast<int64_t>(row) + 0] = s0;
-        A.y[3 * static_cast<int64_t>(row) + 1] = s1;
-        A.y[3 * static_cast<int64_t>(row) + 2] = s2;
-        if (A.out) {
-            const int dst = A.perm_out[row];
-            A.out[3 * static_cast<int64_t>(dst) + 0] = s0;
-            A.out[3 * static_cast<int64_t>(dst) + 1] = s1;
-            A.out[3 * static_cast<int64_t>(dst) + 2] = s2;
+    if (live) {
+        const int s = A.sn_of[row];
+        const int c0 = A.sn_begin[s], w = A.sn_begin[s + 1] - c0;
+        int64_t o;
+        int cb, len;
+        dense_row<LOWER>(row - c0, w, o, cb, len);
+        const double* D = A.dinv + A.dinv_off[s] + o;
+        const double* t = A.t + 3 * static_cast<int64_t>(c0 + cb);
+#pragma unroll 4
+        for (int c = sl; c < len; c += G) {
+            const double d = D[c];
+            s0 += d * t[3 * c + 0];
+            s1 += d * t[3 * c + 1];
+            s2 += d * t[3 * c + 2];
         }
     }
+    block_group_sum3(s0, s1, s2, G, sh);
+    if (live && sl == 0) store_solution(A, row, s0, s1, s2);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -442,105 +471,139 @@ static rpb_status ensure_h1(rpb_mesh* m)
     const std::string serr = supernodal_schedule(F, kMaxSupernodeWidth, SS);
     if (!serr.empty()) { set_error(serr); return RPB_EINVAL; }
     s.sn_levels_fwd = SS.fwd_levels();
-    s.sn_levels_bwd = SS.bwd_levels();
-    s.fwd_level_ptr = SS.fwd_level_ptr;
-    s.bwd_level_ptr = SS.bwd_level_ptr;
-    s.fwd_level_width = SS.fwd_level_width;
-    s.bwd_level_width = SS.bwd_level_width;
     cudaStream_t st = m->stream;
     auto up = [st](auto& dst, const auto& src) -> cudaError_t {
         cudaError_t e = dst.alloc(src.size());
         if (e != cudaSuccess) return e;
         return cudaMemcpyAsync(dst.ptr, src.data(), dst.bytes(), cudaMemcpyHostToDevice, st);
     };
-    RPB_CUDA(up(s.lo_rp, F.lower_rp));
-    RPB_CUDA(up(s.lo_ci, F.lower_ci));
-    RPB_CUDA(up(s.lo_val, F.lower_val));
-    RPB_CUDA(up(s.up_rp, F.upper_rp));
-    RPB_CUDA(up(s.up_ci, F.upper_ci));
-    RPB_CUDA(up(s.up_val, F.upper_val));
-    RPB_CUDA(up(s.perm, F.perm));
-    RPB_CUDA(up(s.sn_begin, SS.sn_begin));
-    RPB_CUDA(up(s.fwd_level_sn, SS.fwd_level_sn));
-    RPB_CUDA(up(s.bwd_level_sn, SS.bwd_level_sn));
-    RPB_CUDA(up(s.dinv_off, SS.dinv_off));
-    RPB_CUDA(up(s.dinv, SS.dinv));
-    RPB_CUDA(up(s.dinvT, SS.dinvT));
-    // levels with fewer supernodes than kSplitBelow run split over their rows
-    std::vector<int> sn_of(m->nV);
+    const int n = m->nV;
+    std::vector<int> sn_of(n);
     for (int sn = 0; sn < SS.nsn; ++sn)
         for (int c = SS.sn_begin[sn]; c < SS.sn_begin[sn + 1]; ++c) sn_of[c] = sn;
-    auto split_rows = [&](const std::vector<int>& lptr, const std::vector<int>& lsn, std::vector<int>& rptr,
-                          std::vector<int>& rows) {
-        const int L = static_cast<int>(lptr.size()) - 1;
-        rptr.assign(static_cast<size_t>(L) + 1, 0);
-        rows.clear();
-        for (int l = 0; l < L; ++l) {
-            if (lptr[l + 1] - lptr[l] < kSplitBelow)
-                for (int q = lptr[l]; q < lptr[l + 1]; ++q)
-                    for (int c = SS.sn_begin[lsn[q]]; c < SS.sn_begin[lsn[q] + 1]; ++c) rows.push_back(c);
-            rptr[l + 1] = static_cast<int>(rows.size());
-        }
+    auto pow2ceil = [](int64_t v) {
+        int p = 1;
+        while (p < v) p <<= 1;
+        return p;
     };
-    std::vector<int> frows, brows;
-    split_rows(SS.fwd_level_ptr, SS.fwd_level_sn, s.fwd_split_ptr, frows);
-    split_rows(SS.bwd_level_ptr, SS.bwd_level_sn, s.bwd_split_ptr, brows);
+    for (int d = 0; d < 2; ++d) {
+        const bool lower = d == 0;
+        const std::vector<int64_t>& rp = lower ? F.lower_rp : F.upper_rp;
+        const std::vector<int>& ci = lower ? F.lower_ci : F.upper_ci;
+        const std::vector<double>& val = lower ? F.lower_val : F.upper_val;
+        // each row's entries outside its own supernode
+        std::vector<int64_t> xrp(static_cast<size_t>(n) + 1, 0);
+        std::vector<int> xci;
+        std::vector<double> xval;
+        xci.reserve(ci.size());
+        xval.reserve(ci.size());
+        for (int r = 0; r < n; ++r) {
+            const int c0 = SS.sn_begin[sn_of[r]], c1 = SS.sn_begin[sn_of[r] + 1];
+            for (int64_t k = rp[r]; k < rp[r + 1]; ++k) {
+                const int j = ci[k];
+                if (lower ? (j < c0) : (j >= c1)) {
+                    xci.push_back(j);
+                    xval.push_back(val[k]);
+                }
+            }
+            xrp[r + 1] = static_cast<int64_t>(xci.size());
+        }
+        // level plans
+        const std::vector<int>& lptr = lower ? SS.fwd_level_ptr : SS.bwd_level_ptr;
+        const std::vector<int>& lsn = lower ? SS.fwd_level_sn : SS.bwd_level_sn;
+        Solver::Direction& D = s.dir[d];
+        D.levels.clear();
+        std::vector<int> sn_list, row_list;
+        for (size_t l = 0; l + 1 < lptr.size(); ++l) {
+            bool warp = true;
+            int maxw = 0;
+            int64_t maxext = 0;
+            for (int q = lptr[l]; q < lptr[l + 1]; ++q) {
+                const int sn = lsn[q], c0 = SS.sn_begin[sn], w = SS.sn_begin[sn + 1] - c0;
+                maxw = std::max(maxw, w);
+                const int g = w <= 32 ? 32 / pow2ceil(w) : 1;
+                for (int r = c0; r < c0 + w; ++r) {
+                    const int64_t len = xrp[r + 1] - xrp[r];
+                    maxext = std::max(maxext, len);
+                    if (w > 32 || (len + g - 1) / g > kWarpExtIters) warp = false;
+                }
+            }
+            Solver::Level L;
+            L.warp = warp;
+            if (warp) {
+                L.first = static_cast<int>(sn_list.size());
+                for (int q = lptr[l]; q < lptr[l + 1]; ++q) sn_list.push_back(lsn[q]);
+                L.count = static_cast<int>(sn_list.size()) - L.first;
+            } else {
+                L.first = static_cast<int>(row_list.size());
+                for (int q = lptr[l]; q < lptr[l + 1]; ++q)
+                    for (int c = SS.sn_begin[lsn[q]]; c < SS.sn_begin[lsn[q] + 1]; ++c) row_list.push_back(c);
+                L.count = static_cast<int>(row_list.size()) - L.first;
+                L.g_ext = std::min(SN_BLOCK, std::max(4, pow2ceil((maxext + 3) / 4)));
+                L.g_dense = std::min(SN_BLOCK, std::max(4, pow2ceil((maxw + 3) / 4)));
+            }
+            D.levels.push_back(L);
+        }
+        RPB_CUDA(up(D.ext_rp, xrp));
+        RPB_CUDA(up(D.ext_ci, xci));
+        RPB_CUDA(up(D.ext_val, xval));
+        RPB_CUDA(up(D.sn_list, sn_list));
+        RPB_CUDA(up(D.row_list, row_list));
+        RPB_CUDA(up(D.dinv, lower ? SS.dinv : SS.dinvT));
+        // the copies read pageable host vectors that go out of scope
+        RPB_CUDA(cudaStreamSynchronize(st));
+    }
+    RPB_CUDA(up(s.perm, F.perm));
+    RPB_CUDA(up(s.sn_begin, SS.sn_begin));
+    RPB_CUDA(up(s.dinv_off, SS.dinv_off));
     RPB_CUDA(up(s.sn_of, sn_of));
-    RPB_CUDA(up(s.fwd_split_rows, frows));
-    RPB_CUDA(up(s.bwd_split_rows, brows));
-    RPB_CUDA(s.tri.alloc(3 * static_cast<size_t>(m->nV)));
-    RPB_CUDA(s.tmp.alloc(3 * static_cast<size_t>(m->nV)));
-    RPB_CUDA(s.tbuf.alloc(3 * static_cast<size_t>(m->nV)));
+    RPB_CUDA(s.tri.alloc(3 * static_cast<size_t>(n)));
+    RPB_CUDA(s.tmp.alloc(3 * static_cast<size_t>(n)));
+    RPB_CUDA(s.tbuf.alloc(3 * static_cast<size_t>(n)));
     RPB_CUDA(cudaStreamSynchronize(st));
     s.h1_version = m->geometry_version;
     return RPB_OK;
 }
 
 // out = H1^{-1} b (b, out: n x 3 contiguous, device): forward levels on L, backward
-// levels on L^T, one launch per level
+// levels on L^T, one or two launches per level
 static rpb_status h1_solve(rpb_mesh* m, const double* b, double* out)
 {
     Solver& s = *m->solver;
-    SnArgs A;
-    A.sn_begin = s.sn_begin.ptr; A.dinv_off = s.dinv_off.ptr;
-    A.rp = s.lo_rp.ptr; A.ci = s.lo_ci.ptr; A.val = s.lo_val.ptr; A.dinv = s.dinv.ptr;
-    A.b = b; A.perm_in = s.perm.ptr; A.y = s.tri.ptr; A.out = nullptr; A.perm_out = nullptr;
-    SnSplitArgs P;
-    P.sn_of = s.sn_of.ptr; P.sn_begin = s.sn_begin.ptr; P.dinv_off = s.dinv_off.ptr; P.t = s.tbuf.ptr;
-    auto level = [&](const SnArgs& a, const int* level_sn, int nsn, int width, const int* rows, int nrows, bool lower) {
-        if (nrows > 0) {
-            P.rows = rows; P.nrows = nrows;
-            P.rp = a.rp; P.ci = a.ci; P.val = a.val; P.dinv = a.dinv;
-            P.b = a.b; P.perm_in = a.perm_in; P.y = a.y; P.out = a.out; P.perm_out = a.perm_out;
-            const int grid = (nrows + SN_BLOCK / 32 - 1) / (SN_BLOCK / 32);
-            if (lower) {
-                k_sn_external<true><<<grid, SN_BLOCK, 0, m->stream>>>(P);
-                k_sn_dense<true><<<grid, SN_BLOCK, 0, m->stream>>>(P);
-            } else {
-                k_sn_external<false><<<grid, SN_BLOCK, 0, m->stream>>>(P);
-                k_sn_dense<false><<<grid, SN_BLOCK, 0, m->stream>>>(P);
-            }
-            return;
+    cudaStream_t st = m->stream;
+    for (int d = 0; d < 2; ++d) {
+        const bool lower = d == 0;
+        const Solver::Direction& D = s.dir[d];
+        SnTri A;
+        A.sn_begin = s.sn_begin.ptr; A.sn_of = s.sn_of.ptr; A.dinv_off = s.dinv_off.ptr;
+        A.ext_rp = D.ext_rp.ptr; A.ext_ci = D.ext_ci.ptr; A.ext_val = D.ext_val.ptr; A.dinv = D.dinv.ptr;
+        A.t = s.tbuf.ptr;
+        if (lower) {
+            A.b = b; A.perm_in = s.perm.ptr; A.y = s.tri.ptr; A.out = nullptr; A.perm_out = nullptr;
+        } else {
+            A.b = s.tri.ptr; A.perm_in = nullptr; A.y = s.tmp.ptr; A.out = out; A.perm_out = s.perm.ptr;
         }
-        SnArgs a2 = a;
-        a2.level_sn = level_sn;
-        const size_t smem = 3 * sizeof(double) * static_cast<size_t>(width);
-        if (lower) k_sn_solve<true><<<nsn, SN_BLOCK, smem, m->stream>>>(a2);
-        else k_sn_solve<false><<<nsn, SN_BLOCK, smem, m->stream>>>(a2);
-    };
-    for (int l = 0; l < s.sn_levels_fwd; ++l)
-        level(A, s.fwd_level_sn.ptr + s.fwd_level_ptr[l], s.fwd_level_ptr[l + 1] - s.fwd_level_ptr[l],
-              s.fwd_level_width[l], s.fwd_split_rows.ptr + s.fwd_split_ptr[l],
-              s.fwd_split_ptr[l + 1] - s.fwd_split_ptr[l], true);
-    RPB_CUDA(cudaGetLastError());
-    SnArgs U = A;
-    U.rp = s.up_rp.ptr; U.ci = s.up_ci.ptr; U.val = s.up_val.ptr; U.dinv = s.dinvT.ptr;
-    U.b = s.tri.ptr; U.perm_in = nullptr; U.y = s.tmp.ptr; U.out = out; U.perm_out = s.perm.ptr;
-    for (int l = 0; l < s.sn_levels_bwd; ++l)
-        level(U, s.bwd_level_sn.ptr + s.bwd_level_ptr[l], s.bwd_level_ptr[l + 1] - s.bwd_level_ptr[l],
-              s.bwd_level_width[l], s.bwd_split_rows.ptr + s.bwd_split_ptr[l],
-              s.bwd_split_ptr[l + 1] - s.bwd_split_ptr[l], false);
-    RPB_CUDA(cudaGetLastError());
+        for (const Solver::Level& L : D.levels) {
+            if (L.warp) {
+                const int grid = (L.count + SN_BLOCK / 32 - 1) / (SN_BLOCK / 32);
+                const int* list = D.sn_list.ptr + L.first;
+                if (lower) k_sn_warp<true><<<grid, SN_BLOCK, 0, st>>>(A, list, L.count);
+                else k_sn_warp<false><<<grid, SN_BLOCK, 0, st>>>(A, list, L.count);
+            } else {
+                const int* rows = D.row_list.ptr + L.first;
+                const int ge = static_cast<int>((static_cast<int64_t>(L.count) * L.g_ext + SN_BLOCK - 1) / SN_BLOCK);
+                const int gd = static_cast<int>((static_cast<int64_t>(L.count) * L.g_dense + SN_BLOCK - 1) / SN_BLOCK);
+                if (lower) {
+                    k_sn_split_ext<true><<<ge, SN_BLOCK, 0, st>>>(A, rows, L.count, L.g_ext);
+                    k_sn_split_dense<true><<<gd, SN_BLOCK, 0, st>>>(A, rows, L.count, L.g_dense);
+                } else {
+                    k_sn_split_ext<false><<<ge, SN_BLOCK, 0, st>>>(A, rows, L.count, L.g_ext);
+                    k_sn_split_dense<false><<<gd, SN_BLOCK, 0, st>>>(A, rows, L.count, L.g_dense);
+                }
+            }
+        }
+        RPB_CUDA(cudaGetLastError());
+    }
     return RPB_OK;
 }
 

@@ -21,12 +21,24 @@ struct Solver {
     // H1 Cholesky factor (reference preconditioner) and its supernodal level schedule
     int64_t h1_version = -1;
     std::vector<int> nd_perm;
-    DevBuf<int64_t> lo_rp, up_rp, dinv_off;
-    DevBuf<int> lo_ci, up_ci, perm, sn_begin, fwd_level_sn, bwd_level_sn, sn_of, fwd_split_rows, bwd_split_rows;
-    DevBuf<double> lo_val, up_val, dinv, dinvT, tri, tmp, tbuf;
-    int sn_levels_fwd = 0, sn_levels_bwd = 0;
-    std::vector<int> fwd_level_ptr, bwd_level_ptr, fwd_level_width, bwd_level_width;
-    std::vector<int> fwd_split_ptr, bwd_split_ptr;   // per level: rows of split levels (empty range: fused)
+    // one launch plan per level: a warp level (sn_list[first .. first + count)) or a split
+    // level (row_list[first .. first + count), G lanes per row for the external part and
+    // for the diagonal block)
+    struct Level {
+        bool warp = true;
+        int first = 0, count = 0, g_ext = 32, g_dense = 32;
+    };
+    // per direction (0: forward on L, 1: backward on L^T)
+    struct Direction {
+        DevBuf<int64_t> ext_rp;
+        DevBuf<int> ext_ci, sn_list, row_list;
+        DevBuf<double> ext_val, dinv;
+        std::vector<Level> levels;
+    } dir[2];
+    DevBuf<int64_t> dinv_off;
+    DevBuf<int> perm, sn_begin, sn_of;
+    DevBuf<double> tri, tmp, tbuf;
+    int sn_levels_fwd = 0;
     double factor_seconds = 0;
     int64_t factor_nnz = 0;
     // statistics of the last Solve
