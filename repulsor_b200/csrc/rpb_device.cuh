@@ -8,6 +8,32 @@ namespace rpb {
 
 constexpr int WARP = 32;
 
+// Programmatic dependent launch (sm_90+). A kernel launched with launch_pdl may start while
+// its predecessor in the stream still runs: it reads only data that no kernel writes
+// (patterns, offsets, plans) before pdl_wait(), which returns once the predecessor has
+// completed and its writes are visible; pdl_launch_dependents() then lets the next
+// kernel of the stream start its own prologue. Without the launch attribute both are
+// no-ops.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t stream,
+                              Args... args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
+
 // Pair data of a primitive: barycentre and unit normal (triangles) or unit tangent
 // (edges), weight a (all FP64) and diameter. The normal projector is P = n n^T
 // (triangles) or I - t t^T (edges); keeping n/t in FP64 lets v^T P v be formed

@@ -157,8 +157,12 @@ __global__ void __launch_bounds__(SN_BLOCK) k_sn_warp(SnTri A, const int* sn_lis
     const int g = 32 / p2, r = lane / g, sl = lane - r * g;
     const bool live = r < w;
     const int rr = live ? r : 0, row = c0 + rr;
+    const int64_t k0 = A.ext_rp[row] + sl, k1 = A.ext_rp[row + 1];
+    const double* D = A.dinv + A.dinv_off[s];
+    pdl_wait();
+    pdl_launch_dependents();
     double s0 = 0, s1 = 0, s2 = 0;
-    if (live) ext_dot(A, A.ext_rp[row] + sl, A.ext_rp[row + 1], g, s0, s1, s2);
+    if (live) ext_dot(A, k0, k1, g, s0, s1, s2);
     s0 = lane_group_sum(s0, g);
     s1 = lane_group_sum(s1, g);
     s2 = lane_group_sum(s2, g);
@@ -173,7 +177,6 @@ __global__ void __launch_bounds__(SN_BLOCK) k_sn_warp(SnTri A, const int* sn_lis
     int64_t o;
     int cb, len;
     dense_row<LOWER>(rr, w, o, cb, len);
-    const double* D = A.dinv + A.dinv_off[s];
     double a0 = 0, a1 = 0, a2 = 0;
     for (int it = 0; it < p2; it += g) {
         const int c = it + sl, col = cb + c;
@@ -201,8 +204,11 @@ __global__ void __launch_bounds__(SN_BLOCK) k_sn_split_ext(SnTri A, const int* r
     const int q = (blockIdx.x * blockDim.x + threadIdx.x) / G, sl = threadIdx.x & (G - 1);
     const bool live = q < nrows;
     const int row = live ? rows[q] : 0;
+    const int64_t k0 = A.ext_rp[row] + sl, k1 = A.ext_rp[row + 1];
+    pdl_wait();
+    pdl_launch_dependents();
     double s0 = 0, s1 = 0, s2 = 0;
-    if (live) ext_dot(A, A.ext_rp[row] + sl, A.ext_rp[row + 1], G, s0, s1, s2);
+    if (live) ext_dot(A, k0, k1, G, s0, s1, s2);
     block_group_sum3(s0, s1, s2, G, sh);
     if (live && sl == 0) {
         const int src = A.perm_in ? A.perm_in[row] : row;
@@ -219,14 +225,16 @@ __global__ void __launch_bounds__(SN_BLOCK) k_sn_split_dense(SnTri A, const int*
     const int q = (blockIdx.x * blockDim.x + threadIdx.x) / G, sl = threadIdx.x & (G - 1);
     const bool live = q < nrows;
     const int row = live ? rows[q] : 0;
+    const int s = A.sn_of[row];
+    const int c0 = A.sn_begin[s], w = A.sn_begin[s + 1] - c0;
+    int64_t o;
+    int cb, len;
+    dense_row<LOWER>(row - c0, w, o, cb, len);
+    const double* D = A.dinv + A.dinv_off[s] + o;
+    pdl_wait();
+    pdl_launch_dependents();
     double s0 = 0, s1 = 0, s2 = 0;
     if (live) {
-        const int s = A.sn_of[row];
-        const int c0 = A.sn_begin[s], w = A.sn_begin[s + 1] - c0;
-        int64_t o;
-        int cb, len;
-        dense_row<LOWER>(row - c0, w, o, cb, len);
-        const double* D = A.dinv + A.dinv_off[s] + o;
         const double* t = A.t + 3 * static_cast<int64_t>(c0 + cb);
 #pragma unroll 4
         for (int c = sl; c < len; c += G) {
@@ -587,19 +595,15 @@ static rpb_status h1_solve(rpb_mesh* m, const double* b, double* out)
             if (L.warp) {
                 const int grid = (L.count + SN_BLOCK / 32 - 1) / (SN_BLOCK / 32);
                 const int* list = D.sn_list.ptr + L.first;
-                if (lower) k_sn_warp<true><<<grid, SN_BLOCK, 0, st>>>(A, list, L.count);
-                else k_sn_warp<false><<<grid, SN_BLOCK, 0, st>>>(A, list, L.count);
+                RPB_CUDA(launch_pdl(lower ? k_sn_warp<true> : k_sn_warp<false>, grid, SN_BLOCK, 0, st, A, list, L.count));
             } else {
                 const int* rows = D.row_list.ptr + L.first;
                 const int ge = static_cast<int>((static_cast<int64_t>(L.count) * L.g_ext + SN_BLOCK - 1) / SN_BLOCK);
                 const int gd = static_cast<int>((static_cast<int64_t>(L.count) * L.g_dense + SN_BLOCK - 1) / SN_BLOCK);
-                if (lower) {
-                    k_sn_split_ext<true><<<ge, SN_BLOCK, 0, st>>>(A, rows, L.count, L.g_ext);
-                    k_sn_split_dense<true><<<gd, SN_BLOCK, 0, st>>>(A, rows, L.count, L.g_dense);
-                } else {
-                    k_sn_split_ext<false><<<ge, SN_BLOCK, 0, st>>>(A, rows, L.count, L.g_ext);
-                    k_sn_split_dense<false><<<gd, SN_BLOCK, 0, st>>>(A, rows, L.count, L.g_dense);
-                }
+                RPB_CUDA(launch_pdl(lower ? k_sn_split_ext<true> : k_sn_split_ext<false>, ge, SN_BLOCK, 0, st, A, rows,
+                                    L.count, L.g_ext));
+                RPB_CUDA(launch_pdl(lower ? k_sn_split_dense<true> : k_sn_split_dense<false>, gd, SN_BLOCK, 0, st, A,
+                                    rows, L.count, L.g_dense));
             }
         }
         RPB_CUDA(cudaGetLastError());
