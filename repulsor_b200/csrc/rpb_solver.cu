@@ -95,6 +95,42 @@ __device__ __forceinline__ void ext_dot(const SnTri& A, int64_t k0, int64_t k1, 
     }
 }
 
+// The first PRE external entries k0, k0 + step, ... < k1 of a row, loaded before pdl_wait()
+// (pattern and values are fixed during a solve); only the gathers of y wait for the
+// predecessor.
+template <int PRE>
+struct ExtPre {
+    int j[PRE];
+    double v[PRE];
+};
+
+template <int PRE>
+__device__ __forceinline__ void ext_preload(const SnTri& A, int64_t k0, int64_t k1, int step, ExtPre<PRE>& e)
+{
+#pragma unroll
+    for (int i = 0; i < PRE; ++i) {
+        const int64_t k = k0 + static_cast<int64_t>(i) * step;
+        const bool in = k < k1;
+        e.j[i] = in ? __ldg(A.ext_ci + k) : -1;
+        e.v[i] = in ? __ldg(A.ext_val + k) : 0.0;
+    }
+}
+
+template <int PRE>
+__device__ __forceinline__ void ext_finish(const SnTri& A, const ExtPre<PRE>& e, int64_t k0, int64_t k1, int step,
+                                           double& s0, double& s1, double& s2)
+{
+#pragma unroll
+    for (int i = 0; i < PRE; ++i)
+        if (e.j[i] >= 0) {
+            const double* yj = A.y + 3 * static_cast<int64_t>(e.j[i]);
+            s0 += e.v[i] * yj[0];
+            s1 += e.v[i] * yj[1];
+            s2 += e.v[i] * yj[2];
+        }
+    ext_dot(A, k0 + static_cast<int64_t>(PRE) * step, k1, step, s0, s1, s2);
+}
+
 // sum over aligned groups of g lanes (g a power of two, at most 32, uniform in the warp)
 __device__ __forceinline__ double lane_group_sum(double v, int g)
 {
@@ -157,12 +193,25 @@ __global__ void __launch_bounds__(SN_BLOCK) k_sn_warp(SnTri A, const int* sn_lis
     const int g = 32 / p2, r = lane / g, sl = lane - r * g;
     const bool live = r < w;
     const int rr = live ? r : 0, row = c0 + rr;
-    const int64_t k0 = A.ext_rp[row] + sl, k1 = A.ext_rp[row + 1];
+    const int64_t k0 = A.ext_rp[row] + sl, k1 = live ? A.ext_rp[row + 1] : k0;
+    ExtPre<kWarpExtIters> e;
+    ext_preload(A, k0, k1, g, e);
+    // the first kDensePre entries of this lane's part of row r of the inverse diagonal block
+    constexpr int kDensePre = 8;
     const double* D = A.dinv + A.dinv_off[s];
+    int64_t o;
+    int cb, len;
+    dense_row<LOWER>(rr, w, o, cb, len);
+    double dp[kDensePre];
+#pragma unroll
+    for (int i = 0; i < kDensePre; ++i) {
+        const int c = i * g + sl;
+        dp[i] = (live && c < len) ? __ldg(D + o + c) : 0.0;
+    }
     pdl_wait();
     pdl_launch_dependents();
     double s0 = 0, s1 = 0, s2 = 0;
-    if (live) ext_dot(A, k0, k1, g, s0, s1, s2);
+    ext_finish(A, e, k0, k1, g, s0, s1, s2);
     s0 = lane_group_sum(s0, g);
     s1 = lane_group_sum(s1, g);
     s2 = lane_group_sum(s2, g);
@@ -174,11 +223,20 @@ __global__ void __launch_bounds__(SN_BLOCK) k_sn_warp(SnTri A, const int* sn_lis
         t2 = A.b[3 * static_cast<int64_t>(src) + 2] - s2;
     }
     // y_r = sum_c Dinv[r][c] t_c; t_c lives in the lanes of row c's group
-    int64_t o;
-    int cb, len;
-    dense_row<LOWER>(rr, w, o, cb, len);
     double a0 = 0, a1 = 0, a2 = 0;
-    for (int it = 0; it < p2; it += g) {
+#pragma unroll
+    for (int i = 0; i < kDensePre; ++i) {
+        if (i * g >= p2) break;   // warp-uniform
+        const int col = cb + i * g + sl;
+        const int src = (col < w ? col : 0) * g;
+        const double u0 = __shfl_sync(0xffffffffu, t0, src);
+        const double u1 = __shfl_sync(0xffffffffu, t1, src);
+        const double u2 = __shfl_sync(0xffffffffu, t2, src);
+        a0 += dp[i] * u0;
+        a1 += dp[i] * u1;
+        a2 += dp[i] * u2;
+    }
+    for (int it = kDensePre * g; it < p2; it += g) {
         const int c = it + sl, col = cb + c;
         const int src = (col < w ? col : 0) * g;
         const double u0 = __shfl_sync(0xffffffffu, t0, src);
@@ -204,11 +262,13 @@ __global__ void __launch_bounds__(SN_BLOCK) k_sn_split_ext(SnTri A, const int* r
     const int q = (blockIdx.x * blockDim.x + threadIdx.x) / G, sl = threadIdx.x & (G - 1);
     const bool live = q < nrows;
     const int row = live ? rows[q] : 0;
-    const int64_t k0 = A.ext_rp[row] + sl, k1 = A.ext_rp[row + 1];
+    const int64_t k0 = A.ext_rp[row] + sl, k1 = live ? A.ext_rp[row + 1] : k0;
+    ExtPre<4> e;
+    ext_preload(A, k0, k1, G, e);
     pdl_wait();
     pdl_launch_dependents();
     double s0 = 0, s1 = 0, s2 = 0;
-    if (live) ext_dot(A, k0, k1, G, s0, s1, s2);
+    ext_finish(A, e, k0, k1, G, s0, s1, s2);
     block_group_sum3(s0, s1, s2, G, sh);
     if (live && sl == 0) {
         const int src = A.perm_in ? A.perm_in[row] : row;
@@ -231,13 +291,29 @@ __global__ void __launch_bounds__(SN_BLOCK) k_sn_split_dense(SnTri A, const int*
     int cb, len;
     dense_row<LOWER>(row - c0, w, o, cb, len);
     const double* D = A.dinv + A.dinv_off[s] + o;
+    constexpr int kPre = 4;
+    double dp[kPre];
+#pragma unroll
+    for (int i = 0; i < kPre; ++i) {
+        const int c = i * G + sl;
+        dp[i] = (live && c < len) ? __ldg(D + c) : 0.0;
+    }
     pdl_wait();
     pdl_launch_dependents();
     double s0 = 0, s1 = 0, s2 = 0;
     if (live) {
         const double* t = A.t + 3 * static_cast<int64_t>(c0 + cb);
+#pragma unroll
+        for (int i = 0; i < kPre; ++i) {
+            const int c = i * G + sl;
+            if (c < len) {
+                s0 += dp[i] * t[3 * c + 0];
+                s1 += dp[i] * t[3 * c + 1];
+                s2 += dp[i] * t[3 * c + 2];
+            }
+        }
 #pragma unroll 4
-        for (int c = sl; c < len; c += G) {
+        for (int c = kPre * G + sl; c < len; c += G) {
             const double d = D[c];
             s0 += d * t[3 * c + 0];
             s1 += d * t[3 * c + 1];
