@@ -135,6 +135,8 @@ __device__ __forceinline__ void block_exclusive_scan(double (&v)[W], double (&to
 template <int W>
 __global__ void k_scan_rows(double* rows, int n)
 {
+    pdl_wait();
+    pdl_launch_dependents();
     __shared__ double carry[W];
     if (threadIdx.x < W) carry[threadIdx.x] = 0.0;
     __syncthreads();
@@ -252,6 +254,8 @@ static __global__ void k_cluster_moments(GeomArgs g)
     const int C = blockIdx.x * blockDim.x + threadIdx.x;
     if (C >= g.NC) return;
     const int b = g.C_begin[C], e = g.C_end[C];
+    pdl_wait();
+    pdl_launch_dependents();
     double m[10];
     const double* lb = g.local + 10 * static_cast<int64_t>(b);
     const double* bb = g.blocks + 10 * static_cast<int64_t>(b / SCAN_BLOCK);
@@ -678,6 +682,16 @@ __global__ void __launch_bounds__(PAIR_TILE_THREADS, 2) k_tp0_pairs_tiled(PairAr
     const int u0 = T.cols_rp[b], un = T.cols_rp[b + 1] - u0;
     float4* sdat = tile_smem;
     int* sid = reinterpret_cast<int*>(reinterpret_cast<char*>(tile_smem) + sizeof(ColDatum) * static_cast<size_t>(un));
+    // the tile's pattern first; the primitive / cluster data once the producer has finished
+    for (int u = threadIdx.x; u < un; u += blockDim.x) sid[u] = __ldg(T.cols + u0 + u);
+    const int r0 = T.row0[b];
+    const int lm = __ldg(T.lane_map + static_cast<int64_t>(b) * PAIR_TILE_THREADS + threadIdx.x);
+    const bool active = lm >= 0;
+    const int sub = active ? (lm & 31) : 0, size = active ? (1 << ((lm >> 5) & 7)) : 1;
+    const int warp_size_max = __reduce_max_sync(0xffffffffu, size);
+    const int i = active ? T.order[r0 + (lm >> 8)] : 0;
+    pdl_wait();
+    pdl_launch_dependents();
     if constexpr (FAR) {
         for (int idx = threadIdx.x; idx < 4 * un; idx += blockDim.x) {
             const int u = idx >> 2, q = idx & 3;
@@ -702,18 +716,8 @@ __global__ void __launch_bounds__(PAIR_TILE_THREADS, 2) k_tp0_pairs_tiled(PairAr
             st[u] = t;
         }
     }
-    for (int u = threadIdx.x; u < un; u += blockDim.x) sid[u] = __ldg(T.cols + u0 + u);
-    const int r0 = T.row0[b];
-    const int lm = __ldg(T.lane_map + static_cast<int64_t>(b) * PAIR_TILE_THREADS + threadIdx.x);
-    const bool active = lm >= 0;
-    const int sub = active ? (lm & 31) : 0, size = active ? (1 << ((lm >> 5) & 7)) : 1;
-    const int warp_size_max = __reduce_max_sync(0xffffffffu, size);
-    int i = 0;
     Datum X;
-    if (active) {
-        i = T.order[r0 + (lm >> 8)];
-        X = load_datum(base, i);
-    }
+    if (active) X = load_datum(base, i);
     if constexpr (FAR) cp_async_wait_all();
     __syncthreads();
     double e_row = 0.0;
@@ -758,7 +762,10 @@ static __global__ void k_collect_chain(CollectArgs A)
     const int size = A.dom + 1;
     const int j = A.perm[i];
     SimplexGeom g;
+    // the coordinates were written before the pair kernels that precede this launch
     simplex_geometry(A.dom, A.V, A.S + static_cast<int64_t>(size) * j, A.charge_v, g);
+    pdl_wait();
+    pdl_launch_dependents();
 
     // near field (centred at the primitive barycentre)
     const double* dn = A.D_near + 10 * static_cast<int64_t>(i);
@@ -838,6 +845,8 @@ static __global__ void k_gather_vertices(GatherArgs A)
 {
     const int v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= A.nV) return;
+    pdl_wait();
+    pdl_launch_dependents();
     double acc[3] = {0, 0, 0};
     for (int k = A.v_rp[v]; k < A.v_rp[v + 1]; ++k) {
         const double* b = A.B + 3 * static_cast<int64_t>(A.v_slot[k]);

@@ -134,8 +134,8 @@ rpb_status launch_geometry(rpb_mesh* m)
     g.blocks = m->scan_blocks.ptr;
     const int nb = (m->N + SCAN_BLOCK - 1) / SCAN_BLOCK;
     k_geometry_prims<<<nb, SCAN_BLOCK, 0, m->stream>>>(g);
-    k_scan_rows<10><<<1, SCAN_BLOCK, 0, m->stream>>>(m->scan_blocks.ptr, nb);
-    k_cluster_moments<<<(m->NC + 255) / 256, 256, 0, m->stream>>>(g);
+    launch_pdl(k_scan_rows<10>, 1, SCAN_BLOCK, 0, m->stream, m->scan_blocks.ptr, nb);
+    launch_pdl(k_cluster_moments, (m->NC + 255) / 256, 256, 0, m->stream, g);
     RPB_CUDA(cudaGetLastError());
     m->geometry_valid = true;
     m->geometry_version++;
@@ -269,8 +269,9 @@ static void launch_pairs_t(rpb_mesh* m, const PairArgs& An, const PairArgs& Af, 
             int first, count;
             shard_tiles(t, shard, m->shards, first, count);
             const size_t smem = pair_tile_smem(t.max_union, false);
-            if (diff) k_tp0_pairs_tiled<false, QH, PH, true><<<count, PAIR_TILE_THREADS, smem, m->stream>>>(An, tiles_view(t, first));
-            else k_tp0_pairs_tiled<false, QH, PH, false><<<count, PAIR_TILE_THREADS, smem, m->stream>>>(An, tiles_view(t, first));
+            if (count > 0)
+                launch_pdl(diff ? k_tp0_pairs_tiled<false, QH, PH, true> : k_tp0_pairs_tiled<false, QH, PH, false>, count,
+                           PAIR_TILE_THREADS, smem, m->stream, An, tiles_view(t, first));
         } else if (diff) k_tp0_pairs<false, QH, PH, true, NEAR_LANES><<<m->near_blocks, PAIR_BLOCK, 0, m->stream>>>(An);
         else k_tp0_pairs<false, QH, PH, false, NEAR_LANES><<<m->near_blocks, PAIR_BLOCK, 0, m->stream>>>(An);
     }
@@ -281,8 +282,9 @@ static void launch_pairs_t(rpb_mesh* m, const PairArgs& An, const PairArgs& Af, 
             int first, count;
             shard_tiles(t, shard, m->shards, first, count);
             const size_t smem = pair_tile_smem(t.max_union, true);
-            if (diff) k_tp0_pairs_tiled<true, QH, PH, true><<<count, PAIR_TILE_THREADS, smem, m->stream>>>(Af, tiles_view(t, first));
-            else k_tp0_pairs_tiled<true, QH, PH, false><<<count, PAIR_TILE_THREADS, smem, m->stream>>>(Af, tiles_view(t, first));
+            if (count > 0)
+                launch_pdl(diff ? k_tp0_pairs_tiled<true, QH, PH, true> : k_tp0_pairs_tiled<true, QH, PH, false>, count,
+                           PAIR_TILE_THREADS, smem, m->stream, Af, tiles_view(t, first));
         } else if (diff) k_tp0_pairs<true, QH, PH, true, FAR_LANES><<<m->far_blocks, PAIR_BLOCK, 0, m->stream>>>(Af);
         else k_tp0_pairs<true, QH, PH, false, FAR_LANES><<<m->far_blocks, PAIR_BLOCK, 0, m->stream>>>(Af);
     }
@@ -353,7 +355,7 @@ rpb_status launch_collect_gather(rpb_mesh* m, double alpha, double beta, double*
     C.D_far = D_far ? D_far : m->D_far.ptr;
     C.D_vf = with_vf ? m->D_vf.ptr : nullptr;
     C.B = m->B.ptr;
-    k_collect_chain<<<(m->N + 255) / 256, 256, 0, m->stream>>>(C);
+    launch_pdl(k_collect_chain, (m->N + 255) / 256, 256, 0, m->stream, C);
     RPB_CUDA(cudaGetLastError());
     GatherArgs G;
     G.nV = m->nV;
@@ -364,7 +366,7 @@ rpb_status launch_collect_gather(rpb_mesh* m, double alpha, double beta, double*
     G.beta = beta;
     G.Y = Y;
     G.ldY = ldY;
-    k_gather_vertices<<<(m->nV + 255) / 256, 256, 0, m->stream>>>(G);
+    launch_pdl(k_gather_vertices, (m->nV + 255) / 256, 256, 0, m->stream, G);
     RPB_CUDA(cudaGetLastError());
     return RPB_OK;
 }
