@@ -35,6 +35,9 @@ OFF_W3 = OFF_B2 + NH
 OFF_B3 = OFF_W3 + NO * NH
 NPARAM = OFF_B3 + NO
 GAIN_CLAMP = 3.0
+# level exponent of the multilevel coefficients R_C (A_C / A_root)^k / A_C (kLevelExponent
+# in repulsor_b200/csrc/rpb_learned.cu)
+LEVEL_EXPONENT = 0.5
 
 
 def bf16_round(x):
@@ -194,14 +197,16 @@ class LearnedGeometry:
         return F.astype(np.float32).astype(np.float64), s
 
     def apply(self, theta, R, return_cache=False, quantize=True):
-        """z = M(R): gains exp(clamp(o_C)) on the multilevel coefficients R_C / A_C,
-        expanded to the primitives, gathered to the vertices, column means removed."""
+        """z = M(R): gains exp(clamp(o_C)) on the multilevel coefficients
+        R_C (A_C / A_root)^LEVEL_EXPONENT / A_C, expanded to the primitives, gathered to the
+        vertices, column means removed."""
         R = np.asarray(R, np.float64)
         F, s = self.features(R)
         O, cache = mlp_forward(theta, F, quantize)
         O32 = O.astype(np.float32).astype(np.float64) if quantize else O
         gain = np.exp(np.clip(O32, -GAIN_CLAMP, GAIN_CLAMP))
-        Rc = self.range_sums(self.prim_from_vertices(R)) / self.A_C[:, None]
+        w = (self.A_C / self.A_C[0]) ** LEVEL_EXPONENT / self.A_C
+        Rc = self.range_sums(self.prim_from_vertices(R)) * w[:, None]
         Z = self.expand(gain * Rc)
         z = self.vertices_from_prims(Z)
         z -= z.mean(0)

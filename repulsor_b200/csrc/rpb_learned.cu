@@ -11,13 +11,13 @@
 //      (zero where the children do not exist),
 //   3. an MLP 16 -> 64 -> 64 -> 3 with GELU, BF16 weights and FP32 accumulation gives
 //      o_C; the per-component gains g_C = exp(clamp(o_C, +-3)) scale the multilevel
-//      coefficient c_C = g_C * R_C / A_C,
+//      coefficient c_C = g_C * R_C * w_C, w_C = (A_C / A_root)^kLevelExponent / A_C,
 //   4. every primitive gets Z_i = sum over the clusters containing i of c_C
 //      (PercolateDown + ClustersToPrimitives, src/ClusterTree.hpp:706-768) and every
 //      vertex z_v = sum_{i at v} a_i/(n+1) Z_i (the transpose of step 1), minus the
 //      column means (translations are the kernel of the metric).
 // With all gains 1 this is the fixed symmetric positive definite multilevel operator
-// W^T E diag(1/A_C) E^T W; the gains make it nonlinear but homogeneous of degree one in r,
+// W^T E diag(w_C) E^T W; the gains make it nonlinear but homogeneous of degree one in r,
 // and z . r > 0 always, so flexible CG cannot break down on it.
 //
 // Training (rpb_mlp_train_step) on (residual r, correction e) pairs with A e = r: the loss
@@ -368,7 +368,7 @@ __global__ void k_adam(int n, float* theta, __nv_bfloat16* w16, const float* g, 
 //   k_prim_scan     primitive moments a_i mean(r) -> in-block prefix sums; sum of |r|^2
 //   k_scan_totals   prefix sums of the block totals; the global sum of |r|^2
 //   k_cluster_mlp   per cluster: R_C (and its children's) as prefix-sum differences,
-//                   16 features, the MLP, gains, c_C = g_C R_C / A_C; sum_C A_C c_C
+//                   16 features, the MLP, gains, c_C = g_C R_C w_C; sum_C A_C c_C
 //   k_prim_expand   Z_i = sum_{C containing i} c_C
 //   k_vertex_expand z_v = sum_{i at v} w_i Z_i - mean(z)
 // ------------------------------------------------------------------------------------------
@@ -481,6 +481,7 @@ struct ClusterMlpArgs {
     float* pre1;              // NC x NH
     float* pre2;              // NC x NH
     double* Rc;               // NC x 3
+    const double* C_w;        // NC: level weights (A_C / A_root)^kLevelExponent / A_C
 };
 
 __device__ __forceinline__ void prefix_at(const double* local, const double* blocks, int N, int k, double* out)
@@ -501,12 +502,20 @@ __device__ __forceinline__ void cluster_moment(const ClusterMlpArgs& A, int C, d
     for (int q = 0; q < 3; ++q) R[q] = se[q] - sb[q];
 }
 
+// Level exponent of the multilevel coefficients c_C = g_C R_C w_C, w_C = (A_C / A_root)^k / A_C.
+// k = 0 weights every level of the tree alike; chosen by FCG iteration counts of the
+// untrained operator (all gains 1) on spherical-harmonic icospheres, plain CG residual
+// 1e-6, q = 6, p = 12: level 5 / 6 / 7 take 735 / 2,037 / 3,945 iterations at k = 0
+// (level 7 stalls into the fallback), 655 / 1,474 / 3,440 at k = 0.5; on level 6, 0.4 and
+// 0.6 are within 15 % of 0.5, 0.8 is worse than 0, 1 needs 5,756 and k >= 1.33 stalls.
+constexpr double kLevelExponent = 0.5;
+
 // Geometric features of the clusters (3..11 of the 16), once per geometry: centre
 // relative to the root over the root diameter, averaged normal, log area ratio, log
-// diameter ratio, depth.
+// diameter ratio, depth; and the level weights w_C.
 constexpr int NFS = 9;
 __global__ void k_static_features(int NC, int max_depth, const ClusterDatum* C_pair, const double* C_an,
-                                  const float* C_diam, const int* C_depth, float* Fs)
+                                  const float* C_diam, const int* C_depth, float* Fs, double* C_w)
 {
     const int C = blockIdx.x * blockDim.x + threadIdx.x;
     if (C >= NC) return;
@@ -519,6 +528,7 @@ __global__ void k_static_features(int NC, int max_depth, const ClusterDatum* C_p
     f[6] = static_cast<float>(log(cd.a / root.a) / 10.0);
     f[7] = static_cast<float>(log(fmax(static_cast<double>(C_diam[C]), 1e-300) / dr) / 10.0);
     f[8] = static_cast<float>(C_depth[C]) / static_cast<float>(max(max_depth, 1));
+    C_w[C] = pow(cd.a / root.a, kLevelExponent) / cd.a;
 }
 
 // Persistent: every block stages the weights once, then each of its warps takes units of
@@ -586,7 +596,7 @@ __global__ void __launch_bounds__(GAIN_BLOCK, 4) k_cluster_mlp(ClusterMlpArgs A)
         if (C < A.NC) {
             float o[NO];
             for (int q = 0; q < NO; ++q) o[q] = sm.O[row * 4 + q];
-            const double inv_a = 1.0 / ca;
+            const double inv_a = __ldg(A.C_w + C);
             for (int q = 0; q < 3; ++q) {
                 const float oc = fminf(fmaxf(o[q], -GAIN_CLAMP), GAIN_CLAMP);
                 const double cq = exp(static_cast<double>(oc)) * R[q] * inv_a;
@@ -708,14 +718,14 @@ __global__ void k_loss_grad(int n, const double* r, const double* Az, const doub
     if (i == 0) *loss_acc += 1.0 - zr * zr / (zAz * er);
 }
 
-// dL/do_C = sum_q gc_Cq R_Cq / A_C * g_Cq (zero where the clamp is active), plus the
+// dL/do_C = sum_q gc_Cq R_Cq w_C * g_Cq (zero where the clamp is active), plus the
 // gradient 2 reg o_C / (3 N_C) of the gain penalty reg * mean(o^2)
 __global__ void k_cluster_out_grad(int NC, const double* gc, const float* O, const double* Rc, const ClusterDatum* C_pair,
-                                   float reg, float* dO)
+                                   float reg, const double* C_w, float* dO)
 {
     const int C = blockIdx.x * blockDim.x + threadIdx.x;
     if (C >= NC) return;
-    const double inv_a = 1.0 / load_datum(C_pair, C).a;
+    const double inv_a = C_w[C];
     for (int q = 0; q < 3; ++q) {
         const int64_t k = 3 * static_cast<int64_t>(C) + q;
         const float o = O[k];
@@ -780,7 +790,7 @@ struct LearnedState {
     int64_t geometry_version = -1;
     int max_depth = 0;
     DevBuf<double> C_an, tmp3, Rc, c, scale, sums, loss, gc, dots, g, r, z, e, Az;
-    DevBuf<double> local, blocks, sq_part, csum_part, zmean;
+    DevBuf<double> local, blocks, sq_part, csum_part, zmean, C_w;
     DevBuf<unsigned> done;
     DevBuf<float> F, O, dO, pre1, pre2, d1, d2, C_diam;
     DevBuf<int> C_depth;
@@ -806,6 +816,7 @@ static rpb_status ensure_learned(rpb_mesh* m)
     const size_t NC = m->NC, N = m->N, nV = m->nV;
     if (!L.F.ptr) {
         RPB_CUDA(L.C_an.alloc(3 * NC));
+        RPB_CUDA(L.C_w.alloc(NC));
         RPB_CUDA(L.tmp3.alloc(3 * N));
         RPB_CUDA(L.Rc.alloc(3 * NC));
         RPB_CUDA(L.c.alloc(3 * NC));
@@ -850,7 +861,7 @@ static rpb_status ensure_learned(rpb_mesh* m)
         rpb_status st = range_sums3(m, L.tmp3.ptr, L.C_an.ptr);
         if (st != RPB_OK) return st;
         k_static_features<<<(m->NC + 255) / 256, 256, 0, m->stream>>>(m->NC, L.max_depth, m->C_pair.ptr, L.C_an.ptr,
-                                                                      L.C_diam.ptr, L.C_depth.ptr, L.Fs.ptr);
+                                                                      L.C_diam.ptr, L.C_depth.ptr, L.Fs.ptr, L.C_w.ptr);
         RPB_CUDA(cudaGetLastError());
         L.geometry_version = m->geometry_version;
     }
@@ -913,6 +924,7 @@ static rpb_status learned_forward(rpb_mesh* m, rpb_mlp* mlp, const double* R, do
     ca.local = L.local.ptr; ca.blocks = L.blocks.ptr; ca.scale = L.scale.ptr;
     ca.c = L.c.ptr; ca.csum_part = L.csum_part.ptr; ca.done = L.done.ptr; ca.zmean = L.zmean.ptr;
     ca.Fs = L.Fs.ptr;
+    ca.C_w = L.C_w.ptr;
     ca.F = training ? L.F.ptr : nullptr;
     ca.O = training ? L.O.ptr : nullptr;
     ca.pre1 = training ? L.pre1.ptr : nullptr;
@@ -1124,7 +1136,7 @@ rpb_status rpb_mlp_train_step(rpb_mlp* mlp, rpb_mesh* m, double q, double p, con
         k_sub_mean<<<eb, 256, 0, s>>>(nV, L.g.ptr, L.sums.ptr);
         if ((st = cluster_moments(m, L.g.ptr, L.gc.ptr)) != RPB_OK) return st;
         k_cluster_out_grad<<<(m->NC + 255) / 256, 256, 0, s>>>(m->NC, L.gc.ptr, L.O.ptr, L.Rc.ptr, m->C_pair.ptr,
-                                                               static_cast<float>(reg), L.dO.ptr);
+                                                               static_cast<float>(reg), L.C_w.ptr, L.dO.ptr);
         RPB_CUDA(cudaGetLastError());
         if ((st = mlp_backward(mlp, m->NC, L.F.ptr, L.pre1.ptr, L.pre2.ptr, L.dO.ptr, L.d1.ptr, L.d2.ptr, mlp->grad.ptr,
                                s)) != RPB_OK)
