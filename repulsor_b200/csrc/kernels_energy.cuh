@@ -540,9 +540,11 @@ __device__ __forceinline__ void pair_row(const PairArgs& A, const Datum& X, int 
 // adds only offsets inside its group), writes the row's derivative, and reduces the
 // energy deterministically: one partial per block, the last block to finish sums the
 // partials in block order.
+// bid / nblocks: this block's index among the launch's blocks for this pattern (the
+// block energies are summed in that order by the last of them)
 template <bool DIFF, bool CROSS>
 __device__ __forceinline__ void pair_epilogue(const PairArgs& A, bool active, int i, int sub, int size, int warp_size_max,
-                                              double e_row, double (&D64)[10])
+                                              double e_row, double (&D64)[10], int bid, int nblocks)
 {
     if constexpr (CROSS) {
         e_row *= 0.5;
@@ -577,15 +579,15 @@ __device__ __forceinline__ void pair_epilogue(const PairArgs& A, bool active, in
     if (threadIdx.x == 0) {
         double s = 0.0;
         for (int w = 0; w < nw; ++w) s += sh[w];
-        A.block_energy[blockIdx.x] = s;
+        A.block_energy[bid] = s;
         __threadfence();
-        last = (atomicAdd(A.done, 1u) == gridDim.x - 1);
+        last = (atomicAdd(A.done, 1u) == static_cast<unsigned>(nblocks) - 1);
     }
     __syncthreads();
     if (last) {
         __threadfence();
         double s = 0.0;
-        for (int b = threadIdx.x; b < gridDim.x; b += blockDim.x) s += __ldcg(A.block_energy + b);
+        for (int b = threadIdx.x; b < nblocks; b += blockDim.x) s += __ldcg(A.block_energy + b);
         s = warp_sum_f64(s);
         __syncthreads();
         if (lane == 0) sh[wib] = s;
@@ -627,7 +629,7 @@ __global__ void __launch_bounds__(PAIR_BLOCK) k_tp0_pairs(PairArgs A)
         };
         pair_row<FAR, QH, PH, DIFF, CROSS, true, Datum>(A, X, i, sub, LANES, index, datum, e_row, D64);
     }
-    pair_epilogue<DIFF, CROSS>(A, active, i, sub, LANES, LANES, e_row, D64);
+    pair_epilogue<DIFF, CROSS>(A, active, i, sub, LANES, LANES, e_row, D64, blockIdx.x, gridDim.x);
 }
 
 // Row tiles (build_row_tiles): block b owns the rows order[row0[b] .. row0[b+1]) and
@@ -672,13 +674,13 @@ __host__ __device__ constexpr size_t pair_tile_smem(int n, bool far)
 }
 
 template <bool FAR, int QH, int PH, bool DIFF>
-__global__ void __launch_bounds__(PAIR_TILE_THREADS, 2) k_tp0_pairs_tiled(PairArgs A, PairTiles T)
+__device__ __forceinline__ void pairs_tiled_body(const PairArgs& A, const PairTiles& T, int bid, int nblocks)
 {
     using Datum = typename std::conditional<FAR, ClusterDatum, PrimDatum>::type;
     using ColDatum = typename std::conditional<FAR, ClusterDatum, PrimTile>::type;
     extern __shared__ float4 tile_smem[];
     const Datum* base = static_cast<const Datum*>(A.data);
-    const int b = T.tile_base + blockIdx.x;
+    const int b = T.tile_base + bid;
     const int u0 = T.cols_rp[b], un = T.cols_rp[b + 1] - u0;
     float4* sdat = tile_smem;
     int* sid = reinterpret_cast<int*>(reinterpret_cast<char*>(tile_smem) + sizeof(ColDatum) * static_cast<size_t>(un));
@@ -731,7 +733,25 @@ __global__ void __launch_bounds__(PAIR_TILE_THREADS, 2) k_tp0_pairs_tiled(PairAr
         };
         pair_row<FAR, QH, PH, DIFF, false, false, ColDatum>(A, X, i, sub, size, index, datum, e_row, D64);
     }
-    pair_epilogue<DIFF, false>(A, active, i, sub, size, warp_size_max, e_row, D64);
+    pair_epilogue<DIFF, false>(A, active, i, sub, size, warp_size_max, e_row, D64, bid, nblocks);
+}
+
+template <bool FAR, int QH, int PH, bool DIFF>
+__global__ void __launch_bounds__(PAIR_TILE_THREADS, 2) k_tp0_pairs_tiled(PairArgs A, PairTiles T)
+{
+    pairs_tiled_body<FAR, QH, PH, DIFF>(A, T, blockIdx.x, gridDim.x);
+}
+
+// Both patterns in one launch: blocks [0, nfar) take the far tiles, the others the near
+// tiles, so the far and near tiles share the waves instead of draining and refilling
+// the GPU between two launches. Each part keeps its own block indices, energy partials
+// and last-block sum, so the results equal those of the two separate launches.
+template <int QH, int PH, bool DIFF>
+__global__ void __launch_bounds__(PAIR_TILE_THREADS, 2)
+    k_tp0_pairs_tiled_both(PairArgs An, PairTiles Tn, PairArgs Af, PairTiles Tf, int nfar)
+{
+    if (static_cast<int>(blockIdx.x) < nfar) pairs_tiled_body<true, QH, PH, DIFF>(Af, Tf, blockIdx.x, nfar);
+    else pairs_tiled_body<false, QH, PH, DIFF>(An, Tn, blockIdx.x - nfar, gridDim.x - nfar);
 }
 
 // energy = near-field part + far-field part (the order evaluate() uses on the host)

@@ -160,6 +160,8 @@ static cudaError_t allow_tile_smem_t()
     set(reinterpret_cast<const void*>(k_tp0_pairs_tiled<false, QH, PH, false>), nb);
     set(reinterpret_cast<const void*>(k_tp0_pairs_tiled<true, QH, PH, true>), fb);
     set(reinterpret_cast<const void*>(k_tp0_pairs_tiled<true, QH, PH, false>), fb);
+    set(reinterpret_cast<const void*>(k_tp0_pairs_tiled_both<QH, PH, true>), std::max(nb, fb));
+    set(reinterpret_cast<const void*>(k_tp0_pairs_tiled_both<QH, PH, false>), std::max(nb, fb));
     return e;
 }
 
@@ -263,6 +265,19 @@ template <int QH, int PH>
 static void launch_pairs_t(rpb_mesh* m, const PairArgs& An, const PairArgs& Af, bool diff, cudaEvent_t between,
                            int shard)
 {
+    if (An.rows > 0 && Af.rows > 0 && m->near_tiles.valid && m->far_tiles.valid && !between) {
+        int nfirst, ncount, ffirst, fcount;
+        shard_tiles(m->near_tiles, shard, m->shards, nfirst, ncount);
+        shard_tiles(m->far_tiles, shard, m->shards, ffirst, fcount);
+        if (ncount > 0 && fcount > 0) {
+            const size_t smem = std::max(pair_tile_smem(m->near_tiles.max_union, false),
+                                         pair_tile_smem(m->far_tiles.max_union, true));
+            launch_pdl(diff ? k_tp0_pairs_tiled_both<QH, PH, true> : k_tp0_pairs_tiled_both<QH, PH, false>,
+                       ncount + fcount, PAIR_TILE_THREADS, smem, m->stream, An, tiles_view(m->near_tiles, nfirst), Af,
+                       tiles_view(m->far_tiles, ffirst), fcount);
+            return;
+        }
+    }
     if (An.rows > 0) {
         const TileBufs& t = m->near_tiles;
         if (t.valid) {
