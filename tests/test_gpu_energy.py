@@ -54,6 +54,24 @@ def test_differential_alpha_beta_and_ldY():
     assert np.array_equal(Y[:, 3:], Y0[:, 3:])      # columns beyond AMB_DIM untouched
 
 
+def test_differential_into_pinned_host_rows():
+    """Y in page-locked host memory (torch pin_memory), with ldY = 3 and 5: the rows equal
+    those of a pageable Y and the columns beyond AMB_DIM stay untouched."""
+    import torch
+
+    dom, V, S, M, O = _pair(2, True)
+    tpe = rpb.TangentPointEnergy0(Q, P)
+    D = np.zeros((V.shape[0], 3))
+    E = tpe.Differential(M, 0.5, 0.0, D)
+    for width in (3, 5):
+        Yt = torch.full((V.shape[0], width), 7.0, dtype=torch.float64).pin_memory()
+        Y = Yt.numpy()
+        E2 = tpe.Differential(M, 0.5, 0.0, Y)
+        assert E2 == E
+        assert np.array_equal(Y[:, :3], D)
+        assert np.all(Y[:, 3:] == 7.0)
+
+
 def test_cached_differential_and_value_consistency():
     dom, V, S, M, O = _pair(1, True)
     tpe = rpb.TangentPointEnergy0(Q, P)
