@@ -31,6 +31,20 @@ def test_preconditioner_matches_oracle(cfg):
     assert rel_max(Y, O.precondition(X, Q, P)) <= 1e-5
 
 
+@pytest.mark.parametrize("cfg", [2, 3])
+def test_preconditioner_matches_oracle_full_size(cfg):
+    """Full-size torus and icosphere level 6: deeper supernode schedules, whose upper levels
+    run as split levels with up to 256 lanes per row (the small meshes use warp levels
+    mostly)."""
+    dom, (V, S) = meshes.config_mesh(cfg, small=False)
+    M = rpb.SimplicialMesh(V, S)
+    O = oracle.OracleMesh(dom, V, S, threads=8)
+    tpm = rpb.TangentPointMetric0(Q, P)
+    X = np.random.default_rng(10 + cfg).standard_normal(V.shape)
+    Y = tpm.MultiplyPreconditioner(M, 1.0, X)
+    assert rel_max(Y, O.precondition(X, Q, P)) <= 1e-5
+
+
 @pytest.mark.parametrize("cfg,precond", [(1, rpb.PRECOND_NONE), (2, rpb.PRECOND_NONE), (3, rpb.PRECOND_NONE),
                                          (2, rpb.PRECOND_REFERENCE), (3, rpb.PRECOND_REFERENCE)])
 def test_solve_reaches_tolerance(cfg, precond):
