@@ -461,6 +461,30 @@ constexpr int FAR_TILE_UNION = 1536;
 // the current pair is evaluated. A row accumulates only its own derivative; each
 // unordered pair contributes its energy once (from the row with the smaller index),
 // CROSS pairs always.
+// A close near-field pair evaluated in FP64: energy and the ten derivative components.
+// Out of line and with its operands passed by value, so that its FP64 temporaries do not
+// count against the registers of the FP32 pair loop that calls it (rarely).
+struct Close64 {
+    double e;
+    double d[10];
+};
+
+template <int QH, int PH, bool DIFF, typename Datum, typename ColDatum>
+__device__ __noinline__ Close64 close_pair_fp64(TPExp ex, int dom, Datum X, ColDatum Y)
+{
+    Proj<double> gd;
+    project_prims(dom, X, Y, gd);
+    PairAcc<double> a64 = {};
+    Close64 c;
+    c.e = tp0_core<double, QH, PH, DIFF>(ex, gd, X.a, Y.a, a64);
+    c.d[0] = a64.d0;
+#pragma unroll
+    for (int m = 0; m < 3; ++m) c.d[1 + m] = a64.dx[m];
+#pragma unroll
+    for (int m = 0; m < 6; ++m) c.d[4 + m] = a64.dP[m];
+    return c;
+}
+
 template <bool FAR, int QH, int PH, bool DIFF, bool CROSS, bool PREFETCH, typename ColDatum, typename Datum,
           typename Index, typename Fetch>
 __device__ __forceinline__ void pair_row(const PairArgs& A, const Datum& X, int i, int sub, int stride, Index index,
@@ -497,15 +521,13 @@ __device__ __forceinline__ void pair_row(const PairArgs& A, const Datum& X, int 
         }
         if (close) {
             // close near-field pair: the same kernel in FP64, added straight into FP64
-            Proj<double> gd;
-            if constexpr (!FAR) project_prims(A.dom, X, Y, gd);
-            PairAcc<double> a64 = {};
-            const double e = tp0_core<double, QH, PH, DIFF>(A.ex, gd, X.a, Y.a, a64);
-            if (CROSS || j > i) e_row += e;
-            if (DIFF) {
-                D64[0] += a64.d0;
-                for (int m = 0; m < 3; ++m) D64[1 + m] += a64.dx[m];
-                for (int m = 0; m < 6; ++m) D64[4 + m] += a64.dP[m];
+            if constexpr (!FAR) {
+                const Close64 c = close_pair_fp64<QH, PH, DIFF>(A.ex, A.dom, X, Y);
+                if (CROSS || j > i) e_row += c.e;
+                if (DIFF) {
+#pragma unroll
+                    for (int m = 0; m < 10; ++m) D64[m] += c.d[m];
+                }
             }
         } else {
             const float e = tp0_core<float, QH, PH, DIFF>(A.ex, g, ax, weight_f(Y), acc);
