@@ -782,6 +782,37 @@ static __global__ void k_add_pair(const double* e2, double* out) { *out = e2[0] 
 // ----------------------------------------------------------------------------------------
 // Collection + chain rule. One thread per primitive (tree order).
 // ----------------------------------------------------------------------------------------
+// Visits every ancestor of cluster C (C itself included) once, in a fixed order. The chain
+// is cut into segments of four clusters by the jump pointers up4 (the fourth ancestor, -1
+// when the root is nearer): the first ANC_SEG - 1 segments are walked interleaved, so their
+// parent loads overlap while the jump pointers are followed, and the last segment walks on
+// to the root. Dependent loads: about ANC_SEG - 1 + max(4, depth - 4 (ANC_SEG - 1)) instead
+// of the depth.
+constexpr int ANC_SEG = 5;
+template <typename Visit>
+__device__ __forceinline__ void ancestor_walk(int C, const int* __restrict__ parent, const int* __restrict__ up4,
+                                              Visit visit)
+{
+    int s[ANC_SEG];
+    s[0] = C;
+#pragma unroll
+    for (int k = 1; k < ANC_SEG; ++k) s[k] = s[k - 1] >= 0 ? __ldg(up4 + s[k - 1]) : -1;
+    int node[ANC_SEG - 1];
+#pragma unroll
+    for (int k = 0; k < ANC_SEG - 1; ++k) node[k] = s[k];
+#pragma unroll
+    for (int step = 0; step < 4; ++step) {
+#pragma unroll
+        for (int k = 0; k < ANC_SEG - 1; ++k) {
+            if (node[k] >= 0) {
+                visit(node[k]);
+                node[k] = __ldg(parent + node[k]);
+            }
+        }
+    }
+    for (int c = s[ANC_SEG - 1]; c >= 0; c = __ldg(parent + c)) visit(c);
+}
+
 struct CollectArgs {
     int dom, N;
     const double* V;
@@ -790,6 +821,7 @@ struct CollectArgs {
     const int* perm;
     const int* leaf_of;
     const int* C_parent;
+    const int* C_up4;
     const ClusterDatum* C_pair;
     const double* D_near;      // N x 10 centred
     const double* D_far;       // NC x 10 centred
@@ -816,16 +848,14 @@ static __global__ void k_collect_chain(CollectArgs A)
     double G6[6];
     for (int k = 0; k < 6; ++k) G6[k] = dn[4 + k];
     // far field: percolate down = sum over all ancestors of the leaf
-    int C = A.leaf_of[i];
-    while (C >= 0) {
+    ancestor_walk(A.leaf_of[i], A.C_parent, A.C_up4, [&](int C) {
         const double* df = A.D_far + 10 * static_cast<int64_t>(C);
         const ClusterDatum cd = load_datum(A.C_pair, C);
         const double dx0 = df[1], dx1 = df[2], dx2 = df[3];
         alpha += df[0] + dx0 * (g.c[0] - cd.c[0]) + dx1 * (g.c[1] - cd.c[1]) + dx2 * (g.c[2] - cd.c[2]);
         gx[0] += dx0; gx[1] += dx1; gx[2] += dx2;
         for (int k = 0; k < 6; ++k) G6[k] += df[4 + k];
-        C = A.C_parent[C];
-    }
+    });
     double hull_extra[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
     if (A.D_vf) {
         const double* dv = A.D_vf + 16 * static_cast<int64_t>(i);

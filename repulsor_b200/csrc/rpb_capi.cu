@@ -37,7 +37,7 @@ int64_t rpb_mesh::device_bytes() const
 {
     int64_t b = 0;
     b += V.bytes() + charge_v.bytes() + S.bytes() + perm.bytes() + leaf_of.bytes() + C_parent.bytes() +
-         C_left.bytes() + C_right.bytes();
+         C_up4.bytes() + C_left.bytes() + C_right.bytes();
     b += near.rp.bytes() + near.ci.bytes() + far.rp.bytes() + far.ci.bytes() + verynear.rp.bytes() +
          verynear.ci.bytes() + near_order.bytes() + far_order.bytes();
     for (const rpb::TileBufs* t : {&near_tiles, &far_tiles})
@@ -365,6 +365,7 @@ rpb_status launch_collect_gather(rpb_mesh* m, double alpha, double beta, double*
     C.perm = m->perm.ptr;
     C.leaf_of = m->leaf_of.ptr;
     C.C_parent = m->C_parent.ptr;
+    C.C_up4 = m->C_up4.ptr;
     C.C_pair = m->C_pair.ptr;
     C.D_near = D_near ? D_near : m->D_near.ptr;
     C.D_far = D_far ? D_far : m->D_far.ptr;
@@ -512,6 +513,15 @@ rpb_status rpb_mesh_create(int dom_dim, int amb_dim, const double* Vh, int64_t n
     UP(m->perm, T.perm.data(), T.perm.size());
     UP(m->leaf_of, T.leaf_of.data(), T.leaf_of.size());
     UP(m->C_parent, T.C_parent.data(), T.C_parent.size());
+    {
+        std::vector<int> up4(T.C_parent.size());
+        for (size_t C = 0; C < up4.size(); ++C) {
+            int a = static_cast<int>(C);
+            for (int k = 0; k < 4 && a >= 0; ++k) a = T.C_parent[a];
+            up4[C] = a;
+        }
+        UP(m->C_up4, up4.data(), up4.size());
+    }
     UP(m->C_left, T.C_left.data(), T.C_left.size());
     UP(m->C_right, T.C_right.data(), T.C_right.size());
     UP(m->C_begin, T.C_begin.data(), T.C_begin.size());

@@ -91,6 +91,7 @@ struct rpb_mesh {
     rpb::DevBuf<int> S;
     // tree
     rpb::DevBuf<int> perm, leaf_of, C_parent, C_left, C_right, C_begin, C_end;
+    rpb::DevBuf<int> C_up4;   // fourth ancestor of every cluster (-1 when the root is nearer)
     rpb::Csr near, far, verynear;
     rpb::DevBuf<int> near_order, far_order;             // pair-kernel row order (length-sorted per chunk)
     rpb::TileBufs near_tiles, far_tiles;                // shared-memory row tiles of the two patterns

@@ -350,6 +350,7 @@ struct PostArgs {
     int N, nV, size;
     const int* leaf_of;
     const int* C_parent;
+    const int* C_up4;
     const double* Pout;
     const double* Cout;
     double* Z;
@@ -369,12 +370,10 @@ __global__ void k_post_primitives(PostArgs<BD> A)
     double z[BD];
 #pragma unroll
     for (int c = 0; c < BD; ++c) z[c] = A.Pout[BD * static_cast<int64_t>(i) + c];
-    int C = A.leaf_of[i];
-    while (C >= 0) {
+    ancestor_walk(A.leaf_of[i], A.C_parent, A.C_up4, [&](int C) {
 #pragma unroll
         for (int c = 0; c < BD; ++c) z[c] += A.Cout[BD * static_cast<int64_t>(C) + c];
-        C = A.C_parent[C];
-    }
+    });
 #pragma unroll
     for (int c = 0; c < BD; ++c) A.Z[BD * static_cast<int64_t>(i) + c] = z[c];
 }
@@ -611,7 +610,7 @@ static rpb_status apply_operator(rpb_mesh* m, const float2* nf, const double2* n
     }
     PostArgs<BD> po;
     po.N = m->N; po.nV = m->nV; po.size = m->size;
-    po.leaf_of = m->leaf_of.ptr; po.C_parent = m->C_parent.ptr;
+    po.leaf_of = m->leaf_of.ptr; po.C_parent = m->C_parent.ptr; po.C_up4 = m->C_up4.ptr;
     po.Pout = m->buf_Pout.ptr; po.Cout = m->buf_Cout.ptr; po.Z = m->buf_Z.ptr;
     po.vp_rp = m->vp_rp.ptr; po.vp_slot = m->vp_slot.ptr; po.pre_vals = m->pre_vals.ptr;
     po.alpha = alpha; po.beta = beta; po.Y = Y; po.ldY = ldY;
