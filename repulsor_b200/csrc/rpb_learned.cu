@@ -648,16 +648,17 @@ __global__ void __launch_bounds__(GAIN_BLOCK, 4) k_cluster_mlp(ClusterMlpArgs A)
 
 // Z_i = sum over the clusters containing primitive i of c_C (PercolateDown +
 // ClustersToPrimitives as an ancestor walk)
-__global__ void k_prim_expand(int N, const int* leaf_of, const int* C_parent, const double* c, double* Z)
+__global__ void k_prim_expand(int N, const int* leaf_of, const int* C_parent, const int* C_up4, const double* c,
+                              double* Z)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= N) return;
     double z0 = 0, z1 = 0, z2 = 0;
-    for (int C = leaf_of[i]; C >= 0; C = C_parent[C]) {
+    ancestor_walk(leaf_of[i], C_parent, C_up4, [&](int C) {
         z0 += c[3 * static_cast<int64_t>(C)];
         z1 += c[3 * static_cast<int64_t>(C) + 1];
         z2 += c[3 * static_cast<int64_t>(C) + 2];
-    }
+    });
     Z[3 * static_cast<int64_t>(i)] = z0;
     Z[3 * static_cast<int64_t>(i) + 1] = z1;
     Z[3 * static_cast<int64_t>(i) + 2] = z2;
@@ -931,7 +932,8 @@ static rpb_status learned_forward(rpb_mesh* m, rpb_mlp* mlp, const double* R, do
     ca.pre2 = training ? L.pre2.ptr : nullptr;
     ca.Rc = training ? L.Rc.ptr : nullptr;
     k_cluster_mlp<<<std::min(L.mlp_grid, (m->NC + GAIN_BLOCK - 1) / GAIN_BLOCK), GAIN_BLOCK, 0, s>>>(ca);
-    k_prim_expand<<<(m->N + 255) / 256, 256, 0, s>>>(m->N, m->leaf_of.ptr, m->C_parent.ptr, L.c.ptr, L.tmp3.ptr);
+    k_prim_expand<<<(m->N + 255) / 256, 256, 0, s>>>(m->N, m->leaf_of.ptr, m->C_parent.ptr, m->C_up4.ptr, L.c.ptr,
+                                                      L.tmp3.ptr);
     k_vertex_expand<<<(m->nV + 255) / 256, 256, 0, s>>>(m->nV, m->size, m->vp_rp.ptr, m->vp_slot.ptr, m->pre_vals.ptr,
                                                         L.tmp3.ptr, L.zmean.ptr, z);
     RPB_CUDA(cudaGetLastError());
