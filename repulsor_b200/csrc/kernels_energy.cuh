@@ -201,7 +201,7 @@ struct GeomArgs {
     const int* C_end;
     PrimDatum* P_pair;        // N
     ClusterDatum* C_pair;     // NC
-    double* C_mom;            // NC x 10 (a, centre, P) in FP64
+    double* C_mom;            // NC x 10 (a, centre, P) in FP64, or null (not written)
     double* local;            // N x 10: exclusive in-block prefix of the moments (a, a c, a P)
     double* blocks;           // (nblocks + 1) x 10: block sums -> exclusive block prefix
 };

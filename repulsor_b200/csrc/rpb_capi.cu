@@ -43,7 +43,7 @@ int64_t rpb_mesh::device_bytes() const
     for (const rpb::TileBufs* t : {&near_tiles, &far_tiles})
         b += t->row0.bytes() + t->cols_rp.bytes() + t->cols.bytes() + t->order.bytes() + t->slot.bytes() +
              t->lane_map.bytes();
-    b += P_pair.bytes() + C_pair.bytes() + C_mom.bytes() + counter.bytes() + P_near.bytes() + scan_local.bytes() +
+    b += P_pair.bytes() + C_pair.bytes() + counter.bytes() + P_near.bytes() + scan_local.bytes() +
          scan_blocks.bytes() + C_begin.bytes() + C_end.bytes();
     b += D_near.bytes() + D_far.bytes() + D_vf.bytes() + B.bytes() + v_rp.bytes() + v_slot.bytes() + Y.bytes();
     b += block_energy.bytes() + energy.bytes() + done.bytes();
@@ -129,7 +129,7 @@ rpb_status launch_geometry(rpb_mesh* m)
     g.C_end = m->C_end.ptr;
     g.P_pair = m->P_pair.ptr;
     g.C_pair = m->C_pair.ptr;
-    g.C_mom = m->C_mom.ptr;
+    g.C_mom = nullptr;   // the FP64 moments are not read by any later kernel
     g.local = m->scan_local.ptr;
     g.blocks = m->scan_blocks.ptr;
     const int nb = (m->N + SCAN_BLOCK - 1) / SCAN_BLOCK;
@@ -540,7 +540,7 @@ rpb_status rpb_mesh_create(int dom_dim, int amb_dim, const double* Vh, int64_t n
         UP(m->v_slot, slot.data(), slot.size());
     }
 #undef UP
-    if (m->P_pair.alloc(m->N) || m->C_pair.alloc(m->NC) || m->C_mom.alloc(10 * static_cast<size_t>(m->NC)) ||
+    if (m->P_pair.alloc(m->N) || m->C_pair.alloc(m->NC) ||
         m->counter.alloc(m->NC) || m->D_near.alloc(10 * static_cast<size_t>(m->N)) ||
         m->scan_local.alloc(10 * static_cast<size_t>(m->N)) ||
         m->scan_blocks.alloc(10 * static_cast<size_t>((m->N + SCAN_BLOCK - 1) / SCAN_BLOCK + 1)) ||

@@ -98,7 +98,6 @@ struct rpb_mesh {
     // geometry state
     rpb::DevBuf<rpb::PrimDatum> P_pair;
     rpb::DevBuf<rpb::ClusterDatum> C_pair;
-    rpb::DevBuf<double> C_mom;
     rpb::DevBuf<double> scan_local, scan_blocks;   // prefix sums of the moment upsweep
     rpb::DevBuf<unsigned> counter;
     // near-hull data for very-near quadrature (N x (1 + 3 size + 6), FP64)
