@@ -86,7 +86,10 @@ rpb_status rpb_mesh_get_stream(const rpb_mesh* m, void** stream);
 
 /* SimplicialMesh::SemiStaticUpdate (src/SimplicialMesh.hpp:354-376): new coordinates,
  * same tree and pair lists; recomputes primitive data and the cluster moment upsweep.
- * transp != 0 reads V column-major (3 x nV). */
+ * transp != 0 reads V column-major (3 x nV). The copy of V is queued on the mesh stream:
+ * pageable host memory is read before the call returns, page-locked memory (cudaHostAlloc,
+ * pinned tensors) only when the stream gets there, so a page-locked V must stay unchanged
+ * until the next synchronizing call (Value, Differential with host Y) has returned. */
 rpb_status rpb_mesh_semistatic_update(rpb_mesh* m, const double* V, int transp);
 rpb_status rpb_mesh_semistatic_update_device(rpb_mesh* m, const double* V_dev);
 
