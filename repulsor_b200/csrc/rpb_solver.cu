@@ -480,7 +480,8 @@ __global__ void k_cg_direction(int n, const double* S, bool flexible, const doub
 // After an iteration: count it, and freeze the columns whose recurrence residual met the
 // tolerance (||r_c||^2 <= tol^2 ||b_c||^2), recording the iteration at which they did.
 // Also keeps rz as rz_old for the next direction update.
-__global__ void k_cg_check(double* S, double tol2)
+// rz_is_rr: no preconditioner (z = r), so the new rz is the (r, r) just computed.
+__global__ void k_cg_check(double* S, double tol2, bool rz_is_rr)
 {
     S[S_IT] += 1.0;
     for (int c = 0; c < 3; ++c) {
@@ -489,6 +490,7 @@ __global__ void k_cg_check(double* S, double tol2)
             S[S_CONV_IT + c] = S[S_IT];
         }
         S[S_RZOLD + c] = S[S_RZ + c];
+        if (rz_is_rr) S[S_RZ + c] = S[S_RR + c];
     }
 }
 
@@ -777,10 +779,13 @@ static rpb_status cg_solve(rpb_mesh* m, double q, double p, const double* B, int
         if ((e = dot3(m, pv, Ap, nullptr, S + S_PAP, nullptr)) != RPB_OK) return e;
         k_cg_update_rr<<<std::min(1024, eb), 256, 0, stream>>>(n, S, x, r, pv, Ap, flexible ? rold : nullptr,
                                                                s.partials.ptr, s.done.ptr);
-        k_cg_check<<<1, 1, 0, stream>>>(S, tol2);
-        if ((e = apply_preconditioner(m, k, q, p, r, z)) != RPB_OK) return e;
-        if ((e = dot3(m, z, r, flexible ? rold : nullptr, S + S_RZ, S + S_ZROLD)) != RPB_OK) return e;
-        k_cg_direction<<<eb, 256, 0, stream>>>(n, S, flexible, z, pv);
+        const bool plain = k == RPB_PRECOND_NONE && !flexible;
+        k_cg_check<<<1, 1, 0, stream>>>(S, tol2, plain);
+        if (!plain) {
+            if ((e = apply_preconditioner(m, k, q, p, r, z)) != RPB_OK) return e;
+            if ((e = dot3(m, z, r, flexible ? rold : nullptr, S + S_RZ, S + S_ZROLD)) != RPB_OK) return e;
+        }
+        k_cg_direction<<<eb, 256, 0, stream>>>(n, S, flexible, plain ? r : z, pv);
         RPB_CUDA(cudaGetLastError());
         return RPB_OK;
     };
