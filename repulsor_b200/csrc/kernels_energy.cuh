@@ -449,10 +449,10 @@ constexpr int pair_blocks(int rows, int lanes) { return (rows * lanes + PAIR_BLO
 // Row tiles of the shared-memory kernels: threads per block (two blocks per SM), the mean
 // rows per tile the host aims below, and the largest column union a tile may stage. The
 // host sizes the tiles so that their count is a whole number of waves of resident blocks.
-constexpr int PAIR_TILE_THREADS = 288;
-constexpr int NEAR_TILE_ROWS = 288;
-constexpr int FAR_TILE_ROWS = 144;
-constexpr int NEAR_TILE_UNION = 1024;
+constexpr int PAIR_TILE_THREADS = 384;
+constexpr int NEAR_TILE_ROWS = 384;
+constexpr int FAR_TILE_ROWS = 192;
+constexpr int NEAR_TILE_UNION = 960;
 constexpr int FAR_TILE_UNION = 1536;
 
 // One lane's share of a row: the row's entries k = k0 + sub, k0 + sub + stride, ... with the
@@ -485,11 +485,18 @@ __device__ __noinline__ Close64 close_pair_fp64(TPExp ex, int dom, Datum X, ColD
     return c;
 }
 
-template <bool FAR, int QH, int PH, bool DIFF, bool CROSS, bool PREFETCH, typename ColDatum, typename Datum,
-          typename Index, typename Fetch>
+// SACC: the row's FP64 derivative accumulators live in shared memory at
+// Dsm[m * PAIR_TILE_THREADS] (zeroed by the caller) instead of D64, which is then filled
+// from them at the end; this keeps 20 registers free inside the loop.
+template <bool FAR, int QH, int PH, bool DIFF, bool CROSS, bool PREFETCH, bool SACC, typename ColDatum,
+          typename Datum, typename Index, typename Fetch>
 __device__ __forceinline__ void pair_row(const PairArgs& A, const Datum& X, int i, int sub, int stride, Index index,
-                                         Fetch datum, double& e_row, double (&D64)[10])
+                                         Fetch datum, double& e_row, double (&D64)[10], double* Dsm)
 {
+    auto add64 = [&](int m, double v) {
+        if constexpr (SACC) Dsm[m * PAIR_TILE_THREADS] += v;
+        else D64[m] += v;
+    };
     const float ax = static_cast<float>(X.a);
     PairAcc<float> acc = {};
     float e32 = 0.0f;
@@ -526,7 +533,7 @@ __device__ __forceinline__ void pair_row(const PairArgs& A, const Datum& X, int 
                 if (CROSS || j > i) e_row += c.e;
                 if (DIFF) {
 #pragma unroll
-                    for (int m = 0; m < 10; ++m) D64[m] += c.d[m];
+                    for (int m = 0; m < 10; ++m) add64(m, c.d[m]);
                 }
             }
         } else {
@@ -537,11 +544,11 @@ __device__ __forceinline__ void pair_row(const PairArgs& A, const Datum& X, int 
                 e_row += e32;
                 e32 = 0.0f;
                 if (DIFF) {
-                    D64[0] += acc.d0;
+                    add64(0, acc.d0);
 #pragma unroll
-                    for (int m = 0; m < 3; ++m) D64[1 + m] += acc.dx[m];
+                    for (int m = 0; m < 3; ++m) add64(1 + m, acc.dx[m]);
 #pragma unroll
-                    for (int m = 0; m < 6; ++m) D64[4 + m] += acc.dP[m];
+                    for (int m = 0; m < 6; ++m) add64(4 + m, acc.dP[m]);
                     acc = PairAcc<float>{};
                 }
             }
@@ -549,11 +556,14 @@ __device__ __forceinline__ void pair_row(const PairArgs& A, const Datum& X, int 
     }
     e_row += e32;
     if (DIFF) {
-        D64[0] += acc.d0;
+        add64(0, acc.d0);
 #pragma unroll
-        for (int m = 0; m < 3; ++m) D64[1 + m] += acc.dx[m];
+        for (int m = 0; m < 3; ++m) add64(1 + m, acc.dx[m]);
 #pragma unroll
-        for (int m = 0; m < 6; ++m) D64[4 + m] += acc.dP[m];
+        for (int m = 0; m < 6; ++m) add64(4 + m, acc.dP[m]);
+        if constexpr (SACC)
+#pragma unroll
+            for (int m = 0; m < 10; ++m) D64[m] = Dsm[m * PAIR_TILE_THREADS];
     }
 }
 
@@ -649,7 +659,7 @@ __global__ void __launch_bounds__(PAIR_BLOCK) k_tp0_pairs(PairArgs A)
             j = u;
             Y = load_datum(cols, u);
         };
-        pair_row<FAR, QH, PH, DIFF, CROSS, true, Datum>(A, X, i, sub, LANES, index, datum, e_row, D64);
+        pair_row<FAR, QH, PH, DIFF, CROSS, true, false, Datum>(A, X, i, sub, LANES, index, datum, e_row, D64, nullptr);
     }
     pair_epilogue<DIFF, CROSS>(A, active, i, sub, LANES, LANES, e_row, D64, blockIdx.x, gridDim.x);
 }
@@ -690,9 +700,15 @@ __device__ __forceinline__ ClusterDatum load_cluster_rot(const float4* sdat, int
 
 // dynamic shared memory per tile of union size n: the data (PrimTile 80 bytes, ClusterDatum
 // 64 bytes), then the column ids
+__host__ __device__ constexpr size_t pair_tile_union_bytes(int n, bool far)
+{
+    return (static_cast<size_t>(n) * ((far ? sizeof(ClusterDatum) : sizeof(PrimTile)) + sizeof(int)) + 15) / 16 * 16;
+}
+
+// union + column ids; near tiles also the FP64 derivative accumulators of every thread
 __host__ __device__ constexpr size_t pair_tile_smem(int n, bool far)
 {
-    return static_cast<size_t>(n) * ((far ? sizeof(ClusterDatum) : sizeof(PrimTile)) + sizeof(int));
+    return pair_tile_union_bytes(n, far) + (far ? 0 : sizeof(double) * 10 * PAIR_TILE_THREADS);
 }
 
 template <bool FAR, int QH, int PH, bool DIFF>
@@ -746,6 +762,14 @@ __device__ __forceinline__ void pairs_tiled_body(const PairArgs& A, const PairTi
     __syncthreads();
     double e_row = 0.0;
     double D64[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    double* Dsm = nullptr;
+    if constexpr (!FAR && DIFF) {
+        // this thread's accumulators, after the union (pair_tile_smem)
+        Dsm = reinterpret_cast<double*>(reinterpret_cast<char*>(tile_smem) + pair_tile_union_bytes(un, false)) +
+              threadIdx.x;
+#pragma unroll
+        for (int m = 0; m < 10; ++m) Dsm[m * PAIR_TILE_THREADS] = 0.0;
+    }
     if (active) {
         auto index = [&](int64_t k) { return static_cast<int>(__ldg(T.slot + k)); };
         auto datum = [&](int u, int& j, ColDatum& Y) {
@@ -753,7 +777,8 @@ __device__ __forceinline__ void pairs_tiled_body(const PairArgs& A, const PairTi
             else Y = reinterpret_cast<const PrimTile*>(tile_smem)[u];
             j = sid[u];
         };
-        pair_row<FAR, QH, PH, DIFF, false, false, ColDatum>(A, X, i, sub, size, index, datum, e_row, D64);
+        pair_row<FAR, QH, PH, DIFF, false, false, !FAR && DIFF, ColDatum>(A, X, i, sub, size, index, datum, e_row, D64,
+                                                                        Dsm);
     }
     pair_epilogue<DIFF, false>(A, active, i, sub, size, warp_size_max, e_row, D64, bid, nblocks);
 }
