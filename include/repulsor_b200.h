@@ -309,20 +309,26 @@ rpb_status rpb_tpm0_learned_apply(rpb_mesh* m, const double* R, double* Z);
 /* --- energy without device allocation -------------------------------------------------- */
 
 /* No counterpart in the reference (Repulsor has no device path). TangentPointEnergy0
- * Value for callers that cannot allocate device memory when they need the energy (inside
- * CUDA graph capture, under a fixed memory arena, in loops that forbid allocation). All
- * pointers are device pointers the caller owns: V (nV x 3), S (nS x (dom_dim+1)), the tree
- * (perm: nS, C_begin/C_end: nC) and the full symmetric near/far patterns as returned by
- * rpb_mesh_tree/rpb_mesh_pattern; the energy (1 double) is written asynchronously on
- * `stream`. Unit charges; the very-near list must be empty. Scratch lives in one static
- * device array of about 12.4 MB (at most 40,960 simplices, larger meshes give RPB_EINVAL)
- * held by every device that loads the library; the first call on a device looks up its
- * address and should come before any stream capture; calls that overlap on the GPU race
- * on the shared scratch. Allocates nothing. */
+ * Value for callers that cannot allocate device memory when they need the energy: hosts
+ * whose device memory belongs to a fixed-size arena or pool, and real-time or inner-loop
+ * code that forbids allocation after start-up (an allocation can synchronize the device or
+ * fail under memory pressure). All pointers are device pointers the caller owns: V
+ * (nV x 3), S (nS x (dom_dim+1)), the tree (perm: nS, C_begin/C_end: nC) and the full
+ * symmetric near/far patterns exactly as rpb_mesh_tree/rpb_mesh_pattern return them for
+ * this mesh (only sizes are checked); verynear_nnz is rpb_stats.verynear_nnz of the mesh
+ * and must be 0 (meshes with very-near pairs give RPB_EINVAL: use rpb_tpe0_value). The
+ * energy (1 double) is written asynchronously on `stream`. Unit charges. Scratch lives in
+ * one static device array of about 12.4 MB (at most 40,960 simplices and 2 nS - 1
+ * clusters; larger meshes give RPB_EINVAL) held by every device that loads the library
+ * until the process exits; the first call on a device looks up the array's address and
+ * should come before any stream capture; all calls share the array, so calls that overlap
+ * on the GPU (other streams, other host threads) race and must be serialised by the
+ * caller. Calls no cudaMalloc, cudaFree or allocating library routine. */
 rpb_status rpb_tpe0_value_noalloc(int dom_dim, const double* V, int64_t nV, const int* S, int64_t nS,
                                   const int* perm, const int* C_begin, const int* C_end, int64_t nC,
                                   const int64_t* near_rowptr, const int* near_colidx, const int64_t* far_rowptr,
-                                  const int* far_colidx, double q, double p, double* energy, void* stream);
+                                  const int* far_colidx, int64_t verynear_nnz, double q, double p, double* energy,
+                                  void* stream);
 
 /* --- measurement (no reference counterpart: Repulsor has no device path) ------------------ */
 

@@ -55,6 +55,9 @@ def _load():
     lib.oracle_partial_derivatives.restype = ctypes.c_double
     lib.oracle_partial_derivatives.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                                ctypes.c_int, _dp, _dp]
+    lib.oracle_row_derivatives.restype = ctypes.c_double
+    lib.oracle_row_derivatives.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double, ctypes.c_int64,
+                                           ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, _dp, _dp]
     lib.oracle_pair_opcounts.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, _lp]
     lib.oracle_maximum_safe_step_size.restype = ctypes.c_double
     lib.oracle_maximum_safe_step_size.argtypes = [ctypes.c_void_p, _dp, ctypes.c_double, ctypes.c_double]
@@ -229,6 +232,21 @@ class OracleMesh:
         Dn = np.zeros((self.nS, nd))
         Df = np.zeros((self.counts()["clusters"], 10))
         e = _load().oracle_partial_derivatives(self._h, q, p, shard, shards, _d(Dn), _d(Df))
+        return Dn, Df, e
+
+    def row_derivatives(self, near_rows, far_rows, q=6.0, p=12.0):
+        """Slices of a disjoint row partition: rows near_rows = [first, last) of the full
+        Near() pattern and far_rows of Far(), each pair evaluated from its row with only
+        the row's derivative accumulated (zero outside the rows), and the energy of the
+        pairs with j > i in those rows. Summed over a partition of all rows they equal
+        the unsharded slices."""
+        nd = 1 + (self.dom + 1) * 3 + 6
+        Dn = np.zeros((self.nS, nd))
+        Df = np.zeros((self.counts()["clusters"], 10))
+        e = _load().oracle_row_derivatives(self._h, q, p, int(near_rows[0]), int(near_rows[1]), int(far_rows[0]),
+                                           int(far_rows[1]), _d(Dn), _d(Df))
+        if np.isnan(e):
+            raise ValueError("row-owned slices are not built for meshes with very-near pairs")
         return Dn, Df, e
 
     def collect(self, Dn, Df, alpha=1.0, beta=0.0, Y=None):

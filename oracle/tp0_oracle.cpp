@@ -2474,6 +2474,65 @@ double oracle_partial_derivatives(void* h, double q, double p, int shard, int sh
     return en;
 }
 
+// Row-owned slices for a disjoint row partition (the decomposition of the device's row
+// shards): rows [near_first, near_last) of the FULL symmetric Near() pattern and rows
+// [far_first, far_last) of Far(), every pair evaluated from its row with only the row's
+// derivative DX accumulated (no column scatter), the energy of the pairs with j > i. The
+// slices of a partition of all rows sum to the upper-triangle traversal's
+// (FMM_Traversor.hpp:56-147 visits each pair once and scatters DY to the column instead).
+// Meshes with very-near pairs are rejected (returns NaN), as by the device's shards.
+double oracle_row_derivatives(void* h, double q, double p, int64_t near_first, int64_t near_last, int64_t far_first,
+                              int64_t far_last, double* D_near, double* D_far)
+{
+    Mesh& M = static_cast<OracleHandle*>(h)->M;
+    if (M.verynear.nnz() > 0) return std::numeric_limits<double>::quiet_NaN();
+    const TPParams T(q, p, M.dom);
+    const int nd = near_dim(M.dom);
+    const int SIZE = M.SIZE;
+    const double S_scale = 1.0 / SIZE;
+    std::fill(D_near, D_near + static_cast<size_t>(M.nS) * nd, 0.0);
+    std::fill(D_far, D_far + static_cast<size_t>(M.NC) * FAR_DIM, 0.0);
+    double en = 0;
+    auto bary = [&](const double* Z, double* x) {
+        for (int k = 0; k < 3; ++k) {
+            x[k] = S_scale * Z[1 + k];
+            for (int v = 1; v < SIZE; ++v) x[k] += S_scale * Z[1 + AMB * v + k];
+        }
+    };
+    for (int64_t i = near_first; i < near_last && M.near.nnz() > 0; ++i) {
+        const double* Xi = &M.P_near[nd * static_cast<size_t>(i)];
+        double x[3];
+        bary(Xi, x);
+        double* DX = &D_near[nd * static_cast<size_t>(i)];
+        for (LInt k = M.near.rp[i]; k < M.near.rp[i + 1]; ++k) {
+            const Int j = M.near.ci[k];
+            const double* Yj = &M.P_near[nd * static_cast<size_t>(j)];
+            double y[3];
+            bary(Yj, y);
+            PairOut o;
+            tp0_pair(T, Xi[0], x, Xi + 1 + AMB * SIZE, Yj[0], y, Yj + 1 + AMB * SIZE, true, false, o);
+            if (j > i) en += o.energy;
+            DX[0] += o.DX[0];
+            for (int v = 0; v < SIZE; ++v)
+                for (int kk = 0; kk < 3; ++kk) DX[1 + 3 * v + kk] += S_scale * o.DX[1 + kk];
+            for (int kk = 0; kk < 6; ++kk) DX[1 + AMB * SIZE + kk] += o.DX[4 + kk];
+        }
+    }
+    for (int64_t i = far_first; i < far_last && M.far.nnz() > 0; ++i) {
+        const double* Xi = &M.C_far[FAR_DIM * static_cast<size_t>(i)];
+        double* DX = &D_far[FAR_DIM * static_cast<size_t>(i)];
+        for (LInt k = M.far.rp[i]; k < M.far.rp[i + 1]; ++k) {
+            const Int j = M.far.ci[k];
+            const double* Yj = &M.C_far[FAR_DIM * static_cast<size_t>(j)];
+            PairOut o;
+            tp0_pair(T, Xi[0], Xi + 1, Xi + 4, Yj[0], Yj + 1, Yj + 4, true, false, o);
+            if (j > i) en += o.energy;
+            for (int kk = 0; kk < 10; ++kk) DX[kk] += o.DX[kk];
+        }
+    }
+    return en;
+}
+
 // Collection (percolate-down, primitive copy, unpermute), chain rule and vertex scatter
 // from summed slices: Y = alpha dE + beta Y.
 void oracle_collect(void* h, const double* D_near, const double* D_far, double alpha, double beta, double* Y, int ldY)

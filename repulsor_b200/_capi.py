@@ -98,8 +98,8 @@ SIGNATURES = {
                                             _dp]),
     "rpb_measure_fp32_peak": (ctypes.c_int, [ctypes.c_int, _dp]),
     "rpb_tpe0_value_noalloc": (ctypes.c_int, [ctypes.c_int, _vp, ctypes.c_int64, _vp, ctypes.c_int64, _vp, _vp, _vp,
-                                              ctypes.c_int64, _vp, _vp, _vp, _vp, ctypes.c_double, ctypes.c_double,
-                                              _vp, _vp]),
+                                              ctypes.c_int64, _vp, _vp, _vp, _vp, ctypes.c_int64, ctypes.c_double,
+                                              ctypes.c_double, _vp, _vp]),
     "rpb_tpm0_solve_info": (ctypes.c_int, [_vp, ctypes.POINTER(SolveInfo)]),
     "rpb_tpe0_energy_device": (ctypes.c_int, [_vp, _vp]),
     "rpb_mesh_maximum_safe_step_size": (ctypes.c_int, [_vp, _dp, ctypes.c_double, ctypes.c_double, _dp]),

@@ -1,16 +1,18 @@
 // Energy evaluation that allocates no device memory.
 //
-// Some callers cannot call cudaMalloc at the point where they need the energy: code that
-// runs while a CUDA graph is being captured (allocations are not capturable), hosts whose
-// device memory is owned by a fixed-size arena or pool with no way to hand out more, and
-// real-time loops that forbid allocation after start-up. rpb_tpe0_value_noalloc serves
+// Some callers cannot call cudaMalloc at the point where they need the energy: hosts whose
+// device memory is owned by a fixed-size arena or pool with no way to hand out more (a
+// simulation or renderer that reserves all of its memory at start-up), and real-time or
+// inner-loop code that forbids allocation after start-up because an allocation can
+// synchronize the device or fail under memory pressure. rpb_tpe0_value_noalloc serves
 // them: it runs the same geometry, moment-upsweep and pair kernels as rpb_tpe0_value, but
 // its scratch memory (primitive and cluster pair data, prefix sums, block partials) lives
 // in one file-scope device array of fixed size instead of buffers owned by an rpb_mesh.
 //
 // Limits and behaviour:
 //  * at most RPB_NOALLOC_MAX_SIMPLICES simplices (40,960) and 2*that-1 clusters; larger
-//    meshes are rejected with RPB_EINVAL;
+//    meshes are rejected with RPB_EINVAL, and so are meshes with very-near primitive pairs
+//    (this entry point evaluates the near and far lists only);
 //  * the array (about 12.4 MB) is part of the module: every GPU that loads the library
 //    holds it until the process exits;
 //  * the first call on a device looks up the array's device address (cudaGetSymbolAddress)
@@ -18,6 +20,8 @@
 //  * all calls share the one array and it keeps the last call's contents, so calls whose
 //    work overlaps on the GPU (different streams, or several host threads) race; the
 //    counters that must start at zero are cleared at the start of every call;
+//  * perm, C_begin and C_end must be the tree of the same mesh as returned by
+//    rpb_mesh_tree, and the patterns those of rpb_mesh_pattern: only the sizes are checked;
 //  * no cudaMalloc, cudaFree or allocating library routine is called.
 #include <mutex>
 #include <string>
@@ -88,18 +92,28 @@ using namespace rpb;
 extern "C" rpb_status rpb_tpe0_value_noalloc(int dom_dim, const double* V, int64_t nV, const int* S, int64_t nS,
                                              const int* perm, const int* C_begin, const int* C_end, int64_t nC,
                                              const int64_t* near_rowptr, const int* near_colidx,
-                                             const int64_t* far_rowptr, const int* far_colidx, double q, double p,
-                                             double* energy, void* stream)
+                                             const int64_t* far_rowptr, const int* far_colidx, int64_t verynear_nnz,
+                                             double q, double p, double* energy, void* stream)
 {
     if (dom_dim != 1 && dom_dim != 2) { set_error("rpb_tpe0_value_noalloc: domain dimension must be 1 or 2"); return RPB_EINVAL; }
     if (!V || !S || !perm || !C_begin || !C_end || !near_rowptr || !far_rowptr || !energy || nV <= 0 || nS <= 0) {
         set_error("rpb_tpe0_value_noalloc: null or empty argument");
         return RPB_EINVAL;
     }
+    if (verynear_nnz != 0) {
+        set_error("rpb_tpe0_value_noalloc: the mesh has very-near primitive pairs (verynear_nnz = " +
+                  std::to_string(verynear_nnz) + "), which this entry point does not evaluate; use rpb_tpe0_value");
+        return RPB_EINVAL;
+    }
     if (nS > kMaxSimplices || nC > kMaxClusters || nC < 1) {
         set_error("rpb_tpe0_value_noalloc: the mesh exceeds the fixed scratch size (at most " +
                   std::to_string(kMaxSimplices) + " simplices and " + std::to_string(kMaxClusters) +
                   " clusters); use rpb_tpe0_value");
+        return RPB_EINVAL;
+    }
+    if (nC > 2 * nS - 1) {
+        set_error("rpb_tpe0_value_noalloc: nC = " + std::to_string(nC) + " exceeds 2 nS - 1 = " +
+                  std::to_string(2 * nS - 1) + "; pass the tree rpb_mesh_tree returns for this mesh");
         return RPB_EINVAL;
     }
     rpb_status st = check_exponents(q, p);

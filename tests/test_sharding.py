@@ -1,8 +1,11 @@
 """Row-sharded evaluation of one mesh over several processes (repulsor_b200/sharding.py,
-rpb_tpe0_pairs_shard / rpb_tpe0_collect_shards). CPU: the partition, and two gloo ranks
-that each evaluate one shard with the oracle (upper-triangle rows split like the
-reference's threads), all-reduce the derivative slices and collect -- the same
-composition the GPU path uses. GPU: the shards of one mesh evaluated in turn on one GPU
+rpb_tpe0_pairs_shard / rpb_tpe0_collect_shards). CPU: the partition; two gloo ranks that
+each evaluate one shard with the oracle (upper-triangle rows split like the reference's
+threads), all-reduce the derivative slices and collect; and the exchange the GPU path
+uses -- ranks that own disjoint rows of the full patterns all-gather only those rows (the
+oracle's row-owned slices, and synthetic buffers on 2 and 3 ranks whose assembly must
+equal the all-reduced sum and whose received bytes are about half a ring all-reduce's).
+GPU: the shards of one mesh evaluated in turn on one GPU
 and summed equal the unsharded Differential, and the torch.distributed driver with a
 one-rank NCCL group equals it too (every GPU call of this build has one GPU)."""
 import ctypes
@@ -19,7 +22,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 sys.path.insert(0, ROOT)
 
 from repulsor_b200 import meshes  # noqa: E402
-from repulsor_b200.sharding import shard_range  # noqa: E402
+from repulsor_b200.sharding import exchange_layout, exchange_rows, shard_range  # noqa: E402
 
 Q, P = 6.0, 12.0
 
@@ -69,6 +72,75 @@ def test_two_gloo_ranks_all_reduce_shard_slices_to_the_full_differential():
         e, E_full, dy = res[r]
         assert abs(e - E_full) <= 1e-13 * abs(E_full)
         assert dy <= 1e-13
+
+
+def _gather_rows_rank(rank, world, port, out):
+    sys.path.insert(0, ROOT)
+    import oracle
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        # the oracle's row-owned slices, exchanged by the all-gather of owned rows
+        dom, (V, S) = meshes.config_mesh(2, small=True)
+        O = oracle.OracleMesh(dom, V, S)
+        N, NC = O.nS, O.counts()["clusters"]
+        near = [shard_range(N, world, s) for s in range(world)]
+        far = [shard_range(NC, world, s) for s in range(world)]
+        Dn, Df, e = O.row_derivatives(near[rank], far[rank], Q, P)
+        nd = Dn.shape[1]
+        buf = torch.from_numpy(np.concatenate([Dn.ravel(), Df.ravel(), [e]]))
+        pieces, chunk = exchange_layout(near, far, N, near_dim=nd, far_dim=10)
+        received = exchange_rows(buf, pieces, chunk, rank)
+        b = buf.numpy()
+        Y = O.collect(b[:Dn.size].reshape(Dn.shape), b[Dn.size:Dn.size + Df.size].reshape(Df.shape))
+        E_full, Y_full = O.differential(Q, P)
+        res = [float(b[-1]), E_full, float(np.abs(Y - Y_full).max() / np.abs(Y_full).max()), received, buf.numel()]
+        # synthetic buffers: random rows owned by this rank, zero elsewhere; the assembly
+        # must equal the sum over ranks (bit for bit: each row has one owner)
+        n_near, n_far = 1001 + 7 * world, 2003
+        near = [shard_range(n_near, world, s) for s in range(world)]
+        far = [shard_range(n_far, world, s) for s in range(world)]
+        pieces, chunk = exchange_layout(near, far, n_near)
+
+        def shard_buffer(s):
+            g = np.random.default_rng(100 + s)
+            x = np.zeros(10 * (n_near + n_far) + 1)
+            for off, n in pieces[s]:
+                x[off:off + n] = g.standard_normal(n)
+            x[-1] = g.standard_normal()
+            return x
+
+        mine = torch.from_numpy(shard_buffer(rank))
+        got = exchange_rows(mine, pieces, chunk, rank)
+        want = np.sum([shard_buffer(s) for s in range(world)], axis=0)
+        e_sum = 0.0
+        for s in range(world):
+            e_sum += shard_buffer(s)[-1]
+        want[-1] = e_sum
+        res += [bool(np.array_equal(mine.numpy(), want)), got, mine.numel()]
+        out[rank] = res
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_all_gather_of_owned_rows_composes_the_full_differential(world):
+    port = 29650 + world + os.getpid() % 900
+    with mp.get_context("spawn").Manager() as manager:
+        out = manager.dict()
+        mp.spawn(_gather_rows_rank, args=(world, port, out), nprocs=world, join=True)
+        res = dict(out)
+    for r in range(world):
+        e, E_full, dy, received, total, exact, got, total2 = res[r]
+        assert abs(e - E_full) <= 1e-13 * abs(E_full)
+        assert dy <= 1e-12
+        assert exact
+        # received doubles: each other shard's rows once (+ its energy); a ring all-reduce
+        # of the whole buffer moves 2 (W-1)/W of it through every rank
+        for rec, n in ((received, total), (got, total2)):
+            assert rec <= (world - 1) / world * n * 1.01 + world
+            assert rec <= 0.51 * 2 * (world - 1) / world * n + world
 
 
 @pytest.mark.gpu
