@@ -305,6 +305,18 @@ rpb_status rpb_mlp_train_step(rpb_mlp* mlp, rpb_mesh* m, double q, double p, con
 rpb_status rpb_mesh_set_learned(rpb_mesh* m, rpb_mlp* mlp);
 /* Z = M(R) for one residual (host arrays, n_v x 3, row-major). */
 rpb_status rpb_tpm0_learned_apply(rpb_mesh* m, const double* R, double* Z);
+/* Z = M(R) and, with Y and ZY non-NULL, ZY = M_R(Y): the preconditioner with the gains the
+ * network gave for R applied to another vector Y (the linearization of M at R with the
+ * gains held fixed), which the adjoint pass of unrolled-solve training needs. */
+rpb_status rpb_tpm0_learned_apply_pair(rpb_mesh* m, const double* R, const double* Y, double* Z, double* ZY);
+/* One Adam step (lr <= 0: none) on the objective sum_k G_k . M(R_k) over npairs pairs of
+ * residuals R_k and sensitivities G_k = dL/dz_k (host, n_v x 3 each, consecutive), plus
+ * reg * mean over clusters and components of o_C^2: the parameter gradient of a loss L that
+ * depends on the preconditioner outputs z_k = M(R_k) through G_k, e.g. the residual after
+ * an unrolled preconditioned CG. objective (sum_k G_k . z_k) and grad (param_count floats,
+ * with the penalty) may be NULL; both are taken before the step. */
+rpb_status rpb_mlp_train_step_sens(rpb_mlp* mlp, rpb_mesh* m, const double* R, const double* G, int npairs,
+                                   double lr, double reg, double* objective, float* grad);
 
 /* --- energy without device allocation -------------------------------------------------- */
 

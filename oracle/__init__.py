@@ -28,6 +28,17 @@ def build():
     subprocess.run(["make", "-s", "-C", _HERE], check=True)
 
 
+def use_timed_build():
+    """Use the build with the reference's optimization flags (-O3 -ffast-math, see the
+    Makefile) for this process; only bench.py's CPU baseline does, before its first call.
+    Returns the library path."""
+    global _LIB_PATH
+    if _lib is not None:
+        raise RuntimeError("the oracle library is already loaded")
+    _LIB_PATH = os.path.join(_HERE, "_build", "libtp0_oracle_timed.so")
+    return _LIB_PATH
+
+
 def _load():
     global _lib
     if _lib is not None:

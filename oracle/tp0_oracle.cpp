@@ -930,12 +930,12 @@ static void subdivide(int dom, const SubSimplex& s, std::vector<SubSimplex>& out
 // the GJK MAC with theta_near holds or the level limit is reached. emit() gets the
 // sub-simplex centres, their weights w_S, w_T and barycentric centres.
 template <typename Emit>
-static void vf_quadrature(const Mesh& M, Int i, Int j, Emit&& emit)
+static void vf_quadrature(const Mesh& M, Int i, const Mesh& O, Int j, Emit&& emit)
 {
     const int dom = M.dom, SIZE = M.SIZE;
     const int nd = near_dim(dom);
     const double* X = &M.P_near[nd * static_cast<size_t>(i)];
-    const double* Y = &M.P_near[nd * static_cast<size_t>(j)];
+    const double* Y = &O.P_near[nd * static_cast<size_t>(j)];
     const double near_t2 = M.set.theta_near * M.set.theta_near;
     SubSimplex root{};
     for (int c = 0; c < 3; ++c)
@@ -1059,7 +1059,7 @@ static double tp0_evaluate(Mesh& M, double q, double p, bool diff, int shards = 
                     const Int j = Pt.ci[k];
                     const double* Xi = &M.P_near[nd * static_cast<size_t>(i)];
                     const double* Yj = &M.P_near[nd * static_cast<size_t>(j)];
-                    vf_quadrature(M, i, j, [&](const double* x, const double* y, double ws, double wt,
+                    vf_quadrature(M, i, M, j, [&](const double* x, const double* y, double ws, double wt,
                                                const double* bs, const double* bt) {
                         // sub-pair with weights a*w_S, b*w_T: energy w a E b, derivatives in
                         // (a, a*hull, a*P) coordinates (TP0_Kernel_VF.hpp:159-301)
@@ -1436,7 +1436,7 @@ static void tp0_metric_values(const Mesh& M, double q, double p, MetricValues& m
                 const Int j = Pt.ci[k];
                 const double* Yj = &M.P_near[nd * static_cast<size_t>(j)];
                 double a0 = 0, a1 = 0;
-                vf_quadrature(M, i, j, [&](const double* x, const double* y, double ws, double wt, const double*, const double*) {
+                vf_quadrature(M, i, M, j, [&](const double* x, const double* y, double ws, double wt, const double*, const double*) {
                     PairOut o;
                     tp0_pair(T, Xi[0], x, Xi + 1 + AMB * SIZE, Yj[0], y, Yj + 1 + AMB * SIZE, false, true, o);
                     a0 += ws * wt * o.a0;
@@ -1816,6 +1816,37 @@ static double obstacle_evaluate(Mesh& M, const Mesh& O, const ObstacleLists& L, 
             for (int v = 0; v < X.SIZE; ++v) c[k] += D[1 + AMB * v + k] / X.SIZE;
         }
     };
+    {   // VF: the subdivision quadrature of TP0_Kernel_VF / FMM_Kernel_VF_Common on the
+        // (mesh, obstacle) very-near pairs, every pair once with the symmetry factor 1/2
+        const CrossPattern& Pt = L.verynear;
+        std::vector<double> part(threads, 0.0);
+        parallel_do(threads, [&](int t) {
+            double local = 0;
+            for (Int i = job_pointer(M.nS, threads, t); i < job_pointer(M.nS, threads, t + 1); ++i) {
+                const double* Xi = &M.P_near[nd * static_cast<size_t>(i)];
+                for (LInt k = Pt.rp[i]; k < Pt.rp[i + 1]; ++k) {
+                    const Int j = Pt.ci[k];
+                    const double* Yj = &O.P_near[near_dim(O.dom) * static_cast<size_t>(j)];
+                    vf_quadrature(M, i, O, j, [&](const double* x, const double* y, double ws, double wt,
+                                                  const double* bs, const double*) {
+                        PairOut o;
+                        tp0_pair(T, Xi[0] * ws, x, Xi + 1 + AMB * SIZE, Yj[0] * wt, y, Yj + 1 + AMB * O.SIZE, diff,
+                                 false, o);
+                        local += sf * o.energy;
+                        if (diff) {
+                            double* DX = &tDn[t][nd * static_cast<size_t>(i)];
+                            DX[0] += sf * ws * o.DX[0];
+                            for (int v = 0; v < SIZE; ++v)
+                                for (int kk = 0; kk < 3; ++kk) DX[1 + 3 * v + kk] += sf * ws * bs[v] * o.DX[1 + kk];
+                            for (int kk = 0; kk < 6; ++kk) DX[1 + AMB * SIZE + kk] += sf * ws * o.DX[4 + kk];
+                        }
+                    });
+                }
+            }
+            part[t] = local;
+        });
+        for (double v : part) en += v;
+    }
     {   // NF
         const CrossPattern& Pt = L.near;
         std::vector<double> part(threads, 0.0);

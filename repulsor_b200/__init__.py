@@ -23,6 +23,7 @@ import ctypes
 import numpy as np
 
 from . import _capi
+from .meshio import read_mesh_file, write_mesh_file
 from ._capi import (PRECOND_LEARNED, PRECOND_NONE, PRECOND_REFERENCE, RepulsorError, Settings, Stats, check,
                     dptr, iptr, lptr)
 
@@ -32,8 +33,12 @@ __all__ = [
     "TangentPointEnergy0",
     "TangentPointMetric0",
     "TangentPointObstacleEnergy",
+    "SimplicialMesh_Factory",
     "TangentPointEnergy0_Factory",
     "TangentPointMetric0_Factory",
+    "TangentPointObstacleEnergy_Factory",
+    "read_mesh_file",
+    "write_mesh_file",
     "RepulsorError",
     "PRECOND_NONE",
     "PRECOND_REFERENCE",
@@ -106,6 +111,11 @@ class SimplicialMesh:
 
     def ClearCache(self):
         self._cache.clear()
+
+    def WriteToFile(self, path):
+        """SimplicialMesh::WriteToFile (src/SimplicialMesh.hpp:780-818): the current
+        coordinates and the simplices in the reference's mesh text format."""
+        write_mesh_file(path, self._V, self._S)
 
     def MaximumSafeStepSize(self, velocities, max_time: float, TOL: float = 0.0625) -> float:
         """SimplicialMesh::MaximumSafeStepSize (src/SimplicialMesh.hpp:441-468): the largest
@@ -504,6 +514,36 @@ class TangentPointMetric0:
         return float(np.sqrt(np.sum(np.asarray(X) * Y)))
 
 
+class SimplicialMesh_Factory:
+    """SimplicialMesh_Factory<MeshBase_T, min_dom, max_dom, min_amb, max_amb>
+    (src/SimplicialMesh/SimplicialMesh_Factory.hpp:8-246): meshes whose dimensions lie in
+    the factory's ranges; this build has domain dimensions 1 and 2 in ambient dimension 3."""
+
+    def __init__(self, min_dom=1, max_dom=2, min_amb=3, max_amb=3):
+        self.min_dom, self.max_dom, self.min_amb, self.max_amb = min_dom, max_dom, min_amb, max_amb
+
+    def Make(self, vertex_coords, vertex_count, amb_dim, vertex_coords_ColMajorQ, simplices, simplex_count,
+             simplex_size, simplices_ColMajorQ, thread_count=1, **settings):
+        dom_dim = simplex_size - 1
+        if not self.min_dom <= dom_dim <= self.max_dom:
+            raise RepulsorError(_capi.RPB_EINVAL, "SimplicialMesh_Factory::Make: dom_dim is out of range.")
+        if not self.min_amb <= amb_dim <= self.max_amb:
+            raise RepulsorError(_capi.RPB_EINVAL, "SimplicialMesh_Factory::Make: amb_dim is out of range.")
+        if amb_dim != 3 or dom_dim not in (1, 2):
+            raise RepulsorError(_capi.RPB_EINVAL, f"SimplicialMesh_Factory cannot create SimplicialMesh with domain "
+                                f"dimension {dom_dim} and ambient dimension {amb_dim}.")
+        V = np.asarray(vertex_coords, dtype=np.float64).reshape(-1)
+        S = np.asarray(simplices).reshape(-1)
+        V = V.reshape(amb_dim, vertex_count).T if vertex_coords_ColMajorQ else V.reshape(vertex_count, amb_dim)
+        S = S.reshape(simplex_size, simplex_count).T if simplices_ColMajorQ else S.reshape(simplex_count, simplex_size)
+        return SimplicialMesh(V, S.astype(np.int32), thread_count=max(1, int(thread_count)), **settings)
+
+    def Make_FromFile(self, path, thread_count=1, **settings):
+        """Reads a mesh in the reference's text format (read_mesh_file) and makes it."""
+        dom, amb, V, S = read_mesh_file(path)
+        return self.Make(V, V.shape[0], amb, False, S, S.shape[0], dom + 1, False, thread_count, **settings)
+
+
 class TangentPointEnergy0_Factory:
     """Runtime dispatch on (dom_dim, amb_dim) (src/Energies/TangentPointEnergy/TP_Factory.hpp:24-44)."""
 
@@ -520,3 +560,15 @@ class TangentPointMetric0_Factory:
         if amb_dim != 3 or dom_dim not in (1, 2):
             raise RepulsorError(_capi.RPB_EINVAL, "TangentPointMetric0_Factory: only (1,3) and (2,3) are built")
         return TangentPointMetric0(q, p)
+
+
+class TangentPointObstacleEnergy_Factory:
+    """Make(dom_dim_S, dom_dim_T, amb_dim, q, p) (src/Energies/TangentPointEnergy/TPO_Factory.hpp:8-95);
+    the mesh and the obstacle must have the same domain dimension in this build."""
+
+    @staticmethod
+    def Make(dom_dim_S, dom_dim_T, amb_dim, q, p):
+        if amb_dim != 3 or dom_dim_S not in (1, 2) or dom_dim_T != dom_dim_S:
+            raise RepulsorError(_capi.RPB_EINVAL, "TangentPointObstacleEnergy_Factory: only equal domain dimensions "
+                                "1 or 2 in ambient dimension 3 are built")
+        return TangentPointObstacleEnergy(q, p)

@@ -128,6 +128,9 @@ SIGNATURES = {
                                           ctypes.c_double, ctypes.c_double, _dp, _fp]),
     "rpb_mesh_set_learned": (ctypes.c_int, [_vp, _vp]),
     "rpb_tpm0_learned_apply": (ctypes.c_int, [_vp, _dp, _dp]),
+    "rpb_tpm0_learned_apply_pair": (ctypes.c_int, [_vp, _dp, _dp, _dp, _dp]),
+    "rpb_mlp_train_step_sens": (ctypes.c_int, [_vp, _vp, _dp, _dp, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                               _dp, ctypes.POINTER(ctypes.c_float)]),
 }
 
 _lib = None

@@ -45,7 +45,8 @@ int64_t rpb_mesh::device_bytes() const
              t->lane_map.bytes();
     b += P_pair.bytes() + C_pair.bytes() + counter.bytes() + P_near.bytes() + scan_local.bytes() +
          scan_blocks.bytes() + C_begin.bytes() + C_end.bytes();
-    b += D_near.bytes() + D_far.bytes() + D_vf.bytes() + B.bytes() + v_rp.bytes() + v_slot.bytes() + Y.bytes();
+    b += near_once.bytes() + far_once.bytes();
+    b += D_near.bytes() + D_far.bytes() + vf.bytes() + B.bytes() + v_rp.bytes() + v_slot.bytes() + Y.bytes();
     b += block_energy.bytes() + energy.bytes() + done.bytes();
     b += pre_cols.bytes() + pre_vals.bytes() + vp_rp.bytes() + vp_slot.bytes();
     b += buf_Pin64.bytes() + buf_Cin64.bytes() + buf_Pout.bytes() + buf_Cout.bytes() + buf_Z.bytes() + X.bytes() +
@@ -162,6 +163,12 @@ static cudaError_t allow_tile_smem_t()
     set(reinterpret_cast<const void*>(k_tp0_pairs_tiled<true, QH, PH, false>), fb);
     set(reinterpret_cast<const void*>(k_tp0_pairs_tiled_both<QH, PH, true>), std::max(nb, fb));
     set(reinterpret_cast<const void*>(k_tp0_pairs_tiled_both<QH, PH, false>), std::max(nb, fb));
+    set(reinterpret_cast<const void*>(k_tp0_pairs_tiled<false, QH, PH, true, true>), nb);
+    set(reinterpret_cast<const void*>(k_tp0_pairs_tiled<false, QH, PH, false, true>), nb);
+    set(reinterpret_cast<const void*>(k_tp0_pairs_tiled<true, QH, PH, true, true>), fb);
+    set(reinterpret_cast<const void*>(k_tp0_pairs_tiled<true, QH, PH, false, true>), fb);
+    set(reinterpret_cast<const void*>(k_tp0_pairs_tiled_both<QH, PH, true, true>), std::max(nb, fb));
+    set(reinterpret_cast<const void*>(k_tp0_pairs_tiled_both<QH, PH, false, true>), std::max(nb, fb));
     return e;
 }
 
@@ -192,72 +199,134 @@ static PairTiles tiles_view(const TileBufs& t, int first)
     return PairTiles{t.row0.ptr, t.cols_rp.ptr, t.cols.ptr, t.slot.ptr, t.order.ptr, t.lane_map.ptr, first};
 }
 
-// Shared-memory row tiles of the near and far patterns (one kernel block per tile). Tiles
-// are balanced by entries and their count is shards x a whole number of waves of resident
-// blocks (no partial last wave, whose few blocks would run while the other SMs idle), so
-// that each of `shards` GPUs owns whole waves; at most NEAR_TILE_ROWS / FAR_TILE_ROWS rows
-// per tile on average. A pattern whose rows exceed the union cap keeps the gather kernel.
-// Sets the launch grids and sizes the per-block energy partials.
-static rpb_status build_pair_tiles(rpb_mesh* m, int shards)
+// Shared-memory row tiles of a CSR pattern (one kernel block per tile). Tiles are balanced
+// by entries and their count is shards x a whole number of waves of resident blocks (no
+// partial last wave, whose few blocks would run while the other SMs idle), so that each
+// of `shards` GPUs owns whole waves; at most NEAR_TILE_ROWS / FAR_TILE_ROWS rows per tile
+// on average. A pattern whose rows exceed the union cap keeps the gather kernel (d.valid
+// stays false).
+static rpb_status tile_pattern(rpb_mesh* m, int rows, const int64_t* rp, const int* ci, int64_t nnz, int ncols,
+                               bool far, const void* kernel, int cap, int shards, TileBufs& d)
 {
     cudaStream_t s = m->stream;
-    rpb_status st;
-    if ((st = allow_tile_smem(m->device)) != RPB_OK) return st;
+    d.valid = false;
+    d.tiles = 0;
     int sms = 0;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, m->device) != cudaSuccess) sms = 0;
-    auto tile = [&](const SymPattern& P, int ncols, bool far, const void* kernel, int cap, TileBufs& d, int& blocks) {
-        d.valid = false;
-        d.tiles = 0;
-        auto resident = [&](int max_union) {
-            int per_sm = 0;
-            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, PAIR_TILE_THREADS,
-                                                              pair_tile_smem(max_union, far)) != cudaSuccess)
-                return 0;
-            return per_sm;
-        };
-        if (sms <= 0 || P.nnz() == 0) return RPB_OK;
-        // resident blocks depend on the tiles' largest union and the tile size on the
-        // resident blocks: start from the cap and re-tile while the count changes
-        int per_sm = resident(cap);
-        RowTiles R;
-        for (int pass = 0; pass < 3 && per_sm > 0; ++pass) {
-            const int64_t slots = static_cast<int64_t>(per_sm) * sms * shards;
-            const int64_t tile_rows = far ? FAR_TILE_ROWS : NEAR_TILE_ROWS;
-            const int64_t waves = std::max<int64_t>(1, (P.rows + slots * tile_rows - 1) / (slots * tile_rows));
-            const int64_t target = (P.nnz() + waves * slots - 1) / (waves * slots);
-            build_row_tiles(P.rp.data(), P.ci.data(), P.rows, ncols, PAIR_TILE_THREADS, target, cap,
-                            std::max(1, m->settings.threads), R);
-            if (!R.valid) break;
-            const int now = resident(R.max_union);
-            if (now == per_sm) break;
-            per_sm = now;
-        }
-        if (per_sm <= 0 || !R.valid || R.tiles() == 0) return RPB_OK;
-        rpb_status e;
-        if ((e = upload(d.row0, R.row0.data(), R.row0.size(), s)) != RPB_OK) return e;
-        if ((e = upload(d.cols_rp, R.cols_rp.data(), R.cols_rp.size(), s)) != RPB_OK) return e;
-        if ((e = upload(d.cols, R.cols.data(), R.cols.size(), s)) != RPB_OK) return e;
-        if ((e = upload(d.order, R.order.data(), R.order.size(), s)) != RPB_OK) return e;
-        if ((e = upload(d.slot, R.slot.data(), R.slot.size(), s)) != RPB_OK) return e;
-        if ((e = upload(d.lane_map, R.lane_map.data(), R.lane_map.size(), s)) != RPB_OK) return e;
-        d.row0_host = R.row0;
-        d.tiles = R.tiles();
-        d.max_union = R.max_union;
-        d.valid = true;
-        blocks = d.tiles;
-        return RPB_OK;
+    auto resident = [&](int max_union) {
+        int per_sm = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, PAIR_TILE_THREADS,
+                                                          pair_tile_smem(max_union, far)) != cudaSuccess)
+            return 0;
+        return per_sm;
     };
+    if (sms <= 0 || nnz == 0) return RPB_OK;
+    // resident blocks depend on the tiles' largest union and the tile size on the resident
+    // blocks: start from the cap and re-tile while the count changes
+    int per_sm = resident(cap);
+    RowTiles R;
+    for (int pass = 0; pass < 3 && per_sm > 0; ++pass) {
+        const int64_t slots = static_cast<int64_t>(per_sm) * sms * shards;
+        const int64_t tile_rows = far ? FAR_TILE_ROWS : NEAR_TILE_ROWS;
+        const int64_t waves = std::max<int64_t>(1, (rows + slots * tile_rows - 1) / (slots * tile_rows));
+        const int64_t target = (nnz + waves * slots - 1) / (waves * slots);
+        build_row_tiles(rp, ci, rows, ncols, PAIR_TILE_THREADS, target, cap, std::max(1, m->settings.threads), R);
+        if (!R.valid) break;
+        const int now = resident(R.max_union);
+        if (now == per_sm) break;
+        per_sm = now;
+    }
+    if (per_sm <= 0 || !R.valid || R.tiles() == 0) return RPB_OK;
+    rpb_status e;
+    if ((e = upload(d.row0, R.row0.data(), R.row0.size(), s)) != RPB_OK) return e;
+    if ((e = upload(d.cols_rp, R.cols_rp.data(), R.cols_rp.size(), s)) != RPB_OK) return e;
+    if ((e = upload(d.cols, R.cols.data(), R.cols.size(), s)) != RPB_OK) return e;
+    if ((e = upload(d.order, R.order.data(), R.order.size(), s)) != RPB_OK) return e;
+    if ((e = upload(d.slot, R.slot.data(), R.slot.size(), s)) != RPB_OK) return e;
+    if ((e = upload(d.lane_map, R.lane_map.data(), R.lane_map.size(), s)) != RPB_OK) return e;
+    d.row0_host = R.row0;
+    d.tiles = R.tiles();
+    d.max_union = R.max_union;
+    d.valid = true;
+    return RPB_OK;
+}
+
+// Per-block energy partials for `blocks` blocks of the pair launches (never shrinks).
+static rpb_status ensure_block_energy(rpb_mesh* m, int blocks)
+{
+    if (m->block_energy.n >= static_cast<size_t>(blocks)) return RPB_OK;
+    if (m->block_energy.alloc(blocks)) {
+        set_error("device allocation failed");
+        return RPB_ENOMEM;
+    }
+    return RPB_OK;
+}
+
+// Row tiles of the two full patterns for `shards` row shards (rpb_mesh_set_shards). Sets
+// the launch grids of the full-pattern kernels.
+static rpb_status build_pair_tiles(rpb_mesh* m, int shards)
+{
+    rpb_status st;
+    if ((st = allow_tile_smem(m->device)) != RPB_OK) return st;
     m->near_blocks = pair_blocks(m->N, NEAR_LANES);
     m->far_blocks = pair_blocks(m->NC, FAR_LANES);
     const void* kn = reinterpret_cast<const void*>(k_tp0_pairs_tiled<false, 3, 6, true>);
     const void* kf = reinterpret_cast<const void*>(k_tp0_pairs_tiled<true, 3, 6, true>);
-    if ((st = tile(m->tree.near, m->N, false, kn, NEAR_TILE_UNION, m->near_tiles, m->near_blocks)) != RPB_OK) return st;
-    if ((st = tile(m->tree.far, m->NC, true, kf, FAR_TILE_UNION, m->far_tiles, m->far_blocks)) != RPB_OK) return st;
+    const SymPattern& Pn = m->tree.near;
+    const SymPattern& Pf = m->tree.far;
+    if ((st = tile_pattern(m, Pn.rows, Pn.rp.data(), Pn.ci.data(), Pn.nnz(), m->N, false, kn, NEAR_TILE_UNION, shards,
+                           m->near_tiles)) != RPB_OK)
+        return st;
+    if ((st = tile_pattern(m, Pf.rows, Pf.rp.data(), Pf.ci.data(), Pf.nnz(), m->NC, true, kf, FAR_TILE_UNION, shards,
+                           m->far_tiles)) != RPB_OK)
+        return st;
+    if (m->near_tiles.valid) m->near_blocks = m->near_tiles.tiles;
+    if (m->far_tiles.valid) m->far_blocks = m->far_tiles.tiles;
     m->shards = shards;
-    if (m->block_energy.alloc(m->near_blocks + m->far_blocks)) {
-        set_error("device allocation failed");
-        return RPB_ENOMEM;
+    return ensure_block_energy(m, m->near_blocks + m->far_blocks);
+}
+
+// The once-per-pair form of both patterns: upper triangles with their lower slots, the
+// column records and the upper triangles' row tiles. once_valid when every non-empty
+// pattern is tiled.
+static rpb_status build_once_tiles(rpb_mesh* m)
+{
+    rpb_status st;
+    if ((st = allow_tile_smem(m->device)) != RPB_OK) return st;
+    cudaStream_t s = m->stream;
+    m->once_valid = false;
+    const void* kn = reinterpret_cast<const void*>(k_tp0_pairs_tiled<false, 3, 6, true, true>);
+    const void* kf = reinterpret_cast<const void*>(k_tp0_pairs_tiled<true, 3, 6, true, true>);
+    bool ok = true;
+    int blocks = 0;
+    const SymPattern* pats[2] = {&m->tree.near, &m->tree.far};
+    OnceBufs* bufs[2] = {&m->near_once, &m->far_once};
+    for (int w = 0; w < 2; ++w) {
+        const SymPattern& P = *pats[w];
+        OnceBufs& d = *bufs[w];
+        const bool far = w == 1;
+        if (P.nnz() == 0) continue;
+        UpperPattern U;
+        build_upper_pattern(P, U);
+        if (!U.valid) { ok = false; continue; }
+        d.up.rows = U.rows;
+        d.up.nnz = U.nnz();
+        if ((st = upload(d.up.rp, U.rp.data(), U.rp.size(), s)) != RPB_OK) return st;
+        if ((st = upload(d.up.ci, U.ci.data(), U.ci.size(), s)) != RPB_OK) return st;
+        if ((st = upload(d.lpos, U.lpos.data(), U.lpos.size(), s)) != RPB_OK) return st;
+        if ((st = upload(d.lrp, U.lrp.data(), U.lrp.size(), s)) != RPB_OK) return st;
+        if (d.rec.alloc(2 * static_cast<size_t>(U.nnz()))) {
+            set_error("device allocation failed");
+            return RPB_ENOMEM;
+        }
+        if ((st = tile_pattern(m, U.rows, U.rp.data(), U.ci.data(), U.nnz(), far ? m->NC : m->N, far,
+                               far ? kf : kn, far ? FAR_TILE_UNION : NEAR_TILE_UNION, 1, d.tiles)) != RPB_OK)
+            return st;
+        if (!d.tiles.valid) ok = false;
+        blocks += d.tiles.tiles;
     }
+    if ((st = ensure_block_energy(m, blocks)) != RPB_OK) return st;
+    m->once_valid = ok && (m->tree.near.nnz() + m->tree.far.nnz() > 0);
     return RPB_OK;
 }
 
@@ -305,14 +374,82 @@ static void launch_pairs_t(rpb_mesh* m, const PairArgs& An, const PairArgs& Af, 
     }
 }
 
+// Once-per-pair launches: the upper triangles' tiles (near and far in one launch unless
+// `between` separates them), then, for the differential, the lower-slot row pass.
+template <int QH, int PH>
+static void launch_pairs_once_t(rpb_mesh* m, const PairArgs& An, const PairArgs& Af, bool diff, cudaEvent_t between)
+{
+    const TileBufs& tn = m->near_once.tiles;
+    const TileBufs& tf = m->far_once.tiles;
+    const bool near = An.rows > 0, far = Af.rows > 0;
+    if (near && far && !between) {
+        const size_t smem = std::max(pair_tile_smem(tn.max_union, false), pair_tile_smem(tf.max_union, true));
+        launch_pdl(diff ? k_tp0_pairs_tiled_both<QH, PH, true, true> : k_tp0_pairs_tiled_both<QH, PH, false, true>,
+                   tn.tiles + tf.tiles, PAIR_TILE_THREADS, smem, m->stream, An, tiles_view(tn, 0), Af, tiles_view(tf, 0),
+                   tf.tiles);
+    } else {
+        if (near)
+            launch_pdl(diff ? k_tp0_pairs_tiled<false, QH, PH, true, true> : k_tp0_pairs_tiled<false, QH, PH, false, true>,
+                       tn.tiles, PAIR_TILE_THREADS, pair_tile_smem(tn.max_union, false), m->stream, An, tiles_view(tn, 0));
+        if (between) cudaEventRecord(between, m->stream);
+        if (far)
+            launch_pdl(diff ? k_tp0_pairs_tiled<true, QH, PH, true, true> : k_tp0_pairs_tiled<true, QH, PH, false, true>,
+                       tf.tiles, PAIR_TILE_THREADS, pair_tile_smem(tf.max_union, true), m->stream, Af, tiles_view(tf, 0));
+    }
+    if (diff) {
+        LowerSumArgs L;
+        L.N = near ? m->N : 0;
+        L.NC = far ? m->NC : 0;
+        L.lrp_near = m->near_once.lrp.ptr; L.rec_near = m->near_once.rec.ptr; L.D_near = An.D;
+        L.lrp_far = m->far_once.lrp.ptr; L.rec_far = m->far_once.rec.ptr; L.D_far = Af.D;
+        const int rows = L.N + L.NC;
+        if (rows > 0) launch_pdl(k_lower_sums, (rows + 255) / 256, 256, 0, m->stream, L);
+    }
+}
+
 // Near- and far-field pair kernels on the mesh stream. shard >= 0: only that row shard's
 // tiles (both patterns tiled), derivatives into D_near / D_far (zeroed first), energies into
-// energy[0..1]; shard < 0: every row, into the mesh's own buffers.
+// energy[0..1]; shard < 0: every row, into the mesh's own buffers -- each unordered pair
+// evaluated once when the upper triangles are tiled and the mesh is not set up for row
+// shards (whose sum then equals the unsharded evaluation with the same tiles bit for bit).
 rpb_status launch_pairs(rpb_mesh* m, const TPExp& ex, bool diff, cudaEvent_t between = nullptr, int shard = -1,
                         double* D_near = nullptr, double* D_far = nullptr)
 {
+    if (shard < 0 && m->once_valid && m->shards <= 1) {
+        PairArgs An, Af;
+        An.col_data = Af.col_data = nullptr;
+        An.dom = Af.dom = m->dom;
+        An.ex = Af.ex = ex;
+        An.close_factor = Af.close_factor = 0.1f;
+        An.order = Af.order = nullptr;
+        An.rows = m->near.nnz > 0 ? m->N : 0;
+        An.rp = m->near_once.up.rp.ptr; An.ci = m->near_once.up.ci.ptr; An.lpos = m->near_once.lpos.ptr;
+        An.rec = m->near_once.rec.ptr; An.data = m->P_pair.ptr; An.D = m->D_near.ptr;
+        An.block_energy = m->block_energy.ptr; An.done = m->done.ptr; An.energy_out = m->energy.ptr;
+        Af.rows = m->far.nnz > 0 ? m->NC : 0;
+        Af.rp = m->far_once.up.rp.ptr; Af.ci = m->far_once.up.ci.ptr; Af.lpos = m->far_once.lpos.ptr;
+        Af.rec = m->far_once.rec.ptr; Af.data = m->C_pair.ptr; Af.D = m->D_far.ptr;
+        Af.block_energy = m->block_energy.ptr + m->near_once.tiles.tiles; Af.done = m->done.ptr + 1;
+        Af.energy_out = m->energy.ptr + 1;
+        if (An.rows == 0) {
+            RPB_CUDA(cudaMemsetAsync(m->energy.ptr, 0, sizeof(double), m->stream));
+            if (diff) RPB_CUDA(cudaMemsetAsync(m->D_near.ptr, 0, m->D_near.bytes(), m->stream));
+        }
+        if (Af.rows == 0) {
+            RPB_CUDA(cudaMemsetAsync(m->energy.ptr + 1, 0, sizeof(double), m->stream));
+            if (diff) RPB_CUDA(cudaMemsetAsync(m->D_far.ptr, 0, m->D_far.bytes(), m->stream));
+        }
+        if (ex.qh == 3 && ex.ph == 6) launch_pairs_once_t<3, 6>(m, An, Af, diff, between);
+        else if (ex.qh == 2 && ex.ph == 4) launch_pairs_once_t<2, 4>(m, An, Af, diff, between);
+        else if (ex.qh == 1 && ex.ph == 2) launch_pairs_once_t<1, 2>(m, An, Af, diff, between);
+        else launch_pairs_once_t<-1, -1>(m, An, Af, diff, between);
+        RPB_CUDA(cudaGetLastError());
+        return RPB_OK;
+    }
     PairArgs An, Af;
     An.col_data = Af.col_data = nullptr;
+    An.lpos = Af.lpos = nullptr;
+    An.rec = Af.rec = nullptr;
     An.dom = Af.dom = m->dom;
     An.ex = Af.ex = ex;
     An.close_factor = Af.close_factor = 0.1f;
@@ -353,7 +490,7 @@ rpb_status launch_pairs(rpb_mesh* m, const TPExp& ex, bool diff, cudaEvent_t bet
     return RPB_OK;
 }
 
-rpb_status launch_collect_gather(rpb_mesh* m, double alpha, double beta, double* Y, int ldY, bool with_vf,
+rpb_status launch_collect_gather(rpb_mesh* m, double alpha, double beta, double* Y, int ldY, const double* D_vf,
                                  const double* D_near, const double* D_far)
 {
     CollectArgs C;
@@ -369,7 +506,7 @@ rpb_status launch_collect_gather(rpb_mesh* m, double alpha, double beta, double*
     C.C_pair = m->C_pair.ptr;
     C.D_near = D_near ? D_near : m->D_near.ptr;
     C.D_far = D_far ? D_far : m->D_far.ptr;
-    C.D_vf = with_vf ? m->D_vf.ptr : nullptr;
+    C.D_vf = D_vf;
     C.B = m->B.ptr;
     launch_pdl(k_collect_chain, (m->N + 255) / 256, 256, 0, m->stream, C);
     RPB_CUDA(cudaGetLastError());
@@ -410,7 +547,7 @@ rpb_status evaluate(rpb_mesh* m, double q, double p, bool diff, double alpha, do
         if (st != RPB_OK) return st;
     }
     if (diff) {
-        st = launch_collect_gather(m, alpha, beta, Y_dev, ldY, with_vf, nullptr, nullptr);
+        st = launch_collect_gather(m, alpha, beta, Y_dev, ldY, with_vf ? m->vf.D.ptr : nullptr, nullptr, nullptr);
         if (st != RPB_OK) return st;
     }
     if (energy_host) {
@@ -418,6 +555,7 @@ rpb_status evaluate(rpb_mesh* m, double q, double p, bool diff, double alpha, do
         RPB_CUDA(cudaMemcpyAsync(e, m->energy.ptr, sizeof(double) * 3, cudaMemcpyDeviceToHost, m->stream));
         RPB_CUDA(cudaStreamSynchronize(m->stream));
         *energy_host = (e[2] + e[0]) + e[1];
+        if (with_vf && (st = vf_take_status(m->vf, m->stream)) != RPB_OK) return st;
     }
     return RPB_OK;
 }
@@ -569,7 +707,11 @@ rpb_status rpb_mesh_create(int dom_dim, int amb_dim, const double* Vh, int64_t n
         if ((st = upload(m->far_order, fo.data(), fo.size(), s)) != RPB_OK) return fail(st);
         m->near_blocks = pair_blocks(m->N, NEAR_LANES);
         m->far_blocks = pair_blocks(m->NC, FAR_LANES);
-        if ((st = build_pair_tiles(m, 1)) != RPB_OK) return fail(st);
+        // each pair once (upper triangles); the full-pattern tiles only where that is not
+        // possible (a row beyond the union cap) and for row shards (rpb_mesh_set_shards)
+        if ((st = ensure_block_energy(m, m->near_blocks + m->far_blocks)) != RPB_OK) return fail(st);
+        if ((st = build_once_tiles(m)) != RPB_OK) return fail(st);
+        if (!m->once_valid && (st = build_pair_tiles(m, 1)) != RPB_OK) return fail(st);
     }
     if (cudaMemsetAsync(m->counter.ptr, 0, m->counter.bytes(), s) != cudaSuccess ||
         cudaMemsetAsync(m->done.ptr, 0, m->done.bytes(), s) != cudaSuccess ||
@@ -578,7 +720,8 @@ rpb_status rpb_mesh_create(int dom_dim, int amb_dim, const double* Vh, int64_t n
         return fail(RPB_ECUDA);
     }
     if (m->verynear.nnz > 0) {
-        if (m->D_vf.alloc(16 * static_cast<size_t>(m->N))) { set_error("device allocation failed"); return fail(RPB_ENOMEM); }
+        const rpb_status vst = vf_alloc(m->vf, m->verynear.nnz, m->N);
+        if (vst != RPB_OK) return fail(vst);
     }
     if ((st = launch_geometry(m)) != RPB_OK) return fail(st);
     if ((st = metric_init(m, Vh, Sh)) != RPB_OK) return fail(st);
@@ -890,7 +1033,7 @@ rpb_status rpb_tpe0_collect_shards(rpb_mesh* m, const double* buf, double alpha,
     RPB_CUDA(cudaSetDevice(m->device));
     const double* D_near = buf;
     const double* D_far = buf + 10 * static_cast<int64_t>(m->N);
-    return launch_collect_gather(m, alpha, beta, Y_dev, ldY, false, D_near, D_far);
+    return launch_collect_gather(m, alpha, beta, Y_dev, ldY, nullptr, D_near, D_far);
 }
 
 rpb_status rpb_tpe0_energy_device(rpb_mesh* m, double* energy_dev)
@@ -917,6 +1060,7 @@ rpb_status rpb_tpe0_differential(rpb_mesh* m, double q, double p, double alpha, 
     RPB_CUDA(copy_rows3(Y, ldY, m->Y.ptr, 3, m->nV, cudaMemcpyDeviceToHost, m->stream));
     RPB_CUDA(cudaStreamSynchronize(m->stream));
     if (energy) *energy = (m->host_energy[2] + m->host_energy[0]) + m->host_energy[1];
+    if (m->verynear.nnz > 0) return vf_take_status(m->vf, m->stream);
     return RPB_OK;
 }
 
@@ -942,7 +1086,9 @@ rpb_status rpb_tpe0_stage_times(rpb_mesh* m, double q, double p, int reps, int64
         if ((st = launch_pairs(m, ex, true, ev[2])) != RPB_OK) return st;
         if (with_vf && (st = launch_vf(m, ex, true)) != RPB_OK) return st;
         RPB_CUDA(cudaEventRecord(ev[3], m->stream));
-        if ((st = launch_collect_gather(m, 1.0, 0.0, m->Y.ptr, 3, with_vf, nullptr, nullptr)) != RPB_OK) return st;
+        if ((st = launch_collect_gather(m, 1.0, 0.0, m->Y.ptr, 3, with_vf ? m->vf.D.ptr : nullptr, nullptr, nullptr)) !=
+            RPB_OK)
+            return st;
         RPB_CUDA(cudaEventRecord(ev[4], m->stream));
         RPB_CUDA(cudaEventSynchronize(ev[4]));
         float t;

@@ -6,8 +6,7 @@
 #include "../../include/repulsor_b200.h"
 #include "host/tree_builder.hpp"
 #include "rpb_device.cuh"
-
-struct rpb_mesh;
+#include "rpb_mesh.cuh"
 
 namespace rpb {
 
@@ -31,15 +30,24 @@ inline cudaError_t copy_rows3(void* dst, int ld_dst, const void* src, int ld_src
     return cudaMemcpy2DAsync(dst, sizeof(double) * ld_dst, src, sizeof(double) * ld_src, sizeof(double) * 3, n, kind, s);
 }
 rpb_status launch_geometry(rpb_mesh* m);
-// near/far moment derivatives (mesh buffers when null) -> chain rule -> Y = alpha dE + beta Y
-rpb_status launch_collect_gather(rpb_mesh* m, double alpha, double beta, double* Y, int ldY, bool with_vf,
+// near/far moment derivatives (mesh buffers when null) and very-near row derivatives (none
+// when D_vf is null) -> chain rule -> Y = alpha dE + beta Y
+rpb_status launch_collect_gather(rpb_mesh* m, double alpha, double beta, double* Y, int ldY, const double* D_vf,
                                  const double* D_near, const double* D_far);
 rpb_status evaluate(rpb_mesh* m, double q, double p, bool diff, double alpha, double beta, double* Y_dev, int ldY,
                     double* energy_host);
 
 // very-near adaptive quadrature (rpb_verynear.cu)
+rpb_status vf_alloc(VFBuffers& b, int64_t nnz, int N);
+// reads (synchronizing) and clears the status of the last very-near evaluations: RPB_EINVAL
+// with the message set if a pair touched or intersected or exceeded the work cap
+rpb_status vf_take_status(VFBuffers& b, cudaStream_t s);
 rpb_status launch_vf(rpb_mesh* m, const TPExp& ex, bool diff);
 rpb_status launch_vf_metric(rpb_mesh* m, const TPExp& ex, float2* vals, double2* diag);
+// mesh x obstacle very-near pairs (CSR rp/ci over m's primitives): row derivatives into
+// b.D, the energy (symmetry factor 1/2) into *energy_out, on m's stream
+rpb_status launch_vf_cross(rpb_mesh* m, const rpb_mesh* obstacle, const int64_t* rp, const int* ci, int64_t nnz,
+                           VFBuffers& b, const TPExp& ex, bool diff, double* energy_out);
 
 // metric (rpb_metric.cu)
 rpb_status metric_init(rpb_mesh* m, const double* Vh, const int* Sh);

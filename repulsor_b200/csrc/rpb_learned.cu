@@ -736,6 +736,22 @@ __global__ void k_cluster_out_grad(int NC, const double* gc, const float* O, con
     }
 }
 
+// Coefficients of the preconditioner with the gains of an earlier application (O, the
+// network's outputs for that residual) on the cluster moments Yc of another vector:
+// c_C = exp(clamp(o_C)) Yc_C w_C. With them the application is the linear operator
+// the earlier residual's gains define, which the unrolled-solve training needs for its
+// adjoint pass.
+__global__ void k_frozen_coef(int NC, const float* O, const double* Yc, const double* C_w, double* c)
+{
+    const int C = blockIdx.x * blockDim.x + threadIdx.x;
+    if (C >= NC) return;
+    for (int q = 0; q < 3; ++q) {
+        const int64_t k = 3 * static_cast<int64_t>(C) + q;
+        const float o = fminf(fmaxf(O[k], -GAIN_CLAMP), GAIN_CLAMP);
+        c[k] = exp(static_cast<double>(o)) * Yc[k] * C_w[C];
+    }
+}
+
 // out[c] = sum_i a[3i+c] * b[3i+c] (b == nullptr: column sums); one block, fixed order
 __global__ void __launch_bounds__(512) k_dot3_single(int n, const double* a, const double* b, double* out)
 {
@@ -1101,6 +1117,105 @@ rpb_status rpb_tpm0_learned_apply(rpb_mesh* m, const double* R, double* Z)
     if ((st = learned_forward(m, L.mlp, L.r.ptr, L.z.ptr, false)) != RPB_OK) return st;
     RPB_CUDA(cudaMemcpyAsync(Z, L.z.ptr, 3 * sizeof(double) * m->nV, cudaMemcpyDeviceToHost, m->stream));
     RPB_CUDA(cudaStreamSynchronize(m->stream));
+    return RPB_OK;
+}
+
+rpb_status rpb_tpm0_learned_apply_pair(rpb_mesh* m, const double* R, const double* Y, double* Z, double* ZY)
+{
+    if (!m || !R || !Z || (!Y) != (!ZY)) { set_error("null argument"); return RPB_EINVAL; }
+    if (!m->learned || !m->learned->mlp) {
+        set_error("no learned preconditioner is attached to this mesh (rpb_mesh_set_learned)");
+        return RPB_EINVAL;
+    }
+    RPB_CUDA(cudaSetDevice(m->device));
+    rpb_status st;
+    if ((st = ensure_learned(m)) != RPB_OK) return st;
+    if ((st = ensure_training_buffers(m)) != RPB_OK) return st;
+    LearnedState& L = *m->learned;
+    cudaStream_t s = m->stream;
+    const size_t n3 = 3 * static_cast<size_t>(m->nV);
+    RPB_CUDA(cudaMemcpyAsync(L.r.ptr, R, n3 * sizeof(double), cudaMemcpyHostToDevice, s));
+    if ((st = learned_forward(m, L.mlp, L.r.ptr, L.z.ptr, true)) != RPB_OK) return st;
+    RPB_CUDA(cudaMemcpyAsync(Z, L.z.ptr, n3 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (Y) {
+        const int eb = (m->nV + 255) / 256;
+        RPB_CUDA(cudaMemcpyAsync(L.e.ptr, Y, n3 * sizeof(double), cudaMemcpyHostToDevice, s));
+        if ((st = cluster_moments(m, L.e.ptr, L.gc.ptr)) != RPB_OK) return st;
+        k_frozen_coef<<<(m->NC + 255) / 256, 256, 0, s>>>(m->NC, L.O.ptr, L.gc.ptr, L.C_w.ptr, L.c.ptr);
+        k_prim_expand<<<(m->N + 255) / 256, 256, 0, s>>>(m->N, m->leaf_of.ptr, m->C_parent.ptr, m->C_up4.ptr, L.c.ptr,
+                                                          L.tmp3.ptr);
+        RPB_CUDA(cudaMemsetAsync(L.dots.ptr, 0, 3 * sizeof(double), s));
+        k_vertex_expand<<<eb, 256, 0, s>>>(m->nV, m->size, m->vp_rp.ptr, m->vp_slot.ptr, m->pre_vals.ptr, L.tmp3.ptr,
+                                          L.dots.ptr, L.g.ptr);
+        if ((st = dot3_dev(m, L.g.ptr, nullptr, L.sums.ptr)) != RPB_OK) return st;
+        k_sub_mean<<<eb, 256, 0, s>>>(m->nV, L.g.ptr, L.sums.ptr);
+        RPB_CUDA(cudaGetLastError());
+        RPB_CUDA(cudaMemcpyAsync(ZY, L.g.ptr, n3 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    }
+    RPB_CUDA(cudaStreamSynchronize(s));
+    return RPB_OK;
+}
+
+rpb_status rpb_mlp_train_step_sens(rpb_mlp* mlp, rpb_mesh* m, const double* R, const double* G, int npairs, double lr,
+                                   double reg, double* objective, float* grad)
+{
+    if (!mlp || !m || !R || !G || npairs <= 0) { set_error("null or empty argument"); return RPB_EINVAL; }
+    if (mlp->device != m->device) { set_error("network and mesh live on different devices"); return RPB_EINVAL; }
+    RPB_CUDA(cudaSetDevice(m->device));
+    rpb_status st;
+    if ((st = ensure_learned(m)) != RPB_OK) return st;
+    if ((st = ensure_training_buffers(m)) != RPB_OK) return st;
+    LearnedState& L = *m->learned;
+    cudaStream_t s = m->stream;
+    const int nV = m->nV;
+    const int eb = (nV + 255) / 256;
+    const size_t n3 = 3 * static_cast<size_t>(nV);
+    DevBuf<float> gsum;
+    DevBuf<double> obj;
+    RPB_CUDA(gsum.alloc(NPARAM));
+    RPB_CUDA(obj.alloc(3 * static_cast<size_t>(npairs)));
+    RPB_CUDA(cudaMemsetAsync(gsum.ptr, 0, gsum.bytes(), s));
+    for (int k = 0; k < npairs; ++k) {
+        RPB_CUDA(cudaMemcpyAsync(L.r.ptr, R + k * n3, n3 * sizeof(double), cudaMemcpyHostToDevice, s));
+        RPB_CUDA(cudaMemcpyAsync(L.g.ptr, G + k * n3, n3 * sizeof(double), cudaMemcpyHostToDevice, s));
+        if ((st = learned_forward(m, mlp, L.r.ptr, L.z.ptr, true)) != RPB_OK) return st;
+        if ((st = dot3_dev(m, L.g.ptr, L.z.ptr, obj.ptr + 3 * k)) != RPB_OK) return st;
+        // back through the mean removal, the vertex sum and the cluster expansion
+        if ((st = dot3_dev(m, L.g.ptr, nullptr, L.sums.ptr)) != RPB_OK) return st;
+        k_sub_mean<<<eb, 256, 0, s>>>(nV, L.g.ptr, L.sums.ptr);
+        if ((st = cluster_moments(m, L.g.ptr, L.gc.ptr)) != RPB_OK) return st;
+        k_cluster_out_grad<<<(m->NC + 255) / 256, 256, 0, s>>>(m->NC, L.gc.ptr, L.O.ptr, L.Rc.ptr, m->C_pair.ptr,
+                                                               static_cast<float>(reg), L.C_w.ptr, L.dO.ptr);
+        RPB_CUDA(cudaGetLastError());
+        if ((st = mlp_backward(mlp, m->NC, L.F.ptr, L.pre1.ptr, L.pre2.ptr, L.dO.ptr, L.d1.ptr, L.d2.ptr, mlp->grad.ptr,
+                               s)) != RPB_OK)
+            return st;
+        k_accumulate<<<(NPARAM + 255) / 256, 256, 0, s>>>(NPARAM, gsum.ptr, mlp->grad.ptr);
+    }
+    std::vector<float> gh;
+    if (grad) {
+        gh.resize(NPARAM);
+        RPB_CUDA(cudaMemcpyAsync(gh.data(), gsum.ptr, gsum.bytes(), cudaMemcpyDeviceToHost, s));
+    }
+    std::vector<double> oh(3 * static_cast<size_t>(npairs));
+    RPB_CUDA(cudaMemcpyAsync(oh.data(), obj.ptr, obj.bytes(), cudaMemcpyDeviceToHost, s));
+    mlp->step += 1;
+    const float b1 = 0.9f, b2 = 0.999f;
+    const float bc1 = 1.0f - std::pow(b1, static_cast<float>(mlp->step));
+    const float bc2 = 1.0f - std::pow(b2, static_cast<float>(mlp->step));
+    if (lr > 0.0)
+        k_adam<<<(NPARAM + 255) / 256, 256, 0, s>>>(NPARAM, mlp->theta.ptr, mlp->w16.ptr, gsum.ptr, mlp->m.ptr, mlp->v.ptr,
+                                                    static_cast<float>(lr), b1, b2, 1e-8f, bc1, bc2);
+    RPB_CUDA(cudaGetLastError());
+    RPB_CUDA(cudaStreamSynchronize(s));
+    if (lr <= 0.0) mlp->step -= 1;
+    if (objective) {
+        double o = 0;
+        for (double v : oh) o += v;
+        *objective = o;
+    }
+    if (grad)
+        for (int k = 0; k < NPARAM; ++k) grad[k] = gh[k];
     return RPB_OK;
 }
 

@@ -64,6 +64,14 @@ struct PseudoLapCache {
     DevBuf<double> nf_diag, ff_diag, vf_diag;
 };
 
+// Very-near quadrature buffers of one list (rpb_verynear.cu): per-entry slots, the row
+// derivatives (N x 16, reference layout a, a*hull, a*P) and the energy reduction state.
+struct VFBuffers {
+    DevBuf<double> part, D, block_energy;
+    DevBuf<unsigned> done;
+    size_t bytes() const { return part.bytes() + D.bytes() + block_energy.bytes() + done.bytes(); }
+};
+
 // Device copy of a pattern's row tiles (RowTiles); valid == false: the gather kernels run.
 struct TileBufs {
     DevBuf<int> row0, cols_rp, cols, order, lane_map;
@@ -71,6 +79,23 @@ struct TileBufs {
     std::vector<int> row0_host;   // tiles + 1: first row of each tile
     int tiles = 0, max_union = 0;
     bool valid = false;
+};
+
+// One pattern evaluated once per unordered pair: its upper triangle (rows' entries j > i),
+// the lower slot of every upper entry, the rows' lower-slot ranges, the column records
+// (two float4 per slot) and the row tiles of the upper triangle.
+struct OnceBufs {
+    Csr up;
+    DevBuf<int> lpos;
+    DevBuf<int64_t> lrp;
+    DevBuf<float4> rec;
+    TileBufs tiles;
+    size_t bytes() const
+    {
+        return up.rp.bytes() + up.ci.bytes() + lpos.bytes() + lrp.bytes() + rec.bytes() + tiles.row0.bytes() +
+               tiles.cols_rp.bytes() + tiles.cols.bytes() + tiles.order.bytes() + tiles.lane_map.bytes() +
+               tiles.slot.bytes();
+    }
 };
 
 }  // namespace rpb
@@ -94,7 +119,10 @@ struct rpb_mesh {
     rpb::DevBuf<int> C_up4;   // fourth ancestor of every cluster (-1 when the root is nearer)
     rpb::Csr near, far, verynear;
     rpb::DevBuf<int> near_order, far_order;             // pair-kernel row order (length-sorted per chunk)
-    rpb::TileBufs near_tiles, far_tiles;                // shared-memory row tiles of the two patterns
+    rpb::TileBufs near_tiles, far_tiles;                // shared-memory row tiles of the two full patterns
+                                                        // (row shards; built by rpb_mesh_set_shards)
+    rpb::OnceBufs near_once, far_once;                  // upper triangles: each pair evaluated once
+    bool once_valid = false;                            // both patterns tiled for the once-per-pair kernels
     // geometry state
     rpb::DevBuf<rpb::PrimDatum> P_pair;
     rpb::DevBuf<rpb::ClusterDatum> C_pair;
@@ -103,7 +131,8 @@ struct rpb_mesh {
     // near-hull data for very-near quadrature (N x (1 + 3 size + 6), FP64)
     rpb::DevBuf<double> P_near;
     // derivative path
-    rpb::DevBuf<double> D_near, D_far, D_vf, B;
+    rpb::DevBuf<double> D_near, D_far, B;
+    rpb::VFBuffers vf;                          // very-near quadrature (when the list is not empty)
     rpb::DevBuf<int> v_rp, v_slot;
     rpb::DevBuf<double> Y;
     rpb::DevBuf<double> block_energy, energy;   // energy[0] near, [1] far, [2] very near

@@ -518,6 +518,8 @@ static rpb_status ensure_metric_values(rpb_mesh* m, double q, double p)
         RPB_CUDA(cudaMemsetAsync(mc.vf_diag.ptr, 0, mc.vf_diag.bytes(), m->stream));
         rpb_status st = launch_vf_metric(m, ex, mc.vf.ptr, mc.vf_diag.ptr);
         if (st != RPB_OK) return st;
+        // once per geometry: pairs in contact make the metric values NaN; report them
+        if ((st = vf_take_status(m->vf, m->stream)) != RPB_OK) return st;
     }
     mc.valid = true;
     mc.q = q;
@@ -551,6 +553,7 @@ static rpb_status ensure_plap_values(rpb_mesh* m, double s_pl)
         rpb_status st = launch_vf_metric(m, ex, reinterpret_cast<float2*>(pc.vf.ptr),
                                          reinterpret_cast<double2*>(pc.vf_diag.ptr));
         if (st != RPB_OK) return st;
+        if ((st = vf_take_status(m->vf, m->stream)) != RPB_OK) return st;
     }
     pc.valid = true;
     pc.s = s_pl;

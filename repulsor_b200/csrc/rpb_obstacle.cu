@@ -9,7 +9,9 @@
 // the mesh's primitives (near) or clusters (far), columns the obstacle's, every pair
 // counts with the symmetry factor 1/2, and only the mesh side's moment derivatives are
 // formed; they then go through the same collection, chain rule and vertex gather as the
-// self energy. The obstacle's own geometry is evaluated once at load (it does not move).
+// self energy. Very-near (mesh, obstacle) pairs run the subdivision quadrature in CROSS
+// mode (rpb_verynear.cu). The obstacle's own geometry is evaluated once at load (it does
+// not move).
 #include <algorithm>
 #include <string>
 #include <vector>
@@ -31,8 +33,9 @@ namespace rpb {
 
 struct ObstacleState {
     rpb_mesh* mesh = nullptr;      // the obstacle (owned)
-    Csr near, far;
+    Csr near, far, verynear;
     DevBuf<int> near_order, far_order;
+    VFBuffers vf;
     int64_t verynear_nnz = 0, inter_nnz = 0;
     CrossLists lists;              // host copy (patterns for inspection)
     DevBuf<double> D_near, D_far, block_energy, energy;
@@ -117,10 +120,6 @@ rpb_status evaluate_obstacle(rpb_mesh* m, double q, double p, bool diff, double 
         return RPB_OK;
     }
     ObstacleState& O = *m->obstacle;
-    if (O.verynear_nnz > 0) {
-        set_error("the obstacle has very-near primitive pairs; their subdivision quadrature is not built for obstacles");
-        return RPB_EINVAL;
-    }
     if (!m->geometry_valid && (st = launch_geometry(m)) != RPB_OK) return st;
     const TPExp ex = make_exp(m->dom, q, p);
     PairArgs An, Af;
@@ -148,13 +147,20 @@ rpb_status evaluate_obstacle(rpb_mesh* m, double q, double p, bool diff, double 
     if (ex.qh == 3 && ex.ph == 6) launch_cross<3, 6>(m, An, Af, diff);
     else launch_cross<-1, -1>(m, An, Af, diff);
     RPB_CUDA(cudaGetLastError());
-    if (diff && (st = launch_collect_gather(m, alpha, beta, Y_dev, ldY, false, O.D_near.ptr, O.D_far.ptr)) != RPB_OK)
+    const bool with_vf = O.verynear.nnz > 0;
+    if (with_vf &&
+        (st = launch_vf_cross(m, O.mesh, O.verynear.rp.ptr, O.verynear.ci.ptr, O.verynear.nnz, O.vf, ex, diff,
+                              O.energy.ptr + 2)) != RPB_OK)
+        return st;
+    if (diff && (st = launch_collect_gather(m, alpha, beta, Y_dev, ldY, with_vf ? O.vf.D.ptr : nullptr, O.D_near.ptr,
+                                            O.D_far.ptr)) != RPB_OK)
         return st;
     if (energy_host) {
-        double e[2] = {0, 0};
+        double e[3] = {0, 0, 0};
         RPB_CUDA(cudaMemcpyAsync(e, O.energy.ptr, sizeof(e), cudaMemcpyDeviceToHost, m->stream));
         RPB_CUDA(cudaStreamSynchronize(m->stream));
-        *energy_host = e[0] + e[1];
+        *energy_host = (e[2] + e[0]) + e[1];   // (very near + near) + far
+        if (with_vf && (st = vf_take_status(O.vf, m->stream)) != RPB_OK) return st;
     }
     return RPB_OK;
 }
@@ -187,6 +193,7 @@ rpb_status rpb_mesh_load_obstacle(rpb_mesh* m, rpb_mesh* obstacle)
     const CrossLists& L = O->lists;
     O->near.rows = L.near.rows; O->near.nnz = L.near.nnz();
     O->far.rows = L.far.rows; O->far.nnz = L.far.nnz();
+    O->verynear.rows = L.verynear.rows; O->verynear.nnz = L.verynear.nnz();
     O->verynear_nnz = L.verynear.nnz();
     O->inter_nnz = L.inter.nnz();
     const std::vector<int> no = chunk_order(L.near), fo = chunk_order(L.far);
@@ -194,14 +201,19 @@ rpb_status rpb_mesh_load_obstacle(rpb_mesh* m, rpb_mesh* obstacle)
     O->far_blocks = pair_blocks(m->NC, FAR_LANES);
     if (upload_vec(O->near.rp, L.near.rp, s) || upload_vec(O->near.ci, L.near.ci, s) ||
         upload_vec(O->far.rp, L.far.rp, s) || upload_vec(O->far.ci, L.far.ci, s) ||
-        upload_vec(O->near_order, no, s) || upload_vec(O->far_order, fo, s)) {
+        upload_vec(O->near_order, no, s) || upload_vec(O->far_order, fo, s) ||
+        upload_vec(O->verynear.rp, L.verynear.rp, s) || upload_vec(O->verynear.ci, L.verynear.ci, s)) {
         set_error("obstacle list upload failed");
         return fail(RPB_ENOMEM);
     }
     if (O->D_near.alloc(10 * static_cast<size_t>(m->N)) || O->D_far.alloc(10 * static_cast<size_t>(m->NC)) ||
-        O->block_energy.alloc(O->near_blocks + O->far_blocks) || O->energy.alloc(2) || O->done.alloc(4)) {
+        O->block_energy.alloc(O->near_blocks + O->far_blocks) || O->energy.alloc(3) || O->done.alloc(4)) {
         set_error("device allocation failed");
         return fail(RPB_ENOMEM);
+    }
+    if (O->verynear.nnz > 0) {
+        const rpb_status vst = vf_alloc(O->vf, O->verynear.nnz, m->N);
+        if (vst != RPB_OK) return fail(vst);
     }
     if (cudaMemsetAsync(O->done.ptr, 0, O->done.bytes(), s) != cudaSuccess ||
         cudaMemsetAsync(O->energy.ptr, 0, O->energy.bytes(), s) != cudaSuccess) {

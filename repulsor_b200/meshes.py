@@ -18,14 +18,19 @@ Workloads (sizes and distributions of the five benchmark configurations):
 * ``linked_tori``     two R=1, r=0.3 tori (480 x 640 grids), the second rotated 90 deg
                       about x and shifted by +1 along x, normal jitter N(0, 0.002^2)
 * ``icosphere``       plain level-L icosphere of a given radius and centre (obstacle)
+
+``reference_mesh`` returns the meshes the reference itself ships (its Meshes/ directory),
+from a committed fixture.
 """
 from __future__ import annotations
 
 import math
+import os
 
 import numpy as np
 
 __all__ = [
+    "reference_mesh",
     "torus_knot",
     "torus",
     "icosphere",
@@ -209,3 +214,21 @@ def config_mesh(cfg: int, small: bool = False):
     if cfg == 5:
         return (2, linked_tori(n_major=48 if small else 480, n_minor=64 if small else 640, seed=1005))
     raise ValueError(f"no single mesh for configuration {cfg}")
+
+
+_REFERENCE_NPZ = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "tests", "golden",
+                              "reference_meshes.npz")
+
+
+def reference_mesh(name: str):
+    """A mesh shipped with the reference (Meshes/ of HenrikSchumacher/Repulsor), from the
+    committed fixture tests/golden/reference_meshes.npz: "torus2400", "torus38400",
+    "sphere40560", "twospheres" (the example's mesh), "twospheres_obstacle" (its
+    obstacle) or "twospheres_union" (both spheres as one mesh: 25 very-near pairs).
+    Returns (V, S)."""
+    d = np.load(_REFERENCE_NPZ)
+    if name == "twospheres_union":
+        V, S = d["twospheres_V"], d["twospheres_S"]
+        VO, SO = d["twospheres_obstacle_V"], d["twospheres_obstacle_S"]
+        return np.vstack([V, VO]), np.vstack([S, SO + V.shape[0]]).astype(np.int32)
+    return np.array(d[f"{name}_V"]), np.array(d[f"{name}_S"])

@@ -1,13 +1,11 @@
-// Drives the header-only C++20 mirror (include/repulsor_b200/Repulsor.hpp) the way
-// Repulsor's own drivers use the reference API (Example/main.cpp): build a mesh, evaluate
-// TangentPointEnergy0 Value/Differential/SimplexDensities, multiply the metric, solve, load
-// an obstacle and evaluate TangentPointObstacleEnergy. Input: a mesh file "nV nS dom"
-// followed by the coordinates and simplices; output: energy, |dE|_max, sum(A dE),
-// iterations, the relative residual, the energy from the densities call and the obstacle
-// energy, one per line.
+// Drives the header-only C++20 mirror (include/repulsor_b200/Repulsor.hpp) through its
+// concrete classes: read a mesh file in the reference's text format (the factory's
+// Make_FromFile), evaluate TangentPointEnergy0 Value/Differential/SimplexDensities,
+// multiply the metric, solve, load an obstacle and evaluate TangentPointObstacleEnergy.
+// Output: energy, |dE|_max, sum(A dE), iterations, the relative residual, the energy
+// from the densities call and the obstacle energy, one per line.
 #include <cmath>
 #include <cstdio>
-#include <fstream>
 #include <memory>
 #include <vector>
 
@@ -16,17 +14,21 @@
 namespace Repulsor = Repulsor_B200;
 
 template <int DOM>
-int run(const std::vector<double>& V, const std::vector<int>& S, int nV, int nS)
+int run(const Repulsor::SimplicialMeshBase<double, int, std::size_t>& file_mesh)
 {
     using Mesh_T = Repulsor::SimplicialMesh<DOM, 3>;
+    const int nV = file_mesh.VertexCount(), nS = file_mesh.SimplexCount();
+    const std::vector<double> V(file_mesh.VertexCoordinates().data(), file_mesh.VertexCoordinates().data() + 3 * nV);
+    const std::vector<int> S(file_mesh.Simplices().data(), file_mesh.Simplices().data() + (DOM + 1) * nS);
     Mesh_T M(V.data(), nV, S.data(), nS, 4);
     M.block_cluster_tree_settings.far_field_separation_parameter = 0.5;
     M.adaptivity_settings.theta = 10.0;
     Repulsor::TangentPointEnergy0<Mesh_T> tpe(6.0, 12.0);
     Repulsor::TangentPointMetric0<Mesh_T> tpm(6.0, 12.0);
     const double E = tpe.Value(M);
-    const std::vector<double>& D = tpe.Differential(M);
-    if (D.size() != static_cast<size_t>(3 * nV)) return 2;
+    const auto& Dt = tpe.Differential(M);
+    if (Dt.Dim(0) != nV || Dt.Dim(1) != 3) return 2;
+    const std::vector<double> D(Dt.data(), Dt.data() + Dt.Size());
     double dmax = 0;
     for (double d : D) dmax = std::fmax(dmax, std::fabs(d));
     std::vector<double> Y(3 * nV, 0.0), X(3 * nV, 0.0);
@@ -42,9 +44,8 @@ int run(const std::vector<double>& V, const std::vector<int>& S, int nV, int nS)
     }
     tpm.SetPreconditioner(RPB_PRECOND_NONE);
     tpm.Solve(M, 1.0, B.data(), 3, 0.0, X.data(), 3, 3, 20000, 1e-6);
-    const std::vector<double> rr = tpm.Solver_RelativeResiduals();
-    double rmax = 0;
-    for (double r : rr) rmax = std::fmax(rmax, r);
+    const auto rr = tpm.Solver_RelativeResiduals();
+    const double rmax = rr.Max();
     std::vector<double> rho(nS);
     const double Ed = tpe.SimplexDensities(M, rho.data());
     // an obstacle: the mesh shifted by 3 along z, loaded into the mesh
@@ -63,13 +64,9 @@ int run(const std::vector<double>& V, const std::vector<int>& S, int nV, int nS)
 int main(int argc, char** argv)
 {
     if (argc < 2) return 1;
-    std::ifstream in(argv[1]);
-    int nV = 0, nS = 0, dom = 0;
-    in >> nV >> nS >> dom;
-    std::vector<double> V(3 * nV);
-    std::vector<int> S((dom + 1) * nS);
-    for (double& x : V) in >> x;
-    for (int& s : S) in >> s;
-    if (!in) return 1;
-    return dom == 1 ? run<1>(V, S, nV, nS) : run<2>(V, S, nV, nS);
+    using MeshBase_T = Repulsor::SimplicialMeshBase<double, int, std::size_t>;
+    Repulsor::SimplicialMesh_Factory<MeshBase_T, 1, 2, 3, 3> factory;
+    std::unique_ptr<MeshBase_T> M = factory.Make_FromFile(argv[1], 4);
+    if (!M) return 1;
+    return M->DomDim() == 1 ? run<1>(*M) : run<2>(*M);
 }
