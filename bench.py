@@ -39,9 +39,8 @@ Q, P = 6.0, 12.0
 FLOPS_FAR_PAIR = 153.0
 FLOPS_NEAR_PAIR = 198.0
 # geometry (primitive data + in-block scans), block scan, cluster moments, near and far
-# pairs (one launch, each unordered pair once), lower-slot row sums, collect + chain rule,
-# vertex gather
-LAUNCHES_PER_STEP = 7
+# pairs (one launch), collect + chain rule, vertex gather
+LAUNCHES_PER_STEP = 6
 
 
 def max_over_ranks(x, dist, device):
@@ -62,10 +61,10 @@ def replica_throughput(world, steps_per_rank, max_ms):
 
 
 def pair_traffic_from_profile():
-    """DRAM bytes (read + write) of the pair launch and the row sums of one evaluation, from
-    the ncu capture summarised in profiles/k_tp0_pairs_once_torus160x120.md (null if absent)."""
+    """DRAM bytes (read + write) of the merged pair launch of one evaluation, from the ncu
+    capture summarised in profiles/k_tp0_pairs_tiled_both_torus160x120.md (null if absent)."""
     import re
-    path = os.path.join(ROOT, "profiles", "k_tp0_pairs_once_torus160x120.md")
+    path = os.path.join(ROOT, "profiles", "k_tp0_pairs_tiled_both_torus160x120.md")
     if not os.path.exists(path):
         return None
     m = re.search(r"DRAM bytes per evaluation[^:]*:\s*([0-9,]+)", open(path).read(), re.IGNORECASE)
@@ -87,8 +86,8 @@ def workload_mesh():
 
 
 WORKLOAD = {"workload": "torus R=1 r=0.4 160x120 (19,200 vertices, 38,400 triangles), q=6 p=12 theta=0.5",
-            "step": "SemiStaticUpdate + Differential (energy + dE, FP32 pair kernels with FP64 near-field projections, "
-                    "each unordered pair evaluated once), one CUDA graph per step",
+            "step": "SemiStaticUpdate + Differential (energy + dE, FP32 pair kernels with FP64 near-field projections), "
+                    "one CUDA graph per step",
             "l2": "256 MiB buffer overwritten before every timed step"}
 REFERENCE_STEP = ("SemiStaticUpdate + Differential in FP64 on host threads: the CPU restatement of the reference "
                   "path (oracle/tp0_oracle.cpp built with the reference's flags -O3 -ffast-math -fno-math-errno), "
@@ -338,10 +337,8 @@ def main():
         traffic = pair_traffic_from_profile()
         roofline = {"bound": "fp32", "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
                     "frac": achieved / peak.value, "traffic": traffic,
-                    "kernel": "k_tp0_pairs_tiled<FAR, 3, 6, DIFF, ONCE> (each unordered pair evaluated once from "
-                              "its upper-triangle row, the column's derivative left as a record in its lower slot) "
-                              "+ k_lower_sums (the records added per row); near and far timed as separate launches "
-                              "with the row sums in the far part, one k_tp0_pairs_tiled_both launch in the step",
+                    "kernel": "k_tp0_pairs_tiled (near and far patterns timed as separate launches; one "
+                              "k_tp0_pairs_tiled_both launch in the step)",
                     "peak_source": "measured FP32 FMA throughput (rpb_measure_fp32_peak); MEASURED_PEAKS.json "
                                    "has no FP32 figure",
                     "flops_per_evaluation": flops,

@@ -231,3 +231,30 @@ class LearnedGeometry:
         if quantize:
             dO = dO.astype(np.float32).astype(np.float64)
         return loss, mlp_backward(theta, cache, dO, quantize)
+
+    def apply_frozen(self, theta, R, Y, quantize=True):
+        """The application to Y with the gains the network gives for the residual R: the
+        linearization of M at R with the gains held fixed (rpb_tpm0_learned_apply_pair)."""
+        R = np.asarray(R, np.float64)
+        F, s = self.features(R)
+        O, _ = mlp_forward(theta, F, quantize)
+        O32 = O.astype(np.float32).astype(np.float64) if quantize else O
+        gain = np.exp(np.clip(O32, -GAIN_CLAMP, GAIN_CLAMP))
+        w = (self.A_C / self.A_C[0]) ** LEVEL_EXPONENT / self.A_C
+        Yc = self.range_sums(self.prim_from_vertices(np.asarray(Y, np.float64))) * w[:, None]
+        z = self.vertices_from_prims(self.expand(gain * Yc))
+        return z - z.mean(0)
+
+    def grad_given(self, theta, R, G, quantize=True, reg=0.0):
+        """Objective G . M(R) and its parameter gradient (with the gain penalty
+        reg * mean(o^2)) for a given sensitivity G = dL/dz (rpb_mlp_train_step_sens)."""
+        R = np.asarray(R, np.float64)
+        G = np.asarray(G, np.float64)
+        z, (cache, O32, gain, Rc) = self.apply(theta, R, return_cache=True, quantize=quantize)
+        g = G - G.mean(0)
+        gc = self.range_sums(self.prim_from_vertices(g))
+        inside = np.abs(O32) < GAIN_CLAMP
+        dO = gc * Rc * gain * inside + 2.0 * reg * O32 / (3.0 * self.NC)
+        if quantize:
+            dO = dO.astype(np.float32).astype(np.float64)
+        return float((G * z).sum()), mlp_backward(theta, cache, dO, quantize)

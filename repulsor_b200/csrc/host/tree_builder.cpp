@@ -586,37 +586,6 @@ std::string build_cross_lists(const HostTree& S, const double* VS, const int* SS
     return std::string();
 }
 
-void build_upper_pattern(const SymPattern& P, UpperPattern& U)
-{
-    U = UpperPattern();
-    const int n = P.rows;
-    U.rows = n;
-    U.rp.assign(static_cast<size_t>(n) + 1, 0);
-    U.lrp.assign(static_cast<size_t>(n) + 1, 0);
-    if (P.rp.empty()) { U.valid = true; return; }
-    for (int i = 0; i < n; ++i) {
-        U.rp[i + 1] = U.rp[i] + (P.rp[i + 1] - P.diag[i]);
-        U.lrp[i + 1] = U.lrp[i] + (P.diag[i] - P.rp[i]);
-    }
-    if (U.rp[n] != U.lrp[n] || U.lrp[n] > 0x7fffffffLL) return;   // not symmetric, or too large
-    U.ci.resize(static_cast<size_t>(U.rp[n]));
-    U.lpos.resize(static_cast<size_t>(U.rp[n]));
-    // rows in ascending order meet the lower entries of each row j in ascending column
-    // order, which is the order of row j's lower part
-    std::vector<int64_t> next(U.lrp.begin(), U.lrp.end() - 1);
-    for (int i = 0; i < n; ++i) {
-        int64_t u = U.rp[i];
-        for (int64_t k = P.diag[i]; k < P.rp[i + 1]; ++k, ++u) {
-            const int j = P.ci[k];
-            U.ci[u] = j;
-            U.lpos[u] = static_cast<int>(next[j]++);
-        }
-    }
-    for (int j = 0; j < n; ++j)
-        if (next[j] != U.lrp[j + 1]) return;   // the pattern was not symmetric
-    U.valid = true;
-}
-
 void build_row_tiles(const int64_t* rp, const int* ci, int rows, int ncols, int block_lanes, int64_t target_entries,
                      int max_union, int threads, RowTiles& out)
 {

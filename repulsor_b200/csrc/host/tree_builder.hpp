@@ -59,24 +59,6 @@ std::string build_cluster_tree(int dom, const double* V, int nV, const int* S, i
                                HostTree& out, std::vector<double>& P);
 void build_block_cluster_tree(HostTree& T, const std::vector<double>& P, const int* S, const TreeSettings& set);
 
-// Upper triangle of a symmetric pattern (the entries j > i of each row, in row order)
-// and, for every upper entry (i, j), the position of its transposed entry (j, i) among
-// the lower-triangle entries (the entries j < i of each row, rows consecutive, columns
-// ascending: row j's lower entries are [lrp[j], lrp[j + 1])). The pair kernels evaluate
-// each unordered pair once from its upper entry and leave the column's derivative in the
-// lower slot, which the row of the lower entry adds up afterwards.
-struct UpperPattern {
-    int rows = 0;
-    std::vector<int64_t> rp;        // rows + 1
-    std::vector<int> ci;            // upper entries' columns
-    std::vector<int> lpos;          // upper entry -> lower slot
-    std::vector<int64_t> lrp;       // rows + 1
-    bool valid = false;             // false when the slots do not fit 32-bit indices
-    int64_t nnz() const { return rp.empty() ? 0 : rp.back(); }
-};
-
-void build_upper_pattern(const SymPattern& P, UpperPattern& U);
-
 // Rectangular CSR (rows of one tree, columns of another), columns sorted.
 struct CrossPattern {
     int rows = 0;

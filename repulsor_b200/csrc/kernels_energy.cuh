@@ -333,63 +333,6 @@ __device__ __forceinline__ R tp0_core(const TPExp& ex, const Proj<R>& g, R a, R 
     return a * E * b;
 }
 
-// One evaluation for both sides of an unordered pair: as tp0_core for the row (x), plus
-// the column's (y) derivative in the same centred form, which follows from the symmetry
-// of the kernel under (x, P, a) <-> (y, Q, b), v -> -v:
-//     d0_y = a (E - q/2 |w|^{q/2-1} w s^{p/2-q/2}),   dx_y = a G,   dP_y = a/2 K_yx v v^T,
-// with G = K_xy P v + K_yx Q v - H v (the row gets dx_x = -b G). The column's part leaves
-// as a record of 8 values, rec = [d0_y, a G, a K_yx / 2, v], from which the row pass
-// (k_lower_sums) rebuilds dP_y.
-template <typename R, int QH, int PH>
-__device__ __forceinline__ R tp0_core_pair(const TPExp& ex, const Proj<R>& g, R a, R b, PairAcc<R>& acc, R (&rec)[8])
-{
-    const R s = dev_rcp(g.r2);
-    const R u = g.cphi * s;
-    const R w = g.cpsi * s;
-    R uq1, wq1, se;
-    if constexpr (QH > 0 && PH >= QH) {
-        uq1 = ipow_pos(fabs(u), QH - 1);
-        wq1 = ipow_pos(fabs(w), QH - 1);
-        se = ipow_pos(s, PH - QH);
-    } else {
-        const R qh = static_cast<R>(ex.q * 0.5), ph = static_cast<R>(ex.p * 0.5);
-        uq1 = (fabs(u) > R(0)) ? dev_pow(fabs(u), qh - R(1)) : R(0);
-        wq1 = (fabs(w) > R(0)) ? dev_pow(fabs(w), qh - R(1)) : R(0);
-        se = dev_pow(s, ph - qh);
-    }
-    const R uq = uq1 * u, wq = wq1 * w;
-    const R E = (uq + wq) * se;
-    const R q = static_cast<R>(ex.q), p = static_cast<R>(ex.p);
-    const R se1 = se * s;
-    const R Kxy = q * uq1 * se1;
-    const R Kyx = q * wq1 * se1;
-    const R H = p * (uq + wq) * se1;
-    const R hq = R(0.5) * q * se;
-    acc.d0 += b * (E - hq * uq);
-    R G[3];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        G[k] = Kxy * g.Pv[k] + Kyx * g.Qv[k] - H * g.v[k];
-        acc.dx[k] -= b * G[k];
-    }
-    const R hb = R(0.5) * b * Kxy;
-    acc.dP[0] += hb * g.v[0] * g.v[0];
-    acc.dP[1] += hb * R(2) * g.v[0] * g.v[1];
-    acc.dP[2] += hb * R(2) * g.v[0] * g.v[2];
-    acc.dP[3] += hb * g.v[1] * g.v[1];
-    acc.dP[4] += hb * R(2) * g.v[1] * g.v[2];
-    acc.dP[5] += hb * g.v[2] * g.v[2];
-    rec[0] = a * (E - hq * wq);
-    rec[1] = a * G[0];
-    rec[2] = a * G[1];
-    rec[3] = a * G[2];
-    rec[4] = R(0.5) * a * Kyx;
-    rec[5] = g.v[0];
-    rec[6] = g.v[1];
-    rec[7] = g.v[2];
-    return a * E * b;
-}
-
 // A primitive's pair data as the tiled near-field kernel keeps it in shared memory: the
 // 64-byte PrimDatum plus FP32 copies of the normal and the weight, converted once when the
 // tile is staged instead of once per pair (80 bytes: consecutive data start on different
@@ -490,10 +433,6 @@ struct PairArgs {
     double* energy_out;       // 1
     TPExp ex;
     float close_factor;       // FP64 path for near pairs with r < close_factor (d_i + d_j)
-    // once-per-pair evaluation (upper-triangle rows): the lower slot of every entry and the
-    // 8-float column records, two float4 per slot
-    const int* lpos;
-    float4* rec;
 };
 
 constexpr int PAIR_BLOCK = 256;
@@ -546,47 +485,11 @@ __device__ __noinline__ Close64 close_pair_fp64(TPExp ex, int dom, Datum X, ColD
     return c;
 }
 
-// The same for a pair evaluated once: the row's part as Close64, the column's record.
-struct Close64Pair {
-    double e;
-    double d[10];
-    float rec[8];
-};
-
-template <int QH, int PH, typename Datum, typename ColDatum>
-__device__ __noinline__ Close64Pair close_pair_fp64_both(TPExp ex, int dom, Datum X, ColDatum Y)
-{
-    Proj<double> gd;
-    project_prims(dom, X, Y, gd);
-    PairAcc<double> a64 = {};
-    double r64[8];
-    Close64Pair c;
-    c.e = tp0_core_pair<double, QH, PH>(ex, gd, X.a, Y.a, a64, r64);
-    c.d[0] = a64.d0;
-#pragma unroll
-    for (int m = 0; m < 3; ++m) c.d[1 + m] = a64.dx[m];
-#pragma unroll
-    for (int m = 0; m < 6; ++m) c.d[4 + m] = a64.dP[m];
-#pragma unroll
-    for (int m = 0; m < 8; ++m) c.rec[m] = static_cast<float>(r64[m]);
-    return c;
-}
-
-__device__ __forceinline__ void store_record(float4* rec, int slot, const float (&r)[8])
-{
-    float4* dst = rec + 2 * static_cast<int64_t>(slot);
-    dst[0] = make_float4(r[0], r[1], r[2], r[3]);
-    dst[1] = make_float4(r[4], r[5], r[6], r[7]);
-}
-
 // SACC: the row's FP64 derivative accumulators live in shared memory at
 // Dsm[m * PAIR_TILE_THREADS] (zeroed by the caller) instead of D64, which is then filled
 // from them at the end; this keeps 20 registers free inside the loop.
-// ONCE: the row holds only its upper entries (columns j > i); every pair counts its energy
-// and, with DIFF, also forms the column's derivative, stored as a record in the entry's
-// lower slot (A.lpos, A.rec).
 template <bool FAR, int QH, int PH, bool DIFF, bool CROSS, bool PREFETCH, bool SACC, typename ColDatum,
-          bool ONCE = false, typename Datum, typename Index, typename Fetch>
+          typename Datum, typename Index, typename Fetch>
 __device__ __forceinline__ void pair_row(const PairArgs& A, const Datum& X, int i, int sub, int stride, Index index,
                                          Fetch datum, double& e_row, double (&D64)[10], double* Dsm)
 {
@@ -626,31 +529,16 @@ __device__ __forceinline__ void pair_row(const PairArgs& A, const Datum& X, int 
         if (close) {
             // close near-field pair: the same kernel in FP64, added straight into FP64
             if constexpr (!FAR) {
-                if constexpr (ONCE && DIFF) {
-                    const Close64Pair c = close_pair_fp64_both<QH, PH>(A.ex, A.dom, X, Y);
-                    e_row += c.e;
+                const Close64 c = close_pair_fp64<QH, PH, DIFF>(A.ex, A.dom, X, Y);
+                if (CROSS || j > i) e_row += c.e;
+                if (DIFF) {
 #pragma unroll
                     for (int m = 0; m < 10; ++m) add64(m, c.d[m]);
-                    store_record(A.rec, __ldg(A.lpos + k), c.rec);
-                } else {
-                    const Close64 c = close_pair_fp64<QH, PH, DIFF>(A.ex, A.dom, X, Y);
-                    if (ONCE || CROSS || j > i) e_row += c.e;
-                    if (DIFF) {
-#pragma unroll
-                        for (int m = 0; m < 10; ++m) add64(m, c.d[m]);
-                    }
                 }
             }
         } else {
-            float e;
-            if constexpr (ONCE && DIFF) {
-                float rec[8];
-                e = tp0_core_pair<float, QH, PH>(A.ex, g, ax, weight_f(Y), acc, rec);
-                store_record(A.rec, __ldg(A.lpos + k), rec);
-            } else {
-                e = tp0_core<float, QH, PH, DIFF>(A.ex, g, ax, weight_f(Y), acc);
-            }
-            if (ONCE || CROSS || j > i) e32 += e;
+            const float e = tp0_core<float, QH, PH, DIFF>(A.ex, g, ax, weight_f(Y), acc);
+            if (CROSS || j > i) e32 += e;
             if (++since_flush == PAIR_FLUSH) {
                 since_flush = 0;
                 e_row += e32;
@@ -823,7 +711,7 @@ __host__ __device__ constexpr size_t pair_tile_smem(int n, bool far)
     return pair_tile_union_bytes(n, far) + (far ? 0 : sizeof(double) * 10 * PAIR_TILE_THREADS);
 }
 
-template <bool FAR, int QH, int PH, bool DIFF, bool ONCE = false>
+template <bool FAR, int QH, int PH, bool DIFF>
 __device__ __forceinline__ void pairs_tiled_body(const PairArgs& A, const PairTiles& T, int bid, int nblocks)
 {
     using Datum = typename std::conditional<FAR, ClusterDatum, PrimDatum>::type;
@@ -889,74 +777,28 @@ __device__ __forceinline__ void pairs_tiled_body(const PairArgs& A, const PairTi
             else Y = reinterpret_cast<const PrimTile*>(tile_smem)[u];
             j = sid[u];
         };
-        pair_row<FAR, QH, PH, DIFF, false, false, !FAR && DIFF, ColDatum, ONCE>(A, X, i, sub, size, index, datum, e_row,
-                                                                              D64, Dsm);
+        pair_row<FAR, QH, PH, DIFF, false, false, !FAR && DIFF, ColDatum>(A, X, i, sub, size, index, datum, e_row, D64,
+                                                                        Dsm);
     }
     pair_epilogue<DIFF, false>(A, active, i, sub, size, warp_size_max, e_row, D64, bid, nblocks);
 }
 
-template <bool FAR, int QH, int PH, bool DIFF, bool ONCE = false>
+template <bool FAR, int QH, int PH, bool DIFF>
 __global__ void __launch_bounds__(PAIR_TILE_THREADS, 2) k_tp0_pairs_tiled(PairArgs A, PairTiles T)
 {
-    pairs_tiled_body<FAR, QH, PH, DIFF, ONCE>(A, T, blockIdx.x, gridDim.x);
+    pairs_tiled_body<FAR, QH, PH, DIFF>(A, T, blockIdx.x, gridDim.x);
 }
 
 // Both patterns in one launch: blocks [0, nfar) take the far tiles, the others the near
 // tiles, so the far and near tiles share the waves instead of draining and refilling
 // the GPU between two launches. Each part keeps its own block indices, energy partials
 // and last-block sum, so the results equal those of the two separate launches.
-template <int QH, int PH, bool DIFF, bool ONCE = false>
+template <int QH, int PH, bool DIFF>
 __global__ void __launch_bounds__(PAIR_TILE_THREADS, 2)
     k_tp0_pairs_tiled_both(PairArgs An, PairTiles Tn, PairArgs Af, PairTiles Tf, int nfar)
 {
-    if (static_cast<int>(blockIdx.x) < nfar) pairs_tiled_body<true, QH, PH, DIFF, ONCE>(Af, Tf, blockIdx.x, nfar);
-    else pairs_tiled_body<false, QH, PH, DIFF, ONCE>(An, Tn, blockIdx.x - nfar, gridDim.x - nfar);
-}
-
-// Lower-slot row pass of the once-per-pair evaluation: every row adds the records left in
-// its lower slots [lrp[i], lrp[i + 1]) (the column derivatives of the pairs evaluated from
-// the rows before it) to the derivative its own upper entries gave, in slot order. Rows
-// [0, N) are the near pattern's, [N, N + NC) the far pattern's.
-struct LowerSumArgs {
-    int N, NC;
-    const int64_t* lrp_near;
-    const float4* rec_near;
-    double* D_near;
-    const int64_t* lrp_far;
-    const float4* rec_far;
-    double* D_far;
-};
-
-static __global__ void k_lower_sums(LowerSumArgs A)
-{
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool far = t >= A.N;
-    const int i = far ? t - A.N : t;
-    if (far ? i >= A.NC : false) return;
-    const int64_t* lrp = far ? A.lrp_far : A.lrp_near;
-    const float4* rec = far ? A.rec_far : A.rec_near;
-    double* D = (far ? A.D_far : A.D_near) + 10 * static_cast<int64_t>(i);
-    const int64_t l0 = lrp ? __ldg(lrp + i) : 0, l1 = lrp ? __ldg(lrp + i + 1) : 0;
-    pdl_wait();
-    pdl_launch_dependents();
-    if (l1 <= l0) return;
-    double d[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
-    for (int64_t l = l0; l < l1; ++l) {
-        const float4 r0 = __ldcs(rec + 2 * l), r1 = __ldcs(rec + 2 * l + 1);
-        const double c = r1.x, v0 = r1.y, v1 = r1.z, v2 = r1.w;
-        d[0] += r0.x;
-        d[1] += r0.y;
-        d[2] += r0.z;
-        d[3] += r0.w;
-        d[4] += c * v0 * v0;
-        d[5] += c * 2.0 * v0 * v1;
-        d[6] += c * 2.0 * v0 * v2;
-        d[7] += c * v1 * v1;
-        d[8] += c * 2.0 * v1 * v2;
-        d[9] += c * v2 * v2;
-    }
-#pragma unroll
-    for (int m = 0; m < 10; ++m) D[m] += d[m];
+    if (static_cast<int>(blockIdx.x) < nfar) pairs_tiled_body<true, QH, PH, DIFF>(Af, Tf, blockIdx.x, nfar);
+    else pairs_tiled_body<false, QH, PH, DIFF>(An, Tn, blockIdx.x - nfar, gridDim.x - nfar);
 }
 
 // energy = near-field part + far-field part (the order evaluate() uses on the host)

@@ -45,7 +45,6 @@ int64_t rpb_mesh::device_bytes() const
              t->lane_map.bytes();
     b += P_pair.bytes() + C_pair.bytes() + counter.bytes() + P_near.bytes() + scan_local.bytes() +
          scan_blocks.bytes() + C_begin.bytes() + C_end.bytes();
-    b += near_once.bytes() + far_once.bytes();
     b += D_near.bytes() + D_far.bytes() + vf.bytes() + B.bytes() + v_rp.bytes() + v_slot.bytes() + Y.bytes();
     b += block_energy.bytes() + energy.bytes() + done.bytes();
     b += pre_cols.bytes() + pre_vals.bytes() + vp_rp.bytes() + vp_slot.bytes();
@@ -163,12 +162,6 @@ static cudaError_t allow_tile_smem_t()
     set(reinterpret_cast<const void*>(k_tp0_pairs_tiled<true, QH, PH, false>), fb);
     set(reinterpret_cast<const void*>(k_tp0_pairs_tiled_both<QH, PH, true>), std::max(nb, fb));
     set(reinterpret_cast<const void*>(k_tp0_pairs_tiled_both<QH, PH, false>), std::max(nb, fb));
-    set(reinterpret_cast<const void*>(k_tp0_pairs_tiled<false, QH, PH, true, true>), nb);
-    set(reinterpret_cast<const void*>(k_tp0_pairs_tiled<false, QH, PH, false, true>), nb);
-    set(reinterpret_cast<const void*>(k_tp0_pairs_tiled<true, QH, PH, true, true>), fb);
-    set(reinterpret_cast<const void*>(k_tp0_pairs_tiled<true, QH, PH, false, true>), fb);
-    set(reinterpret_cast<const void*>(k_tp0_pairs_tiled_both<QH, PH, true, true>), std::max(nb, fb));
-    set(reinterpret_cast<const void*>(k_tp0_pairs_tiled_both<QH, PH, false, true>), std::max(nb, fb));
     return e;
 }
 
@@ -262,8 +255,8 @@ static rpb_status ensure_block_energy(rpb_mesh* m, int blocks)
     return RPB_OK;
 }
 
-// Row tiles of the two full patterns for `shards` row shards (rpb_mesh_set_shards). Sets
-// the launch grids of the full-pattern kernels.
+// Row tiles of the two patterns for `shards` row shards (1 at mesh creation; more with
+// rpb_mesh_set_shards). Sets the launch grids of the pair kernels.
 static rpb_status build_pair_tiles(rpb_mesh* m, int shards)
 {
     rpb_status st;
@@ -284,50 +277,6 @@ static rpb_status build_pair_tiles(rpb_mesh* m, int shards)
     if (m->far_tiles.valid) m->far_blocks = m->far_tiles.tiles;
     m->shards = shards;
     return ensure_block_energy(m, m->near_blocks + m->far_blocks);
-}
-
-// The once-per-pair form of both patterns: upper triangles with their lower slots, the
-// column records and the upper triangles' row tiles. once_valid when every non-empty
-// pattern is tiled.
-static rpb_status build_once_tiles(rpb_mesh* m)
-{
-    rpb_status st;
-    if ((st = allow_tile_smem(m->device)) != RPB_OK) return st;
-    cudaStream_t s = m->stream;
-    m->once_valid = false;
-    const void* kn = reinterpret_cast<const void*>(k_tp0_pairs_tiled<false, 3, 6, true, true>);
-    const void* kf = reinterpret_cast<const void*>(k_tp0_pairs_tiled<true, 3, 6, true, true>);
-    bool ok = true;
-    int blocks = 0;
-    const SymPattern* pats[2] = {&m->tree.near, &m->tree.far};
-    OnceBufs* bufs[2] = {&m->near_once, &m->far_once};
-    for (int w = 0; w < 2; ++w) {
-        const SymPattern& P = *pats[w];
-        OnceBufs& d = *bufs[w];
-        const bool far = w == 1;
-        if (P.nnz() == 0) continue;
-        UpperPattern U;
-        build_upper_pattern(P, U);
-        if (!U.valid) { ok = false; continue; }
-        d.up.rows = U.rows;
-        d.up.nnz = U.nnz();
-        if ((st = upload(d.up.rp, U.rp.data(), U.rp.size(), s)) != RPB_OK) return st;
-        if ((st = upload(d.up.ci, U.ci.data(), U.ci.size(), s)) != RPB_OK) return st;
-        if ((st = upload(d.lpos, U.lpos.data(), U.lpos.size(), s)) != RPB_OK) return st;
-        if ((st = upload(d.lrp, U.lrp.data(), U.lrp.size(), s)) != RPB_OK) return st;
-        if (d.rec.alloc(2 * static_cast<size_t>(U.nnz()))) {
-            set_error("device allocation failed");
-            return RPB_ENOMEM;
-        }
-        if ((st = tile_pattern(m, U.rows, U.rp.data(), U.ci.data(), U.nnz(), far ? m->NC : m->N, far,
-                               far ? kf : kn, far ? FAR_TILE_UNION : NEAR_TILE_UNION, 1, d.tiles)) != RPB_OK)
-            return st;
-        if (!d.tiles.valid) ok = false;
-        blocks += d.tiles.tiles;
-    }
-    if ((st = ensure_block_energy(m, blocks)) != RPB_OK) return st;
-    m->once_valid = ok && (m->tree.near.nnz() + m->tree.far.nnz() > 0);
-    return RPB_OK;
 }
 
 template <int QH, int PH>
@@ -374,82 +323,14 @@ static void launch_pairs_t(rpb_mesh* m, const PairArgs& An, const PairArgs& Af, 
     }
 }
 
-// Once-per-pair launches: the upper triangles' tiles (near and far in one launch unless
-// `between` separates them), then, for the differential, the lower-slot row pass.
-template <int QH, int PH>
-static void launch_pairs_once_t(rpb_mesh* m, const PairArgs& An, const PairArgs& Af, bool diff, cudaEvent_t between)
-{
-    const TileBufs& tn = m->near_once.tiles;
-    const TileBufs& tf = m->far_once.tiles;
-    const bool near = An.rows > 0, far = Af.rows > 0;
-    if (near && far && !between) {
-        const size_t smem = std::max(pair_tile_smem(tn.max_union, false), pair_tile_smem(tf.max_union, true));
-        launch_pdl(diff ? k_tp0_pairs_tiled_both<QH, PH, true, true> : k_tp0_pairs_tiled_both<QH, PH, false, true>,
-                   tn.tiles + tf.tiles, PAIR_TILE_THREADS, smem, m->stream, An, tiles_view(tn, 0), Af, tiles_view(tf, 0),
-                   tf.tiles);
-    } else {
-        if (near)
-            launch_pdl(diff ? k_tp0_pairs_tiled<false, QH, PH, true, true> : k_tp0_pairs_tiled<false, QH, PH, false, true>,
-                       tn.tiles, PAIR_TILE_THREADS, pair_tile_smem(tn.max_union, false), m->stream, An, tiles_view(tn, 0));
-        if (between) cudaEventRecord(between, m->stream);
-        if (far)
-            launch_pdl(diff ? k_tp0_pairs_tiled<true, QH, PH, true, true> : k_tp0_pairs_tiled<true, QH, PH, false, true>,
-                       tf.tiles, PAIR_TILE_THREADS, pair_tile_smem(tf.max_union, true), m->stream, Af, tiles_view(tf, 0));
-    }
-    if (diff) {
-        LowerSumArgs L;
-        L.N = near ? m->N : 0;
-        L.NC = far ? m->NC : 0;
-        L.lrp_near = m->near_once.lrp.ptr; L.rec_near = m->near_once.rec.ptr; L.D_near = An.D;
-        L.lrp_far = m->far_once.lrp.ptr; L.rec_far = m->far_once.rec.ptr; L.D_far = Af.D;
-        const int rows = L.N + L.NC;
-        if (rows > 0) launch_pdl(k_lower_sums, (rows + 255) / 256, 256, 0, m->stream, L);
-    }
-}
-
 // Near- and far-field pair kernels on the mesh stream. shard >= 0: only that row shard's
 // tiles (both patterns tiled), derivatives into D_near / D_far (zeroed first), energies into
-// energy[0..1]; shard < 0: every row, into the mesh's own buffers -- each unordered pair
-// evaluated once when the upper triangles are tiled and the mesh is not set up for row
-// shards (whose sum then equals the unsharded evaluation with the same tiles bit for bit).
+// energy[0..1]; shard < 0: every row, into the mesh's own buffers.
 rpb_status launch_pairs(rpb_mesh* m, const TPExp& ex, bool diff, cudaEvent_t between = nullptr, int shard = -1,
                         double* D_near = nullptr, double* D_far = nullptr)
 {
-    if (shard < 0 && m->once_valid && m->shards <= 1) {
-        PairArgs An, Af;
-        An.col_data = Af.col_data = nullptr;
-        An.dom = Af.dom = m->dom;
-        An.ex = Af.ex = ex;
-        An.close_factor = Af.close_factor = 0.1f;
-        An.order = Af.order = nullptr;
-        An.rows = m->near.nnz > 0 ? m->N : 0;
-        An.rp = m->near_once.up.rp.ptr; An.ci = m->near_once.up.ci.ptr; An.lpos = m->near_once.lpos.ptr;
-        An.rec = m->near_once.rec.ptr; An.data = m->P_pair.ptr; An.D = m->D_near.ptr;
-        An.block_energy = m->block_energy.ptr; An.done = m->done.ptr; An.energy_out = m->energy.ptr;
-        Af.rows = m->far.nnz > 0 ? m->NC : 0;
-        Af.rp = m->far_once.up.rp.ptr; Af.ci = m->far_once.up.ci.ptr; Af.lpos = m->far_once.lpos.ptr;
-        Af.rec = m->far_once.rec.ptr; Af.data = m->C_pair.ptr; Af.D = m->D_far.ptr;
-        Af.block_energy = m->block_energy.ptr + m->near_once.tiles.tiles; Af.done = m->done.ptr + 1;
-        Af.energy_out = m->energy.ptr + 1;
-        if (An.rows == 0) {
-            RPB_CUDA(cudaMemsetAsync(m->energy.ptr, 0, sizeof(double), m->stream));
-            if (diff) RPB_CUDA(cudaMemsetAsync(m->D_near.ptr, 0, m->D_near.bytes(), m->stream));
-        }
-        if (Af.rows == 0) {
-            RPB_CUDA(cudaMemsetAsync(m->energy.ptr + 1, 0, sizeof(double), m->stream));
-            if (diff) RPB_CUDA(cudaMemsetAsync(m->D_far.ptr, 0, m->D_far.bytes(), m->stream));
-        }
-        if (ex.qh == 3 && ex.ph == 6) launch_pairs_once_t<3, 6>(m, An, Af, diff, between);
-        else if (ex.qh == 2 && ex.ph == 4) launch_pairs_once_t<2, 4>(m, An, Af, diff, between);
-        else if (ex.qh == 1 && ex.ph == 2) launch_pairs_once_t<1, 2>(m, An, Af, diff, between);
-        else launch_pairs_once_t<-1, -1>(m, An, Af, diff, between);
-        RPB_CUDA(cudaGetLastError());
-        return RPB_OK;
-    }
     PairArgs An, Af;
     An.col_data = Af.col_data = nullptr;
-    An.lpos = Af.lpos = nullptr;
-    An.rec = Af.rec = nullptr;
     An.dom = Af.dom = m->dom;
     An.ex = Af.ex = ex;
     An.close_factor = Af.close_factor = 0.1f;
@@ -707,11 +588,7 @@ rpb_status rpb_mesh_create(int dom_dim, int amb_dim, const double* Vh, int64_t n
         if ((st = upload(m->far_order, fo.data(), fo.size(), s)) != RPB_OK) return fail(st);
         m->near_blocks = pair_blocks(m->N, NEAR_LANES);
         m->far_blocks = pair_blocks(m->NC, FAR_LANES);
-        // each pair once (upper triangles); the full-pattern tiles only where that is not
-        // possible (a row beyond the union cap) and for row shards (rpb_mesh_set_shards)
-        if ((st = ensure_block_energy(m, m->near_blocks + m->far_blocks)) != RPB_OK) return fail(st);
-        if ((st = build_once_tiles(m)) != RPB_OK) return fail(st);
-        if (!m->once_valid && (st = build_pair_tiles(m, 1)) != RPB_OK) return fail(st);
+        if ((st = build_pair_tiles(m, 1)) != RPB_OK) return fail(st);
     }
     if (cudaMemsetAsync(m->counter.ptr, 0, m->counter.bytes(), s) != cudaSuccess ||
         cudaMemsetAsync(m->done.ptr, 0, m->done.bytes(), s) != cudaSuccess ||

@@ -81,23 +81,6 @@ struct TileBufs {
     bool valid = false;
 };
 
-// One pattern evaluated once per unordered pair: its upper triangle (rows' entries j > i),
-// the lower slot of every upper entry, the rows' lower-slot ranges, the column records
-// (two float4 per slot) and the row tiles of the upper triangle.
-struct OnceBufs {
-    Csr up;
-    DevBuf<int> lpos;
-    DevBuf<int64_t> lrp;
-    DevBuf<float4> rec;
-    TileBufs tiles;
-    size_t bytes() const
-    {
-        return up.rp.bytes() + up.ci.bytes() + lpos.bytes() + lrp.bytes() + rec.bytes() + tiles.row0.bytes() +
-               tiles.cols_rp.bytes() + tiles.cols.bytes() + tiles.order.bytes() + tiles.lane_map.bytes() +
-               tiles.slot.bytes();
-    }
-};
-
 }  // namespace rpb
 
 struct rpb_mesh {
@@ -119,10 +102,7 @@ struct rpb_mesh {
     rpb::DevBuf<int> C_up4;   // fourth ancestor of every cluster (-1 when the root is nearer)
     rpb::Csr near, far, verynear;
     rpb::DevBuf<int> near_order, far_order;             // pair-kernel row order (length-sorted per chunk)
-    rpb::TileBufs near_tiles, far_tiles;                // shared-memory row tiles of the two full patterns
-                                                        // (row shards; built by rpb_mesh_set_shards)
-    rpb::OnceBufs near_once, far_once;                  // upper triangles: each pair evaluated once
-    bool once_valid = false;                            // both patterns tiled for the once-per-pair kernels
+    rpb::TileBufs near_tiles, far_tiles;                // shared-memory row tiles of the two patterns
     // geometry state
     rpb::DevBuf<rpb::PrimDatum> P_pair;
     rpb::DevBuf<rpb::ClusterDatum> C_pair;

@@ -22,7 +22,8 @@ import numpy as np
 from . import _capi
 from ._capi import PRECOND_NONE, RepulsorError, check, dptr, fptr
 
-__all__ = ["LearnedPreconditioner", "training_pairs", "train", "NPARAM_OUTPUT_OFFSET"]
+__all__ = ["LearnedPreconditioner", "training_pairs", "train", "unrolled_sensitivities", "train_unrolled",
+           "NPARAM_OUTPUT_OFFSET"]
 
 # offset of the output layer (W3, b3) in the parameter vector: W1 64x16, b1 64, W2 64x64, b2 64
 NPARAM_OUTPUT_OFFSET = 64 * 16 + 64 + 64 * 64 + 64
@@ -98,6 +99,30 @@ class LearnedPreconditioner:
         check(_capi.load().rpb_tpm0_learned_apply(M._h, dptr(R), dptr(Z)), "rpb_tpm0_learned_apply")
         return Z
 
+    def apply_pair(self, M, R, Y):
+        """(M(R), M_R(Y)): the application to R and, with the gains it gave, to Y."""
+        self.attach(M)
+        R = np.ascontiguousarray(R, dtype=np.float64)
+        Y = np.ascontiguousarray(Y, dtype=np.float64)
+        Z, ZY = np.zeros_like(R), np.zeros_like(R)
+        check(_capi.load().rpb_tpm0_learned_apply_pair(M._h, dptr(R), dptr(Y), dptr(Z), dptr(ZY)),
+              "rpb_tpm0_learned_apply_pair")
+        return Z, ZY
+
+    def train_step_sens(self, M, R, G, lr=1e-3, reg=0.0, want_grad=False):
+        """One Adam step (none for lr <= 0) on sum_k G[k] . M(R[k]) over the pairs of mesh M;
+        returns that objective before the step (and its gradient with want_grad)."""
+        R = np.ascontiguousarray(R, dtype=np.float64)
+        G = np.ascontiguousarray(G, dtype=np.float64)
+        if R.ndim == 2:
+            R, G = R[None], G[None]
+        obj = ctypes.c_double()
+        grad = np.zeros(self.param_count(), np.float32) if want_grad else None
+        check(_capi.load().rpb_mlp_train_step_sens(self._h, M._h, dptr(R), dptr(G), R.shape[0], float(lr), float(reg),
+                                                   ctypes.byref(obj), None if grad is None else fptr(grad)),
+              "rpb_mlp_train_step_sens")
+        return (obj.value, grad) if want_grad else obj.value
+
     def train_step(self, M, metric, R, E, lr=1e-3, want_grad=False, reg=0.0):
         """One Adam step (none for lr <= 0) on the pairs (R[k], E[k]) of mesh M and the
         metric's exponents; returns the loss before the step (and its gradient with
@@ -169,6 +194,96 @@ def train(net: LearnedPreconditioner, metric, data, epochs=200, lr=1e-3, batch=4
             for s in range(0, len(order), batch):
                 idx = order[s:s + batch]
                 losses.append(net.train_step(M, metric, R[idx], E[idx], lr=lr, reg=reg))
+        hist.append(float(np.mean(losses)))
+        if log is not None:
+            log(ep, hist[-1])
+    return hist
+
+
+def _cdot(a, b):
+    return np.einsum("ij,ij->j", a, b)
+
+
+def unrolled_sensitivities(net, M, metric, b, steps=30):
+    """The loss of `steps` iterations of preconditioned CG with z = M(r) from x = 0, one CG
+    per column: L = sum_c log(|r_K,c|^2 / |b_c|^2), and its sensitivities to the
+    preconditioner outputs, dL/dz_k, by the adjoint of the CG recurrences
+
+        q_k = A p_k,  alpha_k = g_k / (p_k . q_k),  r_k+1 = r_k - alpha_k q_k,
+        z_k+1 = M(r_k+1),  g_k+1 = r_k+1 . z_k+1,  beta_k = g_k+1 / g_k,  p_k+1 = z_k+1 + beta_k p_k,
+
+    run backwards; through z = M(r) the adjoint takes the application with the gains of
+    that r held fixed (apply_pair). Returns (L, R, G): the residuals r_0 .. r_K-1 the
+    preconditioner was applied to and the sensitivities dL/dz_k, for train_step_sens."""
+    b = np.ascontiguousarray(b, dtype=np.float64)
+    A = lambda X: metric.MultiplyMetric(M, 1.0, X)
+    r, z, p, q = [b], [net.apply(M, b)], [], []
+    p.append(z[0])
+    g = [_cdot(r[0], z[0])]
+    alpha, beta, delta = [], [], []
+    for k in range(steps):
+        qk = A(p[k])
+        dk = _cdot(p[k], qk)
+        ak = g[k] / dk
+        rk1 = r[k] - ak * qk
+        q.append(qk); delta.append(dk); alpha.append(ak); r.append(rk1)
+        if k + 1 < steps:
+            zk1 = net.apply(M, rk1)
+            gk1 = _cdot(rk1, zk1)
+            bk = gk1 / g[k]
+            z.append(zk1); g.append(gk1); beta.append(bk)
+            p.append(zk1 + bk * p[k])
+    nb2, nr2 = _cdot(b, b), _cdot(r[steps], r[steps])
+    loss = float(np.sum(np.log(nr2 / nb2)))
+    rbar = 2.0 * r[steps] / nr2
+    zbar = [np.zeros_like(b) for _ in range(steps)]
+    pbar_next = np.zeros_like(b)
+    for k in reversed(range(steps)):
+        pbar = np.zeros_like(b)
+        if k + 1 < steps:
+            # p_k+1 = z_k+1 + beta_k p_k; beta_k = g_k+1 / g_k; g_k+1 = r_k+1 . z_k+1
+            zbar[k + 1] += pbar_next
+            bbar = _cdot(pbar_next, p[k])
+            pbar += beta[k] * pbar_next
+            gbar1 = bbar / g[k]
+            gbar_k = -bbar * g[k + 1] / g[k] ** 2
+            rbar = rbar + gbar1 * z[k + 1]
+            zbar[k + 1] += gbar1 * r[k + 1]
+            # z_k+1 = M(r_k+1), gains held fixed
+            _, mz = net.apply_pair(M, r[k + 1], zbar[k + 1])
+            rbar = rbar + mz
+        else:
+            gbar_k = np.zeros(3)
+        # r_k+1 = r_k - alpha_k q_k; alpha_k = g_k / delta_k; delta_k = p_k . q_k; q_k = A p_k
+        abar = -_cdot(rbar, q[k])
+        qbar = -alpha[k] * rbar
+        gbar_k = gbar_k + abar / delta[k]
+        dbar = -abar * g[k] / delta[k] ** 2
+        pbar += dbar * q[k]
+        qbar = qbar + dbar * p[k]
+        pbar += A(qbar)
+        # g_k = r_k . z_k
+        rbar = rbar + gbar_k * z[k]
+        zbar[k] += gbar_k * r[k]
+        pbar_next = pbar
+    zbar[0] += pbar_next            # p_0 = z_0
+    return loss, np.stack(r[:steps]), np.stack(zbar)
+
+
+def train_unrolled(net, metric, meshes_rhs, epochs=1, lr=1e-3, steps=30, reg=1e-3, seed=0, log=None):
+    """Adam on the unrolled-CG loss: for every (mesh, right-hand side) pair in meshes_rhs,
+    the sensitivities of `steps` preconditioned CG iterations with the current network,
+    then one step on them. Returns the mean loss per epoch (the loss of the network each
+    pair was visited with)."""
+    rng = np.random.default_rng(seed)
+    hist = []
+    for ep in range(epochs):
+        losses = []
+        for i in rng.permutation(len(meshes_rhs)):
+            M, b = meshes_rhs[i]
+            loss, R, G = unrolled_sensitivities(net, M, metric, b, steps)
+            net.train_step_sens(M, R, G, lr=lr, reg=reg)
+            losses.append(loss)
         hist.append(float(np.mean(losses)))
         if log is not None:
             log(ep, hist[-1])

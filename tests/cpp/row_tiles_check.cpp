@@ -3,10 +3,7 @@
 // sorted and unique, every entry's slot names its column, each tile's order is a
 // permutation of its rows, and the lane map gives every row one aligned power-of-two
 // group inside a warp (each lane at most once). A row longer than the cap disables the
-// tiles. The upper triangle of a symmetric pattern (build_upper_pattern) holds exactly the
-// entries j > i, and its lower slots are a bijection onto the entries j < i in which the
-// slot of (i, j) lies in row j's range and is the position of i there. Prints "ok" or the
-// first violation.
+// tiles. Prints "ok" or the first violation.
 #include <algorithm>
 #include <cstdio>
 #include <random>
@@ -80,47 +77,6 @@ static int check(int rows, int band, int lanes, int cap, int threads, unsigned s
     return 0;
 }
 
-static int check_upper(int rows, int band, unsigned seed)
-{
-    std::mt19937 rng(seed);
-    std::vector<std::vector<int>> adj(rows);
-    std::uniform_int_distribution<int> off(1, band);
-    for (int i = 0; i < rows; ++i)
-        for (int t = 0; t < band / 2; ++t) {
-            const int j = std::min(rows - 1, i + off(rng));
-            if (j != i) { adj[i].push_back(j); adj[j].push_back(i); }
-        }
-    rpb::SymPattern P;
-    P.rows = rows;
-    P.rp.assign(rows + 1, 0);
-    P.diag.resize(rows);
-    for (int i = 0; i < rows; ++i) {
-        std::sort(adj[i].begin(), adj[i].end());
-        adj[i].erase(std::unique(adj[i].begin(), adj[i].end()), adj[i].end());
-        P.ci.insert(P.ci.end(), adj[i].begin(), adj[i].end());
-        P.rp[i + 1] = static_cast<int64_t>(P.ci.size());
-        P.diag[i] = std::upper_bound(P.ci.begin() + P.rp[i], P.ci.end(), i) - P.ci.begin();
-    }
-    rpb::UpperPattern U;
-    rpb::build_upper_pattern(P, U);
-    if (!U.valid || U.rows != rows) { std::printf("upper pattern invalid\n"); return 1; }
-    if (2 * U.nnz() != P.nnz() || U.lrp[rows] != U.nnz()) { std::printf("upper/lower sizes\n"); return 1; }
-    std::vector<int> hit(static_cast<size_t>(U.nnz()), 0);
-    for (int i = 0; i < rows; ++i) {
-        if (U.rp[i + 1] - U.rp[i] != P.rp[i + 1] - P.diag[i]) { std::printf("upper row %d\n", i); return 1; }
-        if (U.lrp[i + 1] - U.lrp[i] != P.diag[i] - P.rp[i]) { std::printf("lower row %d\n", i); return 1; }
-        for (int64_t u = U.rp[i]; u < U.rp[i + 1]; ++u) {
-            const int j = U.ci[u];
-            if (j <= i) { std::printf("upper entry below the diagonal\n"); return 1; }
-            const int64_t l = U.lpos[u];
-            if (l < U.lrp[j] || l >= U.lrp[j + 1]) { std::printf("slot outside row %d\n", j); return 1; }
-            if (P.ci[P.rp[j] + (l - U.lrp[j])] != i) { std::printf("slot of (%d,%d) is not the transpose\n", i, j); return 1; }
-            if (hit[l]++) { std::printf("slot used twice\n"); return 1; }
-        }
-    }
-    return 0;
-}
-
 int main()
 {
     int bad = 0;
@@ -130,9 +86,6 @@ int main()
     bad |= check(1, 1, 288, 1024, 1, 4u);            // a single row without entries
     bad |= check(70000, 12, 256, 1536, 8, 5u);       // many tiles, short rows
     bad |= check(3000, 120, 64, 4096, 2, 6u);        // long rows, few lanes
-    bad |= check_upper(10000, 40, 7u);
-    bad |= check_upper(1, 1, 8u);                    // one row, no entries
-    bad |= check_upper(3000, 120, 9u);
     if (!bad) std::printf("ok\n");
     return bad;
 }

@@ -142,7 +142,9 @@ def test_example_driver_with_the_obstacle_loaded_first_matches_python_mirror(tmp
     do = tpo.Differential(M)
     for k in ("energy", "differential_max", "gradient_max", "step_size", "energy_new"):
         assert _close(f[k], r[k], 1e-10), (k, f[k], r[k])
-    assert f["energy_pointer"] == pytest.approx(r["energy"], rel=1e-12)
+    # Differential's energy comes from the pair kernel with derivatives, Value's from the one
+    # without: the same sum in other FP32 orders
+    assert f["energy_pointer"] == pytest.approx(r["energy"], rel=1e-8)
     assert int(f["solve_iterations"]) == r["solve_iterations"]
     assert _close(f["solve_relative_residual_max"], r["solve_relative_residual_max"], 1e-5)
     assert 0 < f["step_size"] <= 1 and f["energy_decreased"] == 1

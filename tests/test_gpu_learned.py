@@ -94,6 +94,41 @@ def test_training_gradient_matches_oracle(surface):
     np.testing.assert_array_equal(net.get_params(), th)     # lr = 0: no step
 
 
+def test_frozen_gain_application_matches_oracle(surface):
+    """apply_pair: M(R) as apply gives it, and the application to Y with R's gains."""
+    V, S, M, om, G = surface
+    th = _theta(8, out_scale=0.5)
+    net = LearnedPreconditioner(params=th)
+    rng = np.random.default_rng(3)
+    r, y = rng.normal(size=V.shape), rng.normal(size=V.shape)
+    z, zy = net.apply_pair(M, r, y)
+    z_ref, zy_ref = G.apply(th, r), G.apply_frozen(th, r, y)
+    assert np.abs(z - z_ref).max() <= Z_TOL * np.abs(z_ref).max()
+    assert np.abs(zy - zy_ref).max() <= Z_TOL * np.abs(zy_ref).max()
+    # with Y = R it is the application itself
+    _, zr = net.apply_pair(M, r, r)
+    assert np.abs(zr - z).max() <= 1e-12 * np.abs(z).max()
+
+
+def test_sensitivity_training_gradient_matches_oracle(surface):
+    """train_step_sens: the gradient of sum_k G_k . M(R_k) (with the gain penalty) for given
+    sensitivities, as the unrolled-solve training uses it."""
+    V, S, M, om, G = surface
+    th = _theta(9)
+    net = LearnedPreconditioner(params=th)
+    rng = np.random.default_rng(4)
+    R = rng.normal(size=(3,) + V.shape)
+    Gs = rng.normal(size=(3,) + V.shape)
+    obj, g = net.train_step_sens(M, R, Gs, lr=0.0, reg=0.1, want_grad=True)
+    ref = [G.grad_given(th, R[k], Gs[k], reg=0.1) for k in range(3)]
+    obj_ref = sum(o for o, _ in ref)
+    g_ref = np.sum([gg for _, gg in ref], axis=0)
+    scale = sum(np.abs(Gs[k]).sum() * np.abs(G.apply(th, R[k])).max() for k in range(3))
+    assert abs(obj - obj_ref) <= Z_TOL * scale
+    assert np.linalg.norm(g - g_ref) <= G_TOL * np.linalg.norm(g_ref)
+    np.testing.assert_array_equal(net.get_params(), th)     # lr = 0: no step
+
+
 def test_trained_network_beats_plain_cg(surface):
     """Train on pairs from plain CG solves on the mesh, then solve a held-out right-hand
     side: flexible CG with the trained network needs far fewer iterations than plain CG
