@@ -209,9 +209,17 @@ def main():
     ap.add_argument("--no-extras", action="store_true")
     ap.add_argument("--no-solve", action="store_true", help="skip the Solve timings on the icosphere level-6 mesh")
     ap.add_argument("--no-graph", action="store_true", help="time direct launches instead of a captured CUDA graph")
-    ap.add_argument("--flow-max-iter", type=int, default=3000, help="iteration limit of the full-flow Solve")
+    ap.add_argument("--flow-max-iter", type=int, default=15000, help="iteration limit of the full-flow Solve")
     ap.add_argument("--flow", action="store_true",
                     help="only the full flow step on two linked tori (1,228,800 triangles) with an obstacle")
+    ap.add_argument("--learned", action="store_true",
+                    help="only configuration 4: train the learned preconditioner on seeded icospheres of levels 5-7 "
+                         "and evaluate it on held-out meshes")
+    ap.add_argument("--learned-train", type=int, default=256, help="training meshes (configuration 4: 256)")
+    ap.add_argument("--learned-rhs", type=int, default=8, help="right-hand sides per training mesh (8)")
+    ap.add_argument("--learned-heldout", type=int, default=32, help="held-out meshes (32)")
+    ap.add_argument("--learned-steps", type=int, default=30, help="unrolled CG iterations of the training loss")
+    ap.add_argument("--learned-lr", type=float, default=1e-3, help="Adam learning rate")
     ap.add_argument("--sharded", action="store_true",
                     help="strong scaling: one mesh (the two linked tori) row-sharded over the ranks, one NCCL "
                          "all-reduce of the derivative buffers per evaluation")
@@ -221,6 +229,8 @@ def main():
         return run_reference(args)
     if args.flow:
         return run_flow(args)
+    if args.learned:
+        return run_learned(args)
     if args.sharded:
         return run_sharded(args)
 
@@ -422,39 +432,132 @@ def extras(rpb, torch, with_solve):
     return out
 
 
-def solve_extras(rpb, M, tpm, V):
-    """Solve to 1e-6 relative residual on the icosphere level-6 mesh: plain CG, CG with the
-    reference preconditioner, and flexible CG with the learned preconditioner trained on
-    the GPU (pairs from plain solves on seeded icospheres of levels 4 and 5; training
-    time reported separately). The reference preconditioner's H1 factorization (host
-    Cholesky and upload, cached until the geometry changes) is timed apart as setup_ms;
-    its ms is the Solve with the factor in place."""
+def train_learned_small(rpb, tpm, epochs=3, steps=30, lr=1e-3):
+    """The learned preconditioner trained on GPU for the default extras and the flow:
+    six seeded spherical-harmonic icospheres (levels 4 and 5, seeds 3001-3006), two N(0,1)
+    right-hand sides each, `epochs` passes of the unrolled-CG energy loss over `steps`
+    preconditioned CG iterations (repulsor_b200.learned.train_unrolled), starting from the
+    multilevel operator (output layer zero: every gain 1). Returns (net, prior, info)."""
     from repulsor_b200 import meshes
-    from repulsor_b200.learned import LearnedPreconditioner, train, training_pairs
+    from repulsor_b200.learned import NPARAM_OUTPUT_OFFSET, LearnedPreconditioner, train_unrolled
 
     t0 = time.perf_counter()
-    data = []
-    for lvl, seed in ((4, 2001), (5, 2002)):
+    samples = []
+    for lvl, seed in ((4, 3001), (4, 3002), (5, 3003), (5, 3004), (4, 3005), (5, 3006)):
         Vt, St = meshes.icosphere_sh(level=lvl, seed=seed)
         Mt = rpb.SimplicialMesh(Vt, St)
-        R, E = training_pairs(Mt, tpm, n_rhs=4, checkpoints=(0, 4, 16, 48, 128), seed=seed, exact_tol=1e-9)
-        data.append((Mt, R, E))
+        for j in range(2):
+            samples.append((Mt, meshes.random_rhs(Vt.shape[0], seed=10 * seed + j, project=True)))
     t1 = time.perf_counter()
     net = LearnedPreconditioner(seed=1)
-    hist = train(net, tpm, data, epochs=30, lr=1e-3, batch=4, seed=0)
+    th = net.get_params()
+    th[NPARAM_OUTPUT_OFFSET:] = 0.0
+    net.set_params(th)
+    prior = LearnedPreconditioner(params=th.copy())
+    hist = train_unrolled(net, tpm, samples, epochs=epochs, lr=lr, steps=steps, seed=0)
     t2 = time.perf_counter()
+    info = {"meshes": "icosphere_sh levels 4 and 5 (seeds 3001-3006), 2 RHS each", "samples": len(samples),
+            "loss": "unrolled CG energy -sum log(-phi(x_K)), K = %d" % steps, "epochs": epochs,
+            "mesh_setup_s": t1 - t0, "training_s": t2 - t1, "loss_first_epoch": hist[0], "loss_last_epoch": hist[-1]}
+    return net, prior, info
+
+
+def run_learned(args):
+    """Configuration 4: the learned preconditioner trained on seeded icospheres of levels
+    5, 6 and 7 (spherical-harmonic displacement, 20,480-327,680 triangles) with
+    args.learned_rhs N(0,1) right-hand sides each, by the unrolled-CG energy loss, and
+    evaluated on args.learned_heldout held-out meshes (the same family, other seeds) by
+    iterations and ms to the 1e-6 true residual: flexible CG with the trained network,
+    the same with the untrained multilevel operator (every gain 1), plain CG, and CG with
+    the reference preconditioner (its H1 factorization timed apart). Training time is
+    reported separately. One JSON line."""
+    import numpy as np
+    import torch
+
+    import repulsor_b200 as rpb
+    from repulsor_b200 import meshes
+    from repulsor_b200.learned import NPARAM_OUTPUT_OFFSET, LearnedPreconditioner, train_unrolled
+
+    torch.cuda.set_device(0)
+    tpm = rpb.TangentPointMetric0(Q, P)
+    levels = (5, 6, 7)
+    net = LearnedPreconditioner(seed=1)
+    th = net.get_params()
+    th[NPARAM_OUTPUT_OFFSET:] = 0.0
+    net.set_params(th)
+    prior = LearnedPreconditioner(params=th.copy())
+    t0 = time.perf_counter()
+    setup_s, losses = 0.0, []
+    for i in range(args.learned_train):
+        ts = time.perf_counter()
+        V, S = meshes.icosphere_sh(level=levels[i % 3], seed=5000 + i)
+        M = rpb.SimplicialMesh(V, S)
+        samples = [(M, meshes.random_rhs(V.shape[0], seed=100 * (5000 + i) + j)) for j in range(args.learned_rhs)]
+        setup_s += time.perf_counter() - ts
+        losses += train_unrolled(net, tpm, samples, epochs=1, lr=args.learned_lr, steps=args.learned_steps, seed=i)
+        del M, samples
+    train_s = time.perf_counter() - t0 - setup_s
+    rows = []
+    for j in range(args.learned_heldout):
+        V, S = meshes.icosphere_sh(level=levels[j % 3], seed=9000 + j)
+        M = rpb.SimplicialMesh(V, S)
+        b = meshes.random_rhs(V.shape[0], seed=9000 + j)
+        row = {"level": levels[j % 3], "seed": 9000 + j}
+        for name, pc, n in (("plain_cg", rpb.PRECOND_NONE, None), ("untrained_fcg", rpb.PRECOND_LEARNED, prior),
+                            ("trained_fcg", rpb.PRECOND_LEARNED, net), ("reference_cg", rpb.PRECOND_REFERENCE, None)):
+            if n is not None:
+                n.attach(M)
+            if pc == rpb.PRECOND_REFERENCE:
+                t = time.perf_counter()
+                tpm.MultiplyPreconditioner(M, 1.0, b)
+                row["reference_setup_ms"] = 1e3 * (time.perf_counter() - t)
+            torch.cuda.synchronize()
+            t = time.perf_counter()
+            tpm.Solve(M, 1.0, b, max_iter=40000, tolerance=1e-6, precond=pc, strict=False)
+            ms = 1e3 * (time.perf_counter() - t)
+            rr = max(float(x) for x in tpm.Solver_RelativeResiduals())
+            row[name] = {"iterations": tpm.Solver_IterationCount(), "ms": ms, "rel_residual": rr,
+                         "fallback_iteration": tpm.SolveInfo(M)["fallback_iteration"]}
+        rows.append(row)
+        del M
+
+    def mean(name, key, lvl=None):
+        v = [r[name][key] for r in rows if lvl is None or r["level"] == lvl]
+        return float(np.mean(v)) if v else None
+
+    summary = {name: {"iterations": mean(name, "iterations"), "ms": mean(name, "ms"),
+                      "per_level": {lvl: {"iterations": mean(name, "iterations", lvl), "ms": mean(name, "ms", lvl)}
+                                    for lvl in levels}}
+               for name in ("plain_cg", "untrained_fcg", "trained_fcg", "reference_cg")}
+    out = {"metric": "learned preconditioner: held-out solve iterations and ms to 1e-6 true residual", "unit": "ms",
+           "workload": f"icosphere_sh levels 5-7: {args.learned_train} training meshes x {args.learned_rhs} RHS "
+                       f"(seeds 5000+), {args.learned_heldout} held-out meshes (seeds 9000+), q=6 p=12 theta=0.5",
+           "training": {"loss": f"unrolled CG energy, K = {args.learned_steps} iterations", "lr": args.learned_lr,
+                        "samples": args.learned_train * args.learned_rhs, "training_s": train_s,
+                        "mesh_setup_s": setup_s, "loss_first_mesh": float(np.mean(losses[:args.learned_rhs])),
+                        "loss_last_mesh": float(np.mean(losses[-args.learned_rhs:]))},
+           "summary": summary, "all_converged": all(r[n]["rel_residual"] <= 1e-6 for r in rows
+                                                   for n in ("plain_cg", "untrained_fcg", "trained_fcg",
+                                                             "reference_cg")),
+           "held_out": rows}
+    print(json.dumps(out))
+    return 0
+
+
+def solve_extras(rpb, M, tpm, V):
+    """Solve to 1e-6 relative residual on the icosphere level-6 mesh: plain CG, CG with the
+    reference preconditioner, and flexible CG with the multilevel operator before and after
+    training (train_learned_small: unrolled-CG energy loss on GPU, training time reported
+    separately). The reference preconditioner's H1 factorization (host Cholesky and upload,
+    cached until the geometry changes) is timed apart as setup_ms; its ms is the Solve with
+    the factor in place."""
+    from repulsor_b200 import meshes
+
+    net, prior, training = train_learned_small(rpb, tpm)
     B = meshes.random_rhs(V.shape[0], seed=1003)
     res = {"workload": "icosphere level 6 (40,962 vertices), RHS N(0,1) projected off translations, tol 1e-6 "
                        "(true residual of the plain metric operator)",
-           "training": {"meshes": "icosphere_sh levels 4 and 5 (seeds 2001, 2002), 4 RHS each, CG checkpoints "
-                                  "0/4/16/48/128", "pairs": int(sum(d[1].shape[0] for d in data)),
-                        "pair_generation_s": t1 - t0, "training_s": t2 - t1, "epochs": len(hist),
-                        "loss_first_epoch": hist[0], "loss_last_epoch": hist[-1]}}
-    from repulsor_b200.learned import NPARAM_OUTPUT_OFFSET
-    prior = LearnedPreconditioner(seed=1)
-    p0 = prior.get_params()
-    p0[NPARAM_OUTPUT_OFFSET:] = 0.0          # output layer zero: every gain 1 (the untrained multilevel operator)
-    prior.set_params(p0)
+           "training": training}
     for name, pc, max_iter in (("plain_cg", rpb.PRECOND_NONE, 20000),
                                ("multilevel_prior_fcg", rpb.PRECOND_LEARNED, 20000),
                                ("learned_fcg", rpb.PRECOND_LEARNED, 20000),
@@ -496,7 +599,6 @@ def run_flow(args):
 
     import repulsor_b200 as rpb
     from repulsor_b200 import meshes
-    from repulsor_b200.learned import LearnedPreconditioner, train, training_pairs
 
     torch.cuda.set_device(0)
     out = {"metric": "full flow step (energy+grad, learned FCG solve to 1e-6)", "unit": "s",
@@ -521,16 +623,8 @@ def run_flow(args):
         E += tpo.Differential(M, 1.0, 1.0, D)
         out["energy_grad_s"] = time.perf_counter() - t
     out["energy"] = E
-    t = time.perf_counter()
-    data = []
-    for lvl, seed in ((4, 2001), (5, 2002)):
-        Vt, St = meshes.icosphere_sh(level=lvl, seed=seed)
-        Mt = rpb.SimplicialMesh(Vt, St)
-        R, Er = training_pairs(Mt, tpm, n_rhs=4, checkpoints=(0, 4, 16, 48, 128), seed=seed, exact_tol=1e-9)
-        data.append((Mt, R, Er))
-    net = LearnedPreconditioner(seed=1)
-    train(net, tpm, data, epochs=30, lr=1e-3, batch=4, seed=0)
-    out["training_s"] = time.perf_counter() - t
+    net, _, training = train_learned_small(rpb, tpm)
+    out["training"] = training
     net.attach(M)
     B = D - D.mean(0)
     t = time.perf_counter()

@@ -204,27 +204,32 @@ def _cdot(a, b):
     return np.einsum("ij,ij->j", a, b)
 
 
-def unrolled_sensitivities(net, M, metric, b, steps=30):
+def unrolled_sensitivities(net, M, metric, b, steps=30, loss="energy"):
     """The loss of `steps` iterations of preconditioned CG with z = M(r) from x = 0, one CG
-    per column: L = sum_c log(|r_K,c|^2 / |b_c|^2), and its sensitivities to the
-    preconditioner outputs, dL/dz_k, by the adjoint of the CG recurrences
+    per column, and its sensitivities to the preconditioner outputs, dL/dz_k, by the adjoint
+    of the CG recurrences
 
-        q_k = A p_k,  alpha_k = g_k / (p_k . q_k),  r_k+1 = r_k - alpha_k q_k,
+        q_k = A p_k,  alpha_k = g_k / (p_k . q_k),  x_k+1 = x_k + alpha_k p_k,  r_k+1 = r_k - alpha_k q_k,
         z_k+1 = M(r_k+1),  g_k+1 = r_k+1 . z_k+1,  beta_k = g_k+1 / g_k,  p_k+1 = z_k+1 + beta_k p_k,
 
     run backwards; through z = M(r) the adjoint takes the application with the gains of
-    that r held fixed (apply_pair). Returns (L, R, G): the residuals r_0 .. r_K-1 the
-    preconditioner was applied to and the sensitivities dL/dz_k, for train_step_sens."""
+    that r held fixed (apply_pair). loss = "energy": L = -sum_c log(-phi_c(x_K)) with
+    phi(x) = x.Ax/2 - b.x = -x.(b + r)/2, the functional CG minimizes (phi(x_K) - phi(x*) is
+    half the squared A-norm of the error); loss = "residual": L = sum_c log(|r_K,c|^2 / |b_c|^2).
+    Returns (L, R, G): the residuals r_0 .. r_K-1 the preconditioner was applied to and the
+    sensitivities dL/dz_k, for train_step_sens."""
     b = np.ascontiguousarray(b, dtype=np.float64)
     A = lambda X: metric.MultiplyMetric(M, 1.0, X)
     r, z, p, q = [b], [net.apply(M, b)], [], []
     p.append(z[0])
     g = [_cdot(r[0], z[0])]
     alpha, beta, delta = [], [], []
+    x = np.zeros_like(b)
     for k in range(steps):
         qk = A(p[k])
         dk = _cdot(p[k], qk)
         ak = g[k] / dk
+        x = x + ak * p[k]
         rk1 = r[k] - ak * qk
         q.append(qk); delta.append(dk); alpha.append(ak); r.append(rk1)
         if k + 1 < steps:
@@ -233,9 +238,18 @@ def unrolled_sensitivities(net, M, metric, b, steps=30):
             bk = gk1 / g[k]
             z.append(zk1); g.append(gk1); beta.append(bk)
             p.append(zk1 + bk * p[k])
-    nb2, nr2 = _cdot(b, b), _cdot(r[steps], r[steps])
-    loss = float(np.sum(np.log(nr2 / nb2)))
-    rbar = 2.0 * r[steps] / nr2
+    if loss == "energy":
+        phi = -0.5 * _cdot(x, b + r[steps])
+        value = float(-np.sum(np.log(-phi)))
+        xbar = r[steps] / phi                 # dL/dphi = -1/phi, dphi/dx = A x - b = -r
+        rbar = np.zeros_like(b)
+    elif loss == "residual":
+        nb2, nr2 = _cdot(b, b), _cdot(r[steps], r[steps])
+        value = float(np.sum(np.log(nr2 / nb2)))
+        xbar = np.zeros_like(b)
+        rbar = 2.0 * r[steps] / nr2
+    else:
+        raise ValueError("loss must be 'energy' or 'residual'")
     zbar = [np.zeros_like(b) for _ in range(steps)]
     pbar_next = np.zeros_like(b)
     for k in reversed(range(steps)):
@@ -253,9 +267,11 @@ def unrolled_sensitivities(net, M, metric, b, steps=30):
             _, mz = net.apply_pair(M, r[k + 1], zbar[k + 1])
             rbar = rbar + mz
         else:
-            gbar_k = np.zeros(3)
-        # r_k+1 = r_k - alpha_k q_k; alpha_k = g_k / delta_k; delta_k = p_k . q_k; q_k = A p_k
-        abar = -_cdot(rbar, q[k])
+            gbar_k = np.zeros(b.shape[1])
+        # x_k+1 = x_k + alpha_k p_k; r_k+1 = r_k - alpha_k q_k; alpha_k = g_k / delta_k;
+        # delta_k = p_k . q_k; q_k = A p_k
+        abar = _cdot(xbar, p[k]) - _cdot(rbar, q[k])
+        pbar += alpha[k] * xbar
         qbar = -alpha[k] * rbar
         gbar_k = gbar_k + abar / delta[k]
         dbar = -abar * g[k] / delta[k] ** 2
@@ -267,10 +283,10 @@ def unrolled_sensitivities(net, M, metric, b, steps=30):
         zbar[k] += gbar_k * r[k]
         pbar_next = pbar
     zbar[0] += pbar_next            # p_0 = z_0
-    return loss, np.stack(r[:steps]), np.stack(zbar)
+    return value, np.stack(r[:steps]), np.stack(zbar)
 
 
-def train_unrolled(net, metric, meshes_rhs, epochs=1, lr=1e-3, steps=30, reg=1e-3, seed=0, log=None):
+def train_unrolled(net, metric, meshes_rhs, epochs=1, lr=1e-3, steps=30, reg=1e-3, seed=0, log=None, loss="energy"):
     """Adam on the unrolled-CG loss: for every (mesh, right-hand side) pair in meshes_rhs,
     the sensitivities of `steps` preconditioned CG iterations with the current network,
     then one step on them. Returns the mean loss per epoch (the loss of the network each
@@ -281,9 +297,9 @@ def train_unrolled(net, metric, meshes_rhs, epochs=1, lr=1e-3, steps=30, reg=1e-
         losses = []
         for i in rng.permutation(len(meshes_rhs)):
             M, b = meshes_rhs[i]
-            loss, R, G = unrolled_sensitivities(net, M, metric, b, steps)
+            value, R, G = unrolled_sensitivities(net, M, metric, b, steps, loss)
             net.train_step_sens(M, R, G, lr=lr, reg=reg)
-            losses.append(loss)
+            losses.append(value)
         hist.append(float(np.mean(losses)))
         if log is not None:
             log(ep, hist[-1])

@@ -1,8 +1,10 @@
 """The adjoint of the unrolled preconditioned CG (repulsor_b200.learned.unrolled_sensitivities)
 against finite differences, on the CPU with small dense stand-ins for the metric and the
-preconditioner: for a linear preconditioner M_t = M0 + t M1 the derivative of the loss is
+preconditioner, for both losses (the CG energy functional and the residual norm): for a
+linear preconditioner M_t = M0 + t M1 the derivative of the loss is
 dL/dt = sum_k G_k . M1 r_k, where G_k are the returned sensitivities."""
 import numpy as np
+import pytest
 
 from repulsor_b200.learned import unrolled_sensitivities
 
@@ -31,7 +33,8 @@ def _spd(n, rng, cond):
     return (Q * np.geomspace(1.0, cond, n)) @ Q.T
 
 
-def test_unrolled_cg_sensitivities_match_finite_differences():
+@pytest.mark.parametrize("loss", ["energy", "residual"])
+def test_unrolled_cg_sensitivities_match_finite_differences(loss):
     rng = np.random.default_rng(0)
     n = 40
     A = _spd(n, rng, 1e3)
@@ -41,11 +44,11 @@ def test_unrolled_cg_sensitivities_match_finite_differences():
     b = rng.standard_normal((n, 3))
     metric = _Metric(A)
     for steps in (1, 5, 12):
-        loss, R, G = unrolled_sensitivities(_Dense(M0), None, metric, b, steps)
+        value, R, G = unrolled_sensitivities(_Dense(M0), None, metric, b, steps, loss)
         assert R.shape == (steps, n, 3) and G.shape == (steps, n, 3)
         analytic = float(sum(np.sum(G[k] * (M1 @ R[k])) for k in range(steps)))
         h = 1e-4      # smaller steps lose digits to the rounding CG amplifies
-        lp, _, _ = unrolled_sensitivities(_Dense(M0 + h * M1), None, metric, b, steps)
-        lm, _, _ = unrolled_sensitivities(_Dense(M0 - h * M1), None, metric, b, steps)
+        lp, _, _ = unrolled_sensitivities(_Dense(M0 + h * M1), None, metric, b, steps, loss)
+        lm, _, _ = unrolled_sensitivities(_Dense(M0 - h * M1), None, metric, b, steps, loss)
         fd = (lp - lm) / (2 * h)
         assert abs(analytic - fd) <= 1e-5 * max(1.0, abs(fd)), (steps, analytic, fd)
