@@ -130,13 +130,12 @@ __device__ __forceinline__ void block_exclusive_scan(double (&v)[W], double (&to
     __syncthreads();
 }
 
-// Single-block exclusive scan of `n` rows of W doubles (block sums), in place; row n
-// receives the grand total.
+// Exclusive scan of `n` rows of W doubles (block sums) by one block, in place; row n
+// receives the grand total. The rows are read through L2 (they may have been written by
+// other blocks of the same launch).
 template <int W>
-__global__ void k_scan_rows(double* rows, int n)
+__device__ __forceinline__ void scan_rows_block(double* rows, int n)
 {
-    pdl_wait();
-    pdl_launch_dependents();
     __shared__ double carry[W];
     if (threadIdx.x < W) carry[threadIdx.x] = 0.0;
     __syncthreads();
@@ -144,7 +143,7 @@ __global__ void k_scan_rows(double* rows, int n)
         const int i = base + threadIdx.x;
         double v[W], tot[W];
 #pragma unroll
-        for (int k = 0; k < W; ++k) v[k] = (i < n) ? rows[static_cast<int64_t>(W) * i + k] : 0.0;
+        for (int k = 0; k < W; ++k) v[k] = (i < n) ? __ldcg(rows + static_cast<int64_t>(W) * i + k) : 0.0;
         block_exclusive_scan<W>(v, tot);
         if (i < n) {
 #pragma unroll
@@ -155,6 +154,31 @@ __global__ void k_scan_rows(double* rows, int n)
         __syncthreads();
     }
     if (threadIdx.x < W) rows[static_cast<int64_t>(W) * n + threadIdx.x] = carry[threadIdx.x];
+}
+
+template <int W>
+__global__ void k_scan_rows(double* rows, int n)
+{
+    pdl_wait();
+    pdl_launch_dependents();
+    scan_rows_block<W>(rows, n);
+}
+
+// The last of a launch's `n` blocks to arrive (counter: zero before the launch, zero again
+// after it) scans the rows of W block sums the blocks wrote before arriving. The counter
+// only counts; no block waits for another.
+template <int W>
+__device__ __forceinline__ void last_block_scans_rows(double* rows, int n, unsigned* counter)
+{
+    __shared__ bool last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(counter, 1u) == static_cast<unsigned>(n) - 1;
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    scan_rows_block<W>(rows, n);
+    if (threadIdx.x == 0) *counter = 0u;
 }
 
 // Range sums over clusters of a per-primitive W-vector: in-block scans, block scan
@@ -204,6 +228,8 @@ struct GeomArgs {
     double* C_mom;            // NC x 10 (a, centre, P) in FP64, or null (not written)
     double* local;            // N x 10: exclusive in-block prefix of the moments (a, a c, a P)
     double* blocks;           // (nblocks + 1) x 10: block sums -> exclusive block prefix
+    unsigned* scan_done;      // last-block counter: the last geometry block scans `blocks`
+                              // (null: a separate k_scan_rows launch does)
 };
 
 __device__ __forceinline__ void store_cluster(ClusterDatum* base, int i, const double* mom)
@@ -217,7 +243,8 @@ __device__ __forceinline__ void store_cluster(ClusterDatum* base, int i, const d
 }
 
 // Simplex data in tree order (SimplexDataKernel::ReadSimplex/WriteFar) and the in-block
-// prefix sums of the additive moments (a, a c, a P).
+// prefix sums of the additive moments (a, a c, a P); with scan_done, the last block also
+// turns the block sums into their exclusive prefix.
 static __global__ void __launch_bounds__(SCAN_BLOCK) k_geometry_prims(GeomArgs g)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -244,6 +271,7 @@ static __global__ void __launch_bounds__(SCAN_BLOCK) k_geometry_prims(GeomArgs g
     if (i < g.N)
         for (int k = 0; k < 10; ++k) g.local[10 * static_cast<int64_t>(i) + k] = mom[k];
     if (threadIdx.x < 10) g.blocks[10 * static_cast<int64_t>(blockIdx.x) + threadIdx.x] = tot[threadIdx.x];
+    if (g.scan_done) last_block_scans_rows<10>(g.blocks, gridDim.x, g.scan_done);
 }
 
 // ClusterTree moments (ComputeClusterData_Thread.hpp:50-129): a cluster's moments are
@@ -456,11 +484,12 @@ constexpr int NEAR_TILE_UNION = 960;
 constexpr int FAR_TILE_UNION = 1536;
 
 // One lane's share of a row: the row's entries k = k0 + sub, k0 + sub + stride, ... with the
-// column handle u = index(k) and the column datum from datum(u, j, Y) (j: the column's
-// tree position). The next entry's handle (PREFETCH: and its datum) is requested before
-// the current pair is evaluated. A row accumulates only its own derivative; each
-// unordered pair contributes its energy once (from the row with the smaller index),
-// CROSS pairs always.
+// column handle u = index(k) and the column datum from datum(u, Y). The next entry's handle
+// (PREFETCH: and its datum) is requested before the current pair is evaluated. A row
+// accumulates only its own derivative and the energy of every pair it holds: a symmetric
+// pattern holds each unordered pair twice (the pair energy is symmetric in its two
+// primitives or clusters), a CROSS pattern once with the symmetry factor 1/2, so the
+// epilogue halves the energy in both cases.
 // A close near-field pair evaluated in FP64: energy and the ten derivative components.
 // Out of line and with its operands passed by value, so that its FP64 temporaries do not
 // count against the registers of the FP32 pair loop that calls it (rarely).
@@ -504,18 +533,15 @@ __device__ __forceinline__ void pair_row(const PairArgs& A, const Datum& X, int 
     const int64_t k0 = A.rp[i], k1 = A.rp[i + 1];
     int64_t k = k0 + sub;
     int un = (k < k1) ? index(k) : 0;
-    int jn = 0;
     ColDatum Yn;
-    if (PREFETCH && k < k1) datum(un, jn, Yn);
+    if (PREFETCH && k < k1) datum(un, Yn);
     for (; k < k1; k += stride) {
-        int j;
         ColDatum Y;
         if constexpr (PREFETCH) {
-            j = jn;
             Y = Yn;
-            if (k + stride < k1) datum(index(k + stride), jn, Yn);
+            if (k + stride < k1) datum(index(k + stride), Yn);
         } else {
-            datum(un, j, Y);
+            datum(un, Y);
             if (k + stride < k1) un = index(k + stride);
         }
         Proj<float> g;
@@ -527,10 +553,12 @@ __device__ __forceinline__ void pair_row(const PairArgs& A, const Datum& X, int 
             close = g.r2 < dd * dd;
         }
         if (close) {
-            // close near-field pair: the same kernel in FP64, added straight into FP64
+            // close near-field pair: the same kernel in FP64, added straight into FP64 (the
+            // row datum is read again, so that its weight need not stay in registers)
             if constexpr (!FAR) {
-                const Close64 c = close_pair_fp64<QH, PH, DIFF>(A.ex, A.dom, X, Y);
-                if (CROSS || j > i) e_row += c.e;
+                const Close64 c =
+                    close_pair_fp64<QH, PH, DIFF>(A.ex, A.dom, load_datum(static_cast<const Datum*>(A.data), i), Y);
+                e_row += c.e;
                 if (DIFF) {
 #pragma unroll
                     for (int m = 0; m < 10; ++m) add64(m, c.d[m]);
@@ -538,7 +566,7 @@ __device__ __forceinline__ void pair_row(const PairArgs& A, const Datum& X, int 
             }
         } else {
             const float e = tp0_core<float, QH, PH, DIFF>(A.ex, g, ax, weight_f(Y), acc);
-            if (CROSS || j > i) e32 += e;
+            e32 += e;
             if (++since_flush == PAIR_FLUSH) {
                 since_flush = 0;
                 e_row += e32;
@@ -567,31 +595,32 @@ __device__ __forceinline__ void pair_row(const PairArgs& A, const Datum& X, int 
     }
 }
 
-// Combines the partial sums of a row's lane group (size lanes, aligned: an xor butterfly
-// over offsets below the warp's largest group, every lane of the warp takes part, a lane
-// adds only offsets inside its group), writes the row's derivative, and reduces the
-// energy deterministically: one partial per block, the last block to finish sums the
-// partials in block order.
+// Combines the partial sums of a row's lane group (size consecutive lanes of one warp, sub
+// the lane's place in it) into the group's first lane by a fixed tree — at offset off the
+// lanes whose sub is a multiple of 2 off add the partial of lane sub + off when it is in the
+// group; every lane of the warp takes part in the shuffles —, writes the row's derivative,
+// and reduces the energy deterministically: one partial per block, the last block to
+// finish sums the partials in block order.
 // bid / nblocks: this block's index among the launch's blocks for this pattern (the
 // block energies are summed in that order by the last of them)
 template <bool DIFF, bool CROSS>
 __device__ __forceinline__ void pair_epilogue(const PairArgs& A, bool active, int i, int sub, int size, int warp_size_max,
                                               double e_row, double (&D64)[10], int bid, int nblocks)
 {
+    e_row *= 0.5;
     if constexpr (CROSS) {
-        e_row *= 0.5;
 #pragma unroll
         for (int m = 0; m < 10; ++m) D64[m] *= 0.5;
     }
     for (int off = 1; off < warp_size_max; off <<= 1) {
-        const bool in = off < size;
-        const double e = __shfl_xor_sync(0xffffffffu, e_row, off);
-        if (in) e_row += e;
+        const bool take = (sub & (2 * off - 1)) == 0 && sub + off < size;
+        const double e = __shfl_down_sync(0xffffffffu, e_row, off);
+        if (take) e_row += e;
         if (DIFF) {
 #pragma unroll
             for (int m = 0; m < 10; ++m) {
-                const double d = __shfl_xor_sync(0xffffffffu, D64[m], off);
-                if (in) D64[m] += d;
+                const double d = __shfl_down_sync(0xffffffffu, D64[m], off);
+                if (take) D64[m] += d;
             }
         }
     }
@@ -655,10 +684,7 @@ __global__ void __launch_bounds__(PAIR_BLOCK) k_tp0_pairs(PairArgs A)
         i = A.order ? A.order[slot] : slot;
         const Datum X = load_datum(base, i);
         auto index = [&](int64_t k) { return __ldg(A.ci + k); };
-        auto datum = [&](int u, int& j, Datum& Y) {
-            j = u;
-            Y = load_datum(cols, u);
-        };
+        auto datum = [&](int u, Datum& Y) { Y = load_datum(cols, u); };
         pair_row<FAR, QH, PH, DIFF, CROSS, true, false, Datum>(A, X, i, sub, LANES, index, datum, e_row, D64, nullptr);
     }
     pair_epilogue<DIFF, CROSS>(A, active, i, sub, LANES, LANES, e_row, D64, blockIdx.x, gridDim.x);
@@ -699,13 +725,13 @@ __device__ __forceinline__ ClusterDatum load_cluster_rot(const float4* sdat, int
 }
 
 // dynamic shared memory per tile of union size n: the data (PrimTile 80 bytes, ClusterDatum
-// 64 bytes), then the column ids
+// 64 bytes)
 __host__ __device__ constexpr size_t pair_tile_union_bytes(int n, bool far)
 {
-    return (static_cast<size_t>(n) * ((far ? sizeof(ClusterDatum) : sizeof(PrimTile)) + sizeof(int)) + 15) / 16 * 16;
+    return (static_cast<size_t>(n) * (far ? sizeof(ClusterDatum) : sizeof(PrimTile)) + 15) / 16 * 16;
 }
 
-// union + column ids; near tiles also the FP64 derivative accumulators of every thread
+// union; near tiles also the FP64 derivative accumulators of every thread
 __host__ __device__ constexpr size_t pair_tile_smem(int n, bool far)
 {
     return pair_tile_union_bytes(n, far) + (far ? 0 : sizeof(double) * 10 * PAIR_TILE_THREADS);
@@ -721,15 +747,12 @@ __device__ __forceinline__ void pairs_tiled_body(const PairArgs& A, const PairTi
     const int b = T.tile_base + bid;
     const int u0 = T.cols_rp[b], un = T.cols_rp[b + 1] - u0;
     float4* sdat = tile_smem;
-    int* sid = reinterpret_cast<int*>(reinterpret_cast<char*>(tile_smem) + sizeof(ColDatum) * static_cast<size_t>(un));
-    // the tile's pattern first; the primitive / cluster data once the producer has finished
-    for (int u = threadIdx.x; u < un; u += blockDim.x) sid[u] = __ldg(T.cols + u0 + u);
+    // the tile's lane map first; the primitive / cluster data once the producer has finished
     const int r0 = T.row0[b];
     const int lm = __ldg(T.lane_map + static_cast<int64_t>(b) * PAIR_TILE_THREADS + threadIdx.x);
     const bool active = lm >= 0;
-    const int sub = active ? (lm & 31) : 0, size = active ? (1 << ((lm >> 5) & 7)) : 1;
-    const int warp_size_max = __reduce_max_sync(0xffffffffu, size);
-    const int i = active ? T.order[r0 + (lm >> 8)] : 0;
+    const int sub = active ? (lm & 31) : 0, size = active ? ((lm >> 5) & 31) + 1 : 1;
+    const int i = active ? T.order[r0 + (lm >> 10)] : 0;
     pdl_wait();
     pdl_launch_dependents();
     if constexpr (FAR) {
@@ -772,15 +795,14 @@ __device__ __forceinline__ void pairs_tiled_body(const PairArgs& A, const PairTi
     }
     if (active) {
         auto index = [&](int64_t k) { return static_cast<int>(__ldg(T.slot + k)); };
-        auto datum = [&](int u, int& j, ColDatum& Y) {
+        auto datum = [&](int u, ColDatum& Y) {
             if constexpr (FAR) Y = load_cluster_rot(sdat, u);
             else Y = reinterpret_cast<const PrimTile*>(tile_smem)[u];
-            j = sid[u];
         };
         pair_row<FAR, QH, PH, DIFF, false, false, !FAR && DIFF, ColDatum>(A, X, i, sub, size, index, datum, e_row, D64,
                                                                         Dsm);
     }
-    pair_epilogue<DIFF, false>(A, active, i, sub, size, warp_size_max, e_row, D64, bid, nblocks);
+    pair_epilogue<DIFF, false>(A, active, i, sub, size, __reduce_max_sync(0xffffffffu, size), e_row, D64, bid, nblocks);
 }
 
 template <bool FAR, int QH, int PH, bool DIFF>
@@ -854,44 +876,70 @@ struct CollectArgs {
     double* B;                 // N x (dom+1) x 3, original simplex order
 };
 
+// COLLECT_LANES consecutive lanes per primitive. The far-field part is split over the
+// lanes: lane p visits the ancestors at distances p, p + 4, p + 8, ... from the leaf (the
+// up4 jump pointers), so that a primitive's dependent loads run on four lanes at once; the
+// partial sums are combined by an xor butterfly (every lane ends with the same totals, since
+// a + b == b + a), and lane c < dom + 1 then forms corner c's derivative.
+constexpr int COLLECT_LANES = 4;
+
 static __global__ void k_collect_chain(CollectArgs A)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= A.N) return;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = t / COLLECT_LANES, lane = t % COLLECT_LANES;
+    const bool active = i < A.N;
     const int size = A.dom + 1;
-    const int j = A.perm[i];
+    int j = 0;
     SimplexGeom g;
     // the coordinates were written before the pair kernels that precede this launch
-    simplex_geometry(A.dom, A.V, A.S + static_cast<int64_t>(size) * j, A.charge_v, g);
+    if (active) {
+        j = A.perm[i];
+        simplex_geometry(A.dom, A.V, A.S + static_cast<int64_t>(size) * j, A.charge_v, g);
+    }
     pdl_wait();
     pdl_launch_dependents();
 
-    // near field (centred at the primitive barycentre)
-    const double* dn = A.D_near + 10 * static_cast<int64_t>(i);
-    double alpha = dn[0];
-    double gx[3] = {dn[1], dn[2], dn[3]};
-    double G6[6];
-    for (int k = 0; k < 6; ++k) G6[k] = dn[4 + k];
-    // far field: percolate down = sum over all ancestors of the leaf
-    ancestor_walk(A.leaf_of[i], A.C_parent, A.C_up4, [&](int C) {
-        const double* df = A.D_far + 10 * static_cast<int64_t>(C);
-        const ClusterDatum cd = load_datum(A.C_pair, C);
-        const double dx0 = df[1], dx1 = df[2], dx2 = df[3];
-        alpha += df[0] + dx0 * (g.c[0] - cd.c[0]) + dx1 * (g.c[1] - cd.c[1]) + dx2 * (g.c[2] - cd.c[2]);
-        gx[0] += dx0; gx[1] += dx1; gx[2] += dx2;
-        for (int k = 0; k < 6; ++k) G6[k] += df[4 + k];
-    });
-    double hull_extra[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-    if (A.D_vf) {
-        const double* dv = A.D_vf + 16 * static_cast<int64_t>(i);
-        alpha += dv[0];
-        for (int c = 0; c < size; ++c)
-            for (int k = 0; k < 3; ++k) {
-                alpha += dv[1 + 3 * c + k] * g.h[c][k];
-                hull_extra[c][k] = dv[1 + 3 * c + k];
+    double alpha = 0.0, gx[3] = {0, 0, 0}, G6[6] = {0, 0, 0, 0, 0, 0};
+    if (active) {
+        if (lane == 0) {
+            // near field (centred at the primitive barycentre)
+            const double* dn = A.D_near + 10 * static_cast<int64_t>(i);
+            alpha = dn[0];
+            for (int k = 0; k < 3; ++k) gx[k] = dn[1 + k];
+            for (int k = 0; k < 6; ++k) G6[k] = dn[4 + k];
+            if (A.D_vf) {
+                const double* dv = A.D_vf + 16 * static_cast<int64_t>(i);
+                alpha += dv[0];
+                for (int c = 0; c < size; ++c)
+                    for (int k = 0; k < 3; ++k) alpha += dv[1 + 3 * c + k] * g.h[c][k];
+                for (int k = 0; k < 6; ++k) G6[k] += dv[1 + 3 * size + k];
             }
-        for (int k = 0; k < 6; ++k) G6[k] += dv[1 + 3 * size + k];
+        }
+        // far field: percolate down = sum over all ancestors of the leaf, four levels apart
+        int C = A.leaf_of[i];
+        for (int k = 0; k < lane && C >= 0; ++k) C = __ldg(A.C_parent + C);
+        for (; C >= 0; C = __ldg(A.C_up4 + C)) {
+            const double* df = A.D_far + 10 * static_cast<int64_t>(C);
+            const ClusterDatum cd = load_datum(A.C_pair, C);
+            const double dx0 = df[1], dx1 = df[2], dx2 = df[3];
+            alpha += df[0] + dx0 * (g.c[0] - cd.c[0]) + dx1 * (g.c[1] - cd.c[1]) + dx2 * (g.c[2] - cd.c[2]);
+            gx[0] += dx0; gx[1] += dx1; gx[2] += dx2;
+            for (int k = 0; k < 6; ++k) G6[k] += df[4 + k];
+        }
     }
+#pragma unroll
+    for (int off = 1; off < COLLECT_LANES; off <<= 1) {
+        alpha += __shfl_xor_sync(0xffffffffu, alpha, off);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) gx[k] += __shfl_xor_sync(0xffffffffu, gx[k], off);
+#pragma unroll
+        for (int k = 0; k < 6; ++k) G6[k] += __shfl_xor_sync(0xffffffffu, G6[k], off);
+    }
+    if (!active || lane >= size) return;
+    const int c = lane;
+    double hull_extra[3] = {0, 0, 0};
+    if (A.D_vf)
+        for (int k = 0; k < 3; ++k) hull_extra[k] = A.D_vf[16 * static_cast<int64_t>(i) + 1 + 3 * c + k];
     double P6[6];
     projector_packed(A.dom, g.t, P6);
     for (int k = 0; k < 6; ++k) alpha += G6[k] * P6[k];
@@ -902,30 +950,25 @@ static __global__ void k_collect_chain(CollectArgs A)
     double Gt[3];
     for (int a = 0; a < 3; ++a) Gt[a] = G[a][0] * g.t[0] + G[a][1] * g.t[1] + G[a][2] * g.t[2];
     const double tGt = g.t[0] * Gt[0] + g.t[1] * Gt[1] + g.t[2] * Gt[2];
-    double Bc[3][3];
+    double Bc[3];
     if (A.dom == 2) {
         double w[3];
         for (int a = 0; a < 3; ++a) w[a] = 2.0 * (Gt[a] - tGt * g.t[a]) / g.len;
-        for (int c = 0; c < 3; ++c) {
-            const int c1 = (c + 1) % 3, c2 = (c + 2) % 3;
-            const double u[3] = {g.h[c1][0] - g.h[c2][0], g.h[c1][1] - g.h[c2][1], g.h[c1][2] - g.h[c2][2]};
-            const double un[3] = {u[1] * g.t[2] - u[2] * g.t[1], u[2] * g.t[0] - u[0] * g.t[2], u[0] * g.t[1] - u[1] * g.t[0]};
-            const double uw[3] = {u[1] * w[2] - u[2] * w[1], u[2] * w[0] - u[0] * w[2], u[0] * w[1] - u[1] * w[0]};
-            for (int k = 0; k < 3; ++k)
-                Bc[c][k] = g.charge * (alpha * 0.5 * un[k] + g.vol * (gx[k] / 3.0 + hull_extra[c][k]) + g.vol * uw[k]);
-        }
+        const int c1 = (c + 1) % 3, c2 = (c + 2) % 3;
+        const double u[3] = {g.h[c1][0] - g.h[c2][0], g.h[c1][1] - g.h[c2][1], g.h[c1][2] - g.h[c2][2]};
+        const double un[3] = {u[1] * g.t[2] - u[2] * g.t[1], u[2] * g.t[0] - u[0] * g.t[2], u[0] * g.t[1] - u[1] * g.t[0]};
+        const double uw[3] = {u[1] * w[2] - u[2] * w[1], u[2] * w[0] - u[0] * w[2], u[0] * w[1] - u[1] * w[0]};
+        for (int k = 0; k < 3; ++k)
+            Bc[k] = g.charge * (alpha * 0.5 * un[k] + g.vol * (gx[k] / 3.0 + hull_extra[k]) + g.vol * uw[k]);
     } else {
         double gg[3];
         for (int a = 0; a < 3; ++a) gg[a] = -2.0 * (Gt[a] - tGt * g.t[a]) / g.len;
-        for (int c = 0; c < 2; ++c) {
-            const double sgn = (c == 1) ? 1.0 : -1.0;
-            for (int k = 0; k < 3; ++k)
-                Bc[c][k] = g.charge * (alpha * sgn * g.t[k] + g.vol * (gx[k] * 0.5 + hull_extra[c][k]) + g.vol * sgn * gg[k]);
-        }
+        const double sgn = (c == 1) ? 1.0 : -1.0;
+        for (int k = 0; k < 3; ++k)
+            Bc[k] = g.charge * (alpha * sgn * g.t[k] + g.vol * (gx[k] * 0.5 + hull_extra[k]) + g.vol * sgn * gg[k]);
     }
-    double* dst = A.B + static_cast<int64_t>(size) * 3 * j;
-    for (int c = 0; c < size; ++c)
-        for (int k = 0; k < 3; ++k) dst[3 * c + k] = Bc[c][k];
+    double* dst = A.B + static_cast<int64_t>(size) * 3 * j + 3 * c;
+    for (int k = 0; k < 3; ++k) dst[k] = Bc[k];
 }
 
 struct GatherArgs {
@@ -938,19 +981,35 @@ struct GatherArgs {
     int ldY;
 };
 
+// GATHER_LANES consecutive lanes per vertex, each summing every GATHER_LANES-th of the
+// vertex's slots; an xor butterfly combines them and lane k < 3 writes component k.
+constexpr int GATHER_LANES = 4;
+
 static __global__ void k_gather_vertices(GatherArgs A)
 {
-    const int v = blockIdx.x * blockDim.x + threadIdx.x;
-    if (v >= A.nV) return;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int v = t / GATHER_LANES, lane = t % GATHER_LANES;
+    const bool active = v < A.nV;
+    int k0 = 0, k1 = 0;
+    if (active) {
+        k0 = A.v_rp[v];
+        k1 = A.v_rp[v + 1];
+    }
     pdl_wait();
     pdl_launch_dependents();
     double acc[3] = {0, 0, 0};
-    for (int k = A.v_rp[v]; k < A.v_rp[v + 1]; ++k) {
+    for (int k = k0 + lane; k < k1; k += GATHER_LANES) {
         const double* b = A.B + 3 * static_cast<int64_t>(A.v_slot[k]);
         acc[0] += b[0]; acc[1] += b[1]; acc[2] += b[2];
     }
-    double* y = A.Y + static_cast<int64_t>(A.ldY) * v;
-    for (int k = 0; k < 3; ++k) y[k] = A.alpha * acc[k] + (A.beta == 0.0 ? 0.0 : A.beta * y[k]);
+#pragma unroll
+    for (int off = 1; off < GATHER_LANES; off <<= 1)
+#pragma unroll
+        for (int m = 0; m < 3; ++m) acc[m] += __shfl_xor_sync(0xffffffffu, acc[m], off);
+    if (!active || lane >= 3) return;
+    const double a = lane == 0 ? acc[0] : (lane == 1 ? acc[1] : acc[2]);
+    double* y = A.Y + static_cast<int64_t>(A.ldY) * v + lane;
+    *y = A.alpha * a + (A.beta == 0.0 ? 0.0 : A.beta * *y);
 }
 
 }  // namespace rpb

@@ -132,9 +132,9 @@ rpb_status launch_geometry(rpb_mesh* m)
     g.C_mom = nullptr;   // the FP64 moments are not read by any later kernel
     g.local = m->scan_local.ptr;
     g.blocks = m->scan_blocks.ptr;
+    g.scan_done = m->done.ptr + 2;
     const int nb = (m->N + SCAN_BLOCK - 1) / SCAN_BLOCK;
     k_geometry_prims<<<nb, SCAN_BLOCK, 0, m->stream>>>(g);
-    launch_pdl(k_scan_rows<10>, 1, SCAN_BLOCK, 0, m->stream, m->scan_blocks.ptr, nb);
     launch_pdl(k_cluster_moments, (m->NC + 255) / 256, 256, 0, m->stream, g);
     RPB_CUDA(cudaGetLastError());
     m->geometry_valid = true;
@@ -389,7 +389,8 @@ rpb_status launch_collect_gather(rpb_mesh* m, double alpha, double beta, double*
     C.D_far = D_far ? D_far : m->D_far.ptr;
     C.D_vf = D_vf;
     C.B = m->B.ptr;
-    launch_pdl(k_collect_chain, (m->N + 255) / 256, 256, 0, m->stream, C);
+    launch_pdl(k_collect_chain, static_cast<int>((static_cast<int64_t>(m->N) * COLLECT_LANES + 255) / 256), 256, 0,
+               m->stream, C);
     RPB_CUDA(cudaGetLastError());
     GatherArgs G;
     G.nV = m->nV;
@@ -400,7 +401,8 @@ rpb_status launch_collect_gather(rpb_mesh* m, double alpha, double beta, double*
     G.beta = beta;
     G.Y = Y;
     G.ldY = ldY;
-    launch_pdl(k_gather_vertices, (m->nV + 255) / 256, 256, 0, m->stream, G);
+    launch_pdl(k_gather_vertices, static_cast<int>((static_cast<int64_t>(m->nV) * GATHER_LANES + 255) / 256), 256, 0,
+               m->stream, G);
     RPB_CUDA(cudaGetLastError());
     return RPB_OK;
 }

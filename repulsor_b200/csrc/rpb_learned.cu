@@ -647,21 +647,30 @@ __global__ void __launch_bounds__(GAIN_BLOCK, 4) k_cluster_mlp(ClusterMlpArgs A)
 }
 
 // Z_i = sum over the clusters containing primitive i of c_C (PercolateDown +
-// ClustersToPrimitives as an ancestor walk)
+// ClustersToPrimitives as an ancestor walk). EXPAND_LANES consecutive lanes per primitive
+// (vertex): lane p takes the ancestors at distances p, p + 4, ... (the vertex's slots
+// p, p + 4, ...), an xor butterfly combines the partial sums, lane k < 3 writes component k.
+constexpr int EXPAND_LANES = 4;
+
 __global__ void k_prim_expand(int N, const int* leaf_of, const int* C_parent, const int* C_up4, const double* c,
                               double* Z)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= N) return;
-    double z0 = 0, z1 = 0, z2 = 0;
-    ancestor_walk(leaf_of[i], C_parent, C_up4, [&](int C) {
-        z0 += c[3 * static_cast<int64_t>(C)];
-        z1 += c[3 * static_cast<int64_t>(C) + 1];
-        z2 += c[3 * static_cast<int64_t>(C) + 2];
-    });
-    Z[3 * static_cast<int64_t>(i)] = z0;
-    Z[3 * static_cast<int64_t>(i) + 1] = z1;
-    Z[3 * static_cast<int64_t>(i) + 2] = z2;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = t / EXPAND_LANES, lane = t % EXPAND_LANES;
+    const bool active = i < N;
+    double z[3] = {0, 0, 0};
+    if (active) {
+        int C = leaf_of[i];
+        for (int k = 0; k < lane && C >= 0; ++k) C = __ldg(C_parent + C);
+        for (; C >= 0; C = __ldg(C_up4 + C))
+            for (int m = 0; m < 3; ++m) z[m] += c[3 * static_cast<int64_t>(C) + m];
+    }
+#pragma unroll
+    for (int off = 1; off < EXPAND_LANES; off <<= 1)
+#pragma unroll
+        for (int m = 0; m < 3; ++m) z[m] += __shfl_xor_sync(0xffffffffu, z[m], off);
+    if (!active || lane >= 3) return;
+    Z[3 * static_cast<int64_t>(i) + lane] = lane == 0 ? z[0] : (lane == 1 ? z[1] : z[2]);
 }
 
 // z_v = sum over the primitives i at v of w_i Z_i, minus the mean of z (translations are
@@ -669,20 +678,23 @@ __global__ void k_prim_expand(int N, const int* leaf_of, const int* C_parent, co
 __global__ void k_vertex_expand(int nV, int size, const int* vp_rp, const int* vp_slot, const double* pre_vals,
                                 const double* Z, const double* zmean, double* z)
 {
-    const int v = blockIdx.x * blockDim.x + threadIdx.x;
-    if (v >= nV) return;
-    double a0 = 0, a1 = 0, a2 = 0;
-    for (int k = vp_rp[v]; k < vp_rp[v + 1]; ++k) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int v = t / EXPAND_LANES, lane = t % EXPAND_LANES;
+    const bool active = v < nV;
+    double a[3] = {0, 0, 0};
+    const int k1 = active ? vp_rp[v + 1] : 0;
+    for (int k = (active ? vp_rp[v] : 0) + lane; k < k1; k += EXPAND_LANES) {
         const int slot = vp_slot[k];
         const int i = slot / size, l = slot - i * size;
         const double w = pre_vals[(4 * static_cast<int64_t>(i)) * size + l];
-        a0 += w * Z[3 * static_cast<int64_t>(i)];
-        a1 += w * Z[3 * static_cast<int64_t>(i) + 1];
-        a2 += w * Z[3 * static_cast<int64_t>(i) + 2];
+        for (int m = 0; m < 3; ++m) a[m] += w * Z[3 * static_cast<int64_t>(i) + m];
     }
-    z[3 * static_cast<int64_t>(v)] = a0 - zmean[0];
-    z[3 * static_cast<int64_t>(v) + 1] = a1 - zmean[1];
-    z[3 * static_cast<int64_t>(v) + 2] = a2 - zmean[2];
+#pragma unroll
+    for (int off = 1; off < EXPAND_LANES; off <<= 1)
+#pragma unroll
+        for (int m = 0; m < 3; ++m) a[m] += __shfl_xor_sync(0xffffffffu, a[m], off);
+    if (!active || lane >= 3) return;
+    z[3 * static_cast<int64_t>(v) + lane] = (lane == 0 ? a[0] : (lane == 1 ? a[1] : a[2])) - zmean[lane];
 }
 
 // per-primitive a*n (3) for the averaged-normal feature
@@ -948,9 +960,9 @@ static rpb_status learned_forward(rpb_mesh* m, rpb_mlp* mlp, const double* R, do
     ca.pre2 = training ? L.pre2.ptr : nullptr;
     ca.Rc = training ? L.Rc.ptr : nullptr;
     k_cluster_mlp<<<std::min(L.mlp_grid, (m->NC + GAIN_BLOCK - 1) / GAIN_BLOCK), GAIN_BLOCK, 0, s>>>(ca);
-    k_prim_expand<<<(m->N + 255) / 256, 256, 0, s>>>(m->N, m->leaf_of.ptr, m->C_parent.ptr, m->C_up4.ptr, L.c.ptr,
+    k_prim_expand<<<(m->N * EXPAND_LANES + 255) / 256, 256, 0, s>>>(m->N, m->leaf_of.ptr, m->C_parent.ptr, m->C_up4.ptr, L.c.ptr,
                                                       L.tmp3.ptr);
-    k_vertex_expand<<<(m->nV + 255) / 256, 256, 0, s>>>(m->nV, m->size, m->vp_rp.ptr, m->vp_slot.ptr, m->pre_vals.ptr,
+    k_vertex_expand<<<(m->nV * EXPAND_LANES + 255) / 256, 256, 0, s>>>(m->nV, m->size, m->vp_rp.ptr, m->vp_slot.ptr, m->pre_vals.ptr,
                                                         L.tmp3.ptr, L.zmean.ptr, z);
     RPB_CUDA(cudaGetLastError());
     return RPB_OK;
@@ -1142,10 +1154,11 @@ rpb_status rpb_tpm0_learned_apply_pair(rpb_mesh* m, const double* R, const doubl
         RPB_CUDA(cudaMemcpyAsync(L.e.ptr, Y, n3 * sizeof(double), cudaMemcpyHostToDevice, s));
         if ((st = cluster_moments(m, L.e.ptr, L.gc.ptr)) != RPB_OK) return st;
         k_frozen_coef<<<(m->NC + 255) / 256, 256, 0, s>>>(m->NC, L.O.ptr, L.gc.ptr, L.C_w.ptr, L.c.ptr);
-        k_prim_expand<<<(m->N + 255) / 256, 256, 0, s>>>(m->N, m->leaf_of.ptr, m->C_parent.ptr, m->C_up4.ptr, L.c.ptr,
+        k_prim_expand<<<(m->N * EXPAND_LANES + 255) / 256, 256, 0, s>>>(m->N, m->leaf_of.ptr, m->C_parent.ptr, m->C_up4.ptr, L.c.ptr,
                                                           L.tmp3.ptr);
         RPB_CUDA(cudaMemsetAsync(L.dots.ptr, 0, 3 * sizeof(double), s));
-        k_vertex_expand<<<eb, 256, 0, s>>>(m->nV, m->size, m->vp_rp.ptr, m->vp_slot.ptr, m->pre_vals.ptr, L.tmp3.ptr,
+        k_vertex_expand<<<(m->nV * EXPAND_LANES + 255) / 256, 256, 0, s>>>(m->nV, m->size, m->vp_rp.ptr, m->vp_slot.ptr,
+                                                                          m->pre_vals.ptr, L.tmp3.ptr,
                                           L.dots.ptr, L.g.ptr);
         if ((st = dot3_dev(m, L.g.ptr, nullptr, L.sums.ptr)) != RPB_OK) return st;
         k_sub_mean<<<eb, 256, 0, s>>>(m->nV, L.g.ptr, L.sums.ptr);

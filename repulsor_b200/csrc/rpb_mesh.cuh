@@ -116,7 +116,9 @@ struct rpb_mesh {
     rpb::DevBuf<int> v_rp, v_slot;
     rpb::DevBuf<double> Y;
     rpb::DevBuf<double> block_energy, energy;   // energy[0] near, [1] far, [2] very near
-    rpb::DevBuf<unsigned> done;                 // last-block counters of the two pair kernels
+    rpb::DevBuf<unsigned> done;                 // last-block counters: [0] near, [1] far pairs,
+                                                // [2] the geometry kernel's, [3] the metric
+                                                // Pre kernel's block scan
     int near_blocks = 0, far_blocks = 0;
     int shards = 1;                             // row shards the tiles are grouped for
     int64_t last_step_candidates = 0;           // candidate pairs of the last MaximumSafeStepSize

@@ -125,10 +125,12 @@ struct PreArgs {
     double* Cin;              // NC x BD
     double* local;            // N x BD in-block exclusive prefix
     double* blocks;           // (nblocks + 1) x BD
+    unsigned* scan_done;      // last-block counter: the last k_pre block scans `blocks`
 };
 
 // Pre operator per primitive (mi_pre / lo_pre rows, src/ClusterTree.hpp:410-639) and the
-// in-block prefix sums that give PrimitivesToClusters + PercolateUp as range sums.
+// in-block prefix sums that give PrimitivesToClusters + PercolateUp as range sums; the
+// last block scans the block sums.
 template <int BD>
 __global__ void __launch_bounds__(SCAN_BLOCK) k_pre(PreArgs<BD> A)
 {
@@ -160,6 +162,7 @@ __global__ void __launch_bounds__(SCAN_BLOCK) k_pre(PreArgs<BD> A)
         for (int k = 0; k < BD; ++k) A.local[BD * static_cast<int64_t>(i) + k] = x[k];
     }
     if (threadIdx.x < BD) A.blocks[BD * static_cast<int64_t>(blockIdx.x) + threadIdx.x] = tot[threadIdx.x];
+    last_block_scans_rows<BD>(A.blocks, gridDim.x, A.scan_done);
 }
 
 template <int BD>
@@ -362,30 +365,49 @@ struct PostArgs {
     int ldY;
 };
 
+// POST_LANES consecutive lanes per primitive (vertex): lane p adds the ancestors at
+// distances p, p + 4, ... from the leaf (the vertex's slots p, p + 4, ...); an xor
+// butterfly combines the lanes' partial sums (every lane ends with the same totals) and the
+// lanes write disjoint components.
+constexpr int POST_LANES = 4;
+
 template <int BD>
 __global__ void k_post_primitives(PostArgs<BD> A)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= A.N) return;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = t / POST_LANES, lane = t % POST_LANES;
+    const bool active = i < A.N;
     double z[BD];
 #pragma unroll
-    for (int c = 0; c < BD; ++c) z[c] = A.Pout[BD * static_cast<int64_t>(i) + c];
-    ancestor_walk(A.leaf_of[i], A.C_parent, A.C_up4, [&](int C) {
+    for (int c = 0; c < BD; ++c) z[c] = (active && lane == 0) ? A.Pout[BD * static_cast<int64_t>(i) + c] : 0.0;
+    if (active) {
+        int C = A.leaf_of[i];
+        for (int k = 0; k < lane && C >= 0; ++k) C = __ldg(A.C_parent + C);
+        for (; C >= 0; C = __ldg(A.C_up4 + C)) {
 #pragma unroll
-        for (int c = 0; c < BD; ++c) z[c] += A.Cout[BD * static_cast<int64_t>(C) + c];
-    });
+            for (int c = 0; c < BD; ++c) z[c] += A.Cout[BD * static_cast<int64_t>(C) + c];
+        }
+    }
 #pragma unroll
-    for (int c = 0; c < BD; ++c) A.Z[BD * static_cast<int64_t>(i) + c] = z[c];
+    for (int off = 1; off < POST_LANES; off <<= 1)
+#pragma unroll
+        for (int c = 0; c < BD; ++c) z[c] += __shfl_xor_sync(0xffffffffu, z[c], off);
+    if (!active) return;
+#pragma unroll
+    for (int c = 0; c < BD; ++c)
+        if (c % POST_LANES == lane) A.Z[BD * static_cast<int64_t>(i) + c] = z[c];
 }
 
 template <int BD>
 __global__ void k_post_vertices(PostArgs<BD> A)
 {
-    const int v = blockIdx.x * blockDim.x + threadIdx.x;
-    if (v >= A.nV) return;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int v = t / POST_LANES, lane = t % POST_LANES;
+    const bool active = v < A.nV;
     constexpr int ROWS = BD / 3;
     double acc[3] = {0, 0, 0};
-    for (int k = A.vp_rp[v]; k < A.vp_rp[v + 1]; ++k) {
+    const int k1 = active ? A.vp_rp[v + 1] : 0;
+    for (int k = (active ? A.vp_rp[v] : 0) + lane; k < k1; k += POST_LANES) {
         const int slot = A.vp_slot[k];
         const int i = slot / A.size, l = slot - i * A.size;
         const double* z = A.Z + BD * static_cast<int64_t>(i);
@@ -397,8 +419,14 @@ __global__ void k_post_vertices(PostArgs<BD> A)
             acc[2] += w * z[3 * r + 2];
         }
     }
-    double* y = A.Y + static_cast<int64_t>(A.ldY) * v;
-    for (int c = 0; c < 3; ++c) y[c] = A.alpha * acc[c] + (A.beta == 0.0 ? 0.0 : A.beta * y[c]);
+#pragma unroll
+    for (int off = 1; off < POST_LANES; off <<= 1)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], off);
+    if (!active || lane >= 3) return;
+    const double a = lane == 0 ? acc[0] : (lane == 1 ? acc[1] : acc[2]);
+    double* y = A.Y + static_cast<int64_t>(A.ldY) * v + lane;
+    *y = A.alpha * a + (A.beta == 0.0 ? 0.0 : A.beta * *y);
 }
 
 // ==========================================================================================
@@ -573,9 +601,9 @@ static rpb_status apply_operator(rpb_mesh* m, const float2* nf, const double2* n
     pa.C_begin = m->C_begin.ptr; pa.C_end = m->C_end.ptr;
     pa.Pin = m->buf_Pin64.ptr; pa.Cin = m->buf_Cin64.ptr;
     pa.local = m->buf_scan_local.ptr; pa.blocks = m->buf_scan_blocks.ptr;
+    pa.scan_done = m->done.ptr + 3;
     const int nb = (m->N + SCAN_BLOCK - 1) / SCAN_BLOCK;
     k_pre<BD><<<nb, SCAN_BLOCK, 0, s>>>(pa);
-    k_scan_rows<BD><<<1, SCAN_BLOCK, 0, s>>>(m->buf_scan_blocks.ptr, nb);
     k_cluster_sums<BD><<<(m->NC + 255) / 256, 256, 0, s>>>(pa);
     RPB_CUDA(cudaGetLastError());
 
@@ -617,9 +645,9 @@ static rpb_status apply_operator(rpb_mesh* m, const float2* nf, const double2* n
     po.Pout = m->buf_Pout.ptr; po.Cout = m->buf_Cout.ptr; po.Z = m->buf_Z.ptr;
     po.vp_rp = m->vp_rp.ptr; po.vp_slot = m->vp_slot.ptr; po.pre_vals = m->pre_vals.ptr;
     po.alpha = alpha; po.beta = beta; po.Y = Y; po.ldY = ldY;
-    k_post_primitives<BD><<<(m->N + 255) / 256, 256, 0, s>>>(po);
+    k_post_primitives<BD><<<static_cast<int>((static_cast<int64_t>(m->N) * POST_LANES + 255) / 256), 256, 0, s>>>(po);
     RPB_CUDA(cudaGetLastError());
-    k_post_vertices<BD><<<(m->nV + 255) / 256, 256, 0, s>>>(po);
+    k_post_vertices<BD><<<static_cast<int>((static_cast<int64_t>(m->nV) * POST_LANES + 255) / 256), 256, 0, s>>>(po);
     RPB_CUDA(cudaGetLastError());
     return RPB_OK;
 }
