@@ -209,7 +209,7 @@ def main():
     ap.add_argument("--no-extras", action="store_true")
     ap.add_argument("--no-solve", action="store_true", help="skip the Solve timings on the icosphere level-6 mesh")
     ap.add_argument("--no-graph", action="store_true", help="time direct launches instead of a captured CUDA graph")
-    ap.add_argument("--flow-max-iter", type=int, default=15000, help="iteration limit of the full-flow Solve")
+    ap.add_argument("--flow-max-iter", type=int, default=100000, help="iteration limit of the full-flow Solve")
     ap.add_argument("--flow", action="store_true",
                     help="only the full flow step on two linked tori (1,228,800 triangles) with an obstacle")
     ap.add_argument("--learned", action="store_true",
@@ -220,6 +220,9 @@ def main():
     ap.add_argument("--learned-heldout", type=int, default=32, help="held-out meshes (32)")
     ap.add_argument("--learned-steps", type=int, default=30, help="unrolled CG iterations of the training loss")
     ap.add_argument("--learned-lr", type=float, default=1e-3, help="Adam learning rate")
+    ap.add_argument("--learned-hard", type=int, default=0,
+                    help="train on the residuals left after this many flexible-CG iterations with the untrained "
+                         "operator (repulsor_b200.learned.slow_residual) instead of N(0,1) right-hand sides")
     ap.add_argument("--sharded", action="store_true",
                     help="strong scaling: one mesh (the two linked tori) row-sharded over the ranks, one NCCL "
                          "all-reduce of the derivative buffers per evaluation")
@@ -476,7 +479,7 @@ def run_learned(args):
 
     import repulsor_b200 as rpb
     from repulsor_b200 import meshes
-    from repulsor_b200.learned import NPARAM_OUTPUT_OFFSET, LearnedPreconditioner, train_unrolled
+    from repulsor_b200.learned import NPARAM_OUTPUT_OFFSET, LearnedPreconditioner, slow_residual, train_unrolled
 
     torch.cuda.set_device(0)
     tpm = rpb.TangentPointMetric0(Q, P)
@@ -493,6 +496,8 @@ def run_learned(args):
         V, S = meshes.icosphere_sh(level=levels[i % 3], seed=5000 + i)
         M = rpb.SimplicialMesh(V, S)
         samples = [(M, meshes.random_rhs(V.shape[0], seed=100 * (5000 + i) + j)) for j in range(args.learned_rhs)]
+        if args.learned_hard > 0:
+            samples = [(M, slow_residual(prior, M, tpm, rhs, args.learned_hard)) for _, rhs in samples]
         setup_s += time.perf_counter() - ts
         losses += train_unrolled(net, tpm, samples, epochs=1, lr=args.learned_lr, steps=args.learned_steps, seed=i)
         del M, samples
@@ -533,6 +538,8 @@ def run_learned(args):
            "workload": f"icosphere_sh levels 5-7: {args.learned_train} training meshes x {args.learned_rhs} RHS "
                        f"(seeds 5000+), {args.learned_heldout} held-out meshes (seeds 9000+), q=6 p=12 theta=0.5",
            "training": {"loss": f"unrolled CG energy, K = {args.learned_steps} iterations", "lr": args.learned_lr,
+                        "rhs": (f"residuals after {args.learned_hard} untrained flexible-CG iterations"
+                                if args.learned_hard > 0 else "N(0,1), mean-free"),
                         "samples": args.learned_train * args.learned_rhs, "training_s": train_s,
                         "mesh_setup_s": setup_s, "loss_first_mesh": float(np.mean(losses[:args.learned_rhs])),
                         "loss_last_mesh": float(np.mean(losses[-args.learned_rhs:]))},

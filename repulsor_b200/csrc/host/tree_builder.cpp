@@ -652,50 +652,39 @@ void build_row_tiles(const int64_t* rp, const int* ci, int rows, int ncols, int 
             }
             for (int64_t k = rp[t0]; k < rp[t1]; ++k) out.slot[k] = static_cast<uint16_t>(pos[ci[k]]);
             for (int u : U) pos[u] = -1;
-            // lane groups: the smallest per-lane trip count T for which the groups
-            // g = ceil(len / T) (at most 32 lanes) pack into the block's warps without
-            // straddling one (first fit, largest groups first); every lane of a group then
-            // takes at most T of its row's entries
+            // lane groups: every row starts with one lane; the row with the most entries per
+            // lane doubles its group while the block has lanes left (groups of at most 32)
             auto len = [&](int q) { return rp[t0 + q + 1] - rp[t0 + q]; };
-            const int warps = block_lanes / 32;
-            int64_t entries = rp[t1] - rp[t0], longest = 1;
-            for (int q = 0; q < R; ++q) longest = std::max<int64_t>(longest, len(q));
-            idx.resize(R);
-            std::vector<int> fill(warps), warp_of(R), lane_of(R);
-            for (int64_t T = std::max<int64_t>(1, (entries + block_lanes - 1) / block_lanes);; ++T) {
-                bool fits = true;
-                size.assign(R, 1);
-                for (int q = 0; q < R && fits; ++q) {
-                    size[q] = static_cast<int>(std::min<int64_t>(32, std::max<int64_t>(1, (len(q) + T - 1) / T)));
-                    fits = (len(q) + size[q] - 1) / size[q] <= T;
-                }
-                if (!fits) continue;
-                for (int q = 0; q < R; ++q) idx[q] = q;
-                std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) {
-                    return size[x] > size[y] || (size[x] == size[y] && len(x) > len(y));
-                });
-                std::fill(fill.begin(), fill.end(), 0);
-                for (int q : idx) {
-                    int w = 0;
-                    while (w < warps && fill[w] + size[q] > 32) ++w;
-                    if (w == warps) { fits = false; break; }
-                    warp_of[q] = w;
-                    lane_of[q] = fill[w];
-                    fill[w] += size[q];
-                }
-                if (fits || T >= longest) break;
+            auto load = [&](int q) { return (len(q) + size[q] - 1) / size[q]; };
+            size.assign(R, 1);
+            int used = R;
+            auto cmp = [&](int x, int y) { return load(x) < load(y) || (load(x) == load(y) && x > y); };
+            std::vector<int> heap(R);
+            for (int q = 0; q < R; ++q) heap[q] = q;
+            std::make_heap(heap.begin(), heap.end(), cmp);
+            while (!heap.empty()) {
+                std::pop_heap(heap.begin(), heap.end(), cmp);
+                const int q = heap.back();
+                if (size[q] >= 32 || used + size[q] > block_lanes || len(q) <= size[q]) break;
+                used += size[q];
+                size[q] *= 2;
+                std::push_heap(heap.begin(), heap.end(), cmp);
             }
-            // tile order: warp by warp, each warp's rows by their first lane
+            // groups in decreasing size (then decreasing length) start at multiples of their
+            // size and never straddle a warp
+            idx.resize(R);
+            for (int q = 0; q < R; ++q) idx[q] = q;
             std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) {
-                return warp_of[x] < warp_of[y] || (warp_of[x] == warp_of[y] && lane_of[x] < lane_of[y]);
+                return size[x] > size[y] || (size[x] == size[y] && len(x) > len(y));
             });
+            int lane = 0;
             for (int pos_in_tile = 0; pos_in_tile < R; ++pos_in_tile) {
                 const int q = idx[pos_in_tile];
                 out.order[t0 + pos_in_tile] = t0 + q;
-                const int first = 32 * warp_of[q] + lane_of[q];
                 for (int sub = 0; sub < size[q]; ++sub)
-                    out.lane_map[static_cast<size_t>(b) * block_lanes + first + sub] =
+                    out.lane_map[static_cast<size_t>(b) * block_lanes + lane + sub] =
                         (pos_in_tile << 10) | ((size[q] - 1) << 5) | sub;
+                lane += size[q];
             }
         }
     });

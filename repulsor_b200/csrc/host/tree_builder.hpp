@@ -82,16 +82,16 @@ std::string build_cross_lists(const HostTree& S, const double* VS, const int* SS
 // order, so spatially close) are grouped until a tile holds target_entries entries, at
 // most block_lanes rows and at most max_union distinct columns; a tile's kernel block
 // stages the union's column data once and every entry addresses it by its 16-bit slot.
-// Inside a tile every row gets a group of consecutive lanes (1 to 32, inside one warp):
-// the groups are the smallest ones that let every lane take at most T entries of its row
-// for the smallest T at which the groups still fit the block's warps. valid is false when
-// a single row has more than max_union entries.
+// Inside a tile every row gets a group of lanes (a power of two, at most 32, aligned in
+// its warp): all rows start with one lane and the row with the most entries per lane
+// doubles its group while the block has lanes left. valid is false when a single row has
+// more than max_union entries.
 struct RowTiles {
     std::vector<int> row0;          // tiles + 1: first row of each tile
     std::vector<int> cols_rp;       // tiles + 1: offsets into cols
     std::vector<int> cols;          // union columns of each tile, ascending
     std::vector<uint16_t> slot;     // nnz: index of the entry's column in its tile's union
-    std::vector<int> order;         // rows; inside each tile warp by warp, by first lane
+    std::vector<int> order;         // rows; inside each tile by decreasing group size and length
     std::vector<int> lane_map;      // tiles x block_lanes: (row position in the tile's order << 10)
                                     // | ((group size - 1) << 5) | lane in the group; -1 idle
     int block_lanes = 0;

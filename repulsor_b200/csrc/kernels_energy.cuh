@@ -228,8 +228,6 @@ struct GeomArgs {
     double* C_mom;            // NC x 10 (a, centre, P) in FP64, or null (not written)
     double* local;            // N x 10: exclusive in-block prefix of the moments (a, a c, a P)
     double* blocks;           // (nblocks + 1) x 10: block sums -> exclusive block prefix
-    unsigned* scan_done;      // last-block counter: the last geometry block scans `blocks`
-                              // (null: a separate k_scan_rows launch does)
 };
 
 __device__ __forceinline__ void store_cluster(ClusterDatum* base, int i, const double* mom)
@@ -243,8 +241,7 @@ __device__ __forceinline__ void store_cluster(ClusterDatum* base, int i, const d
 }
 
 // Simplex data in tree order (SimplexDataKernel::ReadSimplex/WriteFar) and the in-block
-// prefix sums of the additive moments (a, a c, a P); with scan_done, the last block also
-// turns the block sums into their exclusive prefix.
+// prefix sums of the additive moments (a, a c, a P).
 static __global__ void __launch_bounds__(SCAN_BLOCK) k_geometry_prims(GeomArgs g)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -271,7 +268,6 @@ static __global__ void __launch_bounds__(SCAN_BLOCK) k_geometry_prims(GeomArgs g
     if (i < g.N)
         for (int k = 0; k < 10; ++k) g.local[10 * static_cast<int64_t>(i) + k] = mom[k];
     if (threadIdx.x < 10) g.blocks[10 * static_cast<int64_t>(blockIdx.x) + threadIdx.x] = tot[threadIdx.x];
-    if (g.scan_done) last_block_scans_rows<10>(g.blocks, gridDim.x, g.scan_done);
 }
 
 // ClusterTree moments (ComputeClusterData_Thread.hpp:50-129): a cluster's moments are
@@ -480,16 +476,17 @@ constexpr int pair_blocks(int rows, int lanes) { return (rows * lanes + PAIR_BLO
 constexpr int PAIR_TILE_THREADS = 384;
 constexpr int NEAR_TILE_ROWS = 384;
 constexpr int FAR_TILE_ROWS = 192;
-constexpr int NEAR_TILE_UNION = 960;
+constexpr int NEAR_TILE_UNION = 768;
 constexpr int FAR_TILE_UNION = 1536;
 
-// One lane's share of a row: the row's entries k = k0 + sub, k0 + sub + stride, ... with the
-// column handle u = index(k) and the column datum from datum(u, Y). The next entry's handle
-// (PREFETCH: and its datum) is requested before the current pair is evaluated. A row
-// accumulates only its own derivative and the energy of every pair it holds: a symmetric
-// pattern holds each unordered pair twice (the pair energy is symmetric in its two
-// primitives or clusters), a CROSS pattern once with the symmetry factor 1/2, so the
-// epilogue halves the energy in both cases.
+// One lane's share of a row: the row's entries t = sub, sub + stride, ... < len (counted
+// from the row's first entry) with the column handle u = index(t) and the column datum
+// from datum(u, j, Y) (j: the column's tree position). The next entry's handle (PREFETCH:
+// and its datum) is requested before the current pair is evaluated. A row accumulates
+// only its own derivative. Energy: with COUNT_ALL every pair the row holds (a symmetric
+// pattern holds each unordered pair twice and the pair energy is symmetric in its two
+// primitives, so the epilogue halves the sum); otherwise each unordered pair from the row
+// with the smaller index (j > i), CROSS pairs always (halved for the symmetry factor).
 // A close near-field pair evaluated in FP64: energy and the ten derivative components.
 // Out of line and with its operands passed by value, so that its FP64 temporaries do not
 // count against the registers of the FP32 pair loop that calls it (rarely).
@@ -517,10 +514,10 @@ __device__ __noinline__ Close64 close_pair_fp64(TPExp ex, int dom, Datum X, ColD
 // SACC: the row's FP64 derivative accumulators live in shared memory at
 // Dsm[m * PAIR_TILE_THREADS] (zeroed by the caller) instead of D64, which is then filled
 // from them at the end; this keeps 20 registers free inside the loop.
-template <bool FAR, int QH, int PH, bool DIFF, bool CROSS, bool PREFETCH, bool SACC, typename ColDatum,
-          typename Datum, typename Index, typename Fetch>
-__device__ __forceinline__ void pair_row(const PairArgs& A, const Datum& X, int i, int sub, int stride, Index index,
-                                         Fetch datum, double& e_row, double (&D64)[10], double* Dsm)
+template <bool FAR, int QH, int PH, bool DIFF, bool CROSS, bool PREFETCH, bool SACC, bool COUNT_ALL,
+          typename ColDatum, typename Datum, typename Index, typename Fetch>
+__device__ __forceinline__ void pair_row(const PairArgs& A, const Datum& X, int i, int len, int sub, int stride,
+                                         Index index, Fetch datum, double& e_row, double (&D64)[10], double* Dsm)
 {
     auto add64 = [&](int m, double v) {
         if constexpr (SACC) Dsm[m * PAIR_TILE_THREADS] += v;
@@ -530,19 +527,21 @@ __device__ __forceinline__ void pair_row(const PairArgs& A, const Datum& X, int 
     PairAcc<float> acc = {};
     float e32 = 0.0f;
     int since_flush = 0;
-    const int64_t k0 = A.rp[i], k1 = A.rp[i + 1];
-    int64_t k = k0 + sub;
-    int un = (k < k1) ? index(k) : 0;
+    int t = sub;
+    int un = (t < len) ? index(t) : 0;
+    int jn = 0;
     ColDatum Yn;
-    if (PREFETCH && k < k1) datum(un, Yn);
-    for (; k < k1; k += stride) {
+    if (PREFETCH && t < len) datum(un, jn, Yn);
+    for (; t < len; t += stride) {
+        int j;
         ColDatum Y;
         if constexpr (PREFETCH) {
+            j = jn;
             Y = Yn;
-            if (k + stride < k1) datum(index(k + stride), Yn);
+            if (t + stride < len) datum(index(t + stride), jn, Yn);
         } else {
-            datum(un, Y);
-            if (k + stride < k1) un = index(k + stride);
+            datum(un, j, Y);
+            if (t + stride < len) un = index(t + stride);
         }
         Proj<float> g;
         if constexpr (FAR) project_clusters(X, Y, g);
@@ -558,7 +557,7 @@ __device__ __forceinline__ void pair_row(const PairArgs& A, const Datum& X, int 
             if constexpr (!FAR) {
                 const Close64 c =
                     close_pair_fp64<QH, PH, DIFF>(A.ex, A.dom, load_datum(static_cast<const Datum*>(A.data), i), Y);
-                e_row += c.e;
+                if (COUNT_ALL || CROSS || j > i) e_row += c.e;
                 if (DIFF) {
 #pragma unroll
                     for (int m = 0; m < 10; ++m) add64(m, c.d[m]);
@@ -566,7 +565,7 @@ __device__ __forceinline__ void pair_row(const PairArgs& A, const Datum& X, int 
             }
         } else {
             const float e = tp0_core<float, QH, PH, DIFF>(A.ex, g, ax, weight_f(Y), acc);
-            e32 += e;
+            if (COUNT_ALL || CROSS || j > i) e32 += e;
             if (++since_flush == PAIR_FLUSH) {
                 since_flush = 0;
                 e_row += e32;
@@ -603,11 +602,11 @@ __device__ __forceinline__ void pair_row(const PairArgs& A, const Datum& X, int 
 // finish sums the partials in block order.
 // bid / nblocks: this block's index among the launch's blocks for this pattern (the
 // block energies are summed in that order by the last of them)
-template <bool DIFF, bool CROSS>
+template <bool DIFF, bool CROSS, bool COUNT_ALL>
 __device__ __forceinline__ void pair_epilogue(const PairArgs& A, bool active, int i, int sub, int size, int warp_size_max,
                                               double e_row, double (&D64)[10], int bid, int nblocks)
 {
-    e_row *= 0.5;
+    if constexpr (COUNT_ALL || CROSS) e_row *= 0.5;
     if constexpr (CROSS) {
 #pragma unroll
         for (int m = 0; m < 10; ++m) D64[m] *= 0.5;
@@ -683,11 +682,17 @@ __global__ void __launch_bounds__(PAIR_BLOCK) k_tp0_pairs(PairArgs A)
     if (active) {
         i = A.order ? A.order[slot] : slot;
         const Datum X = load_datum(base, i);
-        auto index = [&](int64_t k) { return __ldg(A.ci + k); };
-        auto datum = [&](int u, Datum& Y) { Y = load_datum(cols, u); };
-        pair_row<FAR, QH, PH, DIFF, CROSS, true, false, Datum>(A, X, i, sub, LANES, index, datum, e_row, D64, nullptr);
+        const int64_t k0 = A.rp[i];
+        const int* crow = A.ci + k0;
+        auto index = [&](int t) { return __ldg(crow + t); };
+        auto datum = [&](int u, int& j, Datum& Y) {
+            j = u;
+            Y = load_datum(cols, u);
+        };
+        pair_row<FAR, QH, PH, DIFF, CROSS, true, false, false, Datum>(A, X, i, static_cast<int>(A.rp[i + 1] - k0), sub,
+                                                                     LANES, index, datum, e_row, D64, nullptr);
     }
-    pair_epilogue<DIFF, CROSS>(A, active, i, sub, LANES, LANES, e_row, D64, blockIdx.x, gridDim.x);
+    pair_epilogue<DIFF, CROSS, false>(A, active, i, sub, LANES, LANES, e_row, D64, blockIdx.x, gridDim.x);
 }
 
 // Row tiles (build_row_tiles): block b owns the rows order[row0[b] .. row0[b+1]) and
@@ -725,16 +730,34 @@ __device__ __forceinline__ ClusterDatum load_cluster_rot(const float4* sdat, int
 }
 
 // dynamic shared memory per tile of union size n: the data (PrimTile 80 bytes, ClusterDatum
-// 64 bytes)
+// 64 bytes); far tiles also the union's column ids (their rows count each pair's energy
+// from the smaller index; near rows count every pair and halve: measured fastest for each)
 __host__ __device__ constexpr size_t pair_tile_union_bytes(int n, bool far)
 {
-    return (static_cast<size_t>(n) * (far ? sizeof(ClusterDatum) : sizeof(PrimTile)) + 15) / 16 * 16;
+    return (static_cast<size_t>(n) * (far ? sizeof(ClusterDatum) + sizeof(int) : sizeof(PrimTile)) + 15) / 16 * 16;
 }
 
 // union; near tiles also the FP64 derivative accumulators of every thread
-__host__ __device__ constexpr size_t pair_tile_smem(int n, bool far)
+__host__ __device__ constexpr size_t pair_tile_data_bytes(int n, bool far)
 {
     return pair_tile_union_bytes(n, far) + (far ? 0 : sizeof(double) * 10 * PAIR_TILE_THREADS);
+}
+
+// Entries of a near tile's slot copy: its entries [e0, e1) extended down to a multiple of
+// 8 (16-byte pieces) and up to the next one; the slot array holds PAIR_SLOT_PAD spare
+// entries after the last so that the last piece stays inside it. Far tiles read their
+// slots from global memory: staged, they measured slower (44.1 against 41.3 us on the
+// 160 x 120 torus; near tiles 29.7 against 30.8 us).
+constexpr int PAIR_SLOT_PAD = 8;
+__host__ __device__ constexpr size_t pair_tile_slot_bytes(int64_t entries)
+{
+    return static_cast<size_t>((entries + 2 * PAIR_SLOT_PAD - 1) / PAIR_SLOT_PAD * PAIR_SLOT_PAD) * sizeof(uint16_t);
+}
+
+// the whole dynamic shared memory of a tile: data, then (near tiles) the tile's slots
+__host__ __device__ constexpr size_t pair_tile_smem(int n, bool far, int64_t entries)
+{
+    return pair_tile_data_bytes(n, far) + (far ? 0 : pair_tile_slot_bytes(entries));
 }
 
 template <bool FAR, int QH, int PH, bool DIFF>
@@ -747,12 +770,26 @@ __device__ __forceinline__ void pairs_tiled_body(const PairArgs& A, const PairTi
     const int b = T.tile_base + bid;
     const int u0 = T.cols_rp[b], un = T.cols_rp[b + 1] - u0;
     float4* sdat = tile_smem;
+    int* sid = reinterpret_cast<int*>(reinterpret_cast<char*>(tile_smem) + sizeof(ColDatum) * static_cast<size_t>(un));
+    if constexpr (FAR)
+        for (int u = threadIdx.x; u < un; u += blockDim.x) sid[u] = __ldg(T.cols + u0 + u);
     // the tile's lane map first; the primitive / cluster data once the producer has finished
     const int r0 = T.row0[b];
     const int lm = __ldg(T.lane_map + static_cast<int64_t>(b) * PAIR_TILE_THREADS + threadIdx.x);
     const bool active = lm >= 0;
     const int sub = active ? (lm & 31) : 0, size = active ? ((lm >> 5) & 31) + 1 : 1;
     const int i = active ? T.order[r0 + (lm >> 10)] : 0;
+    // near tiles: the tile's slots (entries rp[r0] .. rp[row0[b + 1]], contiguous) into
+    // shared memory by 16-byte pieces from the 8-entry boundary at or below the first
+    int64_t e_lo = 0;
+    uint16_t* sslot = nullptr;
+    if constexpr (!FAR) {
+        e_lo = A.rp[r0] / PAIR_SLOT_PAD * PAIR_SLOT_PAD;
+        const int pieces = static_cast<int>((A.rp[T.row0[b + 1]] - e_lo + PAIR_SLOT_PAD - 1) / PAIR_SLOT_PAD);
+        sslot = reinterpret_cast<uint16_t*>(reinterpret_cast<char*>(tile_smem) + pair_tile_data_bytes(un, false));
+        for (int q = threadIdx.x; q < pieces; q += blockDim.x)
+            cp_async16(sslot + PAIR_SLOT_PAD * q, T.slot + e_lo + PAIR_SLOT_PAD * static_cast<int64_t>(q));
+    }
     pdl_wait();
     pdl_launch_dependents();
     if constexpr (FAR) {
@@ -781,7 +818,7 @@ __device__ __forceinline__ void pairs_tiled_body(const PairArgs& A, const PairTi
     }
     Datum X;
     if (active) X = load_datum(base, i);
-    if constexpr (FAR) cp_async_wait_all();
+    cp_async_wait_all();
     __syncthreads();
     double e_row = 0.0;
     double D64[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
@@ -794,15 +831,35 @@ __device__ __forceinline__ void pairs_tiled_body(const PairArgs& A, const PairTi
         for (int m = 0; m < 10; ++m) Dsm[m * PAIR_TILE_THREADS] = 0.0;
     }
     if (active) {
-        auto index = [&](int64_t k) { return static_cast<int>(__ldg(T.slot + k)); };
-        auto datum = [&](int u, ColDatum& Y) {
-            if constexpr (FAR) Y = load_cluster_rot(sdat, u);
-            else Y = reinterpret_cast<const PrimTile*>(tile_smem)[u];
+        const int64_t k0 = A.rp[i];
+        // near rows: the row's slots by 32-bit shared-memory address (a generic pointer would
+        // hold two more registers in the loop); far rows: from global memory
+        const unsigned srow = FAR ? 0u
+                                  : static_cast<unsigned>(__cvta_generic_to_shared(sslot)) +
+                                        2u * static_cast<unsigned>(k0 - e_lo);
+        const uint16_t* grow = T.slot + k0;
+        auto index = [&](int t) {
+            if constexpr (FAR) {
+                return static_cast<int>(__ldg(grow + t));
+            } else {
+                unsigned short v;
+                asm volatile("ld.shared.u16 %0, [%1];" : "=h"(v) : "r"(srow + 2u * static_cast<unsigned>(t)));
+                return static_cast<int>(v);
+            }
         };
-        pair_row<FAR, QH, PH, DIFF, false, false, !FAR && DIFF, ColDatum>(A, X, i, sub, size, index, datum, e_row, D64,
-                                                                        Dsm);
+        auto datum = [&](int u, int& j, ColDatum& Y) {
+            if constexpr (FAR) {
+                Y = load_cluster_rot(sdat, u);
+                j = sid[u];
+            } else {
+                Y = reinterpret_cast<const PrimTile*>(tile_smem)[u];
+                j = 0;
+            }
+        };
+        pair_row<FAR, QH, PH, DIFF, false, false, !FAR && DIFF, !FAR, ColDatum>(
+            A, X, i, static_cast<int>(A.rp[i + 1] - k0), sub, size, index, datum, e_row, D64, Dsm);
     }
-    pair_epilogue<DIFF, false>(A, active, i, sub, size, __reduce_max_sync(0xffffffffu, size), e_row, D64, bid, nblocks);
+    pair_epilogue<DIFF, false, !FAR>(A, active, i, sub, size, __reduce_max_sync(0xffffffffu, size), e_row, D64, bid, nblocks);
 }
 
 template <bool FAR, int QH, int PH, bool DIFF>
@@ -876,70 +933,44 @@ struct CollectArgs {
     double* B;                 // N x (dom+1) x 3, original simplex order
 };
 
-// COLLECT_LANES consecutive lanes per primitive. The far-field part is split over the
-// lanes: lane p visits the ancestors at distances p, p + 4, p + 8, ... from the leaf (the
-// up4 jump pointers), so that a primitive's dependent loads run on four lanes at once; the
-// partial sums are combined by an xor butterfly (every lane ends with the same totals, since
-// a + b == b + a), and lane c < dom + 1 then forms corner c's derivative.
-constexpr int COLLECT_LANES = 4;
-
 static __global__ void k_collect_chain(CollectArgs A)
 {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    const int i = t / COLLECT_LANES, lane = t % COLLECT_LANES;
-    const bool active = i < A.N;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= A.N) return;
     const int size = A.dom + 1;
-    int j = 0;
+    const int j = A.perm[i];
     SimplexGeom g;
     // the coordinates were written before the pair kernels that precede this launch
-    if (active) {
-        j = A.perm[i];
-        simplex_geometry(A.dom, A.V, A.S + static_cast<int64_t>(size) * j, A.charge_v, g);
-    }
+    simplex_geometry(A.dom, A.V, A.S + static_cast<int64_t>(size) * j, A.charge_v, g);
     pdl_wait();
     pdl_launch_dependents();
 
-    double alpha = 0.0, gx[3] = {0, 0, 0}, G6[6] = {0, 0, 0, 0, 0, 0};
-    if (active) {
-        if (lane == 0) {
-            // near field (centred at the primitive barycentre)
-            const double* dn = A.D_near + 10 * static_cast<int64_t>(i);
-            alpha = dn[0];
-            for (int k = 0; k < 3; ++k) gx[k] = dn[1 + k];
-            for (int k = 0; k < 6; ++k) G6[k] = dn[4 + k];
-            if (A.D_vf) {
-                const double* dv = A.D_vf + 16 * static_cast<int64_t>(i);
-                alpha += dv[0];
-                for (int c = 0; c < size; ++c)
-                    for (int k = 0; k < 3; ++k) alpha += dv[1 + 3 * c + k] * g.h[c][k];
-                for (int k = 0; k < 6; ++k) G6[k] += dv[1 + 3 * size + k];
+    // near field (centred at the primitive barycentre)
+    const double* dn = A.D_near + 10 * static_cast<int64_t>(i);
+    double alpha = dn[0];
+    double gx[3] = {dn[1], dn[2], dn[3]};
+    double G6[6];
+    for (int k = 0; k < 6; ++k) G6[k] = dn[4 + k];
+    // far field: percolate down = sum over all ancestors of the leaf
+    ancestor_walk(A.leaf_of[i], A.C_parent, A.C_up4, [&](int C) {
+        const double* df = A.D_far + 10 * static_cast<int64_t>(C);
+        const ClusterDatum cd = load_datum(A.C_pair, C);
+        const double dx0 = df[1], dx1 = df[2], dx2 = df[3];
+        alpha += df[0] + dx0 * (g.c[0] - cd.c[0]) + dx1 * (g.c[1] - cd.c[1]) + dx2 * (g.c[2] - cd.c[2]);
+        gx[0] += dx0; gx[1] += dx1; gx[2] += dx2;
+        for (int k = 0; k < 6; ++k) G6[k] += df[4 + k];
+    });
+    double hull_extra[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    if (A.D_vf) {
+        const double* dv = A.D_vf + 16 * static_cast<int64_t>(i);
+        alpha += dv[0];
+        for (int c = 0; c < size; ++c)
+            for (int k = 0; k < 3; ++k) {
+                alpha += dv[1 + 3 * c + k] * g.h[c][k];
+                hull_extra[c][k] = dv[1 + 3 * c + k];
             }
-        }
-        // far field: percolate down = sum over all ancestors of the leaf, four levels apart
-        int C = A.leaf_of[i];
-        for (int k = 0; k < lane && C >= 0; ++k) C = __ldg(A.C_parent + C);
-        for (; C >= 0; C = __ldg(A.C_up4 + C)) {
-            const double* df = A.D_far + 10 * static_cast<int64_t>(C);
-            const ClusterDatum cd = load_datum(A.C_pair, C);
-            const double dx0 = df[1], dx1 = df[2], dx2 = df[3];
-            alpha += df[0] + dx0 * (g.c[0] - cd.c[0]) + dx1 * (g.c[1] - cd.c[1]) + dx2 * (g.c[2] - cd.c[2]);
-            gx[0] += dx0; gx[1] += dx1; gx[2] += dx2;
-            for (int k = 0; k < 6; ++k) G6[k] += df[4 + k];
-        }
+        for (int k = 0; k < 6; ++k) G6[k] += dv[1 + 3 * size + k];
     }
-#pragma unroll
-    for (int off = 1; off < COLLECT_LANES; off <<= 1) {
-        alpha += __shfl_xor_sync(0xffffffffu, alpha, off);
-#pragma unroll
-        for (int k = 0; k < 3; ++k) gx[k] += __shfl_xor_sync(0xffffffffu, gx[k], off);
-#pragma unroll
-        for (int k = 0; k < 6; ++k) G6[k] += __shfl_xor_sync(0xffffffffu, G6[k], off);
-    }
-    if (!active || lane >= size) return;
-    const int c = lane;
-    double hull_extra[3] = {0, 0, 0};
-    if (A.D_vf)
-        for (int k = 0; k < 3; ++k) hull_extra[k] = A.D_vf[16 * static_cast<int64_t>(i) + 1 + 3 * c + k];
     double P6[6];
     projector_packed(A.dom, g.t, P6);
     for (int k = 0; k < 6; ++k) alpha += G6[k] * P6[k];
@@ -950,25 +981,30 @@ static __global__ void k_collect_chain(CollectArgs A)
     double Gt[3];
     for (int a = 0; a < 3; ++a) Gt[a] = G[a][0] * g.t[0] + G[a][1] * g.t[1] + G[a][2] * g.t[2];
     const double tGt = g.t[0] * Gt[0] + g.t[1] * Gt[1] + g.t[2] * Gt[2];
-    double Bc[3];
+    double Bc[3][3];
     if (A.dom == 2) {
         double w[3];
         for (int a = 0; a < 3; ++a) w[a] = 2.0 * (Gt[a] - tGt * g.t[a]) / g.len;
-        const int c1 = (c + 1) % 3, c2 = (c + 2) % 3;
-        const double u[3] = {g.h[c1][0] - g.h[c2][0], g.h[c1][1] - g.h[c2][1], g.h[c1][2] - g.h[c2][2]};
-        const double un[3] = {u[1] * g.t[2] - u[2] * g.t[1], u[2] * g.t[0] - u[0] * g.t[2], u[0] * g.t[1] - u[1] * g.t[0]};
-        const double uw[3] = {u[1] * w[2] - u[2] * w[1], u[2] * w[0] - u[0] * w[2], u[0] * w[1] - u[1] * w[0]};
-        for (int k = 0; k < 3; ++k)
-            Bc[k] = g.charge * (alpha * 0.5 * un[k] + g.vol * (gx[k] / 3.0 + hull_extra[k]) + g.vol * uw[k]);
+        for (int c = 0; c < 3; ++c) {
+            const int c1 = (c + 1) % 3, c2 = (c + 2) % 3;
+            const double u[3] = {g.h[c1][0] - g.h[c2][0], g.h[c1][1] - g.h[c2][1], g.h[c1][2] - g.h[c2][2]};
+            const double un[3] = {u[1] * g.t[2] - u[2] * g.t[1], u[2] * g.t[0] - u[0] * g.t[2], u[0] * g.t[1] - u[1] * g.t[0]};
+            const double uw[3] = {u[1] * w[2] - u[2] * w[1], u[2] * w[0] - u[0] * w[2], u[0] * w[1] - u[1] * w[0]};
+            for (int k = 0; k < 3; ++k)
+                Bc[c][k] = g.charge * (alpha * 0.5 * un[k] + g.vol * (gx[k] / 3.0 + hull_extra[c][k]) + g.vol * uw[k]);
+        }
     } else {
         double gg[3];
         for (int a = 0; a < 3; ++a) gg[a] = -2.0 * (Gt[a] - tGt * g.t[a]) / g.len;
-        const double sgn = (c == 1) ? 1.0 : -1.0;
-        for (int k = 0; k < 3; ++k)
-            Bc[k] = g.charge * (alpha * sgn * g.t[k] + g.vol * (gx[k] * 0.5 + hull_extra[k]) + g.vol * sgn * gg[k]);
+        for (int c = 0; c < 2; ++c) {
+            const double sgn = (c == 1) ? 1.0 : -1.0;
+            for (int k = 0; k < 3; ++k)
+                Bc[c][k] = g.charge * (alpha * sgn * g.t[k] + g.vol * (gx[k] * 0.5 + hull_extra[c][k]) + g.vol * sgn * gg[k]);
+        }
     }
-    double* dst = A.B + static_cast<int64_t>(size) * 3 * j + 3 * c;
-    for (int k = 0; k < 3; ++k) dst[k] = Bc[k];
+    double* dst = A.B + static_cast<int64_t>(size) * 3 * j;
+    for (int c = 0; c < size; ++c)
+        for (int k = 0; k < 3; ++k) dst[3 * c + k] = Bc[c][k];
 }
 
 struct GatherArgs {

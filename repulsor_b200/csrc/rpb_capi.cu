@@ -132,9 +132,9 @@ rpb_status launch_geometry(rpb_mesh* m)
     g.C_mom = nullptr;   // the FP64 moments are not read by any later kernel
     g.local = m->scan_local.ptr;
     g.blocks = m->scan_blocks.ptr;
-    g.scan_done = m->done.ptr + 2;
     const int nb = (m->N + SCAN_BLOCK - 1) / SCAN_BLOCK;
     k_geometry_prims<<<nb, SCAN_BLOCK, 0, m->stream>>>(g);
+    launch_pdl(k_scan_rows<10>, 1, SCAN_BLOCK, 0, m->stream, m->scan_blocks.ptr, nb);
     launch_pdl(k_cluster_moments, (m->NC + 255) / 256, 256, 0, m->stream, g);
     RPB_CUDA(cudaGetLastError());
     m->geometry_valid = true;
@@ -147,13 +147,17 @@ rpb_status launch_geometry(rpb_mesh* m)
 // Largest dynamic shared memory a tiled pair kernel may ask for, set once per device for
 // every instantiation (the attribute only permits; each launch asks for its tiles' need).
 template <int QH, int PH>
-static cudaError_t allow_tile_smem_t()
+static cudaError_t allow_tile_smem_t(int optin)
 {
-    const int nb = static_cast<int>(pair_tile_smem(NEAR_TILE_UNION, false));
-    const int fb = static_cast<int>(pair_tile_smem(FAR_TILE_UNION, true));
+    const int nb = optin, fb = optin;
     cudaError_t e = cudaSuccess;
     auto set = [&](const void* f, int bytes) {
-        const cudaError_t r = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        // the block's static shared memory counts against the same per-block limit
+        cudaFuncAttributes fa;
+        cudaError_t r = cudaFuncGetAttributes(&fa, f);
+        if (r == cudaSuccess)
+            r = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     bytes - static_cast<int>(fa.sharedSizeBytes));
         if (e == cudaSuccess) e = r;
     };
     set(reinterpret_cast<const void*>(k_tp0_pairs_tiled<false, QH, PH, true>), nb);
@@ -171,10 +175,12 @@ static rpb_status allow_tile_smem(int device)
     static std::vector<int> done;
     std::lock_guard<std::mutex> lock(mu);
     if (std::find(done.begin(), done.end(), device) != done.end()) return RPB_OK;
-    RPB_CUDA((allow_tile_smem_t<3, 6>()));
-    RPB_CUDA((allow_tile_smem_t<2, 4>()));
-    RPB_CUDA((allow_tile_smem_t<1, 2>()));
-    RPB_CUDA((allow_tile_smem_t<-1, -1>()));
+    int optin = 0;
+    RPB_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+    RPB_CUDA((allow_tile_smem_t<3, 6>(optin)));
+    RPB_CUDA((allow_tile_smem_t<2, 4>(optin)));
+    RPB_CUDA((allow_tile_smem_t<1, 2>(optin)));
+    RPB_CUDA((allow_tile_smem_t<-1, -1>(optin)));
     done.push_back(device);
     return RPB_OK;
 }
@@ -206,18 +212,25 @@ static rpb_status tile_pattern(rpb_mesh* m, int rows, const int64_t* rp, const i
     d.tiles = 0;
     int sms = 0;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, m->device) != cudaSuccess) sms = 0;
-    auto resident = [&](int max_union) {
+    auto resident = [&](int max_union, int64_t max_entries) {
         int per_sm = 0;
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, PAIR_TILE_THREADS,
-                                                          pair_tile_smem(max_union, far)) != cudaSuccess)
+                                                          pair_tile_smem(max_union, far, max_entries)) != cudaSuccess)
             return 0;
         return per_sm;
     };
+    auto most_entries = [&](const RowTiles& R) {
+        int64_t e = 0;
+        for (int b = 0; b < R.tiles(); ++b) e = std::max(e, rp[R.row0[b + 1]] - rp[R.row0[b]]);
+        return e;
+    };
     if (sms <= 0 || nnz == 0) return RPB_OK;
-    // resident blocks depend on the tiles' largest union and the tile size on the resident
-    // blocks: start from the cap and re-tile while the count changes
-    int per_sm = resident(cap);
+    // resident blocks depend on the tiles' largest union and entry count, the tile size on
+    // the resident blocks: start from the union cap and two blocks' share of the entries
+    // and re-tile while the count changes
+    int per_sm = resident(cap, (nnz + 2 * sms * shards - 1) / (2 * sms * shards));
     RowTiles R;
+    int64_t max_entries = 0;
     for (int pass = 0; pass < 3 && per_sm > 0; ++pass) {
         const int64_t slots = static_cast<int64_t>(per_sm) * sms * shards;
         const int64_t tile_rows = far ? FAR_TILE_ROWS : NEAR_TILE_ROWS;
@@ -225,11 +238,15 @@ static rpb_status tile_pattern(rpb_mesh* m, int rows, const int64_t* rp, const i
         const int64_t target = (nnz + waves * slots - 1) / (waves * slots);
         build_row_tiles(rp, ci, rows, ncols, PAIR_TILE_THREADS, target, cap, std::max(1, m->settings.threads), R);
         if (!R.valid) break;
-        const int now = resident(R.max_union);
+        max_entries = most_entries(R);
+        const int now = resident(R.max_union, max_entries);
         if (now == per_sm) break;
         per_sm = now;
     }
     if (per_sm <= 0 || !R.valid || R.tiles() == 0) return RPB_OK;
+    // the kernels copy every tile's slots by 16-byte pieces, the last of which may reach up
+    // to PAIR_SLOT_PAD - 1 entries past the pattern's end
+    R.slot.resize(R.slot.size() + PAIR_SLOT_PAD, 0);
     rpb_status e;
     if ((e = upload(d.row0, R.row0.data(), R.row0.size(), s)) != RPB_OK) return e;
     if ((e = upload(d.cols_rp, R.cols_rp.data(), R.cols_rp.size(), s)) != RPB_OK) return e;
@@ -240,6 +257,7 @@ static rpb_status tile_pattern(rpb_mesh* m, int rows, const int64_t* rp, const i
     d.row0_host = R.row0;
     d.tiles = R.tiles();
     d.max_union = R.max_union;
+    d.max_entries = max_entries;
     d.valid = true;
     return RPB_OK;
 }
@@ -288,8 +306,8 @@ static void launch_pairs_t(rpb_mesh* m, const PairArgs& An, const PairArgs& Af, 
         shard_tiles(m->near_tiles, shard, m->shards, nfirst, ncount);
         shard_tiles(m->far_tiles, shard, m->shards, ffirst, fcount);
         if (ncount > 0 && fcount > 0) {
-            const size_t smem = std::max(pair_tile_smem(m->near_tiles.max_union, false),
-                                         pair_tile_smem(m->far_tiles.max_union, true));
+            const size_t smem = std::max(pair_tile_smem(m->near_tiles.max_union, false, m->near_tiles.max_entries),
+                                         pair_tile_smem(m->far_tiles.max_union, true, m->far_tiles.max_entries));
             launch_pdl(diff ? k_tp0_pairs_tiled_both<QH, PH, true> : k_tp0_pairs_tiled_both<QH, PH, false>,
                        ncount + fcount, PAIR_TILE_THREADS, smem, m->stream, An, tiles_view(m->near_tiles, nfirst), Af,
                        tiles_view(m->far_tiles, ffirst), fcount);
@@ -301,7 +319,7 @@ static void launch_pairs_t(rpb_mesh* m, const PairArgs& An, const PairArgs& Af, 
         if (t.valid) {
             int first, count;
             shard_tiles(t, shard, m->shards, first, count);
-            const size_t smem = pair_tile_smem(t.max_union, false);
+            const size_t smem = pair_tile_smem(t.max_union, false, t.max_entries);
             if (count > 0)
                 launch_pdl(diff ? k_tp0_pairs_tiled<false, QH, PH, true> : k_tp0_pairs_tiled<false, QH, PH, false>, count,
                            PAIR_TILE_THREADS, smem, m->stream, An, tiles_view(t, first));
@@ -314,7 +332,7 @@ static void launch_pairs_t(rpb_mesh* m, const PairArgs& An, const PairArgs& Af, 
         if (t.valid) {
             int first, count;
             shard_tiles(t, shard, m->shards, first, count);
-            const size_t smem = pair_tile_smem(t.max_union, true);
+            const size_t smem = pair_tile_smem(t.max_union, true, t.max_entries);
             if (count > 0)
                 launch_pdl(diff ? k_tp0_pairs_tiled<true, QH, PH, true> : k_tp0_pairs_tiled<true, QH, PH, false>, count,
                            PAIR_TILE_THREADS, smem, m->stream, Af, tiles_view(t, first));
@@ -389,8 +407,7 @@ rpb_status launch_collect_gather(rpb_mesh* m, double alpha, double beta, double*
     C.D_far = D_far ? D_far : m->D_far.ptr;
     C.D_vf = D_vf;
     C.B = m->B.ptr;
-    launch_pdl(k_collect_chain, static_cast<int>((static_cast<int64_t>(m->N) * COLLECT_LANES + 255) / 256), 256, 0,
-               m->stream, C);
+    launch_pdl(k_collect_chain, (m->N + 255) / 256, 256, 0, m->stream, C);
     RPB_CUDA(cudaGetLastError());
     GatherArgs G;
     G.nV = m->nV;

@@ -78,6 +78,7 @@ struct TileBufs {
     DevBuf<uint16_t> slot;
     std::vector<int> row0_host;   // tiles + 1: first row of each tile
     int tiles = 0, max_union = 0;
+    int64_t max_entries = 0;      // most entries in one tile
     bool valid = false;
 };
 
@@ -117,8 +118,7 @@ struct rpb_mesh {
     rpb::DevBuf<double> Y;
     rpb::DevBuf<double> block_energy, energy;   // energy[0] near, [1] far, [2] very near
     rpb::DevBuf<unsigned> done;                 // last-block counters: [0] near, [1] far pairs,
-                                                // [2] the geometry kernel's, [3] the metric
-                                                // Pre kernel's block scan
+                                                // [3] the metric Pre kernel's block scan
     int near_blocks = 0, far_blocks = 0;
     int shards = 1;                             // row shards the tiles are grouped for
     int64_t last_step_candidates = 0;           // candidate pairs of the last MaximumSafeStepSize

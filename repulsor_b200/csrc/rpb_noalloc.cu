@@ -138,7 +138,6 @@ extern "C" rpb_status rpb_tpe0_value_noalloc(int dom_dim, const double* V, int64
     g.dom = dom_dim; g.N = N; g.NC = NC;
     g.V = V; g.S = S; g.charge_v = nullptr; g.perm = perm; g.C_begin = C_begin; g.C_end = C_end;
     g.P_pair = P_pair; g.C_pair = C_pair; g.C_mom = nullptr; g.local = local; g.blocks = blocks;
-    g.scan_done = nullptr;
     const int nb = (N + SCAN_BLOCK - 1) / SCAN_BLOCK;
     k_geometry_prims<<<nb, SCAN_BLOCK, 0, s>>>(g);
     k_scan_rows<10><<<1, SCAN_BLOCK, 0, s>>>(blocks, nb);

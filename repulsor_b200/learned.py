@@ -2,8 +2,10 @@
 
 The network (16 -> 64 -> 64 -> 3, GELU, BF16 weights with FP32 accumulation) lives on
 the device and is trained there by the library's own forward/backward/Adam kernels
-(``rpb_mlp_*`` in include/repulsor_b200.h) on (residual, solve-correction) pairs that
-plain CG solves of the metric produce:
+(``rpb_mlp_*`` in include/repulsor_b200.h), either by the unrolled-CG loss
+(``train_unrolled``: the energy functional after K preconditioned CG iterations,
+differentiated through the CG recurrences) or on (residual, solve-correction) pairs that
+plain CG solves of the metric produce (``train``):
 
     for a right-hand side b with exact solution x* = A^{-1} b (a tight plain CG solve)
     and a CG iterate x_k, the pair is r_k = b - A x_k and e_k = x* - x_k, so that
@@ -23,7 +25,7 @@ from . import _capi
 from ._capi import PRECOND_NONE, RepulsorError, check, dptr, fptr
 
 __all__ = ["LearnedPreconditioner", "training_pairs", "train", "unrolled_sensitivities", "train_unrolled",
-           "NPARAM_OUTPUT_OFFSET"]
+           "slow_residual", "NPARAM_OUTPUT_OFFSET"]
 
 # offset of the output layer (W3, b3) in the parameter vector: W1 64x16, b1 64, W2 64x64, b2 64
 NPARAM_OUTPUT_OFFSET = 64 * 16 + 64 + 64 * 64 + 64
@@ -284,6 +286,21 @@ def unrolled_sensitivities(net, M, metric, b, steps=30, loss="energy"):
         pbar_next = pbar
     zbar[0] += pbar_next            # p_0 = z_0
     return value, np.stack(r[:steps]), np.stack(zbar)
+
+
+def slow_residual(net, M, metric, b, iterations):
+    """The residual b - A x after `iterations` flexible-CG steps from x = 0 with the
+    preconditioner `net`, scaled to unit norm. Its error lies in the modes that the
+    preconditioned solve resolves last, which set the iteration count to a tight tolerance;
+    as a training right-hand side it points the unrolled loss at them."""
+    from ._capi import PRECOND_LEARNED
+
+    net.attach(M)
+    b = np.ascontiguousarray(b, dtype=np.float64)
+    X = metric.Solve(M, 1.0, b, max_iter=iterations, tolerance=1e-30, precond=PRECOND_LEARNED, strict=False)
+    r = b - metric.MultiplyMetric(M, 1.0, X)
+    r -= r.mean(axis=0)
+    return r / np.linalg.norm(r)
 
 
 def train_unrolled(net, metric, meshes_rhs, epochs=1, lr=1e-3, steps=30, reg=1e-3, seed=0, log=None, loss="energy"):

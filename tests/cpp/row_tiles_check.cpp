@@ -1,9 +1,8 @@
 // Invariants of build_row_tiles on seeded random banded symmetric patterns: tiles cover
 // the rows in order and stay within the row, entry and union bounds, every union is
 // sorted and unique, every entry's slot names its column, each tile's order is a
-// permutation of its rows, and the lane map gives every row one group of consecutive
-// lanes inside a warp (each lane at most once, group size 1..32), the smallest group that
-// keeps the row's lanes within the tile's largest per-lane entry count. A row longer than
+// permutation of its rows, and the lane map gives every row one aligned power-of-two
+// group inside a warp (each lane at most once), smaller than twice its row. A row longer than
 // the cap disables the tiles. Prints "ok" or the first violation.
 #include <algorithm>
 #include <cstdio>
@@ -64,24 +63,22 @@ static int check(int rows, int band, int lanes, int cap, int threads, unsigned s
             const int q = m >> 10, size = ((m >> 5) & 31) + 1, sub = m & 31;
             if (q >= r1 - r0 || sub >= size) { std::printf("tile %d lane %d map\n", b, t); return 1; }
             const int start = t - sub;
-            if (start / 32 != (start + size - 1) / 32) { std::printf("tile %d group straddles a warp\n", b); return 1; }
+            if ((size & (size - 1)) != 0 || start % size != 0 || start / 32 != (start + size - 1) / 32) {
+                std::printf("tile %d group alignment\n", b);
+                return 1;
+            }
             if (group_size[q] == 0) group_size[q] = size;
             else if (group_size[q] != size) { std::printf("tile %d group size\n", b); return 1; }
             group_lanes[q] += int64_t(1) << sub;   // each lane of the group exactly once
         }
-        int64_t per_lane = 0;
         for (int q = 0; q < r1 - r0; ++q) {
             if (group_size[q] == 0 || group_lanes[q] != static_cast<int64_t>((1ull << group_size[q]) - 1)) {
                 std::printf("tile %d row %d lanes\n", b, q);
                 return 1;
             }
             const int64_t len = rp[T.order[r0 + q] + 1] - rp[T.order[r0 + q]];
-            per_lane = std::max(per_lane, (len + group_size[q] - 1) / group_size[q]);
-        }
-        for (int q = 0; q < r1 - r0; ++q) {
-            const int64_t len = rp[T.order[r0 + q] + 1] - rp[T.order[r0 + q]];
-            if (group_size[q] > 1 && (len + group_size[q] - 2) / (group_size[q] - 1) <= per_lane) {
-                std::printf("tile %d row %d group larger than needed\n", b, q);
+            if (group_size[q] > 1 && group_size[q] >= 2 * len) {
+                std::printf("tile %d row %d group twice its row\n", b, q);
                 return 1;
             }
         }

@@ -1,7 +1,8 @@
 """Learned preconditioner on the GPU against the CPU oracle (oracle/learned_oracle.py):
 the MLP forward/backward kernels, the preconditioner application, the training
-gradient through the whole chain (including the metric product), and the gain of the
-trained network in flexible CG over plain CG on the same mesh."""
+gradients (one-step pairs and unrolled-CG sensitivities) through the whole chain
+(including the metric product), and flexible CG with the trained network on a held-out
+mesh against plain CG, the untrained operator and the reference preconditioner."""
 import numpy as np
 import pytest
 
@@ -9,7 +10,7 @@ import oracle
 import repulsor_b200 as rpb
 from oracle import learned_oracle as LO
 from repulsor_b200 import meshes
-from repulsor_b200.learned import LearnedPreconditioner, train, training_pairs
+from repulsor_b200.learned import LearnedPreconditioner, training_pairs
 
 pytestmark = pytest.mark.gpu
 
@@ -129,37 +130,56 @@ def test_sensitivity_training_gradient_matches_oracle(surface):
     np.testing.assert_array_equal(net.get_params(), th)     # lr = 0: no step
 
 
-def test_trained_network_beats_plain_cg(surface):
-    """Train on pairs from plain CG solves on the mesh, then solve a held-out right-hand
-    side: flexible CG with the trained network needs far fewer iterations than plain CG
-    to the same 1e-6 true residual (checked with the oracle's FP64 metric product). The
-    untrained multilevel operator (all gains 1) is reported beside it; training may move
-    the count by a few per cent either way, but must not lose the multilevel gain."""
-    V, S, M, om, G = surface
+def test_learned_preconditioner_on_a_held_out_mesh():
+    """Train by the unrolled-CG energy loss on four level-4 meshes (two right-hand sides
+    each), then solve on a held-out level-5 mesh of the same family (another seed) to the
+    1e-6 true residual (the trained solve checked with the oracle's FP64 metric product).
+    The learned operator's multilevel structure is what gains: flexible CG with it, trained
+    or untrained (every gain 1), needs at most 40 % of plain CG's iterations, and the
+    trained network's solve beats CG with the reference preconditioner in wall-clock (its
+    H1 factorization not even counted). Training itself is held to not losing that gain:
+    at most 15 % more iterations than the untrained operator (measured on levels 5-7 it
+    moves the count by +4 to +10 %)."""
+    import time
+
+    from repulsor_b200.learned import train_unrolled
+
     tpm = rpb.TangentPointMetric0(Q, P)
-    R, E = training_pairs(M, tpm, n_rhs=4, checkpoints=(0, 4, 16, 48, 128), seed=100)
-    b = meshes.random_rhs(V.shape[0], seed=7, project=True)
-
-    tpm.Solve(M, 1.0, b, max_iter=20000, tolerance=1e-6, precond=rpb.PRECOND_NONE)
-    it_plain = tpm.Solver_IterationCount()
-
+    samples = []
+    for seed in (61, 62, 63, 64):
+        Vt, St = meshes.icosphere_sh(level=4, seed=seed)
+        Mt = rpb.SimplicialMesh(Vt, St)
+        samples += [(Mt, meshes.random_rhs(Vt.shape[0], seed=10 * seed + j)) for j in range(2)]
     net = LearnedPreconditioner(seed=3)
-    zero = net.get_params()
-    zero[LO.OFF_W3:] = 0.0                          # untrained multilevel operator: gains 1
-    net.set_params(zero)
-    net.attach(M)
-    tpm.Solve(M, 1.0, b, max_iter=20000, tolerance=1e-6, precond=rpb.PRECOND_LEARNED)
-    it_prior = tpm.Solver_IterationCount()
+    th = net.get_params()
+    th[LO.OFF_W3:] = 0.0                            # start from the multilevel operator
+    net.set_params(th)
+    prior = LearnedPreconditioner(params=th.copy())
+    hist = train_unrolled(net, tpm, samples, epochs=1, lr=3e-4, steps=30, seed=0)
+    assert np.all(np.isfinite(hist))
 
-    net = LearnedPreconditioner(seed=3)
-    hist = train(net, tpm, [(M, R, E)], epochs=40, lr=1e-3, batch=4, seed=0)
-    assert hist[-1] < hist[0]
-    net.attach(M)
-    X = tpm.Solve(M, 1.0, b, max_iter=20000, tolerance=1e-6, precond=rpb.PRECOND_LEARNED)
-    it_learned = tpm.Solver_IterationCount()
+    V, S = meshes.icosphere_sh(level=5, seed=71)
+    M = rpb.SimplicialMesh(V, S)
+    om = oracle.OracleMesh(2, V, S, threads=8)
+    b = meshes.random_rhs(V.shape[0], seed=71, project=True)
+
+    def solve(pc, n=None):
+        if n is not None:
+            n.attach(M)
+        tpm.Solve(M, 1.0, b, max_iter=20000, tolerance=1e-6, precond=pc)      # warm-up
+        t = time.perf_counter()
+        X = tpm.Solve(M, 1.0, b, max_iter=20000, tolerance=1e-6, precond=pc)
+        return X, tpm.Solver_IterationCount(), time.perf_counter() - t
+
+    _, it_plain, _ = solve(rpb.PRECOND_NONE)
+    _, it_prior, _ = solve(rpb.PRECOND_LEARNED, prior)
+    X, it_learned, t_learned = solve(rpb.PRECOND_LEARNED, net)
+    _, it_ref, t_ref = solve(rpb.PRECOND_REFERENCE)
     rel = np.linalg.norm(b - om.metric_multiply(X, q=Q, p=P), axis=0) / np.linalg.norm(b, axis=0)
-    print(f"iterations: plain CG {it_plain}, untrained multilevel {it_prior}, learned FCG {it_learned}; "
-          f"loss {hist[0]:.4f} -> {hist[-1]:.4f}")
+    print(f"held-out level 5: plain CG {it_plain}, untrained multilevel FCG {it_prior}, trained FCG "
+          f"{it_learned} ({1e3 * t_learned:.0f} ms), reference-preconditioned CG {it_ref} ({1e3 * t_ref:.0f} ms)")
     assert rel.max() <= 2e-6
-    assert it_learned <= 0.6 * it_plain
-    assert it_learned <= 1.2 * it_prior
+    assert it_prior <= 0.4 * it_plain
+    assert it_learned <= 0.4 * it_plain
+    assert it_learned <= 1.15 * it_prior
+    assert t_learned < t_ref
