@@ -71,6 +71,27 @@ def pair_traffic_from_profile():
     return int(m.group(1).replace(",", "")) if m else None
 
 
+def stage_rooflines(st, ms):
+    """HBM roofline of the two non-pair stages of a step (triangles): algorithmic bytes,
+    each array read or written once, divided by the stage's CUDA-event time.
+    geometry + upsweep: perm, simplices, coordinates and the written primitive data and
+    in-block prefix rows, then the prefix rows read back, the cluster ranges and the
+    written cluster data: N (4 + 12 + 64 + 80 + 80) + nV 24 + NC (8 + 64) bytes.
+    collection + gather: perm, simplices, coordinates, leaf index, near rows, far rows, the
+    clusters' data and tree links, the written and re-read per-corner derivatives, the
+    vertex-to-corner lists and the output: N (4 + 12 + 4 + 80 + 72 + 72 + 12) +
+    NC (80 + 64 + 8) + nV (24 + 4 + 24) bytes."""
+    N, NC, nV = st["simplex_count"], st["cluster_count"], st["vertex_count"]
+    peak = measured_hbm_gbs()
+    out = {}
+    for name, nbytes, t in (("geometry_upsweep", N * 240 + nV * 24 + NC * 72, ms[0]),
+                            ("collect_chain_gather", N * 256 + NC * 152 + nV * 52, ms[3])):
+        gbs = nbytes / (t * 1e-3) / 1e9
+        out[name] = {"bytes": nbytes, "ms": t, "achieved_gbs": gbs, "peak_gbs": peak,
+                     "frac": gbs / peak if peak else None}
+    return out
+
+
 def measured_hbm_gbs():
     """HBM copy bandwidth measured on this pool's B200s (MEASURED_PEAKS.json), else the
     pool's earlier measurement."""
@@ -356,7 +377,8 @@ def main():
                                    "has no FP32 figure",
                     "flops_per_evaluation": flops,
                     "stage_ms": {"geometry_upsweep": ms[0], "near_pairs": ms[1], "far_pairs": ms[2],
-                                 "collect_chain_gather": ms[3], "total": ms[4]}}
+                                 "collect_chain_gather": ms[3], "total": ms[4]},
+                    "stages": stage_rooflines(st, ms)}
         out = {"metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": world, "steps": args.steps,
                "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
                "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
