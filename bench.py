@@ -241,6 +241,8 @@ def main():
     ap.add_argument("--learned-heldout", type=int, default=32, help="held-out meshes (32)")
     ap.add_argument("--learned-steps", type=int, default=30, help="unrolled CG iterations of the training loss")
     ap.add_argument("--learned-lr", type=float, default=1e-3, help="Adam learning rate")
+    ap.add_argument("--learned-hybrid", action="store_true",
+                    help="train the network as the learned part of the hybrid preconditioner P_ref + w M")
     ap.add_argument("--learned-hard", type=int, default=0,
                     help="train on the residuals left after this many flexible-CG iterations with the untrained "
                          "operator (repulsor_b200.learned.slow_residual) instead of N(0,1) right-hand sides")
@@ -493,8 +495,9 @@ def run_learned(args):
     args.learned_rhs N(0,1) right-hand sides each, by the unrolled-CG energy loss, and
     evaluated on args.learned_heldout held-out meshes (the same family, other seeds) by
     iterations and ms to the 1e-6 true residual: flexible CG with the trained network,
-    the same with the untrained multilevel operator (every gain 1), plain CG, and CG with
-    the reference preconditioner (its H1 factorization timed apart). Training time is
+    the same with the untrained multilevel operator (every gain 1), plain CG, CG with the
+    reference preconditioner (its H1 factorization timed apart), and flexible CG with the
+    hybrid preconditioner (reference plus network) for both networks. Training time is
     reported separately. One JSON line."""
     import numpy as np
     import torch
@@ -521,7 +524,8 @@ def run_learned(args):
         if args.learned_hard > 0:
             samples = [(M, slow_residual(prior, M, tpm, rhs, args.learned_hard)) for _, rhs in samples]
         setup_s += time.perf_counter() - ts
-        losses += train_unrolled(net, tpm, samples, epochs=1, lr=args.learned_lr, steps=args.learned_steps, seed=i)
+        losses += train_unrolled(net, tpm, samples, epochs=1, lr=args.learned_lr, steps=args.learned_steps, seed=i,
+                                 hybrid=args.learned_hybrid)
         del M, samples
     train_s = time.perf_counter() - t0 - setup_s
     rows = []
@@ -531,7 +535,9 @@ def run_learned(args):
         b = meshes.random_rhs(V.shape[0], seed=9000 + j)
         row = {"level": levels[j % 3], "seed": 9000 + j}
         for name, pc, n in (("plain_cg", rpb.PRECOND_NONE, None), ("untrained_fcg", rpb.PRECOND_LEARNED, prior),
-                            ("trained_fcg", rpb.PRECOND_LEARNED, net), ("reference_cg", rpb.PRECOND_REFERENCE, None)):
+                            ("trained_fcg", rpb.PRECOND_LEARNED, net), ("reference_cg", rpb.PRECOND_REFERENCE, None),
+                            ("untrained_hybrid_fcg", rpb.PRECOND_HYBRID, prior),
+                            ("trained_hybrid_fcg", rpb.PRECOND_HYBRID, net)):
             if n is not None:
                 n.attach(M)
             if pc == rpb.PRECOND_REFERENCE:
@@ -548,6 +554,9 @@ def run_learned(args):
         rows.append(row)
         del M
 
+    SOLVERS = ("plain_cg", "untrained_fcg", "trained_fcg", "reference_cg", "untrained_hybrid_fcg",
+               "trained_hybrid_fcg")
+
     def mean(name, key, lvl=None):
         v = [r[name][key] for r in rows if lvl is None or r["level"] == lvl]
         return float(np.mean(v)) if v else None
@@ -555,19 +564,18 @@ def run_learned(args):
     summary = {name: {"iterations": mean(name, "iterations"), "ms": mean(name, "ms"),
                       "per_level": {lvl: {"iterations": mean(name, "iterations", lvl), "ms": mean(name, "ms", lvl)}
                                     for lvl in levels}}
-               for name in ("plain_cg", "untrained_fcg", "trained_fcg", "reference_cg")}
+               for name in SOLVERS}
     out = {"metric": "learned preconditioner: held-out solve iterations and ms to 1e-6 true residual", "unit": "ms",
            "workload": f"icosphere_sh levels 5-7: {args.learned_train} training meshes x {args.learned_rhs} RHS "
                        f"(seeds 5000+), {args.learned_heldout} held-out meshes (seeds 9000+), q=6 p=12 theta=0.5",
            "training": {"loss": f"unrolled CG energy, K = {args.learned_steps} iterations", "lr": args.learned_lr,
+                        "preconditioner_trained": "hybrid P_ref + w M" if args.learned_hybrid else "M alone",
                         "rhs": (f"residuals after {args.learned_hard} untrained flexible-CG iterations"
                                 if args.learned_hard > 0 else "N(0,1), mean-free"),
                         "samples": args.learned_train * args.learned_rhs, "training_s": train_s,
                         "mesh_setup_s": setup_s, "loss_first_mesh": float(np.mean(losses[:args.learned_rhs])),
                         "loss_last_mesh": float(np.mean(losses[-args.learned_rhs:]))},
-           "summary": summary, "all_converged": all(r[n]["rel_residual"] <= 1e-6 for r in rows
-                                                   for n in ("plain_cg", "untrained_fcg", "trained_fcg",
-                                                             "reference_cg")),
+           "summary": summary, "all_converged": all(r[n]["rel_residual"] <= 1e-6 for r in rows for n in SOLVERS),
            "held_out": rows}
     print(json.dumps(out))
     return 0
@@ -575,9 +583,10 @@ def run_learned(args):
 
 def solve_extras(rpb, M, tpm, V):
     """Solve to 1e-6 relative residual on the icosphere level-6 mesh: plain CG, CG with the
-    reference preconditioner, and flexible CG with the multilevel operator before and after
+    reference preconditioner, flexible CG with the multilevel operator before and after
     training (train_learned_small: unrolled-CG energy loss on GPU, training time reported
-    separately). The reference preconditioner's H1 factorization (host Cholesky and upload,
+    separately), and flexible CG with the hybrid (reference preconditioner plus the trained
+    network's output; its H1 factorization is already in place). The reference preconditioner's H1 factorization (host Cholesky and upload,
     cached until the geometry changes) is timed apart as setup_ms; its ms is the Solve with
     the factor in place."""
     from repulsor_b200 import meshes
@@ -590,10 +599,11 @@ def solve_extras(rpb, M, tpm, V):
     for name, pc, max_iter in (("plain_cg", rpb.PRECOND_NONE, 20000),
                                ("multilevel_prior_fcg", rpb.PRECOND_LEARNED, 20000),
                                ("learned_fcg", rpb.PRECOND_LEARNED, 20000),
-                               ("reference_precond_cg", rpb.PRECOND_REFERENCE, 2000)):
+                               ("reference_precond_cg", rpb.PRECOND_REFERENCE, 2000),
+                               ("hybrid_fcg", rpb.PRECOND_HYBRID, 2000)):
         if name == "multilevel_prior_fcg":
             prior.attach(M)
-        elif name == "learned_fcg":
+        elif name in ("learned_fcg", "hybrid_fcg"):
             net.attach(M)
         setup_ms = None
         if pc == rpb.PRECOND_REFERENCE:
@@ -619,10 +629,13 @@ def run_flow(args):
     """Full flow step at scale: two linked tori (R=1, r=0.3, 480 x 640 grids, 1,228,800
     triangles) with an icosphere level-5 obstacle of radius 0.3 at (0, 0, 2): energy +
     differential (TangentPointEnergy0 + TangentPointObstacleEnergy), the metric Solve of the
-    differential to 1e-6 by learned-preconditioned flexible CG (network trained on seeded
-    icospheres, time reported separately) with the reference preconditioner as fallback,
-    and the collision-free step size along the solution (MaximumSafeStepSize). One step;
-    times are wall clock around each public call."""
+    differential to 1e-6 by flexible CG with the hybrid preconditioner (the reference
+    preconditioner plus the learned network's output; network trained on seeded icospheres,
+    time reported separately) with the reference preconditioner alone as fallback, and the
+    collision-free step size along the solution (MaximumSafeStepSize). One step; times are
+    wall clock around each public call. With the learned operator alone the flexible CG
+    stalls near iteration 860 and falls back; with the reference preconditioner alone the
+    solve takes 67,140 iterations."""
     import numpy as np
     import torch
 
@@ -630,7 +643,7 @@ def run_flow(args):
     from repulsor_b200 import meshes
 
     torch.cuda.set_device(0)
-    out = {"metric": "full flow step (energy+grad, learned FCG solve to 1e-6)", "unit": "s",
+    out = {"metric": "full flow step (energy+grad, hybrid learned FCG solve to 1e-6)", "unit": "s",
            "workload": "two linked tori 480x640 (614,400 vertices, 1,228,800 triangles) + icosphere L5 obstacle "
                        "r=0.3 at (0,0,2), q=6 p=12 theta=0.5"}
     t = time.perf_counter()
@@ -657,7 +670,7 @@ def run_flow(args):
     net.attach(M)
     B = D - D.mean(0)
     t = time.perf_counter()
-    X = tpm.Solve(M, 1.0, B, max_iter=args.flow_max_iter, tolerance=1e-6, precond=rpb.PRECOND_LEARNED, strict=False)
+    X = tpm.Solve(M, 1.0, B, max_iter=args.flow_max_iter, tolerance=1e-6, precond=rpb.PRECOND_HYBRID, strict=False)
     out["solve_s"] = time.perf_counter() - t
     # the flow's next call: the collision-free step along the descent direction -X, scaled so
     # that the fastest vertex moves by at most the mean edge length at t = 1

@@ -166,7 +166,10 @@ rpb_status rpb_tpm0_precondition(rpb_mesh* m, double q, double p, double alpha, 
 typedef enum rpb_precond {
     RPB_PRECOND_NONE = 0,        /* plain CG */
     RPB_PRECOND_REFERENCE = 1,   /* H1^{-1} L_{2-s} H1^{-1} (the reference's preconditioner) */
-    RPB_PRECOND_LEARNED = 2      /* per-cluster MLP in flexible CG, falls back to REFERENCE on stall */
+    RPB_PRECOND_LEARNED = 2,     /* per-cluster MLP in flexible CG, falls back to REFERENCE on stall */
+    RPB_PRECOND_HYBRID = 3       /* flexible CG with z = P_ref r + w M(r): the reference preconditioner
+                                    plus the attached network's output, w = (r0, P_ref r0) / (2 (r0, M r0))
+                                    on the first residual; falls back to REFERENCE on stall */
 } rpb_precond;
 
 /* MetricBase::Solve (src/Metrics/MetricDimRestricted.hpp:232-289):

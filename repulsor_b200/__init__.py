@@ -24,8 +24,8 @@ import numpy as np
 
 from . import _capi
 from .meshio import read_mesh_file, write_mesh_file
-from ._capi import (PRECOND_LEARNED, PRECOND_NONE, PRECOND_REFERENCE, RepulsorError, Settings, Stats, check,
-                    dptr, iptr, lptr)
+from ._capi import (PRECOND_HYBRID, PRECOND_LEARNED, PRECOND_NONE, PRECOND_REFERENCE, RepulsorError, Settings, Stats,
+                    check, dptr, iptr, lptr)
 
 __all__ = [
     "SimplicialMesh",
@@ -43,6 +43,7 @@ __all__ = [
     "PRECOND_NONE",
     "PRECOND_REFERENCE",
     "PRECOND_LEARNED",
+    "PRECOND_HYBRID",
     "default_settings",
 ]
 

@@ -16,7 +16,7 @@ RPB_OK, RPB_EINVAL, RPB_ENOTCONV, RPB_ESTALL, RPB_ECUDA, RPB_ENOMEM, RPB_ETIMEOU
 STATUS_NAMES = {0: "RPB_OK", 1: "RPB_EINVAL", 2: "RPB_ENOTCONV", 3: "RPB_ESTALL", 4: "RPB_ECUDA",
                 5: "RPB_ENOMEM", 6: "RPB_ETIMEOUT"}
 
-PRECOND_NONE, PRECOND_REFERENCE, PRECOND_LEARNED = 0, 1, 2
+PRECOND_NONE, PRECOND_REFERENCE, PRECOND_LEARNED, PRECOND_HYBRID = 0, 1, 2, 3
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int)

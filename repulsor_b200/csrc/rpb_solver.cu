@@ -329,7 +329,7 @@ __global__ void __launch_bounds__(SN_BLOCK) k_sn_split_dense(SnTri A, const int*
 //   S_RZ rz, S_RZOLD previous rz, S_PAP (p,Ap), S_RR (r,r), S_ZR_OLD (z, r_old)
 // ------------------------------------------------------------------------------------------
 enum { S_RZ = 0, S_RZOLD = 3, S_PAP = 6, S_RR = 9, S_ZROLD = 12, S_ACTIVE = 15, S_BB = 18, S_CONV_IT = 21, S_IT = 24,
-       S_COUNT = 25 };
+       S_HYB_W = 25, S_COUNT = 26 };
 
 struct DotArgs {
     int n;                    // rows (n x 3)
@@ -492,6 +492,16 @@ __global__ void k_cg_check(double* S, double tol2, bool rz_is_rr)
         S[S_RZOLD + c] = S[S_RZ + c];
         if (rz_is_rr) S[S_RZ + c] = S[S_RR + c];
     }
+}
+
+// y += w x over n x 3 values, w read from the device (the hybrid preconditioner's weight,
+// fixed for a solve, so that captured iterations replay with it)
+__global__ void k_add_weighted3(int n, const double* w, const double* x, double* y)
+{
+    const double a = *w;
+    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < 3 * static_cast<int64_t>(n);
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        y[i] += a * x[i];
 }
 
 __global__ void k_axpby3(int n, double alpha, const double* x, double beta, double* y, int ldy)
@@ -743,7 +753,7 @@ static rpb_status cg_solve(rpb_mesh* m, double q, double p, const double* B, int
     double* S = s.scal.ptr;
     cudaStream_t stream = m->stream;
     const int eb = (n + 255) / 256;
-    const bool flexible = (precond == RPB_PRECOND_LEARNED);
+    const bool flexible = (precond == RPB_PRECOND_LEARNED || precond == RPB_PRECOND_HYBRID);
     // iterations without a 10% drop of the best residual that count as a stall
     constexpr int kStallWindow = 500;
     // iterations per captured graph between host checks of the residuals
@@ -809,9 +819,27 @@ static rpb_status cg_solve(rpb_mesh* m, double q, double p, const double* B, int
             if (active[c] != 0.0) done = false;
         }
         if (done || it >= max_iter) break;
-        if (stalled_flag && kind == RPB_PRECOND_LEARNED) {
+        if (stalled_flag && (kind == RPB_PRECOND_LEARNED || kind == RPB_PRECOND_HYBRID)) {
             kind = RPB_PRECOND_REFERENCE;  // fallback on stall
             s.last_fallback_iteration = it;
+        }
+        if (kind == RPB_PRECOND_HYBRID && restarts == 0) {
+            // the weight of the learned operator: half the ratio of the two parts' energies on
+            // the first residual, (r, P_ref r) / (r, M r) / 2 over the three columns
+            double* zr = s.vec.ptr + Solver::V_HYB * n3;
+            if ((st = reference_precondition(m, q, p, r, z)) != RPB_OK) { drop_graph(); return st; }
+            if ((st = learned_precondition(m, q, p, r, zr)) != RPB_OK) { drop_graph(); return st; }
+            if ((st = dot3(m, r, z, nullptr, S + S_RZ, nullptr)) != RPB_OK) { drop_graph(); return st; }
+            if ((st = dot3(m, r, zr, nullptr, S + S_PAP, nullptr)) != RPB_OK) { drop_graph(); return st; }
+            if ((st = read_scalars(m)) != RPB_OK) { drop_graph(); return st; }
+            double er = 0.0, el = 0.0;
+            for (int c = 0; c < 3; ++c) {
+                er += s.host_scal[S_RZ + c];
+                el += s.host_scal[S_PAP + c];
+            }
+            const double w = (el > 0.0 && er > 0.0) ? 0.5 * er / el : 0.0;
+            RPB_CUDA(cudaMemcpyAsync(S + S_HYB_W, &w, sizeof(double), cudaMemcpyHostToDevice, stream));
+            RPB_CUDA(cudaStreamSynchronize(stream));
         }
         stalled_flag = false;
         ++restarts;
@@ -863,7 +891,9 @@ static rpb_status cg_solve(rpb_mesh* m, double q, double p, const double* B, int
             // stall detection only guards the flexible (learned) iteration, which then falls
             // back to the reference preconditioner; fixed-preconditioner CG is never restarted
             since_best += batch;
-            if (flexible && kind == RPB_PRECOND_LEARNED && !conv && since_best > kStallWindow) stalled = true;
+            if (flexible && (kind == RPB_PRECOND_LEARNED || kind == RPB_PRECOND_HYBRID) && !conv &&
+                since_best > kStallWindow)
+                stalled = true;
             if (conv || stalled) {
                 stalled_flag = stalled;
                 since_best = 0;
@@ -895,6 +925,18 @@ rpb_status apply_preconditioner(rpb_mesh* m, int kind, double q, double p, const
         return RPB_OK;
     }
     if (kind == RPB_PRECOND_LEARNED) return learned_precondition(m, q, p, R, Z);
+    if (kind == RPB_PRECOND_HYBRID) {
+        // Z = P_ref R + w M(R), w fixed at the solve's start (S_HYB_W)
+        Solver& s = *m->solver;
+        const int n = m->nV;
+        double* T = s.vec.ptr + Solver::V_HYB * 3 * static_cast<size_t>(n);
+        rpb_status st;
+        if ((st = reference_precondition(m, q, p, R, Z)) != RPB_OK) return st;
+        if ((st = learned_precondition(m, q, p, R, T)) != RPB_OK) return st;
+        k_add_weighted3<<<std::min(1184, (3 * n + 255) / 256), 256, 0, m->stream>>>(n, s.scal.ptr + S_HYB_W, T, Z);
+        RPB_CUDA(cudaGetLastError());
+        return RPB_OK;
+    }
     return reference_precondition(m, q, p, R, Z);
 }
 
@@ -941,7 +983,7 @@ rpb_status rpb_tpm0_solve(rpb_mesh* m, double q, double p, double alpha, const d
         return RPB_EINVAL;
     }
     if (ldB < 3 || ldX < 3) { set_error("leading dimensions must be >= 3"); return RPB_EINVAL; }
-    if (precond < RPB_PRECOND_NONE || precond > RPB_PRECOND_LEARNED) { set_error("unknown preconditioner kind"); return RPB_EINVAL; }
+    if (precond < RPB_PRECOND_NONE || precond > RPB_PRECOND_HYBRID) { set_error("unknown preconditioner kind"); return RPB_EINVAL; }
     if (!(tol > 0) || max_iter < 0) { set_error("tolerance must be positive and max_iter >= 0"); return RPB_EINVAL; }
     rpb_status st = check_exponents(q, p);
     if (st != RPB_OK) return st;

@@ -12,7 +12,7 @@ struct LearnedState;
 struct Solver {
     ~Solver();
     // CG vectors, each n x 3 FP64
-    enum { V_X = 0, V_R, V_Z, V_P, V_AP, V_ROLD, V_B, V_PRE, NVEC };
+    enum { V_X = 0, V_R, V_Z, V_P, V_AP, V_ROLD, V_B, V_PRE, V_HYB, NVEC };
     DevBuf<double> vec;
     DevBuf<double> scal;          // per-column CG scalars
     DevBuf<double> partials;      // block partials of the dot products

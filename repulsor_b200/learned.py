@@ -206,7 +206,7 @@ def _cdot(a, b):
     return np.einsum("ij,ij->j", a, b)
 
 
-def unrolled_sensitivities(net, M, metric, b, steps=30, loss="energy"):
+def unrolled_sensitivities(net, M, metric, b, steps=30, loss="energy", hybrid=False, weight=None):
     """The loss of `steps` iterations of preconditioned CG with z = M(r) from x = 0, one CG
     per column, and its sensitivities to the preconditioner outputs, dL/dz_k, by the adjoint
     of the CG recurrences
@@ -218,11 +218,21 @@ def unrolled_sensitivities(net, M, metric, b, steps=30, loss="energy"):
     that r held fixed (apply_pair). loss = "energy": L = -sum_c log(-phi_c(x_K)) with
     phi(x) = x.Ax/2 - b.x = -x.(b + r)/2, the functional CG minimizes (phi(x_K) - phi(x*) is
     half the squared A-norm of the error); loss = "residual": L = sum_c log(|r_K,c|^2 / |b_c|^2).
+    hybrid: the preconditioner is z = P_ref r + w M(r) (RPB_PRECOND_HYBRID), P_ref the
+    reference preconditioner (linear, symmetric) and w = (b, P_ref b) / (2 (b, M b)) (or
+    `weight`) fixed for the solve; its adjoint adds P_ref to the frozen application.
     Returns (L, R, G): the residuals r_0 .. r_K-1 the preconditioner was applied to and the
-    sensitivities dL/dz_k, for train_step_sens."""
+    sensitivities of L to the network's outputs M(r_k), for train_step_sens."""
     b = np.ascontiguousarray(b, dtype=np.float64)
     A = lambda X: metric.MultiplyMetric(M, 1.0, X)
-    r, z, p, q = [b], [net.apply(M, b)], [], []
+    w = 1.0
+    if hybrid:
+        Pref = lambda X: metric.MultiplyPreconditioner(M, 1.0, X)
+        w = weight if weight is not None else 0.5 * float(np.sum(b * Pref(b))) / float(np.sum(b * net.apply(M, b)))
+        apply = lambda X: Pref(X) + w * net.apply(M, X)
+    else:
+        apply = lambda X: net.apply(M, X)
+    r, z, p, q = [b], [apply(b)], [], []
     p.append(z[0])
     g = [_cdot(r[0], z[0])]
     alpha, beta, delta = [], [], []
@@ -235,7 +245,7 @@ def unrolled_sensitivities(net, M, metric, b, steps=30, loss="energy"):
         rk1 = r[k] - ak * qk
         q.append(qk); delta.append(dk); alpha.append(ak); r.append(rk1)
         if k + 1 < steps:
-            zk1 = net.apply(M, rk1)
+            zk1 = apply(rk1)
             gk1 = _cdot(rk1, zk1)
             bk = gk1 / g[k]
             z.append(zk1); g.append(gk1); beta.append(bk)
@@ -265,9 +275,9 @@ def unrolled_sensitivities(net, M, metric, b, steps=30, loss="energy"):
             gbar_k = -bbar * g[k + 1] / g[k] ** 2
             rbar = rbar + gbar1 * z[k + 1]
             zbar[k + 1] += gbar1 * r[k + 1]
-            # z_k+1 = M(r_k+1), gains held fixed
+            # z_k+1 = M(r_k+1) (+ P_ref r_k+1), gains held fixed
             _, mz = net.apply_pair(M, r[k + 1], zbar[k + 1])
-            rbar = rbar + mz
+            rbar = rbar + (Pref(zbar[k + 1]) + w * mz if hybrid else mz)
         else:
             gbar_k = np.zeros(b.shape[1])
         # x_k+1 = x_k + alpha_k p_k; r_k+1 = r_k - alpha_k q_k; alpha_k = g_k / delta_k;
@@ -285,7 +295,7 @@ def unrolled_sensitivities(net, M, metric, b, steps=30, loss="energy"):
         zbar[k] += gbar_k * r[k]
         pbar_next = pbar
     zbar[0] += pbar_next            # p_0 = z_0
-    return value, np.stack(r[:steps]), np.stack(zbar)
+    return value, np.stack(r[:steps]), w * np.stack(zbar)
 
 
 def slow_residual(net, M, metric, b, iterations):
@@ -303,9 +313,11 @@ def slow_residual(net, M, metric, b, iterations):
     return r / np.linalg.norm(r)
 
 
-def train_unrolled(net, metric, meshes_rhs, epochs=1, lr=1e-3, steps=30, reg=1e-3, seed=0, log=None, loss="energy"):
+def train_unrolled(net, metric, meshes_rhs, epochs=1, lr=1e-3, steps=30, reg=1e-3, seed=0, log=None, loss="energy",
+                   hybrid=False):
     """Adam on the unrolled-CG loss: for every (mesh, right-hand side) pair in meshes_rhs,
-    the sensitivities of `steps` preconditioned CG iterations with the current network,
+    the sensitivities of `steps` preconditioned CG iterations with the current network (as
+    the whole preconditioner, or with hybrid as the learned part of z = P_ref r + w M(r)),
     then one step on them. Returns the mean loss per epoch (the loss of the network each
     pair was visited with)."""
     rng = np.random.default_rng(seed)
@@ -314,7 +326,7 @@ def train_unrolled(net, metric, meshes_rhs, epochs=1, lr=1e-3, steps=30, reg=1e-
         losses = []
         for i in rng.permutation(len(meshes_rhs)):
             M, b = meshes_rhs[i]
-            value, R, G = unrolled_sensitivities(net, M, metric, b, steps, loss)
+            value, R, G = unrolled_sensitivities(net, M, metric, b, steps, loss, hybrid)
             net.train_step_sens(M, R, G, lr=lr, reg=reg)
             losses.append(value)
         hist.append(float(np.mean(losses)))

@@ -79,3 +79,35 @@ def test_solve_reports_non_convergence():
     with pytest.raises(rpb.RepulsorError) as e:
         tpm.Solve(M, 1.0, B, max_iter=2, tolerance=1e-12, precond=rpb.PRECOND_NONE)
     assert "RPB_ENOTCONV" in str(e.value)
+
+
+def test_hybrid_preconditioner_on_linked_tori():
+    """RPB_PRECOND_HYBRID: flexible CG with z = P_ref r + w M(r), the reference
+    preconditioner plus the attached network's multilevel output (untrained: every gain
+    1), on two linked tori of 96 x 128 vertices each (49,152 triangles) with the energy's
+    differential as right-hand side. It reaches the 1e-6 true residual (checked with the
+    oracle's FP64 metric operator) in fewer iterations than CG with the reference
+    preconditioner alone (measured 870-920 against 1,463; on 192 x 256 tori 1,280-1,506
+    against 6,940)."""
+    from repulsor_b200.learned import NPARAM_OUTPUT_OFFSET, LearnedPreconditioner
+
+    V, S = meshes.linked_tori(n_major=96, n_minor=128)
+    M = rpb.SimplicialMesh(V, S)
+    tpm = rpb.TangentPointMetric0(Q, P)
+    D = rpb.TangentPointEnergy0(Q, P).Differential(M)
+    B = D - D.mean(0)
+    net = LearnedPreconditioner(seed=1)
+    th = net.get_params()
+    th[NPARAM_OUTPUT_OFFSET:] = 0.0
+    net.set_params(th)
+    net.attach(M)
+    tpm.Solve(M, 1.0, B, max_iter=6000, tolerance=1e-6, precond=rpb.PRECOND_REFERENCE)
+    it_ref = tpm.Solver_IterationCount()
+    X = tpm.Solve(M, 1.0, B, max_iter=6000, tolerance=1e-6, precond=rpb.PRECOND_HYBRID)
+    it_hyb = tpm.Solver_IterationCount()
+    assert tpm.SolveInfo(M)["fallback_iteration"] == -1
+    O = oracle.OracleMesh(2, V, S, threads=8)
+    rel = np.linalg.norm(B - O.metric_multiply(X, Q, P), axis=0) / np.linalg.norm(B, axis=0)
+    print(f"linked tori 96 x 128: reference CG {it_ref} iterations, hybrid FCG {it_hyb}")
+    assert rel.max() <= 5e-6
+    assert it_hyb <= 0.8 * it_ref
