@@ -168,7 +168,7 @@ typedef enum rpb_precond {
     RPB_PRECOND_REFERENCE = 1,   /* H1^{-1} L_{2-s} H1^{-1} (the reference's preconditioner) */
     RPB_PRECOND_LEARNED = 2,     /* per-cluster MLP in flexible CG, falls back to REFERENCE on stall */
     RPB_PRECOND_HYBRID = 3       /* flexible CG with z = P_ref r + w M(r): the reference preconditioner
-                                    plus the attached network's output, w = (r0, P_ref r0) / (2 (r0, M r0))
+                                    plus the attached network's output, w = (r0, P_ref r0) / (8 (r0, M r0))
                                     on the first residual; falls back to REFERENCE on stall */
 } rpb_precond;
 

@@ -219,7 +219,7 @@ def unrolled_sensitivities(net, M, metric, b, steps=30, loss="energy", hybrid=Fa
     phi(x) = x.Ax/2 - b.x = -x.(b + r)/2, the functional CG minimizes (phi(x_K) - phi(x*) is
     half the squared A-norm of the error); loss = "residual": L = sum_c log(|r_K,c|^2 / |b_c|^2).
     hybrid: the preconditioner is z = P_ref r + w M(r) (RPB_PRECOND_HYBRID), P_ref the
-    reference preconditioner (linear, symmetric) and w = (b, P_ref b) / (2 (b, M b)) (or
+    reference preconditioner (linear, symmetric) and w = (b, P_ref b) / (8 (b, M b)) (or
     `weight`) fixed for the solve; its adjoint adds P_ref to the frozen application.
     Returns (L, R, G): the residuals r_0 .. r_K-1 the preconditioner was applied to and the
     sensitivities of L to the network's outputs M(r_k), for train_step_sens."""
@@ -228,7 +228,7 @@ def unrolled_sensitivities(net, M, metric, b, steps=30, loss="energy", hybrid=Fa
     w = 1.0
     if hybrid:
         Pref = lambda X: metric.MultiplyPreconditioner(M, 1.0, X)
-        w = weight if weight is not None else 0.5 * float(np.sum(b * Pref(b))) / float(np.sum(b * net.apply(M, b)))
+        w = weight if weight is not None else 0.125 * float(np.sum(b * Pref(b))) / float(np.sum(b * net.apply(M, b)))
         apply = lambda X: Pref(X) + w * net.apply(M, X)
     else:
         apply = lambda X: net.apply(M, X)
