@@ -681,7 +681,9 @@ def run_flow(args):
     out["step_size_s"] = time.perf_counter() - t
     info = tpm.SolveInfo(M)
     out["solve"] = {"iterations": info["iterations"], "fallback_iteration": info["fallback_iteration"],
-                    "rel_residual": [float(x) for x in tpm.Solver_RelativeResiduals()]}
+                    "rel_residual": [float(x) for x in tpm.Solver_RelativeResiduals()],
+                    "h1_factor_s": info["factor_seconds"], "h1_factor_nnz": info["factor_nnz"],
+                    "precond": "hybrid: reference H1^-1 L H1^-1 + w x learned multilevel"}
     out["value"] = out["energy_grad_s"] + out["solve_s"] + out["step_size_s"]
     print(json.dumps(out))
     return 0
