@@ -226,7 +226,8 @@ rpb_status rpb_mesh_shard_rows(const rpb_mesh* m, int shard, int64_t near_rows[2
  * (energy part). */
 rpb_status rpb_mesh_shard_buffer_doubles(const rpb_mesh* m, int64_t* doubles);
 /* Pair kernels of shard `shard` on the mesh stream into the device buffer `buf`: the
- * centred moment derivatives of the shard's rows (zero elsewhere) and its energy part.
+ * moment derivatives of the shard's rows (zero elsewhere; near rows centred at the
+ * primitive, far rows with d0 - dx . c_C in their first entry) and its energy part.
  * Meshes with very-near pairs are rejected. */
 rpb_status rpb_tpe0_pairs_shard(rpb_mesh* m, double q, double p, int shard, double* buf);
 /* Collection, chain rule and vertex gather from the sum of all shards' buffers:

@@ -303,7 +303,11 @@ static __global__ void k_cluster_moments(GeomArgs g)
 //     d0 = sum b (E - q/2 |u|^{q/2-1} u s^{p/2-q/2})   (no dEdv.x term),
 //     dx = -sum b dEdv,   dP = sum b/2 K_xy V,
 // where u = (v^T P v)/|v|^2, s = 1/|v|^2. The reference's DX[0] equals d0 - dx.x
-// (TP0_Kernel_FF.hpp:220-255); the x-term is restored in FP64 during collection.
+// (TP0_Kernel_FF.hpp:220-255). Near rows keep the centred d0 and the collection adds
+// dx.(x_i - x) with the primitive's own x; far rows store d0 - dx.c_C (the cluster
+// centre, in FP64 when the row is written), so that the collection's ancestor walk adds
+// dx.x_i without loading the clusters' centres (measured: +2 % evals/s, the FP64 sum
+// keeps ~14 digits against the 1e-5 differential tolerance).
 // Powers are taken of the bounded ratios u, w and of s, which keeps the FP32 range
 // safe for close pairs (r^-p itself would overflow FP32 near r ~ 1e-3).
 // ----------------------------------------------------------------------------------------
@@ -451,7 +455,7 @@ struct PairArgs {
     const int* order;         // rows in processing order (length-sorted within 256-row chunks)
     const void* data;         // PrimDatum* (near) or ClusterDatum* (far)
     const void* col_data;     // CROSS: the obstacle's data the columns index
-    double* D;                // rows x 10 (d0, dx[3], dP[6]) centred moment derivatives
+    double* D;                // rows x 10 (d0, dx[3], dP[6]) moment derivatives (far: d0 - dx.c)
     double* block_energy;     // gridDim.x
     unsigned* done;           // 1 counter, zero between launches
     double* energy_out;       // 1
@@ -691,6 +695,7 @@ __global__ void __launch_bounds__(PAIR_BLOCK) k_tp0_pairs(PairArgs A)
         };
         pair_row<FAR, QH, PH, DIFF, CROSS, true, false, false, Datum>(A, X, i, static_cast<int>(A.rp[i + 1] - k0), sub,
                                                                      LANES, index, datum, e_row, D64, nullptr);
+        if constexpr (FAR && DIFF) D64[0] -= D64[1] * X.c[0] + D64[2] * X.c[1] + D64[3] * X.c[2];
     }
     pair_epilogue<DIFF, CROSS, false>(A, active, i, sub, LANES, LANES, e_row, D64, blockIdx.x, gridDim.x);
 }
@@ -858,6 +863,7 @@ __device__ __forceinline__ void pairs_tiled_body(const PairArgs& A, const PairTi
         };
         pair_row<FAR, QH, PH, DIFF, false, false, !FAR && DIFF, !FAR, ColDatum>(
             A, X, i, static_cast<int>(A.rp[i + 1] - k0), sub, size, index, datum, e_row, D64, Dsm);
+        if constexpr (FAR && DIFF) D64[0] -= D64[1] * X.c[0] + D64[2] * X.c[1] + D64[3] * X.c[2];
     }
     pair_epilogue<DIFF, false, !FAR>(A, active, i, sub, size, __reduce_max_sync(0xffffffffu, size), e_row, D64, bid, nblocks);
 }
@@ -928,7 +934,7 @@ struct CollectArgs {
     const int* C_up4;
     const ClusterDatum* C_pair;
     const double* D_near;      // N x 10 centred
-    const double* D_far;       // NC x 10 centred
+    const double* D_far;       // NC x 10, d0 - dx.c_C in the first entry
     const double* D_vf;        // N x 16 very-near derivatives (reference layout) or nullptr
     double* B;                 // N x (dom+1) x 3, original simplex order
 };
@@ -951,12 +957,11 @@ static __global__ void k_collect_chain(CollectArgs A)
     double gx[3] = {dn[1], dn[2], dn[3]};
     double G6[6];
     for (int k = 0; k < 6; ++k) G6[k] = dn[4 + k];
-    // far field: percolate down = sum over all ancestors of the leaf
+    // far field: percolate down = sum over all ancestors of the leaf (d0 - dx.c_C + dx.x_i)
     ancestor_walk(A.leaf_of[i], A.C_parent, A.C_up4, [&](int C) {
         const double* df = A.D_far + 10 * static_cast<int64_t>(C);
-        const ClusterDatum cd = load_datum(A.C_pair, C);
         const double dx0 = df[1], dx1 = df[2], dx2 = df[3];
-        alpha += df[0] + dx0 * (g.c[0] - cd.c[0]) + dx1 * (g.c[1] - cd.c[1]) + dx2 * (g.c[2] - cd.c[2]);
+        alpha += df[0] + dx0 * g.c[0] + dx1 * g.c[1] + dx2 * g.c[2];
         gx[0] += dx0; gx[1] += dx1; gx[2] += dx2;
         for (int k = 0; k < 6; ++k) G6[k] += df[4 + k];
     });

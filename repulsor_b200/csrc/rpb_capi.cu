@@ -407,7 +407,9 @@ rpb_status launch_collect_gather(rpb_mesh* m, double alpha, double beta, double*
     C.D_far = D_far ? D_far : m->D_far.ptr;
     C.D_vf = D_vf;
     C.B = m->B.ptr;
-    launch_pdl(k_collect_chain, (m->N + 255) / 256, 256, 0, m->stream, C);
+    // a plain launch: with programmatic dependent launch the collection's early blocks hold
+    // SM resources during the pair kernel's last wave (measured: 9,540 against 9,985 evals/s)
+    k_collect_chain<<<(m->N + 255) / 256, 256, 0, m->stream>>>(C);
     RPB_CUDA(cudaGetLastError());
     GatherArgs G;
     G.nV = m->nV;

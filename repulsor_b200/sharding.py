@@ -9,7 +9,7 @@ derivative, so the shards' rows are disjoint: each process sends only the rows i
 (one all-gather over the process group, NCCL between GPUs), every process places the
 other shards' rows into its buffer and adds the shards' energy parts in shard order, and
 then applies the chain rule and the vertex gather (`rpb_tpe0_collect_shards`). The buffer
-holds the centred moment derivatives of the primitives (10 N) and clusters (10 N_C) and
+holds the moment derivatives of the primitives (10 N) and clusters (10 N_C) and
 the energy part (1); an all-gather moves each row once, half the bytes of a ring
 all-reduce of the whole buffer, and adds nothing but the energy parts.
 """
@@ -20,7 +20,7 @@ import ctypes
 from . import _capi
 from ._capi import check
 
-FAR_DIM = 10    # doubles per row of a shard buffer (centred moment derivatives)
+FAR_DIM = 10    # doubles per row of a shard buffer (moment derivatives)
 
 
 def shard_range(count: int, shards: int, shard: int) -> tuple[int, int]:
