@@ -78,6 +78,13 @@ rpb_status rpb_mesh_destroy(rpb_mesh* m);
 
 rpb_status rpb_mesh_stats(const rpb_mesh* m, rpb_stats* out);
 
+/* Where rpb_mesh_create built the cluster tree (the longest-axis splits,
+ * src/ClusterTree/Split_Thread.hpp, src/BoundingVolumes/AABB_LongestAxisSplit.hpp:134-253)
+ * and the block cluster tree (the dual traversal, Traverse_DepthFirst.hpp:52-258): 1 on the
+ * device, 0 on host threads, the fallback when the device work failed. Both give the same
+ * permutation, clusters and pair lists. Either pointer may be NULL. */
+rpb_status rpb_mesh_build_info(const rpb_mesh* m, int* cluster_tree_on_device, int* block_tree_on_device);
+
 /* CUDA stream used by all work of this mesh (a cudaStream_t passed as void*).
  * set: the caller keeps ownership of `stream`; NULL restores the mesh's own stream.
  * No reference counterpart: Repulsor runs on host threads only. */

@@ -173,6 +173,13 @@ class SimplicialMesh:
         check(_capi.load().rpb_mesh_stats(self._h, ctypes.byref(st)), "rpb_mesh_stats")
         return {name: getattr(st, name) for name, _ in Stats._fields_}
 
+    def build_info(self) -> dict:
+        """Where the cluster tree and the block cluster tree were built (True: on the GPU,
+        False: on host threads after the device work failed)."""
+        a, b = ctypes.c_int(), ctypes.c_int()
+        check(_capi.load().rpb_mesh_build_info(self._h, ctypes.byref(a), ctypes.byref(b)), "rpb_mesh_build_info")
+        return {"cluster_tree_on_device": bool(a.value), "block_tree_on_device": bool(b.value)}
+
     def stream(self) -> int:
         p = ctypes.c_void_p()
         check(_capi.load().rpb_mesh_get_stream(self._h, ctypes.byref(p)), "rpb_mesh_get_stream")

@@ -65,6 +65,7 @@ SIGNATURES = {
                                        ctypes.POINTER(Settings), ctypes.POINTER(_vp)]),
     "rpb_mesh_destroy": (ctypes.c_int, [_vp]),
     "rpb_mesh_stats": (ctypes.c_int, [_vp, ctypes.POINTER(Stats)]),
+    "rpb_mesh_build_info": (ctypes.c_int, [_vp, _ip, _ip]),
     "rpb_mesh_set_stream": (ctypes.c_int, [_vp, _vp]),
     "rpb_mesh_get_stream": (ctypes.c_int, [_vp, ctypes.POINTER(_vp)]),
     "rpb_mesh_semistatic_update": (ctypes.c_int, [_vp, _dp, ctypes.c_int]),

@@ -518,15 +518,21 @@ rpb_status rpb_mesh_create(int dom_dim, int amb_dim, const double* Vh, int64_t n
 
     if (cudaSetDevice(m->device) != cudaSuccess) { set_error("cudaSetDevice failed"); return fail(RPB_ECUDA); }
     if (cudaStreamCreateWithFlags(&m->own_stream, cudaStreamNonBlocking) != cudaSuccess) { set_error("stream creation failed"); return fail(RPB_ECUDA); }
-    // the cluster tree on the host, the block cluster tree's traversal on the device (the
-    // host traversal if the device one fails; both give the same patterns)
+    // the cluster tree's splits and the block cluster tree's traversal on the device (each
+    // on the host if the device work fails; both give the same tree and patterns)
     const auto t0 = std::chrono::steady_clock::now();
     {
         std::vector<double> Pser;
-        const std::string err = build_cluster_tree(dom_dim, Vh, m->nV, Sh, m->N, m->settings, m->tree, Pser);
-        if (!err.empty()) { set_error(err); return fail(RPB_EINVAL); }
         std::string derr;
-        if (!build_block_cluster_tree_device(m->tree, Pser, Sh, m->settings, m->own_stream, derr)) {
+        m->cluster_tree_on_device =
+            build_cluster_tree_device(dom_dim, Vh, m->nV, Sh, m->N, m->tree, Pser, m->own_stream, derr);
+        if (!m->cluster_tree_on_device) {
+            cudaGetLastError();
+            const std::string err = build_cluster_tree(dom_dim, Vh, m->nV, Sh, m->N, m->settings, m->tree, Pser);
+            if (!err.empty()) { set_error(err); return fail(RPB_EINVAL); }
+        }
+        m->block_tree_on_device = build_block_cluster_tree_device(m->tree, Pser, Sh, m->settings, m->own_stream, derr);
+        if (!m->block_tree_on_device) {
             cudaGetLastError();
             build_block_cluster_tree(m->tree, Pser, Sh, m->settings);
         }
@@ -671,6 +677,14 @@ rpb_status rpb_mesh_stats(const rpb_mesh* m, rpb_stats* o)
     o->inter_nnz = m->tree.inter.nnz();
     o->tree_build_seconds = m->build_seconds;
     o->device_bytes = m->device_bytes();
+    return RPB_OK;
+}
+
+rpb_status rpb_mesh_build_info(const rpb_mesh* m, int* cluster_tree_on_device, int* block_tree_on_device)
+{
+    if (!m) { set_error("null mesh"); return RPB_EINVAL; }
+    if (cluster_tree_on_device) *cluster_tree_on_device = m->cluster_tree_on_device ? 1 : 0;
+    if (block_tree_on_device) *block_tree_on_device = m->block_tree_on_device ? 1 : 0;
     return RPB_OK;
 }
 

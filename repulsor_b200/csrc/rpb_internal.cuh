@@ -17,6 +17,11 @@ rpb_status check_exponents(double q, double p);
 // untouched and err set if the device work failed
 bool build_block_cluster_tree_device(HostTree& T, const std::vector<double>& P, const int* S, const TreeSettings& set,
                                      cudaStream_t s, std::string& err);
+// the cluster tree of a mesh built on the device (rpb_gputree.cu): the same permutation,
+// ranges, links and boxes as build_cluster_tree, and the serialized polytopes in tree order;
+// false with err set if the input is invalid or the device work failed
+bool build_cluster_tree_device(int dom, const double* V, int nV, const int* S, int N, HostTree& T,
+                               std::vector<double>& P, cudaStream_t s, std::string& err);
 // the obstacle loaded into m (rpb_mesh_load_obstacle), or null
 rpb_mesh* obstacle_mesh(const rpb_mesh* m);
 

@@ -88,6 +88,8 @@ struct rpb_mesh {
     int dom = 2, size = 3, nV = 0, N = 0, NC = 0;
     int device = 0;
     double build_seconds = 0;
+    bool cluster_tree_on_device = false;  // the splits ran on the device (else on the host)
+    bool block_tree_on_device = false;    // the dual traversal ran on the device
     cudaStream_t stream = nullptr;        // stream all work is issued on
     cudaStream_t own_stream = nullptr;    // stream created by the mesh
     double* host_energy = nullptr;        // 3 pinned doubles: energy parts read back with the results

@@ -1,7 +1,10 @@
-"""The block cluster tree built at mesh creation runs its dual traversal on the GPU
-(rpb_gputree.cu, host/bct_rules.hpp); its four patterns must equal the host builder's
-(HostTree, itself checked bit-exactly against the oracle in test_tree_parity.py) entry
-for entry, including very-near and intersecting pairs."""
+"""The cluster tree and the block cluster tree built at mesh creation run on the GPU
+(rpb_gputree.cu: the level-by-level longest-axis splits with the median fallback on the
+host, then the dual traversal with host/bct_rules.hpp); the permutation, the clusters and
+the four patterns must equal the host builder's (HostTree, itself checked bit-exactly
+against the oracle in test_tree_parity.py) entry for entry, including very-near and
+intersecting pairs. The cases include meshes whose splits take the median fallback on
+clusters of more than three primitives (the full torus, the 96 x 128 linked tori)."""
 import numpy as np
 import pytest
 
@@ -16,12 +19,24 @@ def _overlapping_spheres():
     return 2, np.vstack([Va, Vb]), np.vstack([Sa, Sb + Va.shape[0]]).astype(np.int32)
 
 
+def _few(n):
+    # n triangles of a strip: the smallest trees (one leaf, one split, ...)
+    V, S = meshes.torus(n_major=8, n_minor=4)
+    return 2, V, S[:n].copy()
+
+
 CASES = {
     "curve": lambda: (1,) + meshes.config_mesh(1, small=True)[1],
+    "curve_full": lambda: (1,) + meshes.config_mesh(1)[1],
     "torus": lambda: (2,) + meshes.config_mesh(2, small=True)[1],
+    "torus_full": lambda: (2,) + meshes.config_mesh(2)[1],
     "icosphere": lambda: (2,) + meshes.config_mesh(3, small=True)[1],
     "linked_tori": lambda: (2,) + meshes.config_mesh(5, small=True)[1],
+    "linked_tori_96x128": lambda: (2,) + meshes.linked_tori(96, 128),
     "overlapping": _overlapping_spheres,
+    "one_triangle": lambda: _few(1),
+    "two_triangles": lambda: _few(2),
+    "five_triangles": lambda: _few(5),
 }
 
 
@@ -31,7 +46,9 @@ def test_device_traversal_equals_host_builder(case):
     dom, V, S = CASES[case]()
     M = rpb.SimplicialMesh(V, S)
     H = rpb.HostTree(V, S)
+    assert M.build_info() == {"cluster_tree_on_device": True, "block_tree_on_device": True}
     tm, th = M.tree(), H.tree()
+    assert M.stats()["tree_depth"] == H.stats()["tree_depth"]
     for k in th:
         np.testing.assert_array_equal(tm[k], th[k])
     for which in ("near", "far", "verynear", "inter"):
