@@ -194,8 +194,9 @@ typedef struct rpb_solve_info {
     int     restarts;            /* recurrences restarted from the true residual */
     int     fallback_iteration;  /* iteration at which LEARNED switched to REFERENCE, or -1 */
     int     supernode_levels;    /* launches per triangular solve of the H1 factor (0: none built) */
-    double  factor_seconds;      /* host H1 assembly + ordering + Cholesky time of the current factor */
+    double  factor_seconds;      /* H1 assembly + ordering + Cholesky time of the current factor */
     int64_t factor_nnz;          /* nonzeros of the H1 Cholesky factor */
+    int     factor_on_device;    /* 1: the numeric factorization ran on the device, 0: on host threads */
 } rpb_solve_info;
 
 rpb_status rpb_tpm0_solve_info(const rpb_mesh* m, rpb_solve_info* info);

@@ -504,7 +504,8 @@ class TangentPointMetric0:
     @staticmethod
     def SolveInfo(M) -> dict:
         """Statistics of the last Solve on M: iterations, restarts, fallback_iteration (-1: the
-        learned preconditioner never fell back), supernode_levels, factor_seconds, factor_nnz."""
+        learned preconditioner never fell back), supernode_levels, factor_seconds, factor_nnz,
+        factor_on_device (1: the H1 factor's numeric phase ran on the GPU)."""
         info = _capi.SolveInfo()
         check(_capi.load().rpb_tpm0_solve_info(_as_mesh(M)._h, ctypes.byref(info)), "rpb_tpm0_solve_info")
         return {name: getattr(info, name) for name, _ in _capi.SolveInfo._fields_}

@@ -54,7 +54,8 @@ class SolveInfo(ctypes.Structure):
                 ("fallback_iteration", ctypes.c_int),
                 ("supernode_levels", ctypes.c_int),
                 ("factor_seconds", ctypes.c_double),
-                ("factor_nnz", ctypes.c_int64)]
+                ("factor_nnz", ctypes.c_int64),
+                ("factor_on_device", ctypes.c_int)]
 
 
 # name -> (restype, argtypes); every exported symbol of include/repulsor_b200.h

@@ -1,7 +1,10 @@
 // H1 metric, nested-dissection ordering and up-looking sparse Cholesky (host).
 #include "sparse_cholesky.hpp"
+#include "supernodal_chol.hpp"
 
 #include <algorithm>
+#include <atomic>
+#include <thread>
 #include <cmath>
 #include <cstdint>
 
@@ -150,113 +153,14 @@ std::vector<int> nested_dissection_ordering(const HostTree& T, const int* S, int
 
 std::string cholesky_factor(const CsrMatrix& A, const std::vector<int>& perm, CholeskyFactor& F)
 {
-    const int n = A.n;
-    std::vector<int> pinv(n);
-    for (int i = 0; i < n; ++i) pinv[perm[i]] = i;
-    // upper triangle of C = P A P^T in CSC (column j: rows i <= j)
-    std::vector<int64_t> Cp(static_cast<size_t>(n) + 1, 0);
-    for (int r = 0; r < n; ++r)
-        for (int64_t p = A.rp[r]; p < A.rp[r + 1]; ++p) {
-            const int i = pinv[r], j = pinv[A.ci[p]];
-            if (i <= j) Cp[j + 1]++;
-        }
-    for (int j = 0; j < n; ++j) Cp[j + 1] += Cp[j];
-    std::vector<int> Ci(static_cast<size_t>(Cp[n]));
-    std::vector<double> Cx(static_cast<size_t>(Cp[n]));
-    {
-        std::vector<int64_t> pos(Cp.begin(), Cp.end() - 1);
-        for (int r = 0; r < n; ++r)
-            for (int64_t p = A.rp[r]; p < A.rp[r + 1]; ++p) {
-                const int i = pinv[r], j = pinv[A.ci[p]];
-                if (i <= j) {
-                    Ci[pos[j]] = i;
-                    Cx[pos[j]++] = A.val[p];
-                }
-            }
-    }
-    // elimination tree
-    std::vector<int> parent(n, -1), ancestor(n, -1);
-    for (int k = 0; k < n; ++k)
-        for (int64_t p = Cp[k]; p < Cp[k + 1]; ++p) {
-            int i = Ci[p];
-            while (i != -1 && i < k) {
-                const int inext = ancestor[i];
-                ancestor[i] = k;
-                if (inext == -1) parent[i] = k;
-                i = inext;
-            }
-        }
-    // row patterns (ereach) -> column counts
-    std::vector<int> mark(n, -1), stack(n);
-    auto ereach = [&](int k, int* s) {
-        int top = n;
-        mark[k] = k;
-        for (int64_t p = Cp[k]; p < Cp[k + 1]; ++p) {
-            int i = Ci[p];
-            if (i > k) continue;
-            int len = 0;
-            for (; mark[i] != k; i = parent[i]) {
-                s[len++] = i;
-                mark[i] = k;
-            }
-            while (len > 0) s[--top] = s[--len];
-        }
-        return top;
-    };
-    std::vector<int64_t> colcount(n, 1);
-    for (int k = 0; k < n; ++k) {
-        const int top = ereach(k, stack.data());
-        for (int q = top; q < n; ++q) colcount[stack[q]]++;
-    }
-    std::vector<int64_t> Lp(static_cast<size_t>(n) + 1, 0);
-    for (int j = 0; j < n; ++j) Lp[j + 1] = Lp[j] + colcount[j];
-    std::vector<int> Li(static_cast<size_t>(Lp[n]));
-    std::vector<double> Lx(static_cast<size_t>(Lp[n]));
-    std::vector<int64_t> c(Lp.begin(), Lp.end() - 1);
-    std::vector<double> x(n, 0.0);
-    std::fill(mark.begin(), mark.end(), -1);
-    for (int k = 0; k < n; ++k) {
-        const int top = ereach(k, stack.data());
-        x[k] = 0.0;
-        for (int64_t p = Cp[k]; p < Cp[k + 1]; ++p)
-            if (Ci[p] <= k) x[Ci[p]] = Cx[p];
-        double d = x[k];
-        x[k] = 0.0;
-        for (int q = top; q < n; ++q) {
-            const int i = stack[q];
-            const double lki = x[i] / Lx[Lp[i]];
-            x[i] = 0.0;
-            for (int64_t p = Lp[i] + 1; p < c[i]; ++p) x[Li[p]] -= Lx[p] * lki;
-            d -= lki * lki;
-            const int64_t p = c[i]++;
-            Li[p] = k;
-            Lx[p] = lki;
-        }
-        if (!(d > 0.0)) return "H1 metric is not positive definite";
-        const int64_t p = c[k]++;
-        Li[p] = k;
-        Lx[p] = std::sqrt(d);
-    }
-    // upper form = columns of L (rows of L^T), diagonal first
-    F = CholeskyFactor();
-    F.n = n;
-    F.perm = perm;
-    F.upper_rp = Lp;
-    F.upper_ci = Li;
-    F.upper_val = Lx;
-    // lower form = rows of L, diagonal last
-    F.lower_rp.assign(static_cast<size_t>(n) + 1, 0);
-    for (int64_t p = 0; p < Lp[n]; ++p) F.lower_rp[Li[p] + 1]++;
-    for (int i = 0; i < n; ++i) F.lower_rp[i + 1] += F.lower_rp[i];
-    F.lower_ci.resize(static_cast<size_t>(Lp[n]));
-    F.lower_val.resize(static_cast<size_t>(Lp[n]));
-    std::vector<int64_t> pos(F.lower_rp.begin(), F.lower_rp.end() - 1);
-    for (int j = 0; j < n; ++j)
-        for (int64_t p = Lp[j]; p < Lp[j + 1]; ++p) {
-            const int i = Li[p];
-            F.lower_ci[pos[i]] = j;
-            F.lower_val[pos[i]++] = Lx[p];
-        }
+    // supernodal factorization on host threads (host/supernodal_chol.hpp)
+    SupernodalSymbolic S;
+    std::string err = supernodal_symbolic(A, perm, kSupernodalWidth, S);
+    if (!err.empty()) return err;
+    std::vector<double> panels;
+    err = supernodal_numeric_host(S, panels, static_cast<int>(std::max(1u, std::thread::hardware_concurrency())));
+    if (!err.empty()) return err;
+    supernodal_to_factor(S, panels, F);
     return std::string();
 }
 
@@ -364,8 +268,14 @@ std::string supernodal_schedule(const CholeskyFactor& F, int max_width, Supernod
     }
     out.dinv.assign(static_cast<size_t>(out.dinv_off[nsn]), 0.0);
     out.dinvT.assign(static_cast<size_t>(out.dinv_off[nsn]), 0.0);
+    // the blocks are independent: host threads take supernodes by ticket
+    std::atomic<int> ticket{0}, zero_pivot{0};
+    const int threads = static_cast<int>(std::max(1u, std::min(16u, std::thread::hardware_concurrency())));
+    auto invert = [&](int) {
     std::vector<double> D, X;
-    for (int s = 0; s < nsn; ++s) {
+    for (;;) {
+        const int s = ticket.fetch_add(1);
+        if (s >= nsn) break;
         const int c0 = begin[s], w = begin[s + 1] - c0;
         D.assign(static_cast<size_t>(w) * w, 0.0);
         for (int r = 0; r < w; ++r)
@@ -380,7 +290,10 @@ std::string supernodal_schedule(const CholeskyFactor& F, int max_width, Supernod
                 double acc = (r == c) ? 1.0 : 0.0;
                 const double* Dr = &D[static_cast<size_t>(r) * w];
                 for (int k = c; k < r; ++k) acc -= Dr[k] * X[static_cast<size_t>(k) * w + c];
-                if (!(Dr[r] > 0.0)) return "zero pivot in a supernode diagonal block";
+                if (!(Dr[r] > 0.0)) {
+                    zero_pivot.store(1);
+                    return;
+                }
                 X[static_cast<size_t>(r) * w + c] = acc / Dr[r];
             }
         }
@@ -394,6 +307,15 @@ std::string supernodal_schedule(const CholeskyFactor& F, int max_width, Supernod
             for (int r = c; r < w; ++r) Ui[o + (r - c)] = X[static_cast<size_t>(r) * w + c];
         }
     }
+    };
+    if (threads <= 1 || nsn < 64) {
+        invert(0);
+    } else {
+        std::vector<std::thread> th;
+        for (int t = 0; t < threads; ++t) th.emplace_back(invert, t);
+        for (auto& x : th) x.join();
+    }
+    if (zero_pivot.load()) return "zero pivot in a supernode diagonal block";
     return std::string();
 }
 

@@ -28,8 +28,11 @@ CsrMatrix assemble_h1(int dom, const double* V, int nV, const int* S, int N, dou
 // Vertex permutation by nested dissection along the cluster tree: perm[new] = old.
 std::vector<int> nested_dissection_ordering(const HostTree& T, const int* S, int nV);
 
-// Sparse Cholesky L L^T = P A P^T (up-looking, elimination tree). Returns the factor in
-// both row forms used by the GPU triangular solves:
+// widest supernode of the numeric factorization (host/supernodal_chol.hpp)
+constexpr int kSupernodalWidth = 256;
+
+// Sparse Cholesky L L^T = P A P^T (supernodal, on host threads: host/supernodal_chol.hpp).
+// Returns the factor in both row forms used by the GPU triangular solves:
 //   lower: row i of L, columns ascending, diagonal last
 //   upper: row i of L^T (= column i of L), columns ascending, diagonal first
 struct CholeskyFactor {

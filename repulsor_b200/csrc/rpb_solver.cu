@@ -16,9 +16,11 @@
 #include <cmath>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "host/sparse_cholesky.hpp"
+#include "host/supernodal_chol.hpp"
 #include "rpb_internal.cuh"
 #include "rpb_mesh.cuh"
 #include "rpb_solver.cuh"
@@ -544,6 +546,237 @@ void solver_free(rpb_mesh* m)
     }
 }
 
+// ------------------------------------------------------------------------------------------
+// Numeric supernodal Cholesky of H1 on the device (host/supernodal_chol.hpp). The entries of
+// H1 are scattered into the dense supernode panels (one thread per column); then, level by
+// level of the supernodal elimination tree, two launches:
+//   k_chol_update: the updates a supernode J receives from the supernodes K below it, cut
+//     into regions of J's panel (blocks of CHOL_REGION_ROWS structure rows x CHOL_TILE
+//     columns, one CTA each, regions entirely above the diagonal skipped); a CTA walks J's
+//     update list in order and subtracts, for each K, the part of L_K L_K^T that lands in
+//     its region (a 64 x 64-tiled product with the inner dimension staged in shared memory,
+//     or a direct loop for small parts). Every panel entry belongs to one region, so the
+//     sums are formed in a fixed order without atomics;
+//   k_chol_panel: one CTA per supernode factors its updated panel (sn_factor_panel, the
+//     code the host fallback runs on one thread).
+// The symbolic analysis stays on the host.
+// ------------------------------------------------------------------------------------------
+struct CtaBarrier {
+    __host__ __device__ void operator()() const
+    {
+#if defined(__CUDA_ARCH__)
+        __syncthreads();
+#endif
+    }
+};
+
+__global__ void k_chol_scatter(int n, const int64_t* __restrict__ Cp, const int* __restrict__ Ci,
+                               const double* __restrict__ Cx, const int* __restrict__ sn_of, SnView v, unsigned* error)
+{
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    for (int64_t p = Cp[j]; p < Cp[j + 1]; ++p)
+        if (!sn_scatter_entry(v, sn_of, Ci[p], j, Cx[p])) atomicOr(error, 1u);
+}
+
+constexpr int CHOL_BLOCK = 256;
+constexpr int CHOL_TILE = 64;          // rows x columns of an update tile (4 x 4 per thread)
+constexpr int CHOL_KCHUNK = 16;        // inner-dimension chunk staged in shared memory
+constexpr int CHOL_REGION_ROWS = 128;  // structure rows of a panel region
+constexpr int64_t CHOL_DIRECT_PAIRS = 2048;   // smaller parts of an update take the direct loop
+static_assert(CHOL_BLOCK == 256 && CHOL_TILE == 64, "the update tiles map 16 x 16 threads onto 64 x 64 entries");
+
+// Part of the update of J by K: rows a in [alo, ahi) and columns b in [blo, bhi) of K's
+// structure positions (a >= b), subtracted from J's panel. Tiled: 64 x 64 tiles, the inner
+// dimension in chunks of 16 staged in shared memory, thread (ty, tx) accumulating rows
+// ty + 16 i and columns tx + 16 j of a tile.
+__device__ int chol_update_part(const SnView& v, int J, int K, int alo, int ahi, int blo, int bhi,
+                                double (*As)[CHOL_TILE], double (*Bs)[CHOL_TILE])
+{
+    const int tid = threadIdx.x;
+    const int c0 = v.sn_begin[J];
+    const int64_t r0 = v.rows_rp[J];
+    const int nr = static_cast<int>(v.rows_rp[J + 1] - r0);
+    const int* R = v.rows + r0;
+    double* P = v.panels + v.panel_off[J];
+    const int wK = v.sn_begin[K + 1] - v.sn_begin[K];
+    const int64_t q0 = v.rows_rp[K];
+    const int nrK = static_cast<int>(v.rows_rp[K + 1] - q0);
+    const int* RK = v.rows + q0;
+    const double* PK = v.panels + v.panel_off[K];
+    const int na = ahi - alo, nb = bhi - blo;
+    int status = 0;
+    if (static_cast<int64_t>(na) * nb <= CHOL_DIRECT_PAIRS) {
+        for (int idx = tid; idx < na * nb; idx += CHOL_BLOCK) {
+            const int a = alo + idx / nb, b = blo + idx % nb;
+            if (a < b) continue;
+            double acc = 0.0;
+            for (int t = 0; t < wK; ++t)
+                acc += PK[static_cast<int64_t>(t) * nrK + a] * PK[static_cast<int64_t>(t) * nrK + b];
+            const int row = sn_lower_bound(R, 0, nr, RK[a]);
+            if (row >= nr || R[row] != RK[a]) {
+                status = 1;
+                continue;
+            }
+            P[static_cast<int64_t>(RK[b] - c0) * nr + row] -= acc;
+        }
+        return status;
+    }
+    const int tx = tid & 15, ty = tid >> 4;
+    for (int ta = alo; ta < ahi; ta += CHOL_TILE)
+        for (int tb = blo; tb < bhi && tb < ta + CHOL_TILE; tb += CHOL_TILE) {
+            double acc[4][4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+            for (int t0 = 0; t0 < wK; t0 += CHOL_KCHUNK) {
+                for (int e = tid; e < CHOL_KCHUNK * CHOL_TILE; e += CHOL_BLOCK) {
+                    const int tt = e / CHOL_TILE, q = e - tt * CHOL_TILE, t = t0 + tt;
+                    const int64_t base = static_cast<int64_t>(t) * nrK;
+                    As[tt][q] = (t < wK && ta + q < ahi) ? PK[base + ta + q] : 0.0;
+                    Bs[tt][q] = (t < wK && tb + q < bhi) ? PK[base + tb + q] : 0.0;
+                }
+                __syncthreads();
+#pragma unroll 4
+                for (int tt = 0; tt < CHOL_KCHUNK; ++tt) {
+                    double x[4], y[4];
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) x[i] = As[tt][ty + 16 * i];
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) y[j] = Bs[tt][tx + 16 * j];
+#pragma unroll
+                    for (int i = 0; i < 4; ++i)
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) acc[i][j] += x[i] * y[j];
+                }
+                __syncthreads();
+            }
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const int a = ta + ty + 16 * i;
+                if (a >= ahi) continue;
+                int row = -1;
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const int b = tb + tx + 16 * j;
+                    if (b >= bhi || a < b) continue;
+                    if (row < 0) {
+                        row = sn_lower_bound(R, 0, nr, RK[a]);
+                        if (row >= nr || R[row] != RK[a]) {
+                            status = 1;
+                            break;
+                        }
+                    }
+                    P[static_cast<int64_t>(RK[b] - c0) * nr + row] -= acc[i][j];
+                }
+            }
+        }
+    return status;
+}
+
+// One CTA per region (J, first structure row, first column) of the level's supernodes.
+__global__ void __launch_bounds__(CHOL_BLOCK) k_chol_update(SnView v, const int4* __restrict__ regions, unsigned* error)
+{
+    __shared__ double As[CHOL_KCHUNK][CHOL_TILE];
+    __shared__ double Bs[CHOL_KCHUNK][CHOL_TILE];
+    const int4 rg = regions[blockIdx.x];
+    const int J = rg.x;
+    const int c0 = v.sn_begin[J], w = v.sn_begin[J + 1] - c0;
+    const int64_t r0 = v.rows_rp[J];
+    const int nr = static_cast<int>(v.rows_rp[J + 1] - r0);
+    const int* R = v.rows + r0;
+    const int rlo = rg.y, rhi = min(rg.y + CHOL_REGION_ROWS, nr);
+    const int clo = rg.z, chi = min(rg.z + CHOL_TILE, w);
+    int status = 0;
+    for (int u = v.upd_rp[J]; u < v.upd_rp[J + 1]; ++u) {
+        const int K = v.upd_k[u];
+        const int wK = v.sn_begin[K + 1] - v.sn_begin[K];
+        const int64_t q0 = v.rows_rp[K];
+        const int nrK = static_cast<int>(v.rows_rp[K + 1] - q0);
+        const int* RK = v.rows + q0;
+        // K's rows whose place in J is in [rlo, rhi), K's columns of J in [clo, chi)
+        const int alo = sn_lower_bound(RK, wK, nrK, R[rlo]);
+        const int ahi = sn_lower_bound(RK, alo, nrK, R[rhi - 1] + 1);
+        const int blo = sn_lower_bound(RK, wK, nrK, c0 + clo);
+        const int bhi = sn_lower_bound(RK, blo, nrK, c0 + chi);
+        if (alo < ahi && blo < bhi) status |= chol_update_part(v, J, K, alo, ahi, blo, bhi, As, Bs);
+        __syncthreads();
+    }
+    if (status != 0) atomicOr(error, static_cast<unsigned>(status));
+}
+
+__global__ void __launch_bounds__(CHOL_BLOCK) k_chol_panel(SnView v, const int* __restrict__ sns, unsigned* error)
+{
+    const int st = sn_factor_panel(v, sns[blockIdx.x], threadIdx.x, blockDim.x, CtaBarrier());
+    if (st != 0 && threadIdx.x == 0) atomicOr(error, static_cast<unsigned>(st));
+}
+
+// The factor of A (ordering perm) with the numeric phase on the device; "" or the reason it
+// failed (the caller then factors on the host).
+static std::string cholesky_factor_device(const CsrMatrix& A, const std::vector<int>& perm, CholeskyFactor& F,
+                                          cudaStream_t s)
+{
+    SupernodalSymbolic S;
+    std::string err = supernodal_symbolic(A, perm, kSupernodalWidth, S);
+    if (!err.empty()) return err;
+    // update regions of every level: (J, first row, first column), below the diagonal
+    const int L = static_cast<int>(S.level_ptr.size()) - 1;
+    std::vector<int4> regions;
+    std::vector<int> region_ptr(static_cast<size_t>(L) + 1, 0);
+    for (int l = 0; l < L; ++l) {
+        for (int q = S.level_ptr[l]; q < S.level_ptr[l + 1]; ++q) {
+            const int J = S.level_sn[q];
+            if (S.upd_rp[J + 1] == S.upd_rp[J]) continue;
+            const int w = S.sn_begin[J + 1] - S.sn_begin[J];
+            const int nr = static_cast<int>(S.rows_rp[J + 1] - S.rows_rp[J]);
+            for (int rlo = 0; rlo < nr; rlo += CHOL_REGION_ROWS)
+                for (int clo = 0; clo < w; clo += CHOL_TILE)
+                    if (std::min(rlo + CHOL_REGION_ROWS, nr) > clo) regions.push_back(make_int4(J, rlo, clo, 0));
+        }
+        region_ptr[l + 1] = static_cast<int>(regions.size());
+    }
+    DevBuf<int> sn_begin, rows, upd_rp, upd_k, sn_of, Ci, level_sn;
+    DevBuf<int64_t> rows_rp, panel_off, Cp;
+    DevBuf<double> Cx, panels;
+    DevBuf<int4> d_regions;
+    DevBuf<unsigned> error;
+    cudaError_t e = cudaSuccess;
+    auto up = [&](auto& dst, const auto& src) {
+        if (e != cudaSuccess) return;
+        if ((e = dst.alloc(src.size())) != cudaSuccess) return;
+        if (!src.empty()) e = cudaMemcpyAsync(dst.ptr, src.data(), dst.bytes(), cudaMemcpyHostToDevice, s);
+    };
+    up(sn_begin, S.sn_begin); up(rows, S.rows); up(upd_rp, S.upd_rp); up(upd_k, S.upd_k); up(sn_of, S.sn_of);
+    up(Ci, S.Ci); up(level_sn, S.level_sn); up(rows_rp, S.rows_rp); up(panel_off, S.panel_off); up(Cp, S.Cp);
+    up(Cx, S.Cx); up(d_regions, regions);
+    const size_t np = static_cast<size_t>(S.panel_off[S.nsn]);
+    if (e == cudaSuccess) e = panels.alloc(np);
+    if (e == cudaSuccess) e = cudaMemsetAsync(panels.ptr, 0, panels.bytes(), s);
+    if (e == cudaSuccess) e = error.alloc(1);
+    if (e == cudaSuccess) e = cudaMemsetAsync(error.ptr, 0, sizeof(unsigned), s);
+    if (e != cudaSuccess) return std::string("device Cholesky: ") + cudaGetErrorString(e);
+    SnView v{sn_begin.ptr, rows_rp.ptr, rows.ptr, panel_off.ptr, upd_rp.ptr, upd_k.ptr, panels.ptr};
+    k_chol_scatter<<<(S.n + 255) / 256, 256, 0, s>>>(S.n, Cp.ptr, Ci.ptr, Cx.ptr, sn_of.ptr, v, error.ptr);
+    for (int l = 0; l < L; ++l) {
+        const int nreg = region_ptr[l + 1] - region_ptr[l];
+        if (nreg > 0) k_chol_update<<<nreg, CHOL_BLOCK, 0, s>>>(v, d_regions.ptr + region_ptr[l], error.ptr);
+        const int count = S.level_ptr[l + 1] - S.level_ptr[l];
+        if (count > 0) k_chol_panel<<<count, CHOL_BLOCK, 0, s>>>(v, level_sn.ptr + S.level_ptr[l], error.ptr);
+    }
+    std::vector<double> hp(np);
+    unsigned herr = 0;
+    if ((e = cudaGetLastError()) != cudaSuccess ||
+        (e = cudaMemcpyAsync(hp.data(), panels.ptr, panels.bytes(), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(&herr, error.ptr, sizeof(unsigned), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(s)) != cudaSuccess)
+        return std::string("device Cholesky: ") + cudaGetErrorString(e);
+    if (herr & 2u) return "H1 metric is not positive definite";
+    if (herr) return "device Cholesky: an entry outside the supernodal structure";
+    supernodal_to_factor(S, hp, F);
+    return std::string();
+}
+
 // H1 factor for the current geometry (the reference caches H1Metric/H1Solver on the mesh
 // and clears them with the cache on SemiStaticUpdate, src/SimplicialMesh.hpp:368).
 static rpb_status ensure_h1(rpb_mesh* m)
@@ -559,8 +792,13 @@ static rpb_status ensure_h1(rpb_mesh* m)
     const CsrMatrix H = assemble_h1(m->dom, V.data(), m->nV, S.data(), m->N, 1.0, 1.0);
     if (s.nd_perm.empty()) s.nd_perm = nested_dissection_ordering(m->tree, S.data(), m->nV);
     CholeskyFactor F;
-    const std::string err = cholesky_factor(H, s.nd_perm, F);
-    if (!err.empty()) { set_error(err); return RPB_EINVAL; }
+    // numeric factorization on the device; on host threads if that fails
+    s.factor_on_device = cholesky_factor_device(H, s.nd_perm, F, m->stream).empty();
+    if (!s.factor_on_device) {
+        cudaGetLastError();
+        const std::string err = cholesky_factor(H, s.nd_perm, F);
+        if (!err.empty()) { set_error(err); return RPB_EINVAL; }
+    }
     s.factor_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     s.factor_nnz = F.nnz();
     SupernodalSchedule SS;
@@ -591,18 +829,39 @@ static rpb_status ensure_h1(rpb_mesh* m)
         std::vector<int64_t> xrp(static_cast<size_t>(n) + 1, 0);
         std::vector<int> xci;
         std::vector<double> xval;
-        xci.reserve(ci.size());
-        xval.reserve(ci.size());
-        for (int r = 0; r < n; ++r) {
-            const int c0 = SS.sn_begin[sn_of[r]], c1 = SS.sn_begin[sn_of[r] + 1];
-            for (int64_t k = rp[r]; k < rp[r + 1]; ++k) {
-                const int j = ci[k];
-                if (lower ? (j < c0) : (j >= c1)) {
-                    xci.push_back(j);
-                    xval.push_back(val[k]);
+        {
+            // counted, then filled, by host threads over row ranges
+            const int nt = static_cast<int>(std::max(1u, std::min(16u, std::thread::hardware_concurrency())));
+            auto outside = [&](int r, int j) {
+                return lower ? (j < SS.sn_begin[sn_of[r]]) : (j >= SS.sn_begin[sn_of[r] + 1]);
+            };
+            auto pool = [&](auto&& body) {
+                std::vector<std::thread> th;
+                for (int t = 0; t < nt; ++t)
+                    th.emplace_back([&, t] { body(static_cast<int>(static_cast<int64_t>(n) * t / nt),
+                                                  static_cast<int>(static_cast<int64_t>(n) * (t + 1) / nt)); });
+                for (auto& x : th) x.join();
+            };
+            pool([&](int r0, int r1) {
+                for (int r = r0; r < r1; ++r) {
+                    int64_t c = 0;
+                    for (int64_t k = rp[r]; k < rp[r + 1]; ++k) c += outside(r, ci[k]) ? 1 : 0;
+                    xrp[r + 1] = c;
                 }
-            }
-            xrp[r + 1] = static_cast<int64_t>(xci.size());
+            });
+            for (int r = 0; r < n; ++r) xrp[r + 1] += xrp[r];
+            xci.resize(static_cast<size_t>(xrp[n]));
+            xval.resize(static_cast<size_t>(xrp[n]));
+            pool([&](int r0, int r1) {
+                for (int r = r0; r < r1; ++r) {
+                    int64_t o = xrp[r];
+                    for (int64_t k = rp[r]; k < rp[r + 1]; ++k)
+                        if (outside(r, ci[k])) {
+                            xci[o] = ci[k];
+                            xval[o++] = val[k];
+                        }
+                }
+            });
         }
         // level plans
         const std::vector<int>& lptr = lower ? SS.fwd_level_ptr : SS.bwd_level_ptr;
@@ -1021,6 +1280,7 @@ rpb_status rpb_tpm0_solve_info(const rpb_mesh* m, rpb_solve_info* info)
     info->factor_seconds = m->solver ? m->solver->factor_seconds : 0.0;
     info->factor_nnz = m->solver ? m->solver->factor_nnz : 0;
     info->supernode_levels = m->solver ? m->solver->sn_levels_fwd : 0;
+    info->factor_on_device = (m->solver && m->solver->factor_on_device) ? 1 : 0;
     return RPB_OK;
 }
 

@@ -41,6 +41,7 @@ struct Solver {
     int sn_levels_fwd = 0;
     double factor_seconds = 0;
     int64_t factor_nnz = 0;
+    bool factor_on_device = false;   // numeric factorization on the device (else host threads)
     // statistics of the last Solve
     int last_iterations = 0, last_restarts = 0, last_fallback_iteration = -1;
 };

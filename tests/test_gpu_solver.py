@@ -1,7 +1,8 @@
 """MultiplyPreconditioner and Solve on the B200 through the C ABI.
 
 Preconditioner: H1^{-1} L_{2-s} H1^{-1} against the oracle (scipy factorization of the
-oracle's H1 and the oracle pseudo-Laplacian), 1e-5 relative in max norm.
+oracle's H1 and the oracle pseudo-Laplacian), 1e-5 relative in max norm; the H1 factor's
+numeric phase runs on the GPU (supernodal, one CTA per supernode of a level).
 Solve: the true relative residual of the returned solution, measured with the FP64
 oracle's metric operator, is at the requested 1e-6 (plus the 1e-5-level operator
 difference times the solution's conditioning margin: bound 5e-6)."""
@@ -29,6 +30,7 @@ def test_preconditioner_matches_oracle(cfg):
     X = np.random.default_rng(cfg).standard_normal(V.shape)
     Y = tpm.MultiplyPreconditioner(M, 1.0, X)
     assert rel_max(Y, O.precondition(X, Q, P)) <= 1e-5
+    assert tpm.SolveInfo(M)["factor_on_device"] == 1
 
 
 @pytest.mark.parametrize("cfg", [2, 3])
@@ -43,6 +45,7 @@ def test_preconditioner_matches_oracle_full_size(cfg):
     X = np.random.default_rng(10 + cfg).standard_normal(V.shape)
     Y = tpm.MultiplyPreconditioner(M, 1.0, X)
     assert rel_max(Y, O.precondition(X, Q, P)) <= 1e-5
+    assert tpm.SolveInfo(M)["factor_on_device"] == 1
 
 
 @pytest.mark.parametrize("cfg,precond", [(1, rpb.PRECOND_NONE), (2, rpb.PRECOND_NONE), (3, rpb.PRECOND_NONE),
