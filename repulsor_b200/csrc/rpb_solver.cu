@@ -557,8 +557,8 @@ void solver_free(rpb_mesh* m)
 //     its region (a 64 x 64-tiled product with the inner dimension staged in shared memory,
 //     or a direct loop for small parts). Every panel entry belongs to one region, so the
 //     sums are formed in a fixed order without atomics;
-//   k_chol_panel: one CTA per supernode factors its updated panel (sn_factor_panel, the
-//     code the host fallback runs on one thread).
+//   k_chol_panel: one CTA per supernode factors its updated panel, right-looking in blocks
+//     of 16 columns (the host fallback runs the unblocked sn_factor_panel on one thread).
 // The symbolic analysis stays on the host.
 // ------------------------------------------------------------------------------------------
 struct CtaBarrier {
@@ -706,9 +706,89 @@ __global__ void __launch_bounds__(CHOL_BLOCK) k_chol_update(SnView v, const int4
     if (status != 0) atomicOr(error, static_cast<unsigned>(status));
 }
 
+// Blocked panel factorization (right-looking, blocks of CHOL_KCHUNK columns): the columns of
+// a block are factored one by one as in sn_factor_panel, but their updates reach only the
+// block's own columns; the rest of the panel then takes the block's rank-16 update at once as
+// a 64 x 64-tiled product (tiles above the diagonal skipped), so the trailing part is read and
+// written once per block instead of once per column. Returns 0, or 2 for a non-positive pivot
+// (every thread returns it together).
+__device__ int chol_panel_blocked(const SnView& v, int J, double (*As)[CHOL_TILE], double (*Bs)[CHOL_TILE])
+{
+    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+    const int c0 = v.sn_begin[J], w = v.sn_begin[J + 1] - c0;
+    const int64_t r0 = v.rows_rp[J];
+    const int nr = static_cast<int>(v.rows_rp[J + 1] - r0);
+    double* P = v.panels + v.panel_off[J];
+    for (int cb = 0; cb < w; cb += CHOL_KCHUNK) {
+        const int ce = min(cb + CHOL_KCHUNK, w);
+        for (int c = cb; c < ce; ++c) {
+            double* Pc = P + static_cast<int64_t>(c) * nr;
+            if (tid == 0) {
+                const double d = Pc[c];
+                Pc[c] = d > 0.0 ? sqrt(d) : -1.0;
+            }
+            __syncthreads();
+            const double d = Pc[c];
+            if (!(d > 0.0)) return 2;
+            const double inv = 1.0 / d;
+            for (int r = c + 1 + tid; r < nr; r += CHOL_BLOCK) Pc[r] *= inv;
+            __syncthreads();
+            for (int r = c + 1 + tid; r < nr; r += CHOL_BLOCK) {
+                const double lrc = Pc[r];
+                const int cmax = min(r, ce - 1);
+                for (int cc = c + 1; cc <= cmax; ++cc) P[static_cast<int64_t>(cc) * nr + r] -= lrc * Pc[cc];
+            }
+            __syncthreads();
+        }
+        // trailing update: columns cc >= ce, rows r >= cc, minus sum over the block's columns
+        for (int ta = ce; ta < nr; ta += CHOL_TILE)
+            for (int tb = ce; tb < w && tb < ta + CHOL_TILE; tb += CHOL_TILE) {
+                for (int e = tid; e < CHOL_KCHUNK * CHOL_TILE; e += CHOL_BLOCK) {
+                    const int k = e / CHOL_TILE, q = e - k * CHOL_TILE;
+                    const bool in = cb + k < ce;
+                    const int64_t base = static_cast<int64_t>(cb + k) * nr;
+                    As[k][q] = (in && ta + q < nr) ? P[base + ta + q] : 0.0;
+                    Bs[k][q] = (in && tb + q < w) ? P[base + tb + q] : 0.0;
+                }
+                __syncthreads();
+                double acc[4][4];
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+#pragma unroll 4
+                for (int k = 0; k < CHOL_KCHUNK; ++k) {
+                    double x[4], y[4];
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) x[i] = As[k][ty + 16 * i];
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) y[j] = Bs[k][tx + 16 * j];
+#pragma unroll
+                    for (int i = 0; i < 4; ++i)
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) acc[i][j] += x[i] * y[j];
+                }
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const int r = ta + ty + 16 * i;
+                    if (r >= nr) continue;
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        const int cc = tb + tx + 16 * j;
+                        if (cc < w && r >= cc) P[static_cast<int64_t>(cc) * nr + r] -= acc[i][j];
+                    }
+                }
+                __syncthreads();
+            }
+    }
+    return 0;
+}
+
 __global__ void __launch_bounds__(CHOL_BLOCK) k_chol_panel(SnView v, const int* __restrict__ sns, unsigned* error)
 {
-    const int st = sn_factor_panel(v, sns[blockIdx.x], threadIdx.x, blockDim.x, CtaBarrier());
+    __shared__ double As[CHOL_KCHUNK][CHOL_TILE];
+    __shared__ double Bs[CHOL_KCHUNK][CHOL_TILE];
+    const int st = chol_panel_blocked(v, sns[blockIdx.x], As, Bs);
     if (st != 0 && threadIdx.x == 0) atomicOr(error, static_cast<unsigned>(st));
 }
 
