@@ -25,6 +25,22 @@ def _few(n):
     return 2, V, S[:n].copy()
 
 
+def _long_chain():
+    # a strip of 400 small triangles along x in [0, 1] whose first triangle lies far out at
+    # x = 100: the root split moves only that one above the box centre, and the reference's
+    # in-place pass carries it along a chain of 399 swaps (the device finishes such chains by
+    # pointer jumping)
+    n = 400
+    xs = np.concatenate([[100.0], np.linspace(0.0, 1.0, n - 1)])
+    V = np.zeros((3 * n, 3))
+    for i, x in enumerate(xs):
+        V[3 * i] = (x, 0.0, 0.0)
+        V[3 * i + 1] = (x + 1e-3, 0.0, 1e-3)
+        V[3 * i + 2] = (x, 1e-3, 5e-4)
+    S = np.arange(3 * n, dtype=np.int32).reshape(n, 3)
+    return 2, V, S
+
+
 CASES = {
     "curve": lambda: (1,) + meshes.config_mesh(1, small=True)[1],
     "curve_full": lambda: (1,) + meshes.config_mesh(1)[1],
@@ -37,6 +53,7 @@ CASES = {
     "one_triangle": lambda: _few(1),
     "two_triangles": lambda: _few(2),
     "five_triangles": lambda: _few(5),
+    "long_chain": _long_chain,
 }
 
 
