@@ -68,8 +68,10 @@ const char* rpb_last_error(void);
 
 /* SimplicialMesh(V, nV, S, nS[, charges]) (src/SimplicialMesh.hpp:154-220) followed by
  * GetClusterTree()/GetBlockClusterTree() (src/SimplicialMesh.hpp:470-607): builds the
- * cluster tree and the block cluster tree on the host (frozen coordinates) and uploads
- * them. V: nV x amb_dim row-major doubles; S: nS x (dom_dim+1) row-major ints;
+ * cluster tree and the block cluster tree from the frozen coordinates on the device (on
+ * host threads if the device work fails; the same tree either way, rpb_mesh_build_info
+ * tells which) and keeps them there. V: nV x amb_dim row-major doubles; S: nS x (dom_dim+1)
+ * row-major ints;
  * charges: nV doubles or NULL (all ones). Only amb_dim = 3 and dom_dim in {1,2}. */
 rpb_status rpb_mesh_create(int dom_dim, int amb_dim, const double* V, int64_t nV, const int* S, int64_t nS,
                            const double* charges, const rpb_settings* settings, rpb_mesh** out);
